@@ -1,0 +1,447 @@
+"""Benchmark: Mpaths/s at 1080p on the procedural 1M-triangle scene.
+
+One step = one full frame of the configuration "1M-triangle procedural room,
+1920x1080, 4 spp, ReSTIR DI 32 candidates / temporal M-cap 20*M / 5 spatial
+neighbours r=30 px, A-trous 5 iterations":
+    path tracer (4 consecutive frame seeds, depth 5) -> accumulate (4 images)
+    -> ReSTIR DI (initial, temporal, spatial+shade) -> A-trous x5.
+value = W*H*spp paths per step / device time of the whole step (max over
+ranks). Multi-GPU runs are independent replicas (each rank renders its own
+frame sequence; only the timing is reduced).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints exactly one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mpaths/s at 1080p"
+UNIT = "Mpaths/s"
+WORKLOAD = "procedural-room-1M-tris-1080p-4spp-restirdi32-atrous5"
+CFG = dict(width=1920, height=1080, spp=4, max_bounces=5, di_candidates=32, di_neighbors=5, di_radius=30,
+           m_cap_factor=20, atrous_iterations=5, scene_seed=0x5EED0002, triangles=1_000_000, emitters=4096,
+           box_half=20.0, eye=(0.0, 4.0, 34.0), center=(0.0, -3.0, 0.0))
+# Algorithmic bytes (per unit): a ray record 32 B in + 16 B hit out, a BVH2
+# node (two child boxes) 64 B, a triangle (3 vertices) 36 B.
+RAY_BYTES, NODE_BYTES, TRI_BYTES = 48, 64, 36
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--width", type=int, default=CFG["width"])
+    ap.add_argument("--height", type=int, default=CFG["height"])
+    ap.add_argument("--triangles", type=int, default=CFG["triangles"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
+    return ap.parse_args()
+
+
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, x: float) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / f"{kernel}_traffic.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("dram_bytes_per_launch_full_frame:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        u = str(uuid)
+        self.device = u if u.startswith("GPU-") else f"GPU-{u}"
+        self.rows = []
+        self._stop = threading.Event()
+        self._th = None
+
+    def start(self):
+        def run():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.rows.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._th = threading.Thread(target=run, daemon=True)
+        self._th.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._th:
+            self._th.join(timeout=10)
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def build_scene(rr, args):
+    hs = rr.HostScene.procedural(seed=CFG["scene_seed"], target_triangles=args.triangles,
+                                 emissive_triangles=CFG["emitters"], box_half=CFG["box_half"])
+    return hs
+
+
+# ─────────────────────────────── reference arm ──────────────────────────────
+def cpu_frame_sample(O, rr, hs, args, budget_s: float, nthreads: int):
+    """Times the oracle (CPU restatement of the reference passes) on a centre
+    crop of the same frame (PT 4 spp + accumulate + DI + A-trous), repeating
+    until `budget_s` of work; returns (Mpaths/s, description)."""
+    import numpy as np
+    W, H = args.width, args.height
+    cw, ch = min(256, W), min(256, H)
+    x0, y0 = (W - cw) // 2, (H - ch) // 2
+    oscene = O.OracleScene(hs.arrays, use_bvh=True)
+    cam_full = rr.camera_data(rr.camera_desc(W, H, eye=CFG["eye"], center=CFG["center"]))
+    cam_crop = rr.camera_data(rr.camera_desc(cw, ch, eye=CFG["eye"], center=CFG["center"]))
+    acc = np.zeros((ch, cw, 4), np.float32)
+    z = lambda: np.zeros((ch, cw, 4), np.float32)
+    gpos, gnrm, res, prev, out = z(), z(), z(), z(), z()
+    paths = 0
+    frames = 0
+    t0 = time.perf_counter()
+    while True:
+        img, _ = O.pathtrace(oscene, cam_full, frames * CFG["spp"], CFG["max_bounces"], CFG["spp"],
+                             region=(x0, y0, cw, ch), nthreads=nthreads)
+        for k in range(CFG["spp"]):
+            O.accumulate(np.ascontiguousarray(img[k]), acc, 1 if (frames == 0 and k == 0) else 0,
+                         frames * CFG["spp"] + k)
+        p = O.di_params(frames, CFG["di_candidates"], 1, 1, CFG["di_neighbors"], CFG["di_radius"],
+                        CFG["m_cap_factor"])
+        O.restir_di_initial(oscene, cam_crop, p, gpos, gnrm, res, nthreads)
+        O.restir_di_temporal(oscene, cam_crop, p, gpos, gnrm, res, prev, nthreads)
+        O.restir_di_spatial_shade(oscene, cam_crop, p, gpos, gnrm, res, out, nthreads)
+        O.atrous(out, gpos, gnrm, CFG["atrous_iterations"])
+        res, prev = prev, res
+        paths += cw * ch * CFG["spp"]
+        frames += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    oscene.close()
+    desc = (f"oracle port, {cw}x{ch} centre crop of the 1920x1080 frame, {frames} frame(s) of PT {CFG['spp']} spp "
+            f"+ accumulate + ReSTIR DI + A-trous ({dt:.1f} s, {nthreads} threads)")
+    return paths / dt / 1e6, desc
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from research_b200 import build
+    build.build_oracle()
+    from research_b200 import rr
+    import oracle as O
+    hs = build_scene(rr, args)
+    nth = O.threads()
+    per_step = max(2.0, min(30.0, 120.0 / max(1, args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_frame_sample(O, rr, hs, args, 0.5, nth)
+    vals = []
+    descs = []
+    for _ in range(args.steps):
+        v, d = cpu_frame_sample(O, rr, hs, args, per_step, nth)
+        vals.append(v)
+        descs.append(d)
+    value = statistics.median(vals)
+    ms = args.width * args.height * CFG["spp"] / (value * 1e6) * 1e3
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_dict(args),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port", "sample": descs[-1]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(args):
+    return {"workload": WORKLOAD, "width": args.width, "height": args.height, "spp": CFG["spp"],
+            "max_bounces": CFG["max_bounces"], "triangles": args.triangles, "emissive_triangles": CFG["emitters"],
+            "restir_di": {"candidates": CFG["di_candidates"], "m_cap": CFG["m_cap_factor"] * CFG["di_candidates"],
+                          "neighbors": CFG["di_neighbors"], "radius_px": CFG["di_radius"]},
+            "atrous_iterations": CFG["atrous_iterations"], "parallelism": f"replicas{args.gpus}",
+            "l2": "per-step working set (ray queues + images) > 126 MB L2; no explicit flush"}
+
+
+# ───────────────────────────────── our arm ──────────────────────────────────
+class Frame:
+    """One config frame through the C ABI on device buffers."""
+
+    def __init__(self, rr, torch, ctx, scene, W, H):
+        self.rr, self.torch, self.ctx, self.scene = rr, torch, ctx, scene
+        self.W, self.H = W, H
+        self.L = rr.lib()
+        f = lambda *s: torch.zeros(s, device="cuda", dtype=torch.float32)
+        self.rad = f(CFG["spp"], H, W, 4)
+        self.acc = f(H, W, 4)
+        self.gpos, self.gnrm, self.out = f(H, W, 4), f(H, W, 4), f(H, W, 4)
+        self.res = [f(H, W, 4), f(H, W, 4)]
+        self.ping = [f(H, W, 4), f(H, W, 4)]
+        self.frame = 0
+        self.spp_acc = 0
+        self.slot = C.c_uint32()
+        self.desc = rr.camera_desc(W, H, eye=CFG["eye"], center=CFG["center"])
+        self.cam = rr.camera_data(self.desc)
+        self.stage_events = []
+
+    def step(self, stream, pt_flags=0, seed_base=0, stage_timing=False):
+        rr, L, ctx = self.rr, self.L, self.ctx
+        cam = self.cam
+        ev = []
+        mark = (lambda: ev.append(self.torch.cuda.Event(enable_timing=True))) if stage_timing else (lambda: None)
+        rec = (lambda: ev[-1].record()) if stage_timing else (lambda: None)
+        mark(); rec()
+        p = rr.PtParams(seed_base + self.frame * CFG["spp"], CFG["max_bounces"], CFG["spp"], pt_flags)
+        ctx.check(L.rr_pathtracer_execute(ctx.handle, self.scene.handle, C.byref(cam), C.byref(p),
+                                          self.rad.data_ptr(), stream))
+        mark(); rec()
+        ap = rr.AccParams(self.W, self.H, 1 if self.spp_acc == 0 else 0, self.spp_acc)
+        ctx.check(L.rr_accumulate_execute(ctx.handle, self.rad.data_ptr(), CFG["spp"], self.acc.data_ptr(), None,
+                                          C.byref(ap), stream))
+        self.spp_acc += CFG["spp"]
+        mark(); rec()
+        dp = rr.DIParams(seed_base + self.frame, CFG["di_candidates"], 1, 1, CFG["di_neighbors"], CFG["di_radius"],
+                         CFG["m_cap_factor"], 0)
+        cur, prev = self.res[self.frame & 1], self.res[(self.frame & 1) ^ 1]
+        ctx.check(L.rr_restir_di_execute(ctx.handle, self.scene.handle, C.byref(cam), C.byref(dp),
+                                         self.gpos.data_ptr(), self.gnrm.data_ptr(), cur.data_ptr(), prev.data_ptr(),
+                                         self.out.data_ptr(), stream))
+        mark(); rec()
+        atp = rr.AtrousParams(self.W, self.H, CFG["atrous_iterations"], 0, 0.25, 0.20, 1.0, 0)
+        ctx.check(L.rr_atrous_execute(ctx.handle, self.out.data_ptr(), self.gpos.data_ptr(), self.gnrm.data_ptr(),
+                                      self.ping[0].data_ptr(), self.ping[1].data_ptr(), C.byref(atp),
+                                      C.byref(self.slot), stream))
+        mark(); rec()
+        if stage_timing:
+            self.stage_events.append(ev)
+        self.frame += 1
+
+    def denoised(self):
+        return self.ping[self.slot.value]
+
+    def stage_ms(self):
+        self.torch.cuda.synchronize()
+        names = ["pathtracer", "accumulate", "restir_di", "atrous"]
+        tot = {n: 0.0 for n in names}
+        for ev in self.stage_events:
+            for k, n in enumerate(names):
+                tot[n] += ev[k].elapsed_time(ev[k + 1])
+        cnt = max(1, len(self.stage_events))
+        return {n: v / cnt for n, v in tot.items()}
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    from research_b200 import rr
+    torch.cuda.set_device(local)
+    ctx = rr.Context(local)
+    hs = build_scene(rr, args)
+    scene = rr.Scene(ctx, hs.arrays)
+    sst = scene.stats()
+    W, H = args.width, args.height
+    stream = torch.cuda.current_stream().cuda_stream
+    fr = Frame(rr, torch, ctx, scene, W, H)
+    seed_base = rank * 1_000_003
+
+    st = rr.PtStats()
+    # 1) warm-up
+    for _ in range(args.warmup):
+        fr.step(stream, seed_base=seed_base)
+    torch.cuda.synchronize()
+    ctx.check(rr.lib().rr_pathtracer_stats(ctx.handle, C.byref(st), 1))
+    launches0 = st.launches_total
+    # 2) timed region: K device-resident steps
+    first_timed = fr.frame
+    clocks = ClockSampler(torch.cuda.get_device_properties(local).uuid)
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        fr.step(stream, pt_flags=rr.PT_FLAG_TIME_STAGES, seed_base=seed_base, stage_timing=True)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop()
+    ms_total = e0.elapsed_time(e1)
+    ms_step = max_over_ranks(ws, ms_total / args.steps)
+    ctx.check(rr.lib().rr_pathtracer_stats(ctx.handle, C.byref(st), 1))
+    launches = st.launches_total - launches0
+    stage = fr.stage_ms()
+    pt_stage = {"raygen": st.ms_raygen / args.steps, "extend": st.ms_extend / args.steps,
+                "shade": st.ms_shade / args.steps, "shadow": st.ms_shadow / args.steps}
+    paths_per_step = W * H * CFG["spp"]
+    value = paths_per_step * ws / (ms_step * 1e-3) / 1e6
+
+    # 3) algorithmic work of the timed frames: replay the same K frame seeds
+    #    with traversal counters on (untimed; the kernels are deterministic)
+    keys = ("extension_rays", "shadow_rays", "extension_nodes", "extension_tris", "shadow_nodes", "shadow_tris")
+    counted = {k: 0 for k in keys}
+    fr.frame = first_timed
+    for _ in range(args.steps):
+        fr.step(stream, pt_flags=rr.PT_FLAG_COUNT_TRAVERSAL, seed_base=seed_base)
+        ctx.check(rr.lib().rr_pathtracer_stats(ctx.handle, C.byref(st), 1))
+        for k in keys:
+            counted[k] += getattr(st, k)
+    counted = {k: v // args.steps for k, v in counted.items()}
+
+    # 4) e2e through the public API with host buffers: the per-frame input is
+    #    the host GpuCameraData block, handed to rr_pathtracer_execute and
+    #    rr_restir_di_execute (the library forwards it in launch parameters);
+    #    the frame's results, the accumulated and the denoised images, are read
+    #    back into pinned host memory every step.
+    host_acc = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
+    host_den = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
+    h2d = 2 * C.sizeof(rr.GpuCameraData)
+    d2h = 2 * H * W * 16
+    barrier(ws)
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(args.steps):
+        fr.cam = rr.camera_data(fr.desc)
+        fr.step(stream, seed_base=seed_base)
+        host_acc.copy_(fr.acc, non_blocking=True)
+        host_den.copy_(fr.denoised(), non_blocking=True)
+    f1.record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(ws, f0.elapsed_time(f1) / args.steps)
+    e2e_value = paths_per_step * ws / (e2e_ms * 1e-3) / 1e6
+
+    # roofline of the dominant kernel (BVH traversal of extension rays)
+    peak, peak_kind = load_peaks()
+    ext_bytes = (counted["extension_rays"] * RAY_BYTES + counted["extension_nodes"] * NODE_BYTES +
+                 counted["extension_tris"] * TRI_BYTES)
+    ext_ms = pt_stage["extend"]
+    shadow_bytes = (counted["shadow_rays"] * RAY_BYTES + counted["shadow_nodes"] * NODE_BYTES +
+                    counted["shadow_tris"] * TRI_BYTES)
+    achieved = ext_bytes / (ext_ms * 1e-3) / 1e9 if ext_ms > 0 else 0.0
+    traffic = ncu_traffic("extend")
+    roofline = {"kernel": "extend_kernel (closest-hit BVH2 traversal, all bounces of one frame)", "bound": "hbm",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_step": ext_bytes, "launches_per_step": CFG["max_bounces"],
+                "shadow_achieved_gbs": shadow_bytes / (pt_stage["shadow"] * 1e-3) / 1e9 if pt_stage["shadow"] else 0}
+    rays = counted["extension_rays"] + counted["shadow_rays"]
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O
+        v, d = cpu_frame_sample(O, rr, hs, args, args.cpu_seconds, O.threads())
+        cpu = {"value": v, "unit": UNIT, "cores": O.threads(), "kind": "port", "sample": d}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+                "config": config_dict(args),
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "ms_per_step": e2e_ms},
+                "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+                "stages_ms": {**{k: round(v, 4) for k, v in stage.items()},
+                              "pt_" + "raygen": round(pt_stage["raygen"], 4),
+                              "pt_extend": round(pt_stage["extend"], 4), "pt_shade": round(pt_stage["shade"], 4),
+                              "pt_shadow": round(pt_stage["shadow"], 4)},
+                "rays_per_step": rays, "mrays_per_s": rays / (ms_step * 1e-3) / 1e6,
+                "scene": {"triangles": sst.triangle_count, "bvh_nodes": sst.bvh_node_count,
+                          "bvh_depth": sst.bvh_max_depth, "bvh_build_ms": round(sst.build_ms, 1),
+                          "lights": sst.light_count},
+                "traversal_per_step": counted}
+        print(json.dumps(line), flush=True)
+    scene.close()
+    ctx.close()
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init(args)
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+    else:
+        from research_b200 import build
+        if not (ROOT / "research_b200" / "lib" / "librr_cuda.so").exists():
+            build.build_cuda()
+        run_ours(args, ws, rank, local)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

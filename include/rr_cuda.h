@@ -1,0 +1,249 @@
+/*
+ * rr_cuda.h — C ABI of the B200 light-transport library (librr_cuda.so).
+ *
+ * Drop-in boundary for the reference renderer's hot passes. Each entry point
+ * replaces one pass's `execute` (or one compute dispatch inside it) of the
+ * reference's rr::render::RenderPass contract (src/render/RenderPass.h:11-48);
+ * the parameter structs carry the same fields as the reference push-constant
+ * blocks minus the bindless heap indices, which become typed pointers here.
+ *
+ * Conventions
+ *  - Every function returns rr_status; no exception crosses this boundary
+ *    (the reference throws std::runtime_error from initialize(); here the
+ *    caller gets RR_ERR_* and rr_last_error() text instead).
+ *  - Image buffers are caller-owned DEVICE memory, row-major RGBA32F
+ *    (4 floats per pixel), exactly like the reference's storage images.
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream). Execute calls
+ *    only enqueue work; they do not synchronise.
+ *  - The library owns the scene (geometry, BVH) and the wavefront queues.
+ *  - Camera data is passed by host pointer (GpuCameraData, 304 bytes,
+ *    GpuScene.h:80-98) and reaches the kernels as a launch parameter.
+ */
+#ifndef RR_CUDA_H
+#define RR_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "rr_layouts.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RR_ABI_VERSION 1u
+
+typedef enum rr_status {
+    RR_OK = 0,
+    RR_ERR_INVALID_ARGUMENT = 1,
+    RR_ERR_CUDA = 2,
+    RR_ERR_OUT_OF_MEMORY = 3,
+    RR_ERR_NOT_INITIALIZED = 4,
+    RR_ERR_QUEUE_OVERFLOW = 5,
+    RR_ERR_TIMEOUT = 6,
+    RR_ERR_UNSUPPORTED = 7
+} rr_status;
+
+typedef struct rr_ctx rr_ctx;
+typedef struct rr_scene rr_scene;
+
+/* ── context ─────────────────────────────────────────────────────────────
+ * Replaces the per-pass initialize(Device&, SlangSession&, BindlessRegistry&,
+ * Extent2D) plumbing (e.g. PathTracerPass.h:28-31): binds a CUDA device. */
+uint32_t    rr_abi_version(void);
+const char* rr_status_string(rr_status status);
+rr_status   rr_ctx_create(int device_ordinal, rr_ctx** out_ctx);
+rr_status   rr_ctx_destroy(rr_ctx* ctx);
+/* Copies the last error message of this context (NUL-terminated). */
+rr_status   rr_last_error(const rr_ctx* ctx, char* buf, size_t buf_size);
+
+/* ── scene ───────────────────────────────────────────────────────────────
+ * Replaces Scene::upload (Scene.cpp:255-515): copies the flat GpuScene
+ * arrays to the device and builds the acceleration structure (a binned-SAH
+ * BVH2 over world-space triangles instead of the driver BLAS/TLAS of
+ * Scene.cpp:449-507). Host arrays; the call is synchronous. */
+typedef struct rr_scene_desc {
+    const GpuVertex*   vertices;   uint32_t vertex_count;
+    const uint32_t*    indices;    uint32_t index_count;
+    const GpuMesh*     meshes;     uint32_t mesh_count;
+    const GpuMaterial* materials;  uint32_t material_count;
+    const GpuInstance* instances;  uint32_t instance_count;
+    const GpuLight*    lights;     uint32_t light_count;
+} rr_scene_desc;
+
+typedef struct rr_scene_stats {
+    uint32_t triangle_count;
+    uint32_t bvh_node_count;      /* GPU nodes (each holds two child boxes) */
+    uint32_t bvh_max_depth;
+    uint32_t light_count;
+    double   build_ms;            /* host BVH build */
+    double   upload_ms;
+    uint64_t device_bytes;
+} rr_scene_stats;
+
+rr_status rr_scene_create(rr_ctx* ctx, const rr_scene_desc* desc, rr_scene** out_scene);
+rr_status rr_scene_destroy(rr_scene* scene);
+rr_status rr_scene_get_stats(const rr_scene* scene, rr_scene_stats* out);
+
+/* ── reference path tracer: PathTracerPass::execute
+ * (PathTracerPass.cpp:170-224, kernel pathtracer.slang:181-265).
+ * PathTracerPushConstants (PathTracerPass.cpp:15-32) -> frame_seed,
+ * max_bounces; num_lights/num_instances come from the scene. `spp` > 1
+ * renders the consecutive frame seeds frame_seed .. frame_seed+spp-1 in one
+ * call (identical to spp reference frames); radiance_out holds spp images of
+ * screen_width x screen_height RGBA32F, image k for seed frame_seed+k. */
+typedef struct rr_pt_params {
+    uint32_t frame_seed;
+    uint32_t max_bounces;
+    uint32_t spp;
+    uint32_t flags;               /* RR_PT_FLAG_* */
+} rr_pt_params;
+
+/* Count BVH nodes visited and triangles tested (slower; for roofline bytes). */
+#define RR_PT_FLAG_COUNT_TRAVERSAL 1u
+/* Record CUDA events around every stage kernel on `stream`. */
+#define RR_PT_FLAG_TIME_STAGES 2u
+
+rr_status rr_pathtracer_execute(rr_ctx* ctx, const rr_scene* scene,
+                                const GpuCameraData* camera, const rr_pt_params* params,
+                                float* radiance_out, void* stream);
+
+/* Statistics of this context's path tracer (synchronises the device):
+ * ray counts of the last execute, traversal work of the last execute run
+ * with RR_PT_FLAG_COUNT_TRAVERSAL, and stage times summed over all executes
+ * run with RR_PT_FLAG_TIME_STAGES since the last reset. */
+typedef struct rr_pt_stats {
+    uint64_t extension_rays;
+    uint64_t shadow_rays;
+    uint64_t extension_nodes;     /* BVH nodes visited (each = 64 bytes) */
+    uint64_t extension_tris;      /* triangles tested */
+    uint64_t shadow_nodes;
+    uint64_t shadow_tris;
+    double   ms_raygen;
+    double   ms_extend;
+    double   ms_shade;
+    double   ms_shadow;
+    uint64_t launches_extend;     /* timed launches per stage */
+    uint64_t launches_total;      /* kernel launches issued by this context */
+} rr_pt_stats;
+
+rr_status rr_pathtracer_stats(rr_ctx* ctx, rr_pt_stats* out, int reset_times);
+
+/* ── accumulate: AccumulatePass::execute (AccumulatePass.cpp:167-218,
+ * kernel accumulate.slang:21-46). AccumulatePushConstants minus indices.
+ * Folds `image_count` consecutive radiance images into `accumulated` in
+ * order, as image_count reference frames would (the first with the given
+ * camera_moved flag). oracle_sum (nullable, double[4*W*H]) keeps the FP64
+ * per-pixel sum of every folded image (reset together with the FP32 mean),
+ * the judge buffer for RMSE; it is the only FP64 state of the path. */
+typedef struct rr_acc_params {
+    uint32_t width;
+    uint32_t height;
+    uint32_t camera_moved;
+    uint32_t accumulated_spp;     /* spp BEFORE this call */
+} rr_acc_params;
+
+rr_status rr_accumulate_execute(rr_ctx* ctx, const float* radiance, uint32_t image_count,
+                                float* accumulated, double* oracle_sum,
+                                const rr_acc_params* params, void* stream);
+
+/* ── ReSTIR DI: ReSTIRDIPass::execute (ReSTIRDIPass.cpp:306-446; kernels
+ * restir_di.slang cs_initial :186-262, cs_temporal :266-335,
+ * cs_spatial_shade :339-472). ReSTIRDIPushConstants (ReSTIRDIPass.cpp:18-45)
+ * minus indices. m_cap_factor is 20 in the reference (restir_di.slang:300).
+ * gbuf_pos/gbuf_norm/reservoir_curr/reservoir_prev/output: W x H RGBA32F. */
+typedef struct rr_di_params {
+    uint32_t frame_seed;
+    uint32_t num_initial_candidates;
+    uint32_t temporal_enable;
+    uint32_t spatial_enable;
+    uint32_t spatial_num_neighbors;
+    uint32_t spatial_radius;
+    uint32_t m_cap_factor;
+    uint32_t _pad;
+} rr_di_params;
+
+rr_status rr_restir_di_initial(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
+                               const rr_di_params* params, float* gbuf_pos, float* gbuf_norm,
+                               float* reservoir_curr, void* stream);
+rr_status rr_restir_di_temporal(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
+                                const rr_di_params* params, const float* gbuf_pos,
+                                const float* gbuf_norm, float* reservoir_curr,
+                                const float* reservoir_prev, void* stream);
+rr_status rr_restir_di_spatial_shade(rr_ctx* ctx, const rr_scene* scene,
+                                     const GpuCameraData* camera, const rr_di_params* params,
+                                     const float* gbuf_pos, const float* gbuf_norm,
+                                     const float* reservoir_curr, float* output, void* stream);
+/* The three dispatches in order (one ReSTIRDIPass::execute). */
+rr_status rr_restir_di_execute(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
+                               const rr_di_params* params, float* gbuf_pos, float* gbuf_norm,
+                               float* reservoir_curr, const float* reservoir_prev,
+                               float* output, void* stream);
+
+/* ── A-trous denoiser: AtrousPass (AtrousPass.cpp:243-306, kernel
+ * atrous.slang:41-106). rr_atrous_iteration is one cs_main dispatch with
+ * AtrousPushConstants (AtrousPass.cpp:18-34); rr_atrous_execute runs
+ * `iterations` (clamped to 1..7) ping-ponging ping0/ping1 with stride 1<<i
+ * and reports which buffer holds the result ((iterations-1) & 1). */
+typedef struct rr_atrous_params {
+    uint32_t width;
+    uint32_t height;
+    uint32_t iterations;          /* execute: count; iteration: index */
+    uint32_t stride;              /* iteration only */
+    float    sigma_position;
+    float    sigma_normal;
+    float    sigma_luminance;
+    uint32_t _pad;
+} rr_atrous_params;
+
+rr_status rr_atrous_iteration(rr_ctx* ctx, const float* input, const float* gbuf_pos,
+                              const float* gbuf_norm, float* output,
+                              const rr_atrous_params* params, void* stream);
+rr_status rr_atrous_execute(rr_ctx* ctx, const float* input, const float* gbuf_pos,
+                            const float* gbuf_norm, float* ping0, float* ping1,
+                            const rr_atrous_params* params, uint32_t* out_slot, void* stream);
+
+/* ── vMF path-guiding grid (GuidingGrid.slang; host side
+ * ReSTIRPTPass.cpp:311-341, 602-611, 784-810; params ReSTIRPTPass.h:93-100).
+ * accum: int32[4*cell_count] fixed-point sums (x, y, z, count);
+ * fitted: float[4*cell_count] (mu.xyz, kappa). Points are float4 arrays. */
+typedef struct rr_guiding_params {
+    float    base_cell_size;      /* 0.10 */
+    float    distance_slope;      /* 0.02 */
+    uint32_t cell_count;          /* 1 << 20 */
+    uint32_t enabled;
+    uint32_t min_samples;         /* 8 */
+    float    kappa_max;           /* 512 */
+    float    alpha;               /* 0.5, P(guided sample) */
+    uint32_t _pad;
+} rr_guiding_params;
+
+/* guiding_splat at the call site restir_pt.slang:982-994: one direction per
+ * point into the cell of (pos, bsdf_id). */
+rr_status rr_guiding_splat(rr_ctx* ctx, int32_t* accum, const float* pos, const float* dir,
+                           const uint32_t* bsdf_id, uint32_t count, const float camera_pos[3],
+                           const rr_guiding_params* params, void* stream);
+/* cs_fit_guiding (restir_pt.slang:1005-1015): fit every cell, reset accum. */
+rr_status rr_guiding_fit(rr_ctx* ctx, int32_t* accum, float* fitted,
+                         const rr_guiding_params* params, void* stream);
+/* sample_primary_dir (restir_pt.slang:520-563) at `count` points; seeds are
+ * advanced in place; wi_out float4, pdf_out float. */
+rr_status rr_guiding_sample(rr_ctx* ctx, const float* fitted, const float* pos,
+                            const float* normal, const uint32_t* bsdf_id, uint32_t* seeds,
+                            uint32_t count, const float camera_pos[3],
+                            const rr_guiding_params* params, float* wi_out, float* pdf_out,
+                            void* stream);
+/* Host-side grid reset of ReSTIRPTPass.cpp:602-611 (zero accum and fitted). */
+rr_status rr_guiding_reset(rr_ctx* ctx, int32_t* accum, float* fitted,
+                           const rr_guiding_params* params, void* stream);
+
+/* ── ray queries (checking and tooling) ─────────────────────────────────
+ * Closest hit for `count` rays: origins/dirs float4, hits float4
+ * (t, u, v, as_float(instance)) and prims uint32; instance 0xffffffff = miss. */
+rr_status rr_trace_closest(rr_ctx* ctx, const rr_scene* scene, const float* origins,
+                           const float* dirs, float tmin, float tmax, uint32_t count,
+                           float* hits, uint32_t* prims, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RR_CUDA_H */

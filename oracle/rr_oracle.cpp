@@ -1,0 +1,1043 @@
+// rr_oracle.cpp — CPU checker (test infrastructure only; see rr_oracle.h).
+//
+// A scalar restatement of the reference's Slang light-transport kernels.
+// Paths in citations are relative to the reference project root; shader
+// files live under assets/shaders/. Expression order follows the Slang source
+// so that binary32 results are reproducible; compile with -ffp-contract=off.
+
+#include "rr_oracle.h"
+#include "rr_detmath.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+namespace {
+
+// ── float3 / float4 shim with HLSL semantics ──────────────────────────────
+
+struct V3 { float x, y, z; };
+struct V4 { float x, y, z, w; };
+
+inline V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+inline V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+inline V3 operator*(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+inline V3 operator*(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
+inline V3 operator*(float s, V3 a) { return v3(s * a.x, s * a.y, s * a.z); }
+inline V3 operator/(V3 a, float s) { return v3(a.x / s, a.y / s, a.z / s); }
+inline V3 operator/(V3 a, V3 b) { return v3(a.x / b.x, a.y / b.y, a.z / b.z); }
+inline V3 operator-(V3 a) { return v3(-a.x, -a.y, -a.z); }
+inline float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline float length(V3 a) { return sqrtf(dot(a, a)); }
+inline V3 normalize(V3 a) { const float inv = 1.0f / sqrtf(dot(a, a)); return a * inv; }
+inline V3 cross(V3 a, V3 b) {
+    return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+inline float fmaxs(float a, float b) { return a > b ? a : b; }  // max(a,b), no NaN
+inline float fmins(float a, float b) { return a < b ? a : b; }
+inline float clampf(float x, float lo, float hi) { return fmins(fmaxs(x, lo), hi); }
+// HLSL lerp(x, y, s) = x + s * (y - x)
+inline V3 lerp(V3 a, V3 b, float t) { return a + (b - a) * t; }
+inline V3 reflect(V3 i, V3 n) { const float d2 = 2.0f * dot(i, n); return i - n * d2; }
+inline V3 load3(const float* p) { return v3(p[0], p[1], p[2]); }
+
+// mul(M, v) for a row-major float4x4 (Scene.cpp:87-90)
+inline V4 mul44(const float* M, V4 v) {
+    V4 r;
+    r.x = M[0] * v.x + M[1] * v.y + M[2] * v.z + M[3] * v.w;
+    r.y = M[4] * v.x + M[5] * v.y + M[6] * v.z + M[7] * v.w;
+    r.z = M[8] * v.x + M[9] * v.y + M[10] * v.z + M[11] * v.w;
+    r.w = M[12] * v.x + M[13] * v.y + M[14] * v.z + M[15] * v.w;
+    return r;
+}
+// mul((float3x3)M, v)
+inline V3 mul33(const float* M, V3 v) {
+    return v3(M[0] * v.x + M[1] * v.y + M[2] * v.z,
+              M[4] * v.x + M[5] * v.y + M[6] * v.z,
+              M[8] * v.x + M[9] * v.y + M[10] * v.z);
+}
+
+inline float asfloat(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
+inline uint32_t asuint(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+
+// ── constants (BRDF.slang:8-11) ────────────────────────────────────────────
+constexpr float kPi      = 3.14159265358979323846f;
+constexpr float kTwoPi   = 6.28318530717958647692f;
+constexpr float kInvPi   = 0.31830988618379067154f;
+constexpr float kEpsilon = 1e-4f;
+
+// ── RNG (Common.slang:18-28; Sampling.slang:11-30) ────────────────────────
+inline uint32_t pcg_hash(uint32_t seed) {
+    uint32_t state = seed * 747796405u + 2891336453u;
+    uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+    return (word >> 22u) ^ word;
+}
+inline float uint_to_float01(uint32_t v) { return float(v >> 8) * (1.0f / float(1u << 24)); }
+inline float rand_float(uint32_t& seed) { seed = pcg_hash(seed); return uint_to_float01(seed); }
+inline uint32_t make_seed(uint32_t px, uint32_t py, uint32_t frame) {
+    uint32_t h = px ^ (py * 1000003u) ^ (frame * 2654435761u);
+    return pcg_hash(h);
+}
+
+// ── Sampling.slang:37-85 ───────────────────────────────────────────────────
+inline V3 sample_cosine_hemisphere(float u0, float u1, float& pdf) {
+    float r = sqrtf(u0);
+    float phi = 6.28318530717958647692f * u1;
+    float x = r * rr_cosf(phi);
+    float y = r * rr_sinf(phi);
+    float z = sqrtf(fmaxs(0.0f, 1.0f - u0));
+    pdf = z * 0.31830988618379067154f;
+    return v3(x, y, z);
+}
+inline void build_onb(V3 n, V3& T, V3& B) {
+    V3 up = (fabsf(n.x) < 0.9f) ? v3(1.0f, 0.0f, 0.0f) : v3(0.0f, 1.0f, 0.0f);
+    T = normalize(cross(up, n));
+    B = cross(n, T);
+}
+inline V3 tangent_to_world(V3 v, V3 T, V3 B, V3 N) { return v.x * T + v.y * B + v.z * N; }
+inline V3 world_to_tangent(V3 v, V3 T, V3 B, V3 N) { return v3(dot(v, T), dot(v, B), dot(v, N)); }
+
+// ── BRDF.slang:16-187 ──────────────────────────────────────────────────────
+inline V3 fresnel_schlick(float cos_theta, V3 F0) {           // BRDF.slang:16-21
+    float x = clampf(1.0f - cos_theta, 0.0f, 1.0f);
+    float x2 = x * x;
+    float p = x2 * x2 * x;
+    return v3(F0.x + (1.0f - F0.x) * p, F0.y + (1.0f - F0.y) * p, F0.z + (1.0f - F0.z) * p);
+}
+inline float distribution_ggx(float NdotH, float alpha) {     // BRDF.slang:25-30
+    float a2 = alpha * alpha;
+    float d = NdotH * NdotH * (a2 - 1.0f) + 1.0f;
+    return a2 / fmaxs(kPi * d * d, kEpsilon);
+}
+inline float geometry_smith_ggx(float NdotV, float NdotL, float alpha) {  // :34-40
+    float k = alpha * 0.5f;
+    float gv = NdotV / fmaxs(NdotV * (1.0f - k) + k, kEpsilon);
+    float gl = NdotL / fmaxs(NdotL * (1.0f - k) + k, kEpsilon);
+    return gv * gl;
+}
+inline V3 brdf_specular_ggx(V3 n, V3 wo, V3 wi, V3 F0, float roughness) {  // :44-59
+    float alpha = roughness * roughness;
+    V3 h = normalize(wo + wi);
+    float NdotH = fmaxs(dot(n, h), 0.0f);
+    float NdotV = fmaxs(dot(n, wo), 0.0f);
+    float NdotL = fmaxs(dot(n, wi), 0.0f);
+    float VdotH = fmaxs(dot(wo, h), 0.0f);
+    V3 F = fresnel_schlick(VdotH, F0);
+    float D = distribution_ggx(NdotH, alpha);
+    float G = geometry_smith_ggx(NdotV, NdotL, alpha);
+    float DG = D * G;
+    float den = fmaxs(4.0f * NdotV * NdotL, kEpsilon);
+    return v3((DG * F.x) / den, (DG * F.y) / den, (DG * F.z) / den);
+}
+inline V3 brdf_eval(V3 n, V3 wo, V3 wi, V3 base, float metallic, float roughness) {  // :71-83
+    float r = clampf(roughness, 0.04f, 1.0f);
+    V3 F0 = lerp(v3(0.04f, 0.04f, 0.04f), base, metallic);
+    V3 kS = fresnel_schlick(fmaxs(dot(n, wo), 0.0f), F0);
+    float om = 1.0f - metallic;
+    V3 kD = v3((1.0f - kS.x) * om, (1.0f - kS.y) * om, (1.0f - kS.z) * om);
+    V3 lam = base * kInvPi;
+    V3 diffuse = kD * lam;
+    V3 specular = brdf_specular_ggx(n, wo, wi, F0, r);
+    return diffuse + specular;
+}
+inline V3 sample_ggx_vndf(V3 wo, float roughness, float u0, float u1) {  // :87-108
+    float alpha = roughness * roughness;
+    V3 Vh = normalize(v3(alpha * wo.x, alpha * wo.y, wo.z));
+    float lensq = Vh.x * Vh.x + Vh.y * Vh.y;
+    V3 T1;
+    if (lensq > 0.0f) { float s = sqrtf(lensq); T1 = v3(-Vh.y / s, Vh.x / s, 0.0f / s); }
+    else T1 = v3(1.0f, 0.0f, 0.0f);
+    V3 T2 = cross(Vh, T1);
+    float r2 = sqrtf(u0);
+    float phi = kTwoPi * u1;
+    float t1 = r2 * rr_cosf(phi);
+    float t2 = r2 * rr_sinf(phi);
+    float s = 0.5f * (1.0f + Vh.z);
+    t2 = (1.0f - s) * sqrtf(1.0f - t1 * t1) + s * t2;
+    float sq = sqrtf(fmaxs(0.0f, 1.0f - t1 * t1 - t2 * t2));
+    V3 Nh = t1 * T1 + t2 * T2 + sq * Vh;
+    return normalize(v3(alpha * Nh.x, alpha * Nh.y, fmaxs(0.0f, Nh.z)));
+}
+// BRDF.slang:116-172. Returns f; writes wi and pdf.
+inline V3 brdf_sample(V3 wo, V3 n, V3 base, float metallic, float roughness,
+                      float ux, float uy, V3& wi, float& pdf) {
+    float r = clampf(roughness, 0.04f, 1.0f);
+    V3 F0 = lerp(v3(0.04f, 0.04f, 0.04f), base, metallic);
+    V3 kS_approx = fresnel_schlick(fmaxs(dot(n, wo), 0.0f), F0);
+    float p_spec = (kS_approx.x + kS_approx.y + kS_approx.z) / 3.0f;
+    p_spec = clampf(p_spec, 0.1f, 0.9f);
+    V3 T, B;
+    build_onb(n, T, B);
+    V3 wo_local = world_to_tangent(wo, T, B, n);
+    V3 wi_local;
+    if (ux < p_spec) {
+        float u2x = ux / p_spec;
+        V3 h_local = sample_ggx_vndf(wo_local, r, u2x, uy);
+        wi_local = reflect(-wo_local, h_local);
+        if (wi_local.z <= 0.0f) { wi = v3(0.0f, 1.0f, 0.0f); pdf = 1.0f; return v3(0.0f, 0.0f, 0.0f); }
+        // pdf_local of the chosen lobe is recomputed below for the mixture.
+    } else {
+        float u2x = (ux - p_spec) / (1.0f - p_spec);
+        float pdf_local;
+        wi_local = sample_cosine_hemisphere(u2x, uy, pdf_local);
+    }
+    wi = tangent_to_world(wi_local, T, B, n);
+    float NdotWI = fmaxs(wi_local.z, 0.0f);
+    V3 h = normalize(wo_local + wi_local);
+    float NdotH = fmaxs(h.z, 1e-6f);
+    float VdotH = fmaxs(dot(wo_local, h), 1e-6f);
+    float D = distribution_ggx(NdotH, r * r);
+    float pdf_spec_lobe = D * NdotH / fmaxs(4.0f * VdotH, 1e-6f);
+    float pdf_diff_lobe = NdotWI * kInvPi;
+    pdf = p_spec * pdf_spec_lobe + (1.0f - p_spec) * pdf_diff_lobe;
+    pdf = fmaxs(pdf, 1e-6f);
+    return brdf_eval(n, wo, wi, base, metallic, roughness);
+}
+inline float brdf_pdf(V3 wo, V3 wi, V3 n, float roughness) {  // BRDF.slang:176-187
+    float r = clampf(roughness, 0.04f, 1.0f);
+    V3 h = normalize(wo + wi);
+    float NdotH = fmaxs(dot(n, h), 1e-6f);
+    float VdotH = fmaxs(dot(wo, h), 1e-6f);
+    float NdotL = fmaxs(dot(n, wi), 0.0f);
+    float D = distribution_ggx(NdotH, r * r);
+    float pdf_spec = D * NdotH / fmaxs(4.0f * VdotH, 1e-6f);
+    float pdf_diff = NdotL * kInvPi;
+    return 0.5f * pdf_spec + 0.5f * pdf_diff;
+}
+
+inline V3 sky(V3 dir) {  // pathtracer.slang:216-217
+    float t = 0.5f * (dir.y + 1.0f);
+    return lerp(v3(0.1f, 0.1f, 0.1f), v3(0.2f, 0.3f, 0.5f), t);
+}
+
+// ── Ray/triangle: watertight test (Woop, Benthin, Wald, JCGT 2013) ─────────
+struct RayPre {
+    V3 o, d;
+    int kx, ky, kz;
+    float Sx, Sy, Sz;
+    V3 inv;  // for box tests
+};
+inline float comp(V3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+inline RayPre ray_pre(V3 o, V3 d) {
+    RayPre r;
+    r.o = o; r.d = d;
+    int kz = 0;
+    if (fabsf(d.y) > fabsf(comp(d, kz))) kz = 1;
+    if (fabsf(d.z) > fabsf(comp(d, kz))) kz = 2;
+    int kx = kz + 1; if (kx == 3) kx = 0;
+    int ky = kx + 1; if (ky == 3) ky = 0;
+    if (comp(d, kz) < 0.0f) std::swap(kx, ky);
+    r.kx = kx; r.ky = ky; r.kz = kz;
+    r.Sx = comp(d, kx) / comp(d, kz);
+    r.Sy = comp(d, ky) / comp(d, kz);
+    r.Sz = 1.0f / comp(d, kz);
+    auto safe = [](float x) { return fabsf(x) < 1e-20f ? copysignf(1e-20f, x) : x; };
+    r.inv = v3(1.0f / safe(d.x), 1.0f / safe(d.y), 1.0f / safe(d.z));
+    return r;
+}
+// Returns true and t, (bu, bv) = weights of v1, v2 when the ray hits the
+// triangle with tmin <= t <= tmax. Two-sided (AccelStructure.cpp:90 disables
+// facing culling for every instance).
+inline bool intersect_tri(const RayPre& r, V3 p0, V3 p1, V3 p2, float tmin, float tmax,
+                          float& t, float& bu, float& bv) {
+    V3 A = p0 - r.o, B = p1 - r.o, C = p2 - r.o;
+    const float Az0 = comp(A, r.kz), Bz0 = comp(B, r.kz), Cz0 = comp(C, r.kz);
+    const float Ax = comp(A, r.kx) - r.Sx * Az0, Ay = comp(A, r.ky) - r.Sy * Az0;
+    const float Bx = comp(B, r.kx) - r.Sx * Bz0, By = comp(B, r.ky) - r.Sy * Bz0;
+    const float Cx = comp(C, r.kx) - r.Sx * Cz0, Cy = comp(C, r.ky) - r.Sy * Cz0;
+    const float U = Cx * By - Cy * Bx;
+    const float V = Ax * Cy - Ay * Cx;
+    const float W = Bx * Ay - By * Ax;
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    const float det = U + V + W;
+    if (det == 0.0f) return false;
+    const float Az = r.Sz * Az0, Bz = r.Sz * Bz0, Cz = r.Sz * Cz0;
+    const float T = U * Az + V * Bz + W * Cz;
+    const float rcp = 1.0f / det;
+    const float tt = T * rcp;
+    if (!(tt >= tmin && tt <= tmax)) return false;
+    t = tt; bu = V * rcp; bv = W * rcp;
+    return true;
+}
+
+// ── Scene ──────────────────────────────────────────────────────────────────
+struct Tri { V3 p0, p1, p2; uint32_t inst, prim; };
+struct BNode { float lo[3], hi[3]; int left, right; uint32_t first, count; };
+
+} // namespace
+
+struct OracleScene {
+    std::vector<GpuVertex> vertices;
+    std::vector<uint32_t> indices;
+    std::vector<GpuMesh> meshes;
+    std::vector<GpuMaterial> materials;
+    std::vector<GpuInstance> instances;
+    std::vector<GpuLight> lights;
+    std::vector<Tri> tris;           // world space, instance-major (key = index)
+    std::vector<uint32_t> order;     // BVH leaf order -> tri index
+    std::vector<BNode> nodes;
+    bool use_bvh = false;
+};
+
+namespace {
+
+void bounds_of(const Tri& t, float lo[3], float hi[3]) {
+    const V3 ps[3] = {t.p0, t.p1, t.p2};
+    for (int a = 0; a < 3; ++a) { lo[a] = INFINITY; hi[a] = -INFINITY; }
+    for (const V3& p : ps)
+        for (int a = 0; a < 3; ++a) {
+            float c = comp(p, a);
+            lo[a] = std::min(lo[a], c); hi[a] = std::max(hi[a], c);
+        }
+}
+
+// Median-split BVH over triangle centroids (independent of the product's
+// binned-SAH builder; only its closest-hit answers are compared).
+int build_node(OracleScene& s, uint32_t first, uint32_t count, std::vector<float>& cent) {
+    BNode n;
+    for (int a = 0; a < 3; ++a) { n.lo[a] = INFINITY; n.hi[a] = -INFINITY; }
+    float clo[3] = {INFINITY, INFINITY, INFINITY}, chi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t i = first; i < first + count; ++i) {
+        float lo[3], hi[3];
+        bounds_of(s.tris[s.order[i]], lo, hi);
+        for (int a = 0; a < 3; ++a) {
+            n.lo[a] = std::min(n.lo[a], lo[a]); n.hi[a] = std::max(n.hi[a], hi[a]);
+            float c = cent[s.order[i] * 3 + a];
+            clo[a] = std::min(clo[a], c); chi[a] = std::max(chi[a], c);
+        }
+    }
+    const int idx = (int)s.nodes.size();
+    s.nodes.push_back(n);
+    if (count <= 4) {
+        s.nodes[idx].left = s.nodes[idx].right = -1;
+        s.nodes[idx].first = first; s.nodes[idx].count = count;
+        return idx;
+    }
+    int axis = 0;
+    for (int a = 1; a < 3; ++a) if (chi[a] - clo[a] > chi[axis] - clo[axis]) axis = a;
+    const uint32_t mid = first + count / 2;
+    std::nth_element(s.order.begin() + first, s.order.begin() + mid, s.order.begin() + first + count,
+                     [&](uint32_t a, uint32_t b) {
+                         float ca = cent[a * 3 + axis], cb = cent[b * 3 + axis];
+                         return ca < cb || (ca == cb && a < b);
+                     });
+    int l = build_node(s, first, mid - first, cent);
+    int r = build_node(s, mid, first + count - mid, cent);
+    s.nodes[idx].left = l; s.nodes[idx].right = r;
+    s.nodes[idx].first = 0; s.nodes[idx].count = 0;
+    return idx;
+}
+
+// Conservative slab test (Ize, "Robust BVH ray traversal", JCGT 2013): the
+// far distance is widened by 1 + 2*gamma(3) so rounding never culls a box
+// that holds a hit.
+inline bool box_hit(const RayPre& r, const float lo[3], const float hi[3], float tmin, float tmax) {
+    float tn = tmin, tf = tmax;
+    const float o[3] = {r.o.x, r.o.y, r.o.z}, inv[3] = {r.inv.x, r.inv.y, r.inv.z};
+    float bn = -INFINITY, bf = INFINITY;
+    for (int a = 0; a < 3; ++a) {
+        float t0 = (lo[a] - o[a]) * inv[a];
+        float t1 = (hi[a] - o[a]) * inv[a];
+        bn = std::max(bn, std::min(t0, t1));
+        bf = std::min(bf, std::max(t0, t1));
+    }
+    bf = bf * 1.0000006f;
+    tn = std::max(tn, bn); tf = std::min(tf, bf);
+    return tn <= tf;
+}
+
+struct Hit { bool hit; float t, u, v; uint32_t key; };
+
+// Closest hit; ties on t resolve to the lowest (instance, primitive).
+template <bool AnyHit>
+Hit trace_scene(const OracleScene& s, V3 o, V3 d, float tmin, float tmax) {
+    Hit best{false, tmax, 0.0f, 0.0f, 0xffffffffu};
+    const RayPre r = ray_pre(o, d);
+    auto test = [&](uint32_t key) -> bool {
+        const Tri& tr = s.tris[key];
+        float t, u, v;
+        if (intersect_tri(r, tr.p0, tr.p1, tr.p2, tmin, best.t, t, u, v)) {
+            if (!best.hit || t < best.t || (t == best.t && key < best.key)) {
+                best.hit = true; best.t = t; best.u = u; best.v = v; best.key = key;
+            }
+            return true;
+        }
+        return false;
+    };
+    if (!s.use_bvh) {
+        for (uint32_t k = 0; k < (uint32_t)s.tris.size(); ++k)
+            if (test(k) && AnyHit) return best;
+        return best;
+    }
+    if (s.nodes.empty()) return best;
+    int stack[128];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        const BNode& n = s.nodes[stack[--sp]];
+        if (!box_hit(r, n.lo, n.hi, tmin, best.t)) continue;
+        if (n.left < 0) {
+            for (uint32_t i = n.first; i < n.first + n.count; ++i)
+                if (test(s.order[i]) && AnyHit) return best;
+        } else {
+            stack[sp++] = n.right;
+            stack[sp++] = n.left;
+        }
+    }
+    return best;
+}
+
+// Hit attributes (pathtracer.slang:69-118).
+struct Surf { V3 pos, normal; uint32_t material; };
+Surf hit_surface(const OracleScene& s, const Hit& h) {
+    const Tri& tr = s.tris[h.key];
+    const GpuInstance& inst = s.instances[tr.inst];
+    const GpuMesh& mesh = s.meshes[inst.mesh_index];
+    const uint32_t base = mesh.index_byte_offset / 4u + tr.prim * 3u;
+    const uint32_t i0 = s.indices[base], i1 = s.indices[base + 1], i2 = s.indices[base + 2];
+    const GpuVertex& v0 = s.vertices[mesh.vertex_base + i0];
+    const GpuVertex& v1 = s.vertices[mesh.vertex_base + i1];
+    const GpuVertex& v2 = s.vertices[mesh.vertex_base + i2];
+    V3 b3 = v3(1.0f - h.u - h.v, h.u, h.v);
+    V3 lp = b3.x * load3(v0.pos) + b3.y * load3(v1.pos) + b3.z * load3(v2.pos);
+    V3 ln = normalize(b3.x * load3(v0.normal) + b3.y * load3(v1.normal) + b3.z * load3(v2.normal));
+    V4 wp = mul44(inst.transform, V4{lp.x, lp.y, lp.z, 1.0f});
+    V3 wn = normalize(mul33(inst.transform, ln));
+    return Surf{v3(wp.x, wp.y, wp.z), wn, mesh.material_index};
+}
+
+// Primary ray (pathtracer.slang:192-205; restir_di.slang:196-206).
+void primary_ray(const GpuCameraData& cam, uint32_t px, uint32_t py, float jx, float jy,
+                 V3& o, V3& d) {
+    float ndcx = (float(px) + jx) / float(cam.screen_width) * 2.0f - 1.0f;
+    float ndcy = (float(py) + jy) / float(cam.screen_height) * 2.0f - 1.0f;
+    V4 rv = mul44(cam.inv_proj, V4{ndcx, ndcy, 1.0f, 1.0f});
+    rv.z = -1.0f; rv.w = 0.0f;
+    V4 rw = mul44(cam.inv_view, rv);
+    d = normalize(v3(rw.x, rw.y, rw.z));
+    o = load3(cam.position);
+}
+
+template <class F>
+void parallel_rows(uint32_t rows, int threads, F&& fn) {
+    if (threads <= 1 || rows < 2) { for (uint32_t y = 0; y < rows; ++y) fn(y); return; }
+    std::atomic<uint32_t> next{0};
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t)
+        pool.emplace_back([&]() { for (uint32_t y; (y = next.fetch_add(1)) < rows;) fn(y); });
+    for (auto& th : pool) th.join();
+}
+
+// NEE (pathtracer.slang:124-177)
+V3 sample_lights(const OracleScene& s, V3 hit_pos, V3 normal, V3 wo, const GpuMaterial& mat,
+                 uint32_t& seed, uint64_t& shadow_rays) {
+    const uint32_t N = (uint32_t)s.lights.size();
+    if (N == 0) return v3(0, 0, 0);
+    uint32_t light_idx = uint32_t(rand_float(seed) * float(N)) % N;
+    const GpuLight& light = s.lights[light_idx];
+    V3 light_dir; float dist; float pdf_light;
+    if (light.type == 0) {
+        V3 to_light = load3(light.position) - hit_pos;
+        dist = length(to_light);
+        light_dir = to_light / dist;
+        float r2 = dist * dist;
+        pdf_light = r2;
+    } else {
+        light_dir = normalize(-load3(light.direction));
+        dist = 1e9f;
+        pdf_light = 1.0f;
+    }
+    if (dot(light_dir, normal) <= 0.0f) return v3(0, 0, 0);
+    ++shadow_rays;
+    Hit sh = trace_scene<true>(s, hit_pos + normal * 1e-4f, light_dir, 0.001f, dist - 0.01f);
+    if (sh.hit) return v3(0, 0, 0);
+    V3 brdf_val = brdf_eval(normal, wo, light_dir, load3(mat.base_color), mat.metallic, mat.roughness);
+    float n_dot_l = fmaxs(dot(normal, light_dir), 0.0f);
+    float denom = light.type == 0 ? (pdf_light + 1e-6f) : 1.0f;
+    V3 irradiance = v3(light.emission[0] * light.intensity / denom,
+                       light.emission[1] * light.intensity / denom,
+                       light.emission[2] * light.intensity / denom);
+    float mis_weight = 1.0f;
+    if (light.type != 0) {
+        float pdf_bsdf = brdf_pdf(wo, light_dir, normal, mat.roughness);
+        mis_weight = (pdf_light * pdf_light) / (pdf_light * pdf_light + pdf_bsdf * pdf_bsdf + 1e-10f);
+    }
+    V3 r = brdf_val * irradiance;
+    r = r * n_dot_l;
+    r = r * mis_weight;
+    return r * float(N);
+}
+
+inline bool any_positive(const float* e) { return e[0] > 0.0f || e[1] > 0.0f || e[2] > 0.0f; }
+
+// pathtracer.slang:181-265 for one pixel and one frame seed.
+V3 trace_path(const OracleScene& s, const GpuCameraData& cam, uint32_t px, uint32_t py,
+              uint32_t frame_seed, uint32_t max_bounces, uint64_t& ext, uint64_t& shd) {
+    uint32_t seed = make_seed(px, py, frame_seed);
+    float jx = rand_float(seed);
+    float jy = rand_float(seed);
+    V3 ray_orig, ray_dir;
+    primary_ray(cam, px, py, jx, jy, ray_orig, ray_dir);
+    V3 radiance = v3(0, 0, 0), throughput = v3(1, 1, 1);
+    for (uint32_t bounce = 0; bounce < max_bounces; ++bounce) {
+        ++ext;
+        Hit h = trace_scene<false>(s, ray_orig, ray_dir, 0.001f, 1e9f);
+        if (!h.hit) { radiance = radiance + throughput * sky(ray_dir); break; }
+        Surf sf = hit_surface(s, h);
+        const GpuMaterial& mat = s.materials[sf.material];
+        if (any_positive(mat.emissive)) { radiance = radiance + throughput * load3(mat.emissive); break; }
+        V3 wo = -ray_dir;
+        V3 n = sf.normal;
+        if (dot(n, wo) < 0.0f) n = -n;
+        radiance = radiance + throughput * sample_lights(s, sf.pos, n, wo, mat, seed, shd);
+        float u0 = rand_float(seed);
+        float u1 = rand_float(seed);
+        V3 wi; float pdf;
+        V3 f = brdf_sample(wo, n, load3(mat.base_color), mat.metallic, mat.roughness, u0, u1, wi, pdf);
+        if (pdf < 1e-6f) break;
+        float n_dot_wi = fmaxs(dot(n, wi), 0.0f);
+        throughput = throughput * ((f * n_dot_wi) / pdf);
+        if (bounce >= 3) {
+            float survive = fmins(fmaxs(throughput.x, fmaxs(throughput.y, throughput.z)), 0.95f);
+            if (rand_float(seed) > survive) break;
+            throughput = throughput / survive;
+        }
+        ray_orig = sf.pos + n * 1e-4f;
+        ray_dir = wi;
+    }
+    return radiance;
+}
+
+// ── ReSTIR DI helpers (restir_di.slang:57-178) ────────────────────────────
+inline void pack_reservoir(float* out, uint32_t sel, float w_sum, float W, uint32_t M) {
+    out[0] = asfloat(sel); out[1] = w_sum; out[2] = W; out[3] = asfloat(M);
+}
+float compute_p_hat(const OracleScene& s, uint32_t light_idx, V3 hit_pos, V3 normal) {
+    if (light_idx >= (uint32_t)s.lights.size()) return 0.0f;
+    const GpuLight& light = s.lights[light_idx];
+    V3 l, irr;
+    if (light.type == 0) {
+        V3 to = load3(light.position) - hit_pos;
+        float d2 = fmaxs(dot(to, to), 1e-6f);
+        l = normalize(to);
+        irr = v3(light.emission[0] * light.intensity / d2, light.emission[1] * light.intensity / d2,
+                 light.emission[2] * light.intensity / d2);
+    } else {
+        l = normalize(-load3(light.direction));
+        irr = load3(light.emission) * light.intensity;
+    }
+    float n_dot_l = fmaxs(dot(normal, l), 0.0f);
+    float lum = 0.2126f * irr.x + 0.7152f * irr.y + 0.0722f * irr.z;
+    return n_dot_l * lum;
+}
+
+// A-trous (atrous.slang:21-39)
+inline float luminance601(V3 c) { return dot(c, v3(0.299f, 0.587f, 0.114f)); }
+inline float kernel_weight(int offset) {
+    switch (offset) { case -2: case 2: return 1.0f; case -1: case 1: return 4.0f; default: return 6.0f; }
+}
+
+// GuidingGrid.slang:54-67
+uint32_t cell_index(V3 p, uint32_t bsdf_id, V3 cam, const OracleGuidingParams& gp) {
+    float view_dist = length(p - cam);
+    float cell = fmaxs(gp.base_cell_size + gp.distance_slope * view_dist, 1.0e-4f);
+    int qx = (int)floorf(p.x / cell), qy = (int)floorf(p.y / cell), qz = (int)floorf(p.z / cell);
+    uint32_t h = pcg_hash((uint32_t)qx * 73856093u ^ (uint32_t)qy * 19349663u ^
+                          (uint32_t)qz * 83492791u ^ bsdf_id * 2654435761u);
+    return h % std::max(gp.cell_count, 1u);
+}
+// GuidingGrid.slang:160-189
+V3 vmf_sample(V3 mu, float kappa, float ux, float uy, float& pdf) {
+    float k = fmaxs(kappa, 1.0e-3f);
+    float w = 1.0f + (1.0f / k) * rr_logf(ux + (1.0f - ux) * rr_expf(-2.0f * k));
+    w = clampf(w, -1.0f, 1.0f);
+    float s = sqrtf(fmaxs(0.0f, 1.0f - w * w));
+    float phi = 6.28318530717958647692f * uy;
+    V3 local = v3(s * rr_cosf(phi), s * rr_sinf(phi), w);
+    V3 T, B;
+    build_onb(mu, T, B);
+    V3 dir = tangent_to_world(local, T, B, mu);
+    float denom = 6.28318530717958647692f * (1.0f - rr_expf(-2.0f * k));
+    pdf = k * rr_expf(k * (w - 1.0f)) / fmaxs(denom, 1.0e-8f);
+    return dir;
+}
+float vmf_pdf(V3 mu, float kappa, V3 dir) {
+    float k = fmaxs(kappa, 1.0e-3f);
+    float w = clampf(dot(mu, dir), -1.0f, 1.0f);
+    float denom = 6.28318530717958647692f * (1.0f - rr_expf(-2.0f * k));
+    return k * rr_expf(k * (w - 1.0f)) / fmaxs(denom, 1.0e-8f);
+}
+
+} // namespace
+
+// ═══════════════════════════════ C API ═════════════════════════════════════
+
+extern "C" {
+
+uint32_t oracle_pcg_hash(uint32_t seed) { return pcg_hash(seed); }
+uint32_t oracle_make_seed(uint32_t px, uint32_t py, uint32_t f) { return make_seed(px, py, f); }
+float oracle_rand_float(uint32_t* seed) { return rand_float(*seed); }
+
+void oracle_detmath_eval(int which, const float* x, float* y, size_t n) {
+    for (size_t i = 0; i < n; ++i) {
+        switch (which) {
+        case 0: y[i] = rr_sinf(x[i]); break;
+        case 1: y[i] = rr_cosf(x[i]); break;
+        case 2: y[i] = rr_expf(x[i]); break;
+        default: y[i] = rr_logf(x[i]); break;
+        }
+    }
+}
+
+OracleScene* oracle_scene_create(const GpuVertex* vertices, uint32_t vertex_count,
+                                 const uint32_t* indices, uint32_t index_count,
+                                 const GpuMesh* meshes, uint32_t mesh_count,
+                                 const GpuMaterial* materials, uint32_t material_count,
+                                 const GpuInstance* instances, uint32_t instance_count,
+                                 const GpuLight* lights, uint32_t light_count, int use_bvh) {
+    OracleScene* s = new OracleScene;
+    s->vertices.assign(vertices, vertices + vertex_count);
+    s->indices.assign(indices, indices + index_count);
+    s->meshes.assign(meshes, meshes + mesh_count);
+    s->materials.assign(materials, materials + material_count);
+    s->instances.assign(instances, instances + instance_count);
+    if (light_count) s->lights.assign(lights, lights + light_count);
+    // World-space triangles: instance i, mesh-local primitive j, vertex
+    // position transformed by mul(transform, float4(p, 1)).
+    for (uint32_t i = 0; i < instance_count; ++i) {
+        const GpuInstance& inst = instances[i];
+        const GpuMesh& m = meshes[inst.mesh_index];
+        const uint32_t ntri = m.index_count / 3u;
+        for (uint32_t j = 0; j < ntri; ++j) {
+            Tri t;
+            V3 p[3];
+            for (int k = 0; k < 3; ++k) {
+                const GpuVertex& v = vertices[m.vertex_base + indices[m.index_byte_offset / 4u + j * 3u + k]];
+                V4 w = mul44(inst.transform, V4{v.pos[0], v.pos[1], v.pos[2], 1.0f});
+                p[k] = v3(w.x, w.y, w.z);
+            }
+            t.p0 = p[0]; t.p1 = p[1]; t.p2 = p[2]; t.inst = i; t.prim = j;
+            s->tris.push_back(t);
+        }
+    }
+    s->use_bvh = use_bvh != 0;
+    if (s->use_bvh && !s->tris.empty()) {
+        std::vector<float> cent(s->tris.size() * 3);
+        for (size_t i = 0; i < s->tris.size(); ++i) {
+            float lo[3], hi[3];
+            bounds_of(s->tris[i], lo, hi);
+            for (int a = 0; a < 3; ++a) cent[i * 3 + a] = 0.5f * (lo[a] + hi[a]);
+        }
+        s->order.resize(s->tris.size());
+        for (size_t i = 0; i < s->order.size(); ++i) s->order[i] = (uint32_t)i;
+        s->nodes.reserve(s->tris.size());
+        build_node(*s, 0, (uint32_t)s->tris.size(), cent);
+    }
+    return s;
+}
+
+void oracle_scene_destroy(OracleScene* s) { delete s; }
+uint32_t oracle_scene_triangle_count(const OracleScene* s) { return (uint32_t)s->tris.size(); }
+
+int oracle_trace(const OracleScene* s, const float origin[3], const float dir[3], float tmin,
+                 float tmax, float* t, float* bu, float* bv, uint32_t* inst, uint32_t* prim) {
+    Hit h = trace_scene<false>(*s, load3(origin), load3(dir), tmin, tmax);
+    if (!h.hit) { *inst = 0xffffffffu; *prim = 0xffffffffu; return 0; }
+    *t = h.t; *bu = h.u; *bv = h.v;
+    *inst = s->tris[h.key].inst; *prim = s->tris[h.key].prim;
+    return 1;
+}
+
+void oracle_trace_batch(const OracleScene* s, const float* origins, const float* dirs, float tmin,
+                        float tmax, size_t n, float* hits, uint32_t* prims, int threads) {
+    const uint32_t rows = (uint32_t)((n + 255) / 256);
+    parallel_rows(rows, threads, [&](uint32_t row) {
+        for (size_t i = (size_t)row * 256; i < std::min(n, (size_t)row * 256 + 256); ++i) {
+            Hit h = trace_scene<false>(*s, load3(origins + 4 * i), load3(dirs + 4 * i), tmin, tmax);
+            if (h.hit) {
+                hits[4 * i] = h.t; hits[4 * i + 1] = h.u; hits[4 * i + 2] = h.v;
+                hits[4 * i + 3] = asfloat(s->tris[h.key].inst); prims[i] = s->tris[h.key].prim;
+            } else {
+                hits[4 * i] = -1.0f; hits[4 * i + 1] = 0; hits[4 * i + 2] = 0;
+                hits[4 * i + 3] = asfloat(0xffffffffu); prims[i] = 0xffffffffu;
+            }
+        }
+    });
+}
+
+void oracle_primary_ray(const GpuCameraData* cam, uint32_t px, uint32_t py, uint32_t frame_seed,
+                        float origin[3], float dir[3], uint32_t* seed_out) {
+    uint32_t seed = make_seed(px, py, frame_seed);
+    float jx = rand_float(seed);
+    float jy = rand_float(seed);
+    V3 o, d;
+    primary_ray(*cam, px, py, jx, jy, o, d);
+    origin[0] = o.x; origin[1] = o.y; origin[2] = o.z;
+    dir[0] = d.x; dir[1] = d.y; dir[2] = d.z;
+    if (seed_out) *seed_out = seed;
+}
+
+void oracle_pathtrace(const OracleScene* s, const GpuCameraData* cam, uint32_t frame_seed,
+                      uint32_t max_bounces, uint32_t spp, uint32_t x0, uint32_t y0, uint32_t w,
+                      uint32_t h, float* out, int threads, uint64_t* stats) {
+    std::atomic<uint64_t> ext_total{0}, shd_total{0};
+    parallel_rows(h * spp, threads, [&](uint32_t row) {
+        const uint32_t sidx = row / h, y = row % h;
+        uint64_t ext = 0, shd = 0;
+        for (uint32_t x = 0; x < w; ++x) {
+            V3 r = trace_path(*s, *cam, x0 + x, y0 + y, frame_seed + sidx, max_bounces, ext, shd);
+            float* o = out + (((size_t)sidx * h + y) * w + x) * 4;
+            o[0] = r.x; o[1] = r.y; o[2] = r.z; o[3] = 1.0f;
+        }
+        ext_total += ext; shd_total += shd;
+    });
+    if (stats) { stats[0] = ext_total; stats[1] = shd_total; }
+}
+
+void oracle_accumulate(const float* radiance, float* acc, size_t pixels, uint32_t camera_moved,
+                       uint32_t accumulated_spp) {
+    // accumulate.slang:33-45
+    for (size_t i = 0; i < pixels * 4; ++i) {
+        if (camera_moved != 0 || accumulated_spp == 0) {
+            acc[i] = radiance[i];
+        } else {
+            float spp = float(accumulated_spp);
+            float weight = 1.0f / (spp + 1.0f);
+            acc[i] = acc[i] * (spp / (spp + 1.0f)) + radiance[i] * weight;
+        }
+    }
+}
+
+void oracle_restir_di_initial(const OracleScene* s, const GpuCameraData* cam, const OracleDIParams* p,
+                              float* gbuf_pos, float* gbuf_norm, float* res, int threads) {
+    // restir_di.slang:186-262
+    const uint32_t W = cam->screen_width, H = cam->screen_height;
+    const uint32_t N = (uint32_t)s->lights.size();
+    parallel_rows(H, threads, [&](uint32_t y) {
+        for (uint32_t x = 0; x < W; ++x) {
+            const size_t i = ((size_t)y * W + x) * 4;
+            uint32_t seed = make_seed(x, y, p->frame_seed);
+            float jx = rand_float(seed);
+            float jy = rand_float(seed);
+            V3 o, d;
+            primary_ray(*cam, x, y, jx, jy, o, d);
+            Hit h = trace_scene<false>(*s, o, d, 0.001f, 1e9f);
+            if (!h.hit) {
+                gbuf_pos[i] = 0; gbuf_pos[i + 1] = 0; gbuf_pos[i + 2] = 0; gbuf_pos[i + 3] = -1.0f;
+                gbuf_norm[i] = 0; gbuf_norm[i + 1] = 0; gbuf_norm[i + 2] = 0; gbuf_norm[i + 3] = 0;
+                pack_reservoir(res + i, 0xffffffffu, 0.0f, 0.0f, 0);
+                continue;
+            }
+            Surf sf = hit_surface(*s, h);
+            V3 normal = sf.normal;
+            if (dot(normal, -d) < 0.0f) normal = -normal;
+            gbuf_pos[i] = sf.pos.x; gbuf_pos[i + 1] = sf.pos.y; gbuf_pos[i + 2] = sf.pos.z;
+            gbuf_pos[i + 3] = h.t;
+            gbuf_norm[i] = normal.x; gbuf_norm[i + 1] = normal.y; gbuf_norm[i + 2] = normal.z;
+            gbuf_norm[i + 3] = asfloat(sf.material);
+            if (N == 0) { pack_reservoir(res + i, 0xffffffffu, 0.0f, 0.0f, 0); continue; }
+            uint32_t sel = 0xffffffffu;
+            float w_sum = 0.0f;
+            uint32_t M_count = 0;
+            for (uint32_t c = 0; c < p->num_initial_candidates; ++c) {
+                uint32_t cand = uint32_t(rand_float(seed) * float(N)) % N;
+                float ph = compute_p_hat(*s, cand, sf.pos, normal);
+                float w_i = ph * float(N);
+                w_sum += w_i;
+                M_count++;
+                if (w_sum > 0.0f && rand_float(seed) < w_i / w_sum) sel = cand;
+            }
+            float W_final = 0.0f;
+            if (sel != 0xffffffffu) {
+                float ph_y = compute_p_hat(*s, sel, sf.pos, normal);
+                W_final = (ph_y > 1e-10f) ? (w_sum / (float(M_count) * ph_y)) : 0.0f;
+            }
+            pack_reservoir(res + i, sel, w_sum, W_final, M_count);
+        }
+    });
+}
+
+void oracle_restir_di_temporal(const OracleScene* s, const GpuCameraData* cam, const OracleDIParams* p,
+                               const float* gbuf_pos, const float* gbuf_norm, float* res,
+                               const float* prev, int threads) {
+    // restir_di.slang:266-335
+    if (!p->temporal_enable) return;
+    const uint32_t W = cam->screen_width, H = cam->screen_height;
+    parallel_rows(H, threads, [&](uint32_t y) {
+        for (uint32_t x = 0; x < W; ++x) {
+            const size_t i = ((size_t)y * W + x) * 4;
+            if (gbuf_pos[i + 3] < 0.0f) continue;
+            V3 hit_pos = load3(gbuf_pos + i);
+            V3 normal = load3(gbuf_norm + i);
+            uint32_t curr_sel = asuint(res[i]); float curr_wsum = res[i + 1];
+            uint32_t curr_M = asuint(res[i + 3]);
+            uint32_t prev_sel = asuint(prev[i]); float prev_W = prev[i + 2];
+            uint32_t prev_M = asuint(prev[i + 3]);
+            if (prev_sel == 0xffffffffu || prev_M == 0) continue;
+            uint32_t m_cap = std::min(std::max(p->m_cap_factor * p->num_initial_candidates, 1u), 8192u);
+            prev_M = std::min(prev_M, m_cap);
+            float ph_prev = compute_p_hat(*s, prev_sel, hit_pos, normal);
+            float contrib = ph_prev * prev_W * float(prev_M);
+            curr_wsum += contrib;
+            uint32_t new_M = curr_M + prev_M;
+            if (new_M > m_cap) {
+                float scale = float(m_cap) / float(new_M);
+                curr_wsum *= scale;
+                curr_M = m_cap;
+            } else {
+                curr_M = new_M;
+            }
+            uint32_t seed = make_seed(x, y, p->frame_seed + 1u);
+            if (contrib > 0.0f && rand_float(seed) < contrib / curr_wsum) curr_sel = prev_sel;
+            float W_new = 0.0f;
+            if (curr_sel != 0xffffffffu) {
+                float ph_y = compute_p_hat(*s, curr_sel, hit_pos, normal);
+                W_new = (ph_y > 1e-10f) ? (curr_wsum / (float(curr_M) * ph_y)) : 0.0f;
+                W_new = fmins(W_new, 1e4f);
+            }
+            pack_reservoir(res + i, curr_sel, curr_wsum, W_new, curr_M);
+        }
+    });
+}
+
+void oracle_restir_di_spatial_shade(const OracleScene* s, const GpuCameraData* cam,
+                                    const OracleDIParams* p, const float* gbuf_pos,
+                                    const float* gbuf_norm, const float* res, float* output,
+                                    int threads) {
+    // restir_di.slang:339-472
+    const uint32_t W = cam->screen_width, H = cam->screen_height;
+    const uint32_t N = (uint32_t)s->lights.size();
+    parallel_rows(H, threads, [&](uint32_t y) {
+        for (uint32_t x = 0; x < W; ++x) {
+            const size_t i = ((size_t)y * W + x) * 4;
+            float* out = output + i;
+            if (gbuf_pos[i + 3] < 0.0f) {
+                float ndcx = (float(x) + 0.5f) / float(W) * 2.0f - 1.0f;
+                float ndcy = (float(y) + 0.5f) / float(H) * 2.0f - 1.0f;
+                V4 rv = mul44(cam->inv_proj, V4{ndcx, ndcy, 1.0f, 1.0f});
+                rv.z = -1.0f; rv.w = 0.0f;
+                V4 rw = mul44(cam->inv_view, rv);
+                V3 dir = normalize(v3(rw.x, rw.y, rw.z));
+                V3 c = sky(dir);
+                out[0] = c.x; out[1] = c.y; out[2] = c.z; out[3] = 1.0f;
+                continue;
+            }
+            V3 hit_pos = load3(gbuf_pos + i);
+            V3 normal = load3(gbuf_norm + i);
+            uint32_t mat_idx = asuint(gbuf_norm[i + 3]);
+            const GpuMaterial& mat = s->materials[mat_idx];
+            if (any_positive(mat.emissive)) {
+                out[0] = mat.emissive[0]; out[1] = mat.emissive[1]; out[2] = mat.emissive[2]; out[3] = 1.0f;
+                continue;
+            }
+            uint32_t r_sel = asuint(res[i]); float r_wsum = res[i + 1]; float r_W = res[i + 2];
+            uint32_t r_M = asuint(res[i + 3]);
+            if (p->spatial_enable && p->spatial_num_neighbors > 0 && N > 0) {
+                uint32_t seed = make_seed(x, y, p->frame_seed + 2u);
+                for (uint32_t k = 0; k < p->spatial_num_neighbors; ++k) {
+                    float angle = rand_float(seed) * 6.28318530717958f;
+                    float radius = rand_float(seed) * float(p->spatial_radius);
+                    int ox = int(radius * rr_cosf(angle)), oy = int(radius * rr_sinf(angle));
+                    int nx = std::min(std::max((int)x + ox, 0), (int)W - 1);
+                    int ny = std::min(std::max((int)y + oy, 0), (int)H - 1);
+                    const size_t j = ((size_t)ny * W + nx) * 4;
+                    if (gbuf_pos[j + 3] < 0.0f) continue;
+                    uint32_t nb_sel = asuint(res[j]); float nb_W = res[j + 2];
+                    uint32_t nb_M = asuint(res[j + 3]);
+                    if (nb_sel == 0xffffffffu || nb_M == 0) continue;
+                    float ph_nb = compute_p_hat(*s, nb_sel, hit_pos, normal);
+                    float contrib = ph_nb * nb_W * float(nb_M);
+                    r_wsum += contrib;
+                    r_M += nb_M;
+                    if (contrib > 0.0f && rand_float(seed) < contrib / r_wsum) r_sel = nb_sel;
+                }
+                if (r_sel != 0xffffffffu) {
+                    float ph_y = compute_p_hat(*s, r_sel, hit_pos, normal);
+                    r_W = (ph_y > 1e-10f) ? (r_wsum / (float(r_M) * ph_y)) : 0.0f;
+                }
+            }
+            V3 o = v3(0, 0, 0);
+            if (r_sel != 0xffffffffu && r_sel < N && r_W > 0.0f && N > 0) {
+                const GpuLight& light = s->lights[r_sel];
+                V3 l, irr; float dist;
+                if (light.type == 0) {
+                    V3 to = load3(light.position) - hit_pos;
+                    dist = length(to);
+                    l = to / fmaxs(dist, 1e-6f);
+                    float dd = fmaxs(dist * dist, 1e-6f);
+                    irr = v3(light.emission[0] * light.intensity / dd, light.emission[1] * light.intensity / dd,
+                             light.emission[2] * light.intensity / dd);
+                } else {
+                    l = normalize(-load3(light.direction));
+                    dist = 1e9f;
+                    irr = load3(light.emission) * light.intensity;
+                }
+                float n_dot_l = fmaxs(dot(normal, l), 0.0f);
+                if (n_dot_l > 0.0f) {
+                    Hit sh = trace_scene<true>(*s, hit_pos + normal * 1e-4f, l, 0.001f, dist - 0.01f);
+                    if (!sh.hit) {
+                        V3 wo = normalize(load3(cam->position) - hit_pos);
+                        V3 bv = brdf_eval(normal, wo, l, load3(mat.base_color), mat.metallic, mat.roughness);
+                        o = ((bv * irr) * n_dot_l) * r_W;
+                    }
+                }
+            }
+            out[0] = o.x; out[1] = o.y; out[2] = o.z; out[3] = 1.0f;
+        }
+    });
+}
+
+void oracle_atrous_iteration(const float* input, const float* gpos, const float* gnrm, float* output,
+                             uint32_t width, uint32_t height, uint32_t stride_u, float sp, float sn,
+                             float sl, int threads) {
+    // atrous.slang:41-106
+    parallel_rows(height, threads, [&](uint32_t y) {
+        for (uint32_t x = 0; x < width; ++x) {
+            const size_t i = ((size_t)y * width + x) * 4;
+            const float* cpos = gpos + i;
+            const float* crad = input + i;
+            float* out = output + i;
+            if (cpos[3] < 0.0f) { out[0] = crad[0]; out[1] = crad[1]; out[2] = crad[2]; out[3] = crad[3]; continue; }
+            V3 center_normal = normalize(load3(gnrm + i));
+            float center_luma = luminance601(load3(crad));
+            float sigma_pos_sq = fmaxs(sp * sp, 1.0e-6f);
+            float sigma_norm_sq = fmaxs(sn * sn, 1.0e-6f);
+            float sigma_luma_sq = fmaxs(sl * sl, 1.0e-6f);
+            V3 filtered = v3(0, 0, 0);
+            float weight_sum = 0.0f;
+            const int mx = (int)width - 1, my = (int)height - 1;
+            const int stride = (int)stride_u;
+            for (int ty = -2; ty <= 2; ++ty) {
+                for (int tx = -2; tx <= 2; ++tx) {
+                    int sx = std::min(std::max((int)x + tx * stride, 0), mx);
+                    int sy = std::min(std::max((int)y + ty * stride, 0), my);
+                    const size_t j = ((size_t)sy * width + sx) * 4;
+                    if (gpos[j + 3] < 0.0f) continue;
+                    float base_w = (kernel_weight(tx) * kernel_weight(ty)) / 256.0f;
+                    V3 pd = load3(gpos + j) - load3(cpos);
+                    float pos_w = rr_expf(-dot(pd, pd) / sigma_pos_sq);
+                    V3 sn3 = normalize(load3(gnrm + j));
+                    float nd = fmaxs(0.0f, 1.0f - dot(center_normal, sn3));
+                    float normal_w = rr_expf(-nd / sigma_norm_sq);
+                    float ld = luminance601(load3(input + j)) - center_luma;
+                    float luma_w = rr_expf(-(ld * ld) / sigma_luma_sq);
+                    float weight = base_w * pos_w * normal_w * luma_w;
+                    filtered = filtered + load3(input + j) * weight;
+                    weight_sum += weight;
+                }
+            }
+            V3 o = (weight_sum > 0.0f) ? (filtered / weight_sum) : load3(crad);
+            out[0] = o.x; out[1] = o.y; out[2] = o.z; out[3] = crad[3];
+        }
+    });
+}
+
+uint32_t oracle_guiding_cell_index(const float pos[3], uint32_t bsdf_id, const float cam_pos[3],
+                                   const OracleGuidingParams* gp) {
+    return cell_index(load3(pos), bsdf_id, load3(cam_pos), *gp);
+}
+
+void oracle_guiding_splat(int32_t* accum, const float* pos, const float* dir, const uint32_t* bsdf,
+                          size_t n, const float cam_pos[3], const OracleGuidingParams* gp) {
+    // GuidingGrid.slang:73-90 at the call site restir_pt.slang:982-994
+    for (size_t i = 0; i < n; ++i) {
+        uint32_t cell = cell_index(load3(pos + 4 * i), bsdf[i], load3(cam_pos), *gp);
+        const float* d = dir + 4 * i;
+        uint32_t* a = reinterpret_cast<uint32_t*>(accum) + (size_t)cell * 4;
+        for (int c = 0; c < 3; ++c) a[c] += (uint32_t)(int32_t)rintf(d[c] * 1048576.0f);
+        a[3] += 1u;
+    }
+}
+
+void oracle_guiding_fit(int32_t* accum, float* fitted, const OracleGuidingParams* gp) {
+    // GuidingGrid.slang:100-137 via cs_fit_guiding (restir_pt.slang:1005-1015)
+    if (gp->enabled == 0u) return;
+    for (uint32_t cell = 0; cell < gp->cell_count; ++cell) {
+        int32_t* a = accum + (size_t)cell * 4;
+        float* f = fitted + (size_t)cell * 4;
+        int32_t ix = a[0], iy = a[1], iz = a[2];
+        uint32_t n = (uint32_t)a[3];
+        a[0] = a[1] = a[2] = a[3] = 0;
+        if (n < std::max(gp->min_samples, 1u)) { f[3] = -1.0f; continue; }
+        V3 sum = v3(float(ix), float(iy), float(iz)) * (1.0f / 1048576.0f);
+        float len = length(sum);
+        float r = len / float(n);
+        r = clampf(r, 1.0e-4f, 0.9999f);
+        V3 mu = (len > 1.0e-6f) ? (sum / len) : v3(0.0f, 0.0f, 1.0f);
+        float kappa = r * (3.0f - r * r) / (1.0f - r * r);
+        kappa = clampf(kappa, 0.5f, gp->kappa_max);
+        f[0] = mu.x; f[1] = mu.y; f[2] = mu.z; f[3] = kappa;
+    }
+}
+
+void oracle_guiding_sample(const float* fitted, const float* pos, const float* normal,
+                           const uint32_t* bsdf, uint32_t* seeds, size_t n, const float cam_pos[3],
+                           const OracleGuidingParams* gp, float* wi_out, float* pdf_out) {
+    // sample_primary_dir (restir_pt.slang:520-563)
+    for (size_t i = 0; i < n; ++i) {
+        V3 p = load3(pos + 4 * i), nn = load3(normal + 4 * i);
+        uint32_t seed = seeds[i];
+        float alpha = 0.0f;
+        bool valid = false;
+        V3 mu = v3(0, 0, 0);
+        float kappa = 0.0f;
+        if (gp->enabled != 0u && gp->alpha > 0.0f) {
+            uint32_t cell = cell_index(p, bsdf[i], load3(cam_pos), *gp);
+            const float* f = fitted + (size_t)cell * 4;
+            mu = v3(f[0], f[1], f[2]);
+            kappa = f[3];
+            valid = (kappa > 0.0f) && (dot(mu, mu) > 0.25f);
+            if (valid) alpha = gp->alpha;
+        }
+        V3 T, B;
+        build_onb(nn, T, B);
+        V3 wi;
+        if (rand_float(seed) < alpha) {
+            float ux = rand_float(seed);
+            float uy = rand_float(seed);
+            float vpdf;
+            wi = vmf_sample(mu, kappa, ux, uy, vpdf);
+        } else {
+            float u0 = rand_float(seed);  // arguments evaluate left to right
+            float u1 = rand_float(seed);
+            float cpdf;
+            V3 local = sample_cosine_hemisphere(u0, u1, cpdf);
+            wi = tangent_to_world(local, T, B, nn);
+        }
+        float cos_i = dot(nn, wi);
+        float p_cos = (cos_i > 0.0f) ? (cos_i * kInvPi) : 0.0f;
+        float p_vmf = valid ? vmf_pdf(mu, kappa, wi) : 0.0f;
+        float src_pdf = alpha * p_vmf + (1.0f - alpha) * p_cos;
+        wi_out[4 * i] = wi.x; wi_out[4 * i + 1] = wi.y; wi_out[4 * i + 2] = wi.z; wi_out[4 * i + 3] = 0.0f;
+        pdf_out[i] = src_pdf;
+        seeds[i] = seed;
+    }
+}
+
+float oracle_vmf_pdf(const float mu[3], float kappa, const float dir[3]) {
+    return vmf_pdf(load3(mu), kappa, load3(dir));
+}
+
+void oracle_brdf_eval(const float n[3], const float wo[3], const float wi[3], const float base[3],
+                      float metallic, float roughness, float out[3]) {
+    V3 r = brdf_eval(load3(n), load3(wo), load3(wi), load3(base), metallic, roughness);
+    out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
+
+void oracle_brdf_sample(const float wo[3], const float n[3], const float base[3], float metallic,
+                        float roughness, float u0, float u1, float wi[3], float* pdf, float f[3]) {
+    V3 w;
+    V3 r = brdf_sample(load3(wo), load3(n), load3(base), metallic, roughness, u0, u1, w, *pdf);
+    wi[0] = w.x; wi[1] = w.y; wi[2] = w.z;
+    f[0] = r.x; f[1] = r.y; f[2] = r.z;
+}
+
+float oracle_brdf_pdf(const float wo[3], const float wi[3], const float n[3], float roughness) {
+    return brdf_pdf(load3(wo), load3(wi), load3(n), roughness);
+}
+
+} // extern "C"

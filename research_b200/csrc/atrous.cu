@@ -1,0 +1,112 @@
+// atrous.cu — edge-aware A-trous wavelet filter (AtrousPass.cpp:243-306,
+// kernel atrous.slang:41-106): 5x5 B3 taps (1,4,6,4,1)/16 per axis at
+// stride 1<<iter, clamped to the image, skipping G-buffer misses, weighted by
+// exp(-|dp|^2/sp^2) * exp(-max(0, 1-n.n')/sn^2) * exp(-dl^2/sl^2).
+
+#include "rr_internal.h"
+
+namespace rr {
+namespace {
+
+RR_D float luminance601(float3 c) { return dot(c, f3(0.299f, 0.587f, 0.114f)); }
+RR_D float kernel_weight(int o) { return (o == 2 || o == -2) ? 1.0f : ((o == 1 || o == -1) ? 4.0f : 6.0f); }
+
+__global__ void __launch_bounds__(128) atrous_kernel(const float4* __restrict__ in,
+                                                     const float4* __restrict__ gpos,
+                                                     const float4* __restrict__ gnrm,
+                                                     float4* __restrict__ out, int W, int H, int stride,
+                                                     float sp2, float sn2, float sl2) {
+    const int x = blockIdx.x * 16 + (threadIdx.x & 15);
+    const int y = blockIdx.y * 8 + (threadIdx.x >> 4);
+    if (x >= W || y >= H) return;
+    const size_t ci = size_t(y) * W + x;
+    const float4 cpos = gpos[ci];
+    const float4 crad = in[ci];
+    if (cpos.w < 0.0f) { out[ci] = crad; return; }
+    const float3 cn = normalize(xyz(gnrm[ci]));
+    const float cl = luminance601(xyz(crad));
+    float3 filtered = f3(0.0f, 0.0f, 0.0f);
+    float wsum = 0.0f;
+    #pragma unroll
+    for (int ty = -2; ty <= 2; ++ty) {
+        const int sy = min(max(y + ty * stride, 0), H - 1);
+        #pragma unroll
+        for (int tx = -2; tx <= 2; ++tx) {
+            const int sx = min(max(x + tx * stride, 0), W - 1);
+            const size_t si = size_t(sy) * W + sx;
+            const float4 spos = __ldg(gpos + si);
+            if (spos.w < 0.0f) continue;
+            const float base_w = (kernel_weight(tx) * kernel_weight(ty)) / 256.0f;
+            const float3 pd = xyz(spos) - xyz(cpos);
+            const float pos_w = rr_expf(-dot(pd, pd) / sp2);
+            const float3 sn = normalize(xyz(__ldg(gnrm + si)));
+            const float nd = mx(0.0f, 1.0f - dot(cn, sn));
+            const float normal_w = rr_expf(-nd / sn2);
+            const float3 srad = xyz(__ldg(in + si));
+            const float ld = luminance601(srad) - cl;
+            const float luma_w = rr_expf(-(ld * ld) / sl2);
+            const float w = base_w * pos_w * normal_w * luma_w;
+            filtered = filtered + srad * w;
+            wsum += w;
+        }
+    }
+    const float3 o = wsum > 0.0f ? filtered / wsum : xyz(crad);
+    out[ci] = make_float4(o.x, o.y, o.z, crad.w);
+}
+
+} // namespace
+} // namespace rr
+
+static rr_status atrous_launch(rr_ctx* ctx, const float* input, const float* gpos, const float* gnrm,
+                               float* output, uint32_t W, uint32_t H, uint32_t stride, float sp, float sn,
+                               float sl, cudaStream_t stream) {
+    const float sp2 = std::max(sp * sp, 1.0e-6f), sn2 = std::max(sn * sn, 1.0e-6f), sl2 = std::max(sl * sl, 1.0e-6f);
+    dim3 grid((W + 15) / 16, (H + 7) / 8);
+    rr::atrous_kernel<<<grid, 128, 0, stream>>>(
+        reinterpret_cast<const float4*>(input), reinterpret_cast<const float4*>(gpos),
+        reinterpret_cast<const float4*>(gnrm), reinterpret_cast<float4*>(output), int(W), int(H),
+        int(stride), sp2, sn2, sl2);
+    RR_CHECK_LAUNCH(ctx);
+    ctx->launches += 1;
+    return RR_OK;
+}
+
+extern "C" rr_status rr_atrous_iteration(rr_ctx* ctx, const float* input, const float* gpos,
+                                         const float* gnrm, float* output, const rr_atrous_params* p,
+                                         void* stream) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    if (!input || !gpos || !gnrm || !output || !p) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_atrous_iteration: null argument");
+    if (p->width == 0 || p->height == 0 || p->width > 65535u * 16u || p->height > 65535u * 8u)
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_atrous_iteration: bad image size");
+    if (input == output) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_atrous_iteration: input aliases output");
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    return atrous_launch(ctx, input, gpos, gnrm, output, p->width, p->height, p->stride, p->sigma_position,
+                         p->sigma_normal, p->sigma_luminance, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" rr_status rr_atrous_execute(rr_ctx* ctx, const float* input, const float* gpos, const float* gnrm,
+                                       float* ping0, float* ping1, const rr_atrous_params* p,
+                                       uint32_t* out_slot, void* stream) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    if (!input || !gpos || !gnrm || !ping0 || !ping1 || !p)
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_atrous_execute: null argument");
+    if (p->width == 0 || p->height == 0 || p->width > 65535u * 16u || p->height > 65535u * 8u)
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_atrous_execute: bad image size");
+    if (input == ping0 || input == ping1 || ping0 == ping1)
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_atrous_execute: buffers alias");
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    // AtrousPass.cpp:265 clamps to 1..7; slot (iterations-1)&1 holds the result.
+    const uint32_t iters = std::min(std::max(p->iterations, 1u), 7u);
+    const float* read = input;
+    float* ping[2] = {ping0, ping1};
+    for (uint32_t it = 0; it < iters; ++it) {
+        float* write = ping[it & 1u];
+        rr_status st = atrous_launch(ctx, read, gpos, gnrm, write, p->width, p->height, 1u << it,
+                                     p->sigma_position, p->sigma_normal, p->sigma_luminance,
+                                     static_cast<cudaStream_t>(stream));
+        if (st != RR_OK) return st;
+        read = write;
+    }
+    if (out_slot) *out_slot = (iters - 1u) & 1u;
+    return RR_OK;
+}

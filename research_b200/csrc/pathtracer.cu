@@ -1,0 +1,412 @@
+// pathtracer.cu — the reference path tracer as wavefront stages.
+//
+// Restates passes/pathtracer_reference/pathtracer.slang:181-265 (one path per
+// pixel per frame seed) as four kernels over SoA queues:
+//   raygen : make_seed + jittered primary ray (pathtracer.slang:191-205)
+//   extend : closest-hit BVH traversal of the ray queue (trace, :45-120)
+//   shade  : miss/sky and emissive termination (:213-229), NEE light pick and
+//            shadow-ray emission (:124-177), BSDF sample, throughput update,
+//            Russian roulette (:236-260); survivors are compacted into the
+//            next ray queue with one warp ballot + one atomic per warp
+//   shadow : any-hit traversal; unoccluded NEE contributions are added
+// The RNG state travels with each ray, so every path consumes random numbers
+// in the reference order (primary 2, per bounce NEE 1 -> BSDF 2 -> RR 1).
+// Radiance is accumulated into the caller's image in the same order as the
+// reference's `radiance +=` statements, which keeps results bit-identical.
+
+#include "rr_internal.h"
+
+#include <cstring>
+
+namespace rr {
+namespace {
+
+constexpr int kBlock = 256;
+constexpr uint32_t kFull = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Warp-aggregated slot allocation: returns this lane's slot when `want`.
+__device__ __forceinline__ uint32_t warp_alloc(bool want, uint32_t* counter) {
+    const uint32_t mask = __ballot_sync(kFull, want);
+    uint32_t base = 0;
+    if (lane_id() == 0 && mask) base = atomicAdd(counter, __popc(mask));
+    base = __shfl_sync(kFull, base, 0);
+    return base + __popc(mask & ((1u << lane_id()) - 1u));
+}
+
+struct PtLaunch {
+    GpuCameraData cam;
+    uint32_t frame_seed;
+    uint32_t spp;
+    uint32_t width, height;
+    uint32_t tiles_x, tiles_per_image;
+};
+
+// One warp per 8x4 pixel tile so that primary rays of a warp are coherent.
+__global__ void __launch_bounds__(kBlock) raygen_kernel(PtLaunch L, float4* __restrict__ out,
+                                                        float4* qa, float4* qb, float4* qc,
+                                                        uint32_t* counters) {
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t tile = gtid >> 5;
+    const uint32_t lane = lane_id();
+    const uint32_t total_tiles = L.tiles_per_image * L.spp;
+    bool active = tile < total_tiles;
+    uint32_t s = 0, px = 0, py = 0;
+    if (active) {
+        s = tile / L.tiles_per_image;
+        const uint32_t t = tile % L.tiles_per_image;
+        px = (t % L.tiles_x) * 8 + (lane & 7);
+        py = (t / L.tiles_x) * 4 + (lane >> 3);
+        active = px < L.width && py < L.height;
+    }
+    if (__all_sync(kFull, tile >= total_tiles)) return;
+    const uint32_t slot = warp_alloc(active, &counters[0]);
+    if (!active) return;
+    const uint32_t pid = (s * L.height + py) * L.width + px;
+    uint32_t seed = make_seed(px, py, L.frame_seed + s);
+    const float jx = rand_float(seed);
+    const float jy = rand_float(seed);
+    const float3 dir = primary_dir(L.cam, float(px) + jx, float(py) + jy);
+    out[pid] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    qa[slot] = make_float4(L.cam.position[0], L.cam.position[1], L.cam.position[2], __uint_as_float(pid));
+    qb[slot] = make_float4(dir.x, dir.y, dir.z, __uint_as_float(seed));
+    qc[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+}
+
+// Adds per-thread traversal work to two 64-bit counters, one atomic per warp.
+__device__ __forceinline__ void flush_work(const TraceWork& w, unsigned long long* out) {
+    unsigned long long n = w.nodes, t = w.tris;
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        n += __shfl_down_sync(kFull, n, o);
+        t += __shfl_down_sync(kFull, t, o);
+    }
+    if (lane_id() == 0 && (n | t)) { atomicAdd(out, n); atomicAdd(out + 1, t); }
+}
+
+// Closest hit for every ray of the queue; warps fetch 32 rays at a time.
+template <bool Count>
+__global__ void __launch_bounds__(kBlock) extend_kernel(DevScene s, const float4* __restrict__ qa,
+                                                        const float4* __restrict__ qb,
+                                                        float4* __restrict__ hits,
+                                                        const uint32_t* count_ptr, uint32_t* work,
+                                                        unsigned long long* work_out) {
+    const uint32_t count = *count_ptr;
+    TraceWork tw;
+    while (true) {
+        uint32_t base = 0;
+        if (lane_id() == 0) base = atomicAdd(work, 32u);
+        base = __shfl_sync(kFull, base, 0);
+        if (base >= count) break;
+        const uint32_t i = base + lane_id();
+        if (i < count) {
+            const float4 a = qa[i], b = qb[i];
+            const Ray r = make_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z));
+            HitRec h;
+            if (trace<false, Count>(s, r, 0.001f, 1e9f, h, &tw))
+                hits[i] = make_float4(h.u, h.v, __uint_as_float(h.inst), __uint_as_float(h.prim));
+            else
+                hits[i] = make_float4(0.0f, 0.0f, __uint_as_float(kNoIndex), __uint_as_float(kNoIndex));
+        }
+    }
+    if (Count) flush_work(tw, work_out);
+}
+
+__global__ void __launch_bounds__(kBlock) shade_kernel(DevScene s, uint32_t bounce, uint32_t last,
+                                                       const float4* __restrict__ qa,
+                                                       const float4* __restrict__ qb,
+                                                       const float4* __restrict__ qc,
+                                                       const float4* __restrict__ hits,
+                                                       float4* na, float4* nb, float4* nc,
+                                                       float4* sa, float4* sb, float4* sc,
+                                                       float4* __restrict__ out,
+                                                       const uint32_t* count_ptr,
+                                                       uint32_t* next_count, uint32_t* shadow_count) {
+    const uint32_t count = *count_ptr;
+    const uint32_t warp_first = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = warp_first; base < count; base += stride) {
+        const uint32_t i = base + lane_id();
+        bool cont = false, emit_shadow = false;
+        uint32_t pid = 0, seed = 0;
+        float3 new_o = f3(0, 0, 0), wi = f3(0, 0, 0), thp = f3(0, 0, 0);
+        float3 sh_o = f3(0, 0, 0), sh_d = f3(0, 0, 0), contrib = f3(0, 0, 0);
+        float sh_tmax = 0.0f;
+        if (i < count) {
+            const float4 a = qa[i], b = qb[i], c = qc[i];
+            const float4 h = hits[i];
+            pid = __float_as_uint(a.w);
+            seed = __float_as_uint(b.w);
+            const float3 ray_dir = f3(b.x, b.y, b.z);
+            thp = f3(c.x, c.y, c.z);
+            const uint32_t inst = __float_as_uint(h.z);
+            if (inst == kNoIndex) {
+                // Sky / environment (pathtracer.slang:213-219)
+                const float3 L = thp * sky_radiance(ray_dir);
+                float4 o = out[pid];
+                o.x = o.x + L.x; o.y = o.y + L.y; o.z = o.z + L.z;
+                out[pid] = o;
+            } else {
+                const Surface sf = hit_surface(s, inst, __float_as_uint(h.w), h.x, h.y);
+                const float4 m0 = __ldg(s.materials + sf.material * 2);
+                const float4 m1 = __ldg(s.materials + sf.material * 2 + 1);
+                if (m1.x > 0.0f || m1.y > 0.0f || m1.z > 0.0f) {
+                    // Emissive surfaces terminate (pathtracer.slang:225-229)
+                    const float3 L = thp * f3(m1.x, m1.y, m1.z);
+                    float4 o = out[pid];
+                    o.x = o.x + L.x; o.y = o.y + L.y; o.z = o.z + L.z;
+                    out[pid] = o;
+                } else {
+                    const float3 wo = -ray_dir;
+                    float3 n = sf.normal;
+                    if (dot(n, wo) < 0.0f) n = -n;
+                    const float3 base_c = f3(m0.x, m0.y, m0.z);
+                    const float metallic = m0.w, roughness = m1.w;
+                    // NEE (pathtracer.slang:124-177): pick, shadow ray, contribution
+                    if (s.num_lights > 0) {
+                        const uint32_t N = s.num_lights;
+                        const uint32_t li = uint32_t(rand_float(seed) * float(N)) % N;
+                        const float4 l0 = __ldg(s.lights + li * 3);
+                        const float4 l1 = __ldg(s.lights + li * 3 + 1);
+                        const float4 l2 = __ldg(s.lights + li * 3 + 2);
+                        const bool is_point = __float_as_uint(l0.w) == 0u;
+                        float3 ldir; float dist, pdf_light;
+                        if (is_point) {
+                            const float3 to = f3(l0.x, l0.y, l0.z) - sf.pos;
+                            dist = length(to);
+                            ldir = to / dist;
+                            pdf_light = dist * dist;
+                        } else {
+                            ldir = normalize(-f3(l1.x, l1.y, l1.z));
+                            dist = 1e9f;
+                            pdf_light = 1.0f;
+                        }
+                        if (dot(ldir, n) > 0.0f) {
+                            const float3 brdf_val = brdf_eval(n, wo, ldir, base_c, metallic, roughness);
+                            const float n_dot_l = mx(dot(n, ldir), 0.0f);
+                            const float den = is_point ? (pdf_light + 1e-6f) : 1.0f;
+                            const float3 irr = f3(l2.x * l2.w / den, l2.y * l2.w / den, l2.z * l2.w / den);
+                            float mis = 1.0f;
+                            if (!is_point) {
+                                const float pb = brdf_pdf(wo, ldir, n, roughness);
+                                mis = (pdf_light * pdf_light) / (pdf_light * pdf_light + pb * pb + 1e-10f);
+                            }
+                            float3 Lr = brdf_val * irr;
+                            Lr = Lr * n_dot_l;
+                            Lr = Lr * mis;
+                            Lr = Lr * float(N);
+                            contrib = thp * Lr;
+                            sh_o = sf.pos + n * 1e-4f;
+                            sh_d = ldir;
+                            sh_tmax = dist - 0.01f;
+                            emit_shadow = true;
+                        }
+                    }
+                    if (!last) {
+                        const float u0 = rand_float(seed);
+                        const float u1 = rand_float(seed);
+                        float pdf;
+                        const float3 f = brdf_sample(wo, n, base_c, metallic, roughness, u0, u1, wi, pdf);
+                        if (!(pdf < 1e-6f)) {
+                            const float ndwi = mx(dot(n, wi), 0.0f);
+                            thp = thp * ((f * ndwi) / pdf);
+                            bool alive = true;
+                            if (bounce >= 3) {
+                                const float survive = mn(mx(thp.x, mx(thp.y, thp.z)), 0.95f);
+                                if (rand_float(seed) > survive) alive = false;
+                                else thp = thp / survive;
+                            }
+                            if (alive) { cont = true; new_o = sf.pos + n * 1e-4f; }
+                        }
+                    }
+                }
+            }
+        }
+        const uint32_t sslot = warp_alloc(emit_shadow, shadow_count);
+        if (emit_shadow) {
+            sa[sslot] = make_float4(sh_o.x, sh_o.y, sh_o.z, __uint_as_float(pid));
+            sb[sslot] = make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
+            sc[sslot] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+        }
+        const uint32_t rslot = warp_alloc(cont, next_count);
+        if (cont) {
+            na[rslot] = make_float4(new_o.x, new_o.y, new_o.z, __uint_as_float(pid));
+            nb[rslot] = make_float4(wi.x, wi.y, wi.z, __uint_as_float(seed));
+            nc[rslot] = make_float4(thp.x, thp.y, thp.z, 0.0f);
+        }
+    }
+}
+
+// Any-hit shadow rays; unoccluded contributions are added to the image.
+template <bool Count>
+__global__ void __launch_bounds__(kBlock) shadow_kernel(DevScene s, const float4* __restrict__ sa,
+                                                        const float4* __restrict__ sb,
+                                                        const float4* __restrict__ sc,
+                                                        float4* __restrict__ out,
+                                                        const uint32_t* count_ptr, uint32_t* work,
+                                                        unsigned long long* work_out) {
+    const uint32_t count = *count_ptr;
+    TraceWork tw;
+    while (true) {
+        uint32_t base = 0;
+        if (lane_id() == 0) base = atomicAdd(work, 32u);
+        base = __shfl_sync(kFull, base, 0);
+        if (base >= count) break;
+        const uint32_t i = base + lane_id();
+        if (i < count) {
+            const float4 a = sa[i], b = sb[i];
+            const Ray r = make_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z));
+            HitRec h;
+            if (!trace<true, Count>(s, r, 0.001f, b.w, h, &tw)) {
+                const float4 c = sc[i];
+                const uint32_t pid = __float_as_uint(a.w);
+                float4 o = out[pid];
+                o.x = o.x + c.x; o.y = o.y + c.y; o.z = o.z + c.z;
+                out[pid] = o;
+            }
+        }
+    }
+    if (Count) flush_work(tw, work_out);
+}
+
+int persistent_grid(const rr_ctx* ctx, const void* kernel) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, 0);
+    return ctx->sm_count * (per_sm > 0 ? per_sm : 1);
+}
+
+rr_status ensure_queues(rr_ctx* ctx, size_t n) {
+    rr_pt_queues& q = ctx->pt;
+    if (q.capacity >= n) return RR_OK;
+    for (int i = 0; i < 2; ++i) { cudaFree(q.ray_a[i]); cudaFree(q.ray_b[i]); cudaFree(q.ray_c[i]); }
+    cudaFree(q.hits); cudaFree(q.shadow_a); cudaFree(q.shadow_b); cudaFree(q.shadow_c);
+    q = rr_pt_queues();
+    const size_t bytes = n * sizeof(float4);
+    for (int i = 0; i < 2; ++i) {
+        RR_TRY_CUDA(ctx, cudaMalloc(&q.ray_a[i], bytes));
+        RR_TRY_CUDA(ctx, cudaMalloc(&q.ray_b[i], bytes));
+        RR_TRY_CUDA(ctx, cudaMalloc(&q.ray_c[i], bytes));
+    }
+    RR_TRY_CUDA(ctx, cudaMalloc(&q.hits, bytes));
+    RR_TRY_CUDA(ctx, cudaMalloc(&q.shadow_a, bytes));
+    RR_TRY_CUDA(ctx, cudaMalloc(&q.shadow_b, bytes));
+    RR_TRY_CUDA(ctx, cudaMalloc(&q.shadow_c, bytes));
+    q.capacity = n;
+    return RR_OK;
+}
+
+} // namespace
+} // namespace rr
+
+using namespace rr;
+
+extern "C" rr_status rr_pathtracer_execute(rr_ctx* ctx, const rr_scene* scene,
+                                           const GpuCameraData* cam, const rr_pt_params* p,
+                                           float* radiance_out, void* stream_v) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    if (!scene || !cam || !p || !radiance_out)
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_pathtracer_execute: null argument");
+    const uint32_t W = cam->screen_width, H = cam->screen_height;
+    if (W == 0 || H == 0 || p->spp == 0)
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_pathtracer_execute: empty image (%ux%u, spp %u)", W, H, p->spp);
+    if (p->max_bounces > uint32_t(kMaxBounces))
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "max_bounces %u exceeds %d", p->max_bounces, kMaxBounces);
+    const uint64_t n64 = uint64_t(W) * H * p->spp;
+    if (n64 >= (1ull << 31)) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "too many paths");
+    const size_t n = size_t(n64);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    rr_status st = ensure_queues(ctx, n);
+    if (st != RR_OK) return st;
+    rr_pt_queues& q = ctx->pt;
+    uint32_t* C = ctx->counters;
+    RR_TRY_CUDA(ctx, cudaMemsetAsync(C, 0, sizeof(uint32_t) * kCounterWords, stream));
+
+    PtLaunch L;
+    L.cam = *cam;
+    L.frame_seed = p->frame_seed;
+    L.spp = p->spp;
+    L.width = W; L.height = H;
+    L.tiles_x = (W + 7) / 8;
+    L.tiles_per_image = L.tiles_x * ((H + 3) / 4);
+    {
+        const uint64_t threads = uint64_t(L.tiles_per_image) * p->spp * 32;
+        const uint32_t blocks = uint32_t((threads + kBlock - 1) / kBlock);
+        float4* out = reinterpret_cast<float4*>(radiance_out);
+        rr_stage_timer t0(ctx, stream, (p->flags & RR_PT_FLAG_TIME_STAGES) != 0);
+        t0.begin(0);
+        raygen_kernel<<<blocks, kBlock, 0, stream>>>(L, out, q.ray_a[0], q.ray_b[0], q.ray_c[0], C);
+        RR_CHECK_LAUNCH(ctx);
+        t0.end(0);
+        rr_status st0 = t0.commit();
+        if (st0 != RR_OK) return st0;
+    }
+    const bool count = (p->flags & RR_PT_FLAG_COUNT_TRAVERSAL) != 0;
+    const bool timed = (p->flags & RR_PT_FLAG_TIME_STAGES) != 0;
+    auto ext_k = count ? extend_kernel<true> : extend_kernel<false>;
+    auto sh_k = count ? shadow_kernel<true> : shadow_kernel<false>;
+    const int g_ext = persistent_grid(ctx, reinterpret_cast<const void*>(ext_k));
+    const int g_sh = persistent_grid(ctx, reinterpret_cast<const void*>(sh_k));
+    const int g_shade = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(shade_kernel)),
+                                      int((n + kBlock - 1) / kBlock));
+    if (count) RR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->work64, 0, sizeof(unsigned long long) * 4, stream));
+    const DevScene& S = scene->dev;
+    float4* out = reinterpret_cast<float4*>(radiance_out);
+    rr_stage_timer timer(ctx, stream, timed);
+    for (uint32_t b = 0; b < p->max_bounces; ++b) {
+        const int cur = b & 1, nxt = cur ^ 1;
+        uint32_t* cb = C + 4 * b;
+        uint32_t* cn = C + 4 * (b + 1);
+        timer.begin(1);
+        ext_k<<<g_ext, kBlock, 0, stream>>>(S, q.ray_a[cur], q.ray_b[cur], q.hits, cb, cb + 1, ctx->work64);
+        RR_CHECK_LAUNCH(ctx);
+        timer.end(1);
+        timer.begin(2);
+        shade_kernel<<<g_shade, kBlock, 0, stream>>>(S, b, b + 1 == p->max_bounces ? 1u : 0u,
+                                                     q.ray_a[cur], q.ray_b[cur], q.ray_c[cur], q.hits,
+                                                     q.ray_a[nxt], q.ray_b[nxt], q.ray_c[nxt],
+                                                     q.shadow_a, q.shadow_b, q.shadow_c, out,
+                                                     cb, cn, cb + 2);
+        RR_CHECK_LAUNCH(ctx);
+        timer.end(2);
+        timer.begin(3);
+        sh_k<<<g_sh, kBlock, 0, stream>>>(S, q.shadow_a, q.shadow_b, q.shadow_c, out, cb + 2, cb + 3,
+                                          ctx->work64 + 2);
+        RR_CHECK_LAUNCH(ctx);
+        timer.end(3);
+    }
+    ctx->launches += 1 + 3 * uint64_t(p->max_bounces);
+    ctx->last_max_bounces = p->max_bounces;
+    ctx->last_counted = count;
+    return timer.commit();
+}
+
+extern "C" rr_status rr_pathtracer_stats(rr_ctx* ctx, rr_pt_stats* out, int reset) {
+    if (!ctx || !out) return RR_ERR_INVALID_ARGUMENT;
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    RR_TRY_CUDA(ctx, cudaDeviceSynchronize());
+    uint32_t h[kCounterWords];
+    RR_TRY_CUDA(ctx, cudaMemcpy(h, ctx->counters, sizeof(h), cudaMemcpyDeviceToHost));
+    std::memset(out, 0, sizeof(*out));
+    for (uint32_t b = 0; b < ctx->last_max_bounces; ++b) {
+        out->extension_rays += h[4 * b];
+        out->shadow_rays += h[4 * b + 2];
+    }
+    if (ctx->last_counted) {
+        unsigned long long w[4];
+        RR_TRY_CUDA(ctx, cudaMemcpy(w, ctx->work64, sizeof(w), cudaMemcpyDeviceToHost));
+        out->extension_nodes = w[0]; out->extension_tris = w[1];
+        out->shadow_nodes = w[2]; out->shadow_tris = w[3];
+    }
+    rr_status st = rr_stage_timer::collect(ctx);
+    if (st != RR_OK) return st;
+    out->ms_raygen = ctx->stage_ms[0]; out->ms_extend = ctx->stage_ms[1];
+    out->ms_shade = ctx->stage_ms[2]; out->ms_shadow = ctx->stage_ms[3];
+    out->launches_extend = ctx->stage_launches[1];
+    out->launches_total = ctx->launches;
+    if (reset) {
+        for (int k = 0; k < 4; ++k) { ctx->stage_ms[k] = 0.0; ctx->stage_launches[k] = 0; }
+    }
+    return RR_OK;
+}

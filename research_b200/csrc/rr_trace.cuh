@@ -1,0 +1,234 @@
+// rr_trace.cuh — BVH traversal and watertight ray/triangle intersection.
+//
+// Replaces the hardware RayQuery of pathtracer.slang:45-120 /
+// restir_di.slang:86-146 (driver-built BLAS/TLAS, AccelStructure.cpp:98-330).
+// Semantics kept from the reference: opaque geometry, closest hit in
+// [t_min, t_max], no face culling (every TLAS instance sets
+// TRIANGLE_FACING_CULL_DISABLE, AccelStructure.cpp:90), hit reports the
+// instance index, the mesh-local primitive index and the barycentric weights
+// of vertices 1 and 2. Ties on t go to the lowest (instance, primitive).
+//
+// Geometry is flattened to world space at scene creation (one BVH over every
+// instance's triangles), so a ray is never transformed per instance.
+#pragma once
+
+#include "rr_dev.cuh"
+
+namespace rr {
+
+// One BVH2 node holds the boxes of both children (64 bytes):
+//   a = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)
+//   b = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
+//   c = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)
+//   d = (child0, child1, count0, count1); child >= 0 is an inner node,
+//       child < 0 a leaf whose triangles start at ~child (count in d.z/d.w).
+// One triangle record (48 bytes): (v0.xyz, v1.x), (v1.yz, v2.xy),
+// (v2.z, instance, primitive, flattened id).
+struct DevScene {
+    const float4* nodes;
+    const float4* tris;
+    const float4* vertices;   // GpuVertex as 3 float4
+    const uint32_t* indices;
+    const uint4* meshes;      // GpuMesh as 2 uint4
+    const float4* instances;  // GpuInstance as 5 float4
+    const float4* materials;  // (base.rgb, metallic), (emissive.rgb, roughness)
+    const float4* lights;     // GpuLight as 3 float4
+    uint32_t num_lights;
+    uint32_t num_instances;
+    uint32_t num_tris;
+    uint32_t num_materials;
+};
+
+struct Ray {
+    float3 o, d, inv;
+    float Sx, Sy, Sz;
+    int kx, ky, kz;
+};
+
+RR_D float comp(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+// Per-ray shear constants (Woop, Benthin, Wald, JCGT 2013).
+RR_D Ray make_ray(float3 o, float3 d) {
+    Ray r;
+    r.o = o; r.d = d;
+    int kz = 0;
+    if (fabsf(d.y) > fabsf(comp(d, kz))) kz = 1;
+    if (fabsf(d.z) > fabsf(comp(d, kz))) kz = 2;
+    int kx = kz + 1; if (kx == 3) kx = 0;
+    int ky = kx + 1; if (ky == 3) ky = 0;
+    const float dz = comp(d, kz);
+    if (dz < 0.0f) { const int t = kx; kx = ky; ky = t; }
+    r.kx = kx; r.ky = ky; r.kz = kz;
+    r.Sx = comp(d, kx) / dz;
+    r.Sy = comp(d, ky) / dz;
+    r.Sz = 1.0f / dz;
+    const float sx = fabsf(d.x) < 1e-20f ? copysignf(1e-20f, d.x) : d.x;
+    const float sy = fabsf(d.y) < 1e-20f ? copysignf(1e-20f, d.y) : d.y;
+    const float sz = fabsf(d.z) < 1e-20f ? copysignf(1e-20f, d.z) : d.z;
+    r.inv = f3(1.0f / sx, 1.0f / sy, 1.0f / sz);
+    return r;
+}
+
+// Watertight test; two-sided. On hit writes t and the weights of v1, v2.
+RR_D bool intersect_triangle(const Ray& r, float3 p0, float3 p1, float3 p2, float tmin,
+                             float tmax, float& t, float& bu, float& bv) {
+    const float3 A = p0 - r.o, B = p1 - r.o, C = p2 - r.o;
+    const float Az0 = comp(A, r.kz), Bz0 = comp(B, r.kz), Cz0 = comp(C, r.kz);
+    const float Ax = comp(A, r.kx) - r.Sx * Az0, Ay = comp(A, r.ky) - r.Sy * Az0;
+    const float Bx = comp(B, r.kx) - r.Sx * Bz0, By = comp(B, r.ky) - r.Sy * Bz0;
+    const float Cx = comp(C, r.kx) - r.Sx * Cz0, Cy = comp(C, r.ky) - r.Sy * Cz0;
+    const float U = Cx * By - Cy * Bx;
+    const float V = Ax * Cy - Ay * Cx;
+    const float W = Bx * Ay - By * Ax;
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    const float det = U + V + W;
+    if (det == 0.0f) return false;
+    const float Az = r.Sz * Az0, Bz = r.Sz * Bz0, Cz = r.Sz * Cz0;
+    const float T = U * Az + V * Bz + W * Cz;
+    const float rcp = 1.0f / det;
+    const float tt = T * rcp;
+    if (!(tt >= tmin && tt <= tmax)) return false;
+    t = tt; bu = V * rcp; bv = W * rcp;
+    return true;
+}
+
+// Conservative slab test: the far distance is widened by a few ulps so that
+// rounding never culls a box that holds a hit (Ize, JCGT 2013).
+RR_D void box_pair(const Ray& r, float4 a, float4 b, float4 c, float tmin, float tmax,
+                   bool& h0, bool& h1, float& n0, float& n1) {
+    const float ox = r.o.x, oy = r.o.y, oz = r.o.z;
+    const float ix = r.inv.x, iy = r.inv.y, iz = r.inv.z;
+    {
+        const float tx0 = (a.x - ox) * ix, tx1 = (a.y - ox) * ix;
+        const float ty0 = (a.z - oy) * iy, ty1 = (a.w - oy) * iy;
+        const float tz0 = (c.x - oz) * iz, tz1 = (c.y - oz) * iz;
+        const float nn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+        const float ff = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)) , fmaxf(tz0, tz1)) * 1.000002f;
+        h0 = nn <= fminf(ff, tmax);
+        n0 = nn;
+    }
+    {
+        const float tx0 = (b.x - ox) * ix, tx1 = (b.y - ox) * ix;
+        const float ty0 = (b.z - oy) * iy, ty1 = (b.w - oy) * iy;
+        const float tz0 = (c.z - oz) * iz, tz1 = (c.w - oz) * iz;
+        const float nn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+        const float ff = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1)) * 1.000002f;
+        h1 = nn <= fminf(ff, tmax);
+        n1 = nn;
+    }
+}
+
+struct HitRec {
+    float t, u, v;
+    uint32_t inst, prim, key;
+};
+
+constexpr int kStackSize = 64;
+
+// Work counters of one traversal (only maintained when Count = true).
+struct TraceWork {
+    uint32_t nodes = 0;
+    uint32_t tris = 0;
+};
+
+// Closest hit (AnyHit = false) or any hit (AnyHit = true) in [tmin, tmax].
+// Returns true on hit. `hit` is filled for closest-hit queries.
+template <bool AnyHit, bool Count = false>
+RR_D bool trace(const DevScene& s, const Ray& r, float tmin, float tmax, HitRec& hit, TraceWork* work = nullptr) {
+    int stack[kStackSize];
+    float nears[kStackSize];
+    int sp = 0;
+    int node = 0;
+    bool found = false;
+    hit.t = tmax; hit.key = kNoIndex;
+    while (true) {
+        const float4 a = __ldg(s.nodes + node * 4 + 0);
+        const float4 b = __ldg(s.nodes + node * 4 + 1);
+        const float4 c = __ldg(s.nodes + node * 4 + 2);
+        const int4 d = __ldg(reinterpret_cast<const int4*>(s.nodes) + node * 4 + 3);
+        if (Count) work->nodes++;
+        bool h0, h1; float n0, n1;
+        box_pair(r, a, b, c, tmin, hit.t, h0, h1, n0, n1);
+        // leaves are intersected right away
+        #pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const bool hk = k == 0 ? h0 : h1;
+            const int child = k == 0 ? d.x : d.y;
+            if (hk && child < 0) {
+                const int first = ~child;
+                const int count = k == 0 ? d.z : d.w;
+                for (int i = first; i < first + count; ++i) {
+                    if (Count) work->tris++;
+                    const float4 t0 = __ldg(s.tris + i * 3 + 0);
+                    const float4 t1 = __ldg(s.tris + i * 3 + 1);
+                    const float4 t2 = __ldg(s.tris + i * 3 + 2);
+                    float tt, uu, vv;
+                    if (intersect_triangle(r, f3(t0.x, t0.y, t0.z), f3(t0.w, t1.x, t1.y),
+                                           f3(t1.z, t1.w, t2.x), tmin, hit.t, tt, uu, vv)) {
+                        const uint32_t key = __float_as_uint(t2.w);
+                        if (AnyHit) { hit.t = tt; return true; }
+                        if (!found || tt < hit.t || (tt == hit.t && key < hit.key)) {
+                            found = true;
+                            hit.t = tt; hit.u = uu; hit.v = vv; hit.key = key;
+                            hit.inst = __float_as_uint(t2.y); hit.prim = __float_as_uint(t2.z);
+                        }
+                    }
+                }
+            }
+        }
+        const bool i0 = h0 && d.x >= 0 && n0 <= hit.t;
+        const bool i1 = h1 && d.y >= 0 && n1 <= hit.t;
+        if (i0 && i1) {
+            const bool first0 = n0 <= n1;
+            stack[sp] = first0 ? d.y : d.x;
+            nears[sp] = first0 ? n1 : n0;
+            ++sp;
+            node = first0 ? d.x : d.y;
+        } else if (i0) {
+            node = d.x;
+        } else if (i1) {
+            node = d.y;
+        } else {
+            bool popped = false;
+            while (sp > 0) {
+                --sp;
+                if (nears[sp] <= hit.t) { node = stack[sp]; popped = true; break; }
+            }
+            if (!popped) break;
+        }
+    }
+    return found;
+}
+
+// Hit attributes (pathtracer.slang:69-118 / restir_di.slang:108-144):
+// instance -> mesh -> 3 indices -> 3 vertices, barycentric interpolation in
+// object space, then the row-major instance transform (normals use the upper
+// 3x3, not the inverse transpose, as the reference does).
+struct Surface {
+    float3 pos, normal;
+    uint32_t material;
+};
+
+RR_D Surface hit_surface(const DevScene& s, uint32_t inst_idx, uint32_t prim, float bu, float bv) {
+    const float4* ip = s.instances + inst_idx * 5;
+    const float4 r0 = __ldg(ip + 0), r1 = __ldg(ip + 1), r2 = __ldg(ip + 2);
+    const uint32_t mesh_index = __float_as_uint(__ldg(ip + 4).x);
+    const uint4 m0 = __ldg(s.meshes + mesh_index * 2 + 0);  // vertex_base, vertex_count, index_byte_offset, index_count
+    const uint4 m1 = __ldg(s.meshes + mesh_index * 2 + 1);  // material_index, pad
+    const uint32_t base = m0.z / 4u + prim * 3u;
+    const uint32_t i0 = __ldg(s.indices + base), i1 = __ldg(s.indices + base + 1), i2 = __ldg(s.indices + base + 2);
+    const float4 va0 = __ldg(s.vertices + (m0.x + i0) * 3), vb0 = __ldg(s.vertices + (m0.x + i0) * 3 + 1);
+    const float4 va1 = __ldg(s.vertices + (m0.x + i1) * 3), vb1 = __ldg(s.vertices + (m0.x + i1) * 3 + 1);
+    const float4 va2 = __ldg(s.vertices + (m0.x + i2) * 3), vb2 = __ldg(s.vertices + (m0.x + i2) * 3 + 1);
+    const float b0 = 1.0f - bu - bv;
+    const float3 lp = b0 * xyz(va0) + bu * xyz(va1) + bv * xyz(va2);
+    const float3 n0 = f3(va0.w, vb0.x, vb0.y), n1 = f3(va1.w, vb1.x, vb1.y), n2 = f3(va2.w, vb2.x, vb2.y);
+    const float3 ln = normalize(b0 * n0 + bu * n1 + bv * n2);
+    Surface sf;
+    sf.pos = mul_rows_point(r0, r1, r2, lp, 1.0f);
+    sf.normal = normalize(mul_rows_dir(r0, r1, r2, ln));
+    sf.material = m1.x;
+    return sf;
+}
+
+} // namespace rr

@@ -1,0 +1,295 @@
+"""GPU parity: every kernel against the CPU oracle on the same seeded inputs.
+
+The kernels and the oracle evaluate the same binary32 operations in the same
+order (no FMA contraction, IEEE division/sqrt, the rr_detmath.h elementary
+functions), so the stated tolerance is ZERO: images, G-buffers, reservoirs,
+hits and guiding state must be bit-identical. Calls go through the C ABI.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+def _stream(torch):
+    return torch.cuda.current_stream().cuda_stream
+
+
+@pytest.fixture(scope="module")
+def cornell(rr, O, ctx):
+    hs = rr.HostScene.cornell(0)
+    return hs.arrays, rr.Scene(ctx, hs.arrays), O.OracleScene(hs.arrays, use_bvh=False)
+
+
+@pytest.fixture(scope="module")
+def procedural(rr, O, ctx):
+    hs = rr.HostScene.procedural(seed=0x5EED0002, target_triangles=120_000, emissive_triangles=128, box_half=20.0)
+    return hs.arrays, rr.Scene(ctx, hs.arrays), O.OracleScene(hs.arrays, use_bvh=True)
+
+
+def cam_for(rr, kind, w, h):
+    if kind == "cornell":
+        return rr.camera_data(rr.camera_desc(w, h))
+    return rr.camera_data(rr.camera_desc(w, h, eye=(0.0, 8.0, 45.0), center=(0.0, -2.0, 0.0)))
+
+
+def gpu_pathtrace(rr, ctx, scene, cam, torch, frame_seed, max_bounces, spp):
+    out = torch.empty((spp, cam.screen_height, cam.screen_width, 4), device="cuda", dtype=torch.float32)
+    p = rr.PtParams(frame_seed, max_bounces, spp, 0)
+    ctx.check(rr.lib().rr_pathtracer_execute(ctx.handle, scene.handle, C.byref(cam), C.byref(p), out.data_ptr(),
+                                             _stream(torch)))
+    torch.cuda.synchronize()
+    return _np(out)
+
+
+def test_trace_closest_matches_oracle(rr, O, ctx, torch_cuda, cornell, procedural):
+    torch = torch_cuda
+    rng = np.random.default_rng(11)
+    for arrays, scene, oscene, span in (cornell + (1.0,), procedural + (25.0,)):
+        n = 20000
+        o = np.zeros((n, 4), np.float32)
+        o[:, :3] = rng.uniform(-span, span, (n, 3))
+        d = np.zeros((n, 4), np.float32)
+        v = rng.normal(size=(n, 3))
+        d[:, :3] = v / np.linalg.norm(v, axis=1, keepdims=True)
+        ho, po = oscene.trace(o, d)
+        to, td = torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda()
+        hits = torch.empty((n, 4), device="cuda")
+        prims = torch.empty(n, device="cuda", dtype=torch.int32)
+        ctx.check(rr.lib().rr_trace_closest(ctx.handle, scene.handle, to.data_ptr(), td.data_ptr(), 0.001, 1e9, n,
+                                            hits.data_ptr(), prims.data_ptr(), _stream(torch)))
+        torch.cuda.synchronize()
+        hg, pg = _np(hits), _np(prims).view(np.uint32)
+        assert (ho[:, 3].view(np.uint32) != 0xFFFFFFFF).mean() > 0.3
+        np.testing.assert_array_equal(hg.view(np.uint32), ho.view(np.uint32))
+        np.testing.assert_array_equal(pg, po)
+
+
+@pytest.mark.parametrize("seed", [0, 7])
+def test_pathtracer_cornell_bit_exact(rr, O, ctx, torch_cuda, cornell, seed):
+    _, scene, oscene = cornell
+    cam = cam_for(rr, "cornell", 64, 48)
+    g = gpu_pathtrace(rr, ctx, scene, cam, torch_cuda, seed, 8, 2)
+    o, _ = O.pathtrace(oscene, cam, seed, 8, 2)
+    assert g[..., :3].mean() > 0.1
+    np.testing.assert_array_equal(g.view(np.uint32), o.view(np.uint32))
+
+
+def test_pathtracer_counts_match_oracle(rr, O, ctx, torch_cuda, cornell):
+    _, scene, oscene = cornell
+    cam = cam_for(rr, "cornell", 40, 40)
+    gpu_pathtrace(rr, ctx, scene, cam, torch_cuda, 3, 5, 1)
+    st = rr.PtStats()
+    ctx.check(rr.lib().rr_pathtracer_stats(ctx.handle, C.byref(st), 1))
+    _, (oe, os_) = O.pathtrace(oscene, cam, 3, 5, 1)
+    assert (st.extension_rays, st.shadow_rays) == (oe, os_)
+
+
+def test_pathtracer_count_and_timing_flags_keep_results(rr, O, ctx, torch_cuda, procedural):
+    torch = torch_cuda
+    _, scene, _ = procedural
+    cam = cam_for(rr, "procedural", 64, 40)
+    ref = gpu_pathtrace(rr, ctx, scene, cam, torch, 2, 5, 1)
+    out = torch.empty((1, 40, 64, 4), device="cuda")
+    p = rr.PtParams(2, 5, 1, rr.PT_FLAG_COUNT_TRAVERSAL | rr.PT_FLAG_TIME_STAGES)
+    ctx.check(rr.lib().rr_pathtracer_execute(ctx.handle, scene.handle, C.byref(cam), C.byref(p), out.data_ptr(),
+                                             _stream(torch)))
+    st = rr.PtStats()
+    ctx.check(rr.lib().rr_pathtracer_stats(ctx.handle, C.byref(st), 1))
+    np.testing.assert_array_equal(_np(out), ref)
+    assert st.extension_nodes >= st.extension_rays and st.extension_tris > 0
+    assert st.launches_extend == 5 and st.ms_extend > 0
+
+
+def test_pathtracer_procedural_bit_exact(rr, O, ctx, torch_cuda, procedural):
+    _, scene, oscene = procedural
+    cam = cam_for(rr, "procedural", 96, 64)
+    g = gpu_pathtrace(rr, ctx, scene, cam, torch_cuda, 5, 5, 1)
+    o, _ = O.pathtrace(oscene, cam, 5, 5, 1)
+    np.testing.assert_array_equal(g.view(np.uint32), o.view(np.uint32))
+
+
+def test_pathtracer_region_odd_size(rr, O, ctx, torch_cuda, cornell):
+    # non-multiple-of-tile image sizes exercise the raygen compaction
+    _, scene, oscene = cornell
+    cam = cam_for(rr, "cornell", 37, 19)
+    g = gpu_pathtrace(rr, ctx, scene, cam, torch_cuda, 1, 4, 3)
+    o, _ = O.pathtrace(oscene, cam, 1, 4, 3)
+    np.testing.assert_array_equal(g.view(np.uint32), o.view(np.uint32))
+
+
+def test_accumulate_bit_exact_and_fp64(rr, O, ctx, torch_cuda):
+    torch = torch_cuda
+    rng = np.random.default_rng(5)
+    W, H = 33, 17
+    frames = rng.random((6, H, W, 4)).astype(np.float32) * 3
+    acc_o = np.zeros((H, W, 4), np.float32)
+    acc_g = torch.zeros((H, W, 4), device="cuda")
+    sum64 = torch.zeros((H, W, 4), device="cuda", dtype=torch.float64)
+    fr = torch.from_numpy(frames).cuda()
+    spp = 0
+    # one frame with camera_moved, then batches of 2 and 3 frames
+    for start, count, moved in ((0, 1, 1), (1, 2, 0), (3, 3, 0)):
+        for k in range(count):
+            O.accumulate(np.ascontiguousarray(frames[start + k]), acc_o, moved if k == 0 else 0, spp + k)
+        p = rr.AccParams(W, H, moved, spp)
+        ctx.check(rr.lib().rr_accumulate_execute(ctx.handle, fr[start].data_ptr(), count, acc_g.data_ptr(),
+                                                 sum64.data_ptr(), C.byref(p), _stream(torch)))
+        spp = (0 if moved else spp) + count
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(_np(acc_g).view(np.uint32), acc_o.view(np.uint32))
+    np.testing.assert_allclose(_np(sum64), frames.astype(np.float64).sum(0), rtol=1e-12)
+
+
+def _di_run_gpu(rr, ctx, torch, scene, cam, params_list):
+    W, H = cam.screen_width, cam.screen_height
+    t = lambda: torch.zeros((H, W, 4), device="cuda")
+    gpos, gnrm, out = t(), t(), t()
+    res = [t(), t()]
+    outs = []
+    for f, p in enumerate(params_list):
+        cur, prev = res[f & 1], res[(f & 1) ^ 1]
+        ctx.check(rr.lib().rr_restir_di_execute(ctx.handle, scene.handle, C.byref(cam), C.byref(p), gpos.data_ptr(),
+                                                gnrm.data_ptr(), cur.data_ptr(), prev.data_ptr(), out.data_ptr(),
+                                                _stream(torch)))
+        torch.cuda.synchronize()
+        outs.append((_np(gpos).copy(), _np(gnrm).copy(), _np(cur).copy(), _np(out).copy()))
+    return outs
+
+
+def _di_run_oracle(O, oscene, cam, params_list):
+    W, H = cam.screen_width, cam.screen_height
+    z = lambda: np.zeros((H, W, 4), np.float32)
+    gpos, gnrm, out = z(), z(), z()
+    res = [z(), z()]
+    outs = []
+    for f, p in enumerate(params_list):
+        cur, prev = res[f & 1], res[(f & 1) ^ 1]
+        O.restir_di_initial(oscene, cam, p, gpos, gnrm, cur)
+        O.restir_di_temporal(oscene, cam, p, gpos, gnrm, cur, prev)
+        O.restir_di_spatial_shade(oscene, cam, p, gpos, gnrm, cur, out)
+        outs.append((gpos.copy(), gnrm.copy(), cur.copy(), out.copy()))
+    return outs
+
+
+@pytest.mark.parametrize("kind", ["cornell", "procedural"])
+def test_restir_di_three_frames_bit_exact(rr, O, ctx, torch_cuda, cornell, procedural, kind):
+    arrays, scene, oscene = cornell if kind == "cornell" else procedural
+    cam = cam_for(rr, kind, 80, 56)
+    # config-2 settings: M=32, K=5, R=30, cap 20*M; frames 0..2 exercise temporal reuse
+    plist_g = [rr.DIParams(f, 32, 1, 1, 5, 30, 20, 0) for f in range(3)]
+    plist_o = [O.di_params(f, 32, 1, 1, 5, 30, 20) for f in range(3)]
+    g = _di_run_gpu(rr, ctx, torch_cuda, scene, cam, plist_g)
+    o = _di_run_oracle(O, oscene, cam, plist_o)
+    for (gg, go) in zip(g, o):
+        for a, b in zip(gg, go):
+            np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert (o[-1][2][..., 3].view(np.uint32) > 32).any()  # temporal history was merged
+
+
+def test_restir_di_disabled_paths(rr, O, ctx, torch_cuda, cornell):
+    _, scene, oscene = cornell
+    cam = cam_for(rr, "cornell", 24, 24)
+    plist_g = [rr.DIParams(f, 4, 0, 0, 0, 10, 20, 0) for f in range(2)]
+    plist_o = [O.di_params(f, 4, 0, 0, 0, 10, 20) for f in range(2)]
+    g = _di_run_gpu(rr, ctx, torch_cuda, scene, cam, plist_g)
+    o = _di_run_oracle(O, oscene, cam, plist_o)
+    for a, b in zip(g[-1], o[-1]):
+        np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+@pytest.mark.parametrize("iterations", [1, 5, 7])
+def test_atrous_bit_exact(rr, O, ctx, torch_cuda, procedural, iterations):
+    torch = torch_cuda
+    _, scene, oscene = procedural
+    cam = cam_for(rr, "procedural", 72, 40)
+    p = O.di_params(0, 8, 1, 1, 4, 15, 20)
+    W, H = 72, 40
+    z = lambda: np.zeros((H, W, 4), np.float32)
+    gpos, gnrm, res, prev, out = z(), z(), z(), z(), z()
+    O.restir_di_initial(oscene, cam, p, gpos, gnrm, res)
+    O.restir_di_spatial_shade(oscene, cam, p, gpos, gnrm, res, out)
+    ref = O.atrous(out, gpos, gnrm, iterations)
+    t = lambda a: torch.from_numpy(a).cuda()
+    tin, tp, tn = t(out), t(gpos), t(gnrm)
+    ping = [torch.empty_like(tin), torch.empty_like(tin)]
+    ap = rr.AtrousParams(W, H, iterations, 0, 0.25, 0.20, 1.0, 0)
+    slot = C.c_uint32()
+    ctx.check(rr.lib().rr_atrous_execute(ctx.handle, tin.data_ptr(), tp.data_ptr(), tn.data_ptr(), ping[0].data_ptr(),
+                                         ping[1].data_ptr(), C.byref(ap), C.byref(slot), _stream(torch)))
+    torch.cuda.synchronize()
+    assert slot.value == (min(iterations, 7) - 1) & 1
+    np.testing.assert_array_equal(_np(ping[slot.value]).view(np.uint32), ref.view(np.uint32))
+
+
+def test_guiding_splat_fit_sample_bit_exact(rr, O, ctx, torch_cuda):
+    torch = torch_cuda
+    rng = np.random.default_rng(9)
+    cells = 1 << 12
+    n = 50000
+    pos = np.zeros((n, 4), np.float32); pos[:, :3] = rng.uniform(-2, 2, (n, 3))
+    dirs = np.zeros((n, 4), np.float32)
+    v = rng.normal(size=(n, 3)) + np.array([0.0, 2.0, 0.0])
+    dirs[:, :3] = v / np.linalg.norm(v, axis=1, keepdims=True)
+    bsdf = rng.integers(0, 3, n).astype(np.uint32)
+    cam = np.array([0.0, 0.5, 4.0], np.float32)
+    gp_o = O.guiding_params(cell_count=cells, min_samples=4, base_cell_size=0.5, distance_slope=0.05)
+    gp_g = rr.GuidingParams(0.5, 0.05, cells, 1, 4, 512.0, 0.5, 0)
+    acc_o = np.zeros((cells, 4), np.int32); fit_o = np.zeros((cells, 4), np.float32)
+    O.guiding_splat(acc_o, pos, dirs, bsdf, cam, gp_o)
+    acc_before = acc_o.copy()
+    O.guiding_fit(acc_o, fit_o, gp_o)
+    acc_g = torch.zeros((cells, 4), device="cuda", dtype=torch.int32)
+    fit_g = torch.zeros((cells, 4), device="cuda")
+    t = lambda a: torch.from_numpy(a).cuda()
+    cp = (C.c_float * 3)(*cam.tolist())
+    ctx.check(rr.lib().rr_guiding_splat(ctx.handle, acc_g.data_ptr(), t(pos).data_ptr(), t(dirs).data_ptr(),
+                                        t(bsdf.view(np.int32)).data_ptr(), n, cp, C.byref(gp_g), _stream(torch)))
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(_np(acc_g), acc_before)
+    ctx.check(rr.lib().rr_guiding_fit(ctx.handle, acc_g.data_ptr(), fit_g.data_ptr(), C.byref(gp_g), _stream(torch)))
+    torch.cuda.synchronize()
+    assert not _np(acc_g).any()
+    np.testing.assert_array_equal(_np(fit_g).view(np.uint32), fit_o.view(np.uint32))
+    assert (fit_o[:, 3] > 0).sum() > 50
+    # one-sample MIS sampling at new points, guided where a lobe exists
+    m = 20000
+    sp = np.zeros((m, 4), np.float32); sp[:, :3] = rng.uniform(-2, 2, (m, 3))
+    sn = np.zeros((m, 4), np.float32)
+    vv = rng.normal(size=(m, 3)); sn[:, :3] = vv / np.linalg.norm(vv, axis=1, keepdims=True)
+    sb = rng.integers(0, 3, m).astype(np.uint32)
+    seeds = rng.integers(0, 2 ** 32, m, dtype=np.uint64).astype(np.uint32)
+    so = seeds.copy()
+    wi_o, pdf_o = O.guiding_sample(fit_o, sp, sn, sb, so, cam, gp_o)
+    sg = t(seeds.view(np.int32))
+    wi_g = torch.empty((m, 4), device="cuda"); pdf_g = torch.empty(m, device="cuda")
+    ctx.check(rr.lib().rr_guiding_sample(ctx.handle, fit_g.data_ptr(), t(sp).data_ptr(), t(sn).data_ptr(),
+                                         t(sb.view(np.int32)).data_ptr(), sg.data_ptr(), m, cp, C.byref(gp_g),
+                                         wi_g.data_ptr(), pdf_g.data_ptr(), _stream(torch)))
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(_np(wi_g).view(np.uint32), wi_o.view(np.uint32))
+    np.testing.assert_array_equal(_np(pdf_g).view(np.uint32), pdf_o.view(np.uint32))
+    np.testing.assert_array_equal(_np(sg).view(np.uint32), so)
+
+
+def test_detmath_against_cuda_libm(rr, O, ctx, torch_cuda):
+    """rr_detmath.h through the oracle stays within 2 ulp of CUDA's own
+    sinf/cosf/expf/logf (accurate mode) on the argument ranges of the path."""
+    torch = torch_cuda
+    x = np.linspace(0, 2 * np.pi, 200001, dtype=np.float32)
+    xs = torch.from_numpy(x).cuda()
+    for name, fn in (("sin", torch.sin), ("cos", torch.cos)):
+        ref = _np(fn(xs)).astype(np.float64)
+        ours = O.detmath(name, x).astype(np.float64)
+        ulp = np.spacing(np.abs(ref).astype(np.float32)).astype(np.float64)
+        assert (np.abs(ours - ref) / ulp).max() <= 3.0
+    e = np.linspace(-80, 0, 200001, dtype=np.float32)
+    ref = _np(torch.exp(torch.from_numpy(e).cuda())).astype(np.float64)
+    ulp = np.spacing(np.abs(ref).astype(np.float32)).astype(np.float64)
+    assert (np.abs(O.detmath("exp", e) - ref) / ulp).max() <= 3.0

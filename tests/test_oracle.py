@@ -1,0 +1,143 @@
+"""CPU checks of the oracle itself: known-answer vectors and analytic properties.
+
+The reference ships no tests or golden vectors; the RNG known answers below
+were computed from the formula of Common.slang:18-28 / Sampling.slang:11-30
+(pcg_hash, make_seed, rand_float) in 32-bit unsigned arithmetic, and are also
+re-derived here by an independent pure-Python restatement.
+"""
+import math
+
+import numpy as np
+import pytest
+
+# (input, pcg_hash(input))
+PCG_KAT = [(0, 0x07BB2FE2), (1, 0xA8BEEA3C), (2, 0x7A7ECC88), (0xFFFFFFFF, 0xE62A4902), (12345, 0xF45EAD0E)]
+# ((px, py, frame), make_seed, first two rand_float)
+SEED_KAT = [((0, 0, 0), 0x07BB2FE2, 0.190399349, 0.499476671),
+            ((1, 0, 0), 0xA8BEEA3C, 0.910801947, 0.138429046),
+            ((0, 1, 0), 0x9734F28B, 0.268874466, 0.641497195),
+            ((128, 128, 0), 0x3D67FDC9, 0.935119748, 0.568711281),
+            ((0, 0, 1), 0x703CC78A, 0.98334682, 0.724128723)]
+
+
+def py_pcg(x):
+    s = (x * 747796405 + 2891336453) & 0xFFFFFFFF
+    w = (((s >> ((s >> 28) + 4)) ^ s) * 277803737) & 0xFFFFFFFF
+    return ((w >> 22) ^ w) & 0xFFFFFFFF
+
+
+@pytest.mark.parametrize("x,h", PCG_KAT)
+def test_pcg_hash_kat(O, x, h):
+    assert O.pcg_hash(x) == h
+    assert py_pcg(x) == h
+
+
+@pytest.mark.parametrize("pix,seed,r0,r1", SEED_KAT)
+def test_make_seed_and_rand_kat(O, pix, seed, r0, r1):
+    assert O.make_seed(*pix) == seed
+    h = (pix[0] ^ ((pix[1] * 1000003) & 0xFFFFFFFF) ^ ((pix[2] * 2654435761) & 0xFFFFFFFF)) & 0xFFFFFFFF
+    assert py_pcg(h) == seed
+    (a, b), _ = O.rand_floats(seed, 2)
+    assert a == pytest.approx(r0, abs=5e-9) and b == pytest.approx(r1, abs=5e-9)
+    # rand_float = (pcg(seed) >> 8) * 2^-24 exactly
+    assert a == np.float32((py_pcg(seed) >> 8) * 2.0 ** -24)
+
+
+def _ulp_err(y, ref):
+    ref32 = ref.astype(np.float32)
+    ulp = np.spacing(np.abs(ref32)).astype(np.float64)
+    return np.abs(y.astype(np.float64) - ref) / ulp
+
+
+def test_detmath_accuracy(O):
+    x = np.linspace(0, 8 * math.pi, 400001, dtype=np.float32)
+    assert _ulp_err(O.detmath("sin", x), np.sin(x.astype(np.float64))).max() <= 2.0
+    assert _ulp_err(O.detmath("cos", x), np.cos(x.astype(np.float64))).max() <= 2.0
+    e = np.linspace(-87, 88, 400001, dtype=np.float32)
+    assert _ulp_err(O.detmath("exp", e), np.exp(e.astype(np.float64))).max() <= 2.0
+    lg = (np.linspace(1e-3, 1, 400001) ** 3 * 1e3).astype(np.float32)
+    lg = lg[lg != 1.0]
+    assert _ulp_err(O.detmath("log", lg), np.log(lg.astype(np.float64))).max() <= 2.0
+    # edge values
+    assert O.detmath("log", np.array([0.0], np.float32))[0] == -np.inf
+    assert O.detmath("exp", np.array([-200.0], np.float32))[0] == 0.0
+    assert O.detmath("exp", np.array([0.0], np.float32))[0] == 1.0
+    assert O.detmath("log", np.array([1.0], np.float32))[0] == 0.0
+
+
+def _sphere_dirs(n, seed=0):
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=(n, 3))
+    return (v / np.linalg.norm(v, axis=1, keepdims=True)).astype(np.float32)
+
+
+@pytest.mark.parametrize("kappa", [0.5, 2.0, 10.0, 100.0])
+def test_vmf_pdf_normalised(O, kappa):
+    # integrate vMF pdf over the sphere by quadrature in cos(theta)
+    mu = np.array([0.0, 0.0, 1.0], np.float32)
+    ws = np.linspace(-1, 1, 20001)
+    vals = [O.vmf_pdf(mu, kappa, np.array([math.sqrt(max(0, 1 - w * w)), 0.0, w], np.float32)) for w in ws]
+    integral = 2 * math.pi * np.trapezoid(vals, ws)
+    assert integral == pytest.approx(1.0, rel=2e-3)
+
+
+def test_brdf_sample_pdf_and_value_consistent(O):
+    # brdf_sample returns brdf_eval at the sampled direction (BRDF.slang:171)
+    rng = np.random.default_rng(1)
+    n = np.array([0, 0, 1], np.float32)
+    for _ in range(200):
+        wo = _sphere_dirs(1, rng.integers(1 << 30))[0]
+        wo[2] = abs(wo[2]) + 0.05
+        wo /= np.linalg.norm(wo)
+        base = rng.uniform(0.05, 0.95, 3).astype(np.float32)
+        m, r = float(rng.integers(0, 2)), float(rng.uniform(0.05, 1))
+        wi, pdf, f = O.brdf_sample(wo, n, base, m, r, float(rng.random()), float(rng.random()))
+        assert pdf >= 1e-6
+        if np.any(f != 0):
+            np.testing.assert_array_equal(f, O.brdf_eval(n, wo, wi, base, m, r))
+
+
+def test_banerjee_fit_kappa(O):
+    gp = O.guiding_params(cell_count=4, min_samples=1)
+    accum = np.zeros((4, 4), np.int32)
+    fitted = np.zeros((4, 4), np.float32)
+    # cell 0: 10 identical +z splats -> r clamps to 0.9999 -> kappa clamps to kappa_max
+    # cell 1: +x and -x -> r = 1e-4 -> kappa = 0.5 (clamp)
+    accum[0] = [0, 0, 10 * (1 << 20), 10]
+    accum[1] = [0, 0, 0, 2]
+    accum[2] = [0, 0, 0, 0]
+    O.guiding_fit(accum, fitted, gp)
+    assert fitted[0, 3] == 512.0 and tuple(fitted[0, :3]) == (0.0, 0.0, 1.0)
+    assert fitted[1, 3] == 0.5 and tuple(fitted[1, :3]) == (0.0, 0.0, 1.0)
+    assert fitted[2, 3] == -1.0
+    assert not accum.any()  # accumulators reset by the fit
+    # closed form on a generic r
+    r = np.float32(0.6)
+    k = r * (np.float32(3) - r * r) / (np.float32(1) - r * r)
+    accum[3] = [int(0.6 * (1 << 20)) * 100, 0, 0, 100]
+    O.guiding_fit(accum, fitted, gp)
+    assert fitted[3, 3] == pytest.approx(float(k), rel=1e-5)
+
+
+def test_atrous_flat_image_is_fixed_point(O):
+    # flat radiance + flat G-buffer: every tap weighs the same colour -> identity
+    H, W = 32, 40
+    inp = np.full((H, W, 4), 0.5, np.float32)
+    gpos = np.zeros((H, W, 4), np.float32); gpos[..., 3] = 1.0
+    gnrm = np.zeros((H, W, 4), np.float32); gnrm[..., 2] = 1.0
+    out = O.atrous(inp, gpos, gnrm, 5)
+    np.testing.assert_allclose(out, inp, rtol=1e-6)
+
+
+def test_atrous_kernel_weights_sum_to_one():
+    k = np.array([1, 4, 6, 4, 1], np.float32)
+    assert (np.outer(k, k) / 256.0).sum() == 1.0
+
+
+def test_accumulate_running_mean(O):
+    rng = np.random.default_rng(3)
+    frames = rng.random((5, 8, 8, 4)).astype(np.float32)
+    acc = np.zeros((8, 8, 4), np.float32)
+    for k in range(5):
+        O.accumulate(np.ascontiguousarray(frames[k]), acc, 1 if k == 0 else 0, k)
+    np.testing.assert_allclose(acc, frames.mean(0), rtol=1e-5)
