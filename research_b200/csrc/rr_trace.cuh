@@ -37,6 +37,7 @@ struct DevScene {
     uint32_t num_instances;
     uint32_t num_tris;
     uint32_t num_materials;
+    uint32_t num_nodes;
 };
 
 struct Ray {
@@ -141,7 +142,9 @@ RR_D bool trace(const DevScene& s, const Ray& r, float tmin, float tmax, HitRec&
     int node = 0;
     bool found = false;
     hit.t = tmax; hit.key = kNoIndex;
-    while (true) {
+    // A tree visits each node at most once; the bound only guards against a
+    // malformed node array turning into an endless loop.
+    for (uint32_t visits = 0; visits <= s.num_nodes; ++visits) {
         const float4 a = __ldg(s.nodes + node * 4 + 0);
         const float4 b = __ldg(s.nodes + node * 4 + 1);
         const float4 c = __ldg(s.nodes + node * 4 + 2);

@@ -211,6 +211,7 @@ rr_status rr_scene_create(rr_ctx* ctx, const rr_scene_desc* d, rr_scene** out) {
     s->dev.num_instances = d->instance_count;
     s->dev.num_tris = ntri;
     s->dev.num_materials = d->material_count;
+    s->dev.num_nodes = uint32_t(bvh.nodes.size() / 4);
     auto t2 = std::chrono::steady_clock::now();
     s->stats.triangle_count = ntri;
     s->stats.bvh_node_count = uint32_t(bvh.nodes.size() / 4);

@@ -249,8 +249,10 @@ def test_guiding_splat_fit_sample_bit_exact(rr, O, ctx, torch_cuda):
     fit_g = torch.zeros((cells, 4), device="cuda")
     t = lambda a: torch.from_numpy(a).cuda()
     cp = (C.c_float * 3)(*cam.tolist())
-    ctx.check(rr.lib().rr_guiding_splat(ctx.handle, acc_g.data_ptr(), t(pos).data_ptr(), t(dirs).data_ptr(),
-                                        t(bsdf.view(np.int32)).data_ptr(), n, cp, C.byref(gp_g), _stream(torch)))
+    # keep every input tensor referenced until the kernels have run
+    tpos, tdirs, tbsdf = t(pos), t(dirs), t(bsdf.view(np.int32))
+    ctx.check(rr.lib().rr_guiding_splat(ctx.handle, acc_g.data_ptr(), tpos.data_ptr(), tdirs.data_ptr(),
+                                        tbsdf.data_ptr(), n, cp, C.byref(gp_g), _stream(torch)))
     torch.cuda.synchronize()
     np.testing.assert_array_equal(_np(acc_g), acc_before)
     ctx.check(rr.lib().rr_guiding_fit(ctx.handle, acc_g.data_ptr(), fit_g.data_ptr(), C.byref(gp_g), _stream(torch)))
@@ -269,8 +271,9 @@ def test_guiding_splat_fit_sample_bit_exact(rr, O, ctx, torch_cuda):
     wi_o, pdf_o = O.guiding_sample(fit_o, sp, sn, sb, so, cam, gp_o)
     sg = t(seeds.view(np.int32))
     wi_g = torch.empty((m, 4), device="cuda"); pdf_g = torch.empty(m, device="cuda")
-    ctx.check(rr.lib().rr_guiding_sample(ctx.handle, fit_g.data_ptr(), t(sp).data_ptr(), t(sn).data_ptr(),
-                                         t(sb.view(np.int32)).data_ptr(), sg.data_ptr(), m, cp, C.byref(gp_g),
+    tsp, tsn, tsb = t(sp), t(sn), t(sb.view(np.int32))
+    ctx.check(rr.lib().rr_guiding_sample(ctx.handle, fit_g.data_ptr(), tsp.data_ptr(), tsn.data_ptr(),
+                                         tsb.data_ptr(), sg.data_ptr(), m, cp, C.byref(gp_g),
                                          wi_g.data_ptr(), pdf_g.data_ptr(), _stream(torch)))
     torch.cuda.synchronize()
     np.testing.assert_array_equal(_np(wi_g).view(np.uint32), wi_o.view(np.uint32))
