@@ -202,6 +202,23 @@ rr_status rr_atrous_execute(rr_ctx* ctx, const float* input, const float* gbuf_p
                             const float* gbuf_norm, float* ping0, float* ping1,
                             const rr_atrous_params* params, uint32_t* out_slot, void* stream);
 
+/* No counterpart in the reference: an A-trous entry point that allocates
+ * nothing, for callers that cannot allocate device memory (an engine that
+ * only lends the library buffers from its own fixed budget, a host that
+ * forbids cudaMalloc while it renders frames). It needs no rr_ctx and gives
+ * the same result as rr_atrous_execute, written to `output`. Its one
+ * intermediate image lives in a fixed array in the library's device memory
+ * (RR_ATROUS_STATIC_MAX_PIXELS RGBA32F pixels, 36 MiB, held on every GPU
+ * that loads the library until the process exits). Images with more pixels
+ * return RR_ERR_UNSUPPORTED; null or aliased buffers RR_ERR_INVALID_ARGUMENT.
+ * The first call on each device looks up the array's device address (with
+ * that device current) and should come before any stream capture. All calls
+ * share the array: calls whose kernels overlap on the GPU race on it. */
+#define RR_ATROUS_STATIC_MAX_PIXELS (2048u * 1152u)
+rr_status rr_atrous_execute_static(const float* input, const float* gbuf_pos,
+                                   const float* gbuf_norm, float* output,
+                                   const rr_atrous_params* params, void* stream);
+
 /* ── vMF path-guiding grid (GuidingGrid.slang; host side
  * ReSTIRPTPass.cpp:311-341, 602-611, 784-810; params ReSTIRPTPass.h:93-100).
  * accum: int32[4*cell_count] fixed-point sums (x, y, z, count);

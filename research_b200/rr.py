@@ -128,6 +128,7 @@ _SIGNATURES = {
     "rr_restir_di_execute": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(DIParams), P, P, P, P, P, P]),
     "rr_atrous_iteration": (I, [P, P, P, P, P, C.POINTER(AtrousParams), P]),
     "rr_atrous_execute": (I, [P, P, P, P, P, P, C.POINTER(AtrousParams), C.POINTER(U32), P]),
+    "rr_atrous_execute_static": (I, [P, P, P, P, C.POINTER(AtrousParams), P]),
     "rr_guiding_splat": (I, [P, P, P, P, P, U32, C.POINTER(F32), C.POINTER(GuidingParams), P]),
     "rr_guiding_fit": (I, [P, P, P, C.POINTER(GuidingParams), P]),
     "rr_guiding_sample": (I, [P, P, P, P, P, P, U32, C.POINTER(F32), C.POINTER(GuidingParams), P, P, P]),
