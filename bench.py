@@ -43,8 +43,8 @@ RAY_BYTES, NODE_BYTES, TRI_BYTES = 48, 64, 36
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--width", type=int, default=CFG["width"])
     ap.add_argument("--height", type=int, default=CFG["height"])
@@ -119,7 +119,12 @@ class ClockSampler:
         self._stop = threading.Event()
         self._th = None
 
+    def mark(self):
+        """Only samples taken from now on are reported."""
+        self.first = len(self.rows)
+
     def start(self):
+        self.first = 0
         def run():
             while not self._stop.is_set():
                 try:
@@ -138,16 +143,17 @@ class ClockSampler:
         self._stop.set()
         if self._th:
             self._th.join(timeout=10)
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        rows = self.rows[self.first:] or self.rows[-1:]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         reasons = set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
+        for r in rows:
             for k, nm in enumerate(names):
                 if len(r) > 5 + k and r[5 + k].lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+                "reasons": sorted(reasons), "samples": len(rows)}
 
 
 def build_scene(rr, args):
@@ -318,6 +324,8 @@ def run_ours(args, ws, rank, local):
     seed_base = rank * 1_000_003
 
     st = rr.PtStats()
+    clocks = ClockSampler(torch.cuda.get_device_properties(local).uuid)
+    clocks.start()
     # 1) warm-up
     for _ in range(args.warmup):
         fr.step(stream, seed_base=seed_base)
@@ -326,18 +334,17 @@ def run_ours(args, ws, rank, local):
     launches0 = st.launches_total
     # 2) timed region: K device-resident steps
     first_timed = fr.frame
-    clocks = ClockSampler(torch.cuda.get_device_properties(local).uuid)
     barrier(ws)
     torch.cuda.synchronize()
-    clocks.start()
+    clocks.mark()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.steps):
         fr.step(stream, pt_flags=rr.PT_FLAG_TIME_STAGES, seed_base=seed_base, stage_timing=True)
     e1.record()
     torch.cuda.synchronize()
-    barrier(ws)
     clk = clocks.stop()
+    barrier(ws)
     ms_total = e0.elapsed_time(e1)
     ms_step = max_over_ranks(ws, ms_total / args.steps)
     ctx.check(rr.lib().rr_pathtracer_stats(ctx.handle, C.byref(st), 1))
