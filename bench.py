@@ -324,6 +324,13 @@ def run_ours(args, ws, rank, local):
     seed_base = rank * 1_000_003
 
     st = rr.PtStats()
+    # autotune the traversal variants on this scene and frame (setup, untimed)
+    tune = rr.PtTuneResult()
+    ctx.check(rr.lib().rr_pathtracer_tune(ctx.handle, scene.handle, C.byref(fr.cam),
+                                          C.byref(rr.PtParams(seed_base, CFG["max_bounces"], CFG["spp"], 0)),
+                                          fr.rad.data_ptr(), stream, C.byref(tune)))
+    tuned = {"extend_variant": tune.best_extend, "shadow_variant": tune.best_shadow,
+             "extend_ms": [round(x, 3) for x in tune.extend_ms], "shadow_ms": [round(x, 3) for x in tune.shadow_ms]}
     clocks = ClockSampler(torch.cuda.get_device_properties(local).uuid)
     clocks.start()
     # 1) warm-up
@@ -429,7 +436,7 @@ def run_ours(args, ws, rank, local):
                 "scene": {"triangles": sst.triangle_count, "bvh_nodes": sst.bvh_node_count,
                           "bvh_depth": sst.bvh_max_depth, "bvh_build_ms": round(sst.build_ms, 1),
                           "lights": sst.light_count},
-                "traversal_per_step": counted}
+                "traversal_per_step": counted, "autotune": tuned}
         print(json.dumps(line), flush=True)
     scene.close()
     ctx.close()

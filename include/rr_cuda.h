@@ -128,6 +128,29 @@ typedef struct rr_pt_stats {
 
 rr_status rr_pathtracer_stats(rr_ctx* ctx, rr_pt_stats* out, int reset_times);
 
+/* Traversal kernel variants (no reference counterpart; the reference uses
+ * hardware ray queries): variant = schedule x occupancy target,
+ *   0..2: warps trace 32 consecutive queue entries to completion, register
+ *         budget for 4 (default) / 5 / 6 blocks of 256 threads per SM;
+ *   3..5: persistent warps with per-lane ray refill, same budgets.
+ * Results are identical for every variant; only speed differs. */
+#define RR_PT_VARIANT_COUNT 6
+rr_status rr_pathtracer_set_variants(rr_ctx* ctx, int extend_variant, int shadow_variant);
+
+/* Autotuner: renders the given frame once per variant with stage timing,
+ * keeps the fastest extension and shadow variants on this context and
+ * reports every measured time (ms per frame). Synchronises the device. */
+typedef struct rr_pt_tune_result {
+    double extend_ms[RR_PT_VARIANT_COUNT];
+    double shadow_ms[RR_PT_VARIANT_COUNT];
+    int    best_extend;
+    int    best_shadow;
+} rr_pt_tune_result;
+
+rr_status rr_pathtracer_tune(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
+                             const rr_pt_params* params, float* radiance_out, void* stream,
+                             rr_pt_tune_result* out);
+
 /* ── accumulate: AccumulatePass::execute (AccumulatePass.cpp:167-218,
  * kernel accumulate.slang:21-46). AccumulatePushConstants minus indices.
  * Folds `image_count` consecutive radiance images into `accumulated` in

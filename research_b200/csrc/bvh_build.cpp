@@ -2,7 +2,7 @@
 //
 // Replaces the driver-built BLAS/TLAS of the reference
 // (AccelStructure.cpp:98-330, PREFER_FAST_TRACE). Builds one binary tree
-// over world-space triangles (16 centroid bins per axis, surface-area cost,
+// over world-space triangles (32 centroid bins per axis, surface-area cost,
 // leaves of at most 8 triangles, depth capped at 60 so a 64-entry traversal
 // stack always suffices), then lays it out for the GPU: every inner node
 // stores the boxes of both children, inner nodes in depth-first order.
@@ -41,7 +41,7 @@ struct Node {
     uint32_t first = 0, count = 0;
 };
 
-constexpr int kBins = 16;
+constexpr int kBins = 32;
 constexpr uint32_t kMaxLeaf = 8;
 constexpr uint32_t kMaxDepth = 60;
 

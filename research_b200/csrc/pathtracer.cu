@@ -85,32 +85,125 @@ __device__ __forceinline__ void flush_work(const TraceWork& w, unsigned long lon
     if (lane_id() == 0 && (n | t)) { atomicAdd(out, n); atomicAdd(out + 1, t); }
 }
 
-// Closest hit for every ray of the queue; warps fetch 32 rays at a time.
-template <bool Count>
-__global__ void __launch_bounds__(kBlock) extend_kernel(DevScene s, const float4* __restrict__ qa,
-                                                        const float4* __restrict__ qb,
-                                                        float4* __restrict__ hits,
-                                                        const uint32_t* count_ptr, uint32_t* work,
-                                                        unsigned long long* work_out) {
-    const uint32_t count = *count_ptr;
+// Warp-cooperative ray pool: hands queue indices [0, count) to idle lanes,
+// taking kChunk indices at a time from the launch's global cursor (one
+// atomic per chunk). All fields are warp-uniform.
+constexpr uint32_t kChunk = 256;
+constexpr uint32_t kRefillLanes = 8;
+
+struct WarpPool {
+    uint32_t next = 0, end = 0;
+    bool exhausted = false;
+    __device__ __forceinline__ bool done() const { return exhausted && next >= end; }
+    // Every lane calls this with the same idle mask; idle lanes get an index
+    // (or kNoIndex when the queue is drained).
+    __device__ __forceinline__ uint32_t refill(uint32_t idle_mask, bool idle, uint32_t count, uint32_t* cursor) {
+        const uint32_t n_idle = __popc(idle_mask);
+        const uint32_t rank = __popc(idle_mask & ((1u << lane_id()) - 1u));
+        const uint32_t avail = end - next;
+        const bool need = avail < n_idle && !exhausted;
+        uint32_t nb = 0;
+        if (need) {
+            if (lane_id() == 0) nb = atomicAdd(cursor, kChunk);
+            nb = __shfl_sync(kFull, nb, 0);
+        }
+        uint32_t idx = kNoIndex;
+        if (idle) {
+            if (rank < avail) idx = next + rank;
+            else if (need) idx = nb + (rank - avail);
+        }
+        if (idx >= count) idx = kNoIndex;
+        if (!need) {
+            next = min(next + n_idle, end);
+        } else if (nb >= count) {
+            exhausted = true;
+            next = end = 0;
+        } else {
+            end = min(nb + kChunk, count);
+            next = min(nb + (n_idle - avail), end);
+        }
+        return idx;
+    }
+};
+
+// Queue traversal, two schedules (chosen per context, see rr_pathtracer_tune):
+//  Refill = false: each warp takes 32 consecutive queue entries (neighbouring
+//    paths after compaction, hence coherent rays) and traces them to the end;
+//  Refill = true: persistent warps; a lane whose ray is finished takes a new
+//    one as soon as kRefillLanes lanes are idle, so warps do not wait for
+//    their slowest ray (less coherence, fewer idle lanes).
+// MinBlocks is the occupancy target handed to the register allocator.
+// `Finish(i, found, hit)` consumes a finished ray; `Load(i, ray, tmax)` makes one.
+template <bool AnyHit, bool Count, bool Refill, class Load, class Finish>
+__device__ __forceinline__ void traverse_queue(const DevScene& s, uint32_t count, uint32_t* cursor,
+                                               unsigned long long* work_out, Load load, Finish finish) {
     TraceWork tw;
-    while (true) {
-        uint32_t base = 0;
-        if (lane_id() == 0) base = atomicAdd(work, 32u);
-        base = __shfl_sync(kFull, base, 0);
-        if (base >= count) break;
-        const uint32_t i = base + lane_id();
-        if (i < count) {
-            const float4 a = qa[i], b = qb[i];
-            const Ray r = make_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z));
-            HitRec h;
-            if (trace<false, Count>(s, r, 0.001f, 1e9f, h, &tw))
-                hits[i] = make_float4(h.u, h.v, __uint_as_float(h.inst), __uint_as_float(h.prim));
-            else
-                hits[i] = make_float4(0.0f, 0.0f, __uint_as_float(kNoIndex), __uint_as_float(kNoIndex));
+    int2 stack[kStackSize];  // (node, near distance)
+    if constexpr (!Refill) {
+        while (true) {
+            uint32_t base = 0;
+            if (lane_id() == 0) base = atomicAdd(cursor, 32u);
+            base = __shfl_sync(kFull, base, 0);
+            if (base >= count) break;
+            const uint32_t i = base + lane_id();
+            if (i < count) {
+                Ray r; float tmax;
+                load(i, r, tmax);
+                HitRec h; TravState st;
+                trav_begin(st, h, tmax);
+                while (!trace_step<AnyHit, Count>(s, r, 0.001f, h, st, stack, &tw)) {}
+                finish(i, st.found, h);
+            }
+        }
+    } else {
+        WarpPool pool;
+        Ray r;
+        HitRec h;
+        TravState st;
+        uint32_t idx = kNoIndex;
+        bool has = false;
+        while (true) {
+            const uint32_t idle = __ballot_sync(kFull, !has);
+            if (idle && !pool.done() && (idle == kFull || __popc(idle) >= kRefillLanes)) {
+                const uint32_t ni = pool.refill(idle, !has, count, cursor);
+                if (!has && ni != kNoIndex) {
+                    idx = ni;
+                    float tmax;
+                    load(idx, r, tmax);
+                    trav_begin(st, h, tmax);
+                    has = true;
+                }
+            }
+            if (!__any_sync(kFull, has)) {
+                if (pool.done()) break;
+                continue;
+            }
+            if (has && trace_step<AnyHit, Count>(s, r, 0.001f, h, st, stack, &tw)) {
+                finish(idx, st.found, h);
+                has = false;
+            }
         }
     }
     if (Count) flush_work(tw, work_out);
+}
+
+template <bool Count, bool Refill, int MinBlocks>
+__global__ void __launch_bounds__(kBlock, MinBlocks) extend_kernel(DevScene s, const float4* __restrict__ qa,
+                                                                   const float4* __restrict__ qb,
+                                                                   float4* __restrict__ hits,
+                                                                   const uint32_t* count_ptr, uint32_t* cursor,
+                                                                   unsigned long long* work_out) {
+    traverse_queue<false, Count, Refill>(
+        s, *count_ptr, cursor, work_out,
+        [&](uint32_t i, Ray& r, float& tmax) {
+            const float4 a = qa[i], b = qb[i];
+            r = make_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z));
+            tmax = 1e9f;
+        },
+        [&](uint32_t i, bool found, const HitRec& h) {
+            hits[i] = found ? make_float4(h.u, h.v, __uint_as_float(h.inst), __uint_as_float(h.prim))
+                            : make_float4(0.0f, 0.0f, __uint_as_float(kNoIndex), __uint_as_float(kNoIndex));
+        });
 }
 
 __global__ void __launch_bounds__(kBlock) shade_kernel(DevScene s, uint32_t bounce, uint32_t last,
@@ -238,36 +331,58 @@ __global__ void __launch_bounds__(kBlock) shade_kernel(DevScene s, uint32_t boun
     }
 }
 
-// Any-hit shadow rays; unoccluded contributions are added to the image.
-template <bool Count>
-__global__ void __launch_bounds__(kBlock) shadow_kernel(DevScene s, const float4* __restrict__ sa,
-                                                        const float4* __restrict__ sb,
-                                                        const float4* __restrict__ sc,
-                                                        float4* __restrict__ out,
-                                                        const uint32_t* count_ptr, uint32_t* work,
-                                                        unsigned long long* work_out) {
-    const uint32_t count = *count_ptr;
-    TraceWork tw;
-    while (true) {
-        uint32_t base = 0;
-        if (lane_id() == 0) base = atomicAdd(work, 32u);
-        base = __shfl_sync(kFull, base, 0);
-        if (base >= count) break;
-        const uint32_t i = base + lane_id();
-        if (i < count) {
+// Any-hit shadow rays; unoccluded NEE contributions are added to the image.
+template <bool Count, bool Refill, int MinBlocks>
+__global__ void __launch_bounds__(kBlock, MinBlocks) shadow_kernel(DevScene s, const float4* __restrict__ sa,
+                                                                   const float4* __restrict__ sb,
+                                                                   const float4* __restrict__ sc,
+                                                                   float4* __restrict__ out,
+                                                                   const uint32_t* count_ptr, uint32_t* cursor,
+                                                                   unsigned long long* work_out) {
+    traverse_queue<true, Count, Refill>(
+        s, *count_ptr, cursor, work_out,
+        [&](uint32_t i, Ray& r, float& tmax) {
             const float4 a = sa[i], b = sb[i];
-            const Ray r = make_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z));
-            HitRec h;
-            if (!trace<true, Count>(s, r, 0.001f, b.w, h, &tw)) {
+            r = make_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z));
+            tmax = b.w;
+        },
+        [&](uint32_t i, bool found, const HitRec&) {
+            if (!found) {
                 const float4 c = sc[i];
-                const uint32_t pid = __float_as_uint(a.w);
+                const uint32_t pid = __float_as_uint(sa[i].w);
                 float4 o = out[pid];
                 o.x = o.x + c.x; o.y = o.y + c.y; o.z = o.z + c.z;
                 out[pid] = o;
             }
-        }
+        });
+}
+
+// Traversal kernel variants: schedule x occupancy target.
+using QueueKernel = void (*)(DevScene, const float4*, const float4*, float4*, const uint32_t*, uint32_t*,
+                             unsigned long long*);
+using ShadowKernel = void (*)(DevScene, const float4*, const float4*, const float4*, float4*, const uint32_t*,
+                              uint32_t*, unsigned long long*);
+template <bool Count>
+QueueKernel extend_variant(int v) {
+    switch (v) {
+    case 1: return extend_kernel<Count, false, 5>;
+    case 2: return extend_kernel<Count, false, 6>;
+    case 3: return extend_kernel<Count, true, 1>;
+    case 4: return extend_kernel<Count, true, 5>;
+    case 5: return extend_kernel<Count, true, 6>;
+    default: return extend_kernel<Count, false, 1>;
     }
-    if (Count) flush_work(tw, work_out);
+}
+template <bool Count>
+ShadowKernel shadow_variant(int v) {
+    switch (v) {
+    case 1: return shadow_kernel<Count, false, 5>;
+    case 2: return shadow_kernel<Count, false, 6>;
+    case 3: return shadow_kernel<Count, true, 1>;
+    case 4: return shadow_kernel<Count, true, 5>;
+    case 5: return shadow_kernel<Count, true, 6>;
+    default: return shadow_kernel<Count, false, 1>;
+    }
 }
 
 int persistent_grid(const rr_ctx* ctx, const void* kernel) {
@@ -344,8 +459,8 @@ extern "C" rr_status rr_pathtracer_execute(rr_ctx* ctx, const rr_scene* scene,
     }
     const bool count = (p->flags & RR_PT_FLAG_COUNT_TRAVERSAL) != 0;
     const bool timed = (p->flags & RR_PT_FLAG_TIME_STAGES) != 0;
-    auto ext_k = count ? extend_kernel<true> : extend_kernel<false>;
-    auto sh_k = count ? shadow_kernel<true> : shadow_kernel<false>;
+    QueueKernel ext_k = count ? extend_variant<true>(ctx->extend_variant) : extend_variant<false>(ctx->extend_variant);
+    ShadowKernel sh_k = count ? shadow_variant<true>(ctx->shadow_variant) : shadow_variant<false>(ctx->shadow_variant);
     const int g_ext = persistent_grid(ctx, reinterpret_cast<const void*>(ext_k));
     const int g_sh = persistent_grid(ctx, reinterpret_cast<const void*>(sh_k));
     const int g_shade = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(shade_kernel)),
@@ -408,5 +523,46 @@ extern "C" rr_status rr_pathtracer_stats(rr_ctx* ctx, rr_pt_stats* out, int rese
     if (reset) {
         for (int k = 0; k < 4; ++k) { ctx->stage_ms[k] = 0.0; ctx->stage_launches[k] = 0; }
     }
+    return RR_OK;
+}
+
+extern "C" rr_status rr_pathtracer_set_variants(rr_ctx* ctx, int ev, int sv) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    if (ev < 0 || ev >= RR_PT_VARIANT_COUNT || sv < 0 || sv >= RR_PT_VARIANT_COUNT)
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "traversal variant out of range");
+    ctx->extend_variant = ev;
+    ctx->shadow_variant = sv;
+    return RR_OK;
+}
+
+extern "C" rr_status rr_pathtracer_tune(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* cam,
+                                        const rr_pt_params* p, float* radiance_out, void* stream,
+                                        rr_pt_tune_result* out) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    if (!scene || !cam || !p || !radiance_out || !out)
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_pathtracer_tune: null argument");
+    rr_pt_stats st;
+    rr_status s = rr_pathtracer_stats(ctx, &st, 1);  // drop earlier timings
+    if (s != RR_OK) return s;
+    rr_pt_params q = *p;
+    q.flags = RR_PT_FLAG_TIME_STAGES;
+    double best_e = 1e30, best_s = 1e30;
+    out->best_extend = out->best_shadow = 0;
+    for (int v = 0; v < RR_PT_VARIANT_COUNT; ++v) {
+        ctx->extend_variant = v;
+        ctx->shadow_variant = v;
+        // one untimed pass to settle caches and clocks, then one timed pass
+        rr_pt_params warm = *p;
+        warm.flags = 0;
+        if ((s = rr_pathtracer_execute(ctx, scene, cam, &warm, radiance_out, stream)) != RR_OK) return s;
+        if ((s = rr_pathtracer_execute(ctx, scene, cam, &q, radiance_out, stream)) != RR_OK) return s;
+        if ((s = rr_pathtracer_stats(ctx, &st, 1)) != RR_OK) return s;
+        out->extend_ms[v] = st.ms_extend;
+        out->shadow_ms[v] = st.ms_shadow;
+        if (st.ms_extend < best_e) { best_e = st.ms_extend; out->best_extend = v; }
+        if (st.ms_shadow < best_s) { best_s = st.ms_shadow; out->best_shadow = v; }
+    }
+    ctx->extend_variant = out->best_extend;
+    ctx->shadow_variant = out->best_shadow;
     return RR_OK;
 }

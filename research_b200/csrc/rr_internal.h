@@ -47,6 +47,8 @@ struct rr_ctx {
     uint32_t* counters = nullptr;          // kCounterWords
     unsigned long long* work64 = nullptr;  // traversal work: ext nodes, ext tris, shadow nodes, shadow tris
     uint32_t last_max_bounces = 0;
+    int extend_variant = 0;                // traversal schedule/occupancy variant (rr_pathtracer_tune)
+    int shadow_variant = 0;
     bool last_counted = false;
     uint64_t launches = 0;                 // kernels issued by this context
     double stage_ms[4] = {0, 0, 0, 0};     // raygen, extend, shade, shadow

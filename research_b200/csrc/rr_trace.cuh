@@ -132,75 +132,94 @@ struct TraceWork {
     uint32_t tris = 0;
 };
 
-// Closest hit (AnyHit = false) or any hit (AnyHit = true) in [tmin, tmax].
-// Returns true on hit. `hit` is filled for closest-hit queries.
-template <bool AnyHit, bool Count = false>
-RR_D bool trace(const DevScene& s, const Ray& r, float tmin, float tmax, HitRec& hit, TraceWork* work = nullptr) {
-    int stack[kStackSize];
-    float nears[kStackSize];
-    int sp = 0;
-    int node = 0;
-    bool found = false;
+// Traversal state of one ray between node steps.
+struct TravState {
+    int node;
+    int sp;
+    bool found;
+    uint32_t visits;
+};
+
+RR_D void trav_begin(TravState& st, HitRec& hit, float tmax) {
+    st.node = 0; st.sp = 0; st.found = false; st.visits = 0;
     hit.t = tmax; hit.key = kNoIndex;
+}
+
+// One node of a closest-hit (AnyHit = false) or any-hit traversal: tests the
+// node's two child boxes, intersects the triangles of hit leaf children right
+// away, descends into the nearer inner child and pushes the farther one.
+// Returns true once the traversal is finished (stack empty, or any hit).
+template <bool AnyHit, bool Count>
+RR_D bool trace_step(const DevScene& s, const Ray& r, float tmin, HitRec& hit, TravState& st,
+                     int2* stack, TraceWork* work) {
     // A tree visits each node at most once; the bound only guards against a
     // malformed node array turning into an endless loop.
-    for (uint32_t visits = 0; visits <= s.num_nodes; ++visits) {
-        const float4 a = __ldg(s.nodes + node * 4 + 0);
-        const float4 b = __ldg(s.nodes + node * 4 + 1);
-        const float4 c = __ldg(s.nodes + node * 4 + 2);
-        const int4 d = __ldg(reinterpret_cast<const int4*>(s.nodes) + node * 4 + 3);
-        if (Count) work->nodes++;
-        bool h0, h1; float n0, n1;
-        box_pair(r, a, b, c, tmin, hit.t, h0, h1, n0, n1);
-        // leaves are intersected right away
-        #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const bool hk = k == 0 ? h0 : h1;
-            const int child = k == 0 ? d.x : d.y;
-            if (hk && child < 0) {
-                const int first = ~child;
-                const int count = k == 0 ? d.z : d.w;
-                for (int i = first; i < first + count; ++i) {
-                    if (Count) work->tris++;
-                    const float4 t0 = __ldg(s.tris + i * 3 + 0);
-                    const float4 t1 = __ldg(s.tris + i * 3 + 1);
-                    const float4 t2 = __ldg(s.tris + i * 3 + 2);
-                    float tt, uu, vv;
-                    if (intersect_triangle(r, f3(t0.x, t0.y, t0.z), f3(t0.w, t1.x, t1.y),
-                                           f3(t1.z, t1.w, t2.x), tmin, hit.t, tt, uu, vv)) {
-                        const uint32_t key = __float_as_uint(t2.w);
-                        if (AnyHit) { hit.t = tt; return true; }
-                        if (!found || tt < hit.t || (tt == hit.t && key < hit.key)) {
-                            found = true;
-                            hit.t = tt; hit.u = uu; hit.v = vv; hit.key = key;
-                            hit.inst = __float_as_uint(t2.y); hit.prim = __float_as_uint(t2.z);
-                        }
+    if (++st.visits > s.num_nodes + 1) return true;
+    const int node = st.node;
+    const float4 a = __ldg(s.nodes + node * 4 + 0);
+    const float4 b = __ldg(s.nodes + node * 4 + 1);
+    const float4 c = __ldg(s.nodes + node * 4 + 2);
+    const int4 d = __ldg(reinterpret_cast<const int4*>(s.nodes) + node * 4 + 3);
+    if (Count) work->nodes++;
+    bool h0, h1; float n0, n1;
+    box_pair(r, a, b, c, tmin, hit.t, h0, h1, n0, n1);
+    #pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const bool hk = k == 0 ? h0 : h1;
+        const int child = k == 0 ? d.x : d.y;
+        if (hk && child < 0) {
+            const int first = ~child;
+            const int count = k == 0 ? d.z : d.w;
+            for (int i = first; i < first + count; ++i) {
+                if (Count) work->tris++;
+                const float4 t0 = __ldg(s.tris + i * 3 + 0);
+                const float4 t1 = __ldg(s.tris + i * 3 + 1);
+                const float4 t2 = __ldg(s.tris + i * 3 + 2);
+                float tt, uu, vv;
+                if (intersect_triangle(r, f3(t0.x, t0.y, t0.z), f3(t0.w, t1.x, t1.y),
+                                       f3(t1.z, t1.w, t2.x), tmin, hit.t, tt, uu, vv)) {
+                    const uint32_t key = __float_as_uint(t2.w);
+                    if (AnyHit) { hit.t = tt; st.found = true; return true; }
+                    if (!st.found || tt < hit.t || (tt == hit.t && key < hit.key)) {
+                        st.found = true;
+                        hit.t = tt; hit.u = uu; hit.v = vv; hit.key = key;
+                        hit.inst = __float_as_uint(t2.y); hit.prim = __float_as_uint(t2.z);
                     }
                 }
             }
         }
-        const bool i0 = h0 && d.x >= 0 && n0 <= hit.t;
-        const bool i1 = h1 && d.y >= 0 && n1 <= hit.t;
-        if (i0 && i1) {
-            const bool first0 = n0 <= n1;
-            stack[sp] = first0 ? d.y : d.x;
-            nears[sp] = first0 ? n1 : n0;
-            ++sp;
-            node = first0 ? d.x : d.y;
-        } else if (i0) {
-            node = d.x;
-        } else if (i1) {
-            node = d.y;
-        } else {
-            bool popped = false;
-            while (sp > 0) {
-                --sp;
-                if (nears[sp] <= hit.t) { node = stack[sp]; popped = true; break; }
-            }
-            if (!popped) break;
-        }
     }
-    return found;
+    const bool i0 = h0 && d.x >= 0 && n0 <= hit.t;
+    const bool i1 = h1 && d.y >= 0 && n1 <= hit.t;
+    if (i0 && i1) {
+        const bool first0 = n0 <= n1;
+        stack[st.sp] = make_int2(first0 ? d.y : d.x, __float_as_int(first0 ? n1 : n0));
+        ++st.sp;
+        st.node = first0 ? d.x : d.y;
+    } else if (i0) {
+        st.node = d.x;
+    } else if (i1) {
+        st.node = d.y;
+    } else {
+        while (st.sp > 0) {
+            --st.sp;
+            const int2 e = stack[st.sp];
+            if (__int_as_float(e.y) <= hit.t) { st.node = e.x; return false; }
+        }
+        return true;
+    }
+    return false;
+}
+
+// Closest hit (AnyHit = false) or any hit (AnyHit = true) in [tmin, tmax],
+// one ray per thread. Returns true on hit; `hit` is filled for closest hit.
+template <bool AnyHit, bool Count = false>
+RR_D bool trace(const DevScene& s, const Ray& r, float tmin, float tmax, HitRec& hit, TraceWork* work = nullptr) {
+    int2 stack[kStackSize];  // (node, near distance)
+    TravState st;
+    trav_begin(st, hit, tmax);
+    while (!trace_step<AnyHit, Count>(s, r, tmin, hit, st, stack, work)) {}
+    return st.found;
 }
 
 // Hit attributes (pathtracer.slang:69-118 / restir_di.slang:108-144):

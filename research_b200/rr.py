@@ -59,6 +59,11 @@ class PtStats(C.Structure):
                 ("ms_shadow", C.c_double), ("launches_extend", C.c_uint64), ("launches_total", C.c_uint64)]
 
 
+class PtTuneResult(C.Structure):
+    _fields_ = [("extend_ms", C.c_double * 6), ("shadow_ms", C.c_double * 6), ("best_extend", C.c_int),
+                ("best_shadow", C.c_int)]
+
+
 PT_FLAG_COUNT_TRAVERSAL = 1
 PT_FLAG_TIME_STAGES = 2
 
@@ -121,6 +126,8 @@ _SIGNATURES = {
     "rr_scene_get_stats": (I, [P, C.POINTER(SceneStats)]),
     "rr_pathtracer_execute": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtParams), P, P]),
     "rr_pathtracer_stats": (I, [P, C.POINTER(PtStats), I]),
+    "rr_pathtracer_set_variants": (I, [P, I, I]),
+    "rr_pathtracer_tune": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtParams), P, P, C.POINTER(PtTuneResult)]),
     "rr_accumulate_execute": (I, [P, P, U32, P, P, C.POINTER(AccParams), P]),
     "rr_restir_di_initial": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(DIParams), P, P, P, P]),
     "rr_restir_di_temporal": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(DIParams), P, P, P, P, P]),

@@ -296,3 +296,26 @@ def test_detmath_against_cuda_libm(rr, O, ctx, torch_cuda):
     ref = _np(torch.exp(torch.from_numpy(e).cuda())).astype(np.float64)
     ulp = np.spacing(np.abs(ref).astype(np.float32)).astype(np.float64)
     assert (np.abs(O.detmath("exp", e) - ref) / ulp).max() <= 3.0
+
+
+def test_traversal_variants_identical_and_tuner(rr, O, ctx, torch_cuda, procedural):
+    """Every traversal schedule/occupancy variant renders the same bits; the
+    autotuner keeps the fastest and reports a time for each variant."""
+    torch = torch_cuda
+    _, scene, oscene = procedural
+    cam = cam_for(rr, "procedural", 80, 48)
+    ref, _ = O.pathtrace(oscene, cam, 9, 5, 1)
+    for v in range(6):
+        ctx.check(rr.lib().rr_pathtracer_set_variants(ctx.handle, v, v))
+        g = gpu_pathtrace(rr, ctx, scene, cam, torch, 9, 5, 1)
+        np.testing.assert_array_equal(g.view(np.uint32), ref.view(np.uint32))
+    out = torch.empty((1, 48, 80, 4), device="cuda")
+    res = rr.PtTuneResult()
+    ctx.check(rr.lib().rr_pathtracer_tune(ctx.handle, scene.handle, C.byref(cam), C.byref(rr.PtParams(9, 5, 1, 0)),
+                                          out.data_ptr(), _stream(torch), C.byref(res)))
+    assert all(t > 0 for t in res.extend_ms) and all(t > 0 for t in res.shadow_ms)
+    assert res.extend_ms[res.best_extend] == min(res.extend_ms)
+    g = gpu_pathtrace(rr, ctx, scene, cam, torch, 9, 5, 1)
+    np.testing.assert_array_equal(g.view(np.uint32), ref.view(np.uint32))
+    assert rr.lib().rr_pathtracer_set_variants(ctx.handle, 6, 0) == 1
+    ctx.check(rr.lib().rr_pathtracer_set_variants(ctx.handle, 0, 0))
