@@ -276,6 +276,19 @@ rr_status rr_guiding_sample(rr_ctx* ctx, const float* fitted, const float* pos,
 rr_status rr_guiding_reset(rr_ctx* ctx, int32_t* accum, float* fitted,
                            const rr_guiding_params* params, void* stream);
 
+/* ── output formats (SURVEY "next": tonemap / PNG / MSE utilities) ─────
+ * rr_tonemap_execute: exposure, ACES filmic approximation, clamp, gamma
+ * 1/2.2, 8-bit RGBA (Application.cpp:853-866; tonemap.slang:40-69).
+ * rr_image_mse: FP64 mean squared error over the RGB channels of the window
+ * [x0, x0+w) x [y0, y0+h) of two W x H RGBA32F images, written to a device
+ * double (Application::compute_mse, Application.cpp:892-949). Fixed
+ * reduction order: deterministic. */
+rr_status rr_tonemap_execute(rr_ctx* ctx, const float* hdr, uint32_t width, uint32_t height,
+                             float exposure, uint8_t* rgba8_out, void* stream);
+rr_status rr_image_mse(rr_ctx* ctx, const float* a, const float* b, uint32_t width, uint32_t height,
+                       uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, double* mse_out_dev,
+                       void* stream);
+
 /* ── ray queries (checking and tooling) ─────────────────────────────────
  * Closest hit for `count` rays: origins/dirs float4, hits float4
  * (t, u, v, as_float(instance)) and prims uint32; instance 0xffffffff = miss. */

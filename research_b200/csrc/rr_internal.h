@@ -55,6 +55,7 @@ struct rr_ctx {
     uint64_t stage_launches[4] = {0, 0, 0, 0};
     std::vector<rr_stage_event> pending;   // recorded, not yet read back
     std::vector<cudaEvent_t> event_pool;
+    double* mse_partial = nullptr;         // rr_image_mse block partials
 };
 
 // Records a CUDA event pair around stage launches on the caller's stream;

@@ -87,6 +87,7 @@ rr_status rr_ctx_destroy(rr_ctx* ctx) {
     for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
     cudaFree(ctx->counters);
     cudaFree(ctx->work64);
+    cudaFree(ctx->mse_partial);
     delete ctx;
     return RR_OK;
 }

@@ -141,6 +141,8 @@ _SIGNATURES = {
     "rr_guiding_sample": (I, [P, P, P, P, P, P, U32, C.POINTER(F32), C.POINTER(GuidingParams), P, P, P]),
     "rr_guiding_reset": (I, [P, P, P, C.POINTER(GuidingParams), P]),
     "rr_trace_closest": (I, [P, P, P, P, F32, F32, U32, P, P, P]),
+    "rr_tonemap_execute": (I, [P, P, U32, U32, F32, P, P]),
+    "rr_image_mse": (I, [P, P, P, U32, U32, U32, U32, U32, U32, P, P]),
     "rr_host_scene_cornell": (I, [I, C.POINTER(P)]),
     "rr_host_scene_procedural": (I, [C.POINTER(ProceduralParams), C.POINTER(P)]),
     "rr_host_scene_instanced": (I, [C.POINTER(InstancedParams), C.POINTER(P)]),
