@@ -276,6 +276,79 @@ rr_status rr_guiding_sample(rr_ctx* ctx, const float* fitted, const float* pos,
 rr_status rr_guiding_reset(rr_ctx* ctx, int32_t* accum, float* fitted,
                            const rr_guiding_params* params, void* stream);
 
+/* ── guided path tracing (no reference counterpart beyond the hash grid
+ * above: the reference guides only ReSTIR PT's primary bounce with one vMF
+ * lobe per hashed cell, restir_pt.slang:520-563). A guide predicts a mixture
+ * of up to 8 vMF lobes at every path vertex; the guided tracer draws each
+ * bounce by one-sample MIS between the guide (probability alpha where the
+ * guide has a lobe) and brdf_sample, with pdf = alpha p_guide + (1-alpha)
+ * p_bsdf, so the estimator stays unbiased for any guide. It records, per
+ * vertex, the sampled direction and the radiance that came back along it;
+ * rr_guide_update trains the guide on those samples:
+ *   RR_GUIDE_GRID: dense grid_resolution^3 cells over bounds_min..max, 8
+ *     lobes per cell, stepwise EM whose sufficient statistics are FP64 sums
+ *     reduced in a fixed order (deterministic);
+ *   RR_GUIDE_MLP: a BF16 multilayer perceptron (position frequency encoding,
+ *     normal, view direction -> 8 lobes) run on the tensor cores, trained
+ *     with Adam on mlp_batch samples per update. */
+typedef struct rr_guide rr_guide;
+
+#define RR_GUIDE_GRID 0u
+#define RR_GUIDE_MLP 1u
+
+typedef struct rr_guide_desc {
+    uint32_t kind;
+    uint32_t grid_resolution;      /* cells per axis (64) */
+    float    alpha;                /* P(sample the guide) at a guided vertex (0.5) */
+    float    decay;                /* weight of earlier statistics per update (grid) */
+    float    bounds_min[3];
+    float    bounds_max[3];
+    uint32_t max_samples;          /* training samples kept per frame */
+    uint32_t mlp_batch;            /* samples per Adam step (1 << 18) */
+    float    learning_rate;        /* Adam (1e-2) */
+    uint32_t seed;
+} rr_guide_desc;
+
+typedef struct rr_guide_stats {
+    uint64_t samples_recorded;     /* by the last guided execute */
+    uint64_t samples_used;         /* by the last update */
+    uint32_t cells_valid;          /* grid: cells with a fitted mixture */
+    uint32_t updates;
+    double   last_loss;            /* MLP: weighted NLL of the last step */
+    double   ms_update;            /* device time of the last update */
+} rr_guide_stats;
+
+rr_status rr_guide_create(rr_ctx* ctx, const rr_guide_desc* desc, rr_guide** out);
+rr_status rr_guide_destroy(rr_guide* guide);
+rr_status rr_guide_reset(rr_ctx* ctx, rr_guide* guide, void* stream);
+rr_status rr_guide_update(rr_ctx* ctx, rr_guide* guide, void* stream);
+rr_status rr_guide_get_stats(rr_ctx* ctx, const rr_guide* guide, rr_guide_stats* out);
+/* Same contract as rr_pathtracer_execute (spp images out); guide may not be
+ * NULL. Training samples of this call replace the previous call's. */
+/* Evaluates the guide at `count` surface points: surf holds 3 float4 per
+ * point, (position, 1), (normal, 1 = valid), (view direction wo, 0); mix_out
+ * receives 10 float4 per point: 8 lobes (mu.xyz, kappa) and the 8 lobe
+ * weights (weights all zero where the guide has no mixture). */
+rr_status rr_guide_eval(rr_ctx* ctx, rr_guide* guide, const float* surf, uint32_t count, float* mix_out,
+                        void* stream);
+/* MLP guides: host copies of the FP32 master parameters and of the last
+ * gradient (loss-scaled by 1024), and an optional host overwrite of the
+ * parameters (params_in). count must equal the parameter count (20784:
+ * per layer W[out][in] then b[out], layers 80->64->64->64->64->48).
+ * error_flag receives 1 if a tensor-core wait ever gave up. */
+/* Replaces the training samples a guided execute recorded by caller-made
+ * ones (device array, 16 floats per sample: position, weight; direction wi,
+ * unique id as uint bits; normal, 0; view direction wo, 0), e.g. to train a
+ * guide from another integrator. count <= max_samples. */
+rr_status rr_guide_set_samples(rr_ctx* ctx, rr_guide* guide, const float* samples, uint32_t count,
+                               void* stream);
+#define RR_MLP_PARAM_COUNT 20784u
+rr_status rr_guide_mlp_params(rr_ctx* ctx, rr_guide* guide, float* params_out, float* grad_out,
+                              float* params_in, uint32_t count, int* error_flag);
+rr_status rr_guided_pathtracer_execute(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
+                                       const rr_pt_params* params, rr_guide* guide,
+                                       float* radiance_out, void* stream);
+
 /* ── output formats (SURVEY "next": tonemap / PNG / MSE utilities) ─────
  * rr_tonemap_execute: exposure, ACES filmic approximation, clamp, gamma
  * 1/2.2, 8-bit RGBA (Application.cpp:853-866; tonemap.slang:40-69).

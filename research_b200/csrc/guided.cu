@@ -1,0 +1,719 @@
+// guided.cu — guided wavefront path tracer and the dense vMF-mixture grid guide.
+//
+// The guided tracer reuses the reference stages (raygen, extend, shadow,
+// NEE of pathtracer.slang:124-177, Russian roulette of :252-257) and replaces
+// brdf_sample at each bounce by one-sample MIS between a guide mixture and
+// brdf_sample. Each vertex that continues records (position, normal, wo,
+// sampled wi, sampling pdf, path throughput after the vertex); the next stage
+// stores the radiance gathered so far, and the resolve pass turns the final
+// radiance into one training sample per vertex with weight
+//     w = L_in(wi) / pdf,  L_in = (L_final - L_before) / throughput_after
+// (luminances), an unbiased sample of the incident-radiance distribution.
+//
+// Grid guide: grid_resolution^3 cells over the guide bounds, 8 vMF lobes per
+// cell. rr_guide_update sorts the samples by (cell, vertex id) and runs one
+// stepwise-EM iteration per cell in a fixed sample order, accumulating the
+// sufficient statistics (sum w*gamma, sum w*gamma*omega) in FP64 with
+// exponential forgetting, then refits weights, mean directions and
+// concentrations (Banerjee's closed form, as GuidingGrid.slang:124-131).
+
+#include "rr_wavefront.cuh"
+#include "rr_vmf.cuh"
+#include "rr_guide.h"
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include <chrono>
+#include <cstring>
+
+namespace rr {
+namespace {
+
+RR_D float lum709(float3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
+
+struct GuidedLaunch {
+    uint32_t bounce, last, paths, lobes;
+    float alpha;
+    GridView grid;
+    const float4* mix;        // MLP mode: per queue slot, kMaxLobes lobes + 2 float4 of weights
+    float4* rec0;             // (pos, pdf)
+    float4* rec1;             // (wi, throughput luminance after the vertex)
+    float4* rec2;             // (normal, radiance luminance gathered before the vertex's continuation)
+    float4* rec3;             // (wo, 0)
+};
+
+RR_D void load_mixture_grid(const GridView& g, float3 p, VmfMixture& m, bool& valid) {
+    const uint32_t cell = grid_cell(g, p);
+    float wsum = 0.0f;
+    #pragma unroll
+    for (int j = 0; j < kMaxLobes; ++j) {
+        m.lobe[j] = __ldg(g.lobes + size_t(cell) * kMaxLobes + j);
+        m.weight[j] = __ldg(g.weights + size_t(cell) * kMaxLobes + j);
+        wsum += m.weight[j];
+    }
+    valid = wsum > 0.0f;
+}
+
+RR_D void load_mixture_slot(const float4* mix, uint32_t slot, VmfMixture& m, bool& valid) {
+    const float4* base = mix + size_t(slot) * (kMaxLobes + 2);
+    #pragma unroll
+    for (int j = 0; j < kMaxLobes; ++j) m.lobe[j] = base[j];
+    const float4 w0 = base[kMaxLobes], w1 = base[kMaxLobes + 1];
+    m.weight[0] = w0.x; m.weight[1] = w0.y; m.weight[2] = w0.z; m.weight[3] = w0.w;
+    m.weight[4] = w1.x; m.weight[5] = w1.y; m.weight[6] = w1.z; m.weight[7] = w1.w;
+    float wsum = 0.0f;
+    #pragma unroll
+    for (int j = 0; j < kMaxLobes; ++j) wsum += m.weight[j];
+    valid = wsum > 0.0f;
+}
+
+// Surface inputs of the MLP guide for every queued ray that hit a
+// non-emissive surface: (pos, 1), (normal toward wo, valid), (wo, 0).
+__global__ void __launch_bounds__(kBlock) guided_surface_kernel(DevScene s, const float4* __restrict__ qb,
+                                                                const float4* __restrict__ hits,
+                                                                float4* __restrict__ surf,
+                                                                const uint32_t* count_ptr) {
+    const uint32_t count = *count_ptr;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const float4 h = hits[i];
+        const uint32_t inst = __float_as_uint(h.z);
+        float4 a = make_float4(0, 0, 0, 0), b = make_float4(0, 0, 0, 0), c = make_float4(0, 0, 0, 0);
+        if (inst != kNoIndex) {
+            const Surface sf = hit_surface(s, inst, __float_as_uint(h.w), h.x, h.y);
+            const float4 m1 = __ldg(s.materials + sf.material * 2 + 1);
+            if (!(m1.x > 0.0f || m1.y > 0.0f || m1.z > 0.0f)) {
+                const float4 qd = qb[i];
+                const float3 wo = -f3(qd.x, qd.y, qd.z);
+                float3 n = sf.normal;
+                if (dot(n, wo) < 0.0f) n = -n;
+                a = make_float4(sf.pos.x, sf.pos.y, sf.pos.z, 1.0f);
+                b = make_float4(n.x, n.y, n.z, 1.0f);
+                c = make_float4(wo.x, wo.y, wo.z, 0.0f);
+            }
+        }
+        surf[size_t(i) * 3] = a; surf[size_t(i) * 3 + 1] = b; surf[size_t(i) * 3 + 2] = c;
+    }
+}
+
+// Shade stage of the guided tracer (cf. shade_kernel in pathtracer.cu).
+template <bool SlotMixture>
+__global__ void __launch_bounds__(kBlock) guided_shade_kernel(DevScene s, GuidedLaunch G,
+                                                              const float4* __restrict__ qa,
+                                                              const float4* __restrict__ qb,
+                                                              const float4* __restrict__ qc,
+                                                              const float4* __restrict__ hits,
+                                                              float4* na, float4* nb, float4* nc,
+                                                              float4* sa, float4* sb, float4* sc,
+                                                              float4* __restrict__ out,
+                                                              const uint32_t* count_ptr,
+                                                              uint32_t* next_count, uint32_t* shadow_count) {
+    const uint32_t count = *count_ptr;
+    const uint32_t warp_first = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = warp_first; base < count; base += stride) {
+        const uint32_t i = base + lane_id();
+        bool cont = false, emit_shadow = false;
+        uint32_t pid = 0, seed = 0;
+        float3 new_o = f3(0, 0, 0), wi = f3(0, 0, 0), thp = f3(0, 0, 0);
+        float3 sh_o = f3(0, 0, 0), sh_d = f3(0, 0, 0), contrib = f3(0, 0, 0);
+        float sh_tmax = 0.0f;
+        if (i < count) {
+            const float4 a = qa[i], b = qb[i], c = qc[i];
+            const float4 h = hits[i];
+            pid = __float_as_uint(a.w);
+            seed = __float_as_uint(b.w);
+            const float3 ray_dir = f3(b.x, b.y, b.z);
+            thp = f3(c.x, c.y, c.z);
+            float4 o = out[pid];
+            if (G.bounce > 0)  // radiance gathered before the previous vertex's continuation
+                reinterpret_cast<float*>(G.rec2 + size_t(G.bounce - 1) * G.paths + pid)[3] = lum709(xyz(o));
+            const uint32_t inst = __float_as_uint(h.z);
+            if (inst == kNoIndex) {
+                const float3 L = thp * sky_radiance(ray_dir);
+                o.x = o.x + L.x; o.y = o.y + L.y; o.z = o.z + L.z;
+                out[pid] = o;
+            } else {
+                const Surface sf = hit_surface(s, inst, __float_as_uint(h.w), h.x, h.y);
+                const float4 m0 = __ldg(s.materials + sf.material * 2);
+                const float4 m1 = __ldg(s.materials + sf.material * 2 + 1);
+                if (m1.x > 0.0f || m1.y > 0.0f || m1.z > 0.0f) {
+                    const float3 L = thp * f3(m1.x, m1.y, m1.z);
+                    o.x = o.x + L.x; o.y = o.y + L.y; o.z = o.z + L.z;
+                    out[pid] = o;
+                } else {
+                    const float3 wo = -ray_dir;
+                    float3 n = sf.normal;
+                    if (dot(n, wo) < 0.0f) n = -n;
+                    const float3 base_c = f3(m0.x, m0.y, m0.z);
+                    const float metallic = m0.w, roughness = m1.w;
+                    if (s.num_lights > 0) {  // NEE exactly as the reference
+                        const uint32_t N = s.num_lights;
+                        const uint32_t li = uint32_t(rand_float(seed) * float(N)) % N;
+                        const float4 l0 = __ldg(s.lights + li * 3);
+                        const float4 l1 = __ldg(s.lights + li * 3 + 1);
+                        const float4 l2 = __ldg(s.lights + li * 3 + 2);
+                        const bool is_point = __float_as_uint(l0.w) == 0u;
+                        float3 ldir; float dist, pdf_light;
+                        if (is_point) {
+                            const float3 to = f3(l0.x, l0.y, l0.z) - sf.pos;
+                            dist = length(to);
+                            ldir = to / dist;
+                            pdf_light = dist * dist;
+                        } else {
+                            ldir = normalize(-f3(l1.x, l1.y, l1.z));
+                            dist = 1e9f;
+                            pdf_light = 1.0f;
+                        }
+                        if (dot(ldir, n) > 0.0f) {
+                            const float3 brdf_val = brdf_eval(n, wo, ldir, base_c, metallic, roughness);
+                            const float n_dot_l = mx(dot(n, ldir), 0.0f);
+                            const float den = is_point ? (pdf_light + 1e-6f) : 1.0f;
+                            const float3 irr = f3(l2.x * l2.w / den, l2.y * l2.w / den, l2.z * l2.w / den);
+                            float mis = 1.0f;
+                            if (!is_point) {
+                                const float pb = brdf_pdf(wo, ldir, n, roughness);
+                                mis = (pdf_light * pdf_light) / (pdf_light * pdf_light + pb * pb + 1e-10f);
+                            }
+                            contrib = thp * ((((brdf_val * irr) * n_dot_l) * mis) * float(N));
+                            sh_o = sf.pos + n * 1e-4f;
+                            sh_d = ldir;
+                            sh_tmax = dist - 0.01f;
+                            emit_shadow = true;
+                        }
+                    }
+                    if (!G.last) {
+                        VmfMixture mix;
+                        bool valid;
+                        if (SlotMixture) load_mixture_slot(G.mix, i, mix, valid);
+                        else load_mixture_grid(G.grid, sf.pos, mix, valid);
+                        const float alpha = valid ? G.alpha : 0.0f;
+                        const float u_sel = rand_float(seed);
+                        const float u0 = rand_float(seed);
+                        const float u1 = rand_float(seed);
+                        if (u_sel < alpha) {
+                            const float u2 = rand_float(seed);
+                            wi = mixture_sample(mix, G.lobes, u0, u1, u2);
+                        } else {
+                            float pdf_b;
+                            brdf_sample(wo, n, base_c, metallic, roughness, u0, u1, wi, pdf_b);
+                        }
+                        const float cos_i = dot(n, wi);
+                        float pdf = 0.0f;
+                        if (cos_i > 0.0f) {
+                            const float pb = brdf_sample_pdf(wo, n, base_c, metallic, roughness, wi);
+                            const float pg = valid ? mixture_pdf(mix, G.lobes, wi) : 0.0f;
+                            pdf = alpha * pg + (1.0f - alpha) * pb;
+                        }
+                        if (pdf > 1e-6f) {
+                            const float3 f = brdf_eval(n, wo, wi, base_c, metallic, roughness);
+                            thp = thp * ((f * cos_i) / pdf);
+                            bool alive = true;
+                            if (G.bounce >= 3) {
+                                const float survive = mn(mx(thp.x, mx(thp.y, thp.z)), 0.95f);
+                                if (rand_float(seed) > survive) alive = false;
+                                else thp = thp / survive;
+                            }
+                            if (alive) {
+                                cont = true;
+                                new_o = sf.pos + n * 1e-4f;
+                                const size_t r = size_t(G.bounce) * G.paths + pid;
+                                G.rec0[r] = make_float4(sf.pos.x, sf.pos.y, sf.pos.z, pdf);
+                                G.rec1[r] = make_float4(wi.x, wi.y, wi.z, lum709(thp));
+                                G.rec2[r] = make_float4(n.x, n.y, n.z, __int_as_float(-1));
+                                G.rec3[r] = make_float4(wo.x, wo.y, wo.z, 0.0f);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        const uint32_t sslot = warp_alloc(emit_shadow, shadow_count);
+        if (emit_shadow) {
+            sa[sslot] = make_float4(sh_o.x, sh_o.y, sh_o.z, __uint_as_float(pid));
+            sb[sslot] = make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
+            sc[sslot] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+        }
+        const uint32_t rslot = warp_alloc(cont, next_count);
+        if (cont) {
+            na[rslot] = make_float4(new_o.x, new_o.y, new_o.z, __uint_as_float(pid));
+            nb[rslot] = make_float4(wi.x, wi.y, wi.z, __uint_as_float(seed));
+            nc[rslot] = make_float4(thp.x, thp.y, thp.z, 0.0f);
+        }
+    }
+}
+
+// One training sample per recorded vertex whose continuation was traced.
+__global__ void __launch_bounds__(kBlock) resolve_kernel(const float4* __restrict__ out, const float4* __restrict__ rec0,
+                                                         const float4* __restrict__ rec1, const float4* __restrict__ rec2,
+                                                         const float4* __restrict__ rec3, uint32_t paths,
+                                                         uint32_t bounces, GuideSamples S) {
+    const uint64_t total = uint64_t(paths) * bounces;
+    for (uint64_t k = uint64_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u); k < total;
+         k += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t r = k + lane_id();
+        bool emit = false;
+        float4 s0, s1, s2, s3;
+        if (r < total) {
+            const float4 c = rec2[r];
+            const float before = c.w;
+            if (before >= 0.0f) {  // NaN (never filled) fails this test
+                const float4 a = rec0[r], b = rec1[r];
+                const uint32_t pid = uint32_t(r % paths);
+                const float final_l = lum709(xyz(out[pid]));
+                const float lin = mx(final_l - before, 0.0f) / mx(b.w, 1e-20f);
+                const float w = lin / a.w;
+                if (w > 0.0f && w < 3.0e38f) {
+                    emit = true;
+                    s0 = make_float4(a.x, a.y, a.z, w);
+                    s1 = make_float4(b.x, b.y, b.z, __uint_as_float(uint32_t(r)));
+                    s2 = make_float4(c.x, c.y, c.z, 0.0f);
+                    const float4 d = rec3[r];
+                    s3 = make_float4(d.x, d.y, d.z, 0.0f);
+                }
+            }
+        }
+        const uint32_t slot = warp_alloc(emit, S.count);
+        if (emit && slot < S.capacity) {
+            S.s0[slot] = s0; S.s1[slot] = s1; S.s2[slot] = s2; S.s3[slot] = s3;
+        }
+    }
+}
+
+// ── grid guide update ──────────────────────────────────────────────────────
+__global__ void __launch_bounds__(256) grid_keys_kernel(GridView g, GuideSamples S, uint32_t n,
+                                                        unsigned long long* keys, uint32_t* vals) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = S.s0[i], b = S.s1[i];
+    keys[i] = (static_cast<unsigned long long>(grid_cell(g, xyz(a))) << 32) | __float_as_uint(b.w);
+    vals[i] = i;
+}
+
+__global__ void __launch_bounds__(256) grid_ranges_kernel(const unsigned long long* keys, uint32_t n,
+                                                          uint32_t* start, uint32_t* end) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t c = uint32_t(keys[i] >> 32);
+    if (i == 0 || uint32_t(keys[i - 1] >> 32) != c) start[c] = i;
+    if (i + 1 == n || uint32_t(keys[i + 1] >> 32) != c) end[c] = i + 1;
+}
+
+// One stepwise-EM iteration per cell over its samples in sorted order.
+__global__ void __launch_bounds__(128) grid_em_kernel(GridView g, GuideSamples S, const uint32_t* __restrict__ order,
+                                                      const uint32_t* __restrict__ start,
+                                                      const uint32_t* __restrict__ end, double* __restrict__ stats,
+                                                      float4* lobes, float* weights, float decay,
+                                                      uint32_t* valid_cells) {
+    const uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= g.cells) return;
+    const uint32_t b = start[cell], e = end[cell];
+    if (e <= b) {  // no new samples: the mixture is kept as it is
+        float w = 0.0f;
+        for (int j = 0; j < kMaxLobes; ++j) w += weights[size_t(cell) * kMaxLobes + j];
+        if (w > 0.0f) atomicAdd(valid_cells, 1u);
+        return;
+    }
+    VmfMixture m;
+    float wsum = 0.0f;
+    for (int j = 0; j < kMaxLobes; ++j) {
+        m.lobe[j] = lobes[size_t(cell) * kMaxLobes + j];
+        m.weight[j] = weights[size_t(cell) * kMaxLobes + j];
+        wsum += m.weight[j];
+    }
+    if (!(wsum > 0.0f)) {  // unfitted cell: 8 lobes on the cube diagonals
+        for (int j = 0; j < kMaxLobes; ++j) {
+            const float k = 0.57735026918962576f;
+            m.lobe[j] = make_float4((j & 1) ? k : -k, (j & 2) ? k : -k, (j & 4) ? k : -k, 2.0f);
+            m.weight[j] = 1.0f / kMaxLobes;
+        }
+    }
+    double s0[kMaxLobes], s1x[kMaxLobes], s1y[kMaxLobes], s1z[kMaxLobes];
+    double* st = stats + size_t(cell) * kMaxLobes * 4;
+    for (int j = 0; j < kMaxLobes; ++j) {
+        s0[j] = double(decay) * st[j * 4 + 0];
+        s1x[j] = double(decay) * st[j * 4 + 1];
+        s1y[j] = double(decay) * st[j * 4 + 2];
+        s1z[j] = double(decay) * st[j * 4 + 3];
+    }
+    for (uint32_t k = b; k < e; ++k) {
+        const uint32_t si = order[k];
+        const float4 a = S.s0[si];
+        const float4 d = S.s1[si];
+        const float3 om = f3(d.x, d.y, d.z);
+        float gam[kMaxLobes];
+        float gsum = 0.0f;
+        for (int j = 0; j < kMaxLobes; ++j) {
+            gam[j] = m.weight[j] > 0.0f ? m.weight[j] * vmf_pdf(xyz(m.lobe[j]), m.lobe[j].w, om) : 0.0f;
+            gsum += gam[j];
+        }
+        if (!(gsum > 0.0f)) continue;
+        const double w = double(a.w);
+        for (int j = 0; j < kMaxLobes; ++j) {
+            const double r = w * double(gam[j] / gsum);
+            s0[j] += r;
+            s1x[j] += r * double(om.x);
+            s1y[j] += r * double(om.y);
+            s1z[j] += r * double(om.z);
+        }
+    }
+    double tot = 0.0;
+    for (int j = 0; j < kMaxLobes; ++j) tot += s0[j];
+    for (int j = 0; j < kMaxLobes; ++j) {
+        st[j * 4 + 0] = s0[j]; st[j * 4 + 1] = s1x[j]; st[j * 4 + 2] = s1y[j]; st[j * 4 + 3] = s1z[j];
+        float4 lobe = m.lobe[j];
+        float wj = 0.0f;
+        if (tot > 0.0 && s0[j] > 0.0) {
+            const double len = sqrt(s1x[j] * s1x[j] + s1y[j] * s1y[j] + s1z[j] * s1z[j]);
+            double r = len / s0[j];
+            r = r < 1e-4 ? 1e-4 : (r > 0.9999 ? 0.9999 : r);
+            double kappa = r * (3.0 - r * r) / (1.0 - r * r);
+            kappa = kappa < 0.5 ? 0.5 : (kappa > 512.0 ? 512.0 : kappa);
+            if (len > 1e-12) lobe = make_float4(float(s1x[j] / len), float(s1y[j] / len), float(s1z[j] / len), float(kappa));
+            wj = float(s0[j] / tot);
+        }
+        lobes[size_t(cell) * kMaxLobes + j] = lobe;
+        weights[size_t(cell) * kMaxLobes + j] = wj;
+    }
+    if (tot > 0.0) atomicAdd(valid_cells, 1u);
+}
+
+} // namespace
+} // namespace rr
+
+using namespace rr;
+
+// ── host side ──────────────────────────────────────────────────────────────
+static rr_status guide_alloc(rr_ctx* ctx, rr_guide* g, void** p, size_t bytes) {
+    RR_TRY_CUDA(ctx, cudaMalloc(p, bytes));
+    g->allocations.push_back(*p);
+    return RR_OK;
+}
+
+extern "C" rr_status rr_guide_create(rr_ctx* ctx, const rr_guide_desc* d, rr_guide** out) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    if (!d || !out) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_guide_create: null argument");
+    *out = nullptr;
+    if (d->kind != RR_GUIDE_GRID && d->kind != RR_GUIDE_MLP)
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_guide_create: unknown guide kind %u", d->kind);
+    if (d->kind == RR_GUIDE_GRID && (d->grid_resolution == 0 || d->grid_resolution > 256))
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "grid_resolution must be 1..256");
+    for (int a = 0; a < 3; ++a)
+        if (!(d->bounds_max[a] > d->bounds_min[a])) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "empty guide bounds");
+    if (d->max_samples == 0 || !(d->alpha >= 0.0f && d->alpha <= 1.0f))
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_guide_create: bad max_samples or alpha");
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    rr_guide* g = new rr_guide;
+    g->ctx = ctx;
+    g->desc = *d;
+    rr_status st;
+    auto fail = [&](rr_status s) { rr_guide_destroy(g); return s; };
+    const uint32_t cap = d->max_samples;
+    g->samples.capacity = cap;
+    for (int k = 0; k < 4; ++k) {
+        void* p;
+        if ((st = guide_alloc(ctx, g, &p, size_t(cap) * sizeof(float4))) != RR_OK) return fail(st);
+        (&g->samples.s0)[k] = static_cast<float4*>(p);
+    }
+    {
+        void* p;
+        if ((st = guide_alloc(ctx, g, &p, sizeof(uint32_t) * 4)) != RR_OK) return fail(st);
+        g->samples.count = static_cast<uint32_t*>(p);
+        cudaMemset(p, 0, sizeof(uint32_t) * 4);
+    }
+    if (d->kind == RR_GUIDE_GRID) {
+        const uint32_t R = d->grid_resolution;
+        const size_t cells = size_t(R) * R * R;
+        GridView& v = g->grid;
+        v.res = R;
+        v.cells = uint32_t(cells);
+        v.bmin = make_float3(d->bounds_min[0], d->bounds_min[1], d->bounds_min[2]);
+        v.scale = make_float3(float(R) / (d->bounds_max[0] - d->bounds_min[0]),
+                              float(R) / (d->bounds_max[1] - d->bounds_min[1]),
+                              float(R) / (d->bounds_max[2] - d->bounds_min[2]));
+        void* p;
+        if ((st = guide_alloc(ctx, g, &p, cells * kMaxLobes * sizeof(float4))) != RR_OK) return fail(st);
+        v.lobes = static_cast<float4*>(p);
+        if ((st = guide_alloc(ctx, g, &p, cells * kMaxLobes * sizeof(float))) != RR_OK) return fail(st);
+        v.weights = static_cast<float*>(p);
+        if ((st = guide_alloc(ctx, g, &p, cells * kMaxLobes * 4 * sizeof(double))) != RR_OK) return fail(st);
+        g->stats64 = static_cast<double*>(p);
+        if ((st = guide_alloc(ctx, g, &p, cells * sizeof(uint32_t))) != RR_OK) return fail(st);
+        g->cell_start = static_cast<uint32_t*>(p);
+        if ((st = guide_alloc(ctx, g, &p, cells * sizeof(uint32_t))) != RR_OK) return fail(st);
+        g->cell_end = static_cast<uint32_t*>(p);
+        if ((st = guide_alloc(ctx, g, &p, size_t(cap) * 8)) != RR_OK) return fail(st);
+        g->keys_in = static_cast<unsigned long long*>(p);
+        if ((st = guide_alloc(ctx, g, &p, size_t(cap) * 8)) != RR_OK) return fail(st);
+        g->keys_out = static_cast<unsigned long long*>(p);
+        if ((st = guide_alloc(ctx, g, &p, size_t(cap) * 4)) != RR_OK) return fail(st);
+        g->vals_in = static_cast<uint32_t*>(p);
+        if ((st = guide_alloc(ctx, g, &p, size_t(cap) * 4)) != RR_OK) return fail(st);
+        g->vals_out = static_cast<uint32_t*>(p);
+        size_t tmp = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tmp, g->keys_in, g->keys_out, g->vals_in, g->vals_out, int(cap), 0, 64);
+        if ((st = guide_alloc(ctx, g, &p, tmp)) != RR_OK) return fail(st);
+        g->sort_tmp = p;
+        g->sort_tmp_bytes = tmp;
+    } else {
+        if ((st = rr_mlp_guide_init(ctx, g)) != RR_OK) return fail(st);
+    }
+    if ((st = rr_guide_reset(ctx, g, nullptr)) != RR_OK) return fail(st);
+    RR_TRY_CUDA(ctx, cudaDeviceSynchronize());
+    *out = g;
+    return RR_OK;
+}
+
+extern "C" rr_status rr_guide_destroy(rr_guide* g) {
+    if (!g) return RR_ERR_INVALID_ARGUMENT;
+    if (g->ctx) cudaSetDevice(g->ctx->device);
+    for (void* p : g->allocations) cudaFree(p);
+    if (g->ev0) cudaEventDestroy(g->ev0);
+    if (g->ev1) cudaEventDestroy(g->ev1);
+    delete g;
+    return RR_OK;
+}
+
+extern "C" rr_status rr_guide_reset(rr_ctx* ctx, rr_guide* g, void* stream_v) {
+    if (!ctx || !g) return RR_ERR_INVALID_ARGUMENT;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    RR_TRY_CUDA(ctx, cudaMemsetAsync(g->samples.count, 0, sizeof(uint32_t) * 4, stream));
+    if (g->desc.kind == RR_GUIDE_GRID) {
+        const size_t cells = g->grid.cells;
+        RR_TRY_CUDA(ctx, cudaMemsetAsync(g->grid.lobes, 0, cells * kMaxLobes * sizeof(float4), stream));
+        RR_TRY_CUDA(ctx, cudaMemsetAsync(g->grid.weights, 0, cells * kMaxLobes * sizeof(float), stream));
+        RR_TRY_CUDA(ctx, cudaMemsetAsync(g->stats64, 0, cells * kMaxLobes * 4 * sizeof(double), stream));
+    } else {
+        rr_status st = rr_mlp_guide_reset(ctx, g, stream);
+        if (st != RR_OK) return st;
+    }
+    g->stats = rr_guide_stats{};
+    return RR_OK;
+}
+
+static rr_status ensure_records(rr_ctx* ctx, rr_guide* g, size_t paths, uint32_t bounces) {
+    const size_t need = paths * bounces;
+    if (g->rec_capacity >= need) return RR_OK;
+    for (int k = 0; k < 4; ++k) { cudaFree(g->rec[k]); g->rec[k] = nullptr; }
+    g->rec_capacity = 0;
+    for (int k = 0; k < 4; ++k) RR_TRY_CUDA(ctx, cudaMalloc(&g->rec[k], need * sizeof(float4)));
+    g->rec_capacity = need;
+    return RR_OK;
+}
+
+extern "C" rr_status rr_guided_pathtracer_execute(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* cam,
+                                                  const rr_pt_params* p, rr_guide* g, float* radiance_out,
+                                                  void* stream_v) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    if (!scene || !cam || !p || !g || !radiance_out)
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_guided_pathtracer_execute: null argument");
+    const uint32_t W = cam->screen_width, H = cam->screen_height;
+    if (W == 0 || H == 0 || p->spp == 0 || p->max_bounces == 0 || p->max_bounces > uint32_t(kMaxBounces))
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_guided_pathtracer_execute: bad size or bounces");
+    const uint64_t n64 = uint64_t(W) * H * p->spp;
+    if (n64 >= (1ull << 31) || n64 * p->max_bounces >= (1ull << 32))
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_guided_pathtracer_execute: too many paths");
+    const size_t n = size_t(n64);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    rr_status st = ensure_queues(ctx, n);
+    if (st != RR_OK) return st;
+    if ((st = ensure_records(ctx, g, n, p->max_bounces)) != RR_OK) return st;
+    const bool mlp = g->desc.kind == RR_GUIDE_MLP;
+    if (mlp && (st = rr_mlp_guide_ensure(ctx, g, n)) != RR_OK) return st;
+    rr_pt_queues& q = ctx->pt;
+    uint32_t* C = ctx->counters;
+    RR_TRY_CUDA(ctx, cudaMemsetAsync(C, 0, sizeof(uint32_t) * kCounterWords, stream));
+    RR_TRY_CUDA(ctx, cudaMemsetAsync(g->samples.count, 0, sizeof(uint32_t) * 4, stream));
+    // unfilled records read as NaN and are skipped by the resolve pass
+    RR_TRY_CUDA(ctx, cudaMemsetAsync(g->rec[2], 0xff, n * p->max_bounces * sizeof(float4), stream));
+
+    PtLaunch L;
+    L.cam = *cam;
+    L.frame_seed = p->frame_seed;
+    L.spp = p->spp;
+    L.width = W; L.height = H;
+    L.tiles_x = (W + 7) / 8;
+    L.tiles_per_image = L.tiles_x * ((H + 3) / 4);
+    float4* out = reinterpret_cast<float4*>(radiance_out);
+    {
+        const uint64_t threads = uint64_t(L.tiles_per_image) * p->spp * 32;
+        raygen_kernel<<<uint32_t((threads + kBlock - 1) / kBlock), kBlock, 0, stream>>>(L, out, q.ray_a[0], q.ray_b[0],
+                                                                                       q.ray_c[0], C);
+        RR_CHECK_LAUNCH(ctx);
+    }
+    QueueKernel ext_k = extend_variant<false>(ctx->extend_variant);
+    ShadowKernel sh_k = shadow_variant<false>(ctx->shadow_variant);
+    const int g_ext = persistent_grid(ctx, reinterpret_cast<const void*>(ext_k));
+    const int g_sh = persistent_grid(ctx, reinterpret_cast<const void*>(sh_k));
+    auto shade_k = mlp ? guided_shade_kernel<true> : guided_shade_kernel<false>;
+    const int g_shade = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(shade_k)),
+                                      int((n + kBlock - 1) / kBlock));
+    GuidedLaunch G;
+    G.paths = uint32_t(n);
+    G.lobes = kMaxLobes;
+    G.alpha = g->desc.alpha;
+    G.grid = g->grid;
+    G.mix = mlp ? g->mlp_mix : nullptr;
+    G.rec0 = g->rec[0]; G.rec1 = g->rec[1]; G.rec2 = g->rec[2]; G.rec3 = g->rec[3];
+    const DevScene& S = scene->dev;
+    uint64_t launches = 1;
+    for (uint32_t b = 0; b < p->max_bounces; ++b) {
+        const int cur = b & 1, nxt = cur ^ 1;
+        uint32_t* cb = C + 4 * b;
+        uint32_t* cn = C + 4 * (b + 1);
+        G.bounce = b;
+        G.last = b + 1 == p->max_bounces ? 1u : 0u;
+        ext_k<<<g_ext, kBlock, 0, stream>>>(S, q.ray_a[cur], q.ray_b[cur], q.hits, cb, cb + 1, ctx->work64);
+        RR_CHECK_LAUNCH(ctx);
+        if (mlp && !G.last) {
+            guided_surface_kernel<<<g_shade, kBlock, 0, stream>>>(S, q.ray_b[cur], q.hits, g->mlp_surf, cb);
+            RR_CHECK_LAUNCH(ctx);
+            if ((st = rr_mlp_guide_infer(ctx, g, cb, uint32_t(n), stream)) != RR_OK) return st;
+            launches += 1 + g->mlp_infer_launches;
+        }
+        shade_k<<<g_shade, kBlock, 0, stream>>>(S, G, q.ray_a[cur], q.ray_b[cur], q.ray_c[cur], q.hits,
+                                                q.ray_a[nxt], q.ray_b[nxt], q.ray_c[nxt], q.shadow_a, q.shadow_b,
+                                                q.shadow_c, out, cb, cn, cb + 2);
+        RR_CHECK_LAUNCH(ctx);
+        sh_k<<<g_sh, kBlock, 0, stream>>>(S, q.shadow_a, q.shadow_b, q.shadow_c, out, cb + 2, cb + 3, ctx->work64 + 2);
+        RR_CHECK_LAUNCH(ctx);
+        launches += 3;
+    }
+    if (p->max_bounces > 1) {
+        resolve_kernel<<<std::max(1, ctx->sm_count * 8), kBlock, 0, stream>>>(
+            out, g->rec[0], g->rec[1], g->rec[2], g->rec[3], uint32_t(n), p->max_bounces - 1, g->samples);
+        RR_CHECK_LAUNCH(ctx);
+        launches += 1;
+    }
+    ctx->launches += launches;
+    ctx->last_max_bounces = p->max_bounces;
+    ctx->last_counted = false;
+    g->frame_paths = uint32_t(n);
+    return RR_OK;
+}
+
+extern "C" rr_status rr_guide_update(rr_ctx* ctx, rr_guide* g, void* stream_v) {
+    if (!ctx || !g) return RR_ERR_INVALID_ARGUMENT;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (!g->ev0) { RR_TRY_CUDA(ctx, cudaEventCreate(&g->ev0)); RR_TRY_CUDA(ctx, cudaEventCreate(&g->ev1)); }
+    // the sample count decides the launch sizes: read it back (one small copy)
+    uint32_t n = 0;
+    RR_TRY_CUDA(ctx, cudaMemcpyAsync(&n, g->samples.count, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    RR_TRY_CUDA(ctx, cudaStreamSynchronize(stream));
+    g->stats.samples_recorded = n;
+    n = std::min(n, g->samples.capacity);
+    RR_TRY_CUDA(ctx, cudaEventRecord(g->ev0, stream));
+    if (g->desc.kind == RR_GUIDE_GRID) {
+        GridView& v = g->grid;
+        RR_TRY_CUDA(ctx, cudaMemsetAsync(g->cell_start, 0, size_t(v.cells) * 4, stream));
+        RR_TRY_CUDA(ctx, cudaMemsetAsync(g->cell_end, 0, size_t(v.cells) * 4, stream));
+        RR_TRY_CUDA(ctx, cudaMemsetAsync(g->samples.count + 1, 0, sizeof(uint32_t), stream));
+        if (n > 0) {
+            grid_keys_kernel<<<(n + 255) / 256, 256, 0, stream>>>(v, g->samples, n, g->keys_in, g->vals_in);
+            RR_CHECK_LAUNCH(ctx);
+            size_t tmp = g->sort_tmp_bytes;
+            RR_TRY_CUDA(ctx, cub::DeviceRadixSort::SortPairs(g->sort_tmp, tmp, g->keys_in, g->keys_out, g->vals_in,
+                                                             g->vals_out, int(n), 0, 64, stream));
+            grid_ranges_kernel<<<(n + 255) / 256, 256, 0, stream>>>(g->keys_out, n, g->cell_start, g->cell_end);
+            RR_CHECK_LAUNCH(ctx);
+        }
+        grid_em_kernel<<<(v.cells + 127) / 128, 128, 0, stream>>>(v, g->samples, g->vals_out, g->cell_start,
+                                                                   g->cell_end, g->stats64, v.lobes, v.weights,
+                                                                   g->desc.decay, g->samples.count + 1);
+        RR_CHECK_LAUNCH(ctx);
+        ctx->launches += 4;
+    } else {
+        rr_status st = rr_mlp_guide_train(ctx, g, n, stream);
+        if (st != RR_OK) return st;
+    }
+    RR_TRY_CUDA(ctx, cudaEventRecord(g->ev1, stream));
+    g->stats.samples_used = n;
+    g->stats.updates += 1;
+    g->pending_stats = true;
+    return RR_OK;
+}
+
+extern "C" rr_status rr_guide_get_stats(rr_ctx* ctx, const rr_guide* gc, rr_guide_stats* out) {
+    if (!ctx || !gc || !out) return RR_ERR_INVALID_ARGUMENT;
+    rr_guide* g = const_cast<rr_guide*>(gc);
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (g->pending_stats) {
+        RR_TRY_CUDA(ctx, cudaEventSynchronize(g->ev1));
+        float ms = 0.0f;
+        RR_TRY_CUDA(ctx, cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+        g->stats.ms_update = ms;
+        uint32_t c[4];
+        RR_TRY_CUDA(ctx, cudaMemcpy(c, g->samples.count, sizeof(c), cudaMemcpyDeviceToHost));
+        if (g->desc.kind == RR_GUIDE_GRID) g->stats.cells_valid = c[1];
+        else g->stats.last_loss = rr_mlp_guide_last_loss(g);
+        g->pending_stats = false;
+    }
+    *out = g->stats;
+    return RR_OK;
+}
+
+namespace rr {
+namespace {
+__global__ void __launch_bounds__(256) grid_eval_kernel(GridView g, const float4* __restrict__ surf,
+                                                        float4* __restrict__ mix, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t cell = grid_cell(g, xyz(surf[size_t(i) * 3]));
+    float4* m = mix + size_t(i) * (kMaxLobes + 2);
+    float w[kMaxLobes];
+    for (int j = 0; j < kMaxLobes; ++j) {
+        m[j] = g.lobes[size_t(cell) * kMaxLobes + j];
+        w[j] = g.weights[size_t(cell) * kMaxLobes + j];
+    }
+    m[kMaxLobes] = make_float4(w[0], w[1], w[2], w[3]);
+    m[kMaxLobes + 1] = make_float4(w[4], w[5], w[6], w[7]);
+}
+__global__ void set_count_kernel(uint32_t* c, uint32_t n) { *c = n; }
+} // namespace
+} // namespace rr
+
+extern "C" rr_status rr_guide_eval(rr_ctx* ctx, rr_guide* g, const float* surf, uint32_t count, float* mix_out,
+                                   void* stream_v) {
+    if (!ctx || !g) return RR_ERR_INVALID_ARGUMENT;
+    if (count == 0) return RR_OK;
+    if (!surf || !mix_out) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_guide_eval: null buffer");
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (g->desc.kind == RR_GUIDE_GRID) {
+        grid_eval_kernel<<<(count + 255) / 256, 256, 0, stream>>>(g->grid, reinterpret_cast<const float4*>(surf),
+                                                                  reinterpret_cast<float4*>(mix_out), count);
+        RR_CHECK_LAUNCH(ctx);
+        ctx->launches += 1;
+        return RR_OK;
+    }
+    set_count_kernel<<<1, 1, 0, stream>>>(g->samples.count + 2, count);
+    RR_CHECK_LAUNCH(ctx);
+    return rr_mlp_guide_eval(ctx, g, reinterpret_cast<const float4*>(surf), reinterpret_cast<float4*>(mix_out),
+                             g->samples.count + 2, count, stream);
+}
+
+namespace rr {
+namespace {
+__global__ void __launch_bounds__(256) set_samples_kernel(const float4* __restrict__ src, GuideSamples S, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) S.count[0] = n;
+    if (i >= n) return;
+    S.s0[i] = src[size_t(i) * 4]; S.s1[i] = src[size_t(i) * 4 + 1];
+    S.s2[i] = src[size_t(i) * 4 + 2]; S.s3[i] = src[size_t(i) * 4 + 3];
+}
+} // namespace
+} // namespace rr
+
+extern "C" rr_status rr_guide_set_samples(rr_ctx* ctx, rr_guide* g, const float* samples, uint32_t count,
+                                          void* stream_v) {
+    if (!ctx || !g) return RR_ERR_INVALID_ARGUMENT;
+    if ((count && !samples) || count > g->samples.capacity)
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_guide_set_samples: null buffer or count above capacity");
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    set_samples_kernel<<<std::max(1u, (count + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream_v)>>>(
+        reinterpret_cast<const float4*>(samples), g->samples, count);
+    RR_CHECK_LAUNCH(ctx);
+    return RR_OK;
+}

@@ -9,6 +9,7 @@
 //           point (sample_primary_dir, restir_pt.slang:520-563)
 
 #include "rr_internal.h"
+#include "rr_vmf.cuh"
 
 namespace rr {
 namespace {
@@ -65,28 +66,6 @@ __global__ void __launch_bounds__(256) fit_kernel(int4* __restrict__ accum, floa
     float kappa = r * (3.0f - r * r) / (1.0f - r * r);
     kappa = clampf(kappa, 0.5f, g.kappa_max);
     fitted[cell] = make_float4(mu.x, mu.y, mu.z, kappa);
-}
-
-// GuidingGrid.slang:160-189
-RR_D float3 vmf_sample(float3 mu, float kappa, float ux, float uy, float& pdf) {
-    const float k = mx(kappa, 1.0e-3f);
-    float w = 1.0f + (1.0f / k) * rr_logf(ux + (1.0f - ux) * rr_expf(-2.0f * k));
-    w = clampf(w, -1.0f, 1.0f);
-    const float s = sqrtf(mx(0.0f, 1.0f - w * w));
-    const float phi = kTwoPi * uy;
-    const float3 local = f3(s * rr_cosf(phi), s * rr_sinf(phi), w);
-    float3 T, B;
-    build_onb(mu, T, B);
-    const float3 dir = tangent_to_world(local, T, B, mu);
-    const float denom = kTwoPi * (1.0f - rr_expf(-2.0f * k));
-    pdf = k * rr_expf(k * (w - 1.0f)) / mx(denom, 1.0e-8f);
-    return dir;
-}
-RR_D float vmf_pdf(float3 mu, float kappa, float3 dir) {
-    const float k = mx(kappa, 1.0e-3f);
-    const float w = clampf(dot(mu, dir), -1.0f, 1.0f);
-    const float denom = kTwoPi * (1.0f - rr_expf(-2.0f * k));
-    return k * rr_expf(k * (w - 1.0f)) / mx(denom, 1.0e-8f);
 }
 
 __global__ void __launch_bounds__(256) sample_kernel(const float4* __restrict__ fitted, const float4* __restrict__ pos,

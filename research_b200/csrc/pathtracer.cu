@@ -14,197 +14,12 @@
 // Radiance is accumulated into the caller's image in the same order as the
 // reference's `radiance +=` statements, which keeps results bit-identical.
 
-#include "rr_internal.h"
+#include "rr_wavefront.cuh"
 
 #include <cstring>
 
 namespace rr {
 namespace {
-
-constexpr int kBlock = 256;
-constexpr uint32_t kFull = 0xffffffffu;
-
-__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
-
-// Warp-aggregated slot allocation: returns this lane's slot when `want`.
-__device__ __forceinline__ uint32_t warp_alloc(bool want, uint32_t* counter) {
-    const uint32_t mask = __ballot_sync(kFull, want);
-    uint32_t base = 0;
-    if (lane_id() == 0 && mask) base = atomicAdd(counter, __popc(mask));
-    base = __shfl_sync(kFull, base, 0);
-    return base + __popc(mask & ((1u << lane_id()) - 1u));
-}
-
-struct PtLaunch {
-    GpuCameraData cam;
-    uint32_t frame_seed;
-    uint32_t spp;
-    uint32_t width, height;
-    uint32_t tiles_x, tiles_per_image;
-};
-
-// One warp per 8x4 pixel tile so that primary rays of a warp are coherent.
-__global__ void __launch_bounds__(kBlock) raygen_kernel(PtLaunch L, float4* __restrict__ out,
-                                                        float4* qa, float4* qb, float4* qc,
-                                                        uint32_t* counters) {
-    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t tile = gtid >> 5;
-    const uint32_t lane = lane_id();
-    const uint32_t total_tiles = L.tiles_per_image * L.spp;
-    bool active = tile < total_tiles;
-    uint32_t s = 0, px = 0, py = 0;
-    if (active) {
-        s = tile / L.tiles_per_image;
-        const uint32_t t = tile % L.tiles_per_image;
-        px = (t % L.tiles_x) * 8 + (lane & 7);
-        py = (t / L.tiles_x) * 4 + (lane >> 3);
-        active = px < L.width && py < L.height;
-    }
-    if (__all_sync(kFull, tile >= total_tiles)) return;
-    const uint32_t slot = warp_alloc(active, &counters[0]);
-    if (!active) return;
-    const uint32_t pid = (s * L.height + py) * L.width + px;
-    uint32_t seed = make_seed(px, py, L.frame_seed + s);
-    const float jx = rand_float(seed);
-    const float jy = rand_float(seed);
-    const float3 dir = primary_dir(L.cam, float(px) + jx, float(py) + jy);
-    out[pid] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-    qa[slot] = make_float4(L.cam.position[0], L.cam.position[1], L.cam.position[2], __uint_as_float(pid));
-    qb[slot] = make_float4(dir.x, dir.y, dir.z, __uint_as_float(seed));
-    qc[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-}
-
-// Adds per-thread traversal work to two 64-bit counters, one atomic per warp.
-__device__ __forceinline__ void flush_work(const TraceWork& w, unsigned long long* out) {
-    unsigned long long n = w.nodes, t = w.tris;
-    #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        n += __shfl_down_sync(kFull, n, o);
-        t += __shfl_down_sync(kFull, t, o);
-    }
-    if (lane_id() == 0 && (n | t)) { atomicAdd(out, n); atomicAdd(out + 1, t); }
-}
-
-// Warp-cooperative ray pool: hands queue indices [0, count) to idle lanes,
-// taking kChunk indices at a time from the launch's global cursor (one
-// atomic per chunk). All fields are warp-uniform.
-constexpr uint32_t kChunk = 256;
-constexpr uint32_t kRefillLanes = 8;
-
-struct WarpPool {
-    uint32_t next = 0, end = 0;
-    bool exhausted = false;
-    __device__ __forceinline__ bool done() const { return exhausted && next >= end; }
-    // Every lane calls this with the same idle mask; idle lanes get an index
-    // (or kNoIndex when the queue is drained).
-    __device__ __forceinline__ uint32_t refill(uint32_t idle_mask, bool idle, uint32_t count, uint32_t* cursor) {
-        const uint32_t n_idle = __popc(idle_mask);
-        const uint32_t rank = __popc(idle_mask & ((1u << lane_id()) - 1u));
-        const uint32_t avail = end - next;
-        const bool need = avail < n_idle && !exhausted;
-        uint32_t nb = 0;
-        if (need) {
-            if (lane_id() == 0) nb = atomicAdd(cursor, kChunk);
-            nb = __shfl_sync(kFull, nb, 0);
-        }
-        uint32_t idx = kNoIndex;
-        if (idle) {
-            if (rank < avail) idx = next + rank;
-            else if (need) idx = nb + (rank - avail);
-        }
-        if (idx >= count) idx = kNoIndex;
-        if (!need) {
-            next = min(next + n_idle, end);
-        } else if (nb >= count) {
-            exhausted = true;
-            next = end = 0;
-        } else {
-            end = min(nb + kChunk, count);
-            next = min(nb + (n_idle - avail), end);
-        }
-        return idx;
-    }
-};
-
-// Queue traversal, two schedules (chosen per context, see rr_pathtracer_tune):
-//  Refill = false: each warp takes 32 consecutive queue entries (neighbouring
-//    paths after compaction, hence coherent rays) and traces them to the end;
-//  Refill = true: persistent warps; a lane whose ray is finished takes a new
-//    one as soon as kRefillLanes lanes are idle, so warps do not wait for
-//    their slowest ray (less coherence, fewer idle lanes).
-// MinBlocks is the occupancy target handed to the register allocator.
-// `Finish(i, found, hit)` consumes a finished ray; `Load(i, ray, tmax)` makes one.
-template <bool AnyHit, bool Count, bool Refill, class Load, class Finish>
-__device__ __forceinline__ void traverse_queue(const DevScene& s, uint32_t count, uint32_t* cursor,
-                                               unsigned long long* work_out, Load load, Finish finish) {
-    TraceWork tw;
-    int2 stack[kStackSize];  // (node, near distance)
-    if constexpr (!Refill) {
-        while (true) {
-            uint32_t base = 0;
-            if (lane_id() == 0) base = atomicAdd(cursor, 32u);
-            base = __shfl_sync(kFull, base, 0);
-            if (base >= count) break;
-            const uint32_t i = base + lane_id();
-            if (i < count) {
-                Ray r; float tmax;
-                load(i, r, tmax);
-                HitRec h; TravState st;
-                trav_begin(st, h, tmax);
-                while (!trace_step<AnyHit, Count>(s, r, 0.001f, h, st, stack, &tw)) {}
-                finish(i, st.found, h);
-            }
-        }
-    } else {
-        WarpPool pool;
-        Ray r;
-        HitRec h;
-        TravState st;
-        uint32_t idx = kNoIndex;
-        bool has = false;
-        while (true) {
-            const uint32_t idle = __ballot_sync(kFull, !has);
-            if (idle && !pool.done() && (idle == kFull || __popc(idle) >= kRefillLanes)) {
-                const uint32_t ni = pool.refill(idle, !has, count, cursor);
-                if (!has && ni != kNoIndex) {
-                    idx = ni;
-                    float tmax;
-                    load(idx, r, tmax);
-                    trav_begin(st, h, tmax);
-                    has = true;
-                }
-            }
-            if (!__any_sync(kFull, has)) {
-                if (pool.done()) break;
-                continue;
-            }
-            if (has && trace_step<AnyHit, Count>(s, r, 0.001f, h, st, stack, &tw)) {
-                finish(idx, st.found, h);
-                has = false;
-            }
-        }
-    }
-    if (Count) flush_work(tw, work_out);
-}
-
-template <bool Count, bool Refill, int MinBlocks>
-__global__ void __launch_bounds__(kBlock, MinBlocks) extend_kernel(DevScene s, const float4* __restrict__ qa,
-                                                                   const float4* __restrict__ qb,
-                                                                   float4* __restrict__ hits,
-                                                                   const uint32_t* count_ptr, uint32_t* cursor,
-                                                                   unsigned long long* work_out) {
-    traverse_queue<false, Count, Refill>(
-        s, *count_ptr, cursor, work_out,
-        [&](uint32_t i, Ray& r, float& tmax) {
-            const float4 a = qa[i], b = qb[i];
-            r = make_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z));
-            tmax = 1e9f;
-        },
-        [&](uint32_t i, bool found, const HitRec& h) {
-            hits[i] = found ? make_float4(h.u, h.v, __uint_as_float(h.inst), __uint_as_float(h.prim))
-                            : make_float4(0.0f, 0.0f, __uint_as_float(kNoIndex), __uint_as_float(kNoIndex));
-        });
-}
 
 __global__ void __launch_bounds__(kBlock) shade_kernel(DevScene s, uint32_t bounce, uint32_t last,
                                                        const float4* __restrict__ qa,
@@ -329,86 +144,6 @@ __global__ void __launch_bounds__(kBlock) shade_kernel(DevScene s, uint32_t boun
             nc[rslot] = make_float4(thp.x, thp.y, thp.z, 0.0f);
         }
     }
-}
-
-// Any-hit shadow rays; unoccluded NEE contributions are added to the image.
-template <bool Count, bool Refill, int MinBlocks>
-__global__ void __launch_bounds__(kBlock, MinBlocks) shadow_kernel(DevScene s, const float4* __restrict__ sa,
-                                                                   const float4* __restrict__ sb,
-                                                                   const float4* __restrict__ sc,
-                                                                   float4* __restrict__ out,
-                                                                   const uint32_t* count_ptr, uint32_t* cursor,
-                                                                   unsigned long long* work_out) {
-    traverse_queue<true, Count, Refill>(
-        s, *count_ptr, cursor, work_out,
-        [&](uint32_t i, Ray& r, float& tmax) {
-            const float4 a = sa[i], b = sb[i];
-            r = make_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z));
-            tmax = b.w;
-        },
-        [&](uint32_t i, bool found, const HitRec&) {
-            if (!found) {
-                const float4 c = sc[i];
-                const uint32_t pid = __float_as_uint(sa[i].w);
-                float4 o = out[pid];
-                o.x = o.x + c.x; o.y = o.y + c.y; o.z = o.z + c.z;
-                out[pid] = o;
-            }
-        });
-}
-
-// Traversal kernel variants: schedule x occupancy target.
-using QueueKernel = void (*)(DevScene, const float4*, const float4*, float4*, const uint32_t*, uint32_t*,
-                             unsigned long long*);
-using ShadowKernel = void (*)(DevScene, const float4*, const float4*, const float4*, float4*, const uint32_t*,
-                              uint32_t*, unsigned long long*);
-template <bool Count>
-QueueKernel extend_variant(int v) {
-    switch (v) {
-    case 1: return extend_kernel<Count, false, 5>;
-    case 2: return extend_kernel<Count, false, 6>;
-    case 3: return extend_kernel<Count, true, 1>;
-    case 4: return extend_kernel<Count, true, 5>;
-    case 5: return extend_kernel<Count, true, 6>;
-    default: return extend_kernel<Count, false, 1>;
-    }
-}
-template <bool Count>
-ShadowKernel shadow_variant(int v) {
-    switch (v) {
-    case 1: return shadow_kernel<Count, false, 5>;
-    case 2: return shadow_kernel<Count, false, 6>;
-    case 3: return shadow_kernel<Count, true, 1>;
-    case 4: return shadow_kernel<Count, true, 5>;
-    case 5: return shadow_kernel<Count, true, 6>;
-    default: return shadow_kernel<Count, false, 1>;
-    }
-}
-
-int persistent_grid(const rr_ctx* ctx, const void* kernel) {
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, 0);
-    return ctx->sm_count * (per_sm > 0 ? per_sm : 1);
-}
-
-rr_status ensure_queues(rr_ctx* ctx, size_t n) {
-    rr_pt_queues& q = ctx->pt;
-    if (q.capacity >= n) return RR_OK;
-    for (int i = 0; i < 2; ++i) { cudaFree(q.ray_a[i]); cudaFree(q.ray_b[i]); cudaFree(q.ray_c[i]); }
-    cudaFree(q.hits); cudaFree(q.shadow_a); cudaFree(q.shadow_b); cudaFree(q.shadow_c);
-    q = rr_pt_queues();
-    const size_t bytes = n * sizeof(float4);
-    for (int i = 0; i < 2; ++i) {
-        RR_TRY_CUDA(ctx, cudaMalloc(&q.ray_a[i], bytes));
-        RR_TRY_CUDA(ctx, cudaMalloc(&q.ray_b[i], bytes));
-        RR_TRY_CUDA(ctx, cudaMalloc(&q.ray_c[i], bytes));
-    }
-    RR_TRY_CUDA(ctx, cudaMalloc(&q.hits, bytes));
-    RR_TRY_CUDA(ctx, cudaMalloc(&q.shadow_a, bytes));
-    RR_TRY_CUDA(ctx, cudaMalloc(&q.shadow_b, bytes));
-    RR_TRY_CUDA(ctx, cudaMalloc(&q.shadow_c, bytes));
-    q.capacity = n;
-    return RR_OK;
 }
 
 } // namespace

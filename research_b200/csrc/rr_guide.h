@@ -1,0 +1,85 @@
+// rr_guide.h — library-private state of a path-guiding guide (rr_guide).
+#pragma once
+
+#include "rr_internal.h"
+
+namespace rr {
+
+// Dense grid of vMF mixtures: cells = res^3 over [bmin, bmin + res/scale].
+struct GridView {
+    uint32_t res = 0;
+    uint32_t cells = 0;
+    float3 bmin{0, 0, 0};
+    float3 scale{0, 0, 0};       // cells per world unit, per axis
+    float4* lobes = nullptr;     // cells * 8: (mu.xyz, kappa)
+    float* weights = nullptr;    // cells * 8
+};
+
+__device__ __forceinline__ uint32_t grid_cell(const GridView& g, float3 p) {
+    const int r = int(g.res) - 1;
+    int cx = int(floorf((p.x - g.bmin.x) * g.scale.x));
+    int cy = int(floorf((p.y - g.bmin.y) * g.scale.y));
+    int cz = int(floorf((p.z - g.bmin.z) * g.scale.z));
+    cx = cx < 0 ? 0 : (cx > r ? r : cx);
+    cy = cy < 0 ? 0 : (cy > r ? r : cy);
+    cz = cz < 0 ? 0 : (cz > r ? r : cz);
+    return (uint32_t(cz) * g.res + uint32_t(cy)) * g.res + uint32_t(cx);
+}
+
+// Training samples: s0 = (pos, weight), s1 = (wi, vertex id), s2 = (normal),
+// s3 = (wo). count[0] = samples appended, count[1] = valid cells (grid).
+struct GuideSamples {
+    float4* s0 = nullptr;
+    float4* s1 = nullptr;
+    float4* s2 = nullptr;
+    float4* s3 = nullptr;
+    uint32_t* count = nullptr;
+    uint32_t capacity = 0;
+};
+
+} // namespace rr
+
+struct rr_mlp_state;
+
+struct rr_guide {
+    rr_ctx* ctx = nullptr;
+    rr_guide_desc desc{};
+    std::vector<void*> allocations;
+    rr::GuideSamples samples;
+    float4* rec[4] = {nullptr, nullptr, nullptr, nullptr};
+    size_t rec_capacity = 0;
+    uint32_t frame_paths = 0;
+    // grid
+    rr::GridView grid;
+    double* stats64 = nullptr;
+    uint32_t* cell_start = nullptr;
+    uint32_t* cell_end = nullptr;
+    unsigned long long* keys_in = nullptr;
+    unsigned long long* keys_out = nullptr;
+    uint32_t* vals_in = nullptr;
+    uint32_t* vals_out = nullptr;
+    void* sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
+    // MLP
+    rr_mlp_state* mlp = nullptr;
+    float4* mlp_surf = nullptr;   // per queue slot: (pos, 1), (normal, valid), (wo, 0)
+    float4* mlp_mix = nullptr;    // per queue slot: 8 lobes + 2 float4 of weights
+    size_t mlp_slots = 0;
+    uint64_t mlp_infer_launches = 0;
+    // statistics
+    rr_guide_stats stats{};
+    bool pending_stats = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    ~rr_guide();
+};
+
+// MLP guide (mlp_guide.cu)
+rr_status rr_mlp_guide_init(rr_ctx* ctx, rr_guide* g);
+rr_status rr_mlp_guide_reset(rr_ctx* ctx, rr_guide* g, cudaStream_t stream);
+rr_status rr_mlp_guide_ensure(rr_ctx* ctx, rr_guide* g, size_t slots);
+rr_status rr_mlp_guide_infer(rr_ctx* ctx, rr_guide* g, const uint32_t* count_dev, uint32_t max_count,
+                             cudaStream_t stream);
+rr_status rr_mlp_guide_train(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t stream);
+double rr_mlp_guide_last_loss(rr_guide* g);
+rr_status rr_mlp_guide_eval(rr_ctx* ctx, rr_guide* g, const float4* surf, float4* mix, const uint32_t* count_dev,
+                            uint32_t count, cudaStream_t stream);

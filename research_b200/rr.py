@@ -95,6 +95,22 @@ class GuidingParams(C.Structure):
                 ("_pad", C.c_uint32)]
 
 
+class GuideDesc(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("grid_resolution", C.c_uint32), ("alpha", C.c_float), ("decay", C.c_float),
+                ("bounds_min", C.c_float * 3), ("bounds_max", C.c_float * 3), ("max_samples", C.c_uint32),
+                ("mlp_batch", C.c_uint32), ("learning_rate", C.c_float), ("seed", C.c_uint32)]
+
+
+class GuideStats(C.Structure):
+    _fields_ = [("samples_recorded", C.c_uint64), ("samples_used", C.c_uint64), ("cells_valid", C.c_uint32),
+                ("updates", C.c_uint32), ("last_loss", C.c_double), ("ms_update", C.c_double)]
+
+
+GUIDE_GRID = 0
+GUIDE_MLP = 1
+MLP_PARAM_COUNT = 20784
+
+
 class ProceduralParams(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("target_triangles", C.c_uint32), ("emissive_triangles", C.c_uint32),
                 ("box_half", C.c_float), ("_pad", C.c_uint32)]
@@ -142,6 +158,15 @@ _SIGNATURES = {
     "rr_guiding_reset": (I, [P, P, P, C.POINTER(GuidingParams), P]),
     "rr_trace_closest": (I, [P, P, P, P, F32, F32, U32, P, P, P]),
     "rr_tonemap_execute": (I, [P, P, U32, U32, F32, P, P]),
+    "rr_guide_create": (I, [P, C.POINTER(GuideDesc), C.POINTER(P)]),
+    "rr_guide_destroy": (I, [P]),
+    "rr_guide_reset": (I, [P, P, P]),
+    "rr_guide_update": (I, [P, P, P]),
+    "rr_guide_get_stats": (I, [P, P, C.POINTER(GuideStats)]),
+    "rr_guide_eval": (I, [P, P, P, U32, P, P]),
+    "rr_guide_set_samples": (I, [P, P, P, U32, P]),
+    "rr_guide_mlp_params": (I, [P, P, P, P, P, U32, C.POINTER(I)]),
+    "rr_guided_pathtracer_execute": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtParams), P, P, P]),
     "rr_image_mse": (I, [P, P, P, U32, U32, U32, U32, U32, U32, P, P]),
     "rr_host_scene_cornell": (I, [I, C.POINTER(P)]),
     "rr_host_scene_procedural": (I, [C.POINTER(ProceduralParams), C.POINTER(P)]),

@@ -1,0 +1,216 @@
+"""GPU tests of the path guides (dense vMF grid with FP64 EM, tensor-core
+MLP) and of the guided path tracer."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _stream(torch):
+    return torch.cuda.current_stream().cuda_stream
+
+
+def make_guide(rr, ctx, kind, bmin=(-1, -1, -1), bmax=(1, 1, 1), max_samples=1 << 20, batch=1 << 18, res=16,
+               lr=1e-2, decay=0.8, alpha=0.5):
+    d = rr.GuideDesc(kind, res, alpha, decay, (C.c_float * 3)(*bmin), (C.c_float * 3)(*bmax), max_samples, batch,
+                     lr, 7)
+    h = C.c_void_p()
+    ctx.check(rr.lib().rr_guide_create(ctx.handle, C.byref(d), C.byref(h)))
+    return h
+
+
+def set_samples(rr, ctx, torch, guide, pos, om, w, n_, wo):
+    N = len(pos)
+    s = np.zeros((N, 16), np.float32)
+    s[:, 0:3] = pos; s[:, 3] = w
+    s[:, 4:7] = om; s[:, 7] = np.arange(N, dtype=np.uint32).view(np.float32)
+    s[:, 8:11] = n_
+    s[:, 12:15] = wo
+    t = torch.from_numpy(s).cuda()
+    ctx.check(rr.lib().rr_guide_set_samples(ctx.handle, guide, t.data_ptr(), N, _stream(torch)))
+    torch.cuda.synchronize()
+    return t
+
+
+def unit(v):
+    return v / np.linalg.norm(v, axis=-1, keepdims=True)
+
+
+def eval_guide(rr, ctx, torch, guide, pos, n_, wo):
+    N = len(pos)
+    surf = np.zeros((N, 3, 4), np.float32)
+    surf[:, 0, :3] = pos; surf[:, 0, 3] = 1
+    surf[:, 1, :3] = n_; surf[:, 1, 3] = 1
+    surf[:, 2, :3] = wo
+    ts = torch.from_numpy(surf).cuda()
+    mix = torch.zeros((N, 10, 4), device="cuda")
+    ctx.check(rr.lib().rr_guide_eval(ctx.handle, guide, ts.data_ptr(), N, mix.data_ptr(), _stream(torch)))
+    torch.cuda.synchronize()
+    m = mix.cpu().numpy()
+    return m[:, :8, :3], m[:, :8, 3], m[:, 8:, :].reshape(N, 8)
+
+
+def test_mlp_forward_matches_fp64(rr, ctx, torch_cuda):
+    import mlp_ref
+    torch = torch_cuda
+    g = make_guide(rr, ctx, rr.GUIDE_MLP)
+    rng = np.random.default_rng(3)
+    params = (rng.normal(size=mlp_ref.PARAM_COUNT) * 0.15).astype(np.float32)
+    flag = C.c_int()
+    ctx.check(rr.lib().rr_guide_mlp_params(ctx.handle, g, None, None, params.ctypes.data, rr.MLP_PARAM_COUNT,
+                                           C.byref(flag)))
+    N = 1000
+    pos = rng.uniform(-1, 1, (N, 3)).astype(np.float32)
+    nrm = unit(rng.normal(size=(N, 3))).astype(np.float32)
+    wo = unit(rng.normal(size=(N, 3))).astype(np.float32)
+    mu, kappa, pi = eval_guide(rr, ctx, torch, g, pos, nrm, wo)
+    # reference on the BF16-rounded weights the tensor cores see
+    p16 = torch.from_numpy(params).bfloat16().float().numpy().astype(np.float64)
+    k = 0
+    for i, o in mlp_ref.LAYERS:   # biases stay FP32
+        p16[k + o * i:k + o * i + o] = params[k + o * i:k + o * i + o]
+        k += o * i + o
+    F = mlp_ref.encode(pos.astype(np.float64), nrm, wo, np.array([-1.0] * 3), np.array([1.0] * 3))
+    raw, _ = mlp_ref.forward(p16, F)
+    rmu, rk, rpi, _ = mlp_ref.mixture(raw)
+    assert np.abs(pi - rpi).max() < 0.03
+    assert np.abs(np.einsum("bjk,bjk->bj", mu, rmu)).min() > 0.97
+    assert np.abs(kappa - rk).max() / rk.max() < 0.05
+    ctx.check(rr.lib().rr_guide_mlp_params(ctx.handle, g, None, None, None, rr.MLP_PARAM_COUNT, C.byref(flag)))
+    assert flag.value == 0
+    rr.lib().rr_guide_destroy(g)
+
+
+def _direction_samples(rng, N, axis):
+    pos = rng.uniform(-1, 1, (N, 3)).astype(np.float32)
+    om = unit(axis + 0.35 * rng.normal(size=(N, 3))).astype(np.float32)
+    nrm = np.tile(np.array([0, 1, 0], np.float32), (N, 1))
+    wo = unit(rng.normal(size=(N, 3)) + np.array([0, 2, 0])).astype(np.float32)
+    w = rng.uniform(0.1, 2.0, N).astype(np.float32)
+    return pos, om, nrm, wo, w
+
+
+def test_mlp_gradient_matches_fp64(rr, ctx, torch_cuda):
+    import mlp_ref
+    torch = torch_cuda
+    rng = np.random.default_rng(5)
+    N = 2000
+    g = make_guide(rr, ctx, rr.GUIDE_MLP, batch=N, max_samples=N)
+    params = (rng.normal(size=mlp_ref.PARAM_COUNT) * 0.1).astype(np.float32)
+    ctx.check(rr.lib().rr_guide_mlp_params(ctx.handle, g, None, None, params.ctypes.data, rr.MLP_PARAM_COUNT, None))
+    pos, om, nrm, wo, w = _direction_samples(rng, N, np.array([0.3, 1.0, 0.2]))
+    keep = set_samples(rr, ctx, torch, g, pos, om, w, nrm, wo)
+    ctx.check(rr.lib().rr_guide_update(ctx.handle, g, _stream(torch)))
+    grad = np.zeros(mlp_ref.PARAM_COUNT, np.float32)
+    flag = C.c_int()
+    ctx.check(rr.lib().rr_guide_mlp_params(ctx.handle, g, None, grad.ctypes.data, None, rr.MLP_PARAM_COUNT,
+                                           C.byref(flag)))
+    assert flag.value == 0
+    p16 = torch.from_numpy(params).bfloat16().float().numpy().astype(np.float64)
+    k = 0
+    for i, o in mlp_ref.LAYERS:
+        p16[k + o * i:k + o * i + o] = params[k + o * i:k + o * i + o]
+        k += o * i + o
+    F = mlp_ref.encode(pos.astype(np.float64), nrm, wo, np.array([-1.0] * 3), np.array([1.0] * 3))
+    loss, ref = mlp_ref.loss_and_grad(p16, F, om.astype(np.float64), w.astype(np.float64))
+    cos = float(grad @ ref / (np.linalg.norm(grad) * np.linalg.norm(ref)))
+    rel = float(np.linalg.norm(grad - ref) / np.linalg.norm(ref))
+    assert cos > 0.99, (cos, rel)
+    assert rel < 0.1, (cos, rel)
+    st = rr.GuideStats()
+    ctx.check(rr.lib().rr_guide_get_stats(ctx.handle, g, C.byref(st)))
+    assert st.last_loss == pytest.approx(loss, rel=0.05)
+    del keep
+    rr.lib().rr_guide_destroy(g)
+
+
+def test_mlp_training_lowers_loss(rr, ctx, torch_cuda):
+    torch = torch_cuda
+    rng = np.random.default_rng(6)
+    N = 1 << 16
+    g = make_guide(rr, ctx, rr.GUIDE_MLP, batch=1 << 14, max_samples=N, lr=5e-3)
+    pos, om, nrm, wo, w = _direction_samples(rng, N, np.array([0.0, 1.0, 0.0]))
+    # direction depends on position: two half-spaces, two lobes
+    om[pos[:, 0] > 0] = unit(np.array([1.0, 0.3, 0.0]) + 0.2 * rng.normal(size=((pos[:, 0] > 0).sum(), 3)))
+    keep = set_samples(rr, ctx, torch, g, pos, om, w, nrm, wo)
+    losses = []
+    for it in range(60):
+        ctx.check(rr.lib().rr_guide_update(ctx.handle, g, _stream(torch)))
+        st = rr.GuideStats()
+        ctx.check(rr.lib().rr_guide_get_stats(ctx.handle, g, C.byref(st)))
+        losses.append(st.last_loss)
+    assert losses[-1] < losses[0] - 1.0, losses[::10]
+    # the learned mixture points where the data points
+    mu, kappa, pi = eval_guide(rr, ctx, torch, g, np.array([[0.5, 0, 0], [-0.5, 0, 0]], np.float32),
+                               np.array([[0, 1, 0]] * 2, np.float32), np.array([[0, 1, 0]] * 2, np.float32))
+    mean_dir = [unit((pi[i][:, None] * mu[i]).sum(0)) for i in range(2)]
+    assert mean_dir[0] @ unit(np.array([1.0, 0.3, 0.0])) > 0.8
+    assert mean_dir[1] @ np.array([0.0, 1.0, 0.0]) > 0.8
+    del keep
+    rr.lib().rr_guide_destroy(g)
+
+
+def test_grid_em_fits_and_is_deterministic(rr, ctx, torch_cuda):
+    torch = torch_cuda
+    rng = np.random.default_rng(8)
+    N = 1 << 16
+    pos, om, nrm, wo, w = _direction_samples(rng, N, np.array([0.0, 0.0, 1.0]))
+    out = []
+    for rep in range(2):
+        g = make_guide(rr, ctx, rr.GUIDE_GRID, res=4)
+        keep = set_samples(rr, ctx, torch, g, pos, om, w, nrm, wo)
+        for it in range(3):
+            ctx.check(rr.lib().rr_guide_update(ctx.handle, g, _stream(torch)))
+        st = rr.GuideStats()
+        ctx.check(rr.lib().rr_guide_get_stats(ctx.handle, g, C.byref(st)))
+        assert st.cells_valid == 64
+        mu, kappa, pi = eval_guide(rr, ctx, torch, g, pos[:200], nrm[:200], wo[:200])
+        out.append((mu, kappa, pi))
+        del keep
+        rr.lib().rr_guide_destroy(g)
+    for a, b in zip(out[0], out[1]):
+        np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+    mu, kappa, pi = out[0]
+    mean_dir = unit((pi[:, :, None] * mu).sum(1))
+    assert (mean_dir @ np.array([0, 0, 1.0])).min() > 0.9
+
+
+def _render(rr, ctx, torch, scene, cam, frames, guide=None, train=True, spp=1, bounces=5):
+    W, H = cam.screen_width, cam.screen_height
+    acc = np.zeros((H, W, 3))
+    rad = torch.empty((spp, H, W, 4), device="cuda")
+    for f in range(frames):
+        p = rr.PtParams(1000 + f * spp, bounces, spp, 0)
+        if guide is None:
+            ctx.check(rr.lib().rr_pathtracer_execute(ctx.handle, scene.handle, C.byref(cam), C.byref(p),
+                                                     rad.data_ptr(), _stream(torch)))
+        else:
+            ctx.check(rr.lib().rr_guided_pathtracer_execute(ctx.handle, scene.handle, C.byref(cam), C.byref(p),
+                                                            guide, rad.data_ptr(), _stream(torch)))
+            if train:
+                ctx.check(rr.lib().rr_guide_update(ctx.handle, guide, _stream(torch)))
+        acc += rad[..., :3].mean(0).cpu().numpy()
+    return acc / frames
+
+
+@pytest.mark.parametrize("kind", ["grid", "mlp"])
+def test_guided_pathtracer_is_unbiased(rr, ctx, torch_cuda, kind):
+    torch = torch_cuda
+    hs = rr.HostScene.cornell(1)
+    scene = rr.Scene(ctx, hs.arrays)
+    cam = rr.camera_data(rr.camera_desc(64, 64))
+    g = make_guide(rr, ctx, rr.GUIDE_GRID if kind == "grid" else rr.GUIDE_MLP, bmin=(-1.01,) * 3,
+                   bmax=(1.01,) * 3, res=16, batch=1 << 14, max_samples=1 << 18)
+    _render(rr, ctx, torch, scene, cam, 16, guide=g, train=True, spp=4)          # learn
+    guided = _render(rr, ctx, torch, scene, cam, 64, guide=g, train=False, spp=4)
+    plain = _render(rr, ctx, torch, scene, cam, 64, spp=4)
+    st = rr.GuideStats()
+    ctx.check(rr.lib().rr_guide_get_stats(ctx.handle, g, C.byref(st)))
+    assert st.samples_recorded > 1000
+    # image means agree (MIS keeps the estimator unbiased for any guide)
+    mg, mp = guided.mean(), plain.mean()
+    assert abs(mg - mp) / mp < 0.03, (mg, mp)
+    rr.lib().rr_guide_destroy(g)
+    scene.close()

@@ -141,3 +141,27 @@ def test_accumulate_running_mean(O):
     for k in range(5):
         O.accumulate(np.ascontiguousarray(frames[k]), acc, 1 if k == 0 else 0, k)
     np.testing.assert_allclose(acc, frames.mean(0), rtol=1e-5)
+
+
+def test_mlp_reference_gradient_finite_differences():
+    """The FP64 reference gradient of the learned guide's loss agrees with
+    central finite differences (it is the checker of the GPU backward pass)."""
+    import mlp_ref
+    rng = np.random.default_rng(0)
+    params = rng.normal(size=mlp_ref.PARAM_COUNT) * 0.2
+    N = 16
+    pos = rng.uniform(-1, 1, (N, 3))
+    nrm = rng.normal(size=(N, 3)); nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    wo = rng.normal(size=(N, 3)); wo /= np.linalg.norm(wo, axis=1, keepdims=True)
+    om = rng.normal(size=(N, 3)); om /= np.linalg.norm(om, axis=1, keepdims=True)
+    w = rng.uniform(0.1, 1.0, N)
+    F = mlp_ref.encode(pos, nrm, wo, np.array([-1.0] * 3), np.array([1.0] * 3))
+    loss, g = mlp_ref.loss_and_grad(params, F, om, w)
+    idx = rng.choice(mlp_ref.PARAM_COUNT, 40, replace=False)
+    idx = np.concatenate([idx, [mlp_ref.PARAM_COUNT - 1, mlp_ref.PARAM_COUNT - 60]])
+    for i in idx:
+        h = 1e-6
+        p1 = params.copy(); p1[i] += h
+        p2 = params.copy(); p2[i] -= h
+        fd = (mlp_ref.loss_and_grad(p1, F, om, w)[0] - mlp_ref.loss_and_grad(p2, F, om, w)[0]) / (2 * h)
+        assert g[i] / mlp_ref.LOSS_SCALE == pytest.approx(fd, rel=1e-4, abs=1e-7)
