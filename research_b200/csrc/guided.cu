@@ -190,23 +190,29 @@ __global__ void __launch_bounds__(kBlock) guided_shade_kernel(DevScene s, Guided
                         const float u_sel = rand_float(seed);
                         const float u0 = rand_float(seed);
                         const float u1 = rand_float(seed);
+                        bool rejected = false;
                         if (u_sel < alpha) {
                             const float u2 = rand_float(seed);
                             wi = mixture_sample(mix, G.lobes, u0, u1, u2);
                         } else {
+                            // brdf_sample rejects a VNDF direction below the
+                            // surface by returning f = 0 (and wi = +y): the
+                            // sample carries nothing, so the path ends here.
                             float pdf_b;
-                            brdf_sample(wo, n, base_c, metallic, roughness, u0, u1, wi, pdf_b);
+                            const float3 fb = brdf_sample(wo, n, base_c, metallic, roughness, u0, u1, wi, pdf_b);
+                            rejected = fb.x == 0.0f && fb.y == 0.0f && fb.z == 0.0f;
                         }
                         const float cos_i = dot(n, wi);
-                        float pdf = 0.0f;
-                        if (cos_i > 0.0f) {
-                            const float pb = brdf_sample_pdf(wo, n, base_c, metallic, roughness, wi);
+                        float pdf = 0.0f, ratio = 0.0f;
+                        if (cos_i > 0.0f && !rejected) {
+                            const BrdfPdfs pb = brdf_sample_pdfs(wo, n, base_c, metallic, roughness, wi);
                             const float pg = valid ? mixture_pdf(mix, G.lobes, wi) : 0.0f;
-                            pdf = alpha * pg + (1.0f - alpha) * pb;
+                            pdf = alpha * pg + (1.0f - alpha) * pb.actual;
+                            ratio = pb.actual / pb.ref;
                         }
                         if (pdf > 1e-6f) {
                             const float3 f = brdf_eval(n, wo, wi, base_c, metallic, roughness);
-                            thp = thp * ((f * cos_i) / pdf);
+                            thp = thp * ((f * cos_i) * (ratio / pdf));
                             bool alive = true;
                             if (G.bounce >= 3) {
                                 const float survive = mn(mx(thp.x, mx(thp.y, thp.z)), 0.95f);

@@ -32,10 +32,25 @@ RR_D float vmf_pdf(float3 mu, float kappa, float3 dir) {
     return k * rr_expf(k * (w - 1.0f)) / mx(denom, 1.0e-8f);
 }
 
-// Density of brdf_sample's direction at an arbitrary wi: the p_spec-weighted
-// mixture of the GGX-VNDF and cosine lobes evaluated exactly as
-// BRDF.slang:229-283 evaluates it for the sampled direction.
-RR_D float brdf_sample_pdf(float3 wo, float3 n, float3 base, float metallic, float roughness, float3 wi) {
+// Two densities of brdf_sample's direction at an arbitrary wi (cos > 0):
+//  ref    — the value brdf_sample returns as its pdf (BRDF.slang:229-283): the
+//           p_spec-weighted mixture of D*NdotH/(4 VdotH) and the cosine lobe,
+//           clamped at 1e-6 exactly as the reference clamps it;
+//  actual — the density brdf_sample really draws from: its specular branch
+//           samples the GGX distribution of visible normals, whose reflected
+//           density is G1(wo) D(h) / (4 wo.z) (Heitz 2018, "Sampling the GGX
+//           Distribution of Visible Normals", eq. 17 with the GGX Smith G1),
+//           written as D / (2 (wo.z + sqrt(a^2 (wo.x^2 + wo.y^2) + wo.z^2)))
+//           so that it stays finite at grazing wo.
+// The reference tracer weights a bounce by f cos / ref, whose expectation is
+// the integral of f cos actual/ref; a guided estimator that samples from
+// another density reproduces that expectation with f cos (actual/ref) / p_mix.
+struct BrdfPdfs {
+    float ref;
+    float actual;
+};
+
+RR_D BrdfPdfs brdf_sample_pdfs(float3 wo, float3 n, float3 base, float metallic, float roughness, float3 wi) {
     const float r = clampf(roughness, 0.04f, 1.0f);
     const float3 F0 = lerp(f3(0.04f, 0.04f, 0.04f), base, metallic);
     const float3 kS = fresnel_schlick(mx(dot(n, wo), 0.0f), F0);
@@ -48,9 +63,17 @@ RR_D float brdf_sample_pdf(float3 wo, float3 n, float3 base, float metallic, flo
     const float3 h = normalize(wo_l + wi_l);
     const float NdotH = mx(h.z, 1e-6f);
     const float VdotH = mx(dot(wo_l, h), 1e-6f);
-    const float D = distribution_ggx(NdotH, r * r);
-    const float pdf_spec = D * NdotH / mx(4.0f * VdotH, 1e-6f);
-    return p_spec * pdf_spec + (1.0f - p_spec) * (NdotWI * kInvPi);
+    const float a = r * r;
+    const float D = distribution_ggx(NdotH, a);
+    const float pdf_diff = NdotWI * kInvPi;
+    const float pdf_spec_ref = D * NdotH / mx(4.0f * VdotH, 1e-6f);
+    const float vz = mx(wo_l.z, 0.0f);
+    const float lam = sqrtf(a * a * (wo_l.x * wo_l.x + wo_l.y * wo_l.y) + vz * vz);
+    const float pdf_spec_vndf = D / mx(2.0f * (vz + lam), 1e-12f);
+    BrdfPdfs p;
+    p.ref = mx(p_spec * pdf_spec_ref + (1.0f - p_spec) * pdf_diff, 1e-6f);
+    p.actual = p_spec * pdf_spec_vndf + (1.0f - p_spec) * pdf_diff;
+    return p;
 }
 
 constexpr int kMaxLobes = 8;
