@@ -12,9 +12,10 @@
 //
 // Grid guide: grid_resolution^3 cells over the guide bounds, 8 vMF lobes per
 // cell. rr_guide_update sorts the samples by (cell, vertex id) and runs one
-// stepwise-EM iteration per cell in a fixed sample order, accumulating the
-// sufficient statistics (sum w*gamma, sum w*gamma*omega) in FP64 with
-// exponential forgetting, then refits weights, mean directions and
+// EM iteration per cell: responsibilities under the cell's current mixture,
+// sufficient statistics (sum w*gamma, sum w*gamma*omega) summed in FP64 in a
+// fixed order (chunks of a cell's samples, one warp each, then the chunks in
+// order) with exponential forgetting, then refits weights, mean directions and
 // concentrations (Banerjee's closed form, as GuidingGrid.slang:124-131).
 
 #include "rr_wavefront.cuh"
@@ -22,6 +23,7 @@
 #include "rr_guide.h"
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <chrono>
 #include <cstring>
@@ -304,44 +306,73 @@ __global__ void __launch_bounds__(256) grid_ranges_kernel(const unsigned long lo
     if (i + 1 == n || uint32_t(keys[i + 1] >> 32) != c) end[c] = i + 1;
 }
 
-// One stepwise-EM iteration per cell over its samples in sorted order.
-__global__ void __launch_bounds__(128) grid_em_kernel(GridView g, GuideSamples S, const uint32_t* __restrict__ order,
-                                                      const uint32_t* __restrict__ start,
-                                                      const uint32_t* __restrict__ end, double* __restrict__ stats,
-                                                      float4* lobes, float* weights, float decay,
-                                                      uint32_t* valid_cells) {
-    const uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x;
-    if (cell >= g.cells) return;
-    const uint32_t b = start[cell], e = end[cell];
-    if (e <= b) {  // no new samples: the mixture is kept as it is
-        float w = 0.0f;
-        for (int j = 0; j < kMaxLobes; ++j) w += weights[size_t(cell) * kMaxLobes + j];
-        if (w > 0.0f) atomicAdd(valid_cells, 1u);
-        return;
-    }
-    VmfMixture m;
+// The EM update is one batch E-step per frame: every sample's responsibilities
+// are taken under the mixture its cell held at the start of the update, so a
+// cell's new sufficient statistics are a plain FP64 sum over its samples.
+// That sum runs in parallel and in a fixed order: each cell's sorted sample
+// range is cut into chunks of kEmChunk samples, one warp sums a chunk (lane l
+// takes samples l, l+32, ... and the warp reduces with a fixed xor butterfly,
+// lane 0's result being kept), and the per-cell M-step adds its chunks in
+// chunk order. Run to run the fitted guide is bit-identical.
+constexpr uint32_t kEmChunk = 1024;
+constexpr int kEmStats = kMaxLobes * 4;   // (s0, s1.xyz) per lobe
+
+// The mixture a cell enters the update with: its fitted lobes, or, for a cell
+// never fitted, 8 lobes of kappa 2 on the cube diagonals with equal weights.
+RR_D void cell_mixture(const float4* __restrict__ lobes, const float* __restrict__ weights, uint32_t cell,
+                       VmfMixture& m) {
     float wsum = 0.0f;
     for (int j = 0; j < kMaxLobes; ++j) {
         m.lobe[j] = lobes[size_t(cell) * kMaxLobes + j];
         m.weight[j] = weights[size_t(cell) * kMaxLobes + j];
         wsum += m.weight[j];
     }
-    if (!(wsum > 0.0f)) {  // unfitted cell: 8 lobes on the cube diagonals
+    if (!(wsum > 0.0f)) {
         for (int j = 0; j < kMaxLobes; ++j) {
             const float k = 0.57735026918962576f;
             m.lobe[j] = make_float4((j & 1) ? k : -k, (j & 2) ? k : -k, (j & 4) ? k : -k, 2.0f);
             m.weight[j] = 1.0f / kMaxLobes;
         }
     }
+}
+
+__global__ void __launch_bounds__(256) grid_chunk_count_kernel(const uint32_t* __restrict__ start,
+                                                               const uint32_t* __restrict__ end, uint32_t cells,
+                                                               uint32_t* __restrict__ cnt) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < cells) cnt[c] = (end[c] - start[c] + kEmChunk - 1) / kEmChunk;
+}
+
+__global__ void __launch_bounds__(256) grid_chunk_map_kernel(const uint32_t* __restrict__ cnt,
+                                                             const uint32_t* __restrict__ off, uint32_t cells,
+                                                             uint32_t* __restrict__ chunk_cell) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cells) return;
+    for (uint32_t q = 0; q < cnt[c]; ++q) chunk_cell[off[c] + q] = c;
+}
+
+// One warp per chunk; launched with an upper bound of warps, the ones past
+// the scanned chunk total return at once.
+__global__ void __launch_bounds__(128) grid_chunk_kernel(GridView g, GuideSamples S,
+                                                         const uint32_t* __restrict__ order,
+                                                         const uint32_t* __restrict__ start,
+                                                         const uint32_t* __restrict__ end,
+                                                         const uint32_t* __restrict__ cnt,
+                                                         const uint32_t* __restrict__ off,
+                                                         const uint32_t* __restrict__ chunk_cell,
+                                                         double* __restrict__ partial) {
+    const uint32_t chunk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t total = off[g.cells - 1] + cnt[g.cells - 1];
+    if (chunk >= total) return;   // whole warps
+    const uint32_t cell = chunk_cell[chunk];
+    const uint32_t b = start[cell] + (chunk - off[cell]) * kEmChunk;
+    const uint32_t e = min(end[cell], b + kEmChunk);
+    VmfMixture m;
+    cell_mixture(g.lobes, g.weights, cell, m);
     double s0[kMaxLobes], s1x[kMaxLobes], s1y[kMaxLobes], s1z[kMaxLobes];
-    double* st = stats + size_t(cell) * kMaxLobes * 4;
-    for (int j = 0; j < kMaxLobes; ++j) {
-        s0[j] = double(decay) * st[j * 4 + 0];
-        s1x[j] = double(decay) * st[j * 4 + 1];
-        s1y[j] = double(decay) * st[j * 4 + 2];
-        s1z[j] = double(decay) * st[j * 4 + 3];
-    }
-    for (uint32_t k = b; k < e; ++k) {
+    for (int j = 0; j < kMaxLobes; ++j) s0[j] = s1x[j] = s1y[j] = s1z[j] = 0.0;
+    for (uint32_t k = b + lane; k < e; k += 32) {
         const uint32_t si = order[k];
         const float4 a = S.s0[si];
         const float4 d = S.s1[si];
@@ -360,6 +391,54 @@ __global__ void __launch_bounds__(128) grid_em_kernel(GridView g, GuideSamples S
             s1x[j] += r * double(om.x);
             s1y[j] += r * double(om.y);
             s1z[j] += r * double(om.z);
+        }
+    }
+    for (int j = 0; j < kMaxLobes; ++j) {
+        for (int o = 16; o > 0; o >>= 1) {
+            s0[j] += __shfl_xor_sync(0xffffffffu, s0[j], o);
+            s1x[j] += __shfl_xor_sync(0xffffffffu, s1x[j], o);
+            s1y[j] += __shfl_xor_sync(0xffffffffu, s1y[j], o);
+            s1z[j] += __shfl_xor_sync(0xffffffffu, s1z[j], o);
+        }
+    }
+    if (lane == 0) {
+        double* out = partial + size_t(chunk) * kEmStats;
+        for (int j = 0; j < kMaxLobes; ++j) {
+            out[j * 4 + 0] = s0[j]; out[j * 4 + 1] = s1x[j]; out[j * 4 + 2] = s1y[j]; out[j * 4 + 3] = s1z[j];
+        }
+    }
+}
+
+// Per cell: decayed statistics + the cell's chunk sums in chunk order, then
+// the M-step (Banerjee kappa, lobe weights = normalised s0).
+__global__ void __launch_bounds__(128) grid_em_kernel(GridView g, const uint32_t* __restrict__ cnt,
+                                                      const uint32_t* __restrict__ off,
+                                                      const double* __restrict__ partial, double* __restrict__ stats,
+                                                      float4* lobes, float* weights, float decay,
+                                                      uint32_t* valid_cells) {
+    const uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= g.cells) return;
+    const uint32_t nq = cnt[cell];
+    if (nq == 0) {  // no new samples: the mixture is kept as it is
+        float w = 0.0f;
+        for (int j = 0; j < kMaxLobes; ++j) w += weights[size_t(cell) * kMaxLobes + j];
+        if (w > 0.0f) atomicAdd(valid_cells, 1u);
+        return;
+    }
+    VmfMixture m;
+    cell_mixture(lobes, weights, cell, m);
+    double s0[kMaxLobes], s1x[kMaxLobes], s1y[kMaxLobes], s1z[kMaxLobes];
+    double* st = stats + size_t(cell) * kEmStats;
+    for (int j = 0; j < kMaxLobes; ++j) {
+        s0[j] = double(decay) * st[j * 4 + 0];
+        s1x[j] = double(decay) * st[j * 4 + 1];
+        s1y[j] = double(decay) * st[j * 4 + 2];
+        s1z[j] = double(decay) * st[j * 4 + 3];
+    }
+    for (uint32_t q = 0; q < nq; ++q) {
+        const double* p = partial + size_t(off[cell] + q) * kEmStats;
+        for (int j = 0; j < kMaxLobes; ++j) {
+            s0[j] += p[j * 4 + 0]; s1x[j] += p[j * 4 + 1]; s1y[j] += p[j * 4 + 2]; s1z[j] += p[j * 4 + 3];
         }
     }
     double tot = 0.0;
@@ -455,11 +534,25 @@ extern "C" rr_status rr_guide_create(rr_ctx* ctx, const rr_guide_desc* d, rr_gui
         g->vals_in = static_cast<uint32_t*>(p);
         if ((st = guide_alloc(ctx, g, &p, size_t(cap) * 4)) != RR_OK) return fail(st);
         g->vals_out = static_cast<uint32_t*>(p);
-        size_t tmp = 0;
+        // EM chunks: at most one partial chunk per non-empty cell plus cap / kEmChunk full ones
+        g->chunk_capacity = cells + cap / kEmChunk + 1;
+        if ((st = guide_alloc(ctx, g, &p, cells * sizeof(uint32_t))) != RR_OK) return fail(st);
+        g->chunk_cnt = static_cast<uint32_t*>(p);
+        if ((st = guide_alloc(ctx, g, &p, cells * sizeof(uint32_t))) != RR_OK) return fail(st);
+        g->chunk_off = static_cast<uint32_t*>(p);
+        if ((st = guide_alloc(ctx, g, &p, g->chunk_capacity * sizeof(uint32_t))) != RR_OK) return fail(st);
+        g->chunk_cell = static_cast<uint32_t*>(p);
+        if ((st = guide_alloc(ctx, g, &p, g->chunk_capacity * kEmStats * sizeof(double))) != RR_OK) return fail(st);
+        g->chunk_partial = static_cast<double*>(p);
+        size_t tmp = 0, scan_tmp = 0;
         cub::DeviceRadixSort::SortPairs(nullptr, tmp, g->keys_in, g->keys_out, g->vals_in, g->vals_out, int(cap), 0, 64);
+        cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp, g->chunk_cnt, g->chunk_off, int(cells));
+        tmp = std::max(tmp, scan_tmp);
         if ((st = guide_alloc(ctx, g, &p, tmp)) != RR_OK) return fail(st);
         g->sort_tmp = p;
         g->sort_tmp_bytes = tmp;
+        g->key_bits = 32;
+        while ((size_t(1) << (g->key_bits - 32)) < cells) ++g->key_bits;
     } else {
         if ((st = rr_mlp_guide_init(ctx, g)) != RR_OK) return fail(st);
     }
@@ -621,15 +714,30 @@ extern "C" rr_status rr_guide_update(rr_ctx* ctx, rr_guide* g, void* stream_v) {
             RR_CHECK_LAUNCH(ctx);
             size_t tmp = g->sort_tmp_bytes;
             RR_TRY_CUDA(ctx, cub::DeviceRadixSort::SortPairs(g->sort_tmp, tmp, g->keys_in, g->keys_out, g->vals_in,
-                                                             g->vals_out, int(n), 0, 64, stream));
+                                                             g->vals_out, int(n), 0, g->key_bits, stream));
             grid_ranges_kernel<<<(n + 255) / 256, 256, 0, stream>>>(g->keys_out, n, g->cell_start, g->cell_end);
             RR_CHECK_LAUNCH(ctx);
         }
-        grid_em_kernel<<<(v.cells + 127) / 128, 128, 0, stream>>>(v, g->samples, g->vals_out, g->cell_start,
-                                                                   g->cell_end, g->stats64, v.lobes, v.weights,
-                                                                   g->desc.decay, g->samples.count + 1);
+        const uint32_t cb = (v.cells + 255) / 256;
+        grid_chunk_count_kernel<<<cb, 256, 0, stream>>>(g->cell_start, g->cell_end, v.cells, g->chunk_cnt);
         RR_CHECK_LAUNCH(ctx);
-        ctx->launches += 4;
+        size_t tmp = g->sort_tmp_bytes;
+        RR_TRY_CUDA(ctx, cub::DeviceScan::ExclusiveSum(g->sort_tmp, tmp, g->chunk_cnt, g->chunk_off, int(v.cells),
+                                                       stream));
+        grid_chunk_map_kernel<<<cb, 256, 0, stream>>>(g->chunk_cnt, g->chunk_off, v.cells, g->chunk_cell);
+        RR_CHECK_LAUNCH(ctx);
+        if (n > 0) {
+            const size_t warps = std::min<size_t>(v.cells, n) + n / kEmChunk + 1;
+            grid_chunk_kernel<<<unsigned((warps * 32 + 127) / 128), 128, 0, stream>>>(
+                v, g->samples, g->vals_out, g->cell_start, g->cell_end, g->chunk_cnt, g->chunk_off, g->chunk_cell,
+                g->chunk_partial);
+            RR_CHECK_LAUNCH(ctx);
+        }
+        grid_em_kernel<<<(v.cells + 127) / 128, 128, 0, stream>>>(v, g->chunk_cnt, g->chunk_off, g->chunk_partial,
+                                                                   g->stats64, v.lobes, v.weights, g->desc.decay,
+                                                                   g->samples.count + 1);
+        RR_CHECK_LAUNCH(ctx);
+        ctx->launches += 8;
     } else {
         rr_status st = rr_mlp_guide_train(ctx, g, n, stream);
         if (st != RR_OK) return st;

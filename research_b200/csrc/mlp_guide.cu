@@ -19,8 +19,10 @@
 //    N=64, K=out), dZ_{l-1} = dX_l * [X_l > 0].
 //  - mlp_wgrad_kernel / mlp_reduce_kernel: dW_l = dZ_l^T X_l, db_l = sum dZ_l
 //    on the CUDA cores in FP32, per-block partials reduced in a fixed order.
-//  - mlp_adam_kernel: Adam on FP32 master weights (gradients carry a static
-//    loss scale), refreshing the BF16 copy used by the tensor cores.
+//  - mlp_adam_kernel: Adam on FP32 master weights and biases (gradients carry
+//    a static loss scale), refreshing the BF16 copy used by the tensor cores;
+//    the forward kernel adds the biases inside the MMA (a constant-1 input
+//    column against a BF16 bias column of the weight tile).
 
 #include "rr_guide.h"
 #include "rr_vmf.cuh"
@@ -36,31 +38,47 @@ constexpr int kIn = 80, kHid = 64, kOut = 48, kLayers = 5, kTile = 128;
 constexpr float kLossScale = 1024.0f;
 __host__ __device__ constexpr int lin(int l) { return l == 0 ? kIn : kHid; }
 __host__ __device__ constexpr int lout(int l) { return l == kLayers - 1 ? kOut : kHid; }
+// Offsets are closed forms (not recursions), so they also fold or stay cheap
+// where the layer index is only known at run time.
 // FP32 master parameters: for each layer W[out][in] then b[out].
 __host__ __device__ constexpr int woff(int l) {
-    return l == 0 ? 0 : woff(l - 1) + lout(l - 1) * lin(l - 1) + lout(l - 1);
+    return l == 0 ? 0
+                  : (kHid * kIn + kHid) + (l - 1) * (kHid * kHid + kHid) -
+                        (l == kLayers ? kHid * kHid + kHid - (kOut * kHid + kOut) : 0);
 }
 __host__ __device__ constexpr int boff(int l) { return woff(l) + lout(l) * lin(l); }
 constexpr int kParams = woff(kLayers);
 // BF16 weights: W[out][in] per layer, contiguous.
-__host__ __device__ constexpr int hoff(int l) { return l == 0 ? 0 : hoff(l - 1) + lout(l - 1) * lin(l - 1); }
+__host__ __device__ constexpr int hoff(int l) {
+    return l == 0 ? 0 : kHid * kIn + (l - 1) * kHid * kHid - (l == kLayers ? kHid * kHid - kOut * kHid : 0);
+}
 constexpr int kWeightsBf16 = hoff(kLayers);
 // activation / gradient columns per layer input (X_l) and output (dZ_l)
-__host__ __device__ constexpr int xoff(int l) { return l == 0 ? 0 : xoff(l - 1) + lin(l - 1); }
+__host__ __device__ constexpr int xoff(int l) { return l == 0 ? 0 : kIn + (l - 1) * kHid; }
 constexpr int kXCols = xoff(kLayers);            // 80 + 4*64 = 336
-__host__ __device__ constexpr int zoff(int l) { return l == 0 ? 0 : zoff(l - 1) + lout(l - 1); }
+__host__ __device__ constexpr int zoff(int l) { return l * kHid - (l == kLayers ? kHid - kOut : 0); }
 constexpr int kZCols = zoff(kLayers);            // 4*64 + 48 = 304
+static_assert(kParams == 80 * 64 + 64 + 3 * (64 * 64 + 64) + 48 * 64 + 48, "parameter count");
+static_assert(kWeightsBf16 == 80 * 64 + 3 * 64 * 64 + 48 * 64 && kXCols == 336 && kZCols == 304, "layouts");
 
-// shared memory map of the forward / backward kernels
-constexpr int kSmWf = 0;                         // forward weight tiles
-constexpr int kSmWt = kSmWf + 2 * kWeightsBf16;  // transposed weight tiles
-constexpr int kSmAct = kSmWt + 2 * kWeightsBf16; // 128 x 80 BF16 activation tile
-constexpr int kSmBias = kSmAct + kTile * kIn * 2;
-constexpr int kSmBar = kSmBias + 4 * 320;
-constexpr int kSmTotal = kSmBar + 64;
-
-__device__ __forceinline__ uint32_t wtile(int l) { return uint32_t(kSmWf + 2 * hoff(l)); }
-__device__ __forceinline__ uint32_t ttile(int l) { return uint32_t(kSmWt + 2 * hoff(l)); }
+// shared memory maps: the forward kernel keeps W (B operand N = out, K = in),
+// the backward kernel W^T (N = in, K = out); each has one 128-row BF16
+// activation tile (the A operand) and one mbarrier
+// Forward weight tiles carry the bias: every layer runs with K = 80, the
+// activation tile holds a constant 1 in column kBiasCol(l) (78 for layer 0,
+// whose inputs 78 and 79 are zero padding; 64 after the 64 hidden values) and
+// the weight tile holds the bias in that column, so the epilogue adds nothing.
+__host__ __device__ constexpr int kBiasCol(int l) { return l == 0 ? 78 : kHid; }
+__host__ __device__ constexpr int fwd_wtile(int l) { return l == 0 ? 0 : l * kHid * kIn * 2; }  // bytes
+constexpr int kSmFwdW = 0;
+constexpr int kSmFwdAct = kSmFwdW + fwd_wtile(kLayers - 1) + kOut * kIn * 2;
+constexpr int kSmFwdBar = kSmFwdAct + kTile * kIn * 2;
+constexpr int kSmFwd = kSmFwdBar + 64;
+constexpr int kSmBwdWt = 0;
+constexpr int kSmBwdAct = kSmBwdWt + 2 * kWeightsBf16;
+constexpr int kSmBwdBar = kSmBwdAct + kTile * kHid * 2;
+constexpr int kSmBwd = kSmBwdBar + 64;
+static_assert(kSmFwdAct % 128 == 0 && kSmBwdAct % 128 == 0, "operand tiles 128-byte aligned");
 
 struct MlpView {
     const __nv_bfloat16* w16;     // kWeightsBf16
@@ -69,37 +87,56 @@ struct MlpView {
     int* error;                   // set when an mbarrier wait gave up
 };
 
-// Loads both weight layouts and the biases into shared memory.
-__device__ void load_weights(unsigned char* sm, const MlpView& V) {
+// W of every layer as the forward's B operand (out x 80), with the BF16 bias
+// in column kBiasCol(l) and zeros in the other columns past the inputs.
+__device__ void load_weights_fwd(unsigned char* sm, const MlpView& V) {
+    #pragma unroll
+    for (int l = 0; l < kLayers; ++l) {
+        const int I = lin(l), O = lout(l);
+        const unsigned short* src = reinterpret_cast<const unsigned short*>(V.w16 + hoff(l));
+        for (int e = threadIdx.x; e < O * kIn; e += blockDim.x) {
+            const int o = e / kIn, k = e % kIn;
+            unsigned short v = 0;
+            if (k == kBiasCol(l)) v = __bfloat16_as_ushort(__float2bfloat16_rn(V.params[boff(l) + o]));
+            else if (k < I) v = src[o * I + k];
+            *reinterpret_cast<unsigned short*>(sm + kSmFwdW + fwd_wtile(l) + tc::tile_offset(o, k, O)) = v;
+        }
+    }
+}
+
+// W^T of every layer as the backward's B operand.
+__device__ void load_weights_bwd(unsigned char* sm, const MlpView& V) {
+    #pragma unroll
     for (int l = 0; l < kLayers; ++l) {
         const int I = lin(l), O = lout(l);
         const unsigned short* src = reinterpret_cast<const unsigned short*>(V.w16 + hoff(l));
         for (int e = threadIdx.x; e < I * O; e += blockDim.x) {
             const int o = e / I, i = e % I;
-            const unsigned short v = src[e];
-            *reinterpret_cast<unsigned short*>(sm + wtile(l) + tc::tile_offset(o, i, O)) = v;
-            *reinterpret_cast<unsigned short*>(sm + ttile(l) + tc::tile_offset(i, o, I)) = v;
+            *reinterpret_cast<unsigned short*>(sm + kSmBwdWt + 2 * hoff(l) + tc::tile_offset(i, o, I)) = src[e];
         }
     }
-    float* bias = reinterpret_cast<float*>(sm + kSmBias);
-    for (int l = 0; l < kLayers; ++l)
-        for (int o = threadIdx.x; o < lout(l); o += blockDim.x) bias[l * 64 + o] = V.params[boff(l) + o];
 }
 
+// Input encoding. Band k of axis a is (sin, cos)(pi 2^k x_a): sincospif gives
+// band 0 with an exact argument, and each further band follows from the
+// double-angle identities sin 2t = 2 sin t cos t, cos 2t = (cos t - sin t)
+// (cos t + sin t). The error doubles per band, to about 1e-4 at band 11,
+// well under the BF16 rounding (2^-9) the tensor cores apply to the inputs.
 __device__ void encode(const MlpView& V, float3 p, float3 n, float3 wo, float* f) {
     const float x[3] = {fminf(fmaxf((p.x - V.bmin.x) * V.inv_ext.x, 0.0f), 1.0f),
                         fminf(fmaxf((p.y - V.bmin.y) * V.inv_ext.y, 0.0f), 1.0f),
                         fminf(fmaxf((p.z - V.bmin.z) * V.inv_ext.z, 0.0f), 1.0f)};
     #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        float fr = 3.14159265358979f;
+        float s, c;
+        sincospif(x[a], &s, &c);
         #pragma unroll
         for (int k = 0; k < 12; ++k) {
-            float s, c;
-            sincosf(fr * x[a], &s, &c);
             f[a * 24 + k] = s;
             f[a * 24 + 12 + k] = c;
-            fr *= 2.0f;
+            const float s2 = 2.0f * s * c;
+            c = (c - s) * (c + s);
+            s = s2;
         }
     }
     f[72] = n.x; f[73] = n.y; f[74] = n.z;
@@ -175,20 +212,64 @@ struct FwdArgs {
     GuideSamples S;
     const uint32_t* sel;          // batch -> sample index
     const double* wnorm;          // [0] = clamp value, [1] = 1 / (sum of clamped weights)
-    __nv_bfloat16* X;             // [batch][kXCols]
-    float* dout;                  // [batch][kOut]
+    __nv_bfloat16* X;             // [batch][kXCols], inputs of every layer
+    __nv_bfloat16* dZ;            // [batch][kZCols], the forward writes the output layer's block
     float* loss_partial;          // per block
 };
 
+__device__ __forceinline__ void store_row_bf16(__nv_bfloat16* dst, const float* v, int n) {
+    uint4* d = reinterpret_cast<uint4*>(dst);
+    #pragma unroll
+    for (int k = 0; k < n; k += 8)
+        d[k / 8] = make_uint4(tc::pack_bf16(v[k], v[k + 1]), tc::pack_bf16(v[k + 2], v[k + 3]),
+                              tc::pack_bf16(v[k + 4], v[k + 5]), tc::pack_bf16(v[k + 6], v[k + 7]));
+}
+
+__device__ __forceinline__ void load_row_bf16(const __nv_bfloat16* src, float* v, int n) {
+    const uint4* s = reinterpret_cast<const uint4*>(src);
+    #pragma unroll
+    for (int k = 0; k < n; k += 8) {
+        const uint4 q = s[k / 8];
+        const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+        #pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            v[k + 2 * j] = __uint_as_float(w[j] << 16);
+            v[k + 2 * j + 1] = __uint_as_float(w[j] & 0xFFFF0000u);
+        }
+    }
+}
+
+// Issues the MMA chain D = A(128 x K) * B(N x K)^T from two K-major tiles and
+// commits it to bar (one thread).
+__device__ __forceinline__ void mma_chain(uint32_t tmem, uint32_t a_addr, uint32_t b_addr, int K, int N,
+                                          uint64_t* bar) {
+    const uint32_t idesc = tc::idesc_bf16(kTile, uint32_t(N));
+    for (int s = 0; s < K / 16; ++s) {
+        const uint64_t ad = tc::smem_desc(a_addr + s * 2 * (kTile / 8) * 128, (kTile / 8) * 128, 128);
+        const uint64_t bd = tc::smem_desc(b_addr + s * 2 * (N / 8) * 128, (N / 8) * 128, 128);
+        tc::mma_bf16(tmem, ad, bd, idesc, s > 0);
+    }
+    tc::mma_commit(bar);
+}
+
+// Waits for the chain committed to bar: the issuing thread polls the mbarrier
+// (bounded), the rest of the CTA waits at the barrier instruction, which
+// takes no issue slots (128 polling threads per CTA would crowd out the other
+// CTAs' epilogues on the SM).
+__device__ __forceinline__ void wait_chain(uint64_t* bar, uint32_t phase, bool& ok) {
+    if (threadIdx.x == 0) ok = tc::mbar_wait(bar, phase) && ok;
+    __syncthreads();
+    tc::fence_after_sync();
+}
+
 template <bool Train>
-__global__ void __launch_bounds__(kTile) mlp_forward_kernel(FwdArgs A) {
+__global__ void __launch_bounds__(kTile, 3) mlp_forward_kernel(FwdArgs A) {
     extern __shared__ __align__(1024) unsigned char sm[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kSmBar);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSmBar + 8);
-    const float* bias = reinterpret_cast<const float*>(sm + kSmBias);
-    unsigned char* act = sm + kSmAct;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kSmFwdBar);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSmFwdBar + 8);
+    unsigned char* act = sm + kSmFwdAct;
     const int t = threadIdx.x, warp = t >> 5;
-    load_weights(sm, A.V);
+    load_weights_fwd(sm, A.V);
     if (warp == 0) tc::tmem_alloc(tslot, 128);
     if (t == 0) tc::mbar_init(bar, 1);
     tc::fence_proxy_async();
@@ -199,41 +280,43 @@ __global__ void __launch_bounds__(kTile) mlp_forward_kernel(FwdArgs A) {
     const uint32_t count = Train ? A.count : *A.count_ptr;
     const uint32_t tiles = (count + kTile - 1) / kTile;
     const uint32_t act_addr = tc::smem_addr(act);
-    const uint32_t sm_base = tc::smem_addr(sm);
+    const uint32_t w_addr = tc::smem_addr(sm + kSmFwdW);
     uint32_t phase = 0;
     float loss_acc = 0.0f;
     bool ok = true;
     for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const uint32_t row = tile * kTile + t;
         const bool valid = row < count;
-        float f[kIn];
         float3 om = f3(0, 0, 0);
         float wgt = 0.0f;
         bool active = false;
-        if (valid) {
-            if (Train) {
-                const uint32_t si = A.sel[row];
-                const float4 s0 = A.S.s0[si], s1 = A.S.s1[si], s2 = A.S.s2[si], s3 = A.S.s3[si];
-                encode(A.V, xyz(s0), xyz(s2), xyz(s3), f);
-                om = xyz(s1);
-                wgt = float(double(fminf(s0.w, float(A.wnorm[0]))) * A.wnorm[1]);
-                active = true;
+        {
+            float f[kIn];
+            if (valid) {
+                if (Train) {
+                    const uint32_t si = A.sel[row];
+                    const float4 s0 = A.S.s0[si], s1 = A.S.s1[si], s2 = A.S.s2[si], s3 = A.S.s3[si];
+                    encode(A.V, xyz(s0), xyz(s2), xyz(s3), f);
+                    om = xyz(s1);
+                    wgt = float(double(fminf(s0.w, float(A.wnorm[0]))) * A.wnorm[1]);
+                    active = true;
+                } else {
+                    const float4 a = A.surf[size_t(row) * 3], b = A.surf[size_t(row) * 3 + 1],
+                                 c = A.surf[size_t(row) * 3 + 2];
+                    active = b.w > 0.0f;
+                    encode(A.V, xyz(a), xyz(b), xyz(c), f);
+                }
             } else {
-                const float4 a = A.surf[size_t(row) * 3], b = A.surf[size_t(row) * 3 + 1], c = A.surf[size_t(row) * 3 + 2];
-                active = b.w > 0.0f;
-                encode(A.V, xyz(a), xyz(b), xyz(c), f);
+                #pragma unroll
+                for (int k = 0; k < kIn; ++k) f[k] = 0.0f;
             }
-        } else {
-            for (int k = 0; k < kIn; ++k) f[k] = 0.0f;
-        }
-        for (int k = 0; k < kIn; k += 8) tc::st_row8(act, kTile, t, k, f + k);
-        if (Train && valid) {
-            uint4* dst = reinterpret_cast<uint4*>(A.X + size_t(row) * kXCols);
-            for (int k = 0; k < kIn; k += 8)
-                dst[k / 8] = make_uint4(tc::pack_bf16(f[k], f[k + 1]), tc::pack_bf16(f[k + 2], f[k + 3]),
-                                        tc::pack_bf16(f[k + 4], f[k + 5]), tc::pack_bf16(f[k + 6], f[k + 7]));
+            if (Train && valid) store_row_bf16(A.X + size_t(row) * kXCols, f, kIn);
+            f[kBiasCol(0)] = 1.0f;
+            #pragma unroll
+            for (int k = 0; k < kIn; k += 8) tc::st_row8(act, kTile, t, k, f + k);
         }
         float out[kHid];
+        #pragma unroll
         for (int l = 0; l < kLayers; ++l) {
             const int I = lin(l), O = lout(l);
             tc::fence_proxy_async();
@@ -241,29 +324,29 @@ __global__ void __launch_bounds__(kTile) mlp_forward_kernel(FwdArgs A) {
             __syncthreads();
             if (t == 0) {
                 tc::fence_after_sync();
-                const uint32_t idesc = tc::idesc_bf16(kTile, O);
-                for (int s = 0; s < I / 16; ++s) {
-                    const uint64_t ad = tc::smem_desc(act_addr + s * 2 * (kTile / 8) * 128, (kTile / 8) * 128, 128);
-                    const uint64_t bd = tc::smem_desc(sm_base + wtile(l) + s * 2 * (O / 8) * 128, (O / 8) * 128, 128);
-                    tc::mma_bf16(tmem, ad, bd, idesc, s > 0);
-                }
-                tc::mma_commit(bar);
+                mma_chain(tmem, act_addr, w_addr + fwd_wtile(l), kIn, O, bar);
             }
-            ok = tc::mbar_wait(bar, phase) && ok;
+            wait_chain(bar, phase, ok);
             phase ^= 1u;
-            tc::fence_after_sync();
-            for (int c = 0; c < O; c += 16) tc::tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + c, out + c);
-            tc::tmem_wait_ld();
-            for (int o = 0; o < O; ++o) out[o] += bias[l * 64 + o];
+            (void)I;
+            const uint32_t trow = tmem + (uint32_t(warp * 32) << 16);
+            tc::tmem_ld32_wait(trow, out);
+            if (O == 64) tc::tmem_ld32_wait(trow + 32, out + 32);
+            else tc::tmem_ld16_wait(trow + 32, out + 32);
+            if (l == 0) {  // the hidden layers' constant columns: 1 at kBiasCol, zeros after it
+                uint4* cst = reinterpret_cast<uint4*>(act + tc::tile_offset(t, kHid, kTile));
+                *cst = make_uint4(0x3F80u, 0u, 0u, 0u);
+                *reinterpret_cast<uint4*>(act + tc::tile_offset(t, kHid + 8, kTile)) = make_uint4(0u, 0u, 0u, 0u);
+            }
             if (l + 1 < kLayers) {
+                #pragma unroll
                 for (int o = 0; o < O; ++o) out[o] = fmaxf(out[o], 0.0f);
+                // the chain that read the tile has completed (mbarrier), so each
+                // thread may overwrite its row; the barrier before the next chain
+                // orders every thread's TMEM reads before that chain's writes
+                #pragma unroll
                 for (int k = 0; k < O; k += 8) tc::st_row8(act, kTile, t, k, out + k);
-                if (Train && valid) {
-                    uint4* dst = reinterpret_cast<uint4*>(A.X + size_t(row) * kXCols + xoff(l + 1));
-                    for (int k = 0; k < O; k += 8)
-                        dst[k / 8] = make_uint4(tc::pack_bf16(out[k], out[k + 1]), tc::pack_bf16(out[k + 2], out[k + 3]),
-                                                tc::pack_bf16(out[k + 4], out[k + 5]), tc::pack_bf16(out[k + 6], out[k + 7]));
-                }
+                if (Train && valid) store_row_bf16(A.X + size_t(row) * kXCols + xoff(l + 1), out, O);
             }
         }
         if (valid) {
@@ -271,8 +354,7 @@ __global__ void __launch_bounds__(kTile) mlp_forward_kernel(FwdArgs A) {
                 float g[kOut];
                 const float nll = head_grad(out, om, wgt * kLossScale, g);
                 loss_acc += wgt * nll;
-                float4* d = reinterpret_cast<float4*>(A.dout + size_t(row) * kOut);
-                for (int q = 0; q < kOut; q += 4) d[q / 4] = make_float4(g[q], g[q + 1], g[q + 2], g[q + 3]);
+                store_row_bf16(A.dZ + size_t(row) * kZCols + zoff(kLayers - 1), g, kOut);
                 (void)active;
             } else {
                 float4 lobe[kMaxLobes];
@@ -280,6 +362,7 @@ __global__ void __launch_bounds__(kTile) mlp_forward_kernel(FwdArgs A) {
                 float4* m = A.mix + size_t(row) * (kMaxLobes + 2);
                 if (active) {
                     head_mixture(out, lobe, pi);
+                    #pragma unroll
                     for (int j = 0; j < kMaxLobes; ++j) m[j] = lobe[j];
                     m[kMaxLobes] = make_float4(pi[0], pi[1], pi[2], pi[3]);
                     m[kMaxLobes + 1] = make_float4(pi[4], pi[5], pi[6], pi[7]);
@@ -313,18 +396,18 @@ struct BwdArgs {
     MlpView V;
     uint32_t count;
     const __nv_bfloat16* X;       // [batch][kXCols]
-    const float* dout;            // [batch][kOut]
-    __nv_bfloat16* dZ;            // [batch][kZCols]
+    __nv_bfloat16* dZ;            // [batch][kZCols]; the output layer's block is an input
 };
 
-// dZ_4 = dout; dX_l = dZ_l W_l (tensor cores), dZ_{l-1} = dX_l * [X_l > 0].
-__global__ void __launch_bounds__(kTile) mlp_backward_kernel(BwdArgs A) {
+// dX_l = dZ_l W_l on the tensor cores (M = 128 samples, N = in, K = out),
+// dZ_{l-1} = dX_l * [X_l > 0], for l = 4 .. 1.
+__global__ void __launch_bounds__(kTile, 3) mlp_backward_kernel(BwdArgs A) {
     extern __shared__ __align__(1024) unsigned char sm[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kSmBar);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSmBar + 8);
-    unsigned char* act = sm + kSmAct;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kSmBwdBar);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSmBwdBar + 8);
+    unsigned char* act = sm + kSmBwdAct;
     const int t = threadIdx.x, warp = t >> 5;
-    load_weights(sm, A.V);
+    load_weights_bwd(sm, A.V);
     if (warp == 0) tc::tmem_alloc(tslot, 128);
     if (t == 0) tc::mbar_init(bar, 1);
     tc::fence_proxy_async();
@@ -334,53 +417,40 @@ __global__ void __launch_bounds__(kTile) mlp_backward_kernel(BwdArgs A) {
     const uint32_t tmem = *tslot;
     const uint32_t tiles = (A.count + kTile - 1) / kTile;
     const uint32_t act_addr = tc::smem_addr(act);
-    const uint32_t sm_base = tc::smem_addr(sm);
+    const uint32_t wt_addr = tc::smem_addr(sm + kSmBwdWt);
     uint32_t phase = 0;
     bool ok = true;
     for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const uint32_t row = tile * kTile + t;
         const bool valid = row < A.count;
         float dz[kHid];
-        for (int q = 0; q < kOut; ++q) dz[q] = valid ? A.dout[size_t(row) * kOut + q] : 0.0f;
-        for (int q = kOut; q < kHid; ++q) dz[q] = 0.0f;
-        for (int l = kLayers - 1; l >= 0; --l) {
+        #pragma unroll
+        for (int q = 0; q < kHid; ++q) dz[q] = 0.0f;
+        if (valid) load_row_bf16(A.dZ + size_t(row) * kZCols + zoff(kLayers - 1), dz, kOut);
+        #pragma unroll
+        for (int l = kLayers - 1; l >= 1; --l) {
             const int I = lin(l), O = lout(l);
-            // dZ_l: keep it for the weight gradient and stage it as the A operand
-            if (valid) {
-                uint4* dst = reinterpret_cast<uint4*>(A.dZ + size_t(row) * kZCols + zoff(l));
-                for (int k = 0; k < O; k += 8)
-                    dst[k / 8] = make_uint4(tc::pack_bf16(dz[k], dz[k + 1]), tc::pack_bf16(dz[k + 2], dz[k + 3]),
-                                            tc::pack_bf16(dz[k + 4], dz[k + 5]), tc::pack_bf16(dz[k + 6], dz[k + 7]));
-            }
-            if (l == 0) break;
+            #pragma unroll
             for (int k = 0; k < O; k += 8) tc::st_row8(act, kTile, t, k, dz + k);
             tc::fence_proxy_async();
             tc::fence_before_sync();
             __syncthreads();
             if (t == 0) {
                 tc::fence_after_sync();
-                const uint32_t idesc = tc::idesc_bf16(kTile, I);
-                for (int s = 0; s < O / 16; ++s) {
-                    const uint64_t ad = tc::smem_desc(act_addr + s * 2 * (kTile / 8) * 128, (kTile / 8) * 128, 128);
-                    const uint64_t bd = tc::smem_desc(sm_base + ttile(l) + s * 2 * (I / 8) * 128, (I / 8) * 128, 128);
-                    tc::mma_bf16(tmem, ad, bd, idesc, s > 0);
-                }
-                tc::mma_commit(bar);
+                mma_chain(tmem, act_addr, wt_addr + 2 * hoff(l), O, I, bar);
             }
-            ok = tc::mbar_wait(bar, phase) && ok;
+            wait_chain(bar, phase, ok);
             phase ^= 1u;
-            tc::fence_after_sync();
             float dx[kHid];
-            for (int c = 0; c < I; c += 16) tc::tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + c, dx + c);
-            tc::tmem_wait_ld();
-            tc::fence_before_sync();
-            __syncthreads();  // every lane has read the accumulator before the next chain
-            // X_l (input of layer l, l >= 1) is ReLU(Z_{l-1}): its mask gates dZ_{l-1}
-            for (int k = 0; k < I; ++k) {
-                float xv = 0.0f;
-                if (valid) xv = __bfloat162float(A.X[size_t(row) * kXCols + xoff(l) + k]);
-                dz[k] = xv > 0.0f ? dx[k] : 0.0f;
-            }
+            tc::tmem_ld32_wait(tmem + (uint32_t(warp * 32) << 16), dx);
+            tc::tmem_ld32_wait(tmem + (uint32_t(warp * 32) << 16) + 32, dx + 32);
+            static_assert(kHid == 64, "dX is read as two 32-column loads");
+            // X_l (the input of layer l >= 1) is ReLU(Z_{l-1}): its mask gates dZ_{l-1}
+            float xv[kHid];
+            if (valid) load_row_bf16(A.X + size_t(row) * kXCols + xoff(l), xv, I);
+            #pragma unroll
+            for (int k = 0; k < I; ++k) dz[k] = (valid && xv[k] > 0.0f) ? dx[k] : 0.0f;
+            if (valid) store_row_bf16(A.dZ + size_t(row) * kZCols + zoff(l - 1), dz, I);
         }
     }
     if (!ok && t == 0) atomicExch(A.V.error, 1);
@@ -392,60 +462,153 @@ __global__ void __launch_bounds__(kTile) mlp_backward_kernel(BwdArgs A) {
     }
 }
 
-// Weight gradients on the CUDA cores: block (layer, chunk) accumulates
-// dW[o][i] (and db[o] as column I) over its sample chunk.
-constexpr int kWgChunk = 2048;
-__global__ void __launch_bounds__(256) mlp_wgrad_kernel(const __nv_bfloat16* __restrict__ X,
-                                                        const __nv_bfloat16* __restrict__ dZ, uint32_t count,
-                                                        float* __restrict__ partial, uint32_t chunks) {
-    const int l = blockIdx.y;
-    const int I = lin(l), O = lout(l);
-    const uint32_t b0 = blockIdx.x * kWgChunk;
-    const uint32_t b1 = min(count, b0 + kWgChunk);
-    __shared__ float sx[32][kIn + 1];
-    __shared__ float sz[32][kHid];
-    const int t = threadIdx.x;
-    const int o = t >> 2;                 // 0..63
-    const int iq = t & 3;                 // columns iq, iq+4, ... (I+1 columns incl. bias)
-    float acc[21];
-    for (int j = 0; j < 21; ++j) acc[j] = 0.0f;
-    for (uint32_t bb = b0; bb < b1; bb += 32) {
-        for (int e = t; e < 32 * (I + 1); e += 256) {
-            const int r = e / (I + 1), c = e % (I + 1);
-            const uint32_t b = bb + r;
-            sx[r][c] = (b < b1) ? (c < I ? __bfloat162float(X[size_t(b) * kXCols + xoff(l) + c]) : 1.0f) : 0.0f;
-        }
-        for (int e = t; e < 32 * O; e += 256) {
-            const int r = e / O, c = e % O;
-            const uint32_t b = bb + r;
-            sz[r][c] = (b < b1) ? __bfloat162float(dZ[size_t(b) * kZCols + zoff(l) + c]) : 0.0f;
-        }
-        __syncthreads();
-        if (o < O) {
-            for (int r = 0; r < 32; ++r) {
-                const float z = sz[r][o];
-                for (int j = 0, i = iq; i <= I; ++j, i += 4) acc[j] += z * sx[r][i];
+// ── weight gradients on the tensor cores ──────────────────────────────────
+// dW_l^T (in x out) = X_l^T dZ_l with the batch as the K dimension. A
+// persistent CTA owns a contiguous range of 64-sample steps. Per step it
+// stages the transposes of the step's X rows (kWgRowsX rows) and dZ rows
+// (kZCols rows) K-major in shared memory; layer l's A operand is the 128-row
+// window from row kWgRow[l]: its I input features, a constant row of ones
+// (whose product with dZ_l is db_l) and rows that are ignored. Layer l
+// accumulates into TMEM columns kWgCol[l] .. + out over all of the CTA's
+// steps; the CTA then writes its FP32 partial gradient, and
+// mlp_reduce_kernel sums the partials in CTA order.
+constexpr int kWgStep = 64;                                  // samples per step (K)
+// first row of layer l's window: layer 0 takes 80 inputs + the ones row (88
+// rows after padding to 8), hidden layers 64 + 1 (72 rows)
+__host__ __device__ constexpr int wg_row(int l) { return l == 0 ? 0 : 88 + (l - 1) * 72; }
+static_assert(wg_row(1) == ((kIn + 1 + 7) / 8) * 8 && wg_row(2) - wg_row(1) == ((kHid + 1 + 7) / 8) * 8, "rows");
+constexpr int kWgRowsX = wg_row(kLayers - 1) + kTile;        // 432
+constexpr int kWgLboX = kWgRowsX * 16 + 16;                  // K-block stride; +16 B keeps the stores conflict-free
+constexpr int kWgLboZ = kZCols * 16 + 16;
+constexpr int kWgBlkX = (kWgStep / 8) * kWgLboX;
+constexpr int kWgBlkZ = (kWgStep / 8) * kWgLboZ;
+constexpr int kWgStage = kWgBlkX + kWgBlkZ;
+constexpr int kSmWg = 2 * kWgStage + 64;
+static_assert(kSmWg <= 227 * 1024, "wgrad stages exceed shared memory");
+static_assert(kZCols <= 512 && zoff(kLayers) <= 304, "wgrad TMEM columns");
+
+__global__ void __launch_bounds__(kTile, 1) mlp_wgrad_kernel(const __nv_bfloat16* __restrict__ X,
+                                                            const __nv_bfloat16* __restrict__ dZ, uint32_t count,
+                                                            float* __restrict__ partial, int* error) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * kWgStage);     // one per stage
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + 2 * kWgStage + 16);
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const uint32_t steps = (count + kWgStep - 1) / kWgStep;
+    const uint32_t s_begin = uint32_t((uint64_t(blockIdx.x) * steps) / gridDim.x);
+    const uint32_t s_end = uint32_t((uint64_t(blockIdx.x + 1) * steps) / gridDim.x);
+    // constant rows: zero everything, then the ones rows of both stages
+    for (int e = t; e < 2 * kWgStage / 16; e += kTile) reinterpret_cast<uint4*>(sm)[e] = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    for (int e = t; e < 2 * kLayers * (kWgStep / 2); e += kTile) {
+        const int stage = e / (kLayers * (kWgStep / 2));
+        const int l = (e / (kWgStep / 2)) % kLayers;
+        const int p = e % (kWgStep / 2);
+        const int r = wg_row(l) + lin(l);
+        *reinterpret_cast<uint32_t*>(sm + stage * kWgStage + (p / 4) * kWgLboX + r * 16 + (p % 4) * 4) = 0x3F803F80u;
+    }
+    if (warp == 0) tc::tmem_alloc(tslot, 512);
+    if (t == 0) { tc::mbar_init(bar, 1); tc::mbar_init(bar + 1, 1); }
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tslot;
+    bool ok = true;
+    for (uint32_t step = s_begin; step < s_end; ++step) {
+        const uint32_t i = step - s_begin;
+        const uint32_t buf = i & 1u;
+        if (i >= 2) wait_chain(bar + buf, ((i >> 1) - 1u) & 1u, ok);   // the MMAs of step i-2 are done
+        unsigned char* xb = sm + buf * kWgStage;
+        unsigned char* zb = xb + kWgBlkX;
+        // lane = sample pair (samples 2*lane, 2*lane+1 of the step); warp w takes feature groups w, w+4, ...
+        const uint32_t s0 = step * kWgStep + 2 * lane, s1 = s0 + 1;
+        for (int g = warp; g < (kXCols + kZCols) / 8; g += 4) {
+            const bool is_x = g < kXCols / 8;
+            const int col = is_x ? g * 8 : (g - kXCols / 8) * 8;
+            const __nv_bfloat16* base = is_x ? X : dZ;
+            const size_t ld = is_x ? kXCols : kZCols;
+            uint4 a = make_uint4(0, 0, 0, 0), b = make_uint4(0, 0, 0, 0);
+            if (s0 < count) a = *reinterpret_cast<const uint4*>(base + size_t(s0) * ld + col);
+            if (s1 < count) b = *reinterpret_cast<const uint4*>(base + size_t(s1) * ld + col);
+            int r0;
+            unsigned char* blk;
+            uint32_t lbo;
+            if (is_x) {
+                int l = 0;
+                #pragma unroll
+                for (int q = 1; q < kLayers; ++q) l += col >= xoff(q) ? 1 : 0;
+                r0 = wg_row(l) + (col - xoff(l));
+                blk = xb;
+                lbo = kWgLboX;
+            } else {
+                r0 = col;
+                blk = zb;
+                lbo = kWgLboZ;
+            }
+            unsigned char* dst = blk + (lane / 4) * lbo + r0 * 16 + (lane % 4) * 4;
+            const uint32_t wa[4] = {a.x, a.y, a.z, a.w}, wb[4] = {b.x, b.y, b.z, b.w};
+            #pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                *reinterpret_cast<uint32_t*>(dst + (2 * j) * 16) = __byte_perm(wa[j], wb[j], 0x5410);
+                *reinterpret_cast<uint32_t*>(dst + (2 * j + 1) * 16) = __byte_perm(wa[j], wb[j], 0x7632);
             }
         }
+        tc::fence_proxy_async();
+        tc::fence_before_sync();
         __syncthreads();
+        if (t == 0) {
+            tc::fence_after_sync();
+            const uint32_t xa = tc::smem_addr(xb), za = tc::smem_addr(zb);
+            #pragma unroll
+            for (int l = 0; l < kLayers; ++l) {
+                const uint32_t idesc = tc::idesc_bf16(kTile, uint32_t(lout(l)));
+                #pragma unroll
+                for (int s = 0; s < kWgStep / 16; ++s) {
+                    const uint64_t ad = tc::smem_desc(xa + wg_row(l) * 16 + s * 2 * kWgLboX, kWgLboX, 128);
+                    const uint64_t bd = tc::smem_desc(za + zoff(l) * 16 + s * 2 * kWgLboZ, kWgLboZ, 128);
+                    tc::mma_bf16(tmem + uint32_t(zoff(l)), ad, bd, idesc, i > 0 || s > 0);
+                }
+            }
+            tc::mma_commit(bar + buf);
+        }
     }
-    if (o < O) {
-        float* dst = partial + (size_t(l) * chunks + blockIdx.x) * (kHid * (kIn + 1));
-        for (int j = 0, i = iq; i <= I; ++j, i += 4) dst[o * (kIn + 1) + i] = acc[j];
+    const uint32_t n = s_end - s_begin;
+    if (n > 0) wait_chain(bar + ((n - 1) & 1u), ((n - 1) >> 1) & 1u, ok);
+    float* dst = partial + size_t(blockIdx.x) * kParams;
+    const int r = warp * 32 + lane;   // TMEM lane = row of dW^T = input feature (I = bias row)
+    #pragma unroll
+    for (int l = 0; l < kLayers; ++l) {
+        const int I = lin(l), O = lout(l);
+        #pragma unroll
+        for (int c = 0; c < O; c += 16) {
+            float v[16];
+            tc::tmem_ld16_wait(tmem + (uint32_t(warp * 32) << 16) + uint32_t(zoff(l) + c), v);
+            #pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const float val = n > 0 ? v[q] : 0.0f;
+                if (r < I) dst[woff(l) + (c + q) * I + r] = val;
+                else if (r == I) dst[boff(l) + c + q] = val;
+            }
+        }
+    }
+    if (!ok && t == 0) atomicExch(error, 1);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_free(tmem, 512);
     }
 }
 
-__global__ void __launch_bounds__(256) mlp_reduce_kernel(const float* __restrict__ partial, uint32_t chunks,
+// grad = sum of the CTA partials in CTA order.
+__global__ void __launch_bounds__(256) mlp_reduce_kernel(const float* __restrict__ partial, uint32_t parts,
                                                          float* __restrict__ grad) {
-    const int l = blockIdx.y;
-    const int I = lin(l), O = lout(l);
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= O * (I + 1)) return;
-    const int o = e / (I + 1), i = e % (I + 1);
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= kParams) return;
     float s = 0.0f;
-    for (uint32_t c = 0; c < chunks; ++c) s += partial[(size_t(l) * chunks + c) * (kHid * (kIn + 1)) + o * (kIn + 1) + i];
-    if (i < I) grad[woff(l) + o * I + i] = s;
-    else grad[boff(l) + o] = s;
+    for (uint32_t c = 0; c < parts; ++c) s += partial[size_t(c) * kParams + p];
+    grad[p] = s;
 }
 
 __global__ void __launch_bounds__(256) mlp_adam_kernel(float* __restrict__ params, const float* __restrict__ grad,
@@ -466,25 +629,38 @@ __global__ void __launch_bounds__(256) mlp_adam_kernel(float* __restrict__ param
         if (p >= woff(l) && p < boff(l)) w16[hoff(l) + (p - woff(l))] = __float2bfloat16_rn(th);
 }
 
-// Sum of clamped weights of the batch (clamp = 20 x mean), fixed order.
-__global__ void __launch_bounds__(256) mlp_weight_norm_kernel(GuideSamples S, const uint32_t* sel, uint32_t n,
-                                                              double* out) {
+// Batch weight normalisation (clamp = 20 x mean, then 1 / sum of clamped
+// weights), as two fixed-order reductions: block b sums the batch slice
+// [b n / G, (b+1) n / G) in FP64, then one thread adds the G partials in order.
+constexpr int kWnBlocks = 148;
+__global__ void __launch_bounds__(256) mlp_wsum_kernel(GuideSamples S, const uint32_t* __restrict__ sel, uint32_t n,
+                                                       const double* __restrict__ wnorm, bool clamped,
+                                                       double* __restrict__ partial) {
     __shared__ double red[256];
     const int t = threadIdx.x;
+    const uint32_t b0 = uint32_t((uint64_t(blockIdx.x) * n) / gridDim.x);
+    const uint32_t b1 = uint32_t((uint64_t(blockIdx.x + 1) * n) / gridDim.x);
+    const double cv = clamped ? wnorm[0] : 0.0;
     double s = 0.0;
-    for (uint32_t i = t; i < n; i += 256) s += double(S.s0[sel[i]].w);
+    for (uint32_t i = b0 + t; i < b1; i += 256) {
+        const double w = double(S.s0[sel[i]].w);
+        s += clamped ? fmin(w, cv) : w;
+    }
     red[t] = s;
     __syncthreads();
-    for (int k = 128; k > 0; k >>= 1) { if (t < k) red[t] += red[t + k]; __syncthreads(); }
-    const double mean = red[0] / double(n > 0 ? n : 1);
-    const double clampv = 20.0 * mean;
-    __syncthreads();
-    s = 0.0;
-    for (uint32_t i = t; i < n; i += 256) s += fmin(double(S.s0[sel[i]].w), clampv);
-    red[t] = s;
-    __syncthreads();
-    for (int k = 128; k > 0; k >>= 1) { if (t < k) red[t] += red[t + k]; __syncthreads(); }
-    if (t == 0) { out[0] = clampv; out[1] = red[0] > 0.0 ? 1.0 / red[0] : 0.0; }
+    for (int k = 128; k > 0; k >>= 1) {
+        if (t < k) red[t] += red[t + k];
+        __syncthreads();
+    }
+    if (t == 0) partial[blockIdx.x] = red[0];
+}
+
+__global__ void mlp_wfinish_kernel(const double* __restrict__ partial, uint32_t parts, uint32_t n, bool clamped,
+                                   double* __restrict__ wnorm) {
+    double s = 0.0;
+    for (uint32_t c = 0; c < parts; ++c) s += partial[c];
+    if (!clamped) wnorm[0] = 20.0 * (s / double(n > 0 ? n : 1));
+    else wnorm[1] = s > 0.0 ? 1.0 / s : 0.0;
 }
 
 __global__ void mlp_select_kernel(uint32_t* sel, uint32_t batch, uint32_t n, uint32_t offset) {
@@ -526,9 +702,10 @@ struct rr_mlp_state {
     double* wnorm = nullptr;
     __nv_bfloat16* X = nullptr;
     __nv_bfloat16* dZ = nullptr;
-    float* dout = nullptr;
     float* loss_partial = nullptr;
-    float* wpartial = nullptr;
+    float* wpartial = nullptr;    // per wgrad CTA: kParams FP32
+    double* wn_partial = nullptr; // per weight-norm block
+    int wg_grid = 0;
     uint32_t batch_cap = 0;
     uint32_t steps = 0;
     int grid = 0;
@@ -577,16 +754,16 @@ rr_status rr_mlp_guide_init(rr_ctx* ctx, rr_guide* g) {
     if ((st = al(reinterpret_cast<void**>(&M.wnorm), 16)) != RR_OK) return st;
     if ((st = al(reinterpret_cast<void**>(&M.X), size_t(B) * kXCols * 2)) != RR_OK) return st;
     if ((st = al(reinterpret_cast<void**>(&M.dZ), size_t(B) * kZCols * 2)) != RR_OK) return st;
-    if ((st = al(reinterpret_cast<void**>(&M.dout), size_t(B) * kOut * 4)) != RR_OK) return st;
-    M.grid = ctx->sm_count;
-    if ((st = al(reinterpret_cast<void**>(&M.loss_partial), size_t(M.grid) * 4 * 4)) != RR_OK) return st;
-    const uint32_t chunks = (B + kWgChunk - 1) / kWgChunk;
-    if ((st = al(reinterpret_cast<void**>(&M.wpartial), size_t(kLayers) * chunks * kHid * (kIn + 1) * 4)) != RR_OK)
-        return st;
-    RR_TRY_CUDA(ctx, cudaMallocHost(&M.loss_host, size_t(M.grid) * 4 * 4));
+    M.grid = 3 * ctx->sm_count;
+    if ((st = al(reinterpret_cast<void**>(&M.loss_partial), size_t(M.grid) * 4)) != RR_OK) return st;
+    M.wg_grid = ctx->sm_count;
+    if ((st = al(reinterpret_cast<void**>(&M.wpartial), size_t(M.wg_grid) * kParams * 4)) != RR_OK) return st;
+    if ((st = al(reinterpret_cast<void**>(&M.wn_partial), size_t(kWnBlocks) * 8)) != RR_OK) return st;
+    RR_TRY_CUDA(ctx, cudaMallocHost(&M.loss_host, size_t(M.grid) * 4));
     for (auto k : {mlp_forward_kernel<true>, mlp_forward_kernel<false>})
-        RR_TRY_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmTotal));
-    RR_TRY_CUDA(ctx, cudaFuncSetAttribute(mlp_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmTotal));
+        RR_TRY_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmFwd));
+    RR_TRY_CUDA(ctx, cudaFuncSetAttribute(mlp_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmBwd));
+    RR_TRY_CUDA(ctx, cudaFuncSetAttribute(mlp_wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmWg));
     return RR_OK;
 }
 
@@ -624,8 +801,8 @@ rr_status rr_mlp_guide_infer(rr_ctx* ctx, rr_guide* g, const uint32_t* count_dev
     A.mix = g->mlp_mix;
     A.count_ptr = count_dev;
     const uint32_t tiles = (max_count + kTile - 1) / kTile;
-    const int grid = int(std::min<uint32_t>(tiles, uint32_t(2 * ctx->sm_count)));
-    mlp_forward_kernel<false><<<std::max(grid, 1), kTile, kSmTotal, stream>>>(A);
+    const int grid = int(std::min<uint32_t>(tiles, uint32_t(3 * ctx->sm_count)));
+    mlp_forward_kernel<false><<<std::max(grid, 1), kTile, kSmFwd, stream>>>(A);
     RR_CHECK_LAUNCH(ctx);
     g->mlp_infer_launches = 1;
     return RR_OK;
@@ -640,8 +817,8 @@ rr_status rr_mlp_guide_eval(rr_ctx* ctx, rr_guide* g, const float4* surf, float4
     A.mix = mix;
     A.count_ptr = count_dev;
     const uint32_t tiles = (count + kTile - 1) / kTile;
-    const int grid = int(std::min<uint32_t>(tiles, uint32_t(2 * ctx->sm_count)));
-    mlp_forward_kernel<false><<<std::max(grid, 1), kTile, kSmTotal, stream>>>(A);
+    const int grid = int(std::min<uint32_t>(tiles, uint32_t(3 * ctx->sm_count)));
+    mlp_forward_kernel<false><<<std::max(grid, 1), kTile, kSmFwd, stream>>>(A);
     RR_CHECK_LAUNCH(ctx);
     ctx->launches += 1;
     return RR_OK;
@@ -653,7 +830,10 @@ rr_status rr_mlp_guide_train(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t 
     const uint32_t B = std::min(n, M.batch_cap);
     mlp_select_kernel<<<(B + 255) / 256, 256, 0, stream>>>(M.sel, B, n, (M.steps * 7919u) % n);
     RR_CHECK_LAUNCH(ctx);
-    mlp_weight_norm_kernel<<<1, 256, 0, stream>>>(g->samples, M.sel, B, M.wnorm);
+    mlp_wsum_kernel<<<kWnBlocks, 256, 0, stream>>>(g->samples, M.sel, B, M.wnorm, false, M.wn_partial);
+    mlp_wfinish_kernel<<<1, 1, 0, stream>>>(M.wn_partial, kWnBlocks, B, false, M.wnorm);
+    mlp_wsum_kernel<<<kWnBlocks, 256, 0, stream>>>(g->samples, M.sel, B, M.wnorm, true, M.wn_partial);
+    mlp_wfinish_kernel<<<1, 1, 0, stream>>>(M.wn_partial, kWnBlocks, B, true, M.wnorm);
     RR_CHECK_LAUNCH(ctx);
     FwdArgs A{};
     A.V = mlp_view(g);
@@ -662,25 +842,25 @@ rr_status rr_mlp_guide_train(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t 
     A.sel = M.sel;
     A.wnorm = M.wnorm;
     A.X = M.X;
-    A.dout = M.dout;
+    A.dZ = M.dZ;
     A.loss_partial = M.loss_partial;
     const uint32_t tiles = (B + kTile - 1) / kTile;
     const int grid = int(std::min<uint32_t>(tiles, uint32_t(M.grid)));
     RR_TRY_CUDA(ctx, cudaMemsetAsync(M.loss_partial, 0, size_t(M.grid) * 4, stream));
-    mlp_forward_kernel<true><<<grid, kTile, kSmTotal, stream>>>(A);
+    mlp_forward_kernel<true><<<grid, kTile, kSmFwd, stream>>>(A);
     RR_CHECK_LAUNCH(ctx);
     BwdArgs Bw{};
     Bw.V = A.V;
     Bw.count = B;
     Bw.X = M.X;
-    Bw.dout = M.dout;
     Bw.dZ = M.dZ;
-    mlp_backward_kernel<<<grid, kTile, kSmTotal, stream>>>(Bw);
+    mlp_backward_kernel<<<grid, kTile, kSmBwd, stream>>>(Bw);
     RR_CHECK_LAUNCH(ctx);
-    const uint32_t chunks = (B + kWgChunk - 1) / kWgChunk;
-    mlp_wgrad_kernel<<<dim3(chunks, kLayers), 256, 0, stream>>>(M.X, M.dZ, B, M.wpartial, chunks);
+    const uint32_t wsteps = (B + kWgStep - 1) / kWgStep;
+    const int wgrid = int(std::min<uint32_t>(wsteps, uint32_t(M.wg_grid)));
+    mlp_wgrad_kernel<<<wgrid, kTile, kSmWg, stream>>>(M.X, M.dZ, B, M.wpartial, M.error);
     RR_CHECK_LAUNCH(ctx);
-    mlp_reduce_kernel<<<dim3((kHid * (kIn + 1) + 255) / 256, kLayers), 256, 0, stream>>>(M.wpartial, chunks, M.grad);
+    mlp_reduce_kernel<<<(kParams + 255) / 256, 256, 0, stream>>>(M.wpartial, uint32_t(wgrid), M.grad);
     RR_CHECK_LAUNCH(ctx);
     M.steps += 1;
     const float bc1 = 1.0f - std::pow(0.9f, float(M.steps));
@@ -689,7 +869,7 @@ rr_status rr_mlp_guide_train(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t 
                                                                g->desc.learning_rate, bc1, bc2);
     RR_CHECK_LAUNCH(ctx);
     RR_TRY_CUDA(ctx, cudaMemcpyAsync(M.loss_host, M.loss_partial, size_t(M.grid) * 4, cudaMemcpyDeviceToHost, stream));
-    ctx->launches += 8;
+    ctx->launches += 11;
     return RR_OK;
 }
 

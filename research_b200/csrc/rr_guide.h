@@ -58,8 +58,14 @@ struct rr_guide {
     unsigned long long* keys_out = nullptr;
     uint32_t* vals_in = nullptr;
     uint32_t* vals_out = nullptr;
-    void* sort_tmp = nullptr;
+    void* sort_tmp = nullptr;       // shared by the key sort and the chunk scan
     size_t sort_tmp_bytes = 0;
+    int key_bits = 64;              // sorted key bits: 32 (vertex id) + cell index bits
+    uint32_t* chunk_cnt = nullptr;  // per cell: EM chunks of its samples
+    uint32_t* chunk_off = nullptr;  // per cell: exclusive scan of chunk_cnt
+    uint32_t* chunk_cell = nullptr; // per chunk: its cell
+    double* chunk_partial = nullptr;// per chunk: 8 x (s0, s1.xyz) FP64 sums
+    size_t chunk_capacity = 0;
     // MLP
     rr_mlp_state* mlp = nullptr;
     float4* mlp_surf = nullptr;   // per queue slot: (pos, 1), (normal, valid), (wo, 0)

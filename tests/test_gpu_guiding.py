@@ -177,6 +177,66 @@ def test_grid_em_fits_and_is_deterministic(rr, ctx, torch_cuda):
     assert (mean_dir @ np.array([0, 0, 1.0])).min() > 0.9
 
 
+def _em_step_fp64(om, w):
+    """One EM update of a never-fitted cell in FP64: responsibilities under 8
+    kappa-2 lobes on the cube diagonals, then Banerjee's kappa and the
+    normalised lobe masses (the grid guide's update, restated)."""
+    k = 1 / np.sqrt(3.0)
+    mu0 = np.array([[k if j & 1 else -k, k if j & 2 else -k, k if j & 4 else -k] for j in range(8)])
+    kap0 = 2.0
+    pdf = kap0 * np.exp(kap0 * (om @ mu0.T - 1)) / (2 * np.pi * (1 - np.exp(-2 * kap0)))
+    gam = pdf / pdf.sum(1, keepdims=True)
+    r = w[:, None] * gam
+    s0 = r.sum(0)
+    s1 = r.T @ om
+    ln = np.linalg.norm(s1, axis=1)
+    rb = np.clip(ln / s0, 1e-4, 0.9999)
+    kappa = np.clip(rb * (3 - rb * rb) / (1 - rb * rb), 0.5, 512.0)
+    return s1 / ln[:, None], kappa, s0 / s0.sum()
+
+
+def test_grid_em_update_matches_fp64_restatement(rr, ctx, torch_cuda):
+    """One update of a 2^3 grid against the FP64 restatement, with cells of
+    very uneven sample counts (a few samples to 40k) so that the chunked
+    reduction runs with one and with many chunks per cell."""
+    torch = torch_cuda
+    rng = np.random.default_rng(21)
+    counts = [3, 17, 1000, 1025, 4096, 40000, 0, 250]
+    pos, om, w = [], [], []
+    for c, n in enumerate(counts):
+        lo = np.array([(c & 1) - 1.0, ((c >> 1) & 1) - 1.0, ((c >> 2) & 1) - 1.0])
+        pos.append(lo + rng.uniform(0.05, 0.95, (n, 3)))
+        axis = unit(rng.normal(size=3))
+        om.append(unit(axis + 0.6 * rng.normal(size=(n, 3))))
+        w.append(rng.uniform(0.1, 2.0, n))
+    pos, om, w = (np.concatenate(a) for a in (pos, om, w))
+    N = len(pos)
+    nrm = np.tile([0.0, 0.0, 1.0], (N, 1)); wo = nrm
+    g = make_guide(rr, ctx, rr.GUIDE_GRID, res=2, max_samples=1 << 16)
+    keep = set_samples(rr, ctx, torch, g, pos.astype(np.float32), om.astype(np.float32), w.astype(np.float32),
+                       nrm.astype(np.float32), wo.astype(np.float32))
+    ctx.check(rr.lib().rr_guide_update(ctx.handle, g, _stream(torch)))
+    st = rr.GuideStats()
+    ctx.check(rr.lib().rr_guide_get_stats(ctx.handle, g, C.byref(st)))
+    assert st.cells_valid == sum(1 for n in counts if n > 0)
+    start = 0
+    for c, n in enumerate(counts):
+        centre = np.array([[(c & 1) - 0.5, ((c >> 1) & 1) - 0.5, ((c >> 2) & 1) - 0.5]], np.float32)
+        mu, kappa, pi = eval_guide(rr, ctx, torch, g, centre, nrm[:1].astype(np.float32), wo[:1].astype(np.float32))
+        if n == 0:
+            assert pi.sum() == 0.0
+            continue
+        f32 = slice(start, start + n)
+        rmu, rk, rpi = _em_step_fp64(om[f32].astype(np.float32).astype(np.float64),
+                                     w[f32].astype(np.float32).astype(np.float64))
+        np.testing.assert_allclose(pi[0], rpi, rtol=2e-5, atol=1e-6)
+        np.testing.assert_allclose(mu[0], rmu, rtol=0, atol=2e-5)
+        np.testing.assert_allclose(kappa[0], rk, rtol=2e-4)
+        start += n
+    del keep
+    rr.lib().rr_guide_destroy(g)
+
+
 def _render(rr, ctx, torch, scene, cam, frames, guide=None, train=True, spp=1, bounces=5):
     W, H = cam.screen_width, cam.screen_height
     acc = np.zeros((H, W, 3))
