@@ -88,31 +88,53 @@ struct MlpView {
 };
 
 // W of every layer as the forward's B operand (out x 80), with the BF16 bias
-// in column kBiasCol(l) and zeros in the other columns past the inputs.
+// in column kBiasCol(l) and zeros in the other columns past the inputs. Each
+// thread issues 8 global loads before its 8 shared stores.
 __device__ void load_weights_fwd(unsigned char* sm, const MlpView& V) {
     #pragma unroll
     for (int l = 0; l < kLayers; ++l) {
         const int I = lin(l), O = lout(l);
         const unsigned short* src = reinterpret_cast<const unsigned short*>(V.w16 + hoff(l));
-        for (int e = threadIdx.x; e < O * kIn; e += blockDim.x) {
-            const int o = e / kIn, k = e % kIn;
-            unsigned short v = 0;
-            if (k == kBiasCol(l)) v = __bfloat16_as_ushort(__float2bfloat16_rn(V.params[boff(l) + o]));
-            else if (k < I) v = src[o * I + k];
-            *reinterpret_cast<unsigned short*>(sm + kSmFwdW + fwd_wtile(l) + tc::tile_offset(o, k, O)) = v;
+        for (int e0 = threadIdx.x; e0 < O * kIn; e0 += 8 * blockDim.x) {
+            unsigned short v[8];
+            #pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int e = e0 + u * blockDim.x, o = e / kIn, k = e % kIn;
+                v[u] = 0;
+                if (e < O * kIn) {
+                    if (k == kBiasCol(l)) v[u] = __bfloat16_as_ushort(__float2bfloat16_rn(V.params[boff(l) + o]));
+                    else if (k < I) v[u] = src[o * I + k];
+                }
+            }
+            #pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int e = e0 + u * blockDim.x, o = e / kIn, k = e % kIn;
+                if (e < O * kIn)
+                    *reinterpret_cast<unsigned short*>(sm + kSmFwdW + fwd_wtile(l) + tc::tile_offset(o, k, O)) = v[u];
+            }
         }
     }
 }
 
-// W^T of every layer as the backward's B operand.
+// W^T of every layer as the backward's B operand (8 loads in flight per thread).
 __device__ void load_weights_bwd(unsigned char* sm, const MlpView& V) {
     #pragma unroll
     for (int l = 0; l < kLayers; ++l) {
         const int I = lin(l), O = lout(l);
         const unsigned short* src = reinterpret_cast<const unsigned short*>(V.w16 + hoff(l));
-        for (int e = threadIdx.x; e < I * O; e += blockDim.x) {
-            const int o = e / I, i = e % I;
-            *reinterpret_cast<unsigned short*>(sm + kSmBwdWt + 2 * hoff(l) + tc::tile_offset(i, o, I)) = src[e];
+        for (int e0 = threadIdx.x; e0 < I * O; e0 += 8 * blockDim.x) {
+            unsigned short v[8];
+            #pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int e = e0 + u * blockDim.x;
+                v[u] = e < I * O ? src[e] : 0;
+            }
+            #pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int e = e0 + u * blockDim.x, o = e / I, i = e % I;
+                if (e < I * O)
+                    *reinterpret_cast<unsigned short*>(sm + kSmBwdWt + 2 * hoff(l) + tc::tile_offset(i, o, I)) = v[u];
+            }
         }
     }
 }
@@ -144,57 +166,73 @@ __device__ void encode(const MlpView& V, float3 p, float3 n, float3 wo, float* f
     f[78] = 0.0f; f[79] = 0.0f;
 }
 
-__device__ __forceinline__ float softplus(float x) { return x > 20.0f ? x : log1pf(expf(x)); }
-__device__ __forceinline__ float sigmoid(float x) { return 1.0f / (1.0f + expf(-x)); }
+// The head uses the fast intrinsics (__expf, __logf, rsqrtf, __fdividef):
+// the mixture only has to be the one the tracer samples and evaluates (its
+// pdf is computed from these same parameters), and the training gradient is
+// compared with the FP64 reference at BF16-level tolerances; IEEE-exact
+// exp/log/sqrt/division here cost thousands of instructions per query.
+__device__ __forceinline__ float softplus(float x) { return x > 20.0f ? x : __logf(1.0f + __expf(x)); }
+__device__ __forceinline__ float sigmoid(float x) {
+    return __fdividef(1.0f, 1.0f + __expf(-fminf(fmaxf(x, -80.0f), 80.0f)));
+}
 
 // Raw outputs -> mixture (mu, kappa, pi).
-__device__ void head_mixture(const float* r, float4* lobe, float* pi) {
-    float mxl = -1e30f;
-    for (int j = 0; j < kMaxLobes; ++j) mxl = fmaxf(mxl, r[5 * j + 4]);
+__device__ __forceinline__ void head_mixture(const float* r, float4* lobe, float* pi) {
+    float mxl = r[4];
+    #pragma unroll
+    for (int j = 1; j < kMaxLobes; ++j) mxl = fmaxf(mxl, r[5 * j + 4]);
     float z = 0.0f;
-    for (int j = 0; j < kMaxLobes; ++j) { pi[j] = expf(r[5 * j + 4] - mxl); z += pi[j]; }
+    #pragma unroll
+    for (int j = 0; j < kMaxLobes; ++j) { pi[j] = __expf(r[5 * j + 4] - mxl); z += pi[j]; }
+    const float iz = __fdividef(1.0f, z);   // z in [1, 8]
+    #pragma unroll
     for (int j = 0; j < kMaxLobes; ++j) {
-        pi[j] /= z;
+        pi[j] *= iz;
         const float vx = r[5 * j], vy = r[5 * j + 1], vz = r[5 * j + 2];
-        const float len = fmaxf(sqrtf(vx * vx + vy * vy + vz * vz), 1e-6f);
+        const float il = rsqrtf(fmaxf(vx * vx + vy * vy + vz * vz, 1e-12f));   // 1 / max(|v|, 1e-6)
         const float kappa = fminf(softplus(r[5 * j + 3]) + 0.1f, 1000.0f);
-        lobe[j] = make_float4(vx / len, vy / len, vz / len, kappa);
+        lobe[j] = make_float4(vx * il, vy * il, vz * il, kappa);
     }
 }
 
 // Weighted NLL of direction om under the mixture and its gradient w.r.t.
 // the 48 raw outputs (scaled by scale). Returns -log p.
-__device__ float head_grad(const float* r, float3 om, float scale, float* g) {
+__device__ __forceinline__ float head_grad(const float* r, float3 om, float scale, float* g) {
     float4 lobe[kMaxLobes];
     float pi[kMaxLobes], lq[kMaxLobes];
     head_mixture(r, lobe, pi);
     float lmax = -1e30f;
+    #pragma unroll
     for (int j = 0; j < kMaxLobes; ++j) {
         const float k = lobe[j].w;
         const float cosw = lobe[j].x * om.x + lobe[j].y * om.y + lobe[j].z * om.z;
-        const float lognorm = logf(k) - logf(6.28318530718f) - log1pf(-expf(-2.0f * k));
-        lq[j] = logf(fmaxf(pi[j], 1e-30f)) + lognorm + k * (cosw - 1.0f);
+        // log vMF normaliser: log k - log 2pi - log(1 - e^{-2k})   (k >= 0.1)
+        const float lognorm = __logf(k) - 1.83787706641f - __logf(1.0f - __expf(-2.0f * k));
+        lq[j] = __logf(fmaxf(pi[j], 1e-30f)) + lognorm + k * (cosw - 1.0f);
         lmax = fmaxf(lmax, lq[j]);
     }
     float s = 0.0f;
-    for (int j = 0; j < kMaxLobes; ++j) s += expf(lq[j] - lmax);
-    const float logp = lmax + logf(s);
+    #pragma unroll
+    for (int j = 0; j < kMaxLobes; ++j) s += __expf(lq[j] - lmax);
+    const float logp = lmax + __logf(s);
+    #pragma unroll
     for (int q = 0; q < kOut; ++q) g[q] = 0.0f;
+    #pragma unroll
     for (int j = 0; j < kMaxLobes; ++j) {
-        const float gam = expf(lq[j] - logp);
+        const float gam = __expf(lq[j] - logp);
         const float k = lobe[j].w;
         const float cosw = lobe[j].x * om.x + lobe[j].y * om.y + lobe[j].z * om.z;
         const float vx = r[5 * j], vy = r[5 * j + 1], vz = r[5 * j + 2];
-        const float len = fmaxf(sqrtf(vx * vx + vy * vy + vz * vz), 1e-6f);
+        const float il = rsqrtf(fmaxf(vx * vx + vy * vy + vz * vz, 1e-12f));
         // d(-log p)/dv = -(gam kappa / |v|) (om - (mu.om) mu)
-        const float cv = -gam * k / len;
+        const float cv = -gam * k * il;
         g[5 * j + 0] = scale * cv * (om.x - cosw * lobe[j].x);
         g[5 * j + 1] = scale * cv * (om.y - cosw * lobe[j].y);
         g[5 * j + 2] = scale * cv * (om.z - cosw * lobe[j].z);
-        // d(-log p)/dkappa = -gam (1/kappa - 2 e^{-2k}/(1 - e^{-2k}) + cos - 1)
-        const float e2 = expf(-2.0f * k);
-        float dk = -gam * (1.0f / k - 2.0f * e2 / (1.0f - e2) + cosw - 1.0f);
-        if (softplus(r[5 * j + 3]) + 0.1f > 1000.0f) dk = 0.0f;
+        // d(-log p)/dkappa = -gam (1/kappa - 2 e^{-2k}/(1 - e^{-2k}) + cos - 1); zero where kappa is clamped
+        const float e2 = __expf(-2.0f * k);
+        float dk = -gam * (__fdividef(1.0f, k) - __fdividef(2.0f * e2, 1.0f - e2) + cosw - 1.0f);
+        if (r[5 * j + 3] > 999.9f) dk = 0.0f;   // softplus(x) + 0.1 > 1000
         g[5 * j + 3] = scale * dk * sigmoid(r[5 * j + 3]);
         g[5 * j + 4] = scale * (pi[j] - gam);
     }
@@ -439,15 +477,16 @@ __global__ void __launch_bounds__(kTile, 3) mlp_backward_kernel(BwdArgs A) {
                 tc::fence_after_sync();
                 mma_chain(tmem, act_addr, wt_addr + 2 * hoff(l), O, I, bar);
             }
+            // X_l (the input of layer l >= 1) is ReLU(Z_{l-1}): its mask gates dZ_{l-1};
+            // the row is fetched while the chain runs
+            float xv[kHid];
+            if (valid) load_row_bf16(A.X + size_t(row) * kXCols + xoff(l), xv, I);
             wait_chain(bar, phase, ok);
             phase ^= 1u;
             float dx[kHid];
             tc::tmem_ld32_wait(tmem + (uint32_t(warp * 32) << 16), dx);
             tc::tmem_ld32_wait(tmem + (uint32_t(warp * 32) << 16) + 32, dx + 32);
             static_assert(kHid == 64, "dX is read as two 32-column loads");
-            // X_l (the input of layer l >= 1) is ReLU(Z_{l-1}): its mask gates dZ_{l-1}
-            float xv[kHid];
-            if (valid) load_row_bf16(A.X + size_t(row) * kXCols + xoff(l), xv, I);
             #pragma unroll
             for (int k = 0; k < I; ++k) dz[k] = (valid && xv[k] > 0.0f) ? dx[k] : 0.0f;
             if (valid) store_row_bf16(A.dZ + size_t(row) * kZCols + zoff(l - 1), dz, I);
@@ -487,7 +526,10 @@ constexpr int kSmWg = 2 * kWgStage + 64;
 static_assert(kSmWg <= 227 * 1024, "wgrad stages exceed shared memory");
 static_assert(kZCols <= 512 && zoff(kLayers) <= 304, "wgrad TMEM columns");
 
-__global__ void __launch_bounds__(kTile, 1) mlp_wgrad_kernel(const __nv_bfloat16* __restrict__ X,
+constexpr int kWgThreads = 256;                              // 8 warps; warps 0-3 also read TMEM
+constexpr int kWgGroups = (kXCols + kZCols) / 8;             // 8-column groups staged per step
+static_assert(kWgGroups % (kWgThreads / 32) == 0, "groups split evenly over the warps");
+__global__ void __launch_bounds__(kWgThreads, 1) mlp_wgrad_kernel(const __nv_bfloat16* __restrict__ X,
                                                             const __nv_bfloat16* __restrict__ dZ, uint32_t count,
                                                             float* __restrict__ partial, int* error) {
     extern __shared__ __align__(1024) unsigned char sm[];
@@ -498,9 +540,9 @@ __global__ void __launch_bounds__(kTile, 1) mlp_wgrad_kernel(const __nv_bfloat16
     const uint32_t s_begin = uint32_t((uint64_t(blockIdx.x) * steps) / gridDim.x);
     const uint32_t s_end = uint32_t((uint64_t(blockIdx.x + 1) * steps) / gridDim.x);
     // constant rows: zero everything, then the ones rows of both stages
-    for (int e = t; e < 2 * kWgStage / 16; e += kTile) reinterpret_cast<uint4*>(sm)[e] = make_uint4(0, 0, 0, 0);
+    for (int e = t; e < 2 * kWgStage / 16; e += kWgThreads) reinterpret_cast<uint4*>(sm)[e] = make_uint4(0, 0, 0, 0);
     __syncthreads();
-    for (int e = t; e < 2 * kLayers * (kWgStep / 2); e += kTile) {
+    for (int e = t; e < 2 * kLayers * (kWgStep / 2); e += kWgThreads) {
         const int stage = e / (kLayers * (kWgStep / 2));
         const int l = (e / (kWgStep / 2)) % kLayers;
         const int p = e % (kWgStep / 2);
@@ -518,26 +560,36 @@ __global__ void __launch_bounds__(kTile, 1) mlp_wgrad_kernel(const __nv_bfloat16
     for (uint32_t step = s_begin; step < s_end; ++step) {
         const uint32_t i = step - s_begin;
         const uint32_t buf = i & 1u;
-        if (i >= 2) wait_chain(bar + buf, ((i >> 1) - 1u) & 1u, ok);   // the MMAs of step i-2 are done
-        unsigned char* xb = sm + buf * kWgStage;
-        unsigned char* zb = xb + kWgBlkX;
-        // lane = sample pair (samples 2*lane, 2*lane+1 of the step); warp w takes feature groups w, w+4, ...
+        // lane = sample pair (samples 2*lane, 2*lane+1 of the step); warp w stages groups w, w+8, ...
+        // all of this thread's global loads are issued before it waits and stores
+        constexpr int kPer = kWgGroups / (kWgThreads / 32);
         const uint32_t s0 = step * kWgStep + 2 * lane, s1 = s0 + 1;
-        for (int g = warp; g < (kXCols + kZCols) / 8; g += 4) {
+        uint4 ra[kPer], rb[kPer];
+        #pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int g = warp + q * (kWgThreads / 32);
             const bool is_x = g < kXCols / 8;
             const int col = is_x ? g * 8 : (g - kXCols / 8) * 8;
             const __nv_bfloat16* base = is_x ? X : dZ;
             const size_t ld = is_x ? kXCols : kZCols;
-            uint4 a = make_uint4(0, 0, 0, 0), b = make_uint4(0, 0, 0, 0);
-            if (s0 < count) a = *reinterpret_cast<const uint4*>(base + size_t(s0) * ld + col);
-            if (s1 < count) b = *reinterpret_cast<const uint4*>(base + size_t(s1) * ld + col);
+            ra[q] = s0 < count ? *reinterpret_cast<const uint4*>(base + size_t(s0) * ld + col) : make_uint4(0, 0, 0, 0);
+            rb[q] = s1 < count ? *reinterpret_cast<const uint4*>(base + size_t(s1) * ld + col) : make_uint4(0, 0, 0, 0);
+        }
+        if (i >= 2) wait_chain(bar + buf, ((i >> 1) - 1u) & 1u, ok);   // the MMAs of step i-2 are done
+        unsigned char* xb = sm + buf * kWgStage;
+        unsigned char* zb = xb + kWgBlkX;
+        #pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int g = warp + q * (kWgThreads / 32);
+            const bool is_x = g < kXCols / 8;
+            const int col = is_x ? g * 8 : (g - kXCols / 8) * 8;
             int r0;
             unsigned char* blk;
             uint32_t lbo;
             if (is_x) {
                 int l = 0;
                 #pragma unroll
-                for (int q = 1; q < kLayers; ++q) l += col >= xoff(q) ? 1 : 0;
+                for (int u = 1; u < kLayers; ++u) l += col >= xoff(u) ? 1 : 0;
                 r0 = wg_row(l) + (col - xoff(l));
                 blk = xb;
                 lbo = kWgLboX;
@@ -547,12 +599,15 @@ __global__ void __launch_bounds__(kTile, 1) mlp_wgrad_kernel(const __nv_bfloat16
                 lbo = kWgLboZ;
             }
             unsigned char* dst = blk + (lane / 4) * lbo + r0 * 16 + (lane % 4) * 4;
-            const uint32_t wa[4] = {a.x, a.y, a.z, a.w}, wb[4] = {b.x, b.y, b.z, b.w};
-            #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                *reinterpret_cast<uint32_t*>(dst + (2 * j) * 16) = __byte_perm(wa[j], wb[j], 0x5410);
-                *reinterpret_cast<uint32_t*>(dst + (2 * j + 1) * 16) = __byte_perm(wa[j], wb[j], 0x7632);
-            }
+            const uint4 a4 = ra[q], b4 = rb[q];
+            *reinterpret_cast<uint32_t*>(dst + 0 * 16) = __byte_perm(a4.x, b4.x, 0x5410);
+            *reinterpret_cast<uint32_t*>(dst + 1 * 16) = __byte_perm(a4.x, b4.x, 0x7632);
+            *reinterpret_cast<uint32_t*>(dst + 2 * 16) = __byte_perm(a4.y, b4.y, 0x5410);
+            *reinterpret_cast<uint32_t*>(dst + 3 * 16) = __byte_perm(a4.y, b4.y, 0x7632);
+            *reinterpret_cast<uint32_t*>(dst + 4 * 16) = __byte_perm(a4.z, b4.z, 0x5410);
+            *reinterpret_cast<uint32_t*>(dst + 5 * 16) = __byte_perm(a4.z, b4.z, 0x7632);
+            *reinterpret_cast<uint32_t*>(dst + 6 * 16) = __byte_perm(a4.w, b4.w, 0x5410);
+            *reinterpret_cast<uint32_t*>(dst + 7 * 16) = __byte_perm(a4.w, b4.w, 0x7632);
         }
         tc::fence_proxy_async();
         tc::fence_before_sync();
@@ -578,7 +633,7 @@ __global__ void __launch_bounds__(kTile, 1) mlp_wgrad_kernel(const __nv_bfloat16
     float* dst = partial + size_t(blockIdx.x) * kParams;
     const int r = warp * 32 + lane;   // TMEM lane = row of dW^T = input feature (I = bias row)
     #pragma unroll
-    for (int l = 0; l < kLayers; ++l) {
+    for (int l = 0; l < kLayers && warp < 4; ++l) {
         const int I = lin(l), O = lout(l);
         #pragma unroll
         for (int c = 0; c < O; c += 16) {
@@ -858,7 +913,7 @@ rr_status rr_mlp_guide_train(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t 
     RR_CHECK_LAUNCH(ctx);
     const uint32_t wsteps = (B + kWgStep - 1) / kWgStep;
     const int wgrid = int(std::min<uint32_t>(wsteps, uint32_t(M.wg_grid)));
-    mlp_wgrad_kernel<<<wgrid, kTile, kSmWg, stream>>>(M.X, M.dZ, B, M.wpartial, M.error);
+    mlp_wgrad_kernel<<<wgrid, kWgThreads, kSmWg, stream>>>(M.X, M.dZ, B, M.wpartial, M.error);
     RR_CHECK_LAUNCH(ctx);
     mlp_reduce_kernel<<<(kParams + 255) / 256, 256, 0, stream>>>(M.wpartial, uint32_t(wgrid), M.grad);
     RR_CHECK_LAUNCH(ctx);
