@@ -377,14 +377,21 @@ __global__ void __launch_bounds__(kTile, 3) mlp_forward_kernel(FwdArgs A) {
                 *reinterpret_cast<uint4*>(act + tc::tile_offset(t, kHid + 8, kTile)) = make_uint4(0u, 0u, 0u, 0u);
             }
             if (l + 1 < kLayers) {
+                // ReLU in the BF16 conversion; the same words go to the activation
+                // tile and (training) to X. The chain that read the tile has
+                // completed (mbarrier), so each thread may overwrite its row; the
+                // barrier before the next chain orders every thread's TMEM reads
+                // before that chain's writes.
+                uint4* xrow = reinterpret_cast<uint4*>(A.X + size_t(row) * kXCols + xoff(l + 1));
                 #pragma unroll
-                for (int o = 0; o < O; ++o) out[o] = fmaxf(out[o], 0.0f);
-                // the chain that read the tile has completed (mbarrier), so each
-                // thread may overwrite its row; the barrier before the next chain
-                // orders every thread's TMEM reads before that chain's writes
-                #pragma unroll
-                for (int k = 0; k < O; k += 8) tc::st_row8(act, kTile, t, k, out + k);
-                if (Train && valid) store_row_bf16(A.X + size_t(row) * kXCols + xoff(l + 1), out, O);
+                for (int k = 0; k < O; k += 8) {
+                    const uint4 q = make_uint4(tc::pack_bf16_relu(out[k], out[k + 1]),
+                                               tc::pack_bf16_relu(out[k + 2], out[k + 3]),
+                                               tc::pack_bf16_relu(out[k + 4], out[k + 5]),
+                                               tc::pack_bf16_relu(out[k + 6], out[k + 7]));
+                    *reinterpret_cast<uint4*>(act + tc::tile_offset(t, k, kTile)) = q;
+                    if (Train && valid) xrow[k / 8] = q;
+                }
             }
         }
         if (valid) {

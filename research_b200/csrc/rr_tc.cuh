@@ -143,6 +143,15 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
     return *reinterpret_cast<const uint32_t*>(&v);
 }
 
+// As pack_bf16, with ReLU applied in the conversion (cvt.rn.relu.bf16x2.f32):
+// bf16(max(x, 0)) == max(bf16(x), 0), and the fused form keeps the epilogue
+// that feeds the next layer short.
+__device__ __forceinline__ uint32_t pack_bf16_relu(float a, float b) {
+    uint32_t d;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %2, %1;" : "=r"(d) : "f"(a), "f"(b));
+    return d;
+}
+
 // Stores 8 consecutive K values of row r (k0 multiple of 8) into a tile.
 __device__ __forceinline__ void st_row8(unsigned char* tile, uint32_t rows, uint32_t r, uint32_t k0, const float* v) {
     uint4 q;
