@@ -22,13 +22,18 @@ CUDA events; the RMSE evaluation is outside the timed region. Each method
 also keeps its even and odd frames in two accumulators, whose difference
 estimates its own MSE without the judge: s2_x = MSE(even, odd)/4.
 
-Time to target. The first time the judge-corrected relative RMSE
-sqrt(MSE(x,J) - s2_J) / mean(J) falls to --target is reported when it
-happens within --budget-s; otherwise (and always, as a second figure) the
-time is extrapolated from the final efficiency: an unbiased estimator's MSE
-falls as 1/t, so t_target = t * s2_x / (target * mean(J))^2.
+Time to target. The judge-corrected relative RMSE
+sqrt(MSE(x,J) - s2_J) / mean(J) is taken after every frame. Its samples are
+heavy-tailed (a rare bright path lifts the error long after it first dipped
+under the target), so the measured time is the one after which the error
+stays at or under --target up to the end of the --budget-s run
+(time_to_target_ms; the first dip is reported too). The time is also
+extrapolated from the run's efficiency: an unbiased estimator's MSE falls as
+1/t, so t_target = t * s2_x / (target * mean(J))^2, which uses the whole run
+(time_to_target_extrapolated_ms). learned_speedup_vs_grid is the grid's
+extrapolated time over the MLP's.
 
-    python bench_guiding.py [--target 0.01 --budget-s 20 --judge-spp 1048576]
+    python bench_guiding.py [--target 0.01 --budget-s 15 --judge-spp 2097152]
 """
 import argparse
 import ctypes as C
@@ -50,9 +55,9 @@ def main():
     ap.add_argument("--view-height", type=int, default=1080)
     ap.add_argument("--spp", type=int, default=256, help="samples per pixel per frame")
     ap.add_argument("--bounces", type=int, default=5)
-    ap.add_argument("--judge-spp", type=int, default=1 << 20)
+    ap.add_argument("--judge-spp", type=int, default=1 << 21)
     ap.add_argument("--target", type=float, default=0.01)
-    ap.add_argument("--budget-s", type=float, default=20.0, help="device-time budget per method")
+    ap.add_argument("--budget-s", type=float, default=15.0, help="device-time budget per method")
     ap.add_argument("--triangles", type=int, default=1_000_000)
     ap.add_argument("--methods", default="unguided,grid,mlp")
     ap.add_argument("--mlp-batch", type=int, default=1 << 18)
@@ -127,6 +132,7 @@ def main():
         par = [torch.zeros((H, W, 4), device="cuda") for _ in range(2)]
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         elapsed_ms, frame, reached, curve = 0.0, 0, None, []
+        stable = None   # (ms, spp) of the first frame of the final run of frames at or under the target
         next_log = 1
         while elapsed_ms < args.budget_s * 1e3:
             e0.record()
@@ -145,8 +151,13 @@ def main():
             if frame >= next_log:
                 curve.append((round(elapsed_ms, 1), frame * spp, round(math.sqrt(max(corrected, 0.0)) / judge_mean, 5)))
                 next_log *= 2
-            if reached is None and frame >= 4 and corrected <= target_mse:
-                reached = (elapsed_ms, frame * spp)
+            if frame >= 4 and corrected <= target_mse:
+                if reached is None:
+                    reached = (elapsed_ms, frame * spp)
+                if stable is None:
+                    stable = (elapsed_ms, frame * spp)
+            else:
+                stable = None
         x = acc[..., :3].double()
         ok = finite & torch.isfinite(x).all(-1)
         bad = int((~ok).sum())
@@ -161,8 +172,9 @@ def main():
                      "loss": round(st.last_loss, 4)}
             L.rr_guide_destroy(guide)
         results[method] = {
-            "time_to_target_ms": round(reached[0], 1) if reached else None,
-            "spp_to_target": reached[1] if reached else None,
+            "time_to_target_ms": round(stable[0], 1) if stable else None,
+            "spp_to_target": stable[1] if stable else None,
+            "first_under_target_ms": round(reached[0], 1) if reached else None,
             "time_to_target_extrapolated_ms": round(elapsed_ms * s2_x / target_mse, 1),
             "final_rel_rmse_vs_judge": round(math.sqrt(max(corrected, 0.0)) / judge_mean, 5),
             "final_rel_rmse_self": round(math.sqrt(s2_x) / judge_mean, 5),
@@ -184,8 +196,8 @@ def main():
             "judge": {"mean": round(judge_mean, 5), "rel_rmse_own": round(math.sqrt(s2_J) / judge_mean, 5),
                       "seconds": round(judge_s, 1), "nonfinite_pixels": int((~finite).sum())},
             "results": results,
-            "grid_over_mlp_time": ratio("grid", "mlp", "time_to_target_ms"),
-            "grid_over_mlp_time_extrapolated": ratio("grid", "mlp", "time_to_target_extrapolated_ms")}
+            "learned_speedup_vs_grid": ratio("grid", "mlp", "time_to_target_extrapolated_ms"),
+            "learned_speedup_vs_grid_measured": ratio("grid", "mlp", "time_to_target_ms")}
     print(json.dumps(line), flush=True)
     scene.close()
     ctx.close()
