@@ -276,6 +276,70 @@ rr_status rr_guiding_sample(rr_ctx* ctx, const float* fitted, const float* pos,
 rr_status rr_guiding_reset(rr_ctx* ctx, int32_t* accum, float* fitted,
                            const rr_guiding_params* params, void* stream);
 
+/* ── ReSTIR PT: ReSTIRPTPass::execute (ReSTIRPTPass.cpp:529-812; kernels in
+ * passes/restir_pt/restir_pt.slang) ──────────────────────────────────────
+ * rr_restir_pt_params holds the ReSTIRPTPushConstants fields
+ * (ReSTIRPTPass.cpp:34-83) other than the bindless indices; the guiding
+ * fields are an rr_guiding_params (guiding_enable -> enabled, guiding_alpha ->
+ * alpha). Reference defaults (ReSTIRPTPass.h:86-100) in comments. */
+typedef struct rr_restir_pt_params {
+    uint32_t frame_seed;               /* frame_count_++ */
+    uint32_t num_initial_candidates;   /* 8 */
+    uint32_t max_bounces;              /* 4 */
+    uint32_t temporal_enable;          /* 1 */
+    uint32_t spatial_enable;           /* 1 */
+    uint32_t spatial_num_neighbors;    /* 4 */
+    uint32_t spatial_radius;           /* 12 */
+    uint32_t include_direct_lighting;  /* 1 */
+    float    indirect_strength;        /* 1.0 */
+    float    ray_bias;                 /* 1e-3 */
+    uint32_t _pad[2];
+    rr_guiding_params guiding;         /* enabled 1, alpha 0.5, 0.10 / 0.02, 1 << 20 cells, 8, 512 */
+} rr_restir_pt_params;
+
+/* The pass's images, every one width x height RGBA32F (float4 per pixel),
+ * device memory owned by the caller. The reservoir is four images
+ * (restir_pt.slang:10-25): [0] (rc_pos, w_sum), [1] (rc_normal, asfloat(M)),
+ * [2] (suffix radiance, W), [3] (prefix throughput, valid); the primary
+ * history is (position, t) and (normal, asfloat(material)). "curr" and "prev"
+ * swap after every frame, as ReSTIRPTPass::execute flips reservoir_flip_. */
+typedef struct rr_restir_pt_images {
+    const float* gbuf_pos;        /* ReSTIR DI's G-buffer (restir_di.slang:212-223) */
+    const float* gbuf_norm;
+    const float* direct;          /* direct lighting to add (the DI output) or NULL */
+    float*       reservoir_curr[4];
+    float*       reservoir_prev[4];
+    float*       history_curr[2];
+    float*       history_prev[2];
+    float*       output;
+    int32_t*     guiding_accum;   /* guiding.cell_count x int32 x 4 */
+    float*       guiding_fitted;  /* guiding.cell_count x float x 4 */
+} rr_restir_pt_images;
+
+/* cs_initial (restir_pt.slang:567-757). */
+rr_status rr_restir_pt_initial(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
+                               const rr_restir_pt_params* params, const rr_restir_pt_images* images,
+                               void* stream);
+/* cs_temporal (restir_pt.slang:760-857); returns at once when temporal_enable is 0. */
+rr_status rr_restir_pt_temporal(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
+                                const rr_restir_pt_params* params, const rr_restir_pt_images* images,
+                                void* stream);
+/* cs_spatial_shade (restir_pt.slang:860-1000), including the guiding splat. */
+rr_status rr_restir_pt_spatial_shade(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
+                                     const rr_restir_pt_params* params,
+                                     const rr_restir_pt_images* images, void* stream);
+/* The dispatches of one ReSTIRPTPass::execute in order: initial, temporal,
+ * spatial shade, and cs_fit_guiding when guiding is enabled. The caller swaps
+ * curr and prev afterwards. */
+rr_status rr_restir_pt_execute(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
+                               const rr_restir_pt_params* params, const rr_restir_pt_images* images,
+                               void* stream);
+/* History reset (ReSTIRPTPass.cpp:616-652, consume_history_dirty): the prev
+ * reservoir images to zero, the prev history position to (0, 0, 0, -1) and
+ * normal to zero. */
+rr_status rr_restir_pt_reset_history(rr_ctx* ctx, const rr_restir_pt_images* images, uint32_t width,
+                                     uint32_t height, void* stream);
+
 /* ── guided path tracing (no reference counterpart beyond the hash grid
  * above: the reference guides only ReSTIR PT's primary bounce with one vMF
  * lobe per hashed cell, restir_pt.slang:520-563). A guide predicts a mixture

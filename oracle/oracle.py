@@ -29,6 +29,20 @@ class GuidingParams(C.Structure):
                 ("min_samples", U32), ("kappa_max", F32), ("alpha", F32), ("_pad", U32)]
 
 
+class PtReuseParams(C.Structure):
+    """OracleRestirPtParams (ReSTIRPTPushConstants minus the bindless indices)."""
+    _fields_ = [("frame_seed", U32), ("num_initial_candidates", U32), ("max_bounces", U32),
+                ("temporal_enable", U32), ("spatial_enable", U32), ("spatial_num_neighbors", U32),
+                ("spatial_radius", U32), ("include_direct_lighting", U32), ("indirect_strength", F32),
+                ("ray_bias", F32), ("_pad", U32 * 2), ("guiding", GuidingParams)]
+
+
+class PtReuseImages(C.Structure):
+    _fields_ = [("gbuf_pos", P), ("gbuf_norm", P), ("direct", P), ("reservoir_curr", P * 4),
+                ("reservoir_prev", P * 4), ("history_curr", P * 2), ("history_prev", P * 2), ("output", P),
+                ("guiding_accum", P), ("guiding_fitted", P)]
+
+
 _SIG = {
     "oracle_pcg_hash": (U32, [U32]),
     "oracle_make_seed": (U32, [U32, U32, U32]),
@@ -53,6 +67,9 @@ _SIG = {
     "oracle_brdf_eval": (None, [P, P, P, P, F32, F32, P]),
     "oracle_brdf_sample": (None, [P, P, P, F32, F32, F32, F32, P, P, P]),
     "oracle_brdf_pdf": (F32, [P, P, P, F32]),
+    "oracle_restir_pt_initial": (None, [P, P, C.POINTER(PtReuseParams), C.POINTER(PtReuseImages), I]),
+    "oracle_restir_pt_temporal": (None, [P, P, C.POINTER(PtReuseParams), C.POINTER(PtReuseImages), I]),
+    "oracle_restir_pt_spatial_shade": (None, [P, P, C.POINTER(PtReuseParams), C.POINTER(PtReuseImages), I]),
 }
 
 _lib = None
@@ -187,6 +204,39 @@ def restir_di_temporal(scene, cam, p, gpos, gnrm, res, prev, nthreads=None):
 def restir_di_spatial_shade(scene, cam, p, gpos, gnrm, res, out, nthreads=None):
     lib().oracle_restir_di_spatial_shade(scene.handle, _cam_ptr(cam), C.byref(p), _p(gpos), _p(gnrm), _p(res),
                                          _p(out), nthreads or threads())
+
+
+def pt_reuse_params(frame_seed=0, candidates=8, max_bounces=4, temporal=1, spatial=1, neighbors=4, radius=12,
+                    include_direct=1, indirect_strength=1.0, ray_bias=1e-3, gp=None):
+    """ReSTIRPTPass.h:86-100 defaults; gp = guiding_params(...)."""
+    return PtReuseParams(frame_seed, candidates, max_bounces, temporal, spatial, neighbors, radius, include_direct,
+                         indirect_strength, ray_bias, (U32 * 2)(0, 0), gp if gp is not None else guiding_params())
+
+
+def pt_reuse_images(img: dict) -> PtReuseImages:
+    """img: gbuf_pos, gbuf_norm, direct (or None), res_curr[4], res_prev[4], hist_curr[2], hist_prev[2], output,
+    accum, fitted — C-contiguous float32 (H, W, 4) images, int32 / float32 (cells, 4) grids."""
+    def ptr(a):
+        return None if a is None else _p(a)
+    return PtReuseImages(ptr(img["gbuf_pos"]), ptr(img["gbuf_norm"]), ptr(img.get("direct")),
+                         (P * 4)(*[ptr(a) for a in img["res_curr"]]), (P * 4)(*[ptr(a) for a in img["res_prev"]]),
+                         (P * 2)(*[ptr(a) for a in img["hist_curr"]]), (P * 2)(*[ptr(a) for a in img["hist_prev"]]),
+                         ptr(img["output"]), ptr(img["accum"]), ptr(img["fitted"]))
+
+
+def restir_pt_initial(scene, cam, p, img, nthreads=None):
+    lib().oracle_restir_pt_initial(scene.handle, _cam_ptr(cam), C.byref(p), C.byref(pt_reuse_images(img)),
+                                   nthreads or threads())
+
+
+def restir_pt_temporal(scene, cam, p, img, nthreads=None):
+    lib().oracle_restir_pt_temporal(scene.handle, _cam_ptr(cam), C.byref(p), C.byref(pt_reuse_images(img)),
+                                    nthreads or threads())
+
+
+def restir_pt_spatial_shade(scene, cam, p, img, nthreads=None):
+    lib().oracle_restir_pt_spatial_shade(scene.handle, _cam_ptr(cam), C.byref(p), C.byref(pt_reuse_images(img)),
+                                         nthreads or threads())
 
 
 def atrous_iteration(inp, gpos, gnrm, out, stride, sp=0.25, sn=0.20, sl=1.0, nthreads=None):

@@ -572,6 +572,158 @@ float vmf_pdf(V3 mu, float kappa, V3 dir) {
     return k * rr_expf(k * (w - 1.0f)) / fmaxs(denom, 1.0e-8f);
 }
 
+// sample_primary_dir (restir_pt.slang:520-563)
+V3 sample_primary_dir(const float* fitted, V3 p, V3 nn, uint32_t bsdf, V3 cam, const OracleGuidingParams& gp,
+                      uint32_t& seed, float& src_pdf) {
+    float alpha = 0.0f;
+    bool valid = false;
+    V3 mu = v3(0, 0, 0);
+    float kappa = 0.0f;
+    if (gp.enabled != 0u && gp.alpha > 0.0f) {
+        uint32_t cell = cell_index(p, bsdf, cam, gp);
+        const float* f = fitted + (size_t)cell * 4;
+        mu = v3(f[0], f[1], f[2]);
+        kappa = f[3];
+        valid = (kappa > 0.0f) && (dot(mu, mu) > 0.25f);   // guiding_load_lobe, GuidingGrid.slang:140-157
+        if (valid) alpha = gp.alpha;
+    }
+    V3 T, B;
+    build_onb(nn, T, B);
+    V3 wi;
+    if (rand_float(seed) < alpha) {
+        float ux = rand_float(seed);   // rand_float2: x then y
+        float uy = rand_float(seed);
+        float vpdf;
+        wi = vmf_sample(mu, kappa, ux, uy, vpdf);
+    } else {
+        float u0 = rand_float(seed);   // arguments evaluate left to right
+        float u1 = rand_float(seed);
+        float cpdf;
+        V3 local = sample_cosine_hemisphere(u0, u1, cpdf);
+        wi = tangent_to_world(local, T, B, nn);
+    }
+    float cos_i = dot(nn, wi);
+    float p_cos = (cos_i > 0.0f) ? (cos_i * kInvPi) : 0.0f;
+    float p_vmf = valid ? vmf_pdf(mu, kappa, wi) : 0.0f;
+    src_pdf = alpha * p_vmf + (1.0f - alpha) * p_cos;
+    return wi;
+}
+
+// ── ReSTIR PT (restir_pt.slang) ────────────────────────────────────────────
+struct PtRes {   // Reservoir (restir_pt.slang:231-261)
+    V3 rc_pos, rc_normal, suffix_rad, prefix_thp;
+    float w_sum, W;
+    uint32_t M;
+    float valid;
+};
+inline PtRes pt_load(float* const* img, size_t px) {
+    const float* p = img[0] + 4 * px; const float* n = img[1] + 4 * px;
+    const float* r = img[2] + 4 * px; const float* e = img[3] + 4 * px;
+    PtRes res;
+    res.rc_pos = load3(p); res.w_sum = p[3];
+    res.rc_normal = load3(n); res.M = asuint(n[3]);
+    res.suffix_rad = load3(r); res.W = r[3];
+    res.prefix_thp = load3(e); res.valid = e[3];
+    return res;
+}
+inline void put4(float* d, V3 v, float w) { d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = w; }
+inline void pt_store(float* const* img, size_t px, const PtRes& r) {
+    put4(img[0] + 4 * px, r.rc_pos, r.w_sum);
+    put4(img[1] + 4 * px, r.rc_normal, asfloat(r.M));
+    put4(img[2] + 4 * px, r.suffix_rad, r.W);
+    put4(img[3] + 4 * px, r.prefix_thp, r.valid);
+}
+inline void pt_store_empty(float* const* img, size_t px) {   // write_empty_reservoir (:223-229)
+    put4(img[0] + 4 * px, v3(0, 0, 0), 0.0f);
+    put4(img[1] + 4 * px, v3(0, 0, 0), asfloat(0u));
+    put4(img[2] + 4 * px, v3(0, 0, 0), 0.0f);
+    put4(img[3] + 4 * px, v3(0, 0, 0), 0.0f);
+}
+inline float rsqrt_hlsl(float x) { return 1.0f / sqrtf(x); }   // restated as 1 / sqrt, both correctly rounded
+inline float frac_hlsl(float x) { return x - floorf(x); }
+inline float luminance709(V3 c) { return dot(c, v3(0.2126f, 0.7152f, 0.0722f)); }   // :161-164
+
+// load_surface_from_images (:287-305)
+bool pt_surface(const OracleScene& s, const float* pos_img, const float* nrm_img, size_t px, V3& pos, V3& n,
+                uint32_t& mat) {
+    const float* p4 = pos_img + 4 * px;
+    const float* n4 = nrm_img + 4 * px;
+    if (p4[3] < 0.0f) return false;
+    pos = load3(p4);
+    n = normalize(load3(n4));
+    mat = asuint(n4[3]);
+    return mat < s.materials.size();
+}
+
+// sample_lights (:172-221)
+V3 pt_sample_lights(const OracleScene& s, V3 hit_pos, V3 normal, V3 wo, const GpuMaterial& mat, float bias,
+                    uint32_t& seed) {
+    const uint32_t N = (uint32_t)s.lights.size();
+    if (N == 0) return v3(0, 0, 0);
+    uint32_t light_idx = uint32_t(rand_float(seed) * float(N)) % N;
+    const GpuLight& light = s.lights[light_idx];
+    V3 light_dir; float dist; float pdf_light;
+    if (light.type == 0) {
+        V3 to_light = load3(light.position) - hit_pos;
+        dist = length(to_light);
+        light_dir = to_light / fmaxs(dist, 1e-6f);
+        pdf_light = dist * dist;
+    } else {
+        light_dir = normalize(-load3(light.direction));
+        dist = 1e9f;
+        pdf_light = 1.0f;
+    }
+    if (dot(light_dir, normal) <= 0.0f) return v3(0, 0, 0);
+    Hit sh = trace_scene<true>(s, hit_pos + normal * bias, light_dir, bias, dist - 0.01f);
+    if (sh.hit) return v3(0, 0, 0);
+    V3 brdf_val = brdf_eval(normal, wo, light_dir, load3(mat.base_color), mat.metallic, mat.roughness);
+    float n_dot_l = fmaxs(dot(normal, light_dir), 0.0f);
+    float denom = light.type == 0 ? (pdf_light + 1e-6f) : 1.0f;
+    V3 irradiance = v3(light.emission[0] * light.intensity / denom, light.emission[1] * light.intensity / denom,
+                       light.emission[2] * light.intensity / denom);
+    float pdf_bsdf = brdf_pdf(wo, light_dir, normal, mat.roughness);
+    float mis_weight = (light.type == 0) ? 1.0f
+                                         : (pdf_light * pdf_light) / (pdf_light * pdf_light + pdf_bsdf * pdf_bsdf + 1e-10f);
+    return brdf_val * irradiance * n_dot_l * mis_weight * float(N);
+}
+
+// evaluate_contribution / target_function (:474-503)
+V3 pt_contribution(V3 pp, V3 pn, const GpuMaterial& pm, V3 cam, const PtRes& r) {
+    V3 to_rc = r.rc_pos - pp;
+    float dist2 = dot(to_rc, to_rc);
+    if (dist2 <= 1e-8f) return v3(0, 0, 0);
+    V3 wi = to_rc * rsqrt_hlsl(dist2);
+    float cos_x = fmaxs(dot(pn, wi), 0.0f);
+    if (cos_x <= 0.0f) return v3(0, 0, 0);
+    V3 wo = normalize(cam - pp);
+    V3 brdf_val = brdf_eval(pn, wo, wi, load3(pm.base_color), pm.metallic, pm.roughness);
+    return brdf_val * cos_x * r.prefix_thp * r.suffix_rad;
+}
+float pt_target(V3 pp, V3 pn, const GpuMaterial& pm, V3 cam, const PtRes& r) {
+    return luminance709(pt_contribution(pp, pn, pm, cam, r));
+}
+
+// reconnection_jacobian (:437-457)
+float pt_jacobian(V3 src, V3 tgt, V3 rc_pos, V3 rc_n) {
+    V3 sd = rc_pos - src, td = rc_pos - tgt;
+    float sd2 = dot(sd, sd), td2 = dot(td, td);
+    if (sd2 <= 1e-8f || td2 <= 1e-8f) return 0.0f;
+    V3 sdir = sd * rsqrt_hlsl(sd2), tdir = td * rsqrt_hlsl(td2);
+    float scos = fabsf(dot(rc_n, -sdir)), tcos = fabsf(dot(rc_n, -tdir));
+    if (scos <= 0.05f || tcos <= 0.05f) return 0.0f;
+    float j = (tcos * sd2) / (scos * td2);
+    return clampf(j, 0.0f, 3.0f);
+}
+
+// trace_visibility (:459-469)
+bool pt_visible(const OracleScene& s, V3 origin, V3 normal, V3 target, float bias) {
+    V3 delta = target - origin;
+    float dist = length(delta);
+    if (dist <= bias) return false;
+    V3 dir = delta / dist;
+    return !trace_scene<true>(s, origin + normal * bias, dir, bias, dist - bias).hit;
+}
+
 } // namespace
 
 // ═══════════════════════════════ C API ═════════════════════════════════════
@@ -977,41 +1129,11 @@ void oracle_guiding_fit(int32_t* accum, float* fitted, const OracleGuidingParams
 void oracle_guiding_sample(const float* fitted, const float* pos, const float* normal,
                            const uint32_t* bsdf, uint32_t* seeds, size_t n, const float cam_pos[3],
                            const OracleGuidingParams* gp, float* wi_out, float* pdf_out) {
-    // sample_primary_dir (restir_pt.slang:520-563)
     for (size_t i = 0; i < n; ++i) {
-        V3 p = load3(pos + 4 * i), nn = load3(normal + 4 * i);
         uint32_t seed = seeds[i];
-        float alpha = 0.0f;
-        bool valid = false;
-        V3 mu = v3(0, 0, 0);
-        float kappa = 0.0f;
-        if (gp->enabled != 0u && gp->alpha > 0.0f) {
-            uint32_t cell = cell_index(p, bsdf[i], load3(cam_pos), *gp);
-            const float* f = fitted + (size_t)cell * 4;
-            mu = v3(f[0], f[1], f[2]);
-            kappa = f[3];
-            valid = (kappa > 0.0f) && (dot(mu, mu) > 0.25f);
-            if (valid) alpha = gp->alpha;
-        }
-        V3 T, B;
-        build_onb(nn, T, B);
-        V3 wi;
-        if (rand_float(seed) < alpha) {
-            float ux = rand_float(seed);
-            float uy = rand_float(seed);
-            float vpdf;
-            wi = vmf_sample(mu, kappa, ux, uy, vpdf);
-        } else {
-            float u0 = rand_float(seed);  // arguments evaluate left to right
-            float u1 = rand_float(seed);
-            float cpdf;
-            V3 local = sample_cosine_hemisphere(u0, u1, cpdf);
-            wi = tangent_to_world(local, T, B, nn);
-        }
-        float cos_i = dot(nn, wi);
-        float p_cos = (cos_i > 0.0f) ? (cos_i * kInvPi) : 0.0f;
-        float p_vmf = valid ? vmf_pdf(mu, kappa, wi) : 0.0f;
-        float src_pdf = alpha * p_vmf + (1.0f - alpha) * p_cos;
+        float src_pdf;
+        V3 wi = sample_primary_dir(fitted, load3(pos + 4 * i), load3(normal + 4 * i), bsdf[i], load3(cam_pos), *gp,
+                                   seed, src_pdf);
         wi_out[4 * i] = wi.x; wi_out[4 * i + 1] = wi.y; wi_out[4 * i + 2] = wi.z; wi_out[4 * i + 3] = 0.0f;
         pdf_out[i] = src_pdf;
         seeds[i] = seed;
@@ -1038,6 +1160,260 @@ void oracle_brdf_sample(const float wo[3], const float n[3], const float base[3]
 
 float oracle_brdf_pdf(const float wo[3], const float wi[3], const float n[3], float roughness) {
     return brdf_pdf(load3(wo), load3(wi), load3(n), roughness);
+}
+
+// ── ReSTIR PT (restir_pt.slang:567-1000; ReSTIRPTPass.cpp:529-812) ────────────
+void oracle_restir_pt_initial(const OracleScene* scene, const GpuCameraData* cam, const OracleRestirPtParams* p,
+                              const OracleRestirPtImages* img, int threads) {
+    const OracleScene& s = *scene;
+    const uint32_t W = cam->screen_width, H = cam->screen_height;
+    const V3 cp = load3(cam->position);
+    const float bias = p->ray_bias;
+    parallel_rows(H, threads, [&](uint32_t y) {
+        for (uint32_t x = 0; x < W; ++x) {
+            const size_t px = (size_t)y * W + x;
+            uint32_t seed = make_seed(x, y, p->frame_seed);
+            V3 pp, pn; uint32_t pmat;
+            if (!pt_surface(s, img->gbuf_pos, img->gbuf_norm, px, pp, pn, pmat)) {
+                put4(img->history_curr[0] + 4 * px, v3(0, 0, 0), -1.0f);
+                put4(img->history_curr[1] + 4 * px, v3(0, 0, 0), 0.0f);
+                pt_store_empty(img->reservoir_curr, px);
+                continue;
+            }
+            memcpy(img->history_curr[0] + 4 * px, img->gbuf_pos + 4 * px, 16);
+            memcpy(img->history_curr[1] + 4 * px, img->gbuf_norm + 4 * px, 16);
+            const GpuMaterial& pm = s.materials[pmat];
+            PtRes selected{v3(0, 0, 0), v3(0, 0, 0), v3(0, 0, 0), v3(0, 0, 0), 0.0f, 0.0f, 0u, 0.0f};
+            float w_sum = 0.0f;
+            uint32_t M_count = 0;
+            const uint32_t max_b = std::max(p->max_bounces, 1u);
+            for (uint32_t c = 0; c < p->num_initial_candidates; ++c) {
+                float src_pdf;
+                V3 wi0 = sample_primary_dir(img->guiding_fitted, pp, pn, pmat, cp, p->guiding, seed, src_pdf);
+                if (src_pdf <= 1e-6f || dot(pn, wi0) <= 0.0f) continue;
+                Hit rh = trace_scene<false>(s, pp + pn * bias, wi0, bias, 1e9f);
+                if (!rh.hit) continue;
+                Surf rc = hit_surface(s, rh);
+                V3 rc_n = rc.normal;
+                if (dot(rc_n, wi0) > 0.0f) rc_n = -rc_n;
+                const GpuMaterial& rm = s.materials[rc.material];
+                V3 suffix = load3(rm.emissive);
+                V3 rc_wo = -wi0;
+                suffix = suffix + pt_sample_lights(s, rc.pos, rc_n, rc_wo, rm, bias, seed);
+                V3 cur_pos = rc.pos, cur_n = rc_n, cur_wo = rc_wo;
+                const GpuMaterial* cur_mat = &rm;
+                V3 path_thp = v3(1, 1, 1);
+                for (uint32_t b = 1; b < max_b; ++b) {
+                    float u0 = rand_float(seed);   // rand_float2: x then y
+                    float u1 = rand_float(seed);
+                    V3 wi; float pdf;
+                    V3 f = brdf_sample(cur_wo, cur_n, load3(cur_mat->base_color), cur_mat->metallic,
+                                       cur_mat->roughness, u0, u1, wi, pdf);
+                    if (pdf <= 1e-6f || dot(cur_n, wi) <= 0.0f) break;
+                    float cos_at = fmaxs(dot(cur_n, wi), 0.0f);
+                    path_thp = path_thp * (f * cos_at / pdf);
+                    if (fmaxs(path_thp.x, fmaxs(path_thp.y, path_thp.z)) <= 0.0f) break;
+                    Hit hb = trace_scene<false>(s, cur_pos + cur_n * bias, wi, bias, 1e9f);
+                    if (!hb.hit) { suffix = suffix + path_thp * sky(wi); break; }
+                    Surf hs = hit_surface(s, hb);
+                    V3 hn = hs.normal;
+                    if (dot(hn, wi) > 0.0f) hn = -hn;
+                    const GpuMaterial& hm = s.materials[hs.material];
+                    V3 hwo = -wi;
+                    suffix = suffix + path_thp * pt_sample_lights(s, hs.pos, hn, hwo, hm, bias, seed);
+                    cur_pos = hs.pos; cur_n = hn; cur_mat = &hm; cur_wo = hwo;
+                }
+                PtRes cand{rc.pos, rc_n, suffix, v3(1, 1, 1), 0.0f, 0.0f, 1u, 1.0f};
+                float p_hat = pt_target(pp, pn, pm, cp, cand);
+                if (p_hat <= 0.0f) continue;
+                V3 delta = rc.pos - pp;
+                if (dot(delta, delta) <= 1e-8f) continue;
+                float weight = p_hat / fmaxs(src_pdf, 1e-6f);
+                w_sum += weight;
+                M_count++;
+                if (w_sum > 0.0f && rand_float(seed) < weight / w_sum) selected = cand;
+            }
+            bool stored = false;
+            if (M_count > 0 && selected.valid > 0.5f) {
+                float p_hat = pt_target(pp, pn, pm, cp, selected);
+                if (p_hat > 1e-10f) {
+                    selected.M = M_count;
+                    selected.w_sum = w_sum;
+                    selected.W = w_sum / (float(M_count) * p_hat);
+                    pt_store(img->reservoir_curr, px, selected);
+                    stored = true;
+                }
+            }
+            if (!stored) pt_store_empty(img->reservoir_curr, px);
+        }
+    });
+}
+
+void oracle_restir_pt_temporal(const OracleScene* scene, const GpuCameraData* cam, const OracleRestirPtParams* p,
+                               const OracleRestirPtImages* img, int threads) {
+    if (!p->temporal_enable) return;
+    const OracleScene& s = *scene;
+    const uint32_t W = cam->screen_width, H = cam->screen_height;
+    const V3 cp = load3(cam->position);
+    const uint32_t m_cap = std::min(std::max(20u * p->num_initial_candidates, 1u), 8192u);
+    parallel_rows(H, threads, [&](uint32_t y) {
+        for (uint32_t x = 0; x < W; ++x) {
+            const size_t px = (size_t)y * W + x;
+            V3 pp, pn; uint32_t pmat;
+            if (!pt_surface(s, img->gbuf_pos, img->gbuf_norm, px, pp, pn, pmat)) continue;
+            const GpuMaterial& pm = s.materials[pmat];
+            // reproject_to_prev_pixel (:326-340)
+            V4 clip = mul44(cam->prev_view_proj, V4{pp.x, pp.y, pp.z, 1.0f});
+            if (clip.w <= 1.0e-6f) continue;
+            float nx = clip.x / clip.w, ny = clip.y / clip.w;
+            if (fabsf(nx) > 1.0f || fabsf(ny) > 1.0f) continue;
+            float fx = (nx * 0.5f + 0.5f) * float(W) - 0.5f;
+            float fy = (ny * 0.5f + 0.5f) * float(H) - 0.5f;
+            int cx = (int)floorf(fx + 0.5f), cy = (int)floorf(fy + 0.5f);
+            if (cx < 0 || cy < 0 || cx >= (int)W || cy >= (int)H) continue;
+            // find_reprojected_history_surface (:355-409)
+            bool found = false;
+            float best = 1e30f;
+            size_t hist = 0;
+            V3 hpos = v3(0, 0, 0);
+            for (int oy = -1; oy <= 1; ++oy)
+                for (int ox = -1; ox <= 1; ++ox) {
+                    int qx = cx + ox, qy = cy + oy;
+                    if (qx < 0 || qy < 0 || qx >= (int)W || qy >= (int)H) continue;
+                    size_t j = (size_t)qy * W + qx;
+                    const float* h4 = img->history_prev[0] + 4 * j;
+                    const float* hn4 = img->history_prev[1] + 4 * j;
+                    if (h4[3] < 0.0f) continue;
+                    V3 cpos = load3(h4), cn = normalize(load3(hn4));
+                    uint32_t cmat = asuint(hn4[3]);
+                    // is_reprojected_history_compatible (:342-353)
+                    if (pmat != cmat) continue;
+                    if (dot(pn, cn) < 0.9f) continue;
+                    float view_dist = fmaxs(length(pp - cp), 1.0f);
+                    float plane = fabsf(dot(cpos - pp, pn));
+                    float dpos = length(cpos - pp);
+                    if (!(plane <= 0.01f * view_dist && dpos <= 0.05f * view_dist)) continue;
+                    float err = plane * 4.0f + dpos;
+                    if (err < best) { best = err; hist = j; hpos = cpos; found = true; }
+                }
+            if (!found) continue;
+            PtRes cur = pt_load(img->reservoir_curr, px);
+            PtRes prv = pt_load(img->reservoir_prev, hist);
+            if (prv.M == 0 || prv.valid < 0.5f) continue;
+            prv.M = std::min(prv.M, m_cap);
+            float jac = pt_jacobian(hpos, pp, prv.rc_pos, prv.rc_normal);
+            if (jac <= 0.0f) continue;
+            if (!pt_visible(s, pp, pn, prv.rc_pos, p->ray_bias)) continue;
+            float ph_prev = pt_target(pp, pn, pm, cp, prv);
+            float prev_W = fmins(prv.W, 50.0f);
+            float contrib = ph_prev * prev_W * float(prv.M) * jac;
+            if (contrib <= 0.0f) continue;
+            cur.w_sum += contrib;
+            uint32_t seed = make_seed(x, y, p->frame_seed + 1u);
+            if (cur.w_sum > 0.0f && rand_float(seed) < contrib / cur.w_sum) {
+                cur.rc_pos = prv.rc_pos; cur.rc_normal = prv.rc_normal;
+                cur.suffix_rad = prv.suffix_rad; cur.prefix_thp = prv.prefix_thp;
+                cur.valid = 1.0f;
+            }
+            uint32_t new_M = cur.M + prv.M;
+            if (new_M > m_cap) { cur.w_sum *= float(m_cap) / float(new_M); cur.M = m_cap; }
+            else cur.M = new_M;
+            if (cur.M > 0 && cur.valid > 0.5f) {
+                float ph_y = pt_target(pp, pn, pm, cp, cur);
+                cur.W = (ph_y > 1e-10f) ? (cur.w_sum / (float(cur.M) * ph_y)) : 0.0f;
+                cur.W = fmins(cur.W, 50.0f);
+            }
+            pt_store(img->reservoir_curr, px, cur);
+        }
+    });
+}
+
+void oracle_restir_pt_spatial_shade(const OracleScene* scene, const GpuCameraData* cam,
+                                    const OracleRestirPtParams* p, const OracleRestirPtImages* img, int threads) {
+    const OracleScene& s = *scene;
+    const uint32_t W = cam->screen_width, H = cam->screen_height;
+    const V3 cp = load3(cam->position);
+    parallel_rows(H, threads, [&](uint32_t y) {
+        for (uint32_t x = 0; x < W; ++x) {
+            const size_t px = (size_t)y * W + x;
+            V3 radiance = v3(0, 0, 0);
+            if (p->include_direct_lighting != 0 && img->direct) radiance = radiance + load3(img->direct + 4 * px);
+            V3 pp, pn; uint32_t pmat;
+            if (!pt_surface(s, img->gbuf_pos, img->gbuf_norm, px, pp, pn, pmat)) {
+                if (p->include_direct_lighting == 0) {
+                    V3 o, d;
+                    primary_ray(*cam, x, y, 0.5f, 0.5f, o, d);
+                    radiance = radiance + sky(d);
+                }
+                put4(img->output + 4 * px, radiance, 1.0f);
+                continue;
+            }
+            const GpuMaterial& pm = s.materials[pmat];
+            if (any_positive(pm.emissive)) {
+                radiance = radiance + load3(pm.emissive);
+                put4(img->output + 4 * px, radiance, 1.0f);
+                continue;
+            }
+            PtRes res = pt_load(img->reservoir_curr, px);
+            if (p->spatial_enable && p->spatial_num_neighbors > 0 && res.valid > 0.5f) {
+                const float base_phase = frac_hlsl(float(pcg_hash(x ^ (y * 65537u))) * 2.3283064365386963e-10f);
+                for (uint32_t k = 0; k < p->spatial_num_neighbors; ++k) {
+                    float u = (float(k) + 0.5f) / float(p->spatial_num_neighbors);
+                    float angle = frac_hlsl(base_phase + 0.61803398875f * float(k)) * kTwoPi;
+                    float radius = sqrtf(u) * float(p->spatial_radius);
+                    int ox = (int)(radius * rr_cosf(angle)), oy = (int)(radius * rr_sinf(angle));
+                    int nx = std::min(std::max((int)x + ox, 0), (int)W - 1);
+                    int ny = std::min(std::max((int)y + oy, 0), (int)H - 1);
+                    if (nx == (int)x && ny == (int)y) continue;
+                    size_t j = (size_t)ny * W + nx;
+                    // is_spatial_neighbor_compatible (:411-430)
+                    const float* nb4 = img->gbuf_pos + 4 * j;
+                    if (nb4[3] < 0.0f) continue;
+                    V3 nbp = load3(nb4), nbn = normalize(load3(img->gbuf_norm + 4 * j));
+                    if (dot(nbn, pn) < 0.85f) continue;
+                    float plane = fabsf(dot(nbp - pp, pn));
+                    float dscale = fmaxs(length(pp - cp), 1.0f);
+                    if (!(plane <= 0.02f * dscale)) continue;
+                    PtRes nbr = pt_load(img->reservoir_curr, j);
+                    if (nbr.M == 0 || nbr.valid < 0.5f) continue;
+                    float jac = pt_jacobian(nbp, pp, nbr.rc_pos, nbr.rc_normal);
+                    if (jac <= 0.0f) continue;
+                    float contrib = pt_target(pp, pn, pm, cp, nbr) * nbr.W * float(nbr.M) * jac;
+                    if (contrib <= 0.0f) continue;
+                    res.w_sum += contrib;
+                    res.M += nbr.M;
+                    float accept = frac_hlsl(base_phase + 0.754877666f * float(k + 1u));
+                    if (res.w_sum > 0.0f && accept < contrib / res.w_sum) {
+                        res.rc_pos = nbr.rc_pos; res.rc_normal = nbr.rc_normal;
+                        res.suffix_rad = nbr.suffix_rad; res.prefix_thp = nbr.prefix_thp;
+                    }
+                }
+                if (res.M > 0) {
+                    float ph_y = pt_target(pp, pn, pm, cp, res);
+                    res.W = (ph_y > 1e-10f) ? (res.w_sum / (float(res.M) * ph_y)) : 0.0f;
+                }
+            }
+            if (res.M > 0 && res.W > 0.0f && res.valid > 0.5f) {
+                V3 indirect = pt_contribution(pp, pn, pm, cp, res) * res.W;
+                if (luminance709(indirect) > 0.0f && pt_visible(s, pp, pn, res.rc_pos, p->ray_bias))
+                    radiance = radiance + indirect * p->indirect_strength;
+                if (p->guiding.enabled != 0u) {   // splat (:978-994), integer atomics
+                    V3 to_rc = res.rc_pos - pp;
+                    float d2 = dot(to_rc, to_rc);
+                    if (d2 > 1e-8f) {
+                        V3 wi = to_rc * rsqrt_hlsl(d2);
+                        uint32_t cell = cell_index(pp, pmat, cp, p->guiding);
+                        uint32_t* a = reinterpret_cast<uint32_t*>(img->guiding_accum) + (size_t)cell * 4;
+                        __atomic_fetch_add(a + 0, (uint32_t)(int32_t)rintf(wi.x * 1048576.0f), __ATOMIC_RELAXED);
+                        __atomic_fetch_add(a + 1, (uint32_t)(int32_t)rintf(wi.y * 1048576.0f), __ATOMIC_RELAXED);
+                        __atomic_fetch_add(a + 2, (uint32_t)(int32_t)rintf(wi.z * 1048576.0f), __ATOMIC_RELAXED);
+                        __atomic_fetch_add(a + 3, 1u, __ATOMIC_RELAXED);
+                    }
+                }
+            }
+            put4(img->output + 4 * px, radiance, 1.0f);
+        }
+    });
 }
 
 } // extern "C"

@@ -139,6 +139,44 @@ void oracle_guiding_sample(const float* fitted, const float* pos /*n*4*/,
                            float* pdf_out);
 float oracle_vmf_pdf(const float mu[3], float kappa, const float dir[3]);
 
+/* ── ReSTIR PT (restir_pt.slang:567-1000) ───────────────────────────────── */
+typedef struct OracleRestirPtParams {
+    uint32_t frame_seed;
+    uint32_t num_initial_candidates;
+    uint32_t max_bounces;
+    uint32_t temporal_enable;
+    uint32_t spatial_enable;
+    uint32_t spatial_num_neighbors;
+    uint32_t spatial_radius;
+    uint32_t include_direct_lighting;
+    float    indirect_strength;
+    float    ray_bias;
+    uint32_t _pad[2];
+    OracleGuidingParams guiding;
+} OracleRestirPtParams;
+
+/* Images: width x height x 4 floats each (reservoir [0..3], history [0..1]). */
+typedef struct OracleRestirPtImages {
+    const float* gbuf_pos;
+    const float* gbuf_norm;
+    const float* direct;          /* or NULL */
+    float*       reservoir_curr[4];
+    float*       reservoir_prev[4];
+    float*       history_curr[2];
+    float*       history_prev[2];
+    float*       output;
+    int32_t*     guiding_accum;
+    float*       guiding_fitted;
+} OracleRestirPtImages;
+
+void oracle_restir_pt_initial(const OracleScene* scene, const GpuCameraData* cam,
+                              const OracleRestirPtParams* p, const OracleRestirPtImages* img, int threads);
+void oracle_restir_pt_temporal(const OracleScene* scene, const GpuCameraData* cam,
+                               const OracleRestirPtParams* p, const OracleRestirPtImages* img, int threads);
+void oracle_restir_pt_spatial_shade(const OracleScene* scene, const GpuCameraData* cam,
+                                    const OracleRestirPtParams* p, const OracleRestirPtImages* img,
+                                    int threads);
+
 /* ── BRDF (BRDF.slang) for direct checks ────────────────────────────────── */
 void oracle_brdf_eval(const float n[3], const float wo[3], const float wi[3],
                       const float base[3], float metallic, float roughness, float out[3]);

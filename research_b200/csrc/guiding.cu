@@ -8,28 +8,10 @@
 //   sample: one-sample MIS of the fitted lobe and a cosine lobe at a surface
 //           point (sample_primary_dir, restir_pt.slang:520-563)
 
-#include "rr_internal.h"
-#include "rr_vmf.cuh"
+#include "rr_grid.cuh"
 
 namespace rr {
 namespace {
-
-struct GridParams {
-    float base_cell_size, distance_slope;
-    uint32_t cell_count, enabled, min_samples;
-    float kappa_max, alpha;
-    float cam_x, cam_y, cam_z;
-};
-
-// GuidingGrid.slang:54-67
-RR_D uint32_t cell_index(float3 p, uint32_t bsdf, const GridParams& g) {
-    const float view_dist = length(p - f3(g.cam_x, g.cam_y, g.cam_z));
-    const float cell = mx(g.base_cell_size + g.distance_slope * view_dist, 1.0e-4f);
-    const int qx = int(floorf(p.x / cell)), qy = int(floorf(p.y / cell)), qz = int(floorf(p.z / cell));
-    const uint32_t h = pcg_hash(uint32_t(qx) * 73856093u ^ uint32_t(qy) * 19349663u ^
-                                uint32_t(qz) * 83492791u ^ bsdf * 2654435761u);
-    return h % (g.cell_count > 0u ? g.cell_count : 1u);
-}
 
 __global__ void __launch_bounds__(256) splat_kernel(uint32_t* __restrict__ accum, const float4* __restrict__ pos,
                                                     const float4* __restrict__ dir,
@@ -37,14 +19,7 @@ __global__ void __launch_bounds__(256) splat_kernel(uint32_t* __restrict__ accum
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 p = pos[i], d = dir[i];
-    const uint32_t cell = cell_index(xyz(p), bsdf[i], g);
-    uint32_t* a = accum + size_t(cell) * 4;
-    // round() to the nearest integer, ties to even (HLSL round); the scale is
-    // a power of two, so the product is exact.
-    atomicAdd(a + 0, uint32_t(int(rintf(d.x * 1048576.0f))));
-    atomicAdd(a + 1, uint32_t(int(rintf(d.y * 1048576.0f))));
-    atomicAdd(a + 2, uint32_t(int(rintf(d.z * 1048576.0f))));
-    atomicAdd(a + 3, 1u);
+    splat_dir(accum, cell_index(xyz(p), bsdf[i], g), xyz(d));
 }
 
 __global__ void __launch_bounds__(256) fit_kernel(int4* __restrict__ accum, float4* __restrict__ fitted, GridParams g) {
@@ -74,48 +49,12 @@ __global__ void __launch_bounds__(256) sample_kernel(const float4* __restrict__ 
                                                      float4* __restrict__ wi_out, float* __restrict__ pdf_out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float3 p = xyz(pos[i]), nn = xyz(nrm[i]);
     uint32_t seed = seeds[i];
-    float alpha = 0.0f;
-    bool valid = false;
-    float3 mu = f3(0.0f, 0.0f, 0.0f);
-    float kappa = 0.0f;
-    if (g.enabled != 0u && g.alpha > 0.0f) {
-        const float4 f = __ldg(fitted + cell_index(p, bsdf[i], g));
-        mu = xyz(f);
-        kappa = f.w;
-        valid = kappa > 0.0f && dot(mu, mu) > 0.25f;
-        if (valid) alpha = g.alpha;
-    }
-    float3 T, B;
-    build_onb(nn, T, B);
-    float3 wi;
-    if (rand_float(seed) < alpha) {
-        const float ux = rand_float(seed);
-        const float uy = rand_float(seed);
-        float vpdf;
-        wi = vmf_sample(mu, kappa, ux, uy, vpdf);
-    } else {
-        const float u0 = rand_float(seed);
-        const float u1 = rand_float(seed);
-        float cpdf;
-        wi = tangent_to_world(sample_cosine_hemisphere(u0, u1, cpdf), T, B, nn);
-    }
-    const float cos_i = dot(nn, wi);
-    const float p_cos = cos_i > 0.0f ? cos_i * kInvPi : 0.0f;
-    const float p_vmf = valid ? vmf_pdf(mu, kappa, wi) : 0.0f;
+    float pdf;
+    const float3 wi = sample_primary_dir(fitted, xyz(pos[i]), xyz(nrm[i]), bsdf[i], g, seed, pdf);
     wi_out[i] = make_float4(wi.x, wi.y, wi.z, 0.0f);
-    pdf_out[i] = alpha * p_vmf + (1.0f - alpha) * p_cos;
+    pdf_out[i] = pdf;
     seeds[i] = seed;
-}
-
-GridParams to_grid(const rr_guiding_params* p, const float* cam) {
-    GridParams g;
-    g.base_cell_size = p->base_cell_size; g.distance_slope = p->distance_slope;
-    g.cell_count = p->cell_count; g.enabled = p->enabled; g.min_samples = p->min_samples;
-    g.kappa_max = p->kappa_max; g.alpha = p->alpha;
-    g.cam_x = cam ? cam[0] : 0.0f; g.cam_y = cam ? cam[1] : 0.0f; g.cam_z = cam ? cam[2] : 0.0f;
-    return g;
 }
 
 } // namespace

@@ -95,6 +95,32 @@ class GuidingParams(C.Structure):
                 ("_pad", C.c_uint32)]
 
 
+class PtReuseParams(C.Structure):
+    """rr_restir_pt_params (ReSTIRPTPushConstants minus the bindless indices)."""
+    _fields_ = [("frame_seed", C.c_uint32), ("num_initial_candidates", C.c_uint32), ("max_bounces", C.c_uint32),
+                ("temporal_enable", C.c_uint32), ("spatial_enable", C.c_uint32),
+                ("spatial_num_neighbors", C.c_uint32), ("spatial_radius", C.c_uint32),
+                ("include_direct_lighting", C.c_uint32), ("indirect_strength", C.c_float), ("ray_bias", C.c_float),
+                ("_pad", C.c_uint32 * 2), ("guiding", GuidingParams)]
+
+
+class PtReuseImages(C.Structure):
+    """rr_restir_pt_images: device pointers (float4 per pixel)."""
+    _fields_ = [("gbuf_pos", C.c_void_p), ("gbuf_norm", C.c_void_p), ("direct", C.c_void_p),
+                ("reservoir_curr", C.c_void_p * 4), ("reservoir_prev", C.c_void_p * 4),
+                ("history_curr", C.c_void_p * 2), ("history_prev", C.c_void_p * 2), ("output", C.c_void_p),
+                ("guiding_accum", C.c_void_p), ("guiding_fitted", C.c_void_p)]
+
+
+def pt_reuse_params(frame_seed=0, candidates=8, max_bounces=4, temporal=1, spatial=1, neighbors=4, radius=12,
+                    include_direct=1, indirect_strength=1.0, ray_bias=1e-3, guiding=1, alpha=0.5,
+                    cell_count=1 << 20, min_samples=8, kappa_max=512.0) -> "PtReuseParams":
+    """Reference defaults of ReSTIRPTPass.h:86-100."""
+    g = GuidingParams(0.10, 0.02, cell_count, guiding, min_samples, kappa_max, alpha, 0)
+    return PtReuseParams(frame_seed, candidates, max_bounces, temporal, spatial, neighbors, radius, include_direct,
+                         indirect_strength, ray_bias, (C.c_uint32 * 2)(0, 0), g)
+
+
 class GuideDesc(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("grid_resolution", C.c_uint32), ("alpha", C.c_float), ("decay", C.c_float),
                 ("bounds_min", C.c_float * 3), ("bounds_max", C.c_float * 3), ("max_samples", C.c_uint32),
@@ -156,6 +182,12 @@ _SIGNATURES = {
     "rr_guiding_fit": (I, [P, P, P, C.POINTER(GuidingParams), P]),
     "rr_guiding_sample": (I, [P, P, P, P, P, P, U32, C.POINTER(F32), C.POINTER(GuidingParams), P, P, P]),
     "rr_guiding_reset": (I, [P, P, P, C.POINTER(GuidingParams), P]),
+    "rr_restir_pt_initial": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtReuseParams), C.POINTER(PtReuseImages), P]),
+    "rr_restir_pt_temporal": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtReuseParams), C.POINTER(PtReuseImages), P]),
+    "rr_restir_pt_spatial_shade": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtReuseParams),
+                                       C.POINTER(PtReuseImages), P]),
+    "rr_restir_pt_execute": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtReuseParams), C.POINTER(PtReuseImages), P]),
+    "rr_restir_pt_reset_history": (I, [P, C.POINTER(PtReuseImages), U32, U32, P]),
     "rr_trace_closest": (I, [P, P, P, P, F32, F32, U32, P, P, P]),
     "rr_tonemap_execute": (I, [P, P, U32, U32, F32, P, P]),
     "rr_guide_create": (I, [P, C.POINTER(GuideDesc), C.POINTER(P)]),
