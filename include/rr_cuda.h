@@ -151,6 +151,36 @@ rr_status rr_pathtracer_tune(rr_ctx* ctx, const rr_scene* scene, const GpuCamera
                              const rr_pt_params* params, float* radiance_out, void* stream,
                              rr_pt_tune_result* out);
 
+/* ── batches of scenes (no reference counterpart: the reference renders one
+ * scene per PathTracerPass::execute). A batch renders many scenes, each with
+ * its own camera and image size, in one set of wavefront launches (raygen,
+ * then per bounce one extend, one shade and one shadow launch for all
+ * scenes). Every scene's images are bit-identical to rr_pathtracer_execute
+ * of that scene with the same camera and params. The scenes must outlive
+ * the batch. */
+typedef struct rr_batch rr_batch;
+rr_status rr_batch_create(rr_ctx* ctx, const rr_scene* const* scenes, uint32_t count, rr_batch** out);
+rr_status rr_batch_destroy(rr_batch* batch);
+
+/* Capture the batch's launches in a CUDA graph (on the first call with a
+ * given configuration) and replay it; the per-call cameras, frame seed and
+ * output pointers travel in a small table copied before the replay. */
+#define RR_PT_FLAG_GRAPH 4u
+
+/* cameras[i] and radiance_out[i] (spp images of cameras[i]'s size, device
+ * memory) for scene i; params are shared by all scenes (frame_seed,
+ * max_bounces, spp, flags: RR_PT_FLAG_COUNT_TRAVERSAL and
+ * RR_PT_FLAG_TIME_STAGES as for rr_pathtracer_execute, or RR_PT_FLAG_GRAPH).
+ * Host memory of the arguments may be reused as soon as the call returns. */
+rr_status rr_batch_execute(rr_ctx* ctx, rr_batch* batch, const GpuCameraData* cameras,
+                           const rr_pt_params* params, float* const* radiance_out, void* stream);
+
+/* rr_pathtracer_tune for a batch: times every traversal variant on the
+ * batch, keeps the fastest on the context (graphs are recaptured). */
+rr_status rr_batch_tune(rr_ctx* ctx, rr_batch* batch, const GpuCameraData* cameras,
+                        const rr_pt_params* params, float* const* radiance_out, void* stream,
+                        rr_pt_tune_result* out);
+
 /* ── accumulate: AccumulatePass::execute (AccumulatePass.cpp:167-218,
  * kernel accumulate.slang:21-46). AccumulatePushConstants minus indices.
  * Folds `image_count` consecutive radiance images into `accumulated` in

@@ -389,8 +389,18 @@ rr_status rr_host_scene_procedural(const rr_procedural_params* p, rr_host_scene*
         tris += idx.size() / 3;
         add_mesh(*s, v, idx, mat, nullptr);
     };
-    heightfield(256 + int(rng.next() % 257), 0);
-    for (int wall = 1; wall <= 3; ++wall) heightfield(128 + int(rng.next() % 129), wall);
+    // Below 1M triangles the drawn grid sizes are capped (floor at 30 % of
+    // the target, each wall at 7 %) so that small scenes keep the mix of
+    // heightfields and icospheres; from 1M on the draws are used as they are.
+    const bool small = p->target_triangles < 1000000u;
+    auto capped = [&](int G, double share) {
+        if (!small) return G;
+        const double cap = share * double(p->target_triangles);
+        if (2.0 * double(G - 1) * double(G - 1) <= cap) return G;
+        return std::max(8, int(std::sqrt(cap / 2.0)) + 1);
+    };
+    heightfield(capped(256 + int(rng.next() % 257), 0.30), 0);
+    for (int wall = 1; wall <= 3; ++wall) heightfield(capped(128 + int(rng.next() % 129), 0.07), wall);
     // displaced icospheres (subdivision 3..5) inside the room until the
     // triangle target is met
     std::vector<F3> base_pts[3];

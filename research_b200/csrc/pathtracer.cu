@@ -21,8 +21,114 @@
 namespace rr {
 namespace {
 
-__global__ void __launch_bounds__(kBlock) shade_kernel(DevScene s, uint32_t bounce, uint32_t last,
-                                                       const float4* __restrict__ qa,
+// Result of shading one queued ray: the continuation ray and the shadow ray
+// (if any) that the kernel compacts into the next queues.
+struct ShadeResult {
+    bool cont = false, emit_shadow = false;
+    uint32_t pid = 0, seed = 0;
+    float3 new_o = make_float3(0, 0, 0), wi = make_float3(0, 0, 0), thp = make_float3(0, 0, 0);
+    float3 sh_o = make_float3(0, 0, 0), sh_d = make_float3(0, 0, 0), contrib = make_float3(0, 0, 0);
+    float sh_tmax = 0.0f;
+};
+
+// One ray of the shade stage (a = origin|pid, b = direction|seed, c =
+// throughput, h = hit) in scene s, radiance accumulated into out.
+RR_D void shade_ray(const DevScene& s, float4* __restrict__ out, uint32_t bounce, uint32_t last, const float4 a,
+                    const float4 b, const float4 c, const float4 h, ShadeResult& R) {
+    R.pid = __float_as_uint(a.w);
+    R.seed = __float_as_uint(b.w);
+    const float3 ray_dir = f3(b.x, b.y, b.z);
+    R.thp = f3(c.x, c.y, c.z);
+    const uint32_t inst = __float_as_uint(h.z);
+    if (inst == kNoIndex) {
+        // Sky / environment (pathtracer.slang:213-219)
+        const float3 L = R.thp * sky_radiance(ray_dir);
+        float4 o = out[R.pid];
+        o.x = o.x + L.x; o.y = o.y + L.y; o.z = o.z + L.z;
+        out[R.pid] = o;
+    } else {
+        const Surface sf = hit_surface(s, inst, __float_as_uint(h.w), h.x, h.y);
+        const float4 m0 = __ldg(s.materials + sf.material * 2);
+        const float4 m1 = __ldg(s.materials + sf.material * 2 + 1);
+        if (m1.x > 0.0f || m1.y > 0.0f || m1.z > 0.0f) {
+            // Emissive surfaces terminate (pathtracer.slang:225-229)
+            const float3 L = R.thp * f3(m1.x, m1.y, m1.z);
+            float4 o = out[R.pid];
+            o.x = o.x + L.x; o.y = o.y + L.y; o.z = o.z + L.z;
+            out[R.pid] = o;
+        } else {
+            const float3 wo = -ray_dir;
+            float3 n = sf.normal;
+            if (dot(n, wo) < 0.0f) n = -n;
+            const float3 base_c = f3(m0.x, m0.y, m0.z);
+            const float metallic = m0.w, roughness = m1.w;
+            // NEE (pathtracer.slang:124-177): pick, shadow ray, contribution
+            if (s.num_lights > 0) {
+                const uint32_t N = s.num_lights;
+                const uint32_t li = uint32_t(rand_float(R.seed) * float(N)) % N;
+                const float4 l0 = __ldg(s.lights + li * 3);
+                const float4 l1 = __ldg(s.lights + li * 3 + 1);
+                const float4 l2 = __ldg(s.lights + li * 3 + 2);
+                const bool is_point = __float_as_uint(l0.w) == 0u;
+                float3 ldir; float dist, pdf_light;
+                if (is_point) {
+                    const float3 to = f3(l0.x, l0.y, l0.z) - sf.pos;
+                    dist = length(to);
+                    ldir = to / dist;
+                    pdf_light = dist * dist;
+                } else {
+                    ldir = normalize(-f3(l1.x, l1.y, l1.z));
+                    dist = 1e9f;
+                    pdf_light = 1.0f;
+                }
+                if (dot(ldir, n) > 0.0f) {
+                    const float3 brdf_val = brdf_eval(n, wo, ldir, base_c, metallic, roughness);
+                    const float n_dot_l = mx(dot(n, ldir), 0.0f);
+                    const float den = is_point ? (pdf_light + 1e-6f) : 1.0f;
+                    const float3 irr = f3(l2.x * l2.w / den, l2.y * l2.w / den, l2.z * l2.w / den);
+                    float mis = 1.0f;
+                    if (!is_point) {
+                        const float pb = brdf_pdf(wo, ldir, n, roughness);
+                        mis = (pdf_light * pdf_light) / (pdf_light * pdf_light + pb * pb + 1e-10f);
+                    }
+                    float3 Lr = brdf_val * irr;
+                    Lr = Lr * n_dot_l;
+                    Lr = Lr * mis;
+                    Lr = Lr * float(N);
+                    R.contrib = R.thp * Lr;
+                    R.sh_o = sf.pos + n * 1e-4f;
+                    R.sh_d = ldir;
+                    R.sh_tmax = dist - 0.01f;
+                    R.emit_shadow = true;
+                }
+            }
+            if (!last) {
+                const float u0 = rand_float(R.seed);
+                const float u1 = rand_float(R.seed);
+                float pdf;
+                const float3 f = brdf_sample(wo, n, base_c, metallic, roughness, u0, u1, R.wi, pdf);
+                if (!(pdf < 1e-6f)) {
+                    const float ndwi = mx(dot(n, R.wi), 0.0f);
+                    R.thp = R.thp * ((f * ndwi) / pdf);
+                    bool alive = true;
+                    if (bounce >= 3) {
+                        const float survive = mn(mx(R.thp.x, mx(R.thp.y, R.thp.z)), 0.95f);
+                        if (rand_float(R.seed) > survive) alive = false;
+                        else R.thp = R.thp / survive;
+                    }
+                    if (alive) { R.cont = true; R.new_o = sf.pos + n * 1e-4f; }
+                }
+            }
+        }
+    }
+}
+
+// Multi: a batch of scenes; a ray's scene index is in c.w, its scene is
+// table[index] and its image outs[index]; the index is carried on.
+template <bool Multi>
+__global__ void __launch_bounds__(kBlock) shade_kernel(DevScene s, const DevScene* __restrict__ table,
+                                                       float4* const* __restrict__ outs, uint32_t bounce,
+                                                       uint32_t last, const float4* __restrict__ qa,
                                                        const float4* __restrict__ qb,
                                                        const float4* __restrict__ qc,
                                                        const float4* __restrict__ hits,
@@ -36,112 +142,30 @@ __global__ void __launch_bounds__(kBlock) shade_kernel(DevScene s, uint32_t boun
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = warp_first; base < count; base += stride) {
         const uint32_t i = base + lane_id();
-        bool cont = false, emit_shadow = false;
-        uint32_t pid = 0, seed = 0;
-        float3 new_o = f3(0, 0, 0), wi = f3(0, 0, 0), thp = f3(0, 0, 0);
-        float3 sh_o = f3(0, 0, 0), sh_d = f3(0, 0, 0), contrib = f3(0, 0, 0);
-        float sh_tmax = 0.0f;
+        ShadeResult R;
+        uint32_t sid = 0;
         if (i < count) {
             const float4 a = qa[i], b = qb[i], c = qc[i];
             const float4 h = hits[i];
-            pid = __float_as_uint(a.w);
-            seed = __float_as_uint(b.w);
-            const float3 ray_dir = f3(b.x, b.y, b.z);
-            thp = f3(c.x, c.y, c.z);
-            const uint32_t inst = __float_as_uint(h.z);
-            if (inst == kNoIndex) {
-                // Sky / environment (pathtracer.slang:213-219)
-                const float3 L = thp * sky_radiance(ray_dir);
-                float4 o = out[pid];
-                o.x = o.x + L.x; o.y = o.y + L.y; o.z = o.z + L.z;
-                out[pid] = o;
+            if constexpr (Multi) {
+                sid = __float_as_uint(c.w);
+                shade_ray(table[sid], outs[sid], bounce, last, a, b, c, h, R);
             } else {
-                const Surface sf = hit_surface(s, inst, __float_as_uint(h.w), h.x, h.y);
-                const float4 m0 = __ldg(s.materials + sf.material * 2);
-                const float4 m1 = __ldg(s.materials + sf.material * 2 + 1);
-                if (m1.x > 0.0f || m1.y > 0.0f || m1.z > 0.0f) {
-                    // Emissive surfaces terminate (pathtracer.slang:225-229)
-                    const float3 L = thp * f3(m1.x, m1.y, m1.z);
-                    float4 o = out[pid];
-                    o.x = o.x + L.x; o.y = o.y + L.y; o.z = o.z + L.z;
-                    out[pid] = o;
-                } else {
-                    const float3 wo = -ray_dir;
-                    float3 n = sf.normal;
-                    if (dot(n, wo) < 0.0f) n = -n;
-                    const float3 base_c = f3(m0.x, m0.y, m0.z);
-                    const float metallic = m0.w, roughness = m1.w;
-                    // NEE (pathtracer.slang:124-177): pick, shadow ray, contribution
-                    if (s.num_lights > 0) {
-                        const uint32_t N = s.num_lights;
-                        const uint32_t li = uint32_t(rand_float(seed) * float(N)) % N;
-                        const float4 l0 = __ldg(s.lights + li * 3);
-                        const float4 l1 = __ldg(s.lights + li * 3 + 1);
-                        const float4 l2 = __ldg(s.lights + li * 3 + 2);
-                        const bool is_point = __float_as_uint(l0.w) == 0u;
-                        float3 ldir; float dist, pdf_light;
-                        if (is_point) {
-                            const float3 to = f3(l0.x, l0.y, l0.z) - sf.pos;
-                            dist = length(to);
-                            ldir = to / dist;
-                            pdf_light = dist * dist;
-                        } else {
-                            ldir = normalize(-f3(l1.x, l1.y, l1.z));
-                            dist = 1e9f;
-                            pdf_light = 1.0f;
-                        }
-                        if (dot(ldir, n) > 0.0f) {
-                            const float3 brdf_val = brdf_eval(n, wo, ldir, base_c, metallic, roughness);
-                            const float n_dot_l = mx(dot(n, ldir), 0.0f);
-                            const float den = is_point ? (pdf_light + 1e-6f) : 1.0f;
-                            const float3 irr = f3(l2.x * l2.w / den, l2.y * l2.w / den, l2.z * l2.w / den);
-                            float mis = 1.0f;
-                            if (!is_point) {
-                                const float pb = brdf_pdf(wo, ldir, n, roughness);
-                                mis = (pdf_light * pdf_light) / (pdf_light * pdf_light + pb * pb + 1e-10f);
-                            }
-                            float3 Lr = brdf_val * irr;
-                            Lr = Lr * n_dot_l;
-                            Lr = Lr * mis;
-                            Lr = Lr * float(N);
-                            contrib = thp * Lr;
-                            sh_o = sf.pos + n * 1e-4f;
-                            sh_d = ldir;
-                            sh_tmax = dist - 0.01f;
-                            emit_shadow = true;
-                        }
-                    }
-                    if (!last) {
-                        const float u0 = rand_float(seed);
-                        const float u1 = rand_float(seed);
-                        float pdf;
-                        const float3 f = brdf_sample(wo, n, base_c, metallic, roughness, u0, u1, wi, pdf);
-                        if (!(pdf < 1e-6f)) {
-                            const float ndwi = mx(dot(n, wi), 0.0f);
-                            thp = thp * ((f * ndwi) / pdf);
-                            bool alive = true;
-                            if (bounce >= 3) {
-                                const float survive = mn(mx(thp.x, mx(thp.y, thp.z)), 0.95f);
-                                if (rand_float(seed) > survive) alive = false;
-                                else thp = thp / survive;
-                            }
-                            if (alive) { cont = true; new_o = sf.pos + n * 1e-4f; }
-                        }
-                    }
-                }
+                shade_ray(s, out, bounce, last, a, b, c, h, R);
             }
         }
-        const uint32_t sslot = warp_alloc(emit_shadow, shadow_count);
-        if (emit_shadow) {
-            sa[sslot] = make_float4(sh_o.x, sh_o.y, sh_o.z, __uint_as_float(pid));
-            sb[sslot] = make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
-            sc[sslot] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+        const float tag = Multi ? __uint_as_float(sid) : 0.0f;
+        const uint32_t sslot = warp_alloc(R.emit_shadow, shadow_count);
+        if (R.emit_shadow) {
+            sa[sslot] = make_float4(R.sh_o.x, R.sh_o.y, R.sh_o.z, __uint_as_float(R.pid));
+            sb[sslot] = make_float4(R.sh_d.x, R.sh_d.y, R.sh_d.z, R.sh_tmax);
+            sc[sslot] = make_float4(R.contrib.x, R.contrib.y, R.contrib.z, tag);
         }
-        const uint32_t rslot = warp_alloc(cont, next_count);
-        if (cont) {
-            na[rslot] = make_float4(new_o.x, new_o.y, new_o.z, __uint_as_float(pid));
-            nb[rslot] = make_float4(wi.x, wi.y, wi.z, __uint_as_float(seed));
-            nc[rslot] = make_float4(thp.x, thp.y, thp.z, 0.0f);
+        const uint32_t rslot = warp_alloc(R.cont, next_count);
+        if (R.cont) {
+            na[rslot] = make_float4(R.new_o.x, R.new_o.y, R.new_o.z, __uint_as_float(R.pid));
+            nb[rslot] = make_float4(R.wi.x, R.wi.y, R.wi.z, __uint_as_float(R.seed));
+            nc[rslot] = make_float4(R.thp.x, R.thp.y, R.thp.z, tag);
         }
     }
 }
@@ -198,7 +222,7 @@ extern "C" rr_status rr_pathtracer_execute(rr_ctx* ctx, const rr_scene* scene,
     ShadowKernel sh_k = count ? shadow_variant<true>(ctx->shadow_variant) : shadow_variant<false>(ctx->shadow_variant);
     const int g_ext = persistent_grid(ctx, reinterpret_cast<const void*>(ext_k));
     const int g_sh = persistent_grid(ctx, reinterpret_cast<const void*>(sh_k));
-    const int g_shade = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(shade_kernel)),
+    const int g_shade = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(shade_kernel<false>)),
                                       int((n + kBlock - 1) / kBlock));
     if (count) RR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->work64, 0, sizeof(unsigned long long) * 4, stream));
     const DevScene& S = scene->dev;
@@ -213,7 +237,7 @@ extern "C" rr_status rr_pathtracer_execute(rr_ctx* ctx, const rr_scene* scene,
         RR_CHECK_LAUNCH(ctx);
         timer.end(1);
         timer.begin(2);
-        shade_kernel<<<g_shade, kBlock, 0, stream>>>(S, b, b + 1 == p->max_bounces ? 1u : 0u,
+        shade_kernel<false><<<g_shade, kBlock, 0, stream>>>(S, nullptr, nullptr, b, b + 1 == p->max_bounces ? 1u : 0u,
                                                      q.ray_a[cur], q.ray_b[cur], q.ray_c[cur], q.hits,
                                                      q.ray_a[nxt], q.ray_b[nxt], q.ray_c[nxt],
                                                      q.shadow_a, q.shadow_b, q.shadow_c, out,
@@ -291,6 +315,245 @@ extern "C" rr_status rr_pathtracer_tune(rr_ctx* ctx, const rr_scene* scene, cons
         warm.flags = 0;
         if ((s = rr_pathtracer_execute(ctx, scene, cam, &warm, radiance_out, stream)) != RR_OK) return s;
         if ((s = rr_pathtracer_execute(ctx, scene, cam, &q, radiance_out, stream)) != RR_OK) return s;
+        if ((s = rr_pathtracer_stats(ctx, &st, 1)) != RR_OK) return s;
+        out->extend_ms[v] = st.ms_extend;
+        out->shadow_ms[v] = st.ms_shadow;
+        if (st.ms_extend < best_e) { best_e = st.ms_extend; out->best_extend = v; }
+        if (st.ms_shadow < best_s) { best_s = st.ms_shadow; out->best_shadow = v; }
+    }
+    ctx->extend_variant = out->best_extend;
+    ctx->shadow_variant = out->best_shadow;
+    return RR_OK;
+}
+
+// ── batches of scenes ──────────────────────────────────────────────────────
+struct rr_batch {
+    rr_ctx* ctx = nullptr;
+    std::vector<const rr_scene*> scenes;
+    rr::DevScene* d_table = nullptr;       // per scene, uploaded once
+    unsigned char* d_call = nullptr;       // per call: BatchEntry[count], then float4*[count]
+    unsigned char* h_call[2] = {nullptr, nullptr};  // pinned staging of d_call, alternating
+    cudaEvent_t staged[2] = {nullptr, nullptr};     // the copy out of h_call[k] has completed
+    int slot = 0;
+    size_t entries_bytes = 0, call_bytes = 0;
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    struct Key {
+        uint64_t paths = 0;
+        uint32_t total_tiles = 0, max_bounces = 0, ev = 0, sv = 0;
+        const void* queue = nullptr;
+        bool operator!=(const Key& o) const {
+            return paths != o.paths || total_tiles != o.total_tiles || max_bounces != o.max_bounces || ev != o.ev ||
+                   sv != o.sv || queue != o.queue;
+        }
+    } key;
+};
+
+namespace {
+
+// Enqueues one batch frame: counter reset, raygen over every scene's tiles,
+// then per bounce one extend, one shade and one shadow launch for all scenes.
+rr_status enqueue_batch(rr_ctx* ctx, rr_batch* B, uint32_t total_tiles, size_t n, uint32_t max_bounces,
+                        uint32_t flags, cudaStream_t stream) {
+    using namespace rr;
+    rr_pt_queues& q = ctx->pt;
+    uint32_t* C = ctx->counters;
+    const uint32_t count_scenes = uint32_t(B->scenes.size());
+    const BatchEntry* entries = reinterpret_cast<const BatchEntry*>(B->d_call);
+    float4* const* outs = reinterpret_cast<float4* const*>(B->d_call + B->entries_bytes);
+    const bool count = (flags & RR_PT_FLAG_COUNT_TRAVERSAL) != 0;
+    const bool timed = (flags & RR_PT_FLAG_TIME_STAGES) != 0;
+    RR_TRY_CUDA(ctx, cudaMemsetAsync(C, 0, sizeof(uint32_t) * kCounterWords, stream));
+    {
+        const uint64_t threads = uint64_t(total_tiles) * 32;
+        rr_stage_timer t0(ctx, stream, timed);
+        t0.begin(0);
+        raygen_batch_kernel<<<uint32_t((threads + kBlock - 1) / kBlock), kBlock, 0, stream>>>(
+            entries, count_scenes, total_tiles, outs, q.ray_a[0], q.ray_b[0], q.ray_c[0], C);
+        RR_CHECK_LAUNCH(ctx);
+        t0.end(0);
+        rr_status st0 = t0.commit();
+        if (st0 != RR_OK) return st0;
+    }
+    BatchQueueKernel ext_k = count ? extend_batch_variant<true>(ctx->extend_variant)
+                                   : extend_batch_variant<false>(ctx->extend_variant);
+    BatchShadowKernel sh_k = count ? shadow_batch_variant<true>(ctx->shadow_variant)
+                                   : shadow_batch_variant<false>(ctx->shadow_variant);
+    const int g_ext = persistent_grid(ctx, reinterpret_cast<const void*>(ext_k));
+    const int g_sh = persistent_grid(ctx, reinterpret_cast<const void*>(sh_k));
+    const int g_shade = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(shade_kernel<true>)),
+                                      int((n + kBlock - 1) / kBlock));
+    if (count) RR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->work64, 0, sizeof(unsigned long long) * 4, stream));
+    rr_stage_timer timer(ctx, stream, timed);
+    for (uint32_t b = 0; b < max_bounces; ++b) {
+        const int cur = b & 1, nxt = cur ^ 1;
+        uint32_t* cb = C + 4 * b;
+        uint32_t* cn = C + 4 * (b + 1);
+        timer.begin(1);
+        ext_k<<<g_ext, kBlock, 0, stream>>>(B->d_table, q.ray_a[cur], q.ray_b[cur], q.ray_c[cur], q.hits, cb, cb + 1,
+                                            ctx->work64);
+        RR_CHECK_LAUNCH(ctx);
+        timer.end(1);
+        timer.begin(2);
+        shade_kernel<true><<<g_shade, kBlock, 0, stream>>>(DevScene{}, B->d_table, outs, b,
+                                                           b + 1 == max_bounces ? 1u : 0u, q.ray_a[cur],
+                                                           q.ray_b[cur], q.ray_c[cur], q.hits, q.ray_a[nxt],
+                                                           q.ray_b[nxt], q.ray_c[nxt], q.shadow_a, q.shadow_b,
+                                                           q.shadow_c, nullptr, cb, cn, cb + 2);
+        RR_CHECK_LAUNCH(ctx);
+        timer.end(2);
+        timer.begin(3);
+        sh_k<<<g_sh, kBlock, 0, stream>>>(B->d_table, outs, q.shadow_a, q.shadow_b, q.shadow_c, cb + 2, cb + 3,
+                                          ctx->work64 + 2);
+        RR_CHECK_LAUNCH(ctx);
+        timer.end(3);
+    }
+    return timer.commit();
+}
+
+} // namespace
+
+extern "C" rr_status rr_batch_destroy(rr_batch* B) {
+    if (!B) return RR_ERR_INVALID_ARGUMENT;
+    if (B->ctx) cudaSetDevice(B->ctx->device);
+    if (B->exec) cudaGraphExecDestroy(B->exec);
+    if (B->cap_stream) cudaStreamDestroy(B->cap_stream);
+    for (int k = 0; k < 2; ++k) {
+        if (B->staged[k]) cudaEventDestroy(B->staged[k]);
+        if (B->h_call[k]) cudaFreeHost(B->h_call[k]);
+    }
+    cudaFree(B->d_table);
+    cudaFree(B->d_call);
+    delete B;
+    return RR_OK;
+}
+
+extern "C" rr_status rr_batch_create(rr_ctx* ctx, const rr_scene* const* scenes, uint32_t count, rr_batch** out) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    if (!scenes || !out || count == 0) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_create: bad argument");
+    *out = nullptr;
+    for (uint32_t i = 0; i < count; ++i)
+        if (!scenes[i] || scenes[i]->ctx != ctx)
+            return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_create: scene %u is null or of another context", i);
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    rr_batch* B = new rr_batch;
+    B->ctx = ctx;
+    B->scenes.assign(scenes, scenes + count);
+    auto fail = [&](rr_status s) { rr_batch_destroy(B); return s; };
+    std::vector<rr::DevScene> table(count);
+    for (uint32_t i = 0; i < count; ++i) table[i] = scenes[i]->dev;
+    B->entries_bytes = (sizeof(rr::BatchEntry) * count + 15) & ~size_t(15);
+    B->call_bytes = B->entries_bytes + sizeof(void*) * count;
+    cudaError_t e;
+    if ((e = cudaMalloc(&B->d_table, sizeof(rr::DevScene) * count)) != cudaSuccess ||
+        (e = cudaMemcpy(B->d_table, table.data(), sizeof(rr::DevScene) * count, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&B->d_call, B->call_bytes)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&B->cap_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail(rr_fail(ctx, e == cudaErrorMemoryAllocation ? RR_ERR_OUT_OF_MEMORY : RR_ERR_CUDA,
+                            "rr_batch_create: %s", cudaGetErrorString(e)));
+    for (int k = 0; k < 2; ++k) {
+        if ((e = cudaMallocHost(&B->h_call[k], B->call_bytes)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&B->staged[k], cudaEventDisableTiming)) != cudaSuccess)
+            return fail(rr_fail(ctx, RR_ERR_CUDA, "rr_batch_create: %s", cudaGetErrorString(e)));
+    }
+    *out = B;
+    return RR_OK;
+}
+
+extern "C" rr_status rr_batch_execute(rr_ctx* ctx, rr_batch* B, const GpuCameraData* cams, const rr_pt_params* p,
+                                      float* const* radiance_out, void* stream_v) {
+    using namespace rr;
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    if (!B || !cams || !p || !radiance_out) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute: null argument");
+    if (B->ctx != ctx) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute: batch of another context");
+    if (p->spp == 0 || p->max_bounces > uint32_t(kMaxBounces))
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute: bad spp or max_bounces");
+    const bool graph = (p->flags & RR_PT_FLAG_GRAPH) != 0;
+    if (graph && (p->flags & (RR_PT_FLAG_COUNT_TRAVERSAL | RR_PT_FLAG_TIME_STAGES)))
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute: counting and timing flags need non-graph runs");
+    const uint32_t count = uint32_t(B->scenes.size());
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    // per-call table into this call's staging slot (the copy out of it two calls ago has completed)
+    const int k = B->slot;
+    RR_TRY_CUDA(ctx, cudaEventSynchronize(B->staged[k]));
+    BatchEntry* E = reinterpret_cast<BatchEntry*>(B->h_call[k]);
+    float4** O = reinterpret_cast<float4**>(B->h_call[k] + B->entries_bytes);
+    uint64_t paths = 0;
+    uint32_t tiles = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        const GpuCameraData& c = cams[i];
+        if (c.screen_width == 0 || c.screen_height == 0 || !radiance_out[i])
+            return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute: scene %u: empty image or null output", i);
+        BatchEntry& e = E[i];
+        std::memset(&e, 0, sizeof(e));
+        e.L.cam = c;
+        e.L.frame_seed = p->frame_seed;
+        e.L.spp = p->spp;
+        e.L.width = c.screen_width;
+        e.L.height = c.screen_height;
+        e.L.tiles_x = (c.screen_width + 7) / 8;
+        e.L.tiles_per_image = e.L.tiles_x * ((c.screen_height + 3) / 4);
+        e.tile_begin = tiles;
+        const uint64_t t = uint64_t(e.L.tiles_per_image) * p->spp;
+        if (uint64_t(tiles) + t >= (1ull << 26))
+            return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute: too many tiles");
+        tiles += uint32_t(t);
+        paths += uint64_t(c.screen_width) * c.screen_height * p->spp;
+        O[i] = reinterpret_cast<float4*>(radiance_out[i]);
+    }
+    if (paths >= (1ull << 31)) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute: too many paths");
+    rr_status st = ensure_queues(ctx, size_t(paths));
+    if (st != RR_OK) return st;
+    RR_TRY_CUDA(ctx, cudaMemcpyAsync(B->d_call, B->h_call[k], B->call_bytes, cudaMemcpyHostToDevice, stream));
+    RR_TRY_CUDA(ctx, cudaEventRecord(B->staged[k], stream));
+    B->slot ^= 1;
+    if (graph) {
+        rr_batch::Key key;
+        key.paths = paths; key.total_tiles = tiles; key.max_bounces = p->max_bounces;
+        key.ev = uint32_t(ctx->extend_variant); key.sv = uint32_t(ctx->shadow_variant);
+        key.queue = ctx->pt.ray_a[0];
+        if (!B->exec || key != B->key) {
+            if (B->exec) { cudaGraphExecDestroy(B->exec); B->exec = nullptr; }
+            RR_TRY_CUDA(ctx, cudaStreamBeginCapture(B->cap_stream, cudaStreamCaptureModeThreadLocal));
+            st = enqueue_batch(ctx, B, tiles, size_t(paths), p->max_bounces, 0u, B->cap_stream);
+            cudaGraph_t g = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(B->cap_stream, &g);
+            if (st != RR_OK) { if (g) cudaGraphDestroy(g); return st; }
+            if (ce != cudaSuccess) return rr_fail(ctx, RR_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+            const cudaError_t ie = cudaGraphInstantiate(&B->exec, g, 0);
+            cudaGraphDestroy(g);
+            if (ie != cudaSuccess) return rr_fail(ctx, RR_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ie));
+            B->key = key;
+        }
+        RR_TRY_CUDA(ctx, cudaGraphLaunch(B->exec, stream));
+        st = RR_OK;
+    } else {
+        st = enqueue_batch(ctx, B, tiles, size_t(paths), p->max_bounces, p->flags, stream);
+    }
+    ctx->launches += 1 + 3 * uint64_t(p->max_bounces);
+    ctx->last_max_bounces = p->max_bounces;
+    ctx->last_counted = (p->flags & RR_PT_FLAG_COUNT_TRAVERSAL) != 0;
+    return st;
+}
+
+extern "C" rr_status rr_batch_tune(rr_ctx* ctx, rr_batch* B, const GpuCameraData* cams, const rr_pt_params* p,
+                                   float* const* radiance_out, void* stream, rr_pt_tune_result* out) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    if (!B || !cams || !p || !radiance_out || !out)
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_tune: null argument");
+    rr_pt_stats st;
+    rr_status s;
+    if ((s = rr_pathtracer_stats(ctx, &st, 1)) != RR_OK) return s;
+    double best_e = 1e300, best_s = 1e300;
+    rr_pt_params warm = *p, q = *p;
+    warm.flags = 0;
+    q.flags = RR_PT_FLAG_TIME_STAGES;
+    for (int v = 0; v < RR_PT_VARIANT_COUNT; ++v) {
+        ctx->extend_variant = v;
+        ctx->shadow_variant = v;
+        if ((s = rr_batch_execute(ctx, B, cams, &warm, radiance_out, stream)) != RR_OK) return s;
+        if ((s = rr_batch_execute(ctx, B, cams, &q, radiance_out, stream)) != RR_OK) return s;
         if ((s = rr_pathtracer_stats(ctx, &st, 1)) != RR_OK) return s;
         out->extend_ms[v] = st.ms_extend;
         out->shadow_ms[v] = st.ms_shadow;

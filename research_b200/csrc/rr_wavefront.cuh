@@ -120,12 +120,28 @@ struct WarpPool {
 //    one as soon as kRefillLanes lanes are idle, so warps do not wait for
 //    their slowest ray (less coherence, fewer idle lanes).
 // MinBlocks is the occupancy target handed to the register allocator.
-// `Finish(i, found, hit)` consumes a finished ray; `Load(i, ray, tmax)` makes one.
-template <bool AnyHit, bool Count, bool Refill, class Load, class Finish>
-__device__ __forceinline__ void traverse_queue(const DevScene& s, uint32_t count, uint32_t* cursor,
-                                               unsigned long long* work_out, Load load, Finish finish) {
+// `Finish(i, found, hit)` consumes a finished ray; `Load(i, ray, tmax)` makes
+// one and returns its scene index. Multi: a batch of scenes, each ray traced
+// in the scene `table[index]` (the lane binds that scene's node and triangle
+// arrays when it loads the ray); otherwise every ray is traced in `s`.
+template <bool AnyHit, bool Count, bool Refill, bool Multi, class Load, class Finish>
+__device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene* __restrict__ table, uint32_t count,
+                                               uint32_t* cursor, unsigned long long* work_out, Load load,
+                                               Finish finish) {
     TraceWork tw;
     int2 stack[kStackSize];  // (node, near distance)
+    DevScene ls{};           // Multi: the current ray's scene (traversal fields)
+    auto bind = [&](uint32_t sid) {
+        if constexpr (Multi) {
+            ls.nodes = table[sid].nodes;
+            ls.tris = table[sid].tris;
+            ls.num_nodes = table[sid].num_nodes;
+        }
+    };
+    auto step = [&](const Ray& r, HitRec& h, TravState& st) -> bool {
+        if constexpr (Multi) return trace_step<AnyHit, Count>(ls, r, 0.001f, h, st, stack, &tw);
+        else return trace_step<AnyHit, Count>(s, r, 0.001f, h, st, stack, &tw);
+    };
     if constexpr (!Refill) {
         while (true) {
             uint32_t base = 0;
@@ -135,10 +151,10 @@ __device__ __forceinline__ void traverse_queue(const DevScene& s, uint32_t count
             const uint32_t i = base + lane_id();
             if (i < count) {
                 Ray r; float tmax;
-                load(i, r, tmax);
+                bind(load(i, r, tmax));
                 HitRec h; TravState st;
                 trav_begin(st, h, tmax);
-                while (!trace_step<AnyHit, Count>(s, r, 0.001f, h, st, stack, &tw)) {}
+                while (!step(r, h, st)) {}
                 finish(i, st.found, h);
             }
         }
@@ -156,7 +172,7 @@ __device__ __forceinline__ void traverse_queue(const DevScene& s, uint32_t count
                 if (!has && ni != kNoIndex) {
                     idx = ni;
                     float tmax;
-                    load(idx, r, tmax);
+                    bind(load(idx, r, tmax));
                     trav_begin(st, h, tmax);
                     has = true;
                 }
@@ -165,7 +181,7 @@ __device__ __forceinline__ void traverse_queue(const DevScene& s, uint32_t count
                 if (pool.done()) break;
                 continue;
             }
-            if (has && trace_step<AnyHit, Count>(s, r, 0.001f, h, st, stack, &tw)) {
+            if (has && step(r, h, st)) {
                 finish(idx, st.found, h);
                 has = false;
             }
@@ -180,12 +196,13 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) extend_kernel(DevScene s, c
                                                                    float4* __restrict__ hits,
                                                                    const uint32_t* count_ptr, uint32_t* cursor,
                                                                    unsigned long long* work_out) {
-    traverse_queue<false, Count, Refill>(
-        s, *count_ptr, cursor, work_out,
-        [&](uint32_t i, Ray& r, float& tmax) {
+    traverse_queue<false, Count, Refill, false>(
+        s, nullptr, *count_ptr, cursor, work_out,
+        [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = qa[i], b = qb[i];
             r = make_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z));
             tmax = 1e9f;
+            return 0u;
         },
         [&](uint32_t i, bool found, const HitRec& h) {
             hits[i] = found ? make_float4(h.u, h.v, __uint_as_float(h.inst), __uint_as_float(h.prim))
@@ -201,12 +218,13 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) shadow_kernel(DevScene s, c
                                                                    float4* __restrict__ out,
                                                                    const uint32_t* count_ptr, uint32_t* cursor,
                                                                    unsigned long long* work_out) {
-    traverse_queue<true, Count, Refill>(
-        s, *count_ptr, cursor, work_out,
-        [&](uint32_t i, Ray& r, float& tmax) {
+    traverse_queue<true, Count, Refill, false>(
+        s, nullptr, *count_ptr, cursor, work_out,
+        [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = sa[i], b = sb[i];
             r = make_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z));
             tmax = b.w;
+            return 0u;
         },
         [&](uint32_t i, bool found, const HitRec&) {
             if (!found) {
@@ -217,6 +235,135 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) shadow_kernel(DevScene s, c
                 out[pid] = o;
             }
         });
+}
+
+// ── batches of scenes (no reference counterpart: the reference renders one
+// scene per pass execute). Queue entries carry their scene index in the
+// .w of the throughput (rays) and contribution (shadow rays) records.
+struct BatchEntry {
+    PtLaunch L;            // the scene's camera, frame seed, spp and image size
+    uint32_t tile_begin;   // first raygen tile of the scene in the batch
+    uint32_t _pad[3];
+};
+
+// raygen_kernel over all scenes of a batch: the global tile index picks the
+// scene (binary search over tile_begin), the rest is raygen_kernel's.
+__global__ void __launch_bounds__(kBlock) raygen_batch_kernel(const BatchEntry* __restrict__ E, uint32_t n_scenes,
+                                                              uint32_t total_tiles, float4* const* __restrict__ outs,
+                                                              float4* qa, float4* qb, float4* qc,
+                                                              uint32_t* counters) {
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t tile = gtid >> 5;
+    const uint32_t lane = lane_id();
+    bool active = tile < total_tiles;
+    uint32_t sid = 0, s = 0, px = 0, py = 0;
+    if (active) {
+        uint32_t lo = 0, hi = n_scenes - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (E[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
+        }
+        sid = lo;
+        const PtLaunch& L = E[sid].L;
+        const uint32_t local = tile - E[sid].tile_begin;
+        s = local / L.tiles_per_image;
+        const uint32_t t = local % L.tiles_per_image;
+        px = (t % L.tiles_x) * 8 + (lane & 7);
+        py = (t / L.tiles_x) * 4 + (lane >> 3);
+        active = s < L.spp && px < L.width && py < L.height;
+    }
+    if (__all_sync(kFull, tile >= total_tiles)) return;
+    const uint32_t slot = warp_alloc(active, &counters[0]);
+    if (!active) return;
+    const PtLaunch& L = E[sid].L;
+    const uint32_t pid = (s * L.height + py) * L.width + px;
+    uint32_t seed = make_seed(px, py, L.frame_seed + s);
+    const float jx = rand_float(seed);
+    const float jy = rand_float(seed);
+    const float3 dir = primary_dir(L.cam, float(px) + jx, float(py) + jy);
+    outs[sid][pid] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    qa[slot] = make_float4(L.cam.position[0], L.cam.position[1], L.cam.position[2], __uint_as_float(pid));
+    qb[slot] = make_float4(dir.x, dir.y, dir.z, __uint_as_float(seed));
+    qc[slot] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(sid));
+}
+
+template <bool Count, bool Refill, int MinBlocks>
+__global__ void __launch_bounds__(kBlock, MinBlocks) extend_batch_kernel(const DevScene* __restrict__ table,
+                                                                         const float4* __restrict__ qa,
+                                                                         const float4* __restrict__ qb,
+                                                                         const float4* __restrict__ qc,
+                                                                         float4* __restrict__ hits,
+                                                                         const uint32_t* count_ptr, uint32_t* cursor,
+                                                                         unsigned long long* work_out) {
+    const DevScene none{};
+    traverse_queue<false, Count, Refill, true>(
+        none, table, *count_ptr, cursor, work_out,
+        [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
+            const float4 a = qa[i], b = qb[i];
+            r = make_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z));
+            tmax = 1e9f;
+            return __float_as_uint(qc[i].w);
+        },
+        [&](uint32_t i, bool found, const HitRec& h) {
+            hits[i] = found ? make_float4(h.u, h.v, __uint_as_float(h.inst), __uint_as_float(h.prim))
+                            : make_float4(0.0f, 0.0f, __uint_as_float(kNoIndex), __uint_as_float(kNoIndex));
+        });
+}
+
+template <bool Count, bool Refill, int MinBlocks>
+__global__ void __launch_bounds__(kBlock, MinBlocks) shadow_batch_kernel(const DevScene* __restrict__ table,
+                                                                         float4* const* __restrict__ outs,
+                                                                         const float4* __restrict__ sa,
+                                                                         const float4* __restrict__ sb,
+                                                                         const float4* __restrict__ sc,
+                                                                         const uint32_t* count_ptr, uint32_t* cursor,
+                                                                         unsigned long long* work_out) {
+    const DevScene none{};
+    traverse_queue<true, Count, Refill, true>(
+        none, table, *count_ptr, cursor, work_out,
+        [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
+            const float4 a = sa[i], b = sb[i];
+            r = make_ray(f3(a.x, a.y, a.z), f3(b.x, b.y, b.z));
+            tmax = b.w;
+            return __float_as_uint(sc[i].w);
+        },
+        [&](uint32_t i, bool found, const HitRec&) {
+            if (!found) {
+                const float4 c = sc[i];
+                const uint32_t pid = __float_as_uint(sa[i].w);
+                float4* out = outs[__float_as_uint(c.w)];
+                float4 o = out[pid];
+                o.x = o.x + c.x; o.y = o.y + c.y; o.z = o.z + c.z;
+                out[pid] = o;
+            }
+        });
+}
+
+using BatchQueueKernel = void (*)(const DevScene*, const float4*, const float4*, const float4*, float4*,
+                                  const uint32_t*, uint32_t*, unsigned long long*);
+using BatchShadowKernel = void (*)(const DevScene*, float4* const*, const float4*, const float4*, const float4*,
+                                   const uint32_t*, uint32_t*, unsigned long long*);
+template <bool Count>
+BatchQueueKernel extend_batch_variant(int v) {
+    switch (v) {
+    case 1: return extend_batch_kernel<Count, false, 5>;
+    case 2: return extend_batch_kernel<Count, false, 6>;
+    case 3: return extend_batch_kernel<Count, true, 1>;
+    case 4: return extend_batch_kernel<Count, true, 5>;
+    case 5: return extend_batch_kernel<Count, true, 6>;
+    default: return extend_batch_kernel<Count, false, 1>;
+    }
+}
+template <bool Count>
+BatchShadowKernel shadow_batch_variant(int v) {
+    switch (v) {
+    case 1: return shadow_batch_kernel<Count, false, 5>;
+    case 2: return shadow_batch_kernel<Count, false, 6>;
+    case 3: return shadow_batch_kernel<Count, true, 1>;
+    case 4: return shadow_batch_kernel<Count, true, 5>;
+    case 5: return shadow_batch_kernel<Count, true, 6>;
+    default: return shadow_batch_kernel<Count, false, 1>;
+    }
 }
 
 // Traversal kernel variants: schedule x occupancy target.

@@ -66,6 +66,7 @@ class PtTuneResult(C.Structure):
 
 PT_FLAG_COUNT_TRAVERSAL = 1
 PT_FLAG_TIME_STAGES = 2
+PT_FLAG_GRAPH = 4
 
 
 class PtParams(C.Structure):
@@ -182,6 +183,11 @@ _SIGNATURES = {
     "rr_guiding_fit": (I, [P, P, P, C.POINTER(GuidingParams), P]),
     "rr_guiding_sample": (I, [P, P, P, P, P, P, U32, C.POINTER(F32), C.POINTER(GuidingParams), P, P, P]),
     "rr_guiding_reset": (I, [P, P, P, C.POINTER(GuidingParams), P]),
+    "rr_batch_create": (I, [P, C.POINTER(P), U32, C.POINTER(P)]),
+    "rr_batch_destroy": (I, [P]),
+    "rr_batch_execute": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtParams), C.POINTER(P), P]),
+    "rr_batch_tune": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtParams), C.POINTER(P), P,
+                          C.POINTER(PtTuneResult)]),
     "rr_restir_pt_initial": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtReuseParams), C.POINTER(PtReuseImages), P]),
     "rr_restir_pt_temporal": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtReuseParams), C.POINTER(PtReuseImages), P]),
     "rr_restir_pt_spatial_shade": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtReuseParams),
@@ -367,6 +373,41 @@ class Context:
     def close(self):
         if self._h:
             lib().rr_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many scenes rendered by one set of wavefront launches (rr_batch_*)."""
+
+    def __init__(self, ctx: "Context", scenes):
+        self.ctx = ctx
+        self.scenes = list(scenes)
+        arr = (P * len(self.scenes))(*[sc.handle for sc in self.scenes])
+        self._h = P()
+        ctx.check(lib().rr_batch_create(ctx.handle, arr, len(self.scenes), C.byref(self._h)))
+
+    def execute(self, cameras, params, outputs, stream):
+        cams = (GpuCameraData * len(cameras))(*cameras)
+        outs = (P * len(outputs))(*outputs)
+        self.ctx.check(lib().rr_batch_execute(self.ctx.handle, self._h, cams, C.byref(params), outs, stream))
+
+    def tune(self, cameras, params, outputs, stream) -> "PtTuneResult":
+        cams = (GpuCameraData * len(cameras))(*cameras)
+        outs = (P * len(outputs))(*outputs)
+        r = PtTuneResult()
+        self.ctx.check(lib().rr_batch_tune(self.ctx.handle, self._h, cams, C.byref(params), outs, stream,
+                                           C.byref(r)))
+        return r
+
+    def close(self):
+        if self._h:
+            lib().rr_batch_destroy(self._h)
             self._h = None
 
     def __del__(self):
