@@ -370,6 +370,64 @@ rr_status rr_restir_pt_execute(rr_ctx* ctx, const rr_scene* scene, const GpuCame
 rr_status rr_restir_pt_reset_history(rr_ctx* ctx, const rr_restir_pt_images* images, uint32_t width,
                                      uint32_t height, void* stream);
 
+/* ── ReSTIR GI: ReSTIRGIPass::execute (ReSTIRGIPass.cpp:428-650; kernels in
+ * passes/restir_gi/restir_gi.slang) ──────────────────────────────────────
+ * rr_restir_gi_params holds the ReSTIRGIPushConstants fields
+ * (restir_gi.slang:18-55) other than the bindless indices. Reference
+ * defaults (ReSTIRGIPass.h:67-74) in comments. */
+typedef struct rr_restir_gi_params {
+    uint32_t frame_seed;               /* frame_count_++ */
+    uint32_t num_initial_candidates;   /* 8 */
+    uint32_t temporal_enable;          /* 1 */
+    uint32_t spatial_enable;           /* 1 */
+    uint32_t spatial_num_neighbors;    /* 4 */
+    uint32_t spatial_radius;           /* 12 */
+    uint32_t include_direct_lighting;  /* 1 */
+    float    indirect_strength;        /* 1.0 */
+    float    ray_bias;                 /* 1e-3 */
+    uint32_t _pad[3];
+} rr_restir_gi_params;
+
+/* The pass's images, every one width x height RGBA32F, device memory owned
+ * by the caller. The reservoir is three images (restir_gi.slang:3-7):
+ * [0] (sample_pos, w_sum), [1] (sample_radiance, W), [2] (sample_normal,
+ * asfloat(M)); the primary history is (position, t) and (normal,
+ * asfloat(material)). "curr" and "prev" swap after every frame, as
+ * ReSTIRGIPass::execute flips reservoir_flip_. */
+typedef struct rr_restir_gi_images {
+    const float* gbuf_pos;        /* ReSTIR DI's G-buffer (restir_di.slang:212-223) */
+    const float* gbuf_norm;
+    const float* direct;          /* direct lighting to add (the DI output) or NULL */
+    float*       reservoir_curr[3];
+    float*       reservoir_prev[3];
+    float*       history_curr[2];
+    float*       history_prev[2];
+    float*       output;
+} rr_restir_gi_images;
+
+/* cs_initial (restir_gi.slang:568-686): writes reservoir_curr and history_curr. */
+rr_status rr_restir_gi_initial(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
+                               const rr_restir_gi_params* params, const rr_restir_gi_images* images,
+                               void* stream);
+/* cs_temporal (restir_gi.slang:688-848); returns at once when temporal_enable is 0. */
+rr_status rr_restir_gi_temporal(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
+                                const rr_restir_gi_params* params, const rr_restir_gi_images* images,
+                                void* stream);
+/* cs_spatial_shade (restir_gi.slang:851-1000). */
+rr_status rr_restir_gi_spatial_shade(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
+                                     const rr_restir_gi_params* params,
+                                     const rr_restir_gi_images* images, void* stream);
+/* The three dispatches of one ReSTIRGIPass::execute in order; the caller
+ * swaps curr and prev afterwards. */
+rr_status rr_restir_gi_execute(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
+                               const rr_restir_gi_params* params, const rr_restir_gi_images* images,
+                               void* stream);
+/* History reset (ReSTIRGIPass.cpp:484-530, consume_history_dirty): the prev
+ * reservoir images to zero, the prev history position to (0, 0, 0, -1) and
+ * normal to zero. */
+rr_status rr_restir_gi_reset_history(rr_ctx* ctx, const rr_restir_gi_images* images, uint32_t width,
+                                     uint32_t height, void* stream);
+
 /* ── guided path tracing (no reference counterpart beyond the hash grid
  * above: the reference guides only ReSTIR PT's primary bounce with one vMF
  * lobe per hashed cell, restir_pt.slang:520-563). A guide predicts a mixture

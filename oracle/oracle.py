@@ -43,6 +43,18 @@ class PtReuseImages(C.Structure):
                 ("guiding_accum", P), ("guiding_fitted", P)]
 
 
+class GiReuseParams(C.Structure):
+    """OracleRestirGiParams (ReSTIRGIPushConstants minus the bindless indices)."""
+    _fields_ = [("frame_seed", U32), ("num_initial_candidates", U32), ("temporal_enable", U32),
+                ("spatial_enable", U32), ("spatial_num_neighbors", U32), ("spatial_radius", U32),
+                ("include_direct_lighting", U32), ("indirect_strength", F32), ("ray_bias", F32), ("_pad", U32 * 3)]
+
+
+class GiReuseImages(C.Structure):
+    _fields_ = [("gbuf_pos", P), ("gbuf_norm", P), ("direct", P), ("reservoir_curr", P * 3),
+                ("reservoir_prev", P * 3), ("history_curr", P * 2), ("history_prev", P * 2), ("output", P)]
+
+
 _SIG = {
     "oracle_pcg_hash": (U32, [U32]),
     "oracle_make_seed": (U32, [U32, U32, U32]),
@@ -70,6 +82,9 @@ _SIG = {
     "oracle_restir_pt_initial": (None, [P, P, C.POINTER(PtReuseParams), C.POINTER(PtReuseImages), I]),
     "oracle_restir_pt_temporal": (None, [P, P, C.POINTER(PtReuseParams), C.POINTER(PtReuseImages), I]),
     "oracle_restir_pt_spatial_shade": (None, [P, P, C.POINTER(PtReuseParams), C.POINTER(PtReuseImages), I]),
+    "oracle_restir_gi_initial": (None, [P, P, C.POINTER(GiReuseParams), C.POINTER(GiReuseImages), I]),
+    "oracle_restir_gi_temporal": (None, [P, P, C.POINTER(GiReuseParams), C.POINTER(GiReuseImages), I]),
+    "oracle_restir_gi_spatial_shade": (None, [P, P, C.POINTER(GiReuseParams), C.POINTER(GiReuseImages), I]),
 }
 
 _lib = None
@@ -236,6 +251,39 @@ def restir_pt_temporal(scene, cam, p, img, nthreads=None):
 
 def restir_pt_spatial_shade(scene, cam, p, img, nthreads=None):
     lib().oracle_restir_pt_spatial_shade(scene.handle, _cam_ptr(cam), C.byref(p), C.byref(pt_reuse_images(img)),
+                                         nthreads or threads())
+
+
+def gi_reuse_params(frame_seed=0, candidates=8, temporal=1, spatial=1, neighbors=4, radius=12, include_direct=1,
+                    indirect_strength=1.0, ray_bias=1e-3):
+    """ReSTIRGIPass.h:67-74 defaults."""
+    return GiReuseParams(frame_seed, candidates, temporal, spatial, neighbors, radius, include_direct,
+                         indirect_strength, ray_bias, (U32 * 3)(0, 0, 0))
+
+
+def gi_reuse_images(img: dict) -> GiReuseImages:
+    """img: gbuf_pos, gbuf_norm, direct (or None), res_curr[3], res_prev[3], hist_curr[2], hist_prev[2], output —
+    C-contiguous float32 (H, W, 4) images."""
+    def ptr(a):
+        return None if a is None else _p(a)
+    return GiReuseImages(ptr(img["gbuf_pos"]), ptr(img["gbuf_norm"]), ptr(img.get("direct")),
+                         (P * 3)(*[ptr(a) for a in img["res_curr"]]), (P * 3)(*[ptr(a) for a in img["res_prev"]]),
+                         (P * 2)(*[ptr(a) for a in img["hist_curr"]]), (P * 2)(*[ptr(a) for a in img["hist_prev"]]),
+                         ptr(img["output"]))
+
+
+def restir_gi_initial(scene, cam, p, img, nthreads=None):
+    lib().oracle_restir_gi_initial(scene.handle, _cam_ptr(cam), C.byref(p), C.byref(gi_reuse_images(img)),
+                                   nthreads or threads())
+
+
+def restir_gi_temporal(scene, cam, p, img, nthreads=None):
+    lib().oracle_restir_gi_temporal(scene.handle, _cam_ptr(cam), C.byref(p), C.byref(gi_reuse_images(img)),
+                                    nthreads or threads())
+
+
+def restir_gi_spatial_shade(scene, cam, p, img, nthreads=None):
+    lib().oracle_restir_gi_spatial_shade(scene.handle, _cam_ptr(cam), C.byref(p), C.byref(gi_reuse_images(img)),
                                          nthreads or threads())
 
 

@@ -724,6 +724,89 @@ bool pt_visible(const OracleScene& s, V3 origin, V3 normal, V3 target, float bia
     return !trace_scene<true>(s, origin + normal * bias, dir, bias, dist - bias).hit;
 }
 
+// ── ReSTIR GI (restir_gi.slang) ────────────────────────────────────────────
+struct GiRes {   // three-image reservoir (restir_gi.slang:3-7, 199-238)
+    V3 pos, rad, nrm;
+    float w_sum, W;
+    uint32_t M;
+};
+inline GiRes gi_load(float* const* img, size_t px) {
+    const float* a = img[0] + 4 * px; const float* b = img[1] + 4 * px; const float* c = img[2] + 4 * px;
+    return GiRes{load3(a), load3(b), load3(c), a[3], b[3], asuint(c[3])};
+}
+inline void gi_store(float* const* img, size_t px, const GiRes& r) {
+    put4(img[0] + 4 * px, r.pos, r.w_sum);
+    put4(img[1] + 4 * px, r.rad, r.W);
+    put4(img[2] + 4 * px, r.nrm, asfloat(r.M));
+}
+inline void gi_store_empty(float* const* img, size_t px) {   // write_empty_reservoir (:192-197)
+    put4(img[0] + 4 * px, v3(0, 0, 0), 0.0f);
+    put4(img[1] + 4 * px, v3(0, 0, 0), 0.0f);
+    put4(img[2] + 4 * px, v3(0, 0, 0), asfloat(0u));
+}
+// evaluate_indirect_radiance (:487-508)
+V3 gi_indirect(V3 pp, V3 pn, const GpuMaterial& pm, V3 cam, V3 spos, V3 srad) {
+    V3 to_sample = spos - pp;
+    float dist2 = dot(to_sample, to_sample);
+    if (dist2 <= 1e-8f) return v3(0, 0, 0);
+    V3 wi = to_sample * rsqrt_hlsl(dist2);
+    float cos_x = fmaxs(dot(pn, wi), 0.0f);
+    if (cos_x <= 0.0f) return v3(0, 0, 0);
+    V3 wo = normalize(cam - pp);
+    V3 brdf_val = brdf_eval(pn, wo, wi, load3(pm.base_color), pm.metallic, pm.roughness);
+    return brdf_val * srad * cos_x;
+}
+// compute_target_function (:524-537)
+float gi_target(V3 pp, V3 pn, const GpuMaterial& pm, V3 cam, V3 spos, V3 srad) {
+    return luminance709(gi_indirect(pp, pn, pm, cam, spos, srad));
+}
+// sample_primary_pdf (:510-522)
+float gi_primary_pdf(V3 pp, V3 pn, V3 spos) {
+    V3 delta = spos - pp;
+    float dist2 = dot(delta, delta);
+    if (dist2 <= 1e-8f) return 0.0f;
+    V3 wi = delta * rsqrt_hlsl(dist2);
+    float cos_x = fmaxs(dot(pn, wi), 0.0f);
+    return fmaxs(cos_x * kInvPi, 0.0f);
+}
+// find_reprojected_history_surface (:358-433) with reproject_to_prev_pixel (:306-336)
+bool gi_find_history(const GpuCameraData& cam, float* const* hist_prev, V3 pp, V3 pn, uint32_t pmat, V3 cp,
+                     size_t& hist, V3& hpos) {
+    const uint32_t W = cam.screen_width, H = cam.screen_height;
+    V4 clip = mul44(cam.prev_view_proj, V4{pp.x, pp.y, pp.z, 1.0f});
+    if (clip.w <= 1.0e-6f) return false;
+    float nx = clip.x / clip.w, ny = clip.y / clip.w;
+    if (fabsf(nx) > 1.0f || fabsf(ny) > 1.0f) return false;
+    float fx = (nx * 0.5f + 0.5f) * float(W) - 0.5f;
+    float fy = (ny * 0.5f + 0.5f) * float(H) - 0.5f;
+    int cx = (int)floorf(fx + 0.5f), cy = (int)floorf(fy + 0.5f);
+    if (cx < 0 || cy < 0 || cx >= (int)W || cy >= (int)H) return false;
+    bool found = false;
+    float best = 1e30f;
+    hist = 0;
+    hpos = v3(0, 0, 0);
+    for (int oy = -1; oy <= 1; ++oy)
+        for (int ox = -1; ox <= 1; ++ox) {
+            int qx = cx + ox, qy = cy + oy;
+            if (qx < 0 || qy < 0 || qx >= (int)W || qy >= (int)H) continue;
+            size_t j = (size_t)qy * W + qx;
+            const float* h4 = hist_prev[0] + 4 * j;
+            const float* hn4 = hist_prev[1] + 4 * j;
+            if (h4[3] < 0.0f) continue;
+            V3 cpos = load3(h4), cn = normalize(load3(hn4));
+            // is_reprojected_history_compatible (:338-356)
+            if (pmat != asuint(hn4[3])) continue;
+            if (dot(pn, cn) < 0.9f) continue;
+            float view_dist = fmaxs(length(pp - cp), 1.0f);
+            float plane = fabsf(dot(cpos - pp, pn));
+            float dpos = length(cpos - pp);
+            if (!(plane <= 0.01f * view_dist && dpos <= 0.05f * view_dist)) continue;
+            float err = plane * 4.0f + dpos;
+            if (err < best) { best = err; hist = j; hpos = cpos; found = true; }
+        }
+    return found;
+}
+
 } // namespace
 
 // ═══════════════════════════════ C API ═════════════════════════════════════
@@ -1410,6 +1493,194 @@ void oracle_restir_pt_spatial_shade(const OracleScene* scene, const GpuCameraDat
                         __atomic_fetch_add(a + 3, 1u, __ATOMIC_RELAXED);
                     }
                 }
+            }
+            put4(img->output + 4 * px, radiance, 1.0f);
+        }
+    });
+}
+
+// ── ReSTIR GI (restir_gi.slang:568-1000; ReSTIRGIPass.cpp:428-650) ────────────
+void oracle_restir_gi_initial(const OracleScene* scene, const GpuCameraData* cam, const OracleRestirGiParams* p,
+                              const OracleRestirGiImages* img, int threads) {
+    const OracleScene& s = *scene;
+    const uint32_t W = cam->screen_width, H = cam->screen_height;
+    const V3 cp = load3(cam->position);
+    const float bias = p->ray_bias;
+    parallel_rows(H, threads, [&](uint32_t y) {
+        for (uint32_t x = 0; x < W; ++x) {
+            const size_t px = (size_t)y * W + x;
+            uint32_t seed = make_seed(x, y, p->frame_seed);
+            V3 pp, pn; uint32_t pmat;
+            if (!pt_surface(s, img->gbuf_pos, img->gbuf_norm, px, pp, pn, pmat)) {
+                put4(img->history_curr[0] + 4 * px, v3(0, 0, 0), -1.0f);
+                put4(img->history_curr[1] + 4 * px, v3(0, 0, 0), 0.0f);
+                gi_store_empty(img->reservoir_curr, px);
+                continue;
+            }
+            memcpy(img->history_curr[0] + 4 * px, img->gbuf_pos + 4 * px, 16);
+            memcpy(img->history_curr[1] + 4 * px, img->gbuf_norm + 4 * px, 16);
+            const GpuMaterial& pm = s.materials[pmat];
+            V3 sel_pos = v3(0, 0, 0), sel_rad = v3(0, 0, 0), sel_nrm = v3(0, 0, 0);
+            float w_sum = 0.0f;
+            uint32_t M_count = 0;
+            for (uint32_t c = 0; c < p->num_initial_candidates; ++c) {
+                float u0 = rand_float(seed);   // arguments evaluated left to right
+                float u1 = rand_float(seed);
+                float pdf_dir;
+                V3 local = sample_cosine_hemisphere(u0, u1, pdf_dir);
+                V3 T, B;
+                build_onb(pn, T, B);
+                V3 bounce = tangent_to_world(local, T, B, pn);
+                if (dot(pn, bounce) <= 0.0f) continue;
+                Hit sh = trace_scene<false>(s, pp + pn * bias, bounce, bias, 1e9f);
+                if (!sh.hit) continue;
+                Surf sec = hit_surface(s, sh);
+                // evaluate_sample_radiance (:539-552)
+                V3 wo = -bounce;
+                V3 sn = sec.normal;
+                if (dot(sn, wo) < 0.0f) sn = -sn;
+                const GpuMaterial& sm = s.materials[sec.material];
+                V3 rad = load3(sm.emissive);
+                rad = rad + pt_sample_lights(s, sec.pos, sn, wo, sm, bias, seed);
+                float tgt = gi_target(pp, pn, pm, cp, sec.pos, rad);
+                if (tgt <= 0.0f) continue;
+                float pdf = gi_primary_pdf(pp, pn, sec.pos);
+                if (pdf <= 1e-6f) continue;
+                float weight = tgt / pdf;
+                w_sum += weight;
+                M_count++;
+                if (w_sum > 0.0f && rand_float(seed) < weight / w_sum) {
+                    sel_pos = sec.pos; sel_rad = rad; sel_nrm = sec.normal;
+                }
+            }
+            bool stored = false;
+            if (M_count > 0) {
+                float ph_y = gi_target(pp, pn, pm, cp, sel_pos, sel_rad);
+                if (ph_y > 1e-10f) {
+                    gi_store(img->reservoir_curr, px,
+                             GiRes{sel_pos, sel_rad, sel_nrm, w_sum, w_sum / (float(M_count) * ph_y), M_count});
+                    stored = true;
+                }
+            }
+            if (!stored) gi_store_empty(img->reservoir_curr, px);
+        }
+    });
+}
+
+void oracle_restir_gi_temporal(const OracleScene* scene, const GpuCameraData* cam, const OracleRestirGiParams* p,
+                               const OracleRestirGiImages* img, int threads) {
+    if (!p->temporal_enable) return;
+    const OracleScene& s = *scene;
+    const uint32_t W = cam->screen_width, H = cam->screen_height;
+    const V3 cp = load3(cam->position);
+    const uint32_t m_cap = std::min(std::max(20u * p->num_initial_candidates, 1u), 8192u);
+    parallel_rows(H, threads, [&](uint32_t y) {
+        for (uint32_t x = 0; x < W; ++x) {
+            const size_t px = (size_t)y * W + x;
+            V3 pp, pn; uint32_t pmat;
+            if (!pt_surface(s, img->gbuf_pos, img->gbuf_norm, px, pp, pn, pmat)) continue;
+            const GpuMaterial& pm = s.materials[pmat];
+            size_t hist; V3 hpos;
+            if (!gi_find_history(*cam, img->history_prev, pp, pn, pmat, cp, hist, hpos)) continue;
+            GiRes cur = gi_load(img->reservoir_curr, px);
+            GiRes prv = gi_load(img->reservoir_prev, hist);
+            if (prv.M == 0) continue;
+            prv.M = std::min(prv.M, m_cap);
+            float jac = pt_jacobian(hpos, pp, prv.pos, prv.nrm);
+            if (jac <= 0.0f) continue;
+            if (!pt_visible(s, pp, pn, prv.pos, p->ray_bias)) continue;
+            float ph_prev = gi_target(pp, pn, pm, cp, prv.pos, prv.rad);
+            float prev_W = fmins(prv.W, 50.0f);
+            float contrib = ph_prev * prev_W * float(prv.M) * jac;
+            if (contrib <= 0.0f) continue;
+            cur.w_sum += contrib;
+            uint32_t seed = make_seed(x, y, p->frame_seed + 1u);
+            if (cur.w_sum > 0.0f && rand_float(seed) < contrib / cur.w_sum) {
+                cur.pos = prv.pos; cur.rad = prv.rad; cur.nrm = prv.nrm;
+            }
+            uint32_t new_M = cur.M + prv.M;
+            if (new_M > m_cap) { cur.w_sum *= float(m_cap) / float(new_M); cur.M = m_cap; }
+            else cur.M = new_M;
+            float W_new = 0.0f;
+            if (cur.M > 0) {
+                float ph_y = gi_target(pp, pn, pm, cp, cur.pos, cur.rad);
+                W_new = (ph_y > 1e-10f) ? (cur.w_sum / (float(cur.M) * ph_y)) : 0.0f;
+                W_new = fmins(W_new, 50.0f);
+            }
+            cur.W = W_new;
+            gi_store(img->reservoir_curr, px, cur);
+        }
+    });
+}
+
+void oracle_restir_gi_spatial_shade(const OracleScene* scene, const GpuCameraData* cam,
+                                    const OracleRestirGiParams* p, const OracleRestirGiImages* img, int threads) {
+    const OracleScene& s = *scene;
+    const uint32_t W = cam->screen_width, H = cam->screen_height;
+    const V3 cp = load3(cam->position);
+    parallel_rows(H, threads, [&](uint32_t y) {
+        for (uint32_t x = 0; x < W; ++x) {
+            const size_t px = (size_t)y * W + x;
+            V3 radiance = v3(0, 0, 0);
+            if (p->include_direct_lighting != 0 && img->direct) radiance = radiance + load3(img->direct + 4 * px);
+            V3 pp, pn; uint32_t pmat;
+            if (!pt_surface(s, img->gbuf_pos, img->gbuf_norm, px, pp, pn, pmat)) {
+                if (p->include_direct_lighting == 0) {
+                    V3 o, d;
+                    primary_ray(*cam, x, y, 0.5f, 0.5f, o, d);
+                    radiance = radiance + sky(d);
+                }
+                put4(img->output + 4 * px, radiance, 1.0f);
+                continue;
+            }
+            const GpuMaterial& pm = s.materials[pmat];
+            if (any_positive(pm.emissive)) {
+                radiance = radiance + load3(pm.emissive);
+                put4(img->output + 4 * px, radiance, 1.0f);
+                continue;
+            }
+            GiRes r = gi_load(img->reservoir_curr, px);
+            if (p->spatial_enable && p->spatial_num_neighbors > 0) {
+                const float base_phase = frac_hlsl(float(pcg_hash(x ^ (y * 65537u))) * 2.3283064365386963e-10f);
+                for (uint32_t k = 0; k < p->spatial_num_neighbors; ++k) {
+                    float u = (float(k) + 0.5f) / float(p->spatial_num_neighbors);
+                    float angle = frac_hlsl(base_phase + 0.61803398875f * float(k)) * kTwoPi;
+                    float radius = sqrtf(u) * float(p->spatial_radius);
+                    int ox = (int)(radius * rr_cosf(angle)), oy = (int)(radius * rr_sinf(angle));
+                    int nx = std::min(std::max((int)x + ox, 0), (int)W - 1);
+                    int ny = std::min(std::max((int)y + oy, 0), (int)H - 1);
+                    if (nx == (int)x && ny == (int)y) continue;
+                    size_t j = (size_t)ny * W + nx;
+                    // is_spatial_neighbor_compatible (:435-459)
+                    const float* nb4 = img->gbuf_pos + 4 * j;
+                    if (nb4[3] < 0.0f) continue;
+                    V3 nbp = load3(nb4), nbn = normalize(load3(img->gbuf_norm + 4 * j));
+                    if (dot(nbn, pn) < 0.85f) continue;
+                    float plane = fabsf(dot(nbp - pp, pn));
+                    float dscale = fmaxs(length(pp - cp), 1.0f);
+                    if (!(plane <= 0.02f * dscale)) continue;
+                    GiRes nb = gi_load(img->reservoir_curr, j);
+                    if (nb.M == 0) continue;
+                    float jac = pt_jacobian(nbp, pp, nb.pos, nb.nrm);
+                    if (jac <= 0.0f) continue;
+                    float contrib = gi_target(pp, pn, pm, cp, nb.pos, nb.rad) * nb.W * float(nb.M) * jac;
+                    if (contrib <= 0.0f) continue;
+                    r.w_sum += contrib;
+                    r.M += nb.M;
+                    float accept = frac_hlsl(base_phase + 0.754877666f * float(k + 1u));
+                    if (r.w_sum > 0.0f && accept < contrib / r.w_sum) {
+                        r.pos = nb.pos; r.rad = nb.rad; r.nrm = nb.nrm;
+                    }
+                }
+                if (r.M > 0) {
+                    float ph_y = gi_target(pp, pn, pm, cp, r.pos, r.rad);
+                    r.W = (ph_y > 1e-10f) ? (r.w_sum / (float(r.M) * ph_y)) : 0.0f;
+                }
+            }
+            if (r.M > 0 && r.W > 0.0f) {
+                V3 indirect = gi_indirect(pp, pn, pm, cp, r.pos, r.rad) * r.W;
+                if (luminance709(indirect) > 0.0f && pt_visible(s, pp, pn, r.pos, p->ray_bias))
+                    radiance = radiance + indirect * p->indirect_strength;
             }
             put4(img->output + 4 * px, radiance, 1.0f);
         }

@@ -177,6 +177,40 @@ void oracle_restir_pt_spatial_shade(const OracleScene* scene, const GpuCameraDat
                                     const OracleRestirPtParams* p, const OracleRestirPtImages* img,
                                     int threads);
 
+/* ── ReSTIR GI (restir_gi.slang:568-1000) ───────────────────────────────── */
+typedef struct OracleRestirGiParams {
+    uint32_t frame_seed;
+    uint32_t num_initial_candidates;
+    uint32_t temporal_enable;
+    uint32_t spatial_enable;
+    uint32_t spatial_num_neighbors;
+    uint32_t spatial_radius;
+    uint32_t include_direct_lighting;
+    float    indirect_strength;
+    float    ray_bias;
+    uint32_t _pad[3];
+} OracleRestirGiParams;
+
+/* Images: width x height x 4 floats each (reservoir [0..2], history [0..1]). */
+typedef struct OracleRestirGiImages {
+    const float* gbuf_pos;
+    const float* gbuf_norm;
+    const float* direct;          /* or NULL */
+    float*       reservoir_curr[3];
+    float*       reservoir_prev[3];
+    float*       history_curr[2];
+    float*       history_prev[2];
+    float*       output;
+} OracleRestirGiImages;
+
+void oracle_restir_gi_initial(const OracleScene* scene, const GpuCameraData* cam,
+                              const OracleRestirGiParams* p, const OracleRestirGiImages* img, int threads);
+void oracle_restir_gi_temporal(const OracleScene* scene, const GpuCameraData* cam,
+                               const OracleRestirGiParams* p, const OracleRestirGiImages* img, int threads);
+void oracle_restir_gi_spatial_shade(const OracleScene* scene, const GpuCameraData* cam,
+                                    const OracleRestirGiParams* p, const OracleRestirGiImages* img,
+                                    int threads);
+
 /* ── BRDF (BRDF.slang) for direct checks ────────────────────────────────── */
 void oracle_brdf_eval(const float n[3], const float wo[3], const float wi[3],
                       const float base[3], float metallic, float roughness, float out[3]);

@@ -122,6 +122,28 @@ def pt_reuse_params(frame_seed=0, candidates=8, max_bounces=4, temporal=1, spati
                          indirect_strength, ray_bias, (C.c_uint32 * 2)(0, 0), g)
 
 
+class GiReuseParams(C.Structure):
+    """rr_restir_gi_params (ReSTIRGIPushConstants minus the bindless indices)."""
+    _fields_ = [("frame_seed", C.c_uint32), ("num_initial_candidates", C.c_uint32), ("temporal_enable", C.c_uint32),
+                ("spatial_enable", C.c_uint32), ("spatial_num_neighbors", C.c_uint32), ("spatial_radius", C.c_uint32),
+                ("include_direct_lighting", C.c_uint32), ("indirect_strength", C.c_float), ("ray_bias", C.c_float),
+                ("_pad", C.c_uint32 * 3)]
+
+
+class GiReuseImages(C.Structure):
+    """rr_restir_gi_images: device pointers (float4 per pixel)."""
+    _fields_ = [("gbuf_pos", C.c_void_p), ("gbuf_norm", C.c_void_p), ("direct", C.c_void_p),
+                ("reservoir_curr", C.c_void_p * 3), ("reservoir_prev", C.c_void_p * 3),
+                ("history_curr", C.c_void_p * 2), ("history_prev", C.c_void_p * 2), ("output", C.c_void_p)]
+
+
+def gi_reuse_params(frame_seed=0, candidates=8, temporal=1, spatial=1, neighbors=4, radius=12, include_direct=1,
+                    indirect_strength=1.0, ray_bias=1e-3) -> "GiReuseParams":
+    """Reference defaults of ReSTIRGIPass.h:67-74."""
+    return GiReuseParams(frame_seed, candidates, temporal, spatial, neighbors, radius, include_direct,
+                         indirect_strength, ray_bias, (C.c_uint32 * 3)(0, 0, 0))
+
+
 class GuideDesc(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("grid_resolution", C.c_uint32), ("alpha", C.c_float), ("decay", C.c_float),
                 ("bounds_min", C.c_float * 3), ("bounds_max", C.c_float * 3), ("max_samples", C.c_uint32),
@@ -194,6 +216,12 @@ _SIGNATURES = {
                                        C.POINTER(PtReuseImages), P]),
     "rr_restir_pt_execute": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtReuseParams), C.POINTER(PtReuseImages), P]),
     "rr_restir_pt_reset_history": (I, [P, C.POINTER(PtReuseImages), U32, U32, P]),
+    "rr_restir_gi_initial": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(GiReuseParams), C.POINTER(GiReuseImages), P]),
+    "rr_restir_gi_temporal": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(GiReuseParams), C.POINTER(GiReuseImages), P]),
+    "rr_restir_gi_spatial_shade": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(GiReuseParams),
+                                       C.POINTER(GiReuseImages), P]),
+    "rr_restir_gi_execute": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(GiReuseParams), C.POINTER(GiReuseImages), P]),
+    "rr_restir_gi_reset_history": (I, [P, C.POINTER(GiReuseImages), U32, U32, P]),
     "rr_trace_closest": (I, [P, P, P, P, F32, F32, U32, P, P, P]),
     "rr_tonemap_execute": (I, [P, P, U32, U32, F32, P, P]),
     "rr_guide_create": (I, [P, C.POINTER(GuideDesc), C.POINTER(P)]),
