@@ -6,14 +6,16 @@
  * (rr_scene_desc) and the per-frame GpuCameraData block:
  *   - rr_host_scene_cornell: Scene::build_cornell_box (Scene.cpp:144-251)
  *   - rr_host_scene_procedural / _instanced: seeded synthetic scenes of the
- *     benchmark configurations (no reference counterpart; the reference loads
- *     glTF files, GltfLoader.cpp:79-365, which are not part of this build)
+ *     benchmark configurations (no reference counterpart)
+ *   - rr_host_scene_gltf: GltfLoader::load (GltfLoader.cpp:79-365) plus the
+ *     CPU side of Scene::upload (Scene.cpp:255-345)
  *   - rr_camera_*: Camera::look_at / forward / rebuild_matrices
  *     (Camera.cpp:27-36, 120-145) and Scene::update_camera (Scene.cpp:554-585)
  */
 #ifndef RR_HOST_H
 #define RR_HOST_H
 
+#include <stddef.h>
 #include <stdint.h>
 #include "rr_cuda.h"
 
@@ -61,6 +63,17 @@ typedef struct rr_instanced_params {
     uint32_t _pad;
 } rr_instanced_params;
 rr_status rr_host_scene_instanced(const rr_instanced_params* p, rr_host_scene** out);
+
+/* Load a glTF 2.0 file (.gltf with embedded base64 or external buffers, or
+ * binary .glb) as GltfLoader::load does: every TRIANGLES primitive becomes a
+ * mesh, the default scene's node tree gives one instance per primitive
+ * (world = parent * local; node.matrix read as GltfLoader.cpp:36-42 reads
+ * it, else T * R * S), materials from the metallic-roughness factors with
+ * the glTF defaults, no lights. Textures are not decoded (the path never
+ * samples them; Scene::upload binds none). On failure returns
+ * RR_ERR_INVALID_ARGUMENT and writes the reason to err (if given); malformed
+ * or out-of-range data is an error, never read. */
+rr_status rr_host_scene_gltf(const char* path, rr_host_scene** out, char* err, size_t err_size);
 
 /* Pointers stay valid until rr_host_scene_destroy. */
 rr_status rr_host_scene_desc(const rr_host_scene* s, rr_scene_desc* out);

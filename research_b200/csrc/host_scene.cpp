@@ -9,22 +9,13 @@
 // Vulkan Y flip proj[1][1] *= -1); inverses are evaluated in closed form in
 // double precision and rounded to binary32.
 
-#include "rr_host.h"
+#include "rr_host_internal.h"
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
 #include <vector>
-
-struct rr_host_scene {
-    std::vector<GpuVertex> vertices;
-    std::vector<uint32_t> indices;
-    std::vector<GpuMesh> meshes;
-    std::vector<GpuMaterial> materials;
-    std::vector<GpuInstance> instances;
-    std::vector<GpuLight> lights;
-};
 
 namespace {
 

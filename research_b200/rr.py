@@ -8,6 +8,7 @@ is no fallback: a missing library raises immediately.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
@@ -237,6 +238,7 @@ _SIGNATURES = {
     "rr_host_scene_cornell": (I, [I, C.POINTER(P)]),
     "rr_host_scene_procedural": (I, [C.POINTER(ProceduralParams), C.POINTER(P)]),
     "rr_host_scene_instanced": (I, [C.POINTER(InstancedParams), C.POINTER(P)]),
+    "rr_host_scene_gltf": (I, [C.c_char_p, C.POINTER(P), C.c_char_p, C.c_size_t]),
     "rr_host_scene_desc": (I, [P, C.POINTER(SceneDesc)]),
     "rr_host_scene_destroy": (I, [P]),
     "rr_camera_default": (I, [U32, U32, C.POINTER(CameraDesc)]),
@@ -322,6 +324,16 @@ class HostScene:
         h = P()
         p = InstancedParams(seed, base_meshes, tris_per_mesh, instance_count, emissive_triangles, box_half, 0)
         _check(None, lib().rr_host_scene_instanced(C.byref(p), C.byref(h)))
+        return HostScene(h)
+
+    @staticmethod
+    def gltf(path) -> "HostScene":
+        """GltfLoader::load of a .gltf / .glb file (RRError with the reason on failure)."""
+        h = P()
+        err = C.create_string_buffer(1024)
+        st = lib().rr_host_scene_gltf(os.fsencode(str(path)), C.byref(h), err, len(err))
+        if st != 0:
+            raise RRError(st, err.value.decode(errors="replace"))
         return HostScene(h)
 
     def triangle_count(self) -> int:

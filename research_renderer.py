@@ -6,9 +6,11 @@ research_b200 instead of the Vulkan application.
     python research_renderer.py --frames 64 --screenshot out/cornell.png
     python research_renderer.py --pass restir_di --denoise --frames 8 --screenshot out/di.png
     python research_renderer.py procedural --frames 16 --screenshot out/room.png
+    python research_renderer.py scene.glb --pass restir_di --pass restir_pt --frames 8
 
-The optional scene argument is "cornell" (default) or "procedural" (the
-seeded 1M-triangle room); glTF loading is not part of this build. There is no
+The optional scene argument is "cornell" (default), "procedural" (the seeded
+1M-triangle room) or the path of a .gltf / .glb file (a file that fails to
+load falls back to the Cornell box, as the reference does). There is no
 window: --no-input is accepted for compatibility and --frames defaults to 1.
 """
 import argparse
@@ -18,10 +20,10 @@ import sys
 def _parse_args(argv):
     p = argparse.ArgumentParser(prog="research_renderer.py",
                                 description="Research Renderer light-transport passes on a B200 (headless).")
-    p.add_argument("scene", nargs="?", default="cornell", help="cornell | procedural")
+    p.add_argument("scene", nargs="?", default="cornell", help="cornell | procedural | path to .gltf/.glb")
     p.add_argument("--pass", dest="passes", action="append", default=[], metavar="NAME",
                    choices=["restir_di", "restir_gi", "restir_pt"],
-                   help="Enable a pass (repeatable). This build implements restir_di.")
+                   help="Enable a pass (repeatable).")
     p.add_argument("--denoise", action="store_true", help="Enable the A-trous denoiser.")
     p.add_argument("--exposure", type=float, default=None, metavar="X", help="Set tonemap exposure.")
     p.add_argument("--no-input", action="store_true", help="Accepted for compatibility (no window here).")
@@ -40,11 +42,11 @@ def main(argv=None):
     app.initialize(w, h)
     if args.scene == "procedural":
         app.load_procedural()
+    elif args.scene.lower().endswith((".gltf", ".glb")):
+        app.load_gltf(args.scene)
     elif args.scene != "cornell":
-        raise SystemExit(f"unsupported scene '{args.scene}' (cornell | procedural)")
+        raise SystemExit(f"unsupported scene '{args.scene}' (cornell | procedural | .gltf/.glb path)")
     for name in args.passes:
-        if name != "restir_di":
-            raise SystemExit(f"pass '{name}' is not part of this build")
         app.set_pass_enabled(name, True)
     if args.denoise:
         app.set_pass_enabled("denoise", True)

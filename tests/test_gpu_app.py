@@ -101,3 +101,73 @@ def test_research_renderer_cli_writes_png(tmp_path):
     raw = zlib.decompress(data[i + 4:i + 4 + n])
     px = np.frombuffer(raw, np.uint8).reshape(48, 1 + 64 * 4)[:, 1:].reshape(48, 64, 4)
     assert px[..., :3].mean() > 10
+
+
+def test_application_gi_and_pt_modes(rr, torch_cuda):
+    """restir_gi and restir_pt through the Application: PT wins over GI
+    (Application.cpp:417-421), each adds indirect light to DI's direct light,
+    and the displayed image follows current_display_image."""
+    from research_b200.passes import Application
+    torch = torch_cuda
+    app = Application()
+    app.initialize(64, 48)
+    app.set_pass_enabled("restir_di", True)
+    for _ in range(2):
+        app.step()
+    di = app.displayed_image().clone()
+    app.set_pass_enabled("restir_gi", True)
+    for _ in range(3):
+        app.step()
+    assert app.displayed_image() is app.restir_gi.output
+    gi = app.displayed_image().clone()
+    app.set_pass_enabled("restir_pt", True)
+    for _ in range(3):
+        app.step()
+    assert app.displayed_image() is app.restir_pt.output
+    pt = app.displayed_image().clone()
+    torch.cuda.synchronize()
+    assert torch.isfinite(gi).all() and torch.isfinite(pt).all()
+    assert gi[..., :3].mean() > di[..., :3].mean() and pt[..., :3].mean() > di[..., :3].mean()
+    # without DI the indirect passes still run on the G-buffer, with no direct term
+    app.set_pass_enabled("restir_di", False)
+    app.step()
+    assert app.displayed_image() is app.restir_pt.output
+    with pytest.raises(ValueError):
+        app.set_pass_enabled("unknown", True)
+    app.shutdown()
+
+
+def test_gltf_scene_renders_bit_exact(rr, O, ctx, torch_cuda, tmp_path):
+    """A generated .glb room loaded by rr_host_scene_gltf and path traced on the
+    GPU equals the oracle's render of the same arrays."""
+    import gltf_files
+    torch = torch_cuda
+    path = str(tmp_path / "room.glb")
+    gltf_files.room_scene().save(path, "glb")
+    hs = rr.HostScene.gltf(path)
+    scene = rr.Scene(ctx, hs.arrays)
+    osc = O.OracleScene(hs.arrays, use_bvh=False)
+    cam = rr.camera_data(rr.camera_desc(40, 32, eye=(0.0, 0.0, 2.9), center=(0.0, 0.0, 0.0)))
+    out = torch.zeros((2, 32, 40, 4), device="cuda")
+    p = rr.PtParams(3, 6, 2, 0)
+    ctx.check(rr.lib().rr_pathtracer_execute(ctx.handle, scene.handle, C.byref(cam), C.byref(p), out.data_ptr(),
+                                             _stream(torch)))
+    torch.cuda.synchronize()
+    o, _ = O.pathtrace(osc, cam, 3, 6, 2)
+    g = out.cpu().numpy()
+    np.testing.assert_array_equal(g.view(np.uint32), o.view(np.uint32))
+    assert g[..., :3].mean() > 0.01
+    scene.close()
+    hs.close()
+
+
+def test_research_renderer_cli_gltf_and_pt(tmp_path):
+    import gltf_files
+    scene = tmp_path / "room.gltf"
+    gltf_files.room_scene().save(str(scene))
+    out = tmp_path / "pt.png"
+    r = subprocess.run([sys.executable, str(ROOT / "research_renderer.py"), str(scene), "--frames", "3", "--size",
+                        "64x48", "--pass", "restir_di", "--pass", "restir_pt", "--screenshot", str(out)],
+                       capture_output=True, text=True, timeout=300, cwd=str(ROOT))
+    assert r.returncode == 0, r.stderr
+    assert "scene=room.gltf" in r.stdout and out.read_bytes()[:8] == b"\x89PNG\r\n\x1a\n"
