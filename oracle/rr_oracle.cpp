@@ -346,7 +346,10 @@ inline bool box_hit(const RayPre& r, const float lo[3], const float hi[3], float
         bf = std::min(bf, std::max(t0, t1));
     }
     bf = bf * 1.0000006f;
-    tn = std::max(tn, bn); tf = std::min(tf, bf);
+    // the closest-hit bound is widened too, so that a box holding a triangle
+    // at exactly the current t is still opened: ties then go to the lowest
+    // key whatever the visiting order
+    tn = std::max(tn, bn); tf = std::min(tf * 1.00001f, bf);
     return tn <= tf;
 }
 

@@ -40,8 +40,12 @@ struct DevScene {
     uint32_t num_nodes;
 };
 
+// A ray with its shear constants (triangle test) and its slab-test
+// constants: a box plane x is at t = fma(x, inv, alo) for a lower plane and
+// fma(x, inv, ahi) for an upper one (see make_ray).
 struct Ray {
     float3 o, d, inv;
+    float3 alo, ahi;
     float Sx, Sy, Sz;
     int kx, ky, kz;
 };
@@ -67,6 +71,22 @@ RR_D Ray make_ray(float3 o, float3 d) {
     const float sy = fabsf(d.y) < 1e-20f ? copysignf(1e-20f, d.y) : d.y;
     const float sz = fabsf(d.z) < 1e-20f ? copysignf(1e-20f, d.z) : d.z;
     r.inv = f3(1.0f / sx, 1.0f / sy, 1.0f / sz);
+    // Slab offsets: t(x) = (x - o) inv is evaluated as fma(x, inv, a) with
+    // a = -fl(o inv) -/+ m. The fma rounds once and fl(o inv) and a carry
+    // at most 3 u |o inv| between them (u = 2^-24), so m = 2^-22 |o inv|
+    // moves near planes nearer and far planes farther than every rounding
+    // error; which of a box's lower / upper planes is near follows the sign
+    // of inv. Culling therefore stays conservative, as with (x - o) * inv.
+    auto offsets = [](float o, float inv, float& alo, float& ahi) {
+        const float oi = o * inv;
+        const float m = fabsf(oi) * 2.384185791015625e-7f;
+        const float anear = -oi - m, afar = -oi + m;
+        alo = inv >= 0.0f ? anear : afar;
+        ahi = inv >= 0.0f ? afar : anear;
+    };
+    offsets(o.x, r.inv.x, r.alo.x, r.ahi.x);
+    offsets(o.y, r.inv.y, r.alo.y, r.ahi.y);
+    offsets(o.z, r.inv.z, r.alo.z, r.ahi.z);
     return r;
 }
 
@@ -93,28 +113,31 @@ RR_D bool intersect_triangle(const Ray& r, float3 p0, float3 p1, float3 p2, floa
     return true;
 }
 
-// Conservative slab test: the far distance is widened by a few ulps so that
-// rounding never culls a box that holds a hit (Ize, JCGT 2013).
+// Conservative slab test of both children of a node, one fma per plane
+// (offsets from make_ray). The far distance is also widened by a few ulps
+// for the product's rounding (Ize, JCGT 2013), and the closest-hit bound
+// too, so that a box holding a triangle at exactly the current t is opened
+// and ties go to the lowest key whatever the visiting order.
 RR_D void box_pair(const Ray& r, float4 a, float4 b, float4 c, float tmin, float tmax,
                    bool& h0, bool& h1, float& n0, float& n1) {
-    const float ox = r.o.x, oy = r.o.y, oz = r.o.z;
     const float ix = r.inv.x, iy = r.inv.y, iz = r.inv.z;
+    const float tlim = tmax * 1.00001f;
     {
-        const float tx0 = (a.x - ox) * ix, tx1 = (a.y - ox) * ix;
-        const float ty0 = (a.z - oy) * iy, ty1 = (a.w - oy) * iy;
-        const float tz0 = (c.x - oz) * iz, tz1 = (c.y - oz) * iz;
+        const float tx0 = __fmaf_rn(a.x, ix, r.alo.x), tx1 = __fmaf_rn(a.y, ix, r.ahi.x);
+        const float ty0 = __fmaf_rn(a.z, iy, r.alo.y), ty1 = __fmaf_rn(a.w, iy, r.ahi.y);
+        const float tz0 = __fmaf_rn(c.x, iz, r.alo.z), tz1 = __fmaf_rn(c.y, iz, r.ahi.z);
         const float nn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
-        const float ff = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)) , fmaxf(tz0, tz1)) * 1.000002f;
-        h0 = nn <= fminf(ff, tmax);
+        const float ff = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1)) * 1.000002f;
+        h0 = nn <= fminf(ff, tlim);
         n0 = nn;
     }
     {
-        const float tx0 = (b.x - ox) * ix, tx1 = (b.y - ox) * ix;
-        const float ty0 = (b.z - oy) * iy, ty1 = (b.w - oy) * iy;
-        const float tz0 = (c.z - oz) * iz, tz1 = (c.w - oz) * iz;
+        const float tx0 = __fmaf_rn(b.x, ix, r.alo.x), tx1 = __fmaf_rn(b.y, ix, r.ahi.x);
+        const float ty0 = __fmaf_rn(b.z, iy, r.alo.y), ty1 = __fmaf_rn(b.w, iy, r.ahi.y);
+        const float tz0 = __fmaf_rn(c.z, iz, r.alo.z), tz1 = __fmaf_rn(c.w, iz, r.ahi.z);
         const float nn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
         const float ff = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1)) * 1.000002f;
-        h1 = nn <= fminf(ff, tmax);
+        h1 = nn <= fminf(ff, tlim);
         n1 = nn;
     }
 }
