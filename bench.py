@@ -93,12 +93,13 @@ def load_peaks():
 
 
 def ncu_traffic(kernel: str):
-    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    """DRAM bytes of `kernel` over one frame (its launches summed, ncu with cold
+    caches) from the committed ncu summary, if any."""
     f = ROOT / "profiles" / f"{kernel}_traffic.txt"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
-        if line.startswith("dram_bytes_per_launch_full_frame:"):
+        if line.startswith(f"dram_bytes_per_frame_{kernel}:"):
             try:
                 return float(line.split(":", 1)[1].split()[0])
             except ValueError:
@@ -409,6 +410,7 @@ def run_ours(args, ws, rank, local):
     roofline = {"kernel": "extend_kernel (closest-hit BVH2 traversal, all bounces of one frame)", "bound": "hbm",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "traffic": traffic,
+                "traffic_scope": "DRAM bytes of the frame's extend launches (profiles/extend_traffic.txt)",
                 "algorithmic_bytes_per_step": ext_bytes, "launches_per_step": CFG["max_bounces"],
                 "shadow_achieved_gbs": shadow_bytes / (pt_stage["shadow"] * 1e-3) / 1e9 if pt_stage["shadow"] else 0}
     rays = counted["extension_rays"] + counted["shadow_rays"]
