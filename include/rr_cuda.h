@@ -520,6 +520,16 @@ rr_status rr_image_mse(rr_ctx* ctx, const float* a, const float* b, uint32_t wid
 rr_status rr_trace_closest(rr_ctx* ctx, const rr_scene* scene, const float* origins,
                            const float* dirs, float tmin, float tmax, uint32_t count,
                            float* hits, uint32_t* prims, void* stream);
+/* The same query with the traversal's work counters: any_hit selects the
+ * shadow-ray (first hit) form; work receives per ray (BVH nodes visited,
+ * triangles tested), the counts behind RR_PT_FLAG_COUNT_TRAVERSAL. */
+rr_status rr_trace_counted(rr_ctx* ctx, const rr_scene* scene, const float* origins,
+                           const float* dirs, float tmin, float tmax, uint32_t count, int any_hit,
+                           float* hits, uint32_t* prims, uint32_t* work, void* stream);
+/* Host copies of the scene's BVH (rr_scene_stats.bvh_node_count nodes of
+ * 16 floats, layout in rr_trace.cuh) and triangle records (triangle_count
+ * records of 12 floats). Synchronous. */
+rr_status rr_scene_copy_bvh(rr_ctx* ctx, const rr_scene* scene, float* nodes_out, float* tris_out);
 
 #ifdef __cplusplus
 }

@@ -82,6 +82,7 @@ _SIG = {
     "oracle_restir_pt_initial": (None, [P, P, C.POINTER(PtReuseParams), C.POINTER(PtReuseImages), I]),
     "oracle_restir_pt_temporal": (None, [P, P, C.POINTER(PtReuseParams), C.POINTER(PtReuseImages), I]),
     "oracle_restir_pt_spatial_shade": (None, [P, P, C.POINTER(PtReuseParams), C.POINTER(PtReuseImages), I]),
+    "oracle_bvh2_trace": (None, [P, U32, P, P, P, F32, F32, U32, I, P, P, P, I]),
     "oracle_restir_gi_initial": (None, [P, P, C.POINTER(GiReuseParams), C.POINTER(GiReuseImages), I]),
     "oracle_restir_gi_temporal": (None, [P, P, C.POINTER(GiReuseParams), C.POINTER(GiReuseImages), I]),
     "oracle_restir_gi_spatial_shade": (None, [P, P, C.POINTER(GiReuseParams), C.POINTER(GiReuseImages), I]),
@@ -252,6 +253,18 @@ def restir_pt_temporal(scene, cam, p, img, nthreads=None):
 def restir_pt_spatial_shade(scene, cam, p, img, nthreads=None):
     lib().oracle_restir_pt_spatial_shade(scene.handle, _cam_ptr(cam), C.byref(p), C.byref(pt_reuse_images(img)),
                                          nthreads or threads())
+
+
+def bvh2_trace(nodes, tris, origins, dirs, tmin, tmax, any_hit, nthreads=None):
+    """The library's BVH traversal restated on the CPU over its exported arrays:
+    returns (hits (n, 4) float32, prims (n,) uint32, work (n, 2) uint32)."""
+    n = len(origins)
+    hits = np.zeros((n, 4), np.float32)
+    prims = np.zeros(n, np.uint32)
+    work = np.zeros((n, 2), np.uint32)
+    lib().oracle_bvh2_trace(_p(nodes), len(nodes), _p(tris), _p(origins), _p(dirs), tmin, tmax, n, int(any_hit),
+                            _p(hits), _p(prims), _p(work), nthreads or threads())
+    return hits, prims, work
 
 
 def gi_reuse_params(frame_seed=0, candidates=8, temporal=1, spatial=1, neighbors=4, radius=12, include_direct=1,

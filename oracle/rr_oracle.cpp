@@ -1502,6 +1502,113 @@ void oracle_restir_pt_spatial_shade(const OracleScene* scene, const GpuCameraDat
     });
 }
 
+// ── traversal work on the library's own BVH ───────────────────────────────
+// Restatement of the GPU traversal (research_b200/csrc/rr_trace.cuh:
+// make_ray, box_pair, trace_step) over the node and triangle arrays copied
+// from a scene (rr_scene_copy_bvh), so that its hits and its node / triangle
+// counts — the algorithmic work behind the roofline bytes — can be checked
+// ray by ray. Node: (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y), (c1 same),
+// (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z), (child0, child1, count0, count1),
+// child < 0 a leaf starting at triangle ~child.
+void oracle_bvh2_trace(const float* nodes, uint32_t num_nodes, const float* tris, const float* origins,
+                       const float* dirs, float tmin, float tmax, uint32_t n, int any_hit, float* hits,
+                       uint32_t* prims, uint32_t* work, int threads) {
+    auto as_i = [](float f) { int32_t i; memcpy(&i, &f, 4); return i; };
+    auto as_u = [](float f) { uint32_t i; memcpy(&i, &f, 4); return i; };
+    parallel_rows(n, threads, [&](uint32_t i) {
+        const RayPre r = ray_pre(load3(origins + 4 * size_t(i)), load3(dirs + 4 * size_t(i)));
+        // slab offsets: t(x) = fma(x, inv, a), near planes nearer and far planes
+        // farther by m = 2^-22 |o inv|
+        float alo[3], ahi[3];
+        const float o3[3] = {r.o.x, r.o.y, r.o.z}, inv3[3] = {r.inv.x, r.inv.y, r.inv.z};
+        for (int a = 0; a < 3; ++a) {
+            const float oi = o3[a] * inv3[a];
+            const float m = fabsf(oi) * 2.384185791015625e-7f;
+            const float anear = -oi - m, afar = -oi + m;
+            alo[a] = inv3[a] >= 0.0f ? anear : afar;
+            ahi[a] = inv3[a] >= 0.0f ? afar : anear;
+        }
+        float best_t = tmax, bu = 0, bv = 0;
+        uint32_t best_key = 0xffffffffu, best_inst = 0, best_prim = 0, nn_count = 0, tri_count = 0;
+        bool found = false, done = false;
+        int node = 0, sp = 0, stack_node[64];
+        float stack_t[64];
+        uint32_t visits = 0;
+        while (!done) {
+            if (++visits > num_nodes + 1) break;
+            const float* N = nodes + 16 * size_t(node);
+            ++nn_count;
+            const float tlim = best_t * 1.00001f;
+            bool h[2]; float nr[2];
+            for (int k = 0; k < 2; ++k) {
+                const float* xy = N + 4 * k;                  // (lo.x, hi.x, lo.y, hi.y)
+                const float zlo = N[8 + 2 * k], zhi = N[9 + 2 * k];
+                const float tx0 = fmaf(xy[0], inv3[0], alo[0]), tx1 = fmaf(xy[1], inv3[0], ahi[0]);
+                const float ty0 = fmaf(xy[2], inv3[1], alo[1]), ty1 = fmaf(xy[3], inv3[1], ahi[1]);
+                const float tz0 = fmaf(zlo, inv3[2], alo[2]), tz1 = fmaf(zhi, inv3[2], ahi[2]);
+                const float nn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+                const float ff = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1)) * 1.000002f;
+                h[k] = nn <= fminf(ff, tlim);
+                nr[k] = nn;
+            }
+            const int c[2] = {as_i(N[12]), as_i(N[13])}, cnt[2] = {as_i(N[14]), as_i(N[15])};
+            for (int k = 0; k < 2 && !done; ++k) {
+                if (!(h[k] && c[k] < 0)) continue;
+                const int first = ~c[k];
+                for (int t = first; t < first + cnt[k]; ++t) {
+                    ++tri_count;
+                    const float* T = tris + 12 * size_t(t);
+                    float tt, uu, vv;
+                    if (intersect_tri(r, v3(T[0], T[1], T[2]), v3(T[3], T[4], T[5]), v3(T[6], T[7], T[8]), tmin,
+                                      best_t, tt, uu, vv)) {
+                        const uint32_t key = as_u(T[11]);
+                        if (any_hit) { best_t = tt; found = true; done = true; break; }
+                        if (!found || tt < best_t || (tt == best_t && key < best_key)) {
+                            found = true; best_t = tt; bu = uu; bv = vv; best_key = key;
+                            best_inst = as_u(T[9]); best_prim = as_u(T[10]);
+                        }
+                    }
+                }
+            }
+            if (done) break;
+            const bool i0 = h[0] && c[0] >= 0 && nr[0] <= best_t;
+            const bool i1 = h[1] && c[1] >= 0 && nr[1] <= best_t;
+            if (i0 && i1) {
+                const bool first0 = nr[0] <= nr[1];
+                stack_node[sp] = first0 ? c[1] : c[0];
+                stack_t[sp] = first0 ? nr[1] : nr[0];
+                ++sp;
+                node = first0 ? c[0] : c[1];
+            } else if (i0) {
+                node = c[0];
+            } else if (i1) {
+                node = c[1];
+            } else {
+                bool next = false;
+                while (sp > 0) {
+                    --sp;
+                    if (stack_t[sp] <= best_t) { node = stack_node[sp]; next = true; break; }
+                }
+                if (!next) done = true;
+            }
+        }
+        float* H = hits + 4 * size_t(i);
+        if (found) {
+            H[0] = best_t; H[1] = any_hit ? 0.0f : bu; H[2] = any_hit ? 0.0f : bv;
+            const uint32_t inst = any_hit ? 0u : best_inst;
+            memcpy(&H[3], &inst, 4);
+            prims[i] = any_hit ? 0u : best_prim;
+        } else {
+            H[0] = -1.0f; H[1] = H[2] = 0.0f;
+            const uint32_t none = 0xffffffffu;
+            memcpy(&H[3], &none, 4);
+            prims[i] = none;
+        }
+        work[2 * size_t(i)] = nn_count;
+        work[2 * size_t(i) + 1] = tri_count;
+    });
+}
+
 // ── ReSTIR GI (restir_gi.slang:568-1000; ReSTIRGIPass.cpp:428-650) ────────────
 void oracle_restir_gi_initial(const OracleScene* scene, const GpuCameraData* cam, const OracleRestirGiParams* p,
                               const OracleRestirGiImages* img, int threads) {

@@ -177,6 +177,12 @@ void oracle_restir_pt_spatial_shade(const OracleScene* scene, const GpuCameraDat
                                     const OracleRestirPtParams* p, const OracleRestirPtImages* img,
                                     int threads);
 
+/* The library's BVH2 traversal restated over its node / triangle arrays
+ * (rr_scene_copy_bvh): hits as rr_trace_counted, work = (nodes, tris) per ray. */
+void oracle_bvh2_trace(const float* nodes, uint32_t num_nodes, const float* tris, const float* origins,
+                       const float* dirs, float tmin, float tmax, uint32_t n, int any_hit, float* hits,
+                       uint32_t* prims, uint32_t* work, int threads);
+
 /* ── ReSTIR GI (restir_gi.slang:568-1000) ───────────────────────────────── */
 typedef struct OracleRestirGiParams {
     uint32_t frame_seed;

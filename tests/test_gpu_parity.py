@@ -71,6 +71,43 @@ def test_trace_closest_matches_oracle(rr, O, ctx, torch_cuda, cornell, procedura
         np.testing.assert_array_equal(pg, po)
 
 
+def test_traversal_work_matches_cpu_restatement(rr, O, ctx, torch_cuda, cornell, procedural):
+    """The traversal's node / triangle counters (the algorithmic work behind the
+    roofline bytes) equal a CPU restatement walking the library's own BVH in the
+    same front-to-back order, ray by ray, for closest-hit and any-hit rays;
+    the hits agree bit for bit too."""
+    torch = torch_cuda
+    rng = np.random.default_rng(23)
+    L = rr.lib()
+    for arrays, scene, _, span in (cornell + (1.0,), procedural + (25.0,)):
+        stats = rr.SceneStats()
+        ctx.check(L.rr_scene_get_stats(scene.handle, C.byref(stats)))
+        nodes = np.zeros((stats.bvh_node_count, 16), np.float32)
+        tris = np.zeros((max(stats.triangle_count, 1), 12), np.float32)
+        ctx.check(L.rr_scene_copy_bvh(ctx.handle, scene.handle, nodes.ctypes.data, tris.ctypes.data))
+        n = 8192
+        o = np.zeros((n, 4), np.float32)
+        o[:, :3] = rng.uniform(-span, span, (n, 3))
+        d = np.zeros((n, 4), np.float32)
+        v = rng.normal(size=(n, 3))
+        d[:, :3] = v / np.linalg.norm(v, axis=1, keepdims=True)
+        d[:64, :3] = [1.0, 0.0, 0.0]        # axis-parallel rays: zero direction components
+        for any_hit, tmax in ((0, 1e9), (1, 0.7 * span)):
+            to, td = torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda()
+            hits = torch.empty((n, 4), device="cuda")
+            prims = torch.empty(n, device="cuda", dtype=torch.int32)
+            work = torch.empty((n, 2), device="cuda", dtype=torch.int32)
+            ctx.check(L.rr_trace_counted(ctx.handle, scene.handle, to.data_ptr(), td.data_ptr(), 0.001, tmax, n,
+                                         any_hit, hits.data_ptr(), prims.data_ptr(), work.data_ptr(),
+                                         _stream(torch)))
+            torch.cuda.synchronize()
+            oh, op, ow = O.bvh2_trace(nodes, tris, o, d, 0.001, tmax, any_hit)
+            np.testing.assert_array_equal(_np(hits).view(np.uint32), oh.view(np.uint32))
+            np.testing.assert_array_equal(_np(prims).view(np.uint32), op)
+            np.testing.assert_array_equal(_np(work).view(np.uint32), ow)
+            assert ow[:, 0].mean() > 2 and (oh[:, 3].view(np.uint32) != 0xFFFFFFFF).mean() > 0.1
+
+
 @pytest.mark.parametrize("seed", [0, 7])
 def test_pathtracer_cornell_bit_exact(rr, O, ctx, torch_cuda, cornell, seed):
     _, scene, oscene = cornell
