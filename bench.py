@@ -55,33 +55,18 @@ def parse():
 
 
 def dist_init(args):
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        import torch
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-    return ws, rank, local
+    from research_b200 import replicas
+    return replicas.init("nccl")
 
 
 def barrier(ws):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from research_b200 import replicas
+    replicas.barrier(ws)
 
 
 def max_over_ranks(ws, x: float) -> float:
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], device="cuda", dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from research_b200 import replicas
+    return replicas.max_over_ranks(ws, x, "cuda")
 
 
 def load_peaks():
@@ -322,7 +307,9 @@ def run_ours(args, ws, rank, local):
     W, H = args.width, args.height
     stream = torch.cuda.current_stream().cuda_stream
     fr = Frame(rr, torch, ctx, scene, W, H)
-    seed_base = rank * 1_000_003
+    from research_b200 import replicas
+    seed_base = replicas.seed_base(rank)
+    replicas.check_seed_budget((args.warmup + 3 * args.steps + 8) * CFG["spp"])
 
     st = rr.PtStats()
     # autotune the traversal variants on this scene and frame (setup, untimed)
@@ -361,7 +348,7 @@ def run_ours(args, ws, rank, local):
     pt_stage = {"raygen": st.ms_raygen / args.steps, "extend": st.ms_extend / args.steps,
                 "shade": st.ms_shade / args.steps, "shadow": st.ms_shadow / args.steps}
     paths_per_step = W * H * CFG["spp"]
-    value = paths_per_step * ws / (ms_step * 1e-3) / 1e6
+    value = replicas.job_throughput(paths_per_step, ws, ms_step)
 
     # 3) algorithmic work of the timed frames: replay the same K frame seeds
     #    with traversal counters on (untimed; the kernels are deterministic)
@@ -396,7 +383,7 @@ def run_ours(args, ws, rank, local):
     f1.record()
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(ws, f0.elapsed_time(f1) / args.steps)
-    e2e_value = paths_per_step * ws / (e2e_ms * 1e-3) / 1e6
+    e2e_value = replicas.job_throughput(paths_per_step, ws, e2e_ms)
 
     # roofline of the dominant kernel (BVH traversal of extension rays)
     peak, peak_kind = load_peaks()
@@ -454,9 +441,8 @@ def main():
         if not (ROOT / "research_b200" / "lib" / "librr_cuda.so").exists():
             build.build_cuda()
         run_ours(args, ws, rank, local)
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    from research_b200 import replicas
+    replicas.finish(ws)
 
 
 if __name__ == "__main__":
