@@ -130,9 +130,11 @@ rr_status rr_pathtracer_stats(rr_ctx* ctx, rr_pt_stats* out, int reset_times);
 
 /* Traversal kernel variants (no reference counterpart; the reference uses
  * hardware ray queries): variant = schedule x occupancy target,
- *   0..2: warps trace 32 consecutive queue entries to completion, register
- *         budget for 4 (default) / 5 / 6 blocks of 256 threads per SM;
- *   3..5: persistent warps with per-lane ray refill, same budgets.
+ *   0..2: warps trace 32 consecutive queue entries to completion, with the
+ *         compiler's register count (default) / a budget for 5 / 6 blocks of
+ *         256 threads per SM;
+ *   3..5: persistent warps with per-lane ray refill, with the compiler's
+ *         register count / a budget for 4 / 6 blocks.
  * Results are identical for every variant; only speed differs. */
 #define RR_PT_VARIANT_COUNT 6
 rr_status rr_pathtracer_set_variants(rr_ctx* ctx, int extend_variant, int shadow_variant);

@@ -349,7 +349,7 @@ BatchQueueKernel extend_batch_variant(int v) {
     case 1: return extend_batch_kernel<Count, false, 5>;
     case 2: return extend_batch_kernel<Count, false, 6>;
     case 3: return extend_batch_kernel<Count, true, 1>;
-    case 4: return extend_batch_kernel<Count, true, 5>;
+    case 4: return extend_batch_kernel<Count, true, 4>;
     case 5: return extend_batch_kernel<Count, true, 6>;
     default: return extend_batch_kernel<Count, false, 1>;
     }
@@ -360,7 +360,7 @@ BatchShadowKernel shadow_batch_variant(int v) {
     case 1: return shadow_batch_kernel<Count, false, 5>;
     case 2: return shadow_batch_kernel<Count, false, 6>;
     case 3: return shadow_batch_kernel<Count, true, 1>;
-    case 4: return shadow_batch_kernel<Count, true, 5>;
+    case 4: return shadow_batch_kernel<Count, true, 4>;
     case 5: return shadow_batch_kernel<Count, true, 6>;
     default: return shadow_batch_kernel<Count, false, 1>;
     }
@@ -377,7 +377,7 @@ QueueKernel extend_variant(int v) {
     case 1: return extend_kernel<Count, false, 5>;
     case 2: return extend_kernel<Count, false, 6>;
     case 3: return extend_kernel<Count, true, 1>;
-    case 4: return extend_kernel<Count, true, 5>;
+    case 4: return extend_kernel<Count, true, 4>;
     case 5: return extend_kernel<Count, true, 6>;
     default: return extend_kernel<Count, false, 1>;
     }
@@ -388,7 +388,7 @@ ShadowKernel shadow_variant(int v) {
     case 1: return shadow_kernel<Count, false, 5>;
     case 2: return shadow_kernel<Count, false, 6>;
     case 3: return shadow_kernel<Count, true, 1>;
-    case 4: return shadow_kernel<Count, true, 5>;
+    case 4: return shadow_kernel<Count, true, 4>;
     case 5: return shadow_kernel<Count, true, 6>;
     default: return shadow_kernel<Count, false, 1>;
     }
