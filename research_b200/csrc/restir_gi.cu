@@ -90,7 +90,7 @@ RR_D float gi_source_pdf(float3 pp, float3 pn, float3 spos) {
 }
 
 // cs_initial (restir_gi.slang:568-686)
-__global__ void __launch_bounds__(128) gi_initial_kernel(DevScene s, GiLaunch L, GiImages I) {
+__global__ void __launch_bounds__(128, 8) gi_initial_kernel(DevScene s, GiLaunch L, GiImages I) {
     uint32_t x, y;
     if (!pixel_of(L.cam, x, y)) return;
     const size_t i = size_t(y) * L.cam.screen_width + x;
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(128) gi_initial_kernel(DevScene s, GiLaunch L,
 }
 
 // cs_temporal (restir_gi.slang:688-848)
-__global__ void __launch_bounds__(128) gi_temporal_kernel(DevScene s, GiLaunch L, GiImages I) {
+__global__ void __launch_bounds__(128, 8) gi_temporal_kernel(DevScene s, GiLaunch L, GiImages I) {
     uint32_t x, y;
     if (!pixel_of(L.cam, x, y)) return;
     const size_t i = size_t(y) * L.cam.screen_width + x;
@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(128) gi_temporal_kernel(DevScene s, GiLaunch L
 }
 
 // cs_spatial_shade (restir_gi.slang:851-1000)
-__global__ void __launch_bounds__(128) gi_spatial_shade_kernel(DevScene s, GiLaunch L, GiImages I) {
+__global__ void __launch_bounds__(128, 8) gi_spatial_shade_kernel(DevScene s, GiLaunch L, GiImages I) {
     uint32_t x, y;
     if (!pixel_of(L.cam, x, y)) return;
     const uint32_t W = L.cam.screen_width, H = L.cam.screen_height;

@@ -90,7 +90,7 @@ RR_D float target_function(float3 pp, float3 pn, const Mat& pm, float3 cam_pos, 
 }
 
 // cs_initial (restir_pt.slang:567-757)
-__global__ void __launch_bounds__(128) ptr_initial_kernel(DevScene s, PtrLaunch L, PtrImages I) {
+__global__ void __launch_bounds__(128, 8) ptr_initial_kernel(DevScene s, PtrLaunch L, PtrImages I) {
     uint32_t x, y;
     if (!pixel_of(L.cam, x, y)) return;
     const size_t i = size_t(y) * L.cam.screen_width + x;
@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(128) ptr_initial_kernel(DevScene s, PtrLaunch 
 }
 
 // cs_temporal (restir_pt.slang:760-857)
-__global__ void __launch_bounds__(128) ptr_temporal_kernel(DevScene s, PtrLaunch L, PtrImages I) {
+__global__ void __launch_bounds__(128, 8) ptr_temporal_kernel(DevScene s, PtrLaunch L, PtrImages I) {
     uint32_t x, y;
     if (!pixel_of(L.cam, x, y)) return;
     const uint32_t W = L.cam.screen_width, H = L.cam.screen_height;
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(128) ptr_temporal_kernel(DevScene s, PtrLaunch
 }
 
 // cs_spatial_shade (restir_pt.slang:860-1000)
-__global__ void __launch_bounds__(128) ptr_spatial_shade_kernel(DevScene s, PtrLaunch L, PtrImages I) {
+__global__ void __launch_bounds__(128, 8) ptr_spatial_shade_kernel(DevScene s, PtrLaunch L, PtrImages I) {
     uint32_t x, y;
     if (!pixel_of(L.cam, x, y)) return;
     const uint32_t W = L.cam.screen_width, H = L.cam.screen_height;
