@@ -126,7 +126,7 @@ RR_D void shade_ray(const DevScene& s, float4* __restrict__ out, uint32_t bounce
 // Multi: a batch of scenes; a ray's scene index is in c.w, its scene is
 // table[index] and its image outs[index]; the index is carried on.
 template <bool Multi>
-__global__ void __launch_bounds__(kBlock) shade_kernel(DevScene s, const DevScene* __restrict__ table,
+__global__ void __launch_bounds__(kBlock, 4) shade_kernel(DevScene s, const DevScene* __restrict__ table,
                                                        float4* const* __restrict__ outs, uint32_t bounce,
                                                        uint32_t last, const float4* __restrict__ qa,
                                                        const float4* __restrict__ qb,

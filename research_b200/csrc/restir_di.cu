@@ -46,7 +46,7 @@ RR_D bool pixel_of(const GpuCameraData& cam, uint32_t& x, uint32_t& y) {
 }
 
 // cs_initial (restir_di.slang:186-262)
-__global__ void __launch_bounds__(128) di_initial_kernel(DevScene s, DiLaunch L, float4* __restrict__ gpos,
+__global__ void __launch_bounds__(128, 8) di_initial_kernel(DevScene s, DiLaunch L, float4* __restrict__ gpos,
                                                          float4* __restrict__ gnrm, float4* __restrict__ res) {
     uint32_t x, y;
     if (!pixel_of(L.cam, x, y)) return;
@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(128) di_temporal_kernel(DevScene s, DiLaunch L
 }
 
 // cs_spatial_shade (restir_di.slang:339-472)
-__global__ void __launch_bounds__(128) di_spatial_shade_kernel(DevScene s, DiLaunch L, const float4* __restrict__ gpos,
+__global__ void __launch_bounds__(128, 8) di_spatial_shade_kernel(DevScene s, DiLaunch L, const float4* __restrict__ gpos,
                                                                const float4* __restrict__ gnrm,
                                                                const float4* __restrict__ res,
                                                                float4* __restrict__ out) {
