@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(kBlock) guided_surface_kernel(DevScene s, cons
 
 // Shade stage of the guided tracer (cf. shade_kernel in pathtracer.cu).
 template <bool SlotMixture>
-__global__ void __launch_bounds__(kBlock) guided_shade_kernel(DevScene s, GuidedLaunch G,
+__global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s, GuidedLaunch G,
                                                               const float4* __restrict__ qa,
                                                               const float4* __restrict__ qb,
                                                               const float4* __restrict__ qc,
