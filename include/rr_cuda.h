@@ -532,6 +532,12 @@ rr_status rr_trace_counted(rr_ctx* ctx, const rr_scene* scene, const float* orig
  * 16 floats, layout in rr_trace.cuh) and triangle records (triangle_count
  * records of 12 floats). Synchronous. */
 rr_status rr_scene_copy_bvh(rr_ctx* ctx, const rr_scene* scene, float* nodes_out, float* tris_out);
+/* Bounded-wait self-test of the tensor-core kernels' mbarrier waits: one
+ * block waits (at most `limit` tries, 1..2^22) on a barrier that nothing
+ * arrives on and on one that received its arrival. completed_out[0] = 1 if
+ * the first wait completed (0: it gave up, as it must), completed_out[1] =
+ * 1 if the second completed. The kernel returns normally either way. */
+rr_status rr_tc_wait_selftest(rr_ctx* ctx, uint32_t limit, int* completed_out);
 
 #ifdef __cplusplus
 }

@@ -935,6 +935,46 @@ rr_status rr_mlp_guide_train(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t 
     return RR_OK;
 }
 
+namespace rr {
+namespace {
+// Self-test of the bounded mbarrier wait used by the tensor-core kernels:
+// a barrier that receives its one arrival completes; a barrier that nothing
+// arrives on makes the wait give up after `limit` tries, and the kernel
+// returns normally with the outcome recorded.
+__global__ void tc_wait_selftest_kernel(uint32_t limit, int* out) {
+    __shared__ __align__(8) uint64_t bars[2];
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&bars[0], 1);
+        tc::mbar_init(&bars[1], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(
+                         tc::smem_addr(&bars[1]))
+                     : "memory");
+        out[1] = tc::mbar_wait(&bars[1], 0, limit) ? 1 : 0;
+        out[0] = tc::mbar_wait(&bars[0], 0, limit) ? 1 : 0;
+    }
+}
+} // namespace
+} // namespace rr
+
+extern "C" rr_status rr_tc_wait_selftest(rr_ctx* ctx, uint32_t limit, int* completed_out) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    if (!completed_out || limit == 0 || limit > (1u << 22))
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_tc_wait_selftest: bad argument");
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    int* d = nullptr;
+    RR_TRY_CUDA(ctx, cudaMalloc(&d, 2 * sizeof(int)));
+    rr::tc_wait_selftest_kernel<<<1, 32>>>(limit, d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(completed_out, d, 2 * sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return rr_fail(ctx, RR_ERR_CUDA, "rr_tc_wait_selftest: %s", cudaGetErrorString(e));
+    ctx->launches += 1;
+    return RR_OK;
+}
+
 double rr_mlp_guide_last_loss(rr_guide* g) {
     rr_mlp_state& M = *g->mlp;
     double s = 0.0;

@@ -240,6 +240,7 @@ _SIGNATURES = {
     "rr_host_scene_instanced": (I, [C.POINTER(InstancedParams), C.POINTER(P)]),
     "rr_trace_counted": (I, [P, P, P, P, C.c_float, C.c_float, U32, I, P, P, P, P]),
     "rr_scene_copy_bvh": (I, [P, P, P, P]),
+    "rr_tc_wait_selftest": (I, [P, U32, P]),
     "rr_host_scene_gltf": (I, [C.c_char_p, C.POINTER(P), C.c_char_p, C.c_size_t]),
     "rr_host_scene_desc": (I, [P, C.POINTER(SceneDesc)]),
     "rr_host_scene_destroy": (I, [P]),

@@ -315,3 +315,19 @@ def test_guided_pathtracer_is_unbiased(rr, ctx, torch_cuda, kind):
     assert abs(mg - mp) / mp < 0.03, (mg, mp)
     rr.lib().rr_guide_destroy(g)
     scene.close()
+
+
+def test_bounded_mbarrier_wait_gives_up_and_reports(rr, ctx, torch_cuda):
+    """A tensor-core wait on a barrier that nothing completes returns after its
+    bound with the outcome recorded (no hang, no trap); the context stays usable."""
+    import ctypes as C
+    torch = torch_cuda
+    out = (C.c_int * 2)(7, 7)
+    ctx.check(rr.lib().rr_tc_wait_selftest(ctx.handle, 2000, out))
+    assert list(out) == [0, 1]
+    # the device still runs work afterwards
+    a = torch.ones(1024, device="cuda")
+    assert float((a * 2).sum()) == 2048.0
+    with pytest.raises(rr.RRError):
+        ctx.check(rr.lib().rr_tc_wait_selftest(ctx.handle, 0, out))
+
