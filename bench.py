@@ -422,6 +422,9 @@ def run_ours(args, ws, rank, local):
                               "pt_extend": round(pt_stage["extend"], 4), "pt_shade": round(pt_stage["shade"], 4),
                               "pt_shadow": round(pt_stage["shadow"], 4)},
                 "rays_per_step": rays, "mrays_per_s": rays / (ms_step * 1e-3) / 1e6,
+                "stage_mrays_per_s": {
+                    "extend": counted["extension_rays"] / (pt_stage["extend"] * 1e-3) / 1e6 if pt_stage["extend"] else 0,
+                    "shadow": counted["shadow_rays"] / (pt_stage["shadow"] * 1e-3) / 1e6 if pt_stage["shadow"] else 0},
                 "scene": {"triangles": sst.triangle_count, "bvh_nodes": sst.bvh_node_count,
                           "bvh_depth": sst.bvh_max_depth, "bvh_build_ms": round(sst.build_ms, 1),
                           "lights": sst.light_count},
