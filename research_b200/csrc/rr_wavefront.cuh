@@ -75,7 +75,7 @@ __device__ __forceinline__ void flush_work(const TraceWork& w, unsigned long lon
 // Warp-cooperative ray pool: hands queue indices [0, count) to idle lanes,
 // taking kChunk indices at a time from the launch's global cursor (one
 // atomic per chunk). All fields are warp-uniform.
-constexpr uint32_t kChunk = 256;
+constexpr uint32_t kChunk = 64;
 constexpr uint32_t kRefillLanes = 8;
 
 struct WarpPool {
