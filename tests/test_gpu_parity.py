@@ -356,3 +356,47 @@ def test_traversal_variants_identical_and_tuner(rr, O, ctx, torch_cuda, procedur
     np.testing.assert_array_equal(g.view(np.uint32), ref.view(np.uint32))
     assert rr.lib().rr_pathtracer_set_variants(ctx.handle, 6, 0) == 1
     ctx.check(rr.lib().rr_pathtracer_set_variants(ctx.handle, 0, 0))
+
+
+def _edge_scenes(rr):
+    """Cornell variants: a directional plus a point light (the MIS branch of
+    the light sample and of ReSTIR DI's target), no lights at all, and all
+    geometry moved out of view (every ray misses)."""
+    base = rr.HostScene.cornell(0).arrays
+    two = np.zeros(2, rr.LIGHT)
+    two[0]["position"] = (0.0, 0.0, 0.0)
+    two[0]["type"] = 1
+    two[0]["direction"] = (0.3, -1.0, -0.2)
+    two[0]["emission"] = (1.0, 0.9, 0.8)
+    two[0]["intensity"] = 2.5
+    two[1] = base["lights"][0]
+    out = {"directional": dict(base, lights=two),
+           "no_lights": dict(base, lights=np.zeros(0, rr.LIGHT))}
+    away = base["instances"].copy()
+    away["transform"][:, 3] += 1000.0      # every instance far off to the side: no ray hits
+    out["no_geometry"] = dict(base, instances=away)
+    return out
+
+
+@pytest.mark.parametrize("name", ["directional", "no_lights", "no_geometry"])
+def test_edge_scenes_bit_exact(rr, O, ctx, torch_cuda, name):
+    torch = torch_cuda
+    arrays = _edge_scenes(rr)[name]
+    scene = rr.Scene(ctx, arrays)
+    osc = O.OracleScene(arrays, use_bvh=False)
+    cam = cam_for(rr, "cornell", 40, 32)
+    g = gpu_pathtrace(rr, ctx, scene, cam, torch, 4, 6, 2)
+    o, _ = O.pathtrace(osc, cam, 4, 6, 2)
+    np.testing.assert_array_equal(g.view(np.uint32), o.view(np.uint32))
+    plist_g = [rr.DIParams(f, 8, 1, 1, 4, 10, 20, 0) for f in range(2)]
+    plist_o = [O.di_params(f, 8, 1, 1, 4, 10, 20) for f in range(2)]
+    for a, b in zip(_di_run_gpu(rr, ctx, torch, scene, cam, plist_g)[-1], _di_run_oracle(O, osc, cam, plist_o)[-1]):
+        np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+    if name == "no_geometry":
+        assert np.isfinite(g).all() and g[..., :3].min() > 0.05      # sky everywhere
+        # a scene without instances is refused, as Scene::upload throws (Scene.cpp:261-262)
+        with pytest.raises(rr.RRError):
+            rr.Scene(ctx, dict(arrays, instances=np.zeros(0, arrays["instances"].dtype)))
+    else:
+        assert g[..., :3].mean() > 0.01
+    scene.close()

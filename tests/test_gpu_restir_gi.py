@@ -186,3 +186,11 @@ def test_restir_gi_rejects_null_images(rr, ctx, torch_cuda):
         ctx.check(rr.lib().rr_restir_gi_initial(ctx.handle, scene.handle, C.byref(cam), C.byref(p), C.byref(imgs),
                                                 _stream(torch)))
     scene.close()
+
+
+@pytest.mark.parametrize("name", ["directional", "no_lights"])
+def test_restir_gi_light_edge_cases_bit_exact(rr, O, ctx, torch_cuda, name):
+    """The light sample's directional (MIS) branch and a scene without lights."""
+    import test_gpu_parity
+    arrays = test_gpu_parity._edge_scenes(rr)[name]
+    _run(rr, O, ctx, torch_cuda, arrays, 32, 24, 2, (0.0, 0.0, 3.0), (0.0, 0.0, 0.0), (0.003, 0.0, -0.01))

@@ -148,3 +148,11 @@ def test_restir_pt_reset_history(rr, ctx, torch_cuda):
     for k in range(4):
         assert (bufs[k] == 0).all()
     assert (bufs[4][..., :3] == 0).all() and (bufs[4][..., 3] == -1).all() and (bufs[5] == 0).all()
+
+
+@pytest.mark.parametrize("name", ["directional", "no_lights"])
+def test_restir_pt_light_edge_cases_bit_exact(rr, O, ctx, torch_cuda, name):
+    """The light sample's directional (MIS) branch and a scene without lights."""
+    import test_gpu_parity
+    arrays = test_gpu_parity._edge_scenes(rr)[name]
+    _run(rr, O, ctx, torch_cuda, arrays, 32, 24, 2, (0.0, 0.0, 3.0), (0.0, 0.0, 0.0), (0.003, 0.0, -0.01))
