@@ -11,9 +11,21 @@ namespace {
 RR_D float luminance601(float3 c) { return dot(c, f3(0.299f, 0.587f, 0.114f)); }
 RR_D float kernel_weight(int o) { return (o == 2 || o == -2) ? 1.0f : ((o == 1 || o == -1) ? 4.0f : 6.0f); }
 
+// The G-buffer normals normalized once per call (the filter reads each
+// pixel's normal for up to 25 taps per iteration; normalize is deterministic,
+// so the taps see the same values as normalizing on the spot).
+__global__ void __launch_bounds__(256) normalize_kernel(const float4* __restrict__ gnrm, float4* __restrict__ out,
+                                                        size_t n) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float3 v = normalize(xyz(gnrm[i]));
+    out[i] = make_float4(v.x, v.y, v.z, 0.0f);
+}
+
+// `nrm`: unit normals (from normalize_kernel)
 __global__ void __launch_bounds__(128) atrous_kernel(const float4* __restrict__ in,
                                                      const float4* __restrict__ gpos,
-                                                     const float4* __restrict__ gnrm,
+                                                     const float4* __restrict__ nrm,
                                                      float4* __restrict__ out, int W, int H, int stride,
                                                      float sp2, float sn2, float sl2) {
     const int x = blockIdx.x * 16 + (threadIdx.x & 15);
@@ -23,7 +35,7 @@ __global__ void __launch_bounds__(128) atrous_kernel(const float4* __restrict__ 
     const float4 cpos = gpos[ci];
     const float4 crad = in[ci];
     if (cpos.w < 0.0f) { out[ci] = crad; return; }
-    const float3 cn = normalize(xyz(gnrm[ci]));
+    const float3 cn = xyz(nrm[ci]);
     const float cl = luminance601(xyz(crad));
     float3 filtered = f3(0.0f, 0.0f, 0.0f);
     float wsum = 0.0f;
@@ -39,7 +51,7 @@ __global__ void __launch_bounds__(128) atrous_kernel(const float4* __restrict__ 
             const float base_w = (kernel_weight(tx) * kernel_weight(ty)) / 256.0f;
             const float3 pd = xyz(spos) - xyz(cpos);
             const float pos_w = rr_expf(-dot(pd, pd) / sp2);
-            const float3 sn = normalize(xyz(__ldg(gnrm + si)));
+            const float3 sn = xyz(__ldg(nrm + si));
             const float nd = mx(0.0f, 1.0f - dot(cn, sn));
             const float normal_w = rr_expf(-nd / sn2);
             const float3 srad = xyz(__ldg(in + si));
@@ -57,15 +69,33 @@ __global__ void __launch_bounds__(128) atrous_kernel(const float4* __restrict__ 
 } // namespace
 } // namespace rr
 
-static rr_status atrous_launch(rr_ctx* ctx, const float* input, const float* gpos, const float* gnrm,
+// Unit normals of `gnrm` into the context's scratch image.
+static rr_status atrous_normals(rr_ctx* ctx, const float* gnrm, uint32_t W, uint32_t H, cudaStream_t stream,
+                                const float4** out) {
+    const size_t n = size_t(W) * H;
+    if (ctx->atrous_nrm_px < n) {
+        cudaFree(ctx->atrous_nrm);
+        ctx->atrous_nrm = nullptr;
+        ctx->atrous_nrm_px = 0;
+        RR_TRY_CUDA(ctx, cudaMalloc(&ctx->atrous_nrm, n * sizeof(float4)));
+        ctx->atrous_nrm_px = n;
+    }
+    rr::normalize_kernel<<<unsigned((n + 255) / 256), 256, 0, stream>>>(reinterpret_cast<const float4*>(gnrm),
+                                                                        ctx->atrous_nrm, n);
+    RR_CHECK_LAUNCH(ctx);
+    ctx->launches += 1;
+    *out = ctx->atrous_nrm;
+    return RR_OK;
+}
+
+static rr_status atrous_launch(rr_ctx* ctx, const float* input, const float* gpos, const float4* nrm,
                                float* output, uint32_t W, uint32_t H, uint32_t stride, float sp, float sn,
                                float sl, cudaStream_t stream) {
     const float sp2 = std::max(sp * sp, 1.0e-6f), sn2 = std::max(sn * sn, 1.0e-6f), sl2 = std::max(sl * sl, 1.0e-6f);
     dim3 grid((W + 15) / 16, (H + 7) / 8);
     rr::atrous_kernel<<<grid, 128, 0, stream>>>(
-        reinterpret_cast<const float4*>(input), reinterpret_cast<const float4*>(gpos),
-        reinterpret_cast<const float4*>(gnrm), reinterpret_cast<float4*>(output), int(W), int(H),
-        int(stride), sp2, sn2, sl2);
+        reinterpret_cast<const float4*>(input), reinterpret_cast<const float4*>(gpos), nrm,
+        reinterpret_cast<float4*>(output), int(W), int(H), int(stride), sp2, sn2, sl2);
     RR_CHECK_LAUNCH(ctx);
     ctx->launches += 1;
     return RR_OK;
@@ -80,7 +110,10 @@ extern "C" rr_status rr_atrous_iteration(rr_ctx* ctx, const float* input, const 
         return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_atrous_iteration: bad image size");
     if (input == output) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_atrous_iteration: input aliases output");
     RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
-    return atrous_launch(ctx, input, gpos, gnrm, output, p->width, p->height, p->stride, p->sigma_position,
+    const float4* nrm = nullptr;
+    rr_status st = atrous_normals(ctx, gnrm, p->width, p->height, static_cast<cudaStream_t>(stream), &nrm);
+    if (st != RR_OK) return st;
+    return atrous_launch(ctx, input, gpos, nrm, output, p->width, p->height, p->stride, p->sigma_position,
                          p->sigma_normal, p->sigma_luminance, static_cast<cudaStream_t>(stream));
 }
 
@@ -97,11 +130,14 @@ extern "C" rr_status rr_atrous_execute(rr_ctx* ctx, const float* input, const fl
     RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
     // AtrousPass.cpp:265 clamps to 1..7; slot (iterations-1)&1 holds the result.
     const uint32_t iters = std::min(std::max(p->iterations, 1u), 7u);
+    const float4* nrm = nullptr;
+    rr_status st0 = atrous_normals(ctx, gnrm, p->width, p->height, static_cast<cudaStream_t>(stream), &nrm);
+    if (st0 != RR_OK) return st0;
     const float* read = input;
     float* ping[2] = {ping0, ping1};
     for (uint32_t it = 0; it < iters; ++it) {
         float* write = ping[it & 1u];
-        rr_status st = atrous_launch(ctx, read, gpos, gnrm, write, p->width, p->height, 1u << it,
+        rr_status st = atrous_launch(ctx, read, gpos, nrm, write, p->width, p->height, 1u << it,
                                      p->sigma_position, p->sigma_normal, p->sigma_luminance,
                                      static_cast<cudaStream_t>(stream));
         if (st != RR_OK) return st;

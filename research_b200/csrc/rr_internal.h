@@ -56,6 +56,8 @@ struct rr_ctx {
     std::vector<rr_stage_event> pending;   // recorded, not yet read back
     std::vector<cudaEvent_t> event_pool;
     double* mse_partial = nullptr;         // rr_image_mse block partials
+    float4* atrous_nrm = nullptr;          // A-trous: the G-buffer normals, normalized once per call
+    size_t atrous_nrm_px = 0;
 };
 
 // Records a CUDA event pair around stage launches on the caller's stream;

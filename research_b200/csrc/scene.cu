@@ -88,6 +88,7 @@ rr_status rr_ctx_destroy(rr_ctx* ctx) {
     cudaFree(ctx->counters);
     cudaFree(ctx->work64);
     cudaFree(ctx->mse_partial);
+    cudaFree(ctx->atrous_nrm);
     delete ctx;
     return RR_OK;
 }
