@@ -7,6 +7,11 @@ replayed from a captured CUDA graph, with traversal variants picked by the
 batch autotuner. Reported beside it: the same batch without the graph, and
 the scenes rendered one rr_pathtracer_execute call after another, and the
 same three forms at small images (128^2, 1 spp: the launch-bound regime).
+Then guiding per scene (rr_batch_execute_guided): every scene gets its own
+guide (a 32^3 vMF grid, or its own BF16 MLP run by one grouped tensor-core
+launch per bounce for all scenes), the 8 spp are rendered as frames of
+--guided-spp with every guide updated after each frame (rr_guides_update),
+against the same work scene by scene.
 Device time from CUDA events; prints one JSON line (Mpaths/s over the batch).
 
     python bench_batch.py [--scenes 64 --spp 8 --frames 3 --warmup 1]
@@ -32,6 +37,10 @@ def main():
     ap.add_argument("--seed", type=int, default=0x5EED0004)
     ap.add_argument("--small-side", type=int, default=128)
     ap.add_argument("--small-spp", type=int, default=1)
+    ap.add_argument("--guided-spp", type=int, default=2,
+                    help="guided batches: spp per frame; each frame is followed by one update of every guide")
+    ap.add_argument("--guides", default="grid,mlp", help="guide kinds to run per scene ('' for none)")
+    ap.add_argument("--no-guided-sequential", action="store_true")
     args = ap.parse_args()
 
     import numpy as np
@@ -112,6 +121,69 @@ def main():
     ms = timed(sm_sequential)
     sm["sequential"] = {"ms": round(ms, 3), "mpaths_s": round(sm_paths / ms / 1e3, 2)}
     sm["config"] = {"side": args.small_side, "spp": args.small_spp, "paths_per_batch": sm_paths}
+
+    # learned (or grid) guiding per scene: the batch's spp rendered as frames
+    # of --guided-spp with one guide per scene, every guide updated after each
+    # frame (rr_guides_update: one host wait for all sample counts), against
+    # the same work scene by scene (rr_guided_pathtracer_execute +
+    # rr_guide_update per scene)
+    import ctypes as C
+    L = rr.lib()
+    gspp = args.guided_spp
+    gframes = max(1, args.spp // gspp)
+    g_outs = [torch.empty((gspp, int(s), int(s), 4), device="cuda") for s in sides]
+    g_ptrs = [o.data_ptr() for o in g_outs]
+    guided = {}
+    for kind in [k for k in args.guides.split(",") if k]:
+        gk = rr.GUIDE_GRID if kind == "grid" else rr.GUIDE_MLP
+        guides = []
+        for i in range(args.scenes):
+            d = rr.GuideDesc(gk, 32, 0.5, 0.8, (C.c_float * 3)(-52.0, -52.0, -52.0), (C.c_float * 3)(52.0, 52.0, 52.0),
+                             1 << 20, 1 << 16, 1e-2, 100 + i)
+            h = C.c_void_p()
+            ctx.check(L.rr_guide_create(ctx.handle, C.byref(d), C.byref(h)))
+            guides.append(h)
+        garr = (C.c_void_p * len(guides))(*[g.value for g in guides])
+
+        def batch_frames(seed, update=True):
+            for j in range(gframes):
+                batch.execute_guided(cams, rr.PtParams(seed + j * gspp, args.bounces, gspp, rr.PT_FLAG_GRAPH),
+                                     [g.value for g in guides], g_ptrs, st)
+                if update:
+                    ctx.check(L.rr_guides_update(ctx.handle, garr, len(guides), st))
+
+        ms_g = timed(batch_frames)
+        ms_render = timed(lambda seed: batch_frames(seed, update=False))
+        entry = {"ms_per_batch": round(ms_g, 3), "mpaths_s": round(paths / ms_g / 1e3, 2),
+                 "render_only": {"ms": round(ms_render, 3), "mpaths_s": round(paths / ms_render / 1e3, 2)},
+                 "frames_per_batch": gframes, "spp_per_frame": gspp}
+        if not args.no_guided_sequential:
+            def seq_frames(seed):
+                for j in range(gframes):
+                    p = rr.PtParams(seed + j * gspp, args.bounces, gspp, 0)
+                    for sc, cam, o, g in zip(scenes, cams, g_outs, guides):
+                        ctx.check(L.rr_guided_pathtracer_execute(ctx.handle, sc.handle, C.byref(cam), C.byref(p), g,
+                                                                 o.data_ptr(), st))
+                        ctx.check(L.rr_guide_update(ctx.handle, g, st))
+            ms_s = timed(seq_frames)
+            entry["sequential_scenes"] = {"ms": round(ms_s, 3), "mpaths_s": round(paths / ms_s / 1e3, 2)}
+        gst = rr.GuideStats()
+        rec = []
+        for g in guides:
+            ctx.check(L.rr_guide_get_stats(ctx.handle, g, C.byref(gst)))
+            rec.append(gst.samples_recorded)
+        entry["samples_recorded_per_scene"] = {"min": int(min(rec)), "max": int(max(rec))}
+        entry["finite"] = bool(all(torch.isfinite(o).all() for o in g_outs))
+        if gk == rr.GUIDE_MLP:
+            err = C.c_int(0)
+            bad = 0
+            for g in guides:
+                ctx.check(L.rr_guide_mlp_params(ctx.handle, g, None, None, None, rr.MLP_PARAM_COUNT, C.byref(err)))
+                bad += err.value
+            entry["tensor_core_wait_errors"] = bad
+        guided[kind] = entry
+        for g in guides:
+            L.rr_guide_destroy(g)
     line = {"metric": "Mpaths/s, 64-scene batch in one set of launches under a CUDA graph, 1xB200",
             "value": round(paths / ms_graph / 1e3, 2), "unit": "Mpaths/s", "ms_per_batch": round(ms_graph, 3),
             "plain_batch": {"ms": round(ms_plain, 3), "mpaths_s": round(paths / ms_plain / 1e3, 2)},
@@ -124,6 +196,11 @@ def main():
                        "triangles_total": int(built_tris), "pixels_total": int(sum(int(s) ** 2 for s in sides)),
                        "guiding": "none (the reference path tracer)"},
             "small_images": sm,
+            "guided_per_scene": {"config": {"grid": "32^3 cells x 8 vMF lobes per scene",
+                                            "mlp": "80-64-64-64-64-48 BF16 MLP per scene, Adam lr 1e-2, "
+                                                   "2^16 samples per update",
+                                            "max_samples_per_scene": 1 << 20},
+                                 **guided},
             "frames": args.frames, "warmup": args.warmup, "scene_build_s": round(build_s, 1), "finite": finite}
     print(json.dumps(line), flush=True)
     batch.close()

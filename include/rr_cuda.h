@@ -503,6 +503,22 @@ rr_status rr_guided_pathtracer_execute(rr_ctx* ctx, const rr_scene* scene, const
                                        const rr_pt_params* params, rr_guide* guide,
                                        float* radiance_out, void* stream);
 
+/* Guided batches: rr_batch_execute with one guide per scene (guides[i] for
+ * scene i; all of one kind, none twice). Each scene's image, and the training
+ * samples recorded into its guide (as a set), are those of
+ * rr_guided_pathtracer_execute of that scene alone with the same guide,
+ * camera and params. MLP guides run grouped: at every bounce the queries are
+ * gathered per scene and one tensor-core launch runs each group through its
+ * own scene's network. flags: RR_PT_FLAG_GRAPH captures the frame in a CUDA
+ * graph on first use and replays it after; the counting and timing flags are
+ * ignored. */
+rr_status rr_batch_execute_guided(rr_ctx* ctx, rr_batch* batch, const GpuCameraData* cameras,
+                                  const rr_pt_params* params, rr_guide* const* guides,
+                                  float* const* radiance_out, void* stream);
+/* rr_guide_update of `count` guides, with one host wait for all of their
+ * sample counts (rr_guide_update is this call with one guide). */
+rr_status rr_guides_update(rr_ctx* ctx, rr_guide* const* guides, uint32_t count, void* stream);
+
 /* ── output formats (SURVEY "next": tonemap / PNG / MSE utilities) ─────
  * rr_tonemap_execute: exposure, ACES filmic approximation, clamp, gamma
  * 1/2.2, 8-bit RGBA (Application.cpp:853-866; tonemap.slang:40-69).

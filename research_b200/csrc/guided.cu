@@ -21,10 +21,12 @@
 #include "rr_wavefront.cuh"
 #include "rr_vmf.cuh"
 #include "rr_guide.h"
+#include "rr_batch.h"
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 
@@ -97,16 +99,35 @@ __global__ void __launch_bounds__(kBlock) guided_surface_kernel(DevScene s, cons
     }
 }
 
+// A scene's guide as the shade stage uses it.
+struct GuideRefs {
+    GridView grid;
+    float4* rec0;
+    float4* rec1;
+    float4* rec2;
+    float4* rec3;
+    uint32_t paths;
+    float alpha;
+};
+
 // Shade stage of the guided tracer (cf. shade_kernel in pathtracer.cu).
-template <bool SlotMixture>
-__global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s, GuidedLaunch G,
+// SlotMixture: the mixture of queue entry i is in G.mix at slot i, or
+// (Multi) at slot_map[i] (~0: none). Multi: a batch of scenes; a ray's scene
+// index is in c.w, its scene is table[index], its image outs[index] and its
+// guide gtab[index]; the index is carried on to the next queues.
+template <bool SlotMixture, bool Multi>
+__global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s0, GuidedLaunch G,
+                                                              const DevScene* __restrict__ table,
+                                                              float4* const* __restrict__ outs,
+                                                              const GuideEntry* __restrict__ gtab,
+                                                              const uint32_t* __restrict__ slot_map,
                                                               const float4* __restrict__ qa,
                                                               const float4* __restrict__ qb,
                                                               const float4* __restrict__ qc,
                                                               const float4* __restrict__ hits,
                                                               float4* na, float4* nb, float4* nc,
                                                               float4* sa, float4* sb, float4* sc,
-                                                              float4* __restrict__ out,
+                                                              float4* __restrict__ out0,
                                                               const uint32_t* count_ptr,
                                                               uint32_t* next_count, uint32_t* shadow_count) {
     const uint32_t count = *count_ptr;
@@ -115,20 +136,30 @@ __global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s, Gui
     for (uint32_t base = warp_first; base < count; base += stride) {
         const uint32_t i = base + lane_id();
         bool cont = false, emit_shadow = false;
-        uint32_t pid = 0, seed = 0;
+        uint32_t pid = 0, seed = 0, sid = 0;
         float3 new_o = f3(0, 0, 0), wi = f3(0, 0, 0), thp = f3(0, 0, 0);
         float3 sh_o = f3(0, 0, 0), sh_d = f3(0, 0, 0), contrib = f3(0, 0, 0);
         float sh_tmax = 0.0f;
         if (i < count) {
             const float4 a = qa[i], b = qb[i], c = qc[i];
             const float4 h = hits[i];
+            if constexpr (Multi) sid = __float_as_uint(c.w);
+            const DevScene& s = Multi ? table[sid] : s0;
+            float4* const out = Multi ? outs[sid] : out0;
+            GuideRefs R;
+            if constexpr (Multi) {
+                const GuideEntry& E = gtab[sid];
+                R = GuideRefs{E.grid, E.rec[0], E.rec[1], E.rec[2], E.rec[3], E.paths, E.alpha};
+            } else {
+                R = GuideRefs{G.grid, G.rec0, G.rec1, G.rec2, G.rec3, G.paths, G.alpha};
+            }
             pid = __float_as_uint(a.w);
             seed = __float_as_uint(b.w);
             const float3 ray_dir = f3(b.x, b.y, b.z);
             thp = f3(c.x, c.y, c.z);
             float4 o = out[pid];
             if (G.bounce > 0)  // radiance gathered before the previous vertex's continuation
-                reinterpret_cast<float*>(G.rec2 + size_t(G.bounce - 1) * G.paths + pid)[3] = lum709(xyz(o));
+                reinterpret_cast<float*>(R.rec2 + size_t(G.bounce - 1) * R.paths + pid)[3] = lum709(xyz(o));
             const uint32_t inst = __float_as_uint(h.z);
             if (inst == kNoIndex) {
                 const float3 L = thp * sky_radiance(ray_dir);
@@ -186,9 +217,14 @@ __global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s, Gui
                     if (!G.last) {
                         VmfMixture mix;
                         bool valid;
-                        if (SlotMixture) load_mixture_slot(G.mix, i, mix, valid);
-                        else load_mixture_grid(G.grid, sf.pos, mix, valid);
-                        const float alpha = valid ? G.alpha : 0.0f;
+                        if constexpr (SlotMixture) {
+                            const uint32_t slot = Multi ? slot_map[i] : i;
+                            valid = false;
+                            if (slot != kNoIndex) load_mixture_slot(G.mix, slot, mix, valid);
+                        } else {
+                            load_mixture_grid(R.grid, sf.pos, mix, valid);
+                        }
+                        const float alpha = valid ? R.alpha : 0.0f;
                         const float u_sel = rand_float(seed);
                         const float u0 = rand_float(seed);
                         const float u1 = rand_float(seed);
@@ -224,28 +260,29 @@ __global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s, Gui
                             if (alive) {
                                 cont = true;
                                 new_o = sf.pos + n * 1e-4f;
-                                const size_t r = size_t(G.bounce) * G.paths + pid;
-                                G.rec0[r] = make_float4(sf.pos.x, sf.pos.y, sf.pos.z, pdf);
-                                G.rec1[r] = make_float4(wi.x, wi.y, wi.z, lum709(thp));
-                                G.rec2[r] = make_float4(n.x, n.y, n.z, __int_as_float(-1));
-                                G.rec3[r] = make_float4(wo.x, wo.y, wo.z, 0.0f);
+                                const size_t r = size_t(G.bounce) * R.paths + pid;
+                                R.rec0[r] = make_float4(sf.pos.x, sf.pos.y, sf.pos.z, pdf);
+                                R.rec1[r] = make_float4(wi.x, wi.y, wi.z, lum709(thp));
+                                R.rec2[r] = make_float4(n.x, n.y, n.z, __int_as_float(-1));
+                                R.rec3[r] = make_float4(wo.x, wo.y, wo.z, 0.0f);
                             }
                         }
                     }
                 }
             }
         }
+        const float tag = Multi ? __uint_as_float(sid) : 0.0f;
         const uint32_t sslot = warp_alloc(emit_shadow, shadow_count);
         if (emit_shadow) {
             sa[sslot] = make_float4(sh_o.x, sh_o.y, sh_o.z, __uint_as_float(pid));
             sb[sslot] = make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
-            sc[sslot] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+            sc[sslot] = make_float4(contrib.x, contrib.y, contrib.z, tag);
         }
         const uint32_t rslot = warp_alloc(cont, next_count);
         if (cont) {
             na[rslot] = make_float4(new_o.x, new_o.y, new_o.z, __uint_as_float(pid));
             nb[rslot] = make_float4(wi.x, wi.y, wi.z, __uint_as_float(seed));
-            nc[rslot] = make_float4(thp.x, thp.y, thp.z, 0.0f);
+            nc[rslot] = make_float4(thp.x, thp.y, thp.z, tag);
         }
     }
 }
@@ -283,6 +320,128 @@ __global__ void __launch_bounds__(kBlock) resolve_kernel(const float4* __restric
         const uint32_t slot = warp_alloc(emit, S.count);
         if (emit && slot < S.capacity) {
             S.s0[slot] = s0; S.s1[slot] = s1; S.s2[slot] = s2; S.s3[slot] = s3;
+        }
+    }
+}
+
+// ── guided batches ─────────────────────────────────────────────────────────
+// Warp-aggregated slot allocation per scene: the lanes that want a slot and
+// share a scene index take consecutive slots from one atomic on that scene's
+// counter. Returns the lane's offset (counter value before the lane).
+__device__ __forceinline__ uint32_t warp_alloc_keyed(bool want, uint32_t key, uint32_t* counters) {
+    const uint32_t peers = __match_any_sync(kFull, want ? key : kNoIndex);
+    const uint32_t leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (want && lane_id() == leader) base = atomicAdd(counters + key, __popc(peers));
+    base = __shfl_sync(kFull, base, leader);
+    return base + __popc(peers & ((1u << lane_id()) - 1u));
+}
+
+// MLP guides in a batch: the surface inputs of every queued ray that hit a
+// non-emissive surface go to its scene's group of slots (group_base[scene]
+// onwards; a scene has at most as many queued rays as paths), and slot_map
+// records the slot of each queue entry (~0 for none). The grouped forward
+// then runs each group through its scene's network.
+__global__ void __launch_bounds__(kBlock) guided_surface_batch_kernel(const DevScene* __restrict__ table,
+                                                                      const float4* __restrict__ qb,
+                                                                      const float4* __restrict__ qc,
+                                                                      const float4* __restrict__ hits,
+                                                                      const uint32_t* __restrict__ group_base,
+                                                                      uint32_t* group_count, float4* __restrict__ surf,
+                                                                      uint32_t* __restrict__ slot_map,
+                                                                      const uint32_t* count_ptr) {
+    const uint32_t count = *count_ptr;
+    const uint32_t warp_first = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+    for (uint32_t base = warp_first; base < count; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + lane_id();
+        bool want = false;
+        uint32_t sid = 0;
+        float4 a = make_float4(0, 0, 0, 0), b = make_float4(0, 0, 0, 0), c = make_float4(0, 0, 0, 0);
+        if (i < count) {
+            const float4 h = hits[i];
+            sid = __float_as_uint(qc[i].w);
+            const uint32_t inst = __float_as_uint(h.z);
+            if (inst != kNoIndex) {
+                const DevScene& s = table[sid];
+                const Surface sf = hit_surface(s, inst, __float_as_uint(h.w), h.x, h.y);
+                const float4 m1 = __ldg(s.materials + sf.material * 2 + 1);
+                if (!(m1.x > 0.0f || m1.y > 0.0f || m1.z > 0.0f)) {
+                    const float4 qd = qb[i];
+                    const float3 wo = -f3(qd.x, qd.y, qd.z);
+                    float3 n = sf.normal;
+                    if (dot(n, wo) < 0.0f) n = -n;
+                    a = make_float4(sf.pos.x, sf.pos.y, sf.pos.z, 1.0f);
+                    b = make_float4(n.x, n.y, n.z, 1.0f);
+                    c = make_float4(wo.x, wo.y, wo.z, 0.0f);
+                    want = true;
+                }
+            }
+        }
+        const uint32_t off = warp_alloc_keyed(want, sid, group_count);
+        if (i < count) {
+            uint32_t slot = kNoIndex;
+            if (want) {
+                slot = group_base[sid] + off;
+                surf[size_t(slot) * 3] = a; surf[size_t(slot) * 3 + 1] = b; surf[size_t(slot) * 3 + 2] = c;
+            }
+            slot_map[i] = slot;
+        }
+    }
+}
+
+// resolve_kernel over the records of every scene of a batch: record k of
+// the batch is record k - rec_prefix[g] of scene g (the last g with
+// rec_prefix[g] <= k); samples go to that scene's guide.
+__global__ void __launch_bounds__(kBlock) resolve_batch_kernel(const GuideEntry* __restrict__ gtab,
+                                                               float4* const* __restrict__ outs,
+                                                               const unsigned long long* __restrict__ rec_prefix,
+                                                               uint32_t scenes) {
+    const unsigned long long total = rec_prefix[scenes];
+    for (unsigned long long k = (unsigned long long)(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u); k < total;
+         k += (unsigned long long)(gridDim.x) * blockDim.x) {
+        const unsigned long long rg = k + lane_id();
+        bool emit = false;
+        uint32_t sid = 0, r = 0;
+        float4 s0, s1, s2, s3;
+        if (rg < total) {
+            uint32_t lo = 0, hi = scenes - 1;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (rec_prefix[mid] <= rg) lo = mid; else hi = mid - 1;
+            }
+            sid = lo;
+            r = uint32_t(rg - rec_prefix[sid]);
+            const GuideEntry& E = gtab[sid];
+            const float4 c = E.rec[2][r];
+            const float before = c.w;
+            if (before >= 0.0f) {  // NaN (never filled) fails this test
+                const float4 a = E.rec[0][r], b = E.rec[1][r];
+                const uint32_t pid = r % E.paths;
+                const float final_l = lum709(xyz(outs[sid][pid]));
+                const float lin = mx(final_l - before, 0.0f) / mx(b.w, 1e-20f);
+                const float w = lin / a.w;
+                if (w > 0.0f && w < 3.0e38f) {
+                    emit = true;
+                    s0 = make_float4(a.x, a.y, a.z, w);
+                    s1 = make_float4(b.x, b.y, b.z, __uint_as_float(r));
+                    s2 = make_float4(c.x, c.y, c.z, 0.0f);
+                    const float4 d = E.rec[3][r];
+                    s3 = make_float4(d.x, d.y, d.z, 0.0f);
+                }
+            }
+        }
+        // per-scene aggregation onto that scene's sample counter
+        const uint32_t peers = __match_any_sync(kFull, emit ? sid : kNoIndex);
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (emit && lane_id() == leader) base = atomicAdd(gtab[sid].S.count, __popc(peers));
+        base = __shfl_sync(kFull, base, leader);
+        const uint32_t slot = base + __popc(peers & ((1u << lane_id()) - 1u));
+        if (emit) {
+            const GuideSamples& S = gtab[sid].S;
+            if (slot < S.capacity) {
+                S.s0[slot] = s0; S.s1[slot] = s1; S.s2[slot] = s2; S.s3[slot] = s3;
+            }
         }
     }
 }
@@ -504,6 +663,9 @@ extern "C" rr_status rr_guide_create(rr_ctx* ctx, const rr_guide_desc* d, rr_gui
         if ((st = guide_alloc(ctx, g, &p, sizeof(uint32_t) * 4)) != RR_OK) return fail(st);
         g->samples.count = static_cast<uint32_t*>(p);
         cudaMemset(p, 0, sizeof(uint32_t) * 4);
+        const cudaError_t e = cudaMallocHost(&p, sizeof(uint32_t) * 4);
+        if (e != cudaSuccess) return fail(rr_fail(ctx, RR_ERR_OUT_OF_MEMORY, "rr_guide_create: %s", cudaGetErrorString(e)));
+        g->count_host = static_cast<uint32_t*>(p);
     }
     if (d->kind == RR_GUIDE_GRID) {
         const uint32_t R = d->grid_resolution;
@@ -566,6 +728,7 @@ extern "C" rr_status rr_guide_destroy(rr_guide* g) {
     if (!g) return RR_ERR_INVALID_ARGUMENT;
     if (g->ctx) cudaSetDevice(g->ctx->device);
     for (void* p : g->allocations) cudaFree(p);
+    if (g->count_host) cudaFreeHost(g->count_host);
     if (g->ev0) cudaEventDestroy(g->ev0);
     if (g->ev1) cudaEventDestroy(g->ev1);
     delete g;
@@ -645,7 +808,7 @@ extern "C" rr_status rr_guided_pathtracer_execute(rr_ctx* ctx, const rr_scene* s
     ShadowKernel sh_k = shadow_variant<false>(ctx->shadow_variant);
     const int g_ext = persistent_grid(ctx, reinterpret_cast<const void*>(ext_k));
     const int g_sh = persistent_grid(ctx, reinterpret_cast<const void*>(sh_k));
-    auto shade_k = mlp ? guided_shade_kernel<true> : guided_shade_kernel<false>;
+    auto shade_k = mlp ? guided_shade_kernel<true, false> : guided_shade_kernel<false, false>;
     const int g_shade = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(shade_k)),
                                       int((n + kBlock - 1) / kBlock));
     GuidedLaunch G;
@@ -671,7 +834,8 @@ extern "C" rr_status rr_guided_pathtracer_execute(rr_ctx* ctx, const rr_scene* s
             if ((st = rr_mlp_guide_infer(ctx, g, cb, uint32_t(n), stream)) != RR_OK) return st;
             launches += 1 + g->mlp_infer_launches;
         }
-        shade_k<<<g_shade, kBlock, 0, stream>>>(S, G, q.ray_a[cur], q.ray_b[cur], q.ray_c[cur], q.hits,
+        shade_k<<<g_shade, kBlock, 0, stream>>>(S, G, nullptr, nullptr, nullptr, nullptr, q.ray_a[cur], q.ray_b[cur],
+                                                q.ray_c[cur], q.hits,
                                                 q.ray_a[nxt], q.ray_b[nxt], q.ray_c[nxt], q.shadow_a, q.shadow_b,
                                                 q.shadow_c, out, cb, cn, cb + 2);
         RR_CHECK_LAUNCH(ctx);
@@ -692,15 +856,9 @@ extern "C" rr_status rr_guided_pathtracer_execute(rr_ctx* ctx, const rr_scene* s
     return RR_OK;
 }
 
-extern "C" rr_status rr_guide_update(rr_ctx* ctx, rr_guide* g, void* stream_v) {
-    if (!ctx || !g) return RR_ERR_INVALID_ARGUMENT;
-    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
-    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+// One update of guide g from the n samples its last execute recorded.
+static rr_status guide_update_n(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t stream) {
     if (!g->ev0) { RR_TRY_CUDA(ctx, cudaEventCreate(&g->ev0)); RR_TRY_CUDA(ctx, cudaEventCreate(&g->ev1)); }
-    // the sample count decides the launch sizes: read it back (one small copy)
-    uint32_t n = 0;
-    RR_TRY_CUDA(ctx, cudaMemcpyAsync(&n, g->samples.count, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-    RR_TRY_CUDA(ctx, cudaStreamSynchronize(stream));
     g->stats.samples_recorded = n;
     n = std::min(n, g->samples.capacity);
     RR_TRY_CUDA(ctx, cudaEventRecord(g->ev0, stream));
@@ -746,6 +904,33 @@ extern "C" rr_status rr_guide_update(rr_ctx* ctx, rr_guide* g, void* stream_v) {
     g->stats.samples_used = n;
     g->stats.updates += 1;
     g->pending_stats = true;
+    return RR_OK;
+}
+
+extern "C" rr_status rr_guide_update(rr_ctx* ctx, rr_guide* g, void* stream_v) {
+    return rr_guides_update(ctx, &g, 1, stream_v);
+}
+
+extern "C" rr_status rr_guides_update(rr_ctx* ctx, rr_guide* const* guides, uint32_t count, void* stream_v) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    if (!guides) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_guides_update: null argument");
+    for (uint32_t i = 0; i < count; ++i)
+        if (!guides[i] || guides[i]->ctx != ctx)
+            return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_guides_update: guide %u is null or of another context", i);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    // the sample counts decide the launch sizes: read them back (one small
+    // copy per guide into its pinned word, one wait for all)
+    for (uint32_t i = 0; i < count; ++i)
+        RR_TRY_CUDA(ctx, cudaMemcpyAsync(guides[i]->count_host, guides[i]->samples.count, sizeof(uint32_t),
+                                         cudaMemcpyDeviceToHost, stream));
+    RR_TRY_CUDA(ctx, cudaStreamSynchronize(stream));
+    std::vector<uint32_t> n(count);
+    for (uint32_t i = 0; i < count; ++i) n[i] = guides[i]->count_host[0];
+    for (uint32_t i = 0; i < count; ++i) {
+        const rr_status st = guide_update_n(ctx, guides[i], n[i], stream);
+        if (st != RR_OK) return st;
+    }
     return RR_OK;
 }
 
@@ -829,5 +1014,251 @@ extern "C" rr_status rr_guide_set_samples(rr_ctx* ctx, rr_guide* g, const float*
     set_samples_kernel<<<std::max(1u, (count + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream_v)>>>(
         reinterpret_cast<const float4*>(samples), g->samples, count);
     RR_CHECK_LAUNCH(ctx);
+    return RR_OK;
+}
+
+// ── guided batches ─────────────────────────────────────────────────────────
+// Per-call guide table in d_gcall (staged through h_gcall like the batch's
+// own table): GuideEntry[count] | MlpView[count] | u64 rec_prefix[count + 1]
+// (first record of each scene in the batch's record index space) |
+// u32 group_base[count] (first mixture slot of each scene: prefix of paths).
+static size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+void rr_batch_free_guided(rr_batch* B) {
+    if (B->gexec) cudaGraphExecDestroy(B->gexec);
+    B->gexec = nullptr;
+    for (int k = 0; k < 2; ++k) {
+        if (B->gstaged[k]) cudaEventDestroy(B->gstaged[k]);
+        if (B->h_gcall[k]) cudaFreeHost(B->h_gcall[k]);
+        B->gstaged[k] = nullptr;
+        B->h_gcall[k] = nullptr;
+    }
+    cudaFree(B->d_gcall); cudaFree(B->surf); cudaFree(B->mix); cudaFree(B->slot_map);
+    cudaFree(B->group_count); cudaFree(B->tile_prefix);
+    B->d_gcall = nullptr; B->surf = nullptr; B->mix = nullptr; B->slot_map = nullptr;
+    B->group_count = nullptr; B->tile_prefix = nullptr;
+    B->slots = 0;
+}
+
+static rr_status ensure_batch_guided(rr_ctx* ctx, rr_batch* B, size_t slots, bool mlp) {
+    const size_t count = B->scenes.size();
+    if (!B->d_gcall) {
+        B->gcall_bytes = align16(sizeof(GuideEntry) * count) + align16(sizeof(MlpView) * count) +
+                         align16(sizeof(unsigned long long) * (count + 1)) + align16(sizeof(uint32_t) * count);
+        RR_TRY_CUDA(ctx, cudaMalloc(&B->d_gcall, B->gcall_bytes));
+        RR_TRY_CUDA(ctx, cudaMalloc(&B->group_count, sizeof(uint32_t) * count));
+        RR_TRY_CUDA(ctx, cudaMalloc(&B->tile_prefix, sizeof(uint32_t) * (count + 1)));
+        for (int k = 0; k < 2; ++k) {
+            RR_TRY_CUDA(ctx, cudaMallocHost(&B->h_gcall[k], B->gcall_bytes));
+            RR_TRY_CUDA(ctx, cudaEventCreateWithFlags(&B->gstaged[k], cudaEventDisableTiming));
+        }
+    }
+    if (mlp && B->slots < slots) {
+        cudaFree(B->surf); cudaFree(B->mix); cudaFree(B->slot_map);
+        B->surf = nullptr; B->mix = nullptr; B->slot_map = nullptr;
+        B->slots = 0;
+        RR_TRY_CUDA(ctx, cudaMalloc(&B->surf, slots * 3 * sizeof(float4)));
+        RR_TRY_CUDA(ctx, cudaMalloc(&B->mix, slots * (kMaxLobes + 2) * sizeof(float4)));
+        RR_TRY_CUDA(ctx, cudaMalloc(&B->slot_map, slots * sizeof(uint32_t)));
+        B->slots = slots;
+    }
+    return RR_OK;
+}
+
+// Enqueues one guided batch frame; returns the kernels launched.
+static rr_status enqueue_guided_batch(rr_ctx* ctx, rr_batch* B, rr_guide* const* guides, const size_t* paths_of,
+                                      uint32_t tiles, size_t paths, uint32_t max_bounces, bool mlp,
+                                      cudaStream_t stream, uint64_t* launches_out) {
+    const uint32_t count = uint32_t(B->scenes.size());
+    rr_pt_queues& q = ctx->pt;
+    uint32_t* C = ctx->counters;
+    const BatchEntry* entries = reinterpret_cast<const BatchEntry*>(B->d_call);
+    float4* const* outs = reinterpret_cast<float4* const*>(B->d_call + B->entries_bytes);
+    const GuideEntry* gtab = reinterpret_cast<const GuideEntry*>(B->d_gcall);
+    const size_t o_nets = align16(sizeof(GuideEntry) * count);
+    const size_t o_prefix = o_nets + align16(sizeof(MlpView) * count);
+    const size_t o_base = o_prefix + align16(sizeof(unsigned long long) * (count + 1));
+    const MlpView* nets = reinterpret_cast<const MlpView*>(B->d_gcall + o_nets);
+    const unsigned long long* rec_prefix = reinterpret_cast<const unsigned long long*>(B->d_gcall + o_prefix);
+    const uint32_t* group_base = reinterpret_cast<const uint32_t*>(B->d_gcall + o_base);
+    uint64_t launches = 0;
+    RR_TRY_CUDA(ctx, cudaMemsetAsync(C, 0, sizeof(uint32_t) * kCounterWords, stream));
+    for (uint32_t i = 0; i < count; ++i) {
+        rr_guide* g = guides[i];
+        RR_TRY_CUDA(ctx, cudaMemsetAsync(g->samples.count, 0, sizeof(uint32_t) * 4, stream));
+        // unfilled records read as NaN and are skipped by the resolve pass
+        RR_TRY_CUDA(ctx, cudaMemsetAsync(g->rec[2], 0xff, paths_of[i] * max_bounces * sizeof(float4), stream));
+    }
+    {
+        const uint64_t threads = uint64_t(tiles) * 32;
+        raygen_batch_kernel<<<uint32_t((threads + kBlock - 1) / kBlock), kBlock, 0, stream>>>(
+            entries, count, tiles, outs, q.ray_a[0], q.ray_b[0], q.ray_c[0], C);
+        RR_CHECK_LAUNCH(ctx);
+        launches += 1;
+    }
+    BatchQueueKernel ext_k = extend_batch_variant<false>(ctx->extend_variant);
+    BatchShadowKernel sh_k = shadow_batch_variant<false>(ctx->shadow_variant);
+    const int g_ext = persistent_grid(ctx, reinterpret_cast<const void*>(ext_k));
+    const int g_sh = persistent_grid(ctx, reinterpret_cast<const void*>(sh_k));
+    auto shade_k = mlp ? guided_shade_kernel<true, true> : guided_shade_kernel<false, true>;
+    const int g_shade = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(shade_k)),
+                                      int((paths + kBlock - 1) / kBlock));
+    GuidedLaunch G{};
+    G.lobes = kMaxLobes;
+    G.mix = mlp ? B->mix : nullptr;
+    for (uint32_t b = 0; b < max_bounces; ++b) {
+        const int cur = b & 1, nxt = cur ^ 1;
+        uint32_t* cb = C + 4 * b;
+        uint32_t* cn = C + 4 * (b + 1);
+        G.bounce = b;
+        G.last = b + 1 == max_bounces ? 1u : 0u;
+        ext_k<<<g_ext, kBlock, 0, stream>>>(B->d_table, q.ray_a[cur], q.ray_b[cur], q.ray_c[cur], q.hits, cb, cb + 1,
+                                            ctx->work64);
+        RR_CHECK_LAUNCH(ctx);
+        if (mlp && !G.last) {
+            RR_TRY_CUDA(ctx, cudaMemsetAsync(B->group_count, 0, sizeof(uint32_t) * count, stream));
+            guided_surface_batch_kernel<<<g_shade, kBlock, 0, stream>>>(B->d_table, q.ray_b[cur], q.ray_c[cur], q.hits,
+                                                                        group_base, B->group_count, B->surf,
+                                                                        B->slot_map, cb);
+            RR_CHECK_LAUNCH(ctx);
+            const rr_status st = rr_mlp_guide_infer_grouped(ctx, nets, count, B->surf, B->mix, group_base,
+                                                            B->group_count, B->tile_prefix, stream);
+            if (st != RR_OK) return st;
+            launches += 3;
+        }
+        shade_k<<<g_shade, kBlock, 0, stream>>>(DevScene{}, G, B->d_table, outs, gtab, B->slot_map, q.ray_a[cur],
+                                                q.ray_b[cur], q.ray_c[cur], q.hits, q.ray_a[nxt], q.ray_b[nxt],
+                                                q.ray_c[nxt], q.shadow_a, q.shadow_b, q.shadow_c, nullptr, cb, cn,
+                                                cb + 2);
+        RR_CHECK_LAUNCH(ctx);
+        sh_k<<<g_sh, kBlock, 0, stream>>>(B->d_table, outs, q.shadow_a, q.shadow_b, q.shadow_c, cb + 2, cb + 3,
+                                          ctx->work64 + 2);
+        RR_CHECK_LAUNCH(ctx);
+        launches += 3;
+    }
+    if (max_bounces > 1) {
+        resolve_batch_kernel<<<std::max(1, ctx->sm_count * 8), kBlock, 0, stream>>>(gtab, outs, rec_prefix, count);
+        RR_CHECK_LAUNCH(ctx);
+        launches += 1;
+    }
+    *launches_out = launches;
+    return RR_OK;
+}
+
+extern "C" rr_status rr_batch_execute_guided(rr_ctx* ctx, rr_batch* B, const GpuCameraData* cams,
+                                             const rr_pt_params* p, rr_guide* const* guides,
+                                             float* const* radiance_out, void* stream_v) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    if (!B || !cams || !p || !guides || !radiance_out)
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute_guided: null argument");
+    if (B->ctx != ctx) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute_guided: batch of another context");
+    if (p->spp == 0 || p->max_bounces == 0 || p->max_bounces > uint32_t(kMaxBounces))
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute_guided: bad spp or max_bounces");
+    const uint32_t count = uint32_t(B->scenes.size());
+    for (uint32_t i = 0; i < count; ++i)
+        if (!guides[i] || guides[i]->ctx != ctx)
+            return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute_guided: guide %u is null or of another context",
+                           i);
+    const uint32_t kind = guides[0]->desc.kind;
+    for (uint32_t i = 1; i < count; ++i)
+        if (guides[i]->desc.kind != kind)
+            return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute_guided: guides of different kinds");
+    {
+        std::vector<const rr_guide*> sorted(guides, guides + count);
+        std::sort(sorted.begin(), sorted.end());
+        if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end())
+            return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute_guided: a guide appears twice");
+    }
+    std::vector<size_t> paths_of(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        const uint64_t n = uint64_t(cams[i].screen_width) * cams[i].screen_height * p->spp;
+        if (n * p->max_bounces >= (1ull << 32))
+            return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute_guided: scene %u: too many paths", i);
+        paths_of[i] = size_t(n);
+    }
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    uint32_t tiles = 0;
+    uint64_t paths = 0;
+    rr_status st = rr_batch_stage_call(ctx, B, cams, p, radiance_out, stream, &tiles, &paths);
+    if (st != RR_OK) return st;
+    const bool mlp = kind == RR_GUIDE_MLP;
+    if ((st = ensure_batch_guided(ctx, B, size_t(paths), mlp)) != RR_OK) return st;
+    for (uint32_t i = 0; i < count; ++i)
+        if ((st = ensure_records(ctx, guides[i], paths_of[i], p->max_bounces)) != RR_OK) return st;
+    // this call's guide table
+    const int k = B->gslot;
+    RR_TRY_CUDA(ctx, cudaEventSynchronize(B->gstaged[k]));
+    unsigned char* h = B->h_gcall[k];
+    GuideEntry* ge = reinterpret_cast<GuideEntry*>(h);
+    MlpView* nv = reinterpret_cast<MlpView*>(h + align16(sizeof(GuideEntry) * count));
+    unsigned long long* rp = reinterpret_cast<unsigned long long*>(
+        h + align16(sizeof(GuideEntry) * count) + align16(sizeof(MlpView) * count));
+    uint32_t* gb = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(rp) +
+                                               align16(sizeof(unsigned long long) * (count + 1)));
+    unsigned long long racc = 0;
+    uint32_t sacc = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        rr_guide* g = guides[i];
+        std::memset(&ge[i], 0, sizeof(GuideEntry));
+        ge[i].grid = g->grid;
+        for (int r = 0; r < 4; ++r) ge[i].rec[r] = g->rec[r];
+        ge[i].S = g->samples;
+        ge[i].paths = uint32_t(paths_of[i]);
+        ge[i].alpha = g->desc.alpha;
+        std::memset(&nv[i], 0, sizeof(MlpView));
+        if (mlp) nv[i] = rr_mlp_guide_view(g);
+        rp[i] = racc;
+        racc += (unsigned long long)(paths_of[i]) * (p->max_bounces - 1);
+        gb[i] = sacc;
+        sacc += uint32_t(paths_of[i]);
+    }
+    rp[count] = racc;
+    RR_TRY_CUDA(ctx, cudaMemcpyAsync(B->d_gcall, h, B->gcall_bytes, cudaMemcpyHostToDevice, stream));
+    RR_TRY_CUDA(ctx, cudaEventRecord(B->gstaged[k], stream));
+    B->gslot ^= 1;
+
+    uint64_t launches = 0;
+    if (p->flags & RR_PT_FLAG_GRAPH) {
+        // the graph holds the queue, record and sample pointers and the launch sizes
+        std::vector<const void*> key = {reinterpret_cast<const void*>(uintptr_t(paths)),
+                                        reinterpret_cast<const void*>(uintptr_t(tiles)),
+                                        reinterpret_cast<const void*>(uintptr_t(p->max_bounces)),
+                                        reinterpret_cast<const void*>(uintptr_t(ctx->extend_variant)),
+                                        reinterpret_cast<const void*>(uintptr_t(ctx->shadow_variant)),
+                                        ctx->pt.ray_a[0], B->surf};
+        for (uint32_t i = 0; i < count; ++i) {
+            key.push_back(guides[i]);
+            key.push_back(guides[i]->rec[2]);
+            key.push_back(guides[i]->samples.count);
+            key.push_back(reinterpret_cast<const void*>(uintptr_t(paths_of[i])));
+        }
+        if (!B->gexec || key != B->gkey) {
+            if (B->gexec) { cudaGraphExecDestroy(B->gexec); B->gexec = nullptr; }
+            RR_TRY_CUDA(ctx, cudaStreamBeginCapture(B->cap_stream, cudaStreamCaptureModeThreadLocal));
+            st = enqueue_guided_batch(ctx, B, guides, paths_of.data(), tiles, size_t(paths), p->max_bounces, mlp,
+                                      B->cap_stream, &launches);
+            cudaGraph_t gr = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(B->cap_stream, &gr);
+            if (st != RR_OK) { if (gr) cudaGraphDestroy(gr); return st; }
+            if (ce != cudaSuccess) return rr_fail(ctx, RR_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+            const cudaError_t ie = cudaGraphInstantiate(&B->gexec, gr, 0);
+            cudaGraphDestroy(gr);
+            if (ie != cudaSuccess) return rr_fail(ctx, RR_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ie));
+            B->gkey = key;
+        } else {
+            launches = 1 + 3 * uint64_t(p->max_bounces) + (mlp ? 3 * uint64_t(p->max_bounces - 1) : 0) +
+                       (p->max_bounces > 1 ? 1 : 0);
+        }
+        RR_TRY_CUDA(ctx, cudaGraphLaunch(B->gexec, stream));
+    } else {
+        st = enqueue_guided_batch(ctx, B, guides, paths_of.data(), tiles, size_t(paths), p->max_bounces, mlp, stream,
+                                  &launches);
+        if (st != RR_OK) return st;
+    }
+    ctx->launches += launches;
+    ctx->last_max_bounces = p->max_bounces;
+    ctx->last_counted = false;
+    for (uint32_t i = 0; i < count; ++i) guides[i]->frame_paths = uint32_t(paths_of[i]);
     return RR_OK;
 }

@@ -80,13 +80,6 @@ constexpr int kSmBwdBar = kSmBwdAct + kTile * kHid * 2;
 constexpr int kSmBwd = kSmBwdBar + 64;
 static_assert(kSmFwdAct % 128 == 0 && kSmBwdAct % 128 == 0, "operand tiles 128-byte aligned");
 
-struct MlpView {
-    const __nv_bfloat16* w16;     // kWeightsBf16
-    const float* params;          // kParams (biases read from here)
-    float3 bmin, inv_ext;
-    int* error;                   // set when an mbarrier wait gave up
-};
-
 // W of every layer as the forward's B operand (out x 80), with the BF16 bias
 // in column kBiasCol(l) and zeros in the other columns past the inputs. Each
 // thread issues 8 global loads before its 8 shared stores.
@@ -253,6 +246,13 @@ struct FwdArgs {
     __nv_bfloat16* X;             // [batch][kXCols], inputs of every layer
     __nv_bfloat16* dZ;            // [batch][kZCols], the forward writes the output layer's block
     float* loss_partial;          // per block
+    // grouped inference: group g's rows are slots group_base[g] + [0, group_count[g]) of surf/mix,
+    // its tiles [tile_prefix[g], tile_prefix[g + 1]), its network nets[g]
+    const MlpView* nets;
+    uint32_t groups;
+    const uint32_t* group_base;
+    const uint32_t* group_count;
+    const uint32_t* tile_prefix;
 };
 
 __device__ __forceinline__ void store_row_bf16(__nv_bfloat16* dst, const float* v, int n) {
@@ -300,14 +300,18 @@ __device__ __forceinline__ void wait_chain(uint64_t* bar, uint32_t phase, bool& 
     tc::fence_after_sync();
 }
 
-template <bool Train>
+// Grouped (inference only): the CTA takes a contiguous range of the groups'
+// tiles and loads a group's weights when its range enters that group.
+template <bool Train, bool Grouped = false>
 __global__ void __launch_bounds__(kTile, 3) mlp_forward_kernel(FwdArgs A) {
+    static_assert(!(Train && Grouped), "grouped forward is inference only");
     extern __shared__ __align__(1024) unsigned char sm[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kSmFwdBar);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSmFwdBar + 8);
     unsigned char* act = sm + kSmFwdAct;
     const int t = threadIdx.x, warp = t >> 5;
-    load_weights_fwd(sm, A.V);
+    MlpView V = A.V;
+    if constexpr (!Grouped) load_weights_fwd(sm, V);
     if (warp == 0) tc::tmem_alloc(tslot, 128);
     if (t == 0) tc::mbar_init(bar, 1);
     tc::fence_proxy_async();
@@ -315,16 +319,50 @@ __global__ void __launch_bounds__(kTile, 3) mlp_forward_kernel(FwdArgs A) {
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *tslot;
-    const uint32_t count = Train ? A.count : *A.count_ptr;
-    const uint32_t tiles = (count + kTile - 1) / kTile;
+    uint32_t count = 0, tile_first, tile_end, tile_step;
+    if constexpr (Grouped) {
+        const uint32_t tiles = A.tile_prefix[A.groups];
+        const uint32_t per = (tiles + gridDim.x - 1) / gridDim.x;
+        tile_first = blockIdx.x * per;
+        tile_end = min(tiles, tile_first + per);
+        tile_step = 1;
+    } else {
+        count = Train ? A.count : *A.count_ptr;
+        tile_first = blockIdx.x;
+        tile_end = (count + kTile - 1) / kTile;
+        tile_step = gridDim.x;
+    }
     const uint32_t act_addr = tc::smem_addr(act);
     const uint32_t w_addr = tc::smem_addr(sm + kSmFwdW);
     uint32_t phase = 0;
     float loss_acc = 0.0f;
     bool ok = true;
-    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const uint32_t row = tile * kTile + t;
-        const bool valid = row < count;
+    uint32_t loaded = ~0u;
+    for (uint32_t tile = tile_first; tile < tile_end; tile += tile_step) {
+        uint32_t row;
+        bool valid;
+        if constexpr (Grouped) {
+            // the tile's group: the last g with tile_prefix[g] <= tile (empty groups are skipped)
+            uint32_t lo = 0, hi = A.groups - 1;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (A.tile_prefix[mid] <= tile) lo = mid; else hi = mid - 1;
+            }
+            if (lo != loaded) {
+                // the previous tile's chains have completed: the weight tiles are free
+                if (!ok && t == 0) atomicExch(V.error, 1);
+                ok = true;
+                V = A.nets[lo];
+                load_weights_fwd(sm, V);
+                loaded = lo;
+            }
+            const uint32_t local = (tile - A.tile_prefix[lo]) * kTile + t;
+            valid = local < A.group_count[lo];
+            row = A.group_base[lo] + local;
+        } else {
+            row = tile * kTile + t;
+            valid = row < count;
+        }
         float3 om = f3(0, 0, 0);
         float wgt = 0.0f;
         bool active = false;
@@ -334,7 +372,7 @@ __global__ void __launch_bounds__(kTile, 3) mlp_forward_kernel(FwdArgs A) {
                 if (Train) {
                     const uint32_t si = A.sel[row];
                     const float4 s0 = A.S.s0[si], s1 = A.S.s1[si], s2 = A.S.s2[si], s3 = A.S.s3[si];
-                    encode(A.V, xyz(s0), xyz(s2), xyz(s3), f);
+                    encode(V, xyz(s0), xyz(s2), xyz(s3), f);
                     om = xyz(s1);
                     wgt = float(double(fminf(s0.w, float(A.wnorm[0]))) * A.wnorm[1]);
                     active = true;
@@ -342,7 +380,7 @@ __global__ void __launch_bounds__(kTile, 3) mlp_forward_kernel(FwdArgs A) {
                     const float4 a = A.surf[size_t(row) * 3], b = A.surf[size_t(row) * 3 + 1],
                                  c = A.surf[size_t(row) * 3 + 2];
                     active = b.w > 0.0f;
-                    encode(A.V, xyz(a), xyz(b), xyz(c), f);
+                    encode(V, xyz(a), xyz(b), xyz(c), f);
                 }
             } else {
                 #pragma unroll
@@ -428,7 +466,7 @@ __global__ void __launch_bounds__(kTile, 3) mlp_forward_kernel(FwdArgs A) {
         }
         if (t == 0) A.loss_partial[blockIdx.x] = red[0];
     }
-    if (!ok && t == 0) atomicExch(A.V.error, 1);
+    if (!ok && t == 0 && V.error) atomicExch(V.error, 1);
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) {
@@ -783,7 +821,7 @@ rr_guide::~rr_guide() {
     delete mlp;
 }
 
-static MlpView mlp_view(rr_guide* g) {
+MlpView rr_mlp_guide_view(rr_guide* g) {
     MlpView V;
     V.w16 = g->mlp->w16;
     V.params = g->mlp->params;
@@ -822,7 +860,7 @@ rr_status rr_mlp_guide_init(rr_ctx* ctx, rr_guide* g) {
     if ((st = al(reinterpret_cast<void**>(&M.wpartial), size_t(M.wg_grid) * kParams * 4)) != RR_OK) return st;
     if ((st = al(reinterpret_cast<void**>(&M.wn_partial), size_t(kWnBlocks) * 8)) != RR_OK) return st;
     RR_TRY_CUDA(ctx, cudaMallocHost(&M.loss_host, size_t(M.grid) * 4));
-    for (auto k : {mlp_forward_kernel<true>, mlp_forward_kernel<false>})
+    for (auto k : {mlp_forward_kernel<true>, mlp_forward_kernel<false>, mlp_forward_kernel<false, true>})
         RR_TRY_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmFwd));
     RR_TRY_CUDA(ctx, cudaFuncSetAttribute(mlp_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmBwd));
     RR_TRY_CUDA(ctx, cudaFuncSetAttribute(mlp_wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmWg));
@@ -858,7 +896,7 @@ rr_status rr_mlp_guide_ensure(rr_ctx* ctx, rr_guide* g, size_t slots) {
 rr_status rr_mlp_guide_infer(rr_ctx* ctx, rr_guide* g, const uint32_t* count_dev, uint32_t max_count,
                              cudaStream_t stream) {
     FwdArgs A{};
-    A.V = mlp_view(g);
+    A.V = rr_mlp_guide_view(g);
     A.surf = g->mlp_surf;
     A.mix = g->mlp_mix;
     A.count_ptr = count_dev;
@@ -870,11 +908,46 @@ rr_status rr_mlp_guide_infer(rr_ctx* ctx, rr_guide* g, const uint32_t* count_dev
     return RR_OK;
 }
 
+namespace rr {
+namespace {
+// Per group: its first inference tile (one thread; groups are the scenes of
+// one batch).
+__global__ void group_tiles_kernel(const uint32_t* __restrict__ group_count, uint32_t groups,
+                                   uint32_t* __restrict__ tile_prefix) {
+    uint32_t acc = 0;
+    for (uint32_t g = 0; g < groups; ++g) {
+        tile_prefix[g] = acc;
+        acc += (group_count[g] + kTile - 1) / kTile;
+    }
+    tile_prefix[groups] = acc;
+}
+} // namespace
+} // namespace rr
+
+rr_status rr_mlp_guide_infer_grouped(rr_ctx* ctx, const MlpView* nets, uint32_t groups, const float4* surf,
+                                     float4* mix, const uint32_t* group_base, const uint32_t* group_count,
+                                     uint32_t* tile_prefix, cudaStream_t stream) {
+    if (groups == 0) return RR_OK;
+    group_tiles_kernel<<<1, 1, 0, stream>>>(group_count, groups, tile_prefix);
+    RR_CHECK_LAUNCH(ctx);
+    FwdArgs A{};
+    A.surf = surf;
+    A.mix = mix;
+    A.nets = nets;
+    A.groups = groups;
+    A.group_base = group_base;
+    A.group_count = group_count;
+    A.tile_prefix = tile_prefix;
+    mlp_forward_kernel<false, true><<<3 * ctx->sm_count, kTile, kSmFwd, stream>>>(A);
+    RR_CHECK_LAUNCH(ctx);
+    return RR_OK;
+}
+
 // Runs the network on caller-provided surfaces (rr_guide_eval for MLP guides).
 rr_status rr_mlp_guide_eval(rr_ctx* ctx, rr_guide* g, const float4* surf, float4* mix, const uint32_t* count_dev,
                             uint32_t count, cudaStream_t stream) {
     FwdArgs A{};
-    A.V = mlp_view(g);
+    A.V = rr_mlp_guide_view(g);
     A.surf = surf;
     A.mix = mix;
     A.count_ptr = count_dev;
@@ -898,7 +971,7 @@ rr_status rr_mlp_guide_train(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t 
     mlp_wfinish_kernel<<<1, 1, 0, stream>>>(M.wn_partial, kWnBlocks, B, true, M.wnorm);
     RR_CHECK_LAUNCH(ctx);
     FwdArgs A{};
-    A.V = mlp_view(g);
+    A.V = rr_mlp_guide_view(g);
     A.count = B;
     A.S = g->samples;
     A.sel = M.sel;

@@ -15,6 +15,7 @@
 // reference's `radiance +=` statements, which keeps results bit-identical.
 
 #include "rr_wavefront.cuh"
+#include "rr_batch.h"
 
 #include <cstring>
 
@@ -327,28 +328,6 @@ extern "C" rr_status rr_pathtracer_tune(rr_ctx* ctx, const rr_scene* scene, cons
 }
 
 // ── batches of scenes ──────────────────────────────────────────────────────
-struct rr_batch {
-    rr_ctx* ctx = nullptr;
-    std::vector<const rr_scene*> scenes;
-    rr::DevScene* d_table = nullptr;       // per scene, uploaded once
-    unsigned char* d_call = nullptr;       // per call: BatchEntry[count], then float4*[count]
-    unsigned char* h_call[2] = {nullptr, nullptr};  // pinned staging of d_call, alternating
-    cudaEvent_t staged[2] = {nullptr, nullptr};     // the copy out of h_call[k] has completed
-    int slot = 0;
-    size_t entries_bytes = 0, call_bytes = 0;
-    cudaStream_t cap_stream = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    struct Key {
-        uint64_t paths = 0;
-        uint32_t total_tiles = 0, max_bounces = 0, ev = 0, sv = 0;
-        const void* queue = nullptr;
-        bool operator!=(const Key& o) const {
-            return paths != o.paths || total_tiles != o.total_tiles || max_bounces != o.max_bounces || ev != o.ev ||
-                   sv != o.sv || queue != o.queue;
-        }
-    } key;
-};
-
 namespace {
 
 // Enqueues one batch frame: counter reset, raygen over every scene's tiles,
@@ -416,6 +395,7 @@ rr_status enqueue_batch(rr_ctx* ctx, rr_batch* B, uint32_t total_tiles, size_t n
 extern "C" rr_status rr_batch_destroy(rr_batch* B) {
     if (!B) return RR_ERR_INVALID_ARGUMENT;
     if (B->ctx) cudaSetDevice(B->ctx->device);
+    rr_batch_free_guided(B);
     if (B->exec) cudaGraphExecDestroy(B->exec);
     if (B->cap_stream) cudaStreamDestroy(B->cap_stream);
     for (int k = 0; k < 2; ++k) {
@@ -460,20 +440,11 @@ extern "C" rr_status rr_batch_create(rr_ctx* ctx, const rr_scene* const* scenes,
     return RR_OK;
 }
 
-extern "C" rr_status rr_batch_execute(rr_ctx* ctx, rr_batch* B, const GpuCameraData* cams, const rr_pt_params* p,
-                                      float* const* radiance_out, void* stream_v) {
+rr_status rr_batch_stage_call(rr_ctx* ctx, rr_batch* B, const GpuCameraData* cams, const rr_pt_params* p,
+                              float* const* radiance_out, cudaStream_t stream, uint32_t* tiles_out,
+                              uint64_t* paths_out) {
     using namespace rr;
-    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
-    if (!B || !cams || !p || !radiance_out) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute: null argument");
-    if (B->ctx != ctx) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute: batch of another context");
-    if (p->spp == 0 || p->max_bounces > uint32_t(kMaxBounces))
-        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute: bad spp or max_bounces");
-    const bool graph = (p->flags & RR_PT_FLAG_GRAPH) != 0;
-    if (graph && (p->flags & (RR_PT_FLAG_COUNT_TRAVERSAL | RR_PT_FLAG_TIME_STAGES)))
-        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute: counting and timing flags need non-graph runs");
     const uint32_t count = uint32_t(B->scenes.size());
-    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
-    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
     // per-call table into this call's staging slot (the copy out of it two calls ago has completed)
     const int k = B->slot;
     RR_TRY_CUDA(ctx, cudaEventSynchronize(B->staged[k]));
@@ -508,6 +479,28 @@ extern "C" rr_status rr_batch_execute(rr_ctx* ctx, rr_batch* B, const GpuCameraD
     RR_TRY_CUDA(ctx, cudaMemcpyAsync(B->d_call, B->h_call[k], B->call_bytes, cudaMemcpyHostToDevice, stream));
     RR_TRY_CUDA(ctx, cudaEventRecord(B->staged[k], stream));
     B->slot ^= 1;
+    *tiles_out = tiles;
+    *paths_out = paths;
+    return RR_OK;
+}
+
+extern "C" rr_status rr_batch_execute(rr_ctx* ctx, rr_batch* B, const GpuCameraData* cams, const rr_pt_params* p,
+                                      float* const* radiance_out, void* stream_v) {
+    using namespace rr;
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    if (!B || !cams || !p || !radiance_out) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute: null argument");
+    if (B->ctx != ctx) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute: batch of another context");
+    if (p->spp == 0 || p->max_bounces > uint32_t(kMaxBounces))
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute: bad spp or max_bounces");
+    const bool graph = (p->flags & RR_PT_FLAG_GRAPH) != 0;
+    if (graph && (p->flags & (RR_PT_FLAG_COUNT_TRAVERSAL | RR_PT_FLAG_TIME_STAGES)))
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute: counting and timing flags need non-graph runs");
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    uint32_t tiles = 0;
+    uint64_t paths = 0;
+    rr_status st = rr_batch_stage_call(ctx, B, cams, p, radiance_out, stream, &tiles, &paths);
+    if (st != RR_OK) return st;
     if (graph) {
         rr_batch::Key key;
         key.paths = paths; key.total_tiles = tiles; key.max_bounces = p->max_bounces;

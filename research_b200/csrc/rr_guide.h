@@ -3,6 +3,8 @@
 
 #include "rr_internal.h"
 
+#include <cuda_bf16.h>
+
 namespace rr {
 
 // Dense grid of vMF mixtures: cells = res^3 over [bmin, bmin + res/scale].
@@ -37,6 +39,27 @@ struct GuideSamples {
     uint32_t capacity = 0;
 };
 
+// One MLP guide's network as its kernels read it: BF16 weights, FP32 master
+// parameters (the forward takes the biases from them), the bounds of the
+// position encoding and the guide's error flag (set when a tensor-core wait
+// gave up).
+struct MlpView {
+    const __nv_bfloat16* w16;
+    const float* params;
+    float3 bmin, inv_ext;
+    int* error;
+};
+
+// One scene of a guided batch: its guide's grid (grid guides), vertex
+// records and training samples, its paths per bounce and alpha.
+struct GuideEntry {
+    GridView grid;
+    float4* rec[4];
+    GuideSamples S;
+    uint32_t paths;
+    float alpha;
+};
+
 } // namespace rr
 
 struct rr_mlp_state;
@@ -46,6 +69,7 @@ struct rr_guide {
     rr_guide_desc desc{};
     std::vector<void*> allocations;
     rr::GuideSamples samples;
+    uint32_t* count_host = nullptr;   // pinned: the sample count read back by an update
     float4* rec[4] = {nullptr, nullptr, nullptr, nullptr};
     size_t rec_capacity = 0;
     uint32_t frame_paths = 0;
@@ -87,5 +111,13 @@ rr_status rr_mlp_guide_infer(rr_ctx* ctx, rr_guide* g, const uint32_t* count_dev
                              cudaStream_t stream);
 rr_status rr_mlp_guide_train(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t stream);
 double rr_mlp_guide_last_loss(rr_guide* g);
+rr::MlpView rr_mlp_guide_view(rr_guide* g);
+// Grouped inference over the scenes of a guided batch: group g's queries
+// are surf/mix slots [group_base[g], group_base[g] + group_count[g]) and run
+// through network nets[g] (device array); tile_prefix (groups + 1 words) is
+// scratch for the per-group tile ranges. All counts are read on the device.
+rr_status rr_mlp_guide_infer_grouped(rr_ctx* ctx, const rr::MlpView* nets, uint32_t groups, const float4* surf,
+                                     float4* mix, const uint32_t* group_base, const uint32_t* group_count,
+                                     uint32_t* tile_prefix, cudaStream_t stream);
 rr_status rr_mlp_guide_eval(rr_ctx* ctx, rr_guide* g, const float4* surf, float4* mix, const uint32_t* count_dev,
                             uint32_t count, cudaStream_t stream);

@@ -229,6 +229,9 @@ _SIGNATURES = {
     "rr_guide_destroy": (I, [P]),
     "rr_guide_reset": (I, [P, P, P]),
     "rr_guide_update": (I, [P, P, P]),
+    "rr_guides_update": (I, [P, C.POINTER(P), U32, P]),
+    "rr_batch_execute_guided": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtParams), C.POINTER(P), C.POINTER(P),
+                                    P]),
     "rr_guide_get_stats": (I, [P, P, C.POINTER(GuideStats)]),
     "rr_guide_eval": (I, [P, P, P, U32, P, P]),
     "rr_guide_set_samples": (I, [P, P, P, U32, P]),
@@ -439,6 +442,14 @@ class Batch:
         cams = (GpuCameraData * len(cameras))(*cameras)
         outs = (P * len(outputs))(*outputs)
         self.ctx.check(lib().rr_batch_execute(self.ctx.handle, self._h, cams, C.byref(params), outs, stream))
+
+    def execute_guided(self, cameras, params, guides, outputs, stream):
+        """rr_batch_execute_guided: guides[i] (rr_guide handles) guides scene i."""
+        cams = (GpuCameraData * len(cameras))(*cameras)
+        gs = (P * len(guides))(*guides)
+        outs = (P * len(outputs))(*outputs)
+        self.ctx.check(lib().rr_batch_execute_guided(self.ctx.handle, self._h, cams, C.byref(params), gs, outs,
+                                                     stream))
 
     def tune(self, cameras, params, outputs, stream) -> "PtTuneResult":
         cams = (GpuCameraData * len(cameras))(*cameras)
