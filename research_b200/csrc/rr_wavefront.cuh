@@ -343,6 +343,9 @@ using BatchQueueKernel = void (*)(const DevScene*, const float4*, const float4*,
                                   const uint32_t*, uint32_t*, unsigned long long*);
 using BatchShadowKernel = void (*)(const DevScene*, float4* const*, const float4*, const float4*, const float4*,
                                    const uint32_t*, uint32_t*, unsigned long long*);
+// Variant 0 of the batch extend kernel asks for 4 blocks per SM: left free,
+// the per-ray scene binding takes it to 68 registers (3 blocks of 256 per
+// SM), where the single-scene kernel settles at 64 (4 blocks).
 template <bool Count>
 BatchQueueKernel extend_batch_variant(int v) {
     switch (v) {
@@ -351,7 +354,7 @@ BatchQueueKernel extend_batch_variant(int v) {
     case 3: return extend_batch_kernel<Count, true, 1>;
     case 4: return extend_batch_kernel<Count, true, 4>;
     case 5: return extend_batch_kernel<Count, true, 6>;
-    default: return extend_batch_kernel<Count, false, 1>;
+    default: return extend_batch_kernel<Count, false, 4>;
     }
 }
 template <bool Count>
