@@ -229,6 +229,13 @@ extern "C" rr_status rr_pathtracer_execute(rr_ctx* ctx, const rr_scene* scene,
     const DevScene& S = scene->dev;
     float4* out = reinterpret_cast<float4*>(radiance_out);
     rr_stage_timer timer(ctx, stream, timed);
+    // Bounce b's shadow rays only add to the image and read the shadow queue;
+    // bounce b+1's extension rays only read the ray queue and write hits. So
+    // the shadow launch runs on the side stream next to the next extend
+    // launch, and the next shade launch (which writes the image and the
+    // shadow queue) waits for it. Stage timing keeps one stream.
+    const bool overlap = ctx->overlap_shadow && !timed;
+    if (overlap && (st = ensure_side(ctx)) != RR_OK) return st;
     for (uint32_t b = 0; b < p->max_bounces; ++b) {
         const int cur = b & 1, nxt = cur ^ 1;
         uint32_t* cb = C + 4 * b;
@@ -237,6 +244,7 @@ extern "C" rr_status rr_pathtracer_execute(rr_ctx* ctx, const rr_scene* scene,
         ext_k<<<g_ext, kBlock, 0, stream>>>(S, q.ray_a[cur], q.ray_b[cur], q.hits, cb, cb + 1, ctx->work64);
         RR_CHECK_LAUNCH(ctx);
         timer.end(1);
+        if (overlap && b > 0) RR_TRY_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->shadowed[b - 1], 0));
         timer.begin(2);
         shade_kernel<false><<<g_shade, kBlock, 0, stream>>>(S, nullptr, nullptr, b, b + 1 == p->max_bounces ? 1u : 0u,
                                                      q.ray_a[cur], q.ray_b[cur], q.ray_c[cur], q.hits,
@@ -245,12 +253,21 @@ extern "C" rr_status rr_pathtracer_execute(rr_ctx* ctx, const rr_scene* scene,
                                                      cb, cn, cb + 2);
         RR_CHECK_LAUNCH(ctx);
         timer.end(2);
+        cudaStream_t sh_stream = stream;
+        if (overlap) {
+            RR_TRY_CUDA(ctx, cudaEventRecord(ctx->shaded[b], stream));
+            RR_TRY_CUDA(ctx, cudaStreamWaitEvent(ctx->side, ctx->shaded[b], 0));
+            sh_stream = ctx->side;
+        }
         timer.begin(3);
-        sh_k<<<g_sh, kBlock, 0, stream>>>(S, q.shadow_a, q.shadow_b, q.shadow_c, out, cb + 2, cb + 3,
-                                          ctx->work64 + 2);
+        sh_k<<<g_sh, kBlock, 0, sh_stream>>>(S, q.shadow_a, q.shadow_b, q.shadow_c, out, cb + 2, cb + 3,
+                                             ctx->work64 + 2);
         RR_CHECK_LAUNCH(ctx);
         timer.end(3);
+        if (overlap) RR_TRY_CUDA(ctx, cudaEventRecord(ctx->shadowed[b], ctx->side));
     }
+    if (overlap && p->max_bounces > 0)
+        RR_TRY_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->shadowed[p->max_bounces - 1], 0));
     ctx->launches += 1 + 3 * uint64_t(p->max_bounces);
     ctx->last_max_bounces = p->max_bounces;
     ctx->last_counted = count;
@@ -283,6 +300,12 @@ extern "C" rr_status rr_pathtracer_stats(rr_ctx* ctx, rr_pt_stats* out, int rese
     if (reset) {
         for (int k = 0; k < 4; ++k) { ctx->stage_ms[k] = 0.0; ctx->stage_launches[k] = 0; }
     }
+    return RR_OK;
+}
+
+extern "C" rr_status rr_pathtracer_set_overlap(rr_ctx* ctx, int enable) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    ctx->overlap_shadow = enable != 0;
     return RR_OK;
 }
 

@@ -58,6 +58,13 @@ struct rr_ctx {
     double* mse_partial = nullptr;         // rr_image_mse block partials
     float4* atrous_nrm = nullptr;          // A-trous: the G-buffer normals, normalized once per call
     size_t atrous_nrm_px = 0;
+    // The path tracer traces bounce b's shadow rays on a second stream while
+    // bounce b+1's extension rays run on the caller's (fork after shade b,
+    // join before shade b+1); created on first use.
+    bool overlap_shadow = true;
+    cudaStream_t side = nullptr;
+    cudaEvent_t shaded[kMaxBounces] = {};
+    cudaEvent_t shadowed[kMaxBounces] = {};
 };
 
 // Records a CUDA event pair around stage launches on the caller's stream;

@@ -403,6 +403,17 @@ int persistent_grid(const rr_ctx* ctx, const void* kernel) {
     return ctx->sm_count * (per_sm > 0 ? per_sm : 1);
 }
 
+// The second stream and the fork/join events of the shadow overlap.
+rr_status ensure_side(rr_ctx* ctx) {
+    if (ctx->side) return RR_OK;
+    for (int b = 0; b < kMaxBounces; ++b) {
+        RR_TRY_CUDA(ctx, cudaEventCreateWithFlags(&ctx->shaded[b], cudaEventDisableTiming));
+        RR_TRY_CUDA(ctx, cudaEventCreateWithFlags(&ctx->shadowed[b], cudaEventDisableTiming));
+    }
+    RR_TRY_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+    return RR_OK;
+}
+
 rr_status ensure_queues(rr_ctx* ctx, size_t n) {
     rr_pt_queues& q = ctx->pt;
     if (q.capacity >= n) return RR_OK;

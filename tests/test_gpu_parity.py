@@ -358,6 +358,38 @@ def test_traversal_variants_identical_and_tuner(rr, O, ctx, torch_cuda, procedur
     ctx.check(rr.lib().rr_pathtracer_set_variants(ctx.handle, 0, 0))
 
 
+def test_shadow_overlap_is_bit_identical(rr, O, ctx, torch_cuda, procedural):
+    """Bounce b's shadow rays on the context's second stream next to bounce
+    b+1's extension rays (the default) render the same bits as one stream, as
+    the stage-timed form, and as the oracle; repeated frames at a size where
+    the two launches do overlap."""
+    torch = torch_cuda
+    _, scene, oscene = procedural
+    L = rr.lib()
+    cam = cam_for(rr, "procedural", 80, 48)
+    ref, _ = O.pathtrace(oscene, cam, 21, 6, 1)
+    ctx.check(L.rr_pathtracer_set_overlap(ctx.handle, 1))
+    g = gpu_pathtrace(rr, ctx, scene, cam, torch, 21, 6, 1)
+    np.testing.assert_array_equal(g.view(np.uint32), ref.view(np.uint32))
+    big = cam_for(rr, "procedural", 640, 360)
+    outs = {}
+    for name, overlap, flags in (("overlap", 1, 0), ("serial", 0, 0), ("timed", 1, rr.PT_FLAG_TIME_STAGES)):
+        ctx.check(L.rr_pathtracer_set_overlap(ctx.handle, overlap))
+        frames = []
+        for f in range(3):
+            out = torch.empty((4, 360, 640, 4), device="cuda")
+            p = rr.PtParams(100 + 4 * f, 6, 4, flags)
+            ctx.check(L.rr_pathtracer_execute(ctx.handle, scene.handle, C.byref(big), C.byref(p), out.data_ptr(),
+                                              _stream(torch)))
+            frames.append(out)
+        torch.cuda.synchronize()
+        outs[name] = np.stack([_np(o) for o in frames])
+    ctx.check(L.rr_pathtracer_set_overlap(ctx.handle, 1))
+    assert np.isfinite(outs["serial"]).all() and outs["serial"][..., :3].mean() > 0
+    for name in ("overlap", "timed"):
+        np.testing.assert_array_equal(outs[name].view(np.uint32), outs["serial"].view(np.uint32), err_msg=name)
+
+
 def _edge_scenes(rr):
     """Cornell variants: a directional plus a point light (the MIS branch of
     the light sample and of ReSTIR DI's target), no lights at all, and all
