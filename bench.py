@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--triangles", type=int, default=CFG["triangles"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
+    ap.add_argument("--serial-passes", action="store_true",
+                    help="run ReSTIR DI and A-trous after the path tracer on one stream")
     return ap.parse_args()
 
 
@@ -226,6 +228,8 @@ def config_dict(args):
             "restir_di": {"candidates": CFG["di_candidates"], "m_cap": CFG["m_cap_factor"] * CFG["di_candidates"],
                           "neighbors": CFG["di_neighbors"], "radius_px": CFG["di_radius"]},
             "atrous_iterations": CFG["atrous_iterations"], "parallelism": f"replicas{args.gpus}",
+            "pass_schedule": ("one stream" if args.serial_passes else
+                              "ReSTIR DI + A-trous on a second stream beside path tracer + accumulate"),
             "l2": "per-step working set (ray queues + images) > 126 MB L2; no explicit flush"}
 
 
@@ -249,6 +253,13 @@ class Frame:
         self.desc = rr.camera_desc(W, H, eye=CFG["eye"], center=CFG["center"])
         self.cam = rr.camera_data(self.desc)
         self.stage_events = []
+        # ReSTIR DI and A-trous do not read the path tracer's or the
+        # accumulation's buffers (nor they theirs): with `concurrent`, they run
+        # on a second stream that forks from the frame's stream at the start
+        # of the step and joins it at the end
+        self.concurrent = False
+        self.di_stream = torch.cuda.Stream()
+        self.fork, self.join = torch.cuda.Event(), torch.cuda.Event()
 
     def step(self, stream, pt_flags=0, seed_base=0, stage_timing=False):
         rr, L, ctx = self.rr, self.L, self.ctx
@@ -256,6 +267,13 @@ class Frame:
         ev = []
         mark = (lambda: ev.append(self.torch.cuda.Event(enable_timing=True))) if stage_timing else (lambda: None)
         rec = (lambda: ev[-1].record()) if stage_timing else (lambda: None)
+        fork = self.concurrent and not stage_timing
+        di_st = stream
+        if fork:
+            main = self.torch.cuda.current_stream()
+            self.fork.record(main)
+            self.di_stream.wait_event(self.fork)
+            di_st = self.di_stream.cuda_stream
         mark(); rec()
         p = rr.PtParams(seed_base + self.frame * CFG["spp"], CFG["max_bounces"], CFG["spp"], pt_flags)
         ctx.check(L.rr_pathtracer_execute(ctx.handle, self.scene.handle, C.byref(cam), C.byref(p),
@@ -271,12 +289,15 @@ class Frame:
         cur, prev = self.res[self.frame & 1], self.res[(self.frame & 1) ^ 1]
         ctx.check(L.rr_restir_di_execute(ctx.handle, self.scene.handle, C.byref(cam), C.byref(dp),
                                          self.gpos.data_ptr(), self.gnrm.data_ptr(), cur.data_ptr(), prev.data_ptr(),
-                                         self.out.data_ptr(), stream))
+                                         self.out.data_ptr(), di_st))
         mark(); rec()
         atp = rr.AtrousParams(self.W, self.H, CFG["atrous_iterations"], 0, 0.25, 0.20, 1.0, 0)
         ctx.check(L.rr_atrous_execute(ctx.handle, self.out.data_ptr(), self.gpos.data_ptr(), self.gnrm.data_ptr(),
                                       self.ping[0].data_ptr(), self.ping[1].data_ptr(), C.byref(atp),
-                                      C.byref(self.slot), stream))
+                                      C.byref(self.slot), di_st))
+        if fork:
+            self.join.record(self.di_stream)
+            main.wait_event(self.join)
         mark(); rec()
         if stage_timing:
             self.stage_events.append(ev)
@@ -307,6 +328,7 @@ def run_ours(args, ws, rank, local):
     W, H = args.width, args.height
     stream = torch.cuda.current_stream().cuda_stream
     fr = Frame(rr, torch, ctx, scene, W, H)
+    fr.concurrent = not args.serial_passes
     from research_b200 import replicas
     seed_base = replicas.seed_base(rank)
     replicas.check_seed_budget((args.warmup + 3 * args.steps + 8) * CFG["spp"])
