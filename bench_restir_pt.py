@@ -27,6 +27,8 @@ def main():
     ap.add_argument("--frames", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--triangles", type=int, default=1_000_000)
+    ap.add_argument("--initial", choices=["wavefront", "per_pixel"], default="wavefront",
+                    help="form of the initial pass (rr_restir_pt_set_wavefront)")
     args = ap.parse_args()
 
     import torch
@@ -34,6 +36,7 @@ def main():
     torch.cuda.set_device(0)
     L = rr.lib()
     ctx = rr.Context(0)
+    ctx.check(rr.lib().rr_restir_pt_set_wavefront(ctx.handle, 1 if args.initial == "wavefront" else 0))
     hs = rr.HostScene.procedural(target_triangles=args.triangles)
     scene = rr.Scene(ctx, hs.arrays)
     W, H = args.width, args.height
@@ -92,7 +95,8 @@ def main():
             "stages_ms": ms, "frames": args.frames, "warmup": args.warmup,
             "mpixels_per_s": round(W * H / frame_ms / 1e3, 2),
             "config": {"workload": f"procedural-room-1M-tris, {W}x{H}", "candidates": 8, "max_bounces": 4,
-                       "spatial_neighbors": 4, "spatial_radius": 12, "guiding_cells": cells, "di_candidates": 32},
+                       "spatial_neighbors": 4, "spatial_radius": 12, "guiding_cells": cells, "di_candidates": 32,
+                       "initial": args.initial},
             "output_mean": float(o.mean()), "output_finite": bool(torch.isfinite(o).all())}
     print(json.dumps(line), flush=True)
     scene.close()

@@ -357,10 +357,18 @@ typedef struct rr_restir_pt_images {
     float*       guiding_fitted;  /* guiding.cell_count x float x 4 */
 } rr_restir_pt_images;
 
-/* cs_initial (restir_pt.slang:567-757). */
+/* cs_initial (restir_pt.slang:567-757). By default run as a wavefront: the
+ * per-pixel candidate loop is cut at every ray, each pixel's state kept in
+ * device memory, and every step traces one path segment (and its light
+ * sample's shadow ray) of every pixel that has one, through the queue
+ * traversal kernels; the results are those of one thread per pixel running
+ * the loop, bit for bit. */
 rr_status rr_restir_pt_initial(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
                                const rr_restir_pt_params* params, const rr_restir_pt_images* images,
                                void* stream);
+/* 1 (default): rr_restir_pt_initial runs as the wavefront; 0: one thread per
+ * pixel runs the whole candidate loop. */
+rr_status rr_restir_pt_set_wavefront(rr_ctx* ctx, int enable);
 /* cs_temporal (restir_pt.slang:760-857); returns at once when temporal_enable is 0. */
 rr_status rr_restir_pt_temporal(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
                                 const rr_restir_pt_params* params, const rr_restir_pt_images* images,

@@ -16,6 +16,7 @@
 
 #include "rr_grid.cuh"
 #include "rr_reuse.cuh"
+#include "rr_wavefront.cuh"
 
 namespace rr {
 namespace {
@@ -179,6 +180,347 @@ __global__ void __launch_bounds__(128, 8) ptr_initial_kernel(DevScene s, PtrLaun
         }
     }
     store_empty(I.rc, i);
+}
+
+// ── wavefront form of cs_initial ───────────────────────────────────────────
+// The same per-pixel computation as ptr_initial_kernel, cut at every ray.
+// Each pixel keeps its state in HBM (random-number seed, candidate index,
+// segment index, M, w_sum, source pdf, path throughput, suffix radiance, the
+// candidate's reconnection vertex, the selected candidate); each step
+// advances every pixel with work by one path segment:
+//   extend  : closest hit of the step's segment rays (queue traversal)
+//   shade   : the reconnection vertex or a bounce vertex as the inline loop
+//             handles it: sky on a miss, the light sample (its shadow ray is
+//             queued with the contribution it adds if the light is visible),
+//             then the next BSDF direction, or the candidate ends
+//   shadow  : any-hit traversal of the step's shadow rays; each adds its
+//             contribution (or zero) to its pixel's suffix
+//   advance : for every candidate that ended, the resampling step, then the
+//             next candidates' first directions (ray into the next step's
+//             queue) or, after the last one, the reservoir
+// Random numbers are drawn in the inline order (light pick, BSDF pair,
+// resampling, next candidate), and the suffix receives the same additions
+// in the same order: a light sample's contribution lands in the step's
+// shadow stage, before the vertex after it is shaded. Each pixel has at most
+// one segment ray and one shadow ray per step, so a pixel takes at most
+// num_candidates x max(max_bounces, 1) steps.
+constexpr int kWaveWords = 8;   // per step: rays, ray cursor, shadow rays, shadow cursor, ended candidates
+constexpr uint32_t kRis = 0x80000000u;
+
+struct PtrWave {
+    uint4* st;          // (seed, candidate, segment, M)
+    float4* acc;        // (w_sum, source pdf, -, -)
+    float4* thp;        // path throughput after the segment's vertex
+    float4* suf;        // suffix radiance
+    float4* rcp;        // the candidate's reconnection vertex
+    float4* rcn;        // and its normal
+    float4* selp;       // selected candidate: rc_pos, valid
+    float4* seln;       // rc_normal
+    float4* sels;       // suffix radiance
+    float4* qa[2];      // segment rays: (origin, pixel)
+    float4* qb[2];      // (direction, -)
+    float4* hits;
+    float4* sa;         // shadow rays: (origin, pixel)
+    float4* sb;         // (direction, t_max)
+    float4* sc;         // (contribution, -)
+    uint32_t* ended;    // pixel | kRis (the candidate enters resampling)
+    uint32_t* cnt;      // kWaveWords per step
+    uint32_t n;
+};
+
+// The pixel's next candidates from candidate c on: sample_primary_dir until
+// one gives a usable direction (the ones that do not are skipped, as the
+// inline loop's `continue`). Returns false after the last candidate.
+RR_D bool wave_next(const PtrLaunch& L, const PtrImages& I, float3 pp, float3 pn, uint32_t pmat, uint32_t& seed,
+                    uint32_t& c, float& src_pdf, float3& o, float3& d) {
+    for (; c < L.num_candidates; ++c) {
+        const float3 wi0 = sample_primary_dir(I.fitted, pp, pn, pmat, L.grid, seed, src_pdf);
+        if (src_pdf <= 1e-6f || dot(pn, wi0) <= 0.0f) continue;
+        o = pp + pn * L.ray_bias;
+        d = wi0;
+        return true;
+    }
+    return false;
+}
+
+// The end of ptr_initial_kernel: the selected candidate's reservoir or an empty one.
+RR_D void wave_finish(const PtrLaunch& L, const PtrImages& I, const PtrWave& V, size_t i, float3 pp, float3 pn,
+                      const Mat& pm, uint32_t M_count, float w_sum) {
+    const float4 sp = V.selp[i];
+    if (M_count > 0 && sp.w > 0.5f) {
+        Reservoir sel;
+        sel.rc_pos = xyz(sp); sel.rc_normal = xyz(V.seln[i]); sel.suffix_rad = xyz(V.sels[i]);
+        sel.prefix_thp = f3(1.0f, 1.0f, 1.0f);
+        sel.valid = sp.w;
+        const float p_hat = target_function(pp, pn, pm, cam_pos(L.cam), sel);
+        if (p_hat > 1e-10f) {
+            sel.M = M_count;
+            sel.w_sum = w_sum;
+            sel.W = w_sum / (float(M_count) * p_hat);
+            store_reservoir(I.rc, i, sel);
+            return;
+        }
+    }
+    store_empty(I.rc, i);
+}
+
+__global__ void __launch_bounds__(kBlock) ptrw_begin_kernel(DevScene s, PtrLaunch L, PtrImages I, PtrWave V) {
+    const uint32_t W = L.cam.screen_width;
+    const uint32_t warp_first = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+    for (uint32_t base = warp_first; base < V.n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + lane_id();
+        bool emit = false;
+        float3 o = f3(0.0f, 0.0f, 0.0f), d = f3(0.0f, 0.0f, 0.0f);
+        if (i < V.n) {
+            const uint32_t x = i % W, y = i / W;
+            uint32_t seed = make_seed(x, y, L.frame_seed);
+            float4 p4, n4;
+            float3 pp, pn;
+            uint32_t pmat;
+            if (!load_surface(s, I.gpos, I.gnrm, i, p4, n4, pp, pn, pmat)) {
+                I.hc[0][i] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+                I.hc[1][i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                store_empty(I.rc, i);
+            } else {
+                I.hc[0][i] = p4;
+                I.hc[1][i] = n4;
+                V.selp[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                uint32_t c = 0;
+                float src_pdf = 0.0f;
+                emit = wave_next(L, I, pp, pn, pmat, seed, c, src_pdf, o, d);
+                if (emit) {
+                    V.st[i] = make_uint4(seed, c, 0u, 0u);
+                    V.acc[i] = make_float4(0.0f, src_pdf, 0.0f, 0.0f);
+                } else {
+                    store_empty(I.rc, i);   // no candidate: M = 0
+                }
+            }
+        }
+        const uint32_t slot = warp_alloc(emit, V.cnt);
+        if (emit) {
+            V.qa[0][slot] = make_float4(o.x, o.y, o.z, __uint_as_float(i));
+            V.qb[0][slot] = make_float4(d.x, d.y, d.z, 0.0f);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBlock, 4) ptrw_extend_kernel(DevScene s, PtrWave V, uint32_t step, float tmin) {
+    const int cur = step & 1;
+    uint32_t* c0 = V.cnt + size_t(step) * kWaveWords;
+    const float4* qa = V.qa[cur];
+    const float4* qb = V.qb[cur];
+    float4* hits = V.hits;
+    traverse_queue<false, false, false, false>(
+        s, nullptr, c0[0], c0 + 1, nullptr,
+        [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
+            r = make_ray(xyz(qa[i]), xyz(qb[i]));
+            tmax = 1e9f;
+            return 0u;
+        },
+        [&](uint32_t i, bool found, const HitRec& h) {
+            hits[i] = found ? make_float4(h.u, h.v, __uint_as_float(h.inst), __uint_as_float(h.prim))
+                            : make_float4(0.0f, 0.0f, __uint_as_float(kNoIndex), __uint_as_float(kNoIndex));
+        },
+        tmin);
+}
+
+__global__ void __launch_bounds__(kBlock, 4) ptrw_shade_kernel(DevScene s, PtrLaunch L, PtrWave V, uint32_t step) {
+    const int cur = step & 1, nxt = cur ^ 1;
+    uint32_t* c0 = V.cnt + size_t(step) * kWaveWords;
+    uint32_t* c1 = c0 + kWaveWords;
+    const uint32_t count = c0[0];
+    const uint32_t max_b = L.max_bounces > 1u ? L.max_bounces : 1u;
+    const float bias = L.ray_bias;
+    const uint32_t warp_first = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+    for (uint32_t base = warp_first; base < count; base += gridDim.x * blockDim.x) {
+        const uint32_t q = base + lane_id();
+        bool cont = false, shadow = false, ended = false, ris = false;
+        uint32_t pid = 0;
+        float3 no = f3(0.0f, 0.0f, 0.0f), nd = no, so = no, sd = no, sc = no;
+        float stmax = 0.0f;
+        if (q < count) {
+            const float4 a = V.qa[cur][q], b = V.qb[cur][q], h = V.hits[q];
+            pid = __float_as_uint(a.w);
+            const float3 wi = xyz(b);
+            uint4 st = V.st[pid];
+            uint32_t seed = st.x;
+            const uint32_t seg = st.z;
+            const uint32_t inst = __float_as_uint(h.z);
+            float3 suffix = f3(0.0f, 0.0f, 0.0f), thp = f3(1.0f, 1.0f, 1.0f);
+            float3 cur_pos = f3(0.0f, 0.0f, 0.0f), cur_n = cur_pos;
+            Mat cur_mat{};
+            bool vertex = false;
+            if (seg == 0) {
+                // the reconnection vertex: a miss drops the candidate
+                if (inst == kNoIndex) {
+                    ended = true;
+                } else {
+                    const Surface rc = hit_surface(s, inst, __float_as_uint(h.w), h.x, h.y);
+                    float3 rc_n = rc.normal;
+                    if (dot(rc_n, wi) > 0.0f) rc_n = -rc_n;
+                    const Mat rc_mat = load_mat(s, rc.material);
+                    suffix = rc_mat.emissive;
+                    const float3 rc_wo = -wi;
+                    float3 c;
+                    shadow = sample_light_ray(s, rc.pos, rc_n, rc_wo, rc_mat, bias, seed, so, sd, stmax, c);
+                    if (shadow) sc = c;
+                    else suffix = suffix + f3(0.0f, 0.0f, 0.0f);
+                    V.rcp[pid] = make_float4(rc.pos.x, rc.pos.y, rc.pos.z, 0.0f);
+                    V.rcn[pid] = make_float4(rc_n.x, rc_n.y, rc_n.z, 0.0f);
+                    cur_pos = rc.pos; cur_n = rc_n; cur_mat = rc_mat;
+                    vertex = true;
+                }
+            } else {
+                thp = xyz(V.thp[pid]);
+                suffix = xyz(V.suf[pid]);
+                if (inst == kNoIndex) {
+                    suffix = suffix + thp * sky_radiance(wi);
+                    ended = ris = true;
+                } else {
+                    const Surface hs = hit_surface(s, inst, __float_as_uint(h.w), h.x, h.y);
+                    float3 hn = hs.normal;
+                    if (dot(hn, wi) > 0.0f) hn = -hn;
+                    const Mat hm = load_mat(s, hs.material);
+                    const float3 hwo = -wi;
+                    float3 c;
+                    shadow = sample_light_ray(s, hs.pos, hn, hwo, hm, bias, seed, so, sd, stmax, c);
+                    if (shadow) sc = thp * c;
+                    else suffix = suffix + thp * f3(0.0f, 0.0f, 0.0f);
+                    cur_pos = hs.pos; cur_n = hn; cur_mat = hm;
+                    vertex = true;
+                }
+            }
+            uint32_t nseg = seg;
+            if (vertex) {
+                nseg = seg + 1;   // the bounce loop's next index
+                if (nseg >= max_b) {
+                    ended = ris = true;
+                } else {
+                    const float u0 = rand_float(seed);
+                    const float u1 = rand_float(seed);
+                    float3 nwi;
+                    float pdf;
+                    const float3 f = brdf_sample(-wi, cur_n, cur_mat.base, cur_mat.metallic, cur_mat.roughness, u0,
+                                                 u1, nwi, pdf);
+                    if (pdf <= 1e-6f || dot(cur_n, nwi) <= 0.0f) {
+                        ended = ris = true;
+                    } else {
+                        const float cos_at = mx(dot(cur_n, nwi), 0.0f);
+                        thp = thp * ((f * cos_at) / pdf);
+                        if (mx(thp.x, mx(thp.y, thp.z)) <= 0.0f) {
+                            ended = ris = true;
+                        } else {
+                            cont = true;
+                            no = cur_pos + cur_n * bias;
+                            nd = nwi;
+                        }
+                    }
+                }
+                V.thp[pid] = make_float4(thp.x, thp.y, thp.z, 0.0f);
+            }
+            if (vertex || seg > 0) V.suf[pid] = make_float4(suffix.x, suffix.y, suffix.z, 0.0f);
+            st.x = seed;
+            st.z = nseg;
+            V.st[pid] = st;
+        }
+        const uint32_t sslot = warp_alloc(shadow, c0 + 2);
+        if (shadow) {
+            V.sa[sslot] = make_float4(so.x, so.y, so.z, __uint_as_float(pid));
+            V.sb[sslot] = make_float4(sd.x, sd.y, sd.z, stmax);
+            V.sc[sslot] = make_float4(sc.x, sc.y, sc.z, 0.0f);
+        }
+        const uint32_t rslot = warp_alloc(cont, c1);
+        if (cont) {
+            V.qa[nxt][rslot] = make_float4(no.x, no.y, no.z, __uint_as_float(pid));
+            V.qb[nxt][rslot] = make_float4(nd.x, nd.y, nd.z, 0.0f);
+        }
+        const uint32_t eslot = warp_alloc(ended, c0 + 4);
+        if (ended) V.ended[eslot] = pid | (ris ? kRis : 0u);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock, 5) ptrw_shadow_kernel(DevScene s, PtrWave V, uint32_t step, float tmin) {
+    uint32_t* c0 = V.cnt + size_t(step) * kWaveWords;
+    const float4* sa = V.sa;
+    const float4* sb = V.sb;
+    const float4* sc = V.sc;
+    float4* suf = V.suf;
+    traverse_queue<true, false, false, false>(
+        s, nullptr, c0[2], c0 + 3, nullptr,
+        [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
+            const float4 b = sb[i];
+            r = make_ray(xyz(sa[i]), xyz(b));
+            tmax = b.w;
+            return 0u;
+        },
+        [&](uint32_t i, bool found, const HitRec&) {
+            const uint32_t pid = __float_as_uint(sa[i].w);
+            const float3 add = found ? f3(0.0f, 0.0f, 0.0f) : xyz(sc[i]);
+            const float3 v = xyz(suf[pid]) + add;
+            suf[pid] = make_float4(v.x, v.y, v.z, 0.0f);
+        },
+        tmin);
+}
+
+__global__ void __launch_bounds__(kBlock) ptrw_advance_kernel(DevScene s, PtrLaunch L, PtrImages I, PtrWave V,
+                                                              uint32_t step) {
+    const int nxt = (step & 1) ^ 1;
+    uint32_t* c0 = V.cnt + size_t(step) * kWaveWords;
+    uint32_t* c1 = c0 + kWaveWords;
+    const uint32_t count = c0[4];
+    const float3 cp = cam_pos(L.cam);
+    const uint32_t warp_first = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+    for (uint32_t base = warp_first; base < count; base += gridDim.x * blockDim.x) {
+        const uint32_t q = base + lane_id();
+        bool emit = false;
+        uint32_t pid = 0;
+        float3 o = f3(0.0f, 0.0f, 0.0f), d = o;
+        if (q < count) {
+            const uint32_t e = V.ended[q];
+            pid = e & ~kRis;
+            uint4 st = V.st[pid];
+            uint32_t seed = st.x, c = st.y, M_count = st.w;
+            const float4 acc = V.acc[pid];
+            float w_sum = acc.x;
+            float src_pdf = acc.y;
+            float4 p4, n4;
+            float3 pp, pn;
+            uint32_t pmat;
+            load_surface(s, I.gpos, I.gnrm, pid, p4, n4, pp, pn, pmat);
+            const Mat pm = load_mat(s, pmat);
+            if (e & kRis) {
+                Reservoir cand;
+                cand.rc_pos = xyz(V.rcp[pid]); cand.rc_normal = xyz(V.rcn[pid]); cand.suffix_rad = xyz(V.suf[pid]);
+                cand.prefix_thp = f3(1.0f, 1.0f, 1.0f);
+                cand.M = 1u; cand.W = 0.0f; cand.w_sum = 0.0f; cand.valid = 1.0f;
+                const float p_hat = target_function(pp, pn, pm, cp, cand);
+                const float3 delta = cand.rc_pos - pp;
+                if (!(p_hat <= 0.0f) && !(dot(delta, delta) <= 1e-8f)) {
+                    const float weight = p_hat / mx(src_pdf, 1e-6f);
+                    w_sum += weight;
+                    M_count++;
+                    if (w_sum > 0.0f && rand_float(seed) < weight / w_sum) {
+                        V.selp[pid] = make_float4(cand.rc_pos.x, cand.rc_pos.y, cand.rc_pos.z, 1.0f);
+                        V.seln[pid] = make_float4(cand.rc_normal.x, cand.rc_normal.y, cand.rc_normal.z, 0.0f);
+                        V.sels[pid] = make_float4(cand.suffix_rad.x, cand.suffix_rad.y, cand.suffix_rad.z, 0.0f);
+                    }
+                }
+            }
+            ++c;
+            emit = wave_next(L, I, pp, pn, pmat, seed, c, src_pdf, o, d);
+            if (emit) {
+                V.st[pid] = make_uint4(seed, c, 0u, M_count);
+                V.acc[pid] = make_float4(w_sum, src_pdf, 0.0f, 0.0f);
+            } else {
+                wave_finish(L, I, V, pid, pp, pn, pm, M_count, w_sum);
+            }
+        }
+        const uint32_t slot = warp_alloc(emit, c1);
+        if (emit) {
+            V.qa[nxt][slot] = make_float4(o.x, o.y, o.z, __uint_as_float(pid));
+            V.qb[nxt][slot] = make_float4(d.x, d.y, d.z, 0.0f);
+        }
+    }
 }
 
 // cs_temporal (restir_pt.slang:760-857)
@@ -366,10 +708,85 @@ rr_status check(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* cam, co
     return RR_OK;
 }
 
+constexpr int kWaveArrays = 9;   // st, acc, thp, suf, rcp, rcn, selp, seln, sels
+
+// cs_initial as the wavefront of steps above: one launch to start every
+// pixel, then per step extend, shade, shadow and advance.
+rr_status ptr_initial_wavefront(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* cam,
+                                const rr_restir_pt_params* p, const rr_restir_pt_images* b, cudaStream_t stream) {
+    const size_t n = size_t(cam->screen_width) * cam->screen_height;
+    rr_status st = ensure_queues(ctx, n);
+    if (st != RR_OK) return st;
+    if (ctx->ptr_state_px < n) {
+        cudaFree(ctx->ptr_state);
+        ctx->ptr_state = nullptr;
+        ctx->ptr_state_px = 0;
+        RR_TRY_CUDA(ctx, cudaMalloc(&ctx->ptr_state, n * kWaveArrays * sizeof(float4)));
+        ctx->ptr_state_px = n;
+    }
+    const uint32_t max_b = std::max(p->max_bounces, 1u);
+    const uint64_t steps64 = uint64_t(p->num_initial_candidates) * max_b;
+    if (steps64 > (1u << 20)) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "ReSTIR PT: too many candidates x bounces");
+    const uint32_t steps = uint32_t(steps64);
+    const size_t words = size_t(steps + 1) * kWaveWords;
+    if (ctx->ptr_counter_words < words) {
+        cudaFree(ctx->ptr_counters);
+        ctx->ptr_counters = nullptr;
+        ctx->ptr_counter_words = 0;
+        RR_TRY_CUDA(ctx, cudaMalloc(&ctx->ptr_counters, words * sizeof(uint32_t)));
+        ctx->ptr_counter_words = words;
+    }
+    RR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->ptr_counters, 0, words * sizeof(uint32_t), stream));
+    PtrWave V;
+    float4* a = ctx->ptr_state;
+    V.st = reinterpret_cast<uint4*>(a);
+    V.acc = a + n; V.thp = a + 2 * n; V.suf = a + 3 * n; V.rcp = a + 4 * n; V.rcn = a + 5 * n;
+    V.selp = a + 6 * n; V.seln = a + 7 * n; V.sels = a + 8 * n;
+    rr_pt_queues& q = ctx->pt;
+    V.qa[0] = q.ray_a[0]; V.qa[1] = q.ray_a[1];
+    V.qb[0] = q.ray_b[0]; V.qb[1] = q.ray_b[1];
+    V.hits = q.hits;
+    V.sa = q.shadow_a; V.sb = q.shadow_b; V.sc = q.shadow_c;
+    V.ended = reinterpret_cast<uint32_t*>(q.ray_c[0]);   // n words fit in n float4
+    V.cnt = ctx->ptr_counters;
+    V.n = uint32_t(n);
+    const DevScene& S = scene->dev;
+    const PtrLaunch L = make_launch(cam, p);
+    const PtrImages I = make_images(b);
+    const int g_begin = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(ptrw_begin_kernel)),
+                                      int((n + kBlock - 1) / kBlock));
+    ptrw_begin_kernel<<<g_begin, kBlock, 0, stream>>>(S, L, I, V);
+    RR_CHECK_LAUNCH(ctx);
+    const int g_ext = persistent_grid(ctx, reinterpret_cast<const void*>(ptrw_extend_kernel));
+    const int g_sh = persistent_grid(ctx, reinterpret_cast<const void*>(ptrw_shadow_kernel));
+    const int g_shade = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(ptrw_shade_kernel)),
+                                      int((n + kBlock - 1) / kBlock));
+    const int g_adv = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(ptrw_advance_kernel)),
+                                    int((n + kBlock - 1) / kBlock));
+    for (uint32_t k = 0; k < steps; ++k) {
+        ptrw_extend_kernel<<<g_ext, kBlock, 0, stream>>>(S, V, k, L.ray_bias);
+        RR_CHECK_LAUNCH(ctx);
+        ptrw_shade_kernel<<<g_shade, kBlock, 0, stream>>>(S, L, V, k);
+        RR_CHECK_LAUNCH(ctx);
+        ptrw_shadow_kernel<<<g_sh, kBlock, 0, stream>>>(S, V, k, L.ray_bias);
+        RR_CHECK_LAUNCH(ctx);
+        ptrw_advance_kernel<<<g_adv, kBlock, 0, stream>>>(S, L, I, V, k);
+        RR_CHECK_LAUNCH(ctx);
+    }
+    ctx->launches += 1 + 4 * uint64_t(steps);
+    return RR_OK;
+}
+
 } // namespace
 } // namespace rr
 
 using namespace rr;
+
+extern "C" rr_status rr_restir_pt_set_wavefront(rr_ctx* ctx, int enable) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    ctx->ptr_wavefront = enable != 0;
+    return RR_OK;
+}
 
 extern "C" rr_status rr_restir_pt_initial(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* cam,
                                           const rr_restir_pt_params* p, const rr_restir_pt_images* b,
@@ -378,6 +795,8 @@ extern "C" rr_status rr_restir_pt_initial(rr_ctx* ctx, const rr_scene* scene, co
     rr_status st = check(ctx, scene, cam, p, b, kInitial);
     if (st != RR_OK) return st;
     RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (ctx->ptr_wavefront && uint64_t(cam->screen_width) * cam->screen_height < (1ull << 31))
+        return ptr_initial_wavefront(ctx, scene, cam, p, b, static_cast<cudaStream_t>(stream));
     ptr_initial_kernel<<<grid_of(cam), 128, 0, static_cast<cudaStream_t>(stream)>>>(scene->dev, make_launch(cam, p),
                                                                                    make_images(b));
     RR_CHECK_LAUNCH(ctx);

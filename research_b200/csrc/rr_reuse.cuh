@@ -43,12 +43,15 @@ RR_D bool load_surface(const DevScene& s, const float4* pos_img, const float4* n
     return mat < s.num_materials;
 }
 
-// sample_lights (restir_pt.slang:172-221): one light picked uniformly,
-// shadow ray from hit_pos + normal * ray_bias over [ray_bias, dist - 0.01].
-RR_D float3 sample_lights(const DevScene& s, float3 hit_pos, float3 normal, float3 wo, const Mat& m, float bias,
-                          uint32_t& seed) {
+// The light sample of sample_lights without its visibility test: the light
+// pick (one random number), the shadow ray (origin, direction, t_max; t_min
+// is the bias) and the contribution if the light is visible. Returns false
+// where sample_lights returns zero before tracing (no lights, light below
+// the surface).
+RR_D bool sample_light_ray(const DevScene& s, float3 hit_pos, float3 normal, float3 wo, const Mat& m, float bias,
+                           uint32_t& seed, float3& origin, float3& dir, float& tmax, float3& contrib) {
     const uint32_t N = s.num_lights;
-    if (N == 0) return f3(0.0f, 0.0f, 0.0f);
+    if (N == 0) return false;
     const uint32_t li = uint32_t(rand_float(seed) * float(N)) % N;
     const float4 l0 = __ldg(s.lights + li * 3), l1 = __ldg(s.lights + li * 3 + 1), l2 = __ldg(s.lights + li * 3 + 2);
     const bool is_point = __float_as_uint(l0.w) == 0u;
@@ -64,16 +67,30 @@ RR_D float3 sample_lights(const DevScene& s, float3 hit_pos, float3 normal, floa
         dist = 1e9f;
         pdf_light = 1.0f;
     }
-    if (dot(ldir, normal) <= 0.0f) return f3(0.0f, 0.0f, 0.0f);
-    HitRec h;
-    if (trace<true>(s, make_ray(hit_pos + normal * bias, ldir), bias, dist - 0.01f, h)) return f3(0.0f, 0.0f, 0.0f);
+    if (dot(ldir, normal) <= 0.0f) return false;
+    origin = hit_pos + normal * bias;
+    dir = ldir;
+    tmax = dist - 0.01f;
     const float3 brdf_val = brdf_eval(normal, wo, ldir, m.base, m.metallic, m.roughness);
     const float n_dot_l = mx(dot(normal, ldir), 0.0f);
     const float den = is_point ? (pdf_light + 1e-6f) : 1.0f;
     const float3 irr = f3(l2.x * l2.w / den, l2.y * l2.w / den, l2.z * l2.w / den);
     const float pdf_bsdf = brdf_pdf(wo, ldir, normal, m.roughness);
     const float mis = is_point ? 1.0f : (pdf_light * pdf_light) / (pdf_light * pdf_light + pdf_bsdf * pdf_bsdf + 1e-10f);
-    return (((brdf_val * irr) * n_dot_l) * mis) * float(N);
+    contrib = (((brdf_val * irr) * n_dot_l) * mis) * float(N);
+    return true;
+}
+
+// sample_lights (restir_pt.slang:172-221): one light picked uniformly,
+// shadow ray from hit_pos + normal * ray_bias over [ray_bias, dist - 0.01].
+RR_D float3 sample_lights(const DevScene& s, float3 hit_pos, float3 normal, float3 wo, const Mat& m, float bias,
+                          uint32_t& seed) {
+    float3 o, d, c;
+    float tmax;
+    if (!sample_light_ray(s, hit_pos, normal, wo, m, bias, seed, o, d, tmax, c)) return f3(0.0f, 0.0f, 0.0f);
+    HitRec h;
+    if (trace<true>(s, make_ray(o, d), bias, tmax, h)) return f3(0.0f, 0.0f, 0.0f);
+    return c;
 }
 
 // reconnection_jacobian (restir_pt.slang:437-457)

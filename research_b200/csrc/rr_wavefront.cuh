@@ -123,11 +123,12 @@ struct WarpPool {
 // `Finish(i, found, hit)` consumes a finished ray; `Load(i, ray, tmax)` makes
 // one and returns its scene index. Multi: a batch of scenes, each ray traced
 // in the scene `table[index]` (the lane binds that scene's node and triangle
-// arrays when it loads the ray); otherwise every ray is traced in `s`.
+// arrays when it loads the ray); otherwise every ray is traced in `s`. Rays
+// start at t = tmin (the path tracer's 0.001).
 template <bool AnyHit, bool Count, bool Refill, bool Multi, class Load, class Finish>
 __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene* __restrict__ table, uint32_t count,
                                                uint32_t* cursor, unsigned long long* work_out, Load load,
-                                               Finish finish) {
+                                               Finish finish, float tmin = 0.001f) {
     TraceWork tw;
     int2 stack[kStackSize];  // (node, near distance)
     DevScene ls{};           // Multi: the current ray's scene (traversal fields)
@@ -139,8 +140,8 @@ __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene
         }
     };
     auto step = [&](const Ray& r, HitRec& h, TravState& st) -> bool {
-        if constexpr (Multi) return trace_step<AnyHit, Count>(ls, r, 0.001f, h, st, stack, &tw);
-        else return trace_step<AnyHit, Count>(s, r, 0.001f, h, st, stack, &tw);
+        if constexpr (Multi) return trace_step<AnyHit, Count>(ls, r, tmin, h, st, stack, &tw);
+        else return trace_step<AnyHit, Count>(s, r, tmin, h, st, stack, &tw);
     };
     if constexpr (!Refill) {
         while (true) {

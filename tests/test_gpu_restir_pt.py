@@ -112,7 +112,15 @@ def _run(rr, O, ctx, torch, arrays, W, H, frames, eye0, center, move, **kw):
     return stats
 
 
-def test_restir_pt_cornell_bit_exact(rr, O, ctx, torch_cuda):
+@pytest.fixture(params=[1, 0], ids=["wavefront", "per_pixel"])
+def initial_form(request, rr, ctx):
+    """cs_initial as the wavefront (default) and as one thread per pixel."""
+    ctx.check(rr.lib().rr_restir_pt_set_wavefront(ctx.handle, request.param))
+    yield request.param
+    ctx.check(rr.lib().rr_restir_pt_set_wavefront(ctx.handle, 1))
+
+
+def test_restir_pt_cornell_bit_exact(rr, O, ctx, torch_cuda, initial_form):
     torch = torch_cuda
     hs = rr.HostScene.cornell(0)
     s = _run(rr, O, ctx, torch, hs.arrays, 48, 40, 4, (0.0, 0.0, 3.0), (0.0, 0.0, 0.0), (0.004, 0.0, -0.01))
@@ -120,7 +128,7 @@ def test_restir_pt_cornell_bit_exact(rr, O, ctx, torch_cuda):
     assert s["valid"] > 0.9 and s["M"] > 16 and s["lobes"] > 50 and s["out_mean"] > s["direct_mean"]
 
 
-def test_restir_pt_procedural_bit_exact(rr, O, ctx, torch_cuda):
+def test_restir_pt_procedural_bit_exact(rr, O, ctx, torch_cuda, initial_form):
     torch = torch_cuda
     hs = rr.HostScene.procedural(target_triangles=20_000, emissive_triangles=64, box_half=20.0)
     s = _run(rr, O, ctx, torch, hs.arrays, 40, 32, 3, (0.0, 4.0, 34.0), (0.0, -3.0, 0.0), (0.05, 0.0, -0.1))
@@ -133,6 +141,16 @@ def test_restir_pt_options_bit_exact(rr, O, ctx, torch_cuda):
     hs = rr.HostScene.cornell(1)
     _run(rr, O, ctx, torch, hs.arrays, 32, 24, 2, (0.0, 0.0, 3.0), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0),
          temporal=0, spatial=0, include_direct=0, max_bounces=1, guiding=0, candidates=3)
+
+
+def test_restir_pt_deep_paths_bit_exact(rr, O, ctx, torch_cuda):
+    """More candidates and bounces than the defaults (the wavefront runs
+    candidates x bounces steps), on the procedural room."""
+    torch = torch_cuda
+    hs = rr.HostScene.procedural(seed=5, target_triangles=20_000, emissive_triangles=32, box_half=20.0)
+    s = _run(rr, O, ctx, torch, hs.arrays, 24, 20, 2, (0.0, 4.0, 34.0), (0.0, -3.0, 0.0), (0.05, 0.0, -0.1),
+             candidates=5, max_bounces=7)
+    assert s["valid"] > 0.5
 
 
 def test_restir_pt_reset_history(rr, ctx, torch_cuda):
