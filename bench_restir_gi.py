@@ -26,6 +26,8 @@ def main():
     ap.add_argument("--frames", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--triangles", type=int, default=1_000_000)
+    ap.add_argument("--initial", choices=["wavefront", "per_pixel"], default="wavefront",
+                    help="form of the initial pass (rr_reuse_set_wavefront)")
     args = ap.parse_args()
 
     import torch
@@ -33,6 +35,7 @@ def main():
     torch.cuda.set_device(0)
     L = rr.lib()
     ctx = rr.Context(0)
+    ctx.check(rr.lib().rr_reuse_set_wavefront(ctx.handle, 1 if args.initial == "wavefront" else 0))
     hs = rr.HostScene.procedural(target_triangles=args.triangles)
     scene = rr.Scene(ctx, hs.arrays)
     W, H = args.width, args.height
@@ -82,7 +85,8 @@ def main():
     line = {"metric": "ReSTIR GI frame time, 1xB200", "unit": "ms/frame", "value": round(frame_ms, 3),
             "stages_ms": ms, "frames": args.frames, "warmup": args.warmup,
             "mpixels_per_s": round(W * H / frame_ms / 1e3, 2),
-            "config": {"workload": f"procedural-room-1M-tris, {W}x{H}", "candidates": 8, "spatial_neighbors": 4,
+            "config": {"workload": f"procedural-room-1M-tris, {W}x{H}", "initial": args.initial, "candidates": 8,
+                       "spatial_neighbors": 4,
                        "spatial_radius": 12, "di_candidates": 32},
             "mean_M": float(M.float().mean()), "output_mean": float(o.mean()),
             "output_finite": bool(torch.isfinite(o).all())}

@@ -28,7 +28,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--triangles", type=int, default=1_000_000)
     ap.add_argument("--initial", choices=["wavefront", "per_pixel"], default="wavefront",
-                    help="form of the initial pass (rr_restir_pt_set_wavefront)")
+                    help="form of the initial pass (rr_reuse_set_wavefront)")
     args = ap.parse_args()
 
     import torch
@@ -36,7 +36,7 @@ def main():
     torch.cuda.set_device(0)
     L = rr.lib()
     ctx = rr.Context(0)
-    ctx.check(rr.lib().rr_restir_pt_set_wavefront(ctx.handle, 1 if args.initial == "wavefront" else 0))
+    ctx.check(rr.lib().rr_reuse_set_wavefront(ctx.handle, 1 if args.initial == "wavefront" else 0))
     hs = rr.HostScene.procedural(target_triangles=args.triangles)
     scene = rr.Scene(ctx, hs.arrays)
     W, H = args.width, args.height

@@ -366,9 +366,10 @@ typedef struct rr_restir_pt_images {
 rr_status rr_restir_pt_initial(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
                                const rr_restir_pt_params* params, const rr_restir_pt_images* images,
                                void* stream);
-/* 1 (default): rr_restir_pt_initial runs as the wavefront; 0: one thread per
- * pixel runs the whole candidate loop. */
-rr_status rr_restir_pt_set_wavefront(rr_ctx* ctx, int enable);
+/* 1 (default): rr_restir_pt_initial and rr_restir_gi_initial run as
+ * wavefronts; 0: one thread per pixel runs the whole candidate loop. Both
+ * forms give the same bits. */
+rr_status rr_reuse_set_wavefront(rr_ctx* ctx, int enable);
 /* cs_temporal (restir_pt.slang:760-857); returns at once when temporal_enable is 0. */
 rr_status rr_restir_pt_temporal(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
                                 const rr_restir_pt_params* params, const rr_restir_pt_images* images,
@@ -424,7 +425,9 @@ typedef struct rr_restir_gi_images {
     float*       output;
 } rr_restir_gi_images;
 
-/* cs_initial (restir_gi.slang:568-686): writes reservoir_curr and history_curr. */
+/* cs_initial (restir_gi.slang:568-686): writes reservoir_curr and history_curr.
+ * By default run as a wavefront (one candidate of every pixel per step; see
+ * rr_reuse_set_wavefront), bit-identical to one thread per pixel. */
 rr_status rr_restir_gi_initial(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
                                const rr_restir_gi_params* params, const rr_restir_gi_images* images,
                                void* stream);

@@ -13,6 +13,7 @@
 //   (sample_pos, w_sum), (sample_radiance, W), (sample_normal, asfloat(M)).
 
 #include "rr_reuse.cuh"
+#include "rr_wave.cuh"
 
 namespace rr {
 namespace {
@@ -152,6 +153,221 @@ __global__ void __launch_bounds__(128, 8) gi_initial_kernel(DevScene s, GiLaunch
         }
     }
     store_gi_empty(I.rc, i);
+}
+
+// ── wavefront form of cs_initial ───────────────────────────────────────────
+// gi_initial_kernel cut at its rays, as the ReSTIR PT initial pass is (steps
+// in rr_wave.cuh). A candidate is one segment, so each step takes one
+// candidate of every pixel with work: extend (the cosine ray), shade (the
+// secondary vertex: its emission, the light sample with its shadow ray
+// queued), shadow (the light's contribution or zero added to the vertex's
+// radiance), advance (resampling, then the next candidate's direction or the
+// reservoir). Random numbers and additions keep the inline order, so the
+// results are the same bits; num_candidates steps cover every pixel.
+struct GiWave {
+    uint4* st;          // (seed, candidate, -, M)
+    float4* acc;        // (w_sum, -, -, -)
+    float4* spos;       // the candidate's secondary vertex
+    float4* snrm;       // its geometric normal as hit_surface returns it
+    float4* rad;        // its outgoing radiance: emission + light sample
+    float4* selp;       // selected sample: position
+    float4* selr;       // radiance
+    float4* seln;       // normal
+    float4* qa[2];
+    float4* qb[2];
+    float4* hits;
+    float4* sa;
+    float4* sb;
+    float4* sc;
+    uint32_t* ended;
+    uint32_t* cnt;
+    uint32_t n;
+};
+constexpr int kGiWaveArrays = 8;
+
+// The pixel's next candidate direction from candidate c on (cosine lobe;
+// directions below the surface are skipped as the inline `continue`).
+RR_D bool giw_next(const GiLaunch& L, float3 pp, float3 pn, uint32_t& seed, uint32_t& c, float3& o, float3& d) {
+    float3 T, B;
+    build_onb(pn, T, B);
+    for (; c < L.num_candidates; ++c) {
+        const float u0 = rand_float(seed);
+        const float u1 = rand_float(seed);
+        float pdf_dir;
+        const float3 dd = tangent_to_world(sample_cosine_hemisphere(u0, u1, pdf_dir), T, B, pn);
+        if (dot(pn, dd) <= 0.0f) continue;
+        o = pp + pn * L.ray_bias;
+        d = dd;
+        return true;
+    }
+    return false;
+}
+
+// The end of gi_initial_kernel: the selected sample's reservoir or an empty one.
+RR_D void giw_finish(const GiLaunch& L, const GiImages& I, const GiWave& V, size_t i, float3 pp, float3 pn,
+                     const Mat& pm, uint32_t M_count, float w_sum) {
+    if (M_count > 0) {
+        GiRes sel;
+        sel.pos = xyz(V.selp[i]); sel.rad = xyz(V.selr[i]); sel.nrm = xyz(V.seln[i]);
+        const float ph_y = gi_target(pp, pn, pm, cam_pos(L.cam), sel.pos, sel.rad);
+        if (ph_y > 1e-10f) {
+            sel.w_sum = w_sum;
+            sel.W = w_sum / (float(M_count) * ph_y);
+            sel.M = M_count;
+            store_gi(I.rc, i, sel);
+            return;
+        }
+    }
+    store_gi_empty(I.rc, i);
+}
+
+__global__ void __launch_bounds__(kBlock) giw_begin_kernel(DevScene s, GiLaunch L, GiImages I, GiWave V) {
+    const uint32_t W = L.cam.screen_width;
+    const uint32_t warp_first = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+    for (uint32_t base = warp_first; base < V.n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + lane_id();
+        bool emit = false;
+        float3 o = f3(0.0f, 0.0f, 0.0f), d = f3(0.0f, 0.0f, 0.0f);
+        if (i < V.n) {
+            const uint32_t x = i % W, y = i / W;
+            uint32_t seed = make_seed(x, y, L.frame_seed);
+            float4 p4, n4;
+            float3 pp, pn;
+            uint32_t pmat;
+            if (!load_surface(s, I.gpos, I.gnrm, i, p4, n4, pp, pn, pmat)) {
+                I.hc[0][i] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+                I.hc[1][i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                store_gi_empty(I.rc, i);
+            } else {
+                I.hc[0][i] = p4;
+                I.hc[1][i] = n4;
+                const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                V.selp[i] = z; V.selr[i] = z; V.seln[i] = z;
+                uint32_t c = 0;
+                emit = giw_next(L, pp, pn, seed, c, o, d);
+                if (emit) {
+                    V.st[i] = make_uint4(seed, c, 0u, 0u);
+                    V.acc[i] = z;
+                } else {
+                    store_gi_empty(I.rc, i);   // no candidate: M = 0
+                }
+            }
+        }
+        const uint32_t slot = warp_alloc(emit, V.cnt);
+        if (emit) {
+            V.qa[0][slot] = make_float4(o.x, o.y, o.z, __uint_as_float(i));
+            V.qb[0][slot] = make_float4(d.x, d.y, d.z, 0.0f);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBlock, 4) giw_shade_kernel(DevScene s, GiLaunch L, GiWave V, uint32_t step) {
+    const int cur = step & 1;
+    uint32_t* c0 = V.cnt + size_t(step) * kWaveWords;
+    const uint32_t count = c0[0];
+    const float bias = L.ray_bias;
+    const uint32_t warp_first = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+    for (uint32_t base = warp_first; base < count; base += gridDim.x * blockDim.x) {
+        const uint32_t q = base + lane_id();
+        bool shadow = false, ris = false;
+        uint32_t pid = 0;
+        float3 so = f3(0.0f, 0.0f, 0.0f), sd = so, sc = so;
+        float stmax = 0.0f;
+        if (q < count) {
+            const float4 a = V.qa[cur][q], b = V.qb[cur][q], h = V.hits[q];
+            pid = __float_as_uint(a.w);
+            const uint32_t inst = __float_as_uint(h.z);
+            if (inst != kNoIndex) {
+                // evaluate_sample_radiance (:539-552): normal turned toward wo = -d
+                uint4 st = V.st[pid];
+                uint32_t seed = st.x;
+                const float3 d = xyz(b);
+                const Surface sec = hit_surface(s, inst, __float_as_uint(h.w), h.x, h.y);
+                const float3 wo = -d;
+                float3 sn = sec.normal;
+                if (dot(sn, wo) < 0.0f) sn = -sn;
+                const Mat sm = load_mat(s, sec.material);
+                float3 rad = sm.emissive;
+                float3 c;
+                shadow = sample_light_ray(s, sec.pos, sn, wo, sm, bias, seed, so, sd, stmax, c);
+                if (shadow) sc = c;
+                else rad = rad + f3(0.0f, 0.0f, 0.0f);
+                V.spos[pid] = make_float4(sec.pos.x, sec.pos.y, sec.pos.z, 0.0f);
+                V.snrm[pid] = make_float4(sec.normal.x, sec.normal.y, sec.normal.z, 0.0f);
+                V.rad[pid] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+                st.x = seed;
+                V.st[pid] = st;
+                ris = true;
+            }
+        }
+        const uint32_t sslot = warp_alloc(shadow, c0 + 2);
+        if (shadow) {
+            V.sa[sslot] = make_float4(so.x, so.y, so.z, __uint_as_float(pid));
+            V.sb[sslot] = make_float4(sd.x, sd.y, sd.z, stmax);
+            V.sc[sslot] = make_float4(sc.x, sc.y, sc.z, 0.0f);
+        }
+        // every segment ends its candidate (a miss drops it)
+        const uint32_t eslot = warp_alloc(q < count, c0 + 4);
+        if (q < count) V.ended[eslot] = pid | (ris ? kRis : 0u);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) giw_advance_kernel(DevScene s, GiLaunch L, GiImages I, GiWave V,
+                                                             uint32_t step) {
+    const int nxt = (step & 1) ^ 1;
+    uint32_t* c0 = V.cnt + size_t(step) * kWaveWords;
+    uint32_t* c1 = c0 + kWaveWords;
+    const uint32_t count = c0[4];
+    const float3 cp = cam_pos(L.cam);
+    const uint32_t warp_first = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+    for (uint32_t base = warp_first; base < count; base += gridDim.x * blockDim.x) {
+        const uint32_t q = base + lane_id();
+        bool emit = false;
+        uint32_t pid = 0;
+        float3 o = f3(0.0f, 0.0f, 0.0f), d = o;
+        if (q < count) {
+            const uint32_t e = V.ended[q];
+            pid = e & ~kRis;
+            const uint4 st = V.st[pid];
+            uint32_t seed = st.x, c = st.y, M_count = st.w;
+            float w_sum = V.acc[pid].x;
+            float4 p4, n4;
+            float3 pp, pn;
+            uint32_t pmat;
+            load_surface(s, I.gpos, I.gnrm, pid, p4, n4, pp, pn, pmat);
+            const Mat pm = load_mat(s, pmat);
+            if (e & kRis) {
+                const float3 spos = xyz(V.spos[pid]), rad = xyz(V.rad[pid]);
+                const float tgt = gi_target(pp, pn, pm, cp, spos, rad);
+                if (!(tgt <= 0.0f)) {
+                    const float pdf = gi_source_pdf(pp, pn, spos);
+                    if (!(pdf <= 1e-6f)) {
+                        const float weight = tgt / pdf;
+                        w_sum += weight;
+                        M_count++;
+                        if (w_sum > 0.0f && rand_float(seed) < weight / w_sum) {
+                            V.selp[pid] = make_float4(spos.x, spos.y, spos.z, 0.0f);
+                            V.selr[pid] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+                            V.seln[pid] = V.snrm[pid];
+                        }
+                    }
+                }
+            }
+            ++c;
+            emit = giw_next(L, pp, pn, seed, c, o, d);
+            if (emit) {
+                V.st[pid] = make_uint4(seed, c, 0u, M_count);
+                V.acc[pid] = make_float4(w_sum, 0.0f, 0.0f, 0.0f);
+            } else {
+                giw_finish(L, I, V, pid, pp, pn, pm, M_count, w_sum);
+            }
+        }
+        const uint32_t slot = warp_alloc(emit, c1);
+        if (emit) {
+            V.qa[nxt][slot] = make_float4(o.x, o.y, o.z, __uint_as_float(pid));
+            V.qb[nxt][slot] = make_float4(d.x, d.y, d.z, 0.0f);
+        }
+    }
 }
 
 // cs_temporal (restir_gi.slang:688-848)
@@ -324,6 +540,57 @@ rr_status check(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* cam, co
     return RR_OK;
 }
 
+// cs_initial as the wavefront above: one launch to start every pixel, then
+// per candidate extend, shade, shadow and advance.
+rr_status gi_initial_wavefront(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* cam,
+                               const rr_restir_gi_params* p, const rr_restir_gi_images* b, cudaStream_t stream) {
+    const size_t n = size_t(cam->screen_width) * cam->screen_height;
+    rr_status st = ensure_queues(ctx, n);
+    if (st != RR_OK) return st;
+    if (p->num_initial_candidates > (1u << 20))
+        return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "ReSTIR GI: too many candidates");
+    const uint32_t steps = p->num_initial_candidates;
+    float4* a = nullptr;
+    uint32_t* cnt = nullptr;
+    if ((st = wave_scratch(ctx, n, kGiWaveArrays, steps, stream, &a, &cnt)) != RR_OK) return st;
+    GiWave V;
+    V.st = reinterpret_cast<uint4*>(a);
+    V.acc = a + n; V.spos = a + 2 * n; V.snrm = a + 3 * n; V.rad = a + 4 * n;
+    V.selp = a + 5 * n; V.selr = a + 6 * n; V.seln = a + 7 * n;
+    rr_pt_queues& q = ctx->pt;
+    V.qa[0] = q.ray_a[0]; V.qa[1] = q.ray_a[1];
+    V.qb[0] = q.ray_b[0]; V.qb[1] = q.ray_b[1];
+    V.hits = q.hits;
+    V.sa = q.shadow_a; V.sb = q.shadow_b; V.sc = q.shadow_c;
+    V.ended = reinterpret_cast<uint32_t*>(q.ray_c[0]);   // n words fit in n float4
+    V.cnt = cnt;
+    V.n = uint32_t(n);
+    const DevScene& S = scene->dev;
+    const GiLaunch L = make_launch(cam, p);
+    const GiImages I = make_images(b);
+    const int cap = int((n + kBlock - 1) / kBlock);
+    const int g_begin = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(giw_begin_kernel)), cap);
+    giw_begin_kernel<<<g_begin, kBlock, 0, stream>>>(S, L, I, V);
+    RR_CHECK_LAUNCH(ctx);
+    const int g_ext = persistent_grid(ctx, reinterpret_cast<const void*>(wave_extend_kernel));
+    const int g_sh = persistent_grid(ctx, reinterpret_cast<const void*>(wave_shadow_kernel));
+    const int g_shade = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(giw_shade_kernel)), cap);
+    const int g_adv = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(giw_advance_kernel)), cap);
+    for (uint32_t k = 0; k < steps; ++k) {
+        uint32_t* c0 = cnt + size_t(k) * kWaveWords;
+        wave_extend_kernel<<<g_ext, kBlock, 0, stream>>>(S, V.qa[k & 1], V.qb[k & 1], V.hits, c0, L.ray_bias);
+        RR_CHECK_LAUNCH(ctx);
+        giw_shade_kernel<<<g_shade, kBlock, 0, stream>>>(S, L, V, k);
+        RR_CHECK_LAUNCH(ctx);
+        wave_shadow_kernel<<<g_sh, kBlock, 0, stream>>>(S, V.sa, V.sb, V.sc, V.rad, c0, L.ray_bias);
+        RR_CHECK_LAUNCH(ctx);
+        giw_advance_kernel<<<g_adv, kBlock, 0, stream>>>(S, L, I, V, k);
+        RR_CHECK_LAUNCH(ctx);
+    }
+    ctx->launches += 1 + 4 * uint64_t(steps);
+    return RR_OK;
+}
+
 } // namespace
 } // namespace rr
 
@@ -336,6 +603,8 @@ extern "C" rr_status rr_restir_gi_initial(rr_ctx* ctx, const rr_scene* scene, co
     rr_status st = check(ctx, scene, cam, p, b, kInitial);
     if (st != RR_OK) return st;
     RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (ctx->wave_initial && uint64_t(cam->screen_width) * cam->screen_height < (1ull << 31))
+        return gi_initial_wavefront(ctx, scene, cam, p, b, static_cast<cudaStream_t>(stream));
     gi_initial_kernel<<<grid_of(cam), 128, 0, static_cast<cudaStream_t>(stream)>>>(scene->dev, make_launch(cam, p),
                                                                                   make_images(b));
     RR_CHECK_LAUNCH(ctx);

@@ -16,7 +16,7 @@
 
 #include "rr_grid.cuh"
 #include "rr_reuse.cuh"
-#include "rr_wavefront.cuh"
+#include "rr_wave.cuh"
 
 namespace rr {
 namespace {
@@ -183,18 +183,19 @@ __global__ void __launch_bounds__(128, 8) ptr_initial_kernel(DevScene s, PtrLaun
 }
 
 // ── wavefront form of cs_initial ───────────────────────────────────────────
-// The same per-pixel computation as ptr_initial_kernel, cut at every ray.
+// The same per-pixel computation as ptr_initial_kernel, cut at every ray
+// (traversal steps in rr_wave.cuh).
 // Each pixel keeps its state in HBM (random-number seed, candidate index,
 // segment index, M, w_sum, source pdf, path throughput, suffix radiance, the
 // candidate's reconnection vertex, the selected candidate); each step
 // advances every pixel with work by one path segment:
-//   extend  : closest hit of the step's segment rays (queue traversal)
+//   extend  : closest hit of the step's segment rays (wave_extend_kernel)
 //   shade   : the reconnection vertex or a bounce vertex as the inline loop
 //             handles it: sky on a miss, the light sample (its shadow ray is
 //             queued with the contribution it adds if the light is visible),
 //             then the next BSDF direction, or the candidate ends
 //   shadow  : any-hit traversal of the step's shadow rays; each adds its
-//             contribution (or zero) to its pixel's suffix
+//             contribution (or zero) to its pixel's suffix (wave_shadow_kernel)
 //   advance : for every candidate that ended, the resampling step, then the
 //             next candidates' first directions (ray into the next step's
 //             queue) or, after the last one, the reservoir
@@ -204,8 +205,6 @@ __global__ void __launch_bounds__(128, 8) ptr_initial_kernel(DevScene s, PtrLaun
 // shadow stage, before the vertex after it is shaded. Each pixel has at most
 // one segment ray and one shadow ray per step, so a pixel takes at most
 // num_candidates x max(max_bounces, 1) steps.
-constexpr int kWaveWords = 8;   // per step: rays, ray cursor, shadow rays, shadow cursor, ended candidates
-constexpr uint32_t kRis = 0x80000000u;
 
 struct PtrWave {
     uint4* st;          // (seed, candidate, segment, M)
@@ -302,26 +301,6 @@ __global__ void __launch_bounds__(kBlock) ptrw_begin_kernel(DevScene s, PtrLaunc
             V.qb[0][slot] = make_float4(d.x, d.y, d.z, 0.0f);
         }
     }
-}
-
-__global__ void __launch_bounds__(kBlock, 4) ptrw_extend_kernel(DevScene s, PtrWave V, uint32_t step, float tmin) {
-    const int cur = step & 1;
-    uint32_t* c0 = V.cnt + size_t(step) * kWaveWords;
-    const float4* qa = V.qa[cur];
-    const float4* qb = V.qb[cur];
-    float4* hits = V.hits;
-    traverse_queue<false, false, false, false>(
-        s, nullptr, c0[0], c0 + 1, nullptr,
-        [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
-            r = make_ray(xyz(qa[i]), xyz(qb[i]));
-            tmax = 1e9f;
-            return 0u;
-        },
-        [&](uint32_t i, bool found, const HitRec& h) {
-            hits[i] = found ? make_float4(h.u, h.v, __uint_as_float(h.inst), __uint_as_float(h.prim))
-                            : make_float4(0.0f, 0.0f, __uint_as_float(kNoIndex), __uint_as_float(kNoIndex));
-        },
-        tmin);
 }
 
 __global__ void __launch_bounds__(kBlock, 4) ptrw_shade_kernel(DevScene s, PtrLaunch L, PtrWave V, uint32_t step) {
@@ -437,29 +416,6 @@ __global__ void __launch_bounds__(kBlock, 4) ptrw_shade_kernel(DevScene s, PtrLa
         const uint32_t eslot = warp_alloc(ended, c0 + 4);
         if (ended) V.ended[eslot] = pid | (ris ? kRis : 0u);
     }
-}
-
-__global__ void __launch_bounds__(kBlock, 5) ptrw_shadow_kernel(DevScene s, PtrWave V, uint32_t step, float tmin) {
-    uint32_t* c0 = V.cnt + size_t(step) * kWaveWords;
-    const float4* sa = V.sa;
-    const float4* sb = V.sb;
-    const float4* sc = V.sc;
-    float4* suf = V.suf;
-    traverse_queue<true, false, false, false>(
-        s, nullptr, c0[2], c0 + 3, nullptr,
-        [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
-            const float4 b = sb[i];
-            r = make_ray(xyz(sa[i]), xyz(b));
-            tmax = b.w;
-            return 0u;
-        },
-        [&](uint32_t i, bool found, const HitRec&) {
-            const uint32_t pid = __float_as_uint(sa[i].w);
-            const float3 add = found ? f3(0.0f, 0.0f, 0.0f) : xyz(sc[i]);
-            const float3 v = xyz(suf[pid]) + add;
-            suf[pid] = make_float4(v.x, v.y, v.z, 0.0f);
-        },
-        tmin);
 }
 
 __global__ void __launch_bounds__(kBlock) ptrw_advance_kernel(DevScene s, PtrLaunch L, PtrImages I, PtrWave V,
@@ -717,28 +673,14 @@ rr_status ptr_initial_wavefront(rr_ctx* ctx, const rr_scene* scene, const GpuCam
     const size_t n = size_t(cam->screen_width) * cam->screen_height;
     rr_status st = ensure_queues(ctx, n);
     if (st != RR_OK) return st;
-    if (ctx->ptr_state_px < n) {
-        cudaFree(ctx->ptr_state);
-        ctx->ptr_state = nullptr;
-        ctx->ptr_state_px = 0;
-        RR_TRY_CUDA(ctx, cudaMalloc(&ctx->ptr_state, n * kWaveArrays * sizeof(float4)));
-        ctx->ptr_state_px = n;
-    }
     const uint32_t max_b = std::max(p->max_bounces, 1u);
     const uint64_t steps64 = uint64_t(p->num_initial_candidates) * max_b;
     if (steps64 > (1u << 20)) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "ReSTIR PT: too many candidates x bounces");
     const uint32_t steps = uint32_t(steps64);
-    const size_t words = size_t(steps + 1) * kWaveWords;
-    if (ctx->ptr_counter_words < words) {
-        cudaFree(ctx->ptr_counters);
-        ctx->ptr_counters = nullptr;
-        ctx->ptr_counter_words = 0;
-        RR_TRY_CUDA(ctx, cudaMalloc(&ctx->ptr_counters, words * sizeof(uint32_t)));
-        ctx->ptr_counter_words = words;
-    }
-    RR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->ptr_counters, 0, words * sizeof(uint32_t), stream));
+    float4* a = nullptr;
+    uint32_t* cnt = nullptr;
+    if ((st = wave_scratch(ctx, n, kWaveArrays, steps, stream, &a, &cnt)) != RR_OK) return st;
     PtrWave V;
-    float4* a = ctx->ptr_state;
     V.st = reinterpret_cast<uint4*>(a);
     V.acc = a + n; V.thp = a + 2 * n; V.suf = a + 3 * n; V.rcp = a + 4 * n; V.rcn = a + 5 * n;
     V.selp = a + 6 * n; V.seln = a + 7 * n; V.sels = a + 8 * n;
@@ -748,7 +690,7 @@ rr_status ptr_initial_wavefront(rr_ctx* ctx, const rr_scene* scene, const GpuCam
     V.hits = q.hits;
     V.sa = q.shadow_a; V.sb = q.shadow_b; V.sc = q.shadow_c;
     V.ended = reinterpret_cast<uint32_t*>(q.ray_c[0]);   // n words fit in n float4
-    V.cnt = ctx->ptr_counters;
+    V.cnt = cnt;
     V.n = uint32_t(n);
     const DevScene& S = scene->dev;
     const PtrLaunch L = make_launch(cam, p);
@@ -757,18 +699,19 @@ rr_status ptr_initial_wavefront(rr_ctx* ctx, const rr_scene* scene, const GpuCam
                                       int((n + kBlock - 1) / kBlock));
     ptrw_begin_kernel<<<g_begin, kBlock, 0, stream>>>(S, L, I, V);
     RR_CHECK_LAUNCH(ctx);
-    const int g_ext = persistent_grid(ctx, reinterpret_cast<const void*>(ptrw_extend_kernel));
-    const int g_sh = persistent_grid(ctx, reinterpret_cast<const void*>(ptrw_shadow_kernel));
+    const int g_ext = persistent_grid(ctx, reinterpret_cast<const void*>(wave_extend_kernel));
+    const int g_sh = persistent_grid(ctx, reinterpret_cast<const void*>(wave_shadow_kernel));
     const int g_shade = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(ptrw_shade_kernel)),
                                       int((n + kBlock - 1) / kBlock));
     const int g_adv = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(ptrw_advance_kernel)),
                                     int((n + kBlock - 1) / kBlock));
     for (uint32_t k = 0; k < steps; ++k) {
-        ptrw_extend_kernel<<<g_ext, kBlock, 0, stream>>>(S, V, k, L.ray_bias);
+        uint32_t* c0 = cnt + size_t(k) * kWaveWords;
+        wave_extend_kernel<<<g_ext, kBlock, 0, stream>>>(S, V.qa[k & 1], V.qb[k & 1], V.hits, c0, L.ray_bias);
         RR_CHECK_LAUNCH(ctx);
         ptrw_shade_kernel<<<g_shade, kBlock, 0, stream>>>(S, L, V, k);
         RR_CHECK_LAUNCH(ctx);
-        ptrw_shadow_kernel<<<g_sh, kBlock, 0, stream>>>(S, V, k, L.ray_bias);
+        wave_shadow_kernel<<<g_sh, kBlock, 0, stream>>>(S, V.sa, V.sb, V.sc, V.suf, c0, L.ray_bias);
         RR_CHECK_LAUNCH(ctx);
         ptrw_advance_kernel<<<g_adv, kBlock, 0, stream>>>(S, L, I, V, k);
         RR_CHECK_LAUNCH(ctx);
@@ -782,9 +725,9 @@ rr_status ptr_initial_wavefront(rr_ctx* ctx, const rr_scene* scene, const GpuCam
 
 using namespace rr;
 
-extern "C" rr_status rr_restir_pt_set_wavefront(rr_ctx* ctx, int enable) {
+extern "C" rr_status rr_reuse_set_wavefront(rr_ctx* ctx, int enable) {
     if (!ctx) return RR_ERR_INVALID_ARGUMENT;
-    ctx->ptr_wavefront = enable != 0;
+    ctx->wave_initial = enable != 0;
     return RR_OK;
 }
 
@@ -795,7 +738,7 @@ extern "C" rr_status rr_restir_pt_initial(rr_ctx* ctx, const rr_scene* scene, co
     rr_status st = check(ctx, scene, cam, p, b, kInitial);
     if (st != RR_OK) return st;
     RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
-    if (ctx->ptr_wavefront && uint64_t(cam->screen_width) * cam->screen_height < (1ull << 31))
+    if (ctx->wave_initial && uint64_t(cam->screen_width) * cam->screen_height < (1ull << 31))
         return ptr_initial_wavefront(ctx, scene, cam, p, b, static_cast<cudaStream_t>(stream));
     ptr_initial_kernel<<<grid_of(cam), 128, 0, static_cast<cudaStream_t>(stream)>>>(scene->dev, make_launch(cam, p),
                                                                                    make_images(b));

@@ -65,13 +65,13 @@ struct rr_ctx {
     cudaStream_t side = nullptr;
     cudaEvent_t shaded[kMaxBounces] = {};
     cudaEvent_t shadowed[kMaxBounces] = {};
-    // ReSTIR PT initial pass in wavefront form (default) or one thread per
-    // pixel: the wavefront's per-pixel state and per-step counters
-    bool ptr_wavefront = true;
-    float4* ptr_state = nullptr;
-    size_t ptr_state_px = 0;
-    uint32_t* ptr_counters = nullptr;
-    size_t ptr_counter_words = 0;
+    // ReSTIR PT / GI initial passes in wavefront form (default) or one thread
+    // per pixel: the wavefront's per-pixel state and per-step counters
+    bool wave_initial = true;
+    float4* wave_state = nullptr;
+    size_t wave_state_len = 0;             // float4
+    uint32_t* wave_counters = nullptr;
+    size_t wave_counter_words = 0;
 };
 
 // Records a CUDA event pair around stage launches on the caller's stream;

@@ -94,8 +94,8 @@ rr_status rr_ctx_destroy(rr_ctx* ctx) {
         if (ctx->shadowed[b]) cudaEventDestroy(ctx->shadowed[b]);
     }
     if (ctx->side) cudaStreamDestroy(ctx->side);
-    cudaFree(ctx->ptr_state);
-    cudaFree(ctx->ptr_counters);
+    cudaFree(ctx->wave_state);
+    cudaFree(ctx->wave_counters);
     delete ctx;
     return RR_OK;
 }

@@ -95,7 +95,15 @@ def _run(rr, O, ctx, torch, arrays, W, H, frames, eye0, center, move, **kw):
     return stats
 
 
-def test_restir_gi_cornell_bit_exact(rr, O, ctx, torch_cuda):
+@pytest.fixture(params=[1, 0], ids=["wavefront", "per_pixel"])
+def initial_form(request, rr, ctx):
+    """cs_initial as the wavefront (default) and as one thread per pixel."""
+    ctx.check(rr.lib().rr_reuse_set_wavefront(ctx.handle, request.param))
+    yield request.param
+    ctx.check(rr.lib().rr_reuse_set_wavefront(ctx.handle, 1))
+
+
+def test_restir_gi_cornell_bit_exact(rr, O, ctx, torch_cuda, initial_form):
     torch = torch_cuda
     hs = rr.HostScene.cornell(0)
     s = _run(rr, O, ctx, torch, hs.arrays, 48, 40, 4, (0.0, 0.0, 3.0), (0.0, 0.0, 0.0), (0.004, 0.0, -0.01))
@@ -103,7 +111,7 @@ def test_restir_gi_cornell_bit_exact(rr, O, ctx, torch_cuda):
     assert s["filled"] > 0.9 and s["M"] > 16 and s["out_mean"] > s["direct_mean"]
 
 
-def test_restir_gi_procedural_bit_exact(rr, O, ctx, torch_cuda):
+def test_restir_gi_procedural_bit_exact(rr, O, ctx, torch_cuda, initial_form):
     torch = torch_cuda
     hs = rr.HostScene.procedural(target_triangles=20_000, emissive_triangles=64, box_half=20.0)
     s = _run(rr, O, ctx, torch, hs.arrays, 40, 32, 3, (0.0, 4.0, 34.0), (0.0, -3.0, 0.0), (0.05, 0.0, -0.1))

@@ -115,9 +115,9 @@ def _run(rr, O, ctx, torch, arrays, W, H, frames, eye0, center, move, **kw):
 @pytest.fixture(params=[1, 0], ids=["wavefront", "per_pixel"])
 def initial_form(request, rr, ctx):
     """cs_initial as the wavefront (default) and as one thread per pixel."""
-    ctx.check(rr.lib().rr_restir_pt_set_wavefront(ctx.handle, request.param))
+    ctx.check(rr.lib().rr_reuse_set_wavefront(ctx.handle, request.param))
     yield request.param
-    ctx.check(rr.lib().rr_restir_pt_set_wavefront(ctx.handle, 1))
+    ctx.check(rr.lib().rr_reuse_set_wavefront(ctx.handle, 1))
 
 
 def test_restir_pt_cornell_bit_exact(rr, O, ctx, torch_cuda, initial_form):
