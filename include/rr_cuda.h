@@ -134,9 +134,11 @@ rr_status rr_pathtracer_stats(rr_ctx* ctx, rr_pt_stats* out, int reset_times);
  *         compiler's register count (default) / a budget for 5 / 6 blocks of
  *         256 threads per SM;
  *   3..5: persistent warps with per-lane ray refill, with the compiler's
- *         register count / a budget for 4 / 6 blocks.
+ *         register count / a budget for 4 / 6 blocks;
+ *   6..7: as 0, with leaves postponed until every lane of the warp holds one
+ *         (the compiler's register count / a budget for 4 blocks).
  * Results are identical for every variant; only speed differs. */
-#define RR_PT_VARIANT_COUNT 6
+#define RR_PT_VARIANT_COUNT 8
 rr_status rr_pathtracer_set_variants(rr_ctx* ctx, int extend_variant, int shadow_variant);
 
 /* Shadow overlap (default on): rr_pathtracer_execute traces bounce b's

@@ -155,28 +155,82 @@ struct TraceWork {
     uint32_t tris = 0;
 };
 
-// Traversal state of one ray between node steps.
+// Traversal state of one ray between node steps. node < 0: no inner node
+// left, only the postponed leaf (pend_count > 0) to intersect.
 struct TravState {
     int node;
     int sp;
     bool found;
     uint32_t visits;
+    int pend_first, pend_count;
 };
 
 RR_D void trav_begin(TravState& st, HitRec& hit, float tmax) {
     st.node = 0; st.sp = 0; st.found = false; st.visits = 0;
+    st.pend_first = 0; st.pend_count = 0;
     hit.t = tmax; hit.key = kNoIndex;
+}
+
+// The triangles [first, first + count) of a leaf against the ray; closest
+// hit: keeps the lowest (t, key); any hit: returns true at the first hit.
+template <bool AnyHit, bool Count>
+RR_D bool leaf_tris(const DevScene& s, const Ray& r, float tmin, HitRec& hit, TravState& st, int first, int count,
+                    TraceWork* work) {
+    for (int i = first; i < first + count; ++i) {
+        if (Count) work->tris++;
+        const float4 t0 = __ldg(s.tris + i * 3 + 0);
+        const float4 t1 = __ldg(s.tris + i * 3 + 1);
+        const float4 t2 = __ldg(s.tris + i * 3 + 2);
+        float tt, uu, vv;
+        if (intersect_triangle(r, f3(t0.x, t0.y, t0.z), f3(t0.w, t1.x, t1.y), f3(t1.z, t1.w, t2.x), tmin, hit.t,
+                               tt, uu, vv)) {
+            const uint32_t key = __float_as_uint(t2.w);
+            if (AnyHit) { hit.t = tt; st.found = true; return true; }
+            if (!st.found || tt < hit.t || (tt == hit.t && key < hit.key)) {
+                st.found = true;
+                hit.t = tt; hit.u = uu; hit.v = vv; hit.key = key;
+                hit.inst = __float_as_uint(t2.y); hit.prim = __float_as_uint(t2.z);
+            }
+        }
+    }
+    return false;
+}
+
+// Pops the next stacked node not beyond the current hit; false when none is left.
+RR_D bool pop_node(TravState& st, const int2* stack, const HitRec& hit) {
+    while (st.sp > 0) {
+        --st.sp;
+        const int2 e = stack[st.sp];
+        if (__int_as_float(e.y) <= hit.t) { st.node = e.x; return true; }
+    }
+    return false;
 }
 
 // One node of a closest-hit (AnyHit = false) or any-hit traversal: tests the
 // node's two child boxes, intersects the triangles of hit leaf children right
 // away, descends into the nearer inner child and pushes the farther one.
 // Returns true once the traversal is finished (stack empty, or any hit).
-template <bool AnyHit, bool Count>
+// Postpone: a lane keeps its first leaf child for later and goes on with
+// inner nodes; the step intersects the kept leaf once every lane of the warp
+// still traversing holds one (or the lane has no inner node left), so the
+// warp runs its leaves' triangle loops side by side instead of one lane's
+// at a time (Aila and Laine 2009). Culling meanwhile uses the hit found so
+// far, which only visits more, and the kept (t, key) minimum does not depend
+// on the order, so the result is the same.
+template <bool AnyHit, bool Count, bool Postpone = false>
 RR_D bool trace_step(const DevScene& s, const Ray& r, float tmin, HitRec& hit, TravState& st,
                      int2* stack, TraceWork* work) {
-    // A tree visits each node at most once; the bound only guards against a
-    // malformed node array turning into an endless loop.
+    if constexpr (Postpone) {
+        const bool all_hold = __all_sync(__activemask(), st.pend_count > 0);
+        if (st.pend_count > 0 && (st.node < 0 || all_hold)) {
+            if (leaf_tris<AnyHit, Count>(s, r, tmin, hit, st, st.pend_first, st.pend_count, work)) return true;
+            st.pend_count = 0;
+            if (st.node >= 0) return false;
+            return !pop_node(st, stack, hit);
+        }
+    }
+    // A tree visits each inner node at most once; the bound only guards
+    // against a malformed node array turning into an endless loop.
     if (++st.visits > s.num_nodes + 1) return true;
     const int node = st.node;
     const float4 a = __ldg(s.nodes + node * 4 + 0);
@@ -193,23 +247,10 @@ RR_D bool trace_step(const DevScene& s, const Ray& r, float tmin, HitRec& hit, T
         if (hk && child < 0) {
             const int first = ~child;
             const int count = k == 0 ? d.z : d.w;
-            for (int i = first; i < first + count; ++i) {
-                if (Count) work->tris++;
-                const float4 t0 = __ldg(s.tris + i * 3 + 0);
-                const float4 t1 = __ldg(s.tris + i * 3 + 1);
-                const float4 t2 = __ldg(s.tris + i * 3 + 2);
-                float tt, uu, vv;
-                if (intersect_triangle(r, f3(t0.x, t0.y, t0.z), f3(t0.w, t1.x, t1.y),
-                                       f3(t1.z, t1.w, t2.x), tmin, hit.t, tt, uu, vv)) {
-                    const uint32_t key = __float_as_uint(t2.w);
-                    if (AnyHit) { hit.t = tt; st.found = true; return true; }
-                    if (!st.found || tt < hit.t || (tt == hit.t && key < hit.key)) {
-                        st.found = true;
-                        hit.t = tt; hit.u = uu; hit.v = vv; hit.key = key;
-                        hit.inst = __float_as_uint(t2.y); hit.prim = __float_as_uint(t2.z);
-                    }
-                }
+            if constexpr (Postpone) {
+                if (st.pend_count == 0) { st.pend_first = first; st.pend_count = count; continue; }
             }
+            if (leaf_tris<AnyHit, Count>(s, r, tmin, hit, st, first, count, work)) return true;
         }
     }
     const bool i0 = h0 && d.x >= 0 && n0 <= hit.t;
@@ -224,10 +265,9 @@ RR_D bool trace_step(const DevScene& s, const Ray& r, float tmin, HitRec& hit, T
     } else if (i1) {
         st.node = d.y;
     } else {
-        while (st.sp > 0) {
-            --st.sp;
-            const int2 e = stack[st.sp];
-            if (__int_as_float(e.y) <= hit.t) { st.node = e.x; return false; }
+        if (pop_node(st, stack, hit)) return false;
+        if constexpr (Postpone) {
+            if (st.pend_count > 0) { st.node = -1; return false; }
         }
         return true;
     }

@@ -125,7 +125,7 @@ struct WarpPool {
 // in the scene `table[index]` (the lane binds that scene's node and triangle
 // arrays when it loads the ray); otherwise every ray is traced in `s`. Rays
 // start at t = tmin (the path tracer's 0.001).
-template <bool AnyHit, bool Count, bool Refill, bool Multi, class Load, class Finish>
+template <bool AnyHit, bool Count, bool Refill, bool Multi, bool Postpone = false, class Load, class Finish>
 __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene* __restrict__ table, uint32_t count,
                                                uint32_t* cursor, unsigned long long* work_out, Load load,
                                                Finish finish, float tmin = 0.001f) {
@@ -140,8 +140,8 @@ __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene
         }
     };
     auto step = [&](const Ray& r, HitRec& h, TravState& st) -> bool {
-        if constexpr (Multi) return trace_step<AnyHit, Count>(ls, r, tmin, h, st, stack, &tw);
-        else return trace_step<AnyHit, Count>(s, r, tmin, h, st, stack, &tw);
+        if constexpr (Multi) return trace_step<AnyHit, Count, Postpone>(ls, r, tmin, h, st, stack, &tw);
+        else return trace_step<AnyHit, Count, Postpone>(s, r, tmin, h, st, stack, &tw);
     };
     if constexpr (!Refill) {
         while (true) {
@@ -191,13 +191,13 @@ __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene
     if (Count) flush_work(tw, work_out);
 }
 
-template <bool Count, bool Refill, int MinBlocks>
+template <bool Count, bool Refill, int MinBlocks, bool Postpone = false>
 __global__ void __launch_bounds__(kBlock, MinBlocks) extend_kernel(DevScene s, const float4* __restrict__ qa,
                                                                    const float4* __restrict__ qb,
                                                                    float4* __restrict__ hits,
                                                                    const uint32_t* count_ptr, uint32_t* cursor,
                                                                    unsigned long long* work_out) {
-    traverse_queue<false, Count, Refill, false>(
+    traverse_queue<false, Count, Refill, false, Postpone>(
         s, nullptr, *count_ptr, cursor, work_out,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = qa[i], b = qb[i];
@@ -212,14 +212,14 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) extend_kernel(DevScene s, c
 }
 
 // Any-hit shadow rays; unoccluded NEE contributions are added to the image.
-template <bool Count, bool Refill, int MinBlocks>
+template <bool Count, bool Refill, int MinBlocks, bool Postpone = false>
 __global__ void __launch_bounds__(kBlock, MinBlocks) shadow_kernel(DevScene s, const float4* __restrict__ sa,
                                                                    const float4* __restrict__ sb,
                                                                    const float4* __restrict__ sc,
                                                                    float4* __restrict__ out,
                                                                    const uint32_t* count_ptr, uint32_t* cursor,
                                                                    unsigned long long* work_out) {
-    traverse_queue<true, Count, Refill, false>(
+    traverse_queue<true, Count, Refill, false, Postpone>(
         s, nullptr, *count_ptr, cursor, work_out,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = sa[i], b = sb[i];
@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(kBlock) raygen_batch_kernel(const BatchEntry* 
     qc[slot] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(sid));
 }
 
-template <bool Count, bool Refill, int MinBlocks>
+template <bool Count, bool Refill, int MinBlocks, bool Postpone = false>
 __global__ void __launch_bounds__(kBlock, MinBlocks) extend_batch_kernel(const DevScene* __restrict__ table,
                                                                          const float4* __restrict__ qa,
                                                                          const float4* __restrict__ qb,
@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) extend_batch_kernel(const D
                                                                          const uint32_t* count_ptr, uint32_t* cursor,
                                                                          unsigned long long* work_out) {
     const DevScene none{};
-    traverse_queue<false, Count, Refill, true>(
+    traverse_queue<false, Count, Refill, true, Postpone>(
         none, table, *count_ptr, cursor, work_out,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = qa[i], b = qb[i];
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) extend_batch_kernel(const D
         });
 }
 
-template <bool Count, bool Refill, int MinBlocks>
+template <bool Count, bool Refill, int MinBlocks, bool Postpone = false>
 __global__ void __launch_bounds__(kBlock, MinBlocks) shadow_batch_kernel(const DevScene* __restrict__ table,
                                                                          float4* const* __restrict__ outs,
                                                                          const float4* __restrict__ sa,
@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) shadow_batch_kernel(const D
                                                                          const uint32_t* count_ptr, uint32_t* cursor,
                                                                          unsigned long long* work_out) {
     const DevScene none{};
-    traverse_queue<true, Count, Refill, true>(
+    traverse_queue<true, Count, Refill, true, Postpone>(
         none, table, *count_ptr, cursor, work_out,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = sa[i], b = sb[i];
@@ -355,6 +355,8 @@ BatchQueueKernel extend_batch_variant(int v) {
     case 3: return extend_batch_kernel<Count, true, 1>;
     case 4: return extend_batch_kernel<Count, true, 4>;
     case 5: return extend_batch_kernel<Count, true, 6>;
+    case 6: return extend_batch_kernel<Count, false, 1, true>;
+    case 7: return extend_batch_kernel<Count, false, 4, true>;
     default: return extend_batch_kernel<Count, false, 4>;
     }
 }
@@ -366,6 +368,8 @@ BatchShadowKernel shadow_batch_variant(int v) {
     case 3: return shadow_batch_kernel<Count, true, 1>;
     case 4: return shadow_batch_kernel<Count, true, 4>;
     case 5: return shadow_batch_kernel<Count, true, 6>;
+    case 6: return shadow_batch_kernel<Count, false, 1, true>;
+    case 7: return shadow_batch_kernel<Count, false, 4, true>;
     default: return shadow_batch_kernel<Count, false, 1>;
     }
 }
@@ -383,6 +387,8 @@ QueueKernel extend_variant(int v) {
     case 3: return extend_kernel<Count, true, 1>;
     case 4: return extend_kernel<Count, true, 4>;
     case 5: return extend_kernel<Count, true, 6>;
+    case 6: return extend_kernel<Count, false, 1, true>;
+    case 7: return extend_kernel<Count, false, 4, true>;
     default: return extend_kernel<Count, false, 1>;
     }
 }
@@ -394,6 +400,8 @@ ShadowKernel shadow_variant(int v) {
     case 3: return shadow_kernel<Count, true, 1>;
     case 4: return shadow_kernel<Count, true, 4>;
     case 5: return shadow_kernel<Count, true, 6>;
+    case 6: return shadow_kernel<Count, false, 1, true>;
+    case 7: return shadow_kernel<Count, false, 4, true>;
     default: return shadow_kernel<Count, false, 1>;
     }
 }

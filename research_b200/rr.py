@@ -61,13 +61,14 @@ class PtStats(C.Structure):
 
 
 class PtTuneResult(C.Structure):
-    _fields_ = [("extend_ms", C.c_double * 6), ("shadow_ms", C.c_double * 6), ("best_extend", C.c_int),
+    _fields_ = [("extend_ms", C.c_double * 8), ("shadow_ms", C.c_double * 8), ("best_extend", C.c_int),
                 ("best_shadow", C.c_int)]
 
 
 PT_FLAG_COUNT_TRAVERSAL = 1
 PT_FLAG_TIME_STAGES = 2
 PT_FLAG_GRAPH = 4
+PT_VARIANT_COUNT = 8
 
 
 class PtParams(C.Structure):

@@ -67,7 +67,7 @@ def test_batch_tuner_and_counts(rr, ctx, torch_cuda, scenes):
     outs = [torch.empty((2, c.screen_height, c.screen_width, 4), device="cuda") for c in cams]
     ptrs = [o.data_ptr() for o in outs]
     res = b.tune(cams, rr.PtParams(3, 5, 2, 0), ptrs, _stream(torch))
-    assert 0 <= res.best_extend < 6 and 0 <= res.best_shadow < 6
+    assert 0 <= res.best_extend < rr.PT_VARIANT_COUNT and 0 <= res.best_shadow < rr.PT_VARIANT_COUNT
     assert all(t > 0 for t in res.extend_ms) and all(t > 0 for t in res.shadow_ms)
     # after tuning, graph and plain runs still match the single-scene renders
     b.execute(cams, rr.PtParams(3, 5, 2, rr.PT_FLAG_GRAPH), ptrs, _stream(torch))

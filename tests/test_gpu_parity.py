@@ -342,7 +342,7 @@ def test_traversal_variants_identical_and_tuner(rr, O, ctx, torch_cuda, procedur
     _, scene, oscene = procedural
     cam = cam_for(rr, "procedural", 80, 48)
     ref, _ = O.pathtrace(oscene, cam, 9, 5, 1)
-    for v in range(6):
+    for v in range(rr.PT_VARIANT_COUNT):
         ctx.check(rr.lib().rr_pathtracer_set_variants(ctx.handle, v, v))
         g = gpu_pathtrace(rr, ctx, scene, cam, torch, 9, 5, 1)
         np.testing.assert_array_equal(g.view(np.uint32), ref.view(np.uint32))
@@ -354,7 +354,7 @@ def test_traversal_variants_identical_and_tuner(rr, O, ctx, torch_cuda, procedur
     assert res.extend_ms[res.best_extend] == min(res.extend_ms)
     g = gpu_pathtrace(rr, ctx, scene, cam, torch, 9, 5, 1)
     np.testing.assert_array_equal(g.view(np.uint32), ref.view(np.uint32))
-    assert rr.lib().rr_pathtracer_set_variants(ctx.handle, 6, 0) == 1
+    assert rr.lib().rr_pathtracer_set_variants(ctx.handle, rr.PT_VARIANT_COUNT, 0) == 1
     ctx.check(rr.lib().rr_pathtracer_set_variants(ctx.handle, 0, 0))
 
 
