@@ -268,6 +268,14 @@ rr_status rr_atrous_execute(rr_ctx* ctx, const float* input, const float* gbuf_p
                             const float* gbuf_norm, float* ping0, float* ping1,
                             const rr_atrous_params* params, uint32_t* out_slot, void* stream);
 
+/* Strides 1, 2 and 4 run a kernel whose blocks first copy their halo tile
+ * of the three images into shared memory with TMA tensor copies (default
+ * on; the same bits as the direct-load kernel, which strides 8 and up use).
+ * rr_atrous_tma_error reports (synchronously) whether a tile's copies ever
+ * failed to complete within the kernel's bounded wait. */
+rr_status rr_atrous_set_tma(rr_ctx* ctx, int enable);
+rr_status rr_atrous_tma_error(rr_ctx* ctx, int* error_out);
+
 /* No counterpart in the reference: an A-trous entry point that allocates
  * nothing, for callers that cannot allocate device memory (an engine that
  * only lends the library buffers from its own fixed budget, a host that

@@ -4,6 +4,10 @@
 // exp(-|dp|^2/sp^2) * exp(-max(0, 1-n.n')/sn^2) * exp(-dl^2/sl^2).
 
 #include "rr_internal.h"
+#include "rr_tc.cuh"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 namespace rr {
 namespace {
@@ -66,8 +70,152 @@ __global__ void __launch_bounds__(128) atrous_kernel(const float4* __restrict__ 
     out[ci] = make_float4(o.x, o.y, o.z, crad.w);
 }
 
+// TMA-staged form of atrous_kernel for strides 1, 2 and 4: a block of 32 x 8
+// output pixels first loads its halo tile (the 5x5 taps reach 2*S pixels
+// beyond the block on every side) of radiance, position and unit normal
+// with three 3-D tensor copies (cp.async.bulk.tensor, box (4 floats,
+// 32 + 4S, 8 + 4S), started 2S pixels up-left of the block, so at negative
+// coordinates on the image's top and left edges) completing on one
+// mbarrier. A tap clamped to the image lies inside the tile, so each tap
+// reads the tile at its clamped coordinate; the box's out-of-image part
+// (zero-filled) is never read. The arithmetic is atrous_kernel's, on the
+// same values: the results are the same bits.
+template <int S>
+struct AtrousTile {
+    static constexpr int W = 32 + 4 * S, H = 8 + 4 * S;
+    static constexpr uint32_t kBytes = uint32_t(W * H * 16);   // one image's box
+    static constexpr uint32_t kSmem = 3 * kBytes + 16;
+    static_assert(kBytes % 128 == 0, "tiles stay 128-byte aligned");
+};
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(tc::smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2),
+          "r"(tc::smem_addr(bar))
+        : "memory");
+}
+
+template <int S>
+__global__ void __launch_bounds__(256) atrous_tma_kernel(const __grid_constant__ CUtensorMap m_rad,
+                                                         const __grid_constant__ CUtensorMap m_pos,
+                                                         const __grid_constant__ CUtensorMap m_nrm,
+                                                         float4* __restrict__ out, int W, int H, float sp2,
+                                                         float sn2, float sl2, int* error) {
+    using T = AtrousTile<S>;
+    extern __shared__ __align__(128) unsigned char sm[];
+    const float4* t_rad = reinterpret_cast<const float4*>(sm);
+    const float4* t_pos = t_rad + T::W * T::H;
+    const float4* t_nrm = t_pos + T::W * T::H;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 3 * T::kBytes);
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8;
+    const int tx0 = x0 - 2 * S, ty0 = y0 - 2 * S;
+    if (threadIdx.x == 0) {
+        tc::mbar_init(bar, 1);
+        tc::fence_proxy_async();
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_addr(bar)),
+                     "r"(3 * T::kBytes)
+                     : "memory");
+        tma_load_3d(sm, &m_rad, 0, tx0, ty0, bar);
+        tma_load_3d(sm + T::kBytes, &m_pos, 0, tx0, ty0, bar);
+        tma_load_3d(sm + 2 * T::kBytes, &m_nrm, 0, tx0, ty0, bar);
+    }
+    __syncthreads();
+    if (!tc::mbar_wait(bar, 0)) {
+        // the copies never completed: report, give them one more bounded
+        // wait so that none is left writing this block's memory, and leave
+        if (threadIdx.x == 0) atomicExch(error, 1);
+        tc::mbar_wait(bar, 0);
+        return;
+    }
+    const int x = x0 + int(threadIdx.x & 31u), y = y0 + int(threadIdx.x >> 5);
+    if (x >= W || y >= H) return;
+    const size_t ci = size_t(y) * W + x;
+    const int cl_i = (y - ty0) * T::W + (x - tx0);
+    const float4 cpos = t_pos[cl_i];
+    const float4 crad = t_rad[cl_i];
+    if (cpos.w < 0.0f) { out[ci] = crad; return; }
+    const float3 cn = xyz(t_nrm[cl_i]);
+    const float cl = luminance601(xyz(crad));
+    float3 filtered = f3(0.0f, 0.0f, 0.0f);
+    float wsum = 0.0f;
+    #pragma unroll
+    for (int ty = -2; ty <= 2; ++ty) {
+        const int sy = min(max(y + ty * S, 0), H - 1);
+        #pragma unroll
+        for (int tx = -2; tx <= 2; ++tx) {
+            const int sx = min(max(x + tx * S, 0), W - 1);
+            const int si = (sy - ty0) * T::W + (sx - tx0);
+            const float4 spos = t_pos[si];
+            if (spos.w < 0.0f) continue;
+            const float base_w = (kernel_weight(tx) * kernel_weight(ty)) / 256.0f;
+            const float3 pd = xyz(spos) - xyz(cpos);
+            const float pos_w = rr_expf(-dot(pd, pd) / sp2);
+            const float3 sn = xyz(t_nrm[si]);
+            const float nd = mx(0.0f, 1.0f - dot(cn, sn));
+            const float normal_w = rr_expf(-nd / sn2);
+            const float3 srad = xyz(t_rad[si]);
+            const float ld = luminance601(srad) - cl;
+            const float luma_w = rr_expf(-(ld * ld) / sl2);
+            const float w = base_w * pos_w * normal_w * luma_w;
+            filtered = filtered + srad * w;
+            wsum += w;
+        }
+    }
+    const float3 o = wsum > 0.0f ? filtered / wsum : xyz(crad);
+    out[ci] = make_float4(o.x, o.y, o.z, crad.w);
+}
+
 } // namespace
 } // namespace rr
+
+// cuTensorMapEncodeTiled from the driver (no link-time dependency on it).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// A W x H RGBA32F image as a 3-D tensor (4 floats, W, H) with a box of
+// (4, bw, bh); false if the driver refuses it (the caller then uses the
+// direct-load kernel).
+static bool image_map(CUtensorMap* m, const void* img, uint32_t W, uint32_t H, uint32_t bw, uint32_t bh) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || (reinterpret_cast<uintptr_t>(img) & 15u) != 0) return false;
+    const cuuint64_t dims[3] = {4, W, H};
+    const cuuint64_t strides[2] = {16, cuuint64_t(W) * 16};
+    const cuuint32_t box[3] = {4, bw, bh};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(img), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int S>
+static bool atrous_tma_launch(rr_ctx* ctx, const float* input, const float* gpos, const float4* nrm, float* output,
+                              uint32_t W, uint32_t H, float sp2, float sn2, float sl2, cudaStream_t stream) {
+    using T = rr::AtrousTile<S>;
+    CUtensorMap mr, mp, mn;
+    if (!image_map(&mr, input, W, H, T::W, T::H) || !image_map(&mp, gpos, W, H, T::W, T::H) ||
+        !image_map(&mn, nrm, W, H, T::W, T::H))
+        return false;
+    if (cudaFuncSetAttribute(rr::atrous_tma_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, T::kSmem) !=
+        cudaSuccess)
+        return false;
+    const dim3 grid((W + 31) / 32, (H + 7) / 8);
+    rr::atrous_tma_kernel<S><<<grid, 256, T::kSmem, stream>>>(mr, mp, mn, reinterpret_cast<float4*>(output), int(W),
+                                                              int(H), sp2, sn2, sl2, ctx->atrous_error);
+    return true;
+}
 
 // Unit normals of `gnrm` into the context's scratch image.
 static rr_status atrous_normals(rr_ctx* ctx, const float* gnrm, uint32_t W, uint32_t H, cudaStream_t stream,
@@ -92,6 +240,21 @@ static rr_status atrous_launch(rr_ctx* ctx, const float* input, const float* gpo
                                float* output, uint32_t W, uint32_t H, uint32_t stride, float sp, float sn,
                                float sl, cudaStream_t stream) {
     const float sp2 = std::max(sp * sp, 1.0e-6f), sn2 = std::max(sn * sn, 1.0e-6f), sl2 = std::max(sl * sl, 1.0e-6f);
+    if (ctx->atrous_tma && (stride == 1 || stride == 2 || stride == 4)) {
+        if (!ctx->atrous_error) {
+            RR_TRY_CUDA(ctx, cudaMalloc(&ctx->atrous_error, sizeof(int)));
+            RR_TRY_CUDA(ctx, cudaMemset(ctx->atrous_error, 0, sizeof(int)));
+        }
+        bool launched = false;
+        if (stride == 1) launched = atrous_tma_launch<1>(ctx, input, gpos, nrm, output, W, H, sp2, sn2, sl2, stream);
+        else if (stride == 2) launched = atrous_tma_launch<2>(ctx, input, gpos, nrm, output, W, H, sp2, sn2, sl2, stream);
+        else launched = atrous_tma_launch<4>(ctx, input, gpos, nrm, output, W, H, sp2, sn2, sl2, stream);
+        if (launched) {
+            RR_CHECK_LAUNCH(ctx);
+            ctx->launches += 1;
+            return RR_OK;
+        }
+    }
     dim3 grid((W + 15) / 16, (H + 7) / 8);
     rr::atrous_kernel<<<grid, 128, 0, stream>>>(
         reinterpret_cast<const float4*>(input), reinterpret_cast<const float4*>(gpos), nrm,
@@ -144,5 +307,20 @@ extern "C" rr_status rr_atrous_execute(rr_ctx* ctx, const float* input, const fl
         read = write;
     }
     if (out_slot) *out_slot = (iters - 1u) & 1u;
+    return RR_OK;
+}
+
+extern "C" rr_status rr_atrous_set_tma(rr_ctx* ctx, int enable) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    ctx->atrous_tma = enable != 0;
+    return RR_OK;
+}
+
+extern "C" rr_status rr_atrous_tma_error(rr_ctx* ctx, int* error_out) {
+    if (!ctx || !error_out) return RR_ERR_INVALID_ARGUMENT;
+    *error_out = 0;
+    if (!ctx->atrous_error) return RR_OK;
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    RR_TRY_CUDA(ctx, cudaMemcpy(error_out, ctx->atrous_error, sizeof(int), cudaMemcpyDeviceToHost));
     return RR_OK;
 }

@@ -58,6 +58,8 @@ struct rr_ctx {
     double* mse_partial = nullptr;         // rr_image_mse block partials
     float4* atrous_nrm = nullptr;          // A-trous: the G-buffer normals, normalized once per call
     size_t atrous_nrm_px = 0;
+    bool atrous_tma = true;                // strides 1, 2, 4 through TMA-staged tiles
+    int* atrous_error = nullptr;           // set when a tile's copies never completed
     // The path tracer traces bounce b's shadow rays on a second stream while
     // bounce b+1's extension rays run on the caller's (fork after shade b,
     // join before shade b+1); created on first use.

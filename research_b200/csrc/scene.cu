@@ -89,6 +89,7 @@ rr_status rr_ctx_destroy(rr_ctx* ctx) {
     cudaFree(ctx->work64);
     cudaFree(ctx->mse_partial);
     cudaFree(ctx->atrous_nrm);
+    cudaFree(ctx->atrous_error);
     for (int b = 0; b < kMaxBounces; ++b) {
         if (ctx->shaded[b]) cudaEventDestroy(ctx->shaded[b]);
         if (ctx->shadowed[b]) cudaEventDestroy(ctx->shadowed[b]);

@@ -196,6 +196,8 @@ _SIGNATURES = {
     "rr_pathtracer_set_variants": (I, [P, I, I]),
     "rr_pathtracer_set_overlap": (I, [P, I]),
     "rr_reuse_set_wavefront": (I, [P, I]),
+    "rr_atrous_set_tma": (I, [P, I]),
+    "rr_atrous_tma_error": (I, [P, C.POINTER(C.c_int)]),
     "rr_pathtracer_tune": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtParams), P, P, C.POINTER(PtTuneResult)]),
     "rr_accumulate_execute": (I, [P, P, U32, P, P, C.POINTER(AccParams), P]),
     "rr_restir_di_initial": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(DIParams), P, P, P, P]),
