@@ -16,6 +16,10 @@
  *  - `stream` is a cudaStream_t (NULL = legacy default stream). Execute calls
  *    only enqueue work; they do not synchronise.
  *  - The library owns the scene (geometry, BVH) and the wavefront queues.
+ *    Calls that use a context's queues (the path tracers, batches, the
+ *    ReSTIR PT / GI initial passes) must follow one another on one stream;
+ *    ReSTIR DI, accumulate and A-trous use none and may run beside them on
+ *    another stream.
  *  - Camera data is passed by host pointer (GpuCameraData, 304 bytes,
  *    GpuScene.h:80-98) and reaches the kernels as a launch parameter.
  */
