@@ -1106,6 +1106,13 @@ static rr_status enqueue_guided_batch(rr_ctx* ctx, rr_batch* B, rr_guide* const*
     GuidedLaunch G{};
     G.lobes = kMaxLobes;
     G.mix = mlp ? B->mix : nullptr;
+    // shadow rays of bounce b beside bounce b+1's extension rays (and MLP
+    // inference), as in rr_pathtracer_execute; the next shade stage waits
+    const bool overlap = ctx->overlap_shadow;
+    if (overlap) {
+        const rr_status so = ensure_side(ctx);
+        if (so != RR_OK) return so;
+    }
     for (uint32_t b = 0; b < max_bounces; ++b) {
         const int cur = b & 1, nxt = cur ^ 1;
         uint32_t* cb = C + 4 * b;
@@ -1126,16 +1133,25 @@ static rr_status enqueue_guided_batch(rr_ctx* ctx, rr_batch* B, rr_guide* const*
             if (st != RR_OK) return st;
             launches += 3;
         }
+        if (overlap && b > 0) RR_TRY_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->shadowed[b - 1], 0));
         shade_k<<<g_shade, kBlock, 0, stream>>>(DevScene{}, G, B->d_table, outs, gtab, B->slot_map, q.ray_a[cur],
                                                 q.ray_b[cur], q.ray_c[cur], q.hits, q.ray_a[nxt], q.ray_b[nxt],
                                                 q.ray_c[nxt], q.shadow_a, q.shadow_b, q.shadow_c, nullptr, cb, cn,
                                                 cb + 2);
         RR_CHECK_LAUNCH(ctx);
-        sh_k<<<g_sh, kBlock, 0, stream>>>(B->d_table, outs, q.shadow_a, q.shadow_b, q.shadow_c, cb + 2, cb + 3,
-                                          ctx->work64 + 2);
+        cudaStream_t sh_stream = stream;
+        if (overlap) {
+            RR_TRY_CUDA(ctx, cudaEventRecord(ctx->shaded[b], stream));
+            RR_TRY_CUDA(ctx, cudaStreamWaitEvent(ctx->side, ctx->shaded[b], 0));
+            sh_stream = ctx->side;
+        }
+        sh_k<<<g_sh, kBlock, 0, sh_stream>>>(B->d_table, outs, q.shadow_a, q.shadow_b, q.shadow_c, cb + 2, cb + 3,
+                                             ctx->work64 + 2);
         RR_CHECK_LAUNCH(ctx);
+        if (overlap) RR_TRY_CUDA(ctx, cudaEventRecord(ctx->shadowed[b], ctx->side));
         launches += 3;
     }
+    if (overlap) RR_TRY_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->shadowed[max_bounces - 1], 0));
     if (max_bounces > 1) {
         resolve_batch_kernel<<<std::max(1, ctx->sm_count * 8), kBlock, 0, stream>>>(gtab, outs, rec_prefix, count);
         RR_CHECK_LAUNCH(ctx);
@@ -1182,6 +1198,8 @@ extern "C" rr_status rr_batch_execute_guided(rr_ctx* ctx, rr_batch* B, const Gpu
     uint64_t paths = 0;
     rr_status st = rr_batch_stage_call(ctx, B, cams, p, radiance_out, stream, &tiles, &paths);
     if (st != RR_OK) return st;
+    // the overlap's stream and events exist before any graph capture starts
+    if (ctx->overlap_shadow && (st = ensure_side(ctx)) != RR_OK) return st;
     const bool mlp = kind == RR_GUIDE_MLP;
     if ((st = ensure_batch_guided(ctx, B, size_t(paths), mlp)) != RR_OK) return st;
     for (uint32_t i = 0; i < count; ++i)
@@ -1226,6 +1244,7 @@ extern "C" rr_status rr_batch_execute_guided(rr_ctx* ctx, rr_batch* B, const Gpu
                                         reinterpret_cast<const void*>(uintptr_t(p->max_bounces)),
                                         reinterpret_cast<const void*>(uintptr_t(ctx->extend_variant)),
                                         reinterpret_cast<const void*>(uintptr_t(ctx->shadow_variant)),
+                                        reinterpret_cast<const void*>(uintptr_t(ctx->overlap_shadow)),
                                         ctx->pt.ray_a[0], B->surf};
         for (uint32_t i = 0; i < count; ++i) {
             key.push_back(guides[i]);

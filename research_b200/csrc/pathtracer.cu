@@ -387,6 +387,13 @@ rr_status enqueue_batch(rr_ctx* ctx, rr_batch* B, uint32_t total_tiles, size_t n
                                       int((n + kBlock - 1) / kBlock));
     if (count) RR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->work64, 0, sizeof(unsigned long long) * 4, stream));
     rr_stage_timer timer(ctx, stream, timed);
+    // shadow rays of bounce b beside the extension rays of bounce b+1, as in
+    // rr_pathtracer_execute (stage timing keeps one stream)
+    const bool overlap = ctx->overlap_shadow && !timed;
+    if (overlap) {
+        const rr_status so = ensure_side(ctx);
+        if (so != RR_OK) return so;
+    }
     for (uint32_t b = 0; b < max_bounces; ++b) {
         const int cur = b & 1, nxt = cur ^ 1;
         uint32_t* cb = C + 4 * b;
@@ -396,6 +403,7 @@ rr_status enqueue_batch(rr_ctx* ctx, rr_batch* B, uint32_t total_tiles, size_t n
                                             ctx->work64);
         RR_CHECK_LAUNCH(ctx);
         timer.end(1);
+        if (overlap && b > 0) RR_TRY_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->shadowed[b - 1], 0));
         timer.begin(2);
         shade_kernel<true><<<g_shade, kBlock, 0, stream>>>(DevScene{}, B->d_table, outs, b,
                                                            b + 1 == max_bounces ? 1u : 0u, q.ray_a[cur],
@@ -404,12 +412,20 @@ rr_status enqueue_batch(rr_ctx* ctx, rr_batch* B, uint32_t total_tiles, size_t n
                                                            q.shadow_c, nullptr, cb, cn, cb + 2);
         RR_CHECK_LAUNCH(ctx);
         timer.end(2);
+        cudaStream_t sh_stream = stream;
+        if (overlap) {
+            RR_TRY_CUDA(ctx, cudaEventRecord(ctx->shaded[b], stream));
+            RR_TRY_CUDA(ctx, cudaStreamWaitEvent(ctx->side, ctx->shaded[b], 0));
+            sh_stream = ctx->side;
+        }
         timer.begin(3);
-        sh_k<<<g_sh, kBlock, 0, stream>>>(B->d_table, outs, q.shadow_a, q.shadow_b, q.shadow_c, cb + 2, cb + 3,
-                                          ctx->work64 + 2);
+        sh_k<<<g_sh, kBlock, 0, sh_stream>>>(B->d_table, outs, q.shadow_a, q.shadow_b, q.shadow_c, cb + 2, cb + 3,
+                                             ctx->work64 + 2);
         RR_CHECK_LAUNCH(ctx);
         timer.end(3);
+        if (overlap) RR_TRY_CUDA(ctx, cudaEventRecord(ctx->shadowed[b], ctx->side));
     }
+    if (overlap && max_bounces > 0) RR_TRY_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->shadowed[max_bounces - 1], 0));
     return timer.commit();
 }
 
@@ -524,11 +540,14 @@ extern "C" rr_status rr_batch_execute(rr_ctx* ctx, rr_batch* B, const GpuCameraD
     uint64_t paths = 0;
     rr_status st = rr_batch_stage_call(ctx, B, cams, p, radiance_out, stream, &tiles, &paths);
     if (st != RR_OK) return st;
+    // the overlap's stream and events exist before any graph capture starts
+    if (ctx->overlap_shadow && (st = ensure_side(ctx)) != RR_OK) return st;
     if (graph) {
         rr_batch::Key key;
         key.paths = paths; key.total_tiles = tiles; key.max_bounces = p->max_bounces;
         key.ev = uint32_t(ctx->extend_variant); key.sv = uint32_t(ctx->shadow_variant);
         key.queue = ctx->pt.ray_a[0];
+        key.overlap = ctx->overlap_shadow;
         if (!B->exec || key != B->key) {
             if (B->exec) { cudaGraphExecDestroy(B->exec); B->exec = nullptr; }
             RR_TRY_CUDA(ctx, cudaStreamBeginCapture(B->cap_stream, cudaStreamCaptureModeThreadLocal));

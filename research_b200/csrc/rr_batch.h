@@ -26,9 +26,10 @@ struct rr_batch {
         uint64_t paths = 0;
         uint32_t total_tiles = 0, max_bounces = 0, ev = 0, sv = 0;
         const void* queue = nullptr;
+        bool overlap = false;
         bool operator!=(const Key& o) const {
             return paths != o.paths || total_tiles != o.total_tiles || max_bounces != o.max_bounces || ev != o.ev ||
-                   sv != o.sv || queue != o.queue;
+                   sv != o.sv || queue != o.queue || overlap != o.overlap;
         }
     } key;
 
