@@ -145,13 +145,15 @@ rr_status rr_pathtracer_stats(rr_ctx* ctx, rr_pt_stats* out, int reset_times);
 #define RR_PT_VARIANT_COUNT 8
 rr_status rr_pathtracer_set_variants(rr_ctx* ctx, int extend_variant, int shadow_variant);
 
-/* Shadow overlap (default on): rr_pathtracer_execute traces bounce b's
- * shadow rays on a second stream of the context while bounce b+1's
- * extension rays run on the caller's stream; the next shade stage waits for
- * both, and the call's work is joined back into the caller's stream before it
- * returns (so CUDA-graph capture of the caller's stream still works). Results
- * are identical either way. Calls with RR_PT_FLAG_TIME_STAGES run on one
- * stream, so that each stage is timed alone. */
+/* Shadow overlap (default on): the path tracers (rr_pathtracer_execute,
+ * rr_guided_pathtracer_execute, rr_batch_execute, rr_batch_execute_guided)
+ * trace bounce b's shadow rays on a second stream of the context while
+ * bounce b+1's extension rays run on the caller's stream; the next shade
+ * stage waits for both, and the call's work is joined back into the caller's
+ * stream before it returns (so CUDA-graph capture of the caller's stream
+ * still works). Results are identical either way. Calls with
+ * RR_PT_FLAG_TIME_STAGES run on one stream, so that each stage is timed
+ * alone. */
 rr_status rr_pathtracer_set_overlap(rr_ctx* ctx, int enable);
 
 /* Autotuner: renders the given frame once per variant with stage timing,

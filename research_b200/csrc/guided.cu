@@ -820,6 +820,11 @@ extern "C" rr_status rr_guided_pathtracer_execute(rr_ctx* ctx, const rr_scene* s
     G.rec0 = g->rec[0]; G.rec1 = g->rec[1]; G.rec2 = g->rec[2]; G.rec3 = g->rec[3];
     const DevScene& S = scene->dev;
     uint64_t launches = 1;
+    // shadow rays of bounce b beside bounce b+1's extension rays (and MLP
+    // inference), as in rr_pathtracer_execute; the next shade stage, which
+    // reads and writes the image, waits for them
+    const bool overlap = ctx->overlap_shadow;
+    if (overlap && (st = ensure_side(ctx)) != RR_OK) return st;
     for (uint32_t b = 0; b < p->max_bounces; ++b) {
         const int cur = b & 1, nxt = cur ^ 1;
         uint32_t* cb = C + 4 * b;
@@ -834,15 +839,25 @@ extern "C" rr_status rr_guided_pathtracer_execute(rr_ctx* ctx, const rr_scene* s
             if ((st = rr_mlp_guide_infer(ctx, g, cb, uint32_t(n), stream)) != RR_OK) return st;
             launches += 1 + g->mlp_infer_launches;
         }
+        if (overlap && b > 0) RR_TRY_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->shadowed[b - 1], 0));
         shade_k<<<g_shade, kBlock, 0, stream>>>(S, G, nullptr, nullptr, nullptr, nullptr, q.ray_a[cur], q.ray_b[cur],
                                                 q.ray_c[cur], q.hits,
                                                 q.ray_a[nxt], q.ray_b[nxt], q.ray_c[nxt], q.shadow_a, q.shadow_b,
                                                 q.shadow_c, out, cb, cn, cb + 2);
         RR_CHECK_LAUNCH(ctx);
-        sh_k<<<g_sh, kBlock, 0, stream>>>(S, q.shadow_a, q.shadow_b, q.shadow_c, out, cb + 2, cb + 3, ctx->work64 + 2);
+        cudaStream_t sh_stream = stream;
+        if (overlap) {
+            RR_TRY_CUDA(ctx, cudaEventRecord(ctx->shaded[b], stream));
+            RR_TRY_CUDA(ctx, cudaStreamWaitEvent(ctx->side, ctx->shaded[b], 0));
+            sh_stream = ctx->side;
+        }
+        sh_k<<<g_sh, kBlock, 0, sh_stream>>>(S, q.shadow_a, q.shadow_b, q.shadow_c, out, cb + 2, cb + 3,
+                                             ctx->work64 + 2);
         RR_CHECK_LAUNCH(ctx);
+        if (overlap) RR_TRY_CUDA(ctx, cudaEventRecord(ctx->shadowed[b], ctx->side));
         launches += 3;
     }
+    if (overlap) RR_TRY_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->shadowed[p->max_bounces - 1], 0));
     if (p->max_bounces > 1) {
         resolve_kernel<<<std::max(1, ctx->sm_count * 8), kBlock, 0, stream>>>(
             out, g->rec[0], g->rec[1], g->rec[2], g->rec[3], uint32_t(n), p->max_bounces - 1, g->samples);

@@ -317,6 +317,35 @@ def test_guided_pathtracer_is_unbiased(rr, ctx, torch_cuda, kind):
     scene.close()
 
 
+@pytest.mark.parametrize("kind", ["grid", "mlp"])
+def test_guided_shadow_overlap_is_bit_identical(rr, ctx, torch_cuda, kind):
+    """The guided tracer with each bounce's shadow rays beside the next
+    bounce's extension rays (the default) renders the same bits as with one
+    stream, for a trained grid and a (fixed) MLP guide."""
+    torch = torch_cuda
+    L = rr.lib()
+    hs = rr.HostScene.procedural(target_triangles=40_000, emissive_triangles=64, box_half=20.0)
+    scene = rr.Scene(ctx, hs.arrays)
+    cam = rr.camera_data(rr.camera_desc(160, 96, eye=(0.0, 4.0, 34.0), center=(0.0, -3.0, 0.0)))
+    g = make_guide(rr, ctx, rr.GUIDE_GRID if kind == "grid" else rr.GUIDE_MLP, bmin=(-21.0,) * 3, bmax=(21.0,) * 3,
+                   res=16, batch=1 << 14, max_samples=1 << 18)
+    _render(rr, ctx, torch, scene, cam, 2, guide=g, train=True, spp=2)
+    imgs = []
+    for overlap in (1, 0):
+        ctx.check(L.rr_pathtracer_set_overlap(ctx.handle, overlap))
+        out = torch.empty((4, 96, 160, 4), device="cuda")
+        p = rr.PtParams(77, 5, 4, 0)
+        ctx.check(L.rr_guided_pathtracer_execute(ctx.handle, scene.handle, C.byref(cam), C.byref(p), g,
+                                                 out.data_ptr(), _stream(torch)))
+        torch.cuda.synchronize()
+        imgs.append(out.cpu().numpy())
+    ctx.check(L.rr_pathtracer_set_overlap(ctx.handle, 1))
+    assert np.array_equal(imgs[0].view(np.uint32), imgs[1].view(np.uint32))
+    assert imgs[0][..., :3].mean() > 0
+    L.rr_guide_destroy(g)
+    scene.close()
+
+
 def _frame_variance(rr, ctx, torch, scene, cam, frames, spp, guide=None, seed0=5000):
     """Mean over pixels of the variance between frame images (spp each), and
     the mean image."""
