@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--triangles", type=int, default=CFG["triangles"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
+    ap.add_argument("--variants", default=None,
+                    help="E,S: traversal variants for extension and shadow rays instead of the autotuner's choice "
+                         "(profilers distort the tuner's timings)")
     ap.add_argument("--serial-passes", action="store_true",
                     help="run ReSTIR DI and A-trous after the path tracer on one stream")
     return ap.parse_args()
@@ -339,12 +342,18 @@ def run_ours(args, ws, rank, local):
 
     st = rr.PtStats()
     # autotune the traversal variants on this scene and frame (setup, untimed)
-    tune = rr.PtTuneResult()
-    ctx.check(rr.lib().rr_pathtracer_tune(ctx.handle, scene.handle, C.byref(fr.cam),
-                                          C.byref(rr.PtParams(seed_base, CFG["max_bounces"], CFG["spp"], 0)),
-                                          fr.rad.data_ptr(), stream, C.byref(tune)))
-    tuned = {"extend_variant": tune.best_extend, "shadow_variant": tune.best_shadow,
-             "extend_ms": [round(x, 3) for x in tune.extend_ms], "shadow_ms": [round(x, 3) for x in tune.shadow_ms]}
+    if args.variants:
+        ev, sv = (int(x) for x in args.variants.split(","))
+        ctx.check(rr.lib().rr_pathtracer_set_variants(ctx.handle, ev, sv))
+        tuned = {"extend_variant": ev, "shadow_variant": sv, "fixed": True}
+    else:
+        tune = rr.PtTuneResult()
+        ctx.check(rr.lib().rr_pathtracer_tune(ctx.handle, scene.handle, C.byref(fr.cam),
+                                              C.byref(rr.PtParams(seed_base, CFG["max_bounces"], CFG["spp"], 0)),
+                                              fr.rad.data_ptr(), stream, C.byref(tune)))
+        tuned = {"extend_variant": tune.best_extend, "shadow_variant": tune.best_shadow,
+                 "extend_ms": [round(x, 3) for x in tune.extend_ms],
+                 "shadow_ms": [round(x, 3) for x in tune.shadow_ms]}
     clocks = ClockSampler(torch.cuda.get_device_properties(local).uuid)
     clocks.start()
     # 1) warm-up
