@@ -433,6 +433,34 @@ def test_shadow_overlap_is_bit_identical(rr, O, ctx, torch_cuda, procedural):
         np.testing.assert_array_equal(outs[name].view(np.uint32), outs["serial"].view(np.uint32), err_msg=name)
 
 
+def test_pathtracer_in_a_captured_cuda_graph(rr, O, ctx, torch_cuda, procedural):
+    """rr_pathtracer_execute captured into a CUDA graph on the caller's stream
+    (the shadow overlap forks to the context's second stream and joins back
+    inside the capture) replays to the same bits as a direct call."""
+    torch = torch_cuda
+    L = rr.lib()
+    _, scene, _ = procedural
+    cam = cam_for(rr, "procedural", 160, 96)
+    ctx.check(L.rr_pathtracer_set_overlap(ctx.handle, 1))
+    direct = gpu_pathtrace(rr, ctx, scene, cam, torch, 31, 5, 2)       # also sizes the queues
+    out = torch.full((2, 96, 160, 4), -1.0, device="cuda")
+    p = rr.PtParams(31, 5, 2, 0)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(side):
+        with torch.cuda.graph(graph, stream=side):
+            ctx.check(L.rr_pathtracer_execute(ctx.handle, scene.handle, C.byref(cam), C.byref(p), out.data_ptr(),
+                                              side.cuda_stream))
+    torch.cuda.current_stream().wait_stream(side)
+    for _ in range(2):
+        out.fill_(-1.0)
+        graph.replay()
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(_np(out).view(np.uint32), direct.view(np.uint32))
+    del graph
+
+
 def _edge_scenes(rr):
     """Cornell variants: a directional plus a point light (the MIS branch of
     the light sample and of ReSTIR DI's target), no lights at all, and all
