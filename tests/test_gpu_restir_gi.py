@@ -126,6 +126,15 @@ def test_restir_gi_options_bit_exact(rr, O, ctx, torch_cuda):
          temporal=0, spatial=0, include_direct=0, candidates=3, ray_bias=2e-3, indirect_strength=0.5)
 
 
+@pytest.mark.parametrize("candidates", [0, 1])
+def test_restir_gi_few_candidates_bit_exact(rr, O, ctx, torch_cuda, initial_form, candidates):
+    """No candidate at all (zero wavefront steps) and a single one."""
+    torch = torch_cuda
+    hs = rr.HostScene.cornell(0)
+    _run(rr, O, ctx, torch, hs.arrays, 24, 16, 2, (0.0, 0.0, 3.0), (0.0, 0.0, 0.0), (0.002, 0.0, -0.01),
+         candidates=candidates)
+
+
 def test_restir_gi_execute_matches_dispatches(rr, ctx, torch_cuda):
     """rr_restir_gi_execute is the three dispatches in order."""
     torch = torch_cuda
@@ -196,9 +205,11 @@ def test_restir_gi_rejects_null_images(rr, ctx, torch_cuda):
     scene.close()
 
 
-@pytest.mark.parametrize("name", ["directional", "no_lights"])
+@pytest.mark.parametrize("name", ["directional", "no_lights", "no_geometry"])
 def test_restir_gi_light_edge_cases_bit_exact(rr, O, ctx, torch_cuda, name):
-    """The light sample's directional (MIS) branch and a scene without lights."""
+    """The light sample's directional (MIS) branch, a scene without lights, and
+    a view without geometry (no pixel has a surface: the wavefront's first
+    launch finishes every pixel and its steps find empty queues)."""
     import test_gpu_parity
     arrays = test_gpu_parity._edge_scenes(rr)[name]
     _run(rr, O, ctx, torch_cuda, arrays, 32, 24, 2, (0.0, 0.0, 3.0), (0.0, 0.0, 0.0), (0.003, 0.0, -0.01))

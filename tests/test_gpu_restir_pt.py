@@ -153,6 +153,16 @@ def test_restir_pt_deep_paths_bit_exact(rr, O, ctx, torch_cuda):
     assert s["valid"] > 0.5
 
 
+@pytest.mark.parametrize("candidates,bounces", [(0, 4), (1, 0), (2, 1)])
+def test_restir_pt_few_candidates_bit_exact(rr, O, ctx, torch_cuda, initial_form, candidates, bounces):
+    """No candidate at all (zero wavefront steps), max_bounces 0 (treated as
+    one segment), one bounce."""
+    torch = torch_cuda
+    hs = rr.HostScene.cornell(0)
+    _run(rr, O, ctx, torch, hs.arrays, 24, 16, 2, (0.0, 0.0, 3.0), (0.0, 0.0, 0.0), (0.002, 0.0, -0.01),
+         candidates=candidates, max_bounces=bounces)
+
+
 def test_restir_pt_reset_history(rr, ctx, torch_cuda):
     torch = torch_cuda
     W, H = 8, 4
@@ -168,9 +178,11 @@ def test_restir_pt_reset_history(rr, ctx, torch_cuda):
     assert (bufs[4][..., :3] == 0).all() and (bufs[4][..., 3] == -1).all() and (bufs[5] == 0).all()
 
 
-@pytest.mark.parametrize("name", ["directional", "no_lights"])
+@pytest.mark.parametrize("name", ["directional", "no_lights", "no_geometry"])
 def test_restir_pt_light_edge_cases_bit_exact(rr, O, ctx, torch_cuda, name):
-    """The light sample's directional (MIS) branch and a scene without lights."""
+    """The light sample's directional (MIS) branch, a scene without lights, and
+    a view without geometry (no pixel has a surface: the wavefront's first
+    launch finishes every pixel and its steps find empty queues)."""
     import test_gpu_parity
     arrays = test_gpu_parity._edge_scenes(rr)[name]
     _run(rr, O, ctx, torch_cuda, arrays, 32, 24, 2, (0.0, 0.0, 3.0), (0.0, 0.0, 0.0), (0.003, 0.0, -0.01))
