@@ -1,12 +1,14 @@
 """Config 4 on one B200: 64 independent seeded scenes of the config-2 kind
 (procedural rooms) with triangle counts log-uniform in [10k, 500k] and square
 images with pixel counts log-uniform in [256^2, 1024^2], 8 spp each, depth 5.
-All scenes are rendered by one batch (rr_batch_execute: one raygen and, per
-bounce, one extend, one shade and one shadow launch for all scenes),
-replayed from a captured CUDA graph, with traversal variants picked by the
-batch autotuner. Reported beside it: the same batch without the graph, and
-the scenes rendered one rr_pathtracer_execute call after another, and the
-same three forms at small images (128^2, 1 spp: the launch-bound regime).
+All scenes are rendered by one batch call (rr_batch_execute) in the form
+the batch autotuner picked with the traversal variants: one set of wavefront
+launches for all scenes (one raygen and, per bounce, one extend, one shade
+and one shadow launch), replayed from a captured CUDA graph, or the scenes
+one after another. Reported beside it: the wavefront form with and without
+the graph, the scenes rendered one rr_pathtracer_execute call after another,
+and the same forms at small images (128^2, 1 spp: the launch-bound regime,
+tuned again).
 Then guiding per scene (rr_batch_execute_guided): every scene gets its own
 guide (a 32^3 vMF grid, or its own BF16 MLP run by one grouped tensor-core
 launch per bounce for all scenes), the 8 spp are rendered as frames of
@@ -87,6 +89,11 @@ def main():
             ms += ev0.elapsed_time(ev1)
         return ms / args.frames
 
+    mode_names = {rr.BATCH_WAVEFRONT: "wavefront", rr.BATCH_PER_SCENE: "per_scene"}
+    tuned_mode = batch.mode
+    ms_tuned = timed(lambda seed: batch.execute(cams, rr.PtParams(seed, args.bounces, args.spp, rr.PT_FLAG_GRAPH),
+                                                ptrs, st))
+    batch.set_mode(rr.BATCH_WAVEFRONT)
     ms_graph = timed(lambda seed: batch.execute(cams, rr.PtParams(seed, args.bounces, args.spp, rr.PT_FLAG_GRAPH),
                                                 ptrs, st))
     ms_plain = timed(lambda seed: batch.execute(cams, rr.PtParams(seed, args.bounces, args.spp, 0), ptrs, st))
@@ -106,7 +113,13 @@ def main():
     sm_outs = [torch.empty((args.small_spp, args.small_side, args.small_side, 4), device="cuda") for _ in scenes]
     sm_ptrs = [o.data_ptr() for o in sm_outs]
     sm_paths = args.scenes * args.small_side * args.small_side * args.small_spp
-    sm = {}
+    sm_tune = batch.tune(sm_cams, rr.PtParams(0, args.bounces, args.small_spp, 0), sm_ptrs, st)
+    sm = {"autotune": {"mode": mode_names[batch.mode], "best_extend": sm_tune.best_extend,
+                       "best_shadow": sm_tune.best_shadow}}
+    ms = timed(lambda seed: batch.execute(sm_cams, rr.PtParams(seed, args.bounces, args.small_spp, rr.PT_FLAG_GRAPH),
+                                          sm_ptrs, st))
+    sm["tuned"] = {"ms": round(ms, 3), "mpaths_s": round(sm_paths / ms / 1e3, 2)}
+    batch.set_mode(rr.BATCH_WAVEFRONT)
     for name, flags in (("graph", rr.PT_FLAG_GRAPH), ("plain", 0)):
         ms = timed(lambda seed, fl=flags: batch.execute(sm_cams, rr.PtParams(seed, args.bounces, args.small_spp, fl),
                                                         sm_ptrs, st))
@@ -121,6 +134,9 @@ def main():
     ms = timed(sm_sequential)
     sm["sequential"] = {"ms": round(ms, 3), "mpaths_s": round(sm_paths / ms / 1e3, 2)}
     sm["config"] = {"side": args.small_side, "spp": args.small_spp, "paths_per_batch": sm_paths}
+    # back to the large images' tuning for the guided section
+    ctx.check(rr.lib().rr_pathtracer_set_variants(ctx.handle, tune.best_extend, tune.best_shadow))
+    batch.set_mode(tuned_mode)
 
     # learned (or grid) guiding per scene: the batch's spp rendered as frames
     # of --guided-spp with one guide per scene, every guide updated after each
@@ -184,11 +200,13 @@ def main():
         guided[kind] = entry
         for g in guides:
             L.rr_guide_destroy(g)
-    line = {"metric": "Mpaths/s, 64-scene batch in one set of launches under a CUDA graph, 1xB200",
-            "value": round(paths / ms_graph / 1e3, 2), "unit": "Mpaths/s", "ms_per_batch": round(ms_graph, 3),
+    line = {"metric": "Mpaths/s, 64-scene batch (autotuned form, RR_PT_FLAG_GRAPH), 1xB200",
+            "value": round(paths / ms_tuned / 1e3, 2), "unit": "Mpaths/s", "ms_per_batch": round(ms_tuned, 3),
+            "wavefront_graph_batch": {"ms": round(ms_graph, 3), "mpaths_s": round(paths / ms_graph / 1e3, 2)},
             "plain_batch": {"ms": round(ms_plain, 3), "mpaths_s": round(paths / ms_plain / 1e3, 2)},
             "sequential_scenes": {"ms": round(ms_seq, 3), "mpaths_s": round(paths / ms_seq / 1e3, 2)},
-            "autotune": {"best_extend": tune.best_extend, "best_shadow": tune.best_shadow,
+            "autotune": {"mode": mode_names[tuned_mode], "best_extend": tune.best_extend,
+                         "best_shadow": tune.best_shadow,
                          "extend_ms": [round(x, 2) for x in tune.extend_ms],
                          "shadow_ms": [round(x, 2) for x in tune.shadow_ms]},
             "config": {"workload": "64 procedural rooms, 10k-500k triangles, 256^2-1024^2 pixels", "scenes": args.scenes,

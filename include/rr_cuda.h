@@ -195,10 +195,24 @@ rr_status rr_batch_execute(rr_ctx* ctx, rr_batch* batch, const GpuCameraData* ca
                            const rr_pt_params* params, float* const* radiance_out, void* stream);
 
 /* rr_pathtracer_tune for a batch: times every traversal variant on the
- * batch, keeps the fastest on the context (graphs are recaptured). */
+ * batch, keeps the fastest on the context (graphs are recaptured), then
+ * times the batch's two forms with those variants and keeps the faster on
+ * the batch (rr_batch_get_mode). */
 rr_status rr_batch_tune(rr_ctx* ctx, rr_batch* batch, const GpuCameraData* cameras,
                         const rr_pt_params* params, float* const* radiance_out, void* stream,
                         rr_pt_tune_result* out);
+
+/* The batch's form: RR_BATCH_WAVEFRONT (default) renders all scenes in one
+ * set of wavefront launches (graph-replayable); RR_BATCH_PER_SCENE renders
+ * them one rr_pathtracer_execute after another (launched directly, also with
+ * RR_PT_FLAG_GRAPH), which is faster when every scene alone fills the GPU:
+ * the scenes' many short launch tails are then filled by the shadow overlap.
+ * Both give the same images; calls with RR_PT_FLAG_COUNT_TRAVERSAL or
+ * RR_PT_FLAG_TIME_STAGES use the wavefront form. */
+#define RR_BATCH_WAVEFRONT 0
+#define RR_BATCH_PER_SCENE 1
+rr_status rr_batch_set_mode(rr_batch* batch, int mode);
+rr_status rr_batch_get_mode(const rr_batch* batch, int* mode_out);
 
 /* ── accumulate: AccumulatePass::execute (AccumulatePass.cpp:167-218,
  * kernel accumulate.slang:21-46). AccumulatePushConstants minus indices.

@@ -540,6 +540,16 @@ extern "C" rr_status rr_batch_execute(rr_ctx* ctx, rr_batch* B, const GpuCameraD
     uint64_t paths = 0;
     rr_status st = rr_batch_stage_call(ctx, B, cams, p, radiance_out, stream, &tiles, &paths);
     if (st != RR_OK) return st;
+    if (B->mode == RR_BATCH_PER_SCENE && !(p->flags & (RR_PT_FLAG_COUNT_TRAVERSAL | RR_PT_FLAG_TIME_STAGES))) {
+        // scene by scene (the staged table above checked the arguments and
+        // sized the queues for the whole batch)
+        rr_pt_params q = *p;
+        q.flags = 0;
+        for (size_t i = 0; i < B->scenes.size(); ++i)
+            if ((st = rr_pathtracer_execute(ctx, B->scenes[i], &cams[i], &q, radiance_out[i], stream)) != RR_OK)
+                return st;
+        return RR_OK;
+    }
     // the overlap's stream and events exist before any graph capture starts
     if (ctx->overlap_shadow && (st = ensure_side(ctx)) != RR_OK) return st;
     if (graph) {
@@ -597,5 +607,40 @@ extern "C" rr_status rr_batch_tune(rr_ctx* ctx, rr_batch* B, const GpuCameraData
     }
     ctx->extend_variant = out->best_extend;
     ctx->shadow_variant = out->best_shadow;
+    // the batch's form: each timed (after one warm-up call) with the caller's graph flag
+    rr_pt_params m = *p;
+    m.flags = p->flags & RR_PT_FLAG_GRAPH;
+    cudaStream_t st0 = static_cast<cudaStream_t>(stream);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    RR_TRY_CUDA(ctx, cudaEventCreate(&e0));
+    RR_TRY_CUDA(ctx, cudaEventCreate(&e1));
+    float best_ms = 0.0f;
+    int best_mode = RR_BATCH_WAVEFRONT;
+    for (int mode : {RR_BATCH_WAVEFRONT, RR_BATCH_PER_SCENE}) {
+        B->mode = mode;
+        if ((s = rr_batch_execute(ctx, B, cams, &m, radiance_out, stream)) != RR_OK) break;
+        cudaEventRecord(e0, st0);
+        if ((s = rr_batch_execute(ctx, B, cams, &m, radiance_out, stream)) != RR_OK) break;
+        cudaEventRecord(e1, st0);
+        float ms = 0.0f;
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (mode == RR_BATCH_WAVEFRONT || ms < best_ms) { best_ms = ms; best_mode = mode; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    B->mode = best_mode;
+    return s;
+}
+
+extern "C" rr_status rr_batch_set_mode(rr_batch* B, int mode) {
+    if (!B || (mode != RR_BATCH_WAVEFRONT && mode != RR_BATCH_PER_SCENE)) return RR_ERR_INVALID_ARGUMENT;
+    B->mode = mode;
+    return RR_OK;
+}
+
+extern "C" rr_status rr_batch_get_mode(const rr_batch* B, int* mode_out) {
+    if (!B || !mode_out) return RR_ERR_INVALID_ARGUMENT;
+    *mode_out = B->mode;
     return RR_OK;
 }

@@ -19,6 +19,7 @@ struct rr_batch {
     unsigned char* h_call[2] = {nullptr, nullptr};  // pinned staging of d_call, alternating
     cudaEvent_t staged[2] = {nullptr, nullptr};     // the copy out of h_call[k] has completed
     int slot = 0;
+    int mode = RR_BATCH_WAVEFRONT;         // rr_batch_set_mode / rr_batch_tune
     size_t entries_bytes = 0, call_bytes = 0;
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t exec = nullptr;

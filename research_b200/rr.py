@@ -69,6 +69,8 @@ PT_FLAG_COUNT_TRAVERSAL = 1
 PT_FLAG_TIME_STAGES = 2
 PT_FLAG_GRAPH = 4
 PT_VARIANT_COUNT = 8
+BATCH_WAVEFRONT = 0
+BATCH_PER_SCENE = 1
 
 
 class PtParams(C.Structure):
@@ -213,6 +215,8 @@ _SIGNATURES = {
     "rr_guiding_reset": (I, [P, P, P, C.POINTER(GuidingParams), P]),
     "rr_batch_create": (I, [P, C.POINTER(P), U32, C.POINTER(P)]),
     "rr_batch_destroy": (I, [P]),
+    "rr_batch_set_mode": (I, [P, I]),
+    "rr_batch_get_mode": (I, [P, C.POINTER(I)]),
     "rr_batch_execute": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtParams), C.POINTER(P), P]),
     "rr_batch_tune": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtParams), C.POINTER(P), P,
                           C.POINTER(PtTuneResult)]),
@@ -455,6 +459,16 @@ class Batch:
         outs = (P * len(outputs))(*outputs)
         self.ctx.check(lib().rr_batch_execute_guided(self.ctx.handle, self._h, cams, C.byref(params), gs, outs,
                                                      stream))
+
+    @property
+    def mode(self) -> int:
+        """BATCH_WAVEFRONT or BATCH_PER_SCENE (rr_batch_get_mode; set by tune)."""
+        m = C.c_int()
+        self.ctx.check(lib().rr_batch_get_mode(self._h, C.byref(m)))
+        return m.value
+
+    def set_mode(self, mode: int):
+        self.ctx.check(lib().rr_batch_set_mode(self._h, mode))
 
     def tune(self, cameras, params, outputs, stream) -> "PtTuneResult":
         cams = (GpuCameraData * len(cameras))(*cameras)

@@ -42,10 +42,13 @@ def _cams(rr, shift=0.0):
             for (w, h), e, c in zip(sizes, eyes, centers)]
 
 
+@pytest.mark.parametrize("mode", ["wavefront", "per_scene"])
 @pytest.mark.parametrize("graph", [False, True])
-def test_batch_matches_single_scene_renders(rr, ctx, torch_cuda, scenes, graph):
+def test_batch_matches_single_scene_renders(rr, ctx, torch_cuda, scenes, graph, mode):
     torch = torch_cuda
     b = rr.Batch(ctx, scenes)
+    b.set_mode(rr.BATCH_WAVEFRONT if mode == "wavefront" else rr.BATCH_PER_SCENE)
+    assert b.mode == (rr.BATCH_WAVEFRONT if mode == "wavefront" else rr.BATCH_PER_SCENE)
     flags = rr.PT_FLAG_GRAPH if graph else 0
     for frame, shift in ((0, 0.0), (16, 0.05), (32, -0.1)):   # graph replays with new seeds and cameras
         cams = _cams(rr, shift)
@@ -56,7 +59,7 @@ def test_batch_matches_single_scene_renders(rr, ctx, torch_cuda, scenes, graph):
         for k, (sc, cam, o) in enumerate(zip(scenes, cams, outs)):
             ref = _single(rr, ctx, torch, sc, cam, rr.PtParams(frame, 5, 3, 0))
             got = o.cpu().numpy()
-            assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), (graph, frame, k)
+            assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), (graph, mode, frame, k)
     b.close()
 
 
@@ -69,6 +72,7 @@ def test_batch_tuner_and_counts(rr, ctx, torch_cuda, scenes):
     res = b.tune(cams, rr.PtParams(3, 5, 2, 0), ptrs, _stream(torch))
     assert 0 <= res.best_extend < rr.PT_VARIANT_COUNT and 0 <= res.best_shadow < rr.PT_VARIANT_COUNT
     assert all(t > 0 for t in res.extend_ms) and all(t > 0 for t in res.shadow_ms)
+    assert b.mode in (rr.BATCH_WAVEFRONT, rr.BATCH_PER_SCENE)
     # after tuning, graph and plain runs still match the single-scene renders
     b.execute(cams, rr.PtParams(3, 5, 2, rr.PT_FLAG_GRAPH), ptrs, _stream(torch))
     torch.cuda.synchronize()
@@ -97,4 +101,7 @@ def test_batch_rejects_bad_arguments(rr, ctx, torch_cuda, scenes):
         b.execute(cams, rr.PtParams(0, 5, 1, rr.PT_FLAG_GRAPH | rr.PT_FLAG_TIME_STAGES), [0], 0)
     with pytest.raises(rr.RRError):
         b.execute(cams, rr.PtParams(0, 5, 1, 0), [0], 0)   # null output
+    with pytest.raises(rr.RRError):
+        b.set_mode(2)
+    assert b.mode == rr.BATCH_WAVEFRONT
     b.close()
