@@ -1574,7 +1574,8 @@ void oracle_bvh2_trace(const float* nodes, uint32_t num_nodes, const float* tris
             const bool i0 = h[0] && c[0] >= 0 && nr[0] <= best_t;
             const bool i1 = h[1] && c[1] >= 0 && nr[1] <= best_t;
             if (i0 && i1) {
-                const bool first0 = nr[0] <= nr[1];
+                // closest hit: nearer child first; any hit: farther first
+                const bool first0 = any_hit ? nr[0] > nr[1] : nr[0] <= nr[1];
                 stack_node[sp] = first0 ? c[1] : c[0];
                 stack_t[sp] = first0 ? nr[1] : nr[0];
                 ++sp;

@@ -74,7 +74,8 @@ def test_trace_closest_matches_oracle(rr, O, ctx, torch_cuda, cornell, procedura
 def test_traversal_work_matches_cpu_restatement(rr, O, ctx, torch_cuda, cornell, procedural):
     """The traversal's node / triangle counters (the algorithmic work behind the
     roofline bytes) equal a CPU restatement walking the library's own BVH in the
-    same front-to-back order, ray by ray, for closest-hit and any-hit rays;
+    same child order (front to back for closest hit, back to front for any
+    hit), ray by ray, for closest-hit and any-hit rays;
     the hits agree bit for bit too."""
     torch = torch_cuda
     rng = np.random.default_rng(23)
