@@ -59,6 +59,13 @@ rr_status   rr_ctx_create(int device_ordinal, rr_ctx** out_ctx);
 rr_status   rr_ctx_destroy(rr_ctx* ctx);
 /* Copies the last error message of this context (NUL-terminated). */
 rr_status   rr_last_error(const rr_ctx* ctx, char* buf, size_t buf_size);
+/* Caps the wavefront ray queues the context may allocate at `max_entries`
+ * entries (one entry per path in flight; 0 = no cap, the default). A call
+ * whose paths need more (width x height x spp for the path tracers, width x
+ * height for the reuse passes' wavefront steps) returns
+ * RR_ERR_QUEUE_OVERFLOW before launching anything. No counterpart in the
+ * reference, whose passes size their images at initialize(). */
+rr_status   rr_ctx_set_queue_limit(rr_ctx* ctx, uint64_t max_entries);
 
 /* ── scene ───────────────────────────────────────────────────────────────
  * Replaces Scene::upload (Scene.cpp:255-515): copies the flat GpuScene
@@ -291,10 +298,19 @@ rr_status rr_atrous_execute(rr_ctx* ctx, const float* input, const float* gbuf_p
 /* Strides 1, 2 and 4 run a kernel whose blocks first copy their halo tile
  * of the three images into shared memory with TMA tensor copies (default
  * on; the same bits as the direct-load kernel, which strides 8 and up use).
- * rr_atrous_tma_error reports (synchronously) whether a tile's copies ever
- * failed to complete within the kernel's bounded wait. */
+ * A block whose copies miss the kernel's bounded wait (wait_tries tries,
+ * default 2^22) sets a host-mapped flag, waits once more (bounded) for its
+ * copies, and filters its pixels from global memory instead: the output is
+ * still complete and the same bits. The next rr_atrous_iteration or
+ * rr_atrous_execute call on the context then returns RR_ERR_TIMEOUT without
+ * doing its work (the message says so) and clears the flag; calling again
+ * proceeds. rr_atrous_tma_error synchronizes the device, reports the flag
+ * and clears it. rr_atrous_set_tma_wait_tries sets the tries (0 makes every
+ * block give up at once, which exercises that path: the copies still land
+ * before the block leaves). */
 rr_status rr_atrous_set_tma(rr_ctx* ctx, int enable);
 rr_status rr_atrous_tma_error(rr_ctx* ctx, int* error_out);
+rr_status rr_atrous_set_tma_wait_tries(rr_ctx* ctx, uint32_t tries);
 
 /* No counterpart in the reference: an A-trous entry point that allocates
  * nothing, for callers that cannot allocate device memory (an engine that
@@ -304,10 +320,16 @@ rr_status rr_atrous_tma_error(rr_ctx* ctx, int* error_out);
  * intermediate image lives in a fixed array in the library's device memory
  * (RR_ATROUS_STATIC_MAX_PIXELS RGBA32F pixels, 36 MiB, held on every GPU
  * that loads the library until the process exits). Images with more pixels
- * return RR_ERR_UNSUPPORTED; null or aliased buffers RR_ERR_INVALID_ARGUMENT.
- * The first call on each device looks up the array's device address (with
- * that device current) and should come before any stream capture. All calls
- * share the array: calls whose kernels overlap on the GPU race on it. */
+ * return RR_ERR_UNSUPPORTED; null buffers, a width above 65535 x 16 or a
+ * height above 65535 x 8, or an output that overlaps the input or either
+ * G-buffer image return RR_ERR_INVALID_ARGUMENT. The first call in each CUDA
+ * context of a device looks up the array's device address (with that device
+ * current) and should come before any stream capture; the address is cached
+ * with the context's unique id, so a call after cudaDeviceReset (a new
+ * context) looks it up again instead of using a stale address. A failed
+ * launch returns RR_ERR_CUDA; errors left by earlier, unrelated work are not
+ * reported or cleared. All calls share the array: calls whose kernels
+ * overlap on the GPU race on it. */
 #define RR_ATROUS_STATIC_MAX_PIXELS (2048u * 1152u)
 rr_status rr_atrous_execute_static(const float* input, const float* gbuf_pos,
                                    const float* gbuf_norm, float* output,
@@ -569,7 +591,7 @@ rr_status rr_batch_execute_guided(rr_ctx* ctx, rr_batch* batch, const GpuCameraD
  * sample counts (rr_guide_update is this call with one guide). */
 rr_status rr_guides_update(rr_ctx* ctx, rr_guide* const* guides, uint32_t count, void* stream);
 
-/* ── output formats (SURVEY "next": tonemap / PNG / MSE utilities) ─────
+/* ── output formats: tonemap, PNG and the crop MSE ──────────────────────
  * rr_tonemap_execute: exposure, ACES filmic approximation, clamp, gamma
  * 1/2.2, 8-bit RGBA (Application.cpp:853-866; tonemap.slang:40-69).
  * rr_image_mse: FP64 mean squared error over the RGB channels of the window

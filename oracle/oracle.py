@@ -105,6 +105,27 @@ def lib() -> C.CDLL:
     return _lib
 
 
+INPUTS_PATH = HERE / "librr_inputs.so"
+_inputs = None
+
+
+def inputs_lib() -> C.CDLL:
+    """The seeded synthetic inputs (scene factories and camera blocks of
+    include/rr_host.h), built by oracle/Makefile from the same generator
+    source as the product library but without any CUDA code, so that a CPU
+    run builds its scene and camera without loading the CUDA library. Use it
+    as `rr.HostScene.procedural(..., L=inputs_lib())` and
+    `rr.camera_data(rr.camera_desc(..., L=inputs_lib()), L=inputs_lib())`
+    (research_b200.rr only supplies the ctypes layouts here)."""
+    global _inputs
+    if _inputs is None:
+        if not INPUTS_PATH.exists():
+            raise RuntimeError(f"{INPUTS_PATH} missing; run `make -C oracle`")
+        from research_b200 import rr as _rr
+        _inputs = _rr.bind(C.CDLL(str(INPUTS_PATH)), _rr.HOST_FUNCTIONS)
+    return _inputs
+
+
 def threads() -> int:
     return max(1, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1))
 

@@ -6,6 +6,7 @@
 Outputs (git-ignored, shipped in-tree):
     research_b200/lib/librr_cuda.so   CUDA kernels + C ABI (include/rr_cuda.h)
     oracle/librr_oracle.so            CPU checker, built by oracle/Makefile
+    oracle/librr_inputs.so            the seeded scene/camera generators without CUDA (CPU reference arm)
 
 Numerics flags: the kernels are compiled without FMA contraction and with
 IEEE-rounded division and square root (-fmad=false -prec-div=true

@@ -4,6 +4,7 @@
 // exp(-|dp|^2/sp^2) * exp(-max(0, 1-n.n')/sn^2) * exp(-dl^2/sl^2).
 
 #include "rr_internal.h"
+#include "rr_atrous.cuh"
 #include "rr_tc.cuh"
 
 #include <cuda.h>
@@ -11,9 +12,6 @@
 
 namespace rr {
 namespace {
-
-RR_D float luminance601(float3 c) { return dot(c, f3(0.299f, 0.587f, 0.114f)); }
-RR_D float kernel_weight(int o) { return (o == 2 || o == -2) ? 1.0f : ((o == 1 || o == -1) ? 4.0f : 6.0f); }
 
 // The G-buffer normals normalized once per call (the filter reads each
 // pixel's normal for up to 25 taps per iteration; normalize is deterministic,
@@ -35,39 +33,7 @@ __global__ void __launch_bounds__(128) atrous_kernel(const float4* __restrict__ 
     const int x = blockIdx.x * 16 + (threadIdx.x & 15);
     const int y = blockIdx.y * 8 + (threadIdx.x >> 4);
     if (x >= W || y >= H) return;
-    const size_t ci = size_t(y) * W + x;
-    const float4 cpos = gpos[ci];
-    const float4 crad = in[ci];
-    if (cpos.w < 0.0f) { out[ci] = crad; return; }
-    const float3 cn = xyz(nrm[ci]);
-    const float cl = luminance601(xyz(crad));
-    float3 filtered = f3(0.0f, 0.0f, 0.0f);
-    float wsum = 0.0f;
-    #pragma unroll
-    for (int ty = -2; ty <= 2; ++ty) {
-        const int sy = min(max(y + ty * stride, 0), H - 1);
-        #pragma unroll
-        for (int tx = -2; tx <= 2; ++tx) {
-            const int sx = min(max(x + tx * stride, 0), W - 1);
-            const size_t si = size_t(sy) * W + sx;
-            const float4 spos = __ldg(gpos + si);
-            if (spos.w < 0.0f) continue;
-            const float base_w = (kernel_weight(tx) * kernel_weight(ty)) / 256.0f;
-            const float3 pd = xyz(spos) - xyz(cpos);
-            const float pos_w = rr_expf(-dot(pd, pd) / sp2);
-            const float3 sn = xyz(__ldg(nrm + si));
-            const float nd = mx(0.0f, 1.0f - dot(cn, sn));
-            const float normal_w = rr_expf(-nd / sn2);
-            const float3 srad = xyz(__ldg(in + si));
-            const float ld = luminance601(srad) - cl;
-            const float luma_w = rr_expf(-(ld * ld) / sl2);
-            const float w = base_w * pos_w * normal_w * luma_w;
-            filtered = filtered + srad * w;
-            wsum += w;
-        }
-    }
-    const float3 o = wsum > 0.0f ? filtered / wsum : xyz(crad);
-    out[ci] = make_float4(o.x, o.y, o.z, crad.w);
+    out[size_t(y) * W + x] = atrous_pixel(GlobalFetch{in, gpos, nrm, W}, x, y, W, H, stride, sp2, sn2, sl2);
 }
 
 // TMA-staged form of atrous_kernel for strides 1, 2 and 4: a block of 32 x 8
@@ -88,6 +54,19 @@ struct AtrousTile {
     static_assert(kBytes % 128 == 0, "tiles stay 128-byte aligned");
 };
 
+// The images in a block's halo tile in shared memory.
+template <int S>
+struct TileFetch {
+    const float4* rad_t;
+    const float4* pos_t;
+    const float4* nrm_t;
+    int tx0, ty0;
+    RR_D int at(int x, int y) const { return (y - ty0) * AtrousTile<S>::W + (x - tx0); }
+    RR_D float4 rad(int x, int y) const { return rad_t[at(x, y)]; }
+    RR_D float4 pos(int x, int y) const { return pos_t[at(x, y)]; }
+    RR_D float4 nrm(int x, int y) const { return nrm_t[at(x, y)]; }
+};
+
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
                                             uint64_t* bar) {
     asm volatile(
@@ -101,8 +80,11 @@ template <int S>
 __global__ void __launch_bounds__(256) atrous_tma_kernel(const __grid_constant__ CUtensorMap m_rad,
                                                          const __grid_constant__ CUtensorMap m_pos,
                                                          const __grid_constant__ CUtensorMap m_nrm,
+                                                         const float4* __restrict__ in_g,
+                                                         const float4* __restrict__ pos_g,
+                                                         const float4* __restrict__ nrm_g,
                                                          float4* __restrict__ out, int W, int H, float sp2,
-                                                         float sn2, float sl2, int* error) {
+                                                         float sn2, float sl2, int* error, uint32_t wait_tries) {
     using T = AtrousTile<S>;
     extern __shared__ __align__(128) unsigned char sm[];
     const float4* t_rad = reinterpret_cast<const float4*>(sm);
@@ -122,49 +104,24 @@ __global__ void __launch_bounds__(256) atrous_tma_kernel(const __grid_constant__
         tma_load_3d(sm + 2 * T::kBytes, &m_nrm, 0, tx0, ty0, bar);
     }
     __syncthreads();
-    if (!tc::mbar_wait(bar, 0)) {
-        // the copies never completed: report, give them one more bounded
-        // wait so that none is left writing this block's memory, and leave
-        if (threadIdx.x == 0) atomicExch(error, 1);
+    const bool staged = tc::mbar_wait(bar, 0, wait_tries);
+    if (!staged) {
+        // the copies did not complete within the bounded wait: report it in
+        // the host-mapped flag, give them one more bounded wait so that none
+        // is left writing this block's shared memory after it leaves, and
+        // filter this thread's pixel from global memory instead (same bits)
+        *reinterpret_cast<volatile int*>(error) = 1;
         tc::mbar_wait(bar, 0);
-        return;
     }
     const int x = x0 + int(threadIdx.x & 31u), y = y0 + int(threadIdx.x >> 5);
     if (x >= W || y >= H) return;
     const size_t ci = size_t(y) * W + x;
-    const int cl_i = (y - ty0) * T::W + (x - tx0);
-    const float4 cpos = t_pos[cl_i];
-    const float4 crad = t_rad[cl_i];
-    if (cpos.w < 0.0f) { out[ci] = crad; return; }
-    const float3 cn = xyz(t_nrm[cl_i]);
-    const float cl = luminance601(xyz(crad));
-    float3 filtered = f3(0.0f, 0.0f, 0.0f);
-    float wsum = 0.0f;
-    #pragma unroll
-    for (int ty = -2; ty <= 2; ++ty) {
-        const int sy = min(max(y + ty * S, 0), H - 1);
-        #pragma unroll
-        for (int tx = -2; tx <= 2; ++tx) {
-            const int sx = min(max(x + tx * S, 0), W - 1);
-            const int si = (sy - ty0) * T::W + (sx - tx0);
-            const float4 spos = t_pos[si];
-            if (spos.w < 0.0f) continue;
-            const float base_w = (kernel_weight(tx) * kernel_weight(ty)) / 256.0f;
-            const float3 pd = xyz(spos) - xyz(cpos);
-            const float pos_w = rr_expf(-dot(pd, pd) / sp2);
-            const float3 sn = xyz(t_nrm[si]);
-            const float nd = mx(0.0f, 1.0f - dot(cn, sn));
-            const float normal_w = rr_expf(-nd / sn2);
-            const float3 srad = xyz(t_rad[si]);
-            const float ld = luminance601(srad) - cl;
-            const float luma_w = rr_expf(-(ld * ld) / sl2);
-            const float w = base_w * pos_w * normal_w * luma_w;
-            filtered = filtered + srad * w;
-            wsum += w;
-        }
+    if (staged) {
+        const TileFetch<S> f{t_rad, t_pos, t_nrm, tx0, ty0};
+        out[ci] = atrous_pixel(f, x, y, W, H, S, sp2, sn2, sl2);
+    } else {
+        out[ci] = atrous_pixel(GlobalFetch{in_g, pos_g, nrm_g, W}, x, y, W, H, S, sp2, sn2, sl2);
     }
-    const float3 o = wsum > 0.0f ? filtered / wsum : xyz(crad);
-    out[ci] = make_float4(o.x, o.y, o.z, crad.w);
 }
 
 } // namespace
@@ -211,8 +168,10 @@ static bool atrous_tma_launch(rr_ctx* ctx, const float* input, const float* gpos
         cudaSuccess)
         return false;
     const dim3 grid((W + 31) / 32, (H + 7) / 8);
-    rr::atrous_tma_kernel<S><<<grid, 256, T::kSmem, stream>>>(mr, mp, mn, reinterpret_cast<float4*>(output), int(W),
-                                                              int(H), sp2, sn2, sl2, ctx->atrous_error);
+    rr::atrous_tma_kernel<S><<<grid, 256, T::kSmem, stream>>>(
+        mr, mp, mn, reinterpret_cast<const float4*>(input), reinterpret_cast<const float4*>(gpos), nrm,
+        reinterpret_cast<float4*>(output), int(W), int(H), sp2, sn2, sl2, ctx->atrous_error_dev,
+        ctx->atrous_wait_tries);
     return true;
 }
 
@@ -241,8 +200,19 @@ static rr_status atrous_launch(rr_ctx* ctx, const float* input, const float* gpo
     const float sp2 = std::max(sp * sp, 1.0e-6f), sn2 = std::max(sn * sn, 1.0e-6f), sl2 = std::max(sl * sl, 1.0e-6f);
     if (ctx->atrous_tma && (stride == 1 || stride == 2 || stride == 4)) {
         if (!ctx->atrous_error) {
-            RR_TRY_CUDA(ctx, cudaMalloc(&ctx->atrous_error, sizeof(int)));
-            RR_TRY_CUDA(ctx, cudaMemset(ctx->atrous_error, 0, sizeof(int)));
+            // one host-mapped word: a block that gives up writes it, and the
+            // next A-trous call reads it without synchronizing
+            int* h = nullptr;
+            RR_TRY_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void**>(&h), sizeof(int), cudaHostAllocMapped));
+            *reinterpret_cast<volatile int*>(h) = 0;
+            void* d = nullptr;
+            cudaError_t e = cudaHostGetDevicePointer(&d, h, 0);
+            if (e != cudaSuccess) {
+                cudaFreeHost(h);
+                RR_TRY_CUDA(ctx, e);
+            }
+            ctx->atrous_error = h;
+            ctx->atrous_error_dev = static_cast<int*>(d);
         }
         bool launched = false;
         if (stride == 1) launched = atrous_tma_launch<1>(ctx, input, gpos, nrm, output, W, H, sp2, sn2, sl2, stream);
@@ -263,6 +233,19 @@ static rr_status atrous_launch(rr_ctx* ctx, const float* input, const float* gpo
     return RR_OK;
 }
 
+// An earlier call's tile copies missed their bounded wait (the flag the
+// blocks write into host-mapped memory): reported once, here, at the next
+// call, which then does no work. The earlier call's output is complete: the
+// blocks that gave up filtered their pixels from global memory.
+static rr_status atrous_report_give_up(rr_ctx* ctx, const char* who) {
+    if (!ctx->atrous_error || *reinterpret_cast<volatile int*>(ctx->atrous_error) == 0) return RR_OK;
+    *reinterpret_cast<volatile int*>(ctx->atrous_error) = 0;
+    return rr_fail(ctx, RR_ERR_TIMEOUT,
+                   "%s: an earlier A-trous call's TMA tile copies did not complete within the bounded wait "
+                   "(that call's output was filtered from global memory instead); this call did no work",
+                   who);
+}
+
 extern "C" rr_status rr_atrous_iteration(rr_ctx* ctx, const float* input, const float* gpos,
                                          const float* gnrm, float* output, const rr_atrous_params* p,
                                          void* stream) {
@@ -271,6 +254,7 @@ extern "C" rr_status rr_atrous_iteration(rr_ctx* ctx, const float* input, const 
     if (p->width == 0 || p->height == 0 || p->width > 65535u * 16u || p->height > 65535u * 8u)
         return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_atrous_iteration: bad image size");
     if (input == output) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_atrous_iteration: input aliases output");
+    if (rr_status g = atrous_report_give_up(ctx, "rr_atrous_iteration")) return g;
     RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
     const float4* nrm = nullptr;
     rr_status st = atrous_normals(ctx, gnrm, p->width, p->height, static_cast<cudaStream_t>(stream), &nrm);
@@ -289,6 +273,7 @@ extern "C" rr_status rr_atrous_execute(rr_ctx* ctx, const float* input, const fl
         return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_atrous_execute: bad image size");
     if (input == ping0 || input == ping1 || ping0 == ping1)
         return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_atrous_execute: buffers alias");
+    if (rr_status g = atrous_report_give_up(ctx, "rr_atrous_execute")) return g;
     RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
     // AtrousPass.cpp:265 clamps to 1..7; slot (iterations-1)&1 holds the result.
     const uint32_t iters = std::min(std::max(p->iterations, 1u), 7u);
@@ -320,6 +305,14 @@ extern "C" rr_status rr_atrous_tma_error(rr_ctx* ctx, int* error_out) {
     *error_out = 0;
     if (!ctx->atrous_error) return RR_OK;
     RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
-    RR_TRY_CUDA(ctx, cudaMemcpy(error_out, ctx->atrous_error, sizeof(int), cudaMemcpyDeviceToHost));
+    RR_TRY_CUDA(ctx, cudaDeviceSynchronize());
+    *error_out = *reinterpret_cast<volatile int*>(ctx->atrous_error);
+    *reinterpret_cast<volatile int*>(ctx->atrous_error) = 0;
+    return RR_OK;
+}
+
+extern "C" rr_status rr_atrous_set_tma_wait_tries(rr_ctx* ctx, uint32_t tries) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    ctx->atrous_wait_tries = tries;
     return RR_OK;
 }

@@ -17,6 +17,7 @@
 #include "rr_wavefront.cuh"
 #include "rr_batch.h"
 
+#include <algorithm>
 #include <cstring>
 
 namespace rr {
@@ -607,30 +608,45 @@ extern "C" rr_status rr_batch_tune(rr_ctx* ctx, rr_batch* B, const GpuCameraData
     }
     ctx->extend_variant = out->best_extend;
     ctx->shadow_variant = out->best_shadow;
-    // the batch's form: each timed (after one warm-up call) with the caller's graph flag
+    // the batch's form: each timed (after one warm-up call) with the caller's
+    // graph flag, three calls each, compared by their medians (a shared GPU
+    // makes single calls noisy)
     rr_pt_params m = *p;
     m.flags = p->flags & RR_PT_FLAG_GRAPH;
     cudaStream_t st0 = static_cast<cudaStream_t>(stream);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     RR_TRY_CUDA(ctx, cudaEventCreate(&e0));
-    RR_TRY_CUDA(ctx, cudaEventCreate(&e1));
-    float best_ms = 0.0f;
-    int best_mode = RR_BATCH_WAVEFRONT;
-    for (int mode : {RR_BATCH_WAVEFRONT, RR_BATCH_PER_SCENE}) {
-        B->mode = mode;
+    cudaError_t ce = cudaEventCreate(&e1);
+    if (ce != cudaSuccess) {
+        cudaEventDestroy(e0);
+        RR_TRY_CUDA(ctx, ce);
+    }
+    constexpr int kRepeats = 3;
+    float median_ms[2] = {0.0f, 0.0f};
+    const int modes[2] = {RR_BATCH_WAVEFRONT, RR_BATCH_PER_SCENE};
+    s = RR_OK;
+    for (int k = 0; k < 2 && s == RR_OK && ce == cudaSuccess; ++k) {
+        B->mode = modes[k];
         if ((s = rr_batch_execute(ctx, B, cams, &m, radiance_out, stream)) != RR_OK) break;
-        cudaEventRecord(e0, st0);
-        if ((s = rr_batch_execute(ctx, B, cams, &m, radiance_out, stream)) != RR_OK) break;
-        cudaEventRecord(e1, st0);
-        float ms = 0.0f;
-        cudaEventSynchronize(e1);
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (mode == RR_BATCH_WAVEFRONT || ms < best_ms) { best_ms = ms; best_mode = mode; }
+        float ms[kRepeats];
+        for (int r = 0; r < kRepeats && s == RR_OK && ce == cudaSuccess; ++r) {
+            if ((ce = cudaEventRecord(e0, st0)) != cudaSuccess) break;
+            if ((s = rr_batch_execute(ctx, B, cams, &m, radiance_out, stream)) != RR_OK) break;
+            if ((ce = cudaEventRecord(e1, st0)) != cudaSuccess) break;
+            if ((ce = cudaEventSynchronize(e1)) != cudaSuccess) break;
+            ce = cudaEventElapsedTime(&ms[r], e0, e1);
+        }
+        if (s != RR_OK || ce != cudaSuccess) break;
+        std::sort(ms, ms + kRepeats);
+        median_ms[k] = ms[kRepeats / 2];
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    B->mode = best_mode;
-    return s;
+    if (s != RR_OK) return s;
+    if (ce != cudaSuccess)
+        return rr_fail(ctx, RR_ERR_CUDA, "rr_batch_tune: timing the batch forms failed: %s", cudaGetErrorString(ce));
+    B->mode = median_ms[1] < median_ms[0] ? RR_BATCH_PER_SCENE : RR_BATCH_WAVEFRONT;
+    return RR_OK;
 }
 
 extern "C" rr_status rr_batch_set_mode(rr_batch* B, int mode) {

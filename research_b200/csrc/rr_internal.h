@@ -59,7 +59,10 @@ struct rr_ctx {
     float4* atrous_nrm = nullptr;          // A-trous: the G-buffer normals, normalized once per call
     size_t atrous_nrm_px = 0;
     bool atrous_tma = true;                // strides 1, 2, 4 through TMA-staged tiles
-    int* atrous_error = nullptr;           // set when a tile's copies never completed
+    int* atrous_error = nullptr;           // host-mapped word, set when a tile's copies missed the bounded wait
+    int* atrous_error_dev = nullptr;       // its device address
+    uint32_t atrous_wait_tries = 1u << 22; // tries of that bounded wait
+    size_t queue_limit = 0;                // most ray-queue entries the context may hold (0: no limit)
     // The path tracer traces bounce b's shadow rays on a second stream while
     // bounce b+1's extension rays run on the caller's (fork after shade b,
     // join before shade b+1); created on first use.

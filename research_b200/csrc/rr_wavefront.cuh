@@ -425,6 +425,10 @@ rr_status ensure_side(rr_ctx* ctx) {
 
 rr_status ensure_queues(rr_ctx* ctx, size_t n) {
     rr_pt_queues& q = ctx->pt;
+    if (ctx->queue_limit && n > ctx->queue_limit)
+        return rr_fail(ctx, RR_ERR_QUEUE_OVERFLOW,
+                       "the call needs %zu ray-queue entries; the context's queue limit is %zu "
+                       "(rr_ctx_set_queue_limit)", n, ctx->queue_limit);
     if (q.capacity >= n) return RR_OK;
     for (int i = 0; i < 2; ++i) { cudaFree(q.ray_a[i]); cudaFree(q.ray_b[i]); cudaFree(q.ray_c[i]); }
     cudaFree(q.hits); cudaFree(q.shadow_a); cudaFree(q.shadow_b); cudaFree(q.shadow_c);

@@ -89,7 +89,7 @@ rr_status rr_ctx_destroy(rr_ctx* ctx) {
     cudaFree(ctx->work64);
     cudaFree(ctx->mse_partial);
     cudaFree(ctx->atrous_nrm);
-    cudaFree(ctx->atrous_error);
+    if (ctx->atrous_error) cudaFreeHost(ctx->atrous_error);
     for (int b = 0; b < kMaxBounces; ++b) {
         if (ctx->shaded[b]) cudaEventDestroy(ctx->shaded[b]);
         if (ctx->shadowed[b]) cudaEventDestroy(ctx->shadowed[b]);
@@ -98,6 +98,12 @@ rr_status rr_ctx_destroy(rr_ctx* ctx) {
     cudaFree(ctx->wave_state);
     cudaFree(ctx->wave_counters);
     delete ctx;
+    return RR_OK;
+}
+
+rr_status rr_ctx_set_queue_limit(rr_ctx* ctx, uint64_t max_entries) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    ctx->queue_limit = size_t(max_entries);
     return RR_OK;
 }
 

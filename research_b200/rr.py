@@ -190,6 +190,7 @@ _SIGNATURES = {
     "rr_ctx_create": (I, [I, C.POINTER(P)]),
     "rr_ctx_destroy": (I, [P]),
     "rr_last_error": (I, [P, C.c_char_p, C.c_size_t]),
+    "rr_ctx_set_queue_limit": (I, [P, C.c_uint64]),
     "rr_scene_create": (I, [P, C.POINTER(SceneDesc), C.POINTER(P)]),
     "rr_scene_destroy": (I, [P]),
     "rr_scene_get_stats": (I, [P, C.POINTER(SceneStats)]),
@@ -200,6 +201,7 @@ _SIGNATURES = {
     "rr_reuse_set_wavefront": (I, [P, I]),
     "rr_atrous_set_tma": (I, [P, I]),
     "rr_atrous_tma_error": (I, [P, C.POINTER(C.c_int)]),
+    "rr_atrous_set_tma_wait_tries": (I, [P, U32]),
     "rr_pathtracer_tune": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(PtParams), P, P, C.POINTER(PtTuneResult)]),
     "rr_accumulate_execute": (I, [P, P, U32, P, P, C.POINTER(AccParams), P]),
     "rr_restir_di_initial": (I, [P, P, C.POINTER(GpuCameraData), C.POINTER(DIParams), P, P, P, P]),
@@ -277,13 +279,26 @@ def lib() -> C.CDLL:
     if _lib is None:
         if not LIB_PATH.exists():
             raise RRError(4, f"{LIB_PATH} is missing; run `python -m research_b200.build`")
-        L = C.CDLL(str(LIB_PATH))
-        for name, (res, args) in _SIGNATURES.items():
-            fn = getattr(L, name)
-            fn.restype = res
-            fn.argtypes = args
-        _lib = L
+        _lib = bind(C.CDLL(str(LIB_PATH)), _SIGNATURES)
     return _lib
+
+
+# The host-side scene factories and camera helpers (include/rr_host.h minus
+# the glTF loader): the functions another library built from the same
+# generator source also exports.
+HOST_FUNCTIONS = ("rr_host_scene_cornell", "rr_host_scene_procedural", "rr_host_scene_instanced",
+                  "rr_host_scene_desc", "rr_host_scene_destroy", "rr_camera_default", "rr_camera_look_at",
+                  "rr_camera_build")
+
+
+def bind(L: C.CDLL, names) -> C.CDLL:
+    """Sets the ctypes signatures of `names` (rr_cuda.h / rr_host.h functions) on `L`."""
+    for name in names:
+        res, args = _SIGNATURES[name]
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    return L
 
 
 def _f3(v) -> C.Array:
@@ -305,12 +320,14 @@ def ptr(t) -> int:
 
 # ── host scenes and cameras (no GPU needed) ────────────────────────────────
 class HostScene:
-    """Flat GpuScene arrays produced by the library's scene factories."""
+    """Flat GpuScene arrays produced by the library's scene factories. `L`
+    selects the library that runs the factory (default librr_cuda.so)."""
 
-    def __init__(self, handle):
+    def __init__(self, handle, L=None):
+        self._L = L if L is not None else lib()
         self._h = handle
         d = SceneDesc()
-        _check(None, lib().rr_host_scene_desc(handle, C.byref(d)))
+        _check(None, self._L.rr_host_scene_desc(handle, C.byref(d)))
         self.arrays = {
             "vertices": _view(d.vertices, d.vertex_count, VERTEX),
             "indices": _view(d.indices, d.index_count, np.dtype("<u4")),
@@ -321,25 +338,28 @@ class HostScene:
         }
 
     @staticmethod
-    def cornell(variant: int = 0) -> "HostScene":
+    def cornell(variant: int = 0, L=None) -> "HostScene":
+        L = L if L is not None else lib()
         h = P()
-        _check(None, lib().rr_host_scene_cornell(variant, C.byref(h)))
-        return HostScene(h)
+        _check(None, L.rr_host_scene_cornell(variant, C.byref(h)))
+        return HostScene(h, L)
 
     @staticmethod
-    def procedural(seed=0x5EED0002, target_triangles=1_000_000, emissive_triangles=4096, box_half=20.0):
+    def procedural(seed=0x5EED0002, target_triangles=1_000_000, emissive_triangles=4096, box_half=20.0, L=None):
+        L = L if L is not None else lib()
         h = P()
         p = ProceduralParams(seed, target_triangles, emissive_triangles, box_half, 0)
-        _check(None, lib().rr_host_scene_procedural(C.byref(p), C.byref(h)))
-        return HostScene(h)
+        _check(None, L.rr_host_scene_procedural(C.byref(p), C.byref(h)))
+        return HostScene(h, L)
 
     @staticmethod
     def instanced(seed=0x5EED0005, base_meshes=16, tris_per_mesh=2500, instance_count=4096,
-                  emissive_triangles=16384, box_half=250.0):
+                  emissive_triangles=16384, box_half=250.0, L=None):
+        L = L if L is not None else lib()
         h = P()
         p = InstancedParams(seed, base_meshes, tris_per_mesh, instance_count, emissive_triangles, box_half, 0)
-        _check(None, lib().rr_host_scene_instanced(C.byref(p), C.byref(h)))
-        return HostScene(h)
+        _check(None, L.rr_host_scene_instanced(C.byref(p), C.byref(h)))
+        return HostScene(h, L)
 
     @staticmethod
     def gltf(path) -> "HostScene":
@@ -358,7 +378,7 @@ class HostScene:
 
     def close(self):
         if self._h:
-            lib().rr_host_scene_destroy(self._h)
+            self._L.rr_host_scene_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -385,18 +405,20 @@ def scene_desc(arrays) -> tuple[SceneDesc, list]:
     return d, keep
 
 
-def camera_desc(width: int, height: int, eye=None, center=None, frame_index=0) -> CameraDesc:
+def camera_desc(width: int, height: int, eye=None, center=None, frame_index=0, L=None) -> CameraDesc:
+    L = L if L is not None else lib()
     c = CameraDesc()
-    _check(None, lib().rr_camera_default(width, height, C.byref(c)))
+    _check(None, L.rr_camera_default(width, height, C.byref(c)))
     if eye is not None and center is not None:
-        _check(None, lib().rr_camera_look_at(C.byref(c), _f3(eye), _f3(center)))
+        _check(None, L.rr_camera_look_at(C.byref(c), _f3(eye), _f3(center)))
     c.frame_index = frame_index
     return c
 
 
-def camera_data(desc: CameraDesc, prev: CameraDesc | None = None) -> GpuCameraData:
+def camera_data(desc: CameraDesc, prev: CameraDesc | None = None, L=None) -> GpuCameraData:
+    L = L if L is not None else lib()
     out = GpuCameraData()
-    _check(None, lib().rr_camera_build(C.byref(desc), C.byref(prev) if prev is not None else None, C.byref(out)))
+    _check(None, L.rr_camera_build(C.byref(desc), C.byref(prev) if prev is not None else None, C.byref(out)))
     return out
 
 
@@ -420,6 +442,11 @@ class Context:
 
     def check(self, status: int):
         _check(self, status)
+
+    def last_error(self) -> str:
+        buf = C.create_string_buffer(1024)
+        lib().rr_last_error(self._h, buf, 1024)
+        return buf.value.decode(errors="replace")
 
     @property
     def handle(self):

@@ -119,6 +119,18 @@ def test_mlp_gradient_matches_fp64(rr, ctx, torch_cuda):
     rel = float(np.linalg.norm(grad - ref) / np.linalg.norm(ref))
     assert cos > 0.99, (cos, rel)
     assert rel < 0.1, (cos, rel)
+    # every layer's weights and biases on their own: one wrong block (a bias
+    # column, a transposed layer) cannot hide under the global norm
+    per_block = {}
+    k = 0
+    for li, (i, o) in enumerate(mlp_ref.LAYERS):
+        for name, sl in (("W", slice(k, k + o * i)), ("b", slice(k + o * i, k + o * i + o))):
+            a, b = grad[sl].astype(np.float64), ref[sl]
+            nb = np.linalg.norm(b)
+            per_block[f"layer{li}.{name}"] = (float(a @ b / (np.linalg.norm(a) * nb)), float(np.linalg.norm(a - b) / nb))
+        k += o * i + o
+    bad = {n: e for n, e in per_block.items() if not (e[0] > 0.99 and e[1] < 0.1)}
+    assert not bad, per_block
     st = rr.GuideStats()
     ctx.check(rr.lib().rr_guide_get_stats(ctx.handle, g, C.byref(st)))
     assert st.last_loss == pytest.approx(loss, rel=0.05)

@@ -242,6 +242,49 @@ def test_restir_di_disabled_paths(rr, O, ctx, torch_cuda, cornell):
         np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
 
 
+@pytest.fixture(scope="module")
+def room_1m(rr, O, ctx):
+    """The benchmarked scene: the seeded 1M-triangle procedural room."""
+    hs = rr.HostScene.procedural(seed=0x5EED0002, target_triangles=1_000_000, emissive_triangles=4096, box_half=20.0)
+    return hs.arrays, rr.Scene(ctx, hs.arrays), O.OracleScene(hs.arrays, use_bvh=True)
+
+
+def test_room_1m_frame_bit_exact(rr, O, ctx, torch_cuda, room_1m):
+    """The benchmarked configuration (1M-triangle room, its view, 4 spp at
+    depth 5, ReSTIR DI M=32 / cap 20 M / K=5 / R=30 over three frames,
+    A-trous 5 iterations) at a small full image, against the oracle."""
+    torch = torch_cuda
+    _, scene, oscene = room_1m
+    W, H = 240, 136
+    cam = rr.camera_data(rr.camera_desc(W, H, eye=(0.0, 4.0, 34.0), center=(0.0, -3.0, 0.0)))
+    g_img = gpu_pathtrace(rr, ctx, scene, cam, torch, 8, 5, 4)
+    o_img, _ = O.pathtrace(oscene, cam, 8, 5, 4)
+    np.testing.assert_array_equal(g_img.view(np.uint32), o_img.view(np.uint32))
+    plist_g = [rr.DIParams(f, 32, 1, 1, 5, 30, 20, 0) for f in range(3)]
+    plist_o = [O.di_params(f, 32, 1, 1, 5, 30, 20) for f in range(3)]
+    g = _di_run_gpu(rr, ctx, torch, scene, cam, plist_g)
+    o = _di_run_oracle(O, oscene, cam, plist_o)
+    for (gg, go) in zip(g, o):
+        for a, b in zip(gg, go):
+            np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+    gpos, gnrm, _, out = o[-1]
+    ref = O.atrous(out, gpos, gnrm, 5)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    tin, tp, tn = t(g[-1][3]), t(g[-1][0]), t(g[-1][1])
+    ping = [torch.empty_like(tin), torch.empty_like(tin)]
+    slot = C.c_uint32()
+    for tma in (1, 0):
+        ctx.check(rr.lib().rr_atrous_set_tma(ctx.handle, tma))
+        ctx.check(rr.lib().rr_atrous_execute(ctx.handle, tin.data_ptr(), tp.data_ptr(), tn.data_ptr(),
+                                             ping[0].data_ptr(), ping[1].data_ptr(),
+                                             C.byref(rr.AtrousParams(W, H, 5, 0, 0.25, 0.20, 1.0, 0)),
+                                             C.byref(slot), _stream(torch)))
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(_np(ping[slot.value]).view(np.uint32), ref.view(np.uint32))
+    ctx.check(rr.lib().rr_atrous_set_tma(ctx.handle, 1))
+    assert (o[-1][2][..., 3].view(np.uint32) > 32).any()   # temporal history was merged
+
+
 @pytest.mark.parametrize("iterations", [1, 5, 7])
 def test_atrous_bit_exact(rr, O, ctx, torch_cuda, procedural, iterations):
     torch = torch_cuda
@@ -307,6 +350,78 @@ def test_atrous_tma_tiles_bit_identical(rr, O, ctx, torch_cuda, procedural, W, H
     err = C.c_int(-1)
     ctx.check(L.rr_atrous_tma_error(ctx.handle, C.byref(err)))
     assert err.value == 0
+
+
+def test_atrous_tma_give_up_is_reported_and_output_complete(rr, O, ctx, torch_cuda, procedural):
+    """A tile whose copies miss the bounded wait (here: a wait of zero tries,
+    so every block gives up at once while its copies still land) filters its
+    pixels from global memory: the output stays bit-identical to the oracle.
+    The next A-trous call then returns RR_ERR_TIMEOUT without doing work, and
+    the call after it proceeds."""
+    torch = torch_cuda
+    L = rr.lib()
+    _, scene, oscene = procedural
+    W, H = 131, 77
+    cam = cam_for(rr, "procedural", W, H)
+    p = O.di_params(2, 8, 1, 1, 4, 15, 20)
+    z = lambda: np.zeros((H, W, 4), np.float32)
+    gpos, gnrm, res, out = z(), z(), z(), z()
+    O.restir_di_initial(oscene, cam, p, gpos, gnrm, res)
+    O.restir_di_spatial_shade(oscene, cam, p, gpos, gnrm, res, out)
+    ref = O.atrous(out, gpos, gnrm, 5)
+    t = lambda a: torch.from_numpy(a).cuda()
+    tin, tp, tn = t(out), t(gpos), t(gnrm)
+    st = _stream(torch)
+    ap = rr.AtrousParams(W, H, 5, 0, 0.25, 0.20, 1.0, 0)
+    ping = [torch.empty_like(tin), torch.empty_like(tin)]
+    slot = C.c_uint32()
+    run = lambda: L.rr_atrous_execute(ctx.handle, tin.data_ptr(), tp.data_ptr(), tn.data_ptr(), ping[0].data_ptr(),
+                                      ping[1].data_ptr(), C.byref(ap), C.byref(slot), st)
+    ctx.check(L.rr_atrous_set_tma(ctx.handle, 1))
+    try:
+        ctx.check(L.rr_atrous_set_tma_wait_tries(ctx.handle, 0))
+        for p_ in ping:
+            p_.fill_(-7.0)
+        ctx.check(run())
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(_np(ping[slot.value]).view(np.uint32), ref.view(np.uint32))
+        assert run() == 6                                  # RR_ERR_TIMEOUT, reported once
+        assert "bounded wait" in ctx.last_error()
+        ctx.check(L.rr_atrous_set_tma_wait_tries(ctx.handle, 1 << 22))
+        ctx.check(run())                                   # flag cleared: this call works
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(_np(ping[slot.value]).view(np.uint32), ref.view(np.uint32))
+        err = C.c_int(-1)
+        ctx.check(L.rr_atrous_tma_error(ctx.handle, C.byref(err)))
+        assert err.value == 0
+    finally:
+        L.rr_atrous_set_tma_wait_tries(ctx.handle, 1 << 22)
+
+
+def test_queue_limit_returns_queue_overflow(rr, ctx, torch_cuda, cornell):
+    """A context capped below a call's paths in flight refuses the call with
+    RR_ERR_QUEUE_OVERFLOW before launching anything; lifting the cap lets the
+    same call run."""
+    torch = torch_cuda
+    L = rr.lib()
+    _, scene, _ = cornell
+    W, H, spp = 32, 16, 2
+    cam = cam_for(rr, "cornell", W, H)
+    out = torch.full((spp, H, W, 4), -3.0, device="cuda")
+    p = rr.PtParams(0, 4, spp, 0)
+    try:
+        ctx.check(L.rr_ctx_set_queue_limit(ctx.handle, W * H * spp - 1))
+        st = L.rr_pathtracer_execute(ctx.handle, scene.handle, C.byref(cam), C.byref(p), out.data_ptr(), _stream(torch))
+        assert st == 5, rr.RR_STATUS.get(st, st)           # RR_ERR_QUEUE_OVERFLOW
+        torch.cuda.synchronize()
+        assert bool((out == -3.0).all())                    # nothing ran
+        ctx.check(L.rr_ctx_set_queue_limit(ctx.handle, W * H * spp))
+        ctx.check(L.rr_pathtracer_execute(ctx.handle, scene.handle, C.byref(cam), C.byref(p), out.data_ptr(),
+                                          _stream(torch)))
+        torch.cuda.synchronize()
+        assert bool((out[..., 3] == 1.0).all())
+    finally:
+        ctx.check(L.rr_ctx_set_queue_limit(ctx.handle, 0))
 
 
 def test_guiding_splat_fit_sample_bit_exact(rr, O, ctx, torch_cuda):

@@ -133,3 +133,27 @@ def test_null_arguments_rejected_without_device(rr):
     assert L.rr_guiding_fit(None, None, None, None, None) == 1
     assert L.rr_host_scene_cornell(7, C.byref(C.c_void_p())) == 1
     assert L.rr_camera_build(None, None, None) == 1
+
+
+def test_inputs_library_builds_the_same_scenes_and_cameras(rr, O):
+    """The CPU reference arm builds its scene and camera with
+    oracle/librr_inputs.so (the generator source without CUDA); it must give
+    the same bytes as the product library's factories."""
+    I = O.inputs_lib()
+    pairs = [
+        (rr.HostScene.procedural(seed=0x5EED0002, target_triangles=60_000, emissive_triangles=256, box_half=20.0),
+         rr.HostScene.procedural(seed=0x5EED0002, target_triangles=60_000, emissive_triangles=256, box_half=20.0,
+                                 L=I)),
+        (rr.HostScene.instanced(seed=7, base_meshes=4, tris_per_mesh=500, instance_count=64, emissive_triangles=64,
+                                box_half=50.0),
+         rr.HostScene.instanced(seed=7, base_meshes=4, tris_per_mesh=500, instance_count=64, emissive_triangles=64,
+                                box_half=50.0, L=I)),
+        (rr.HostScene.cornell(0), rr.HostScene.cornell(0, L=I)),
+    ]
+    for a, b in pairs:
+        for k, v in a.arrays.items():
+            assert v.tobytes() == b.arrays[k].tobytes(), k
+    for eye, center in (((0.0, 4.0, 34.0), (0.0, -3.0, 0.0)), (None, None)):
+        ca = rr.camera_data(rr.camera_desc(1920, 1080, eye=eye, center=center))
+        cb = rr.camera_data(rr.camera_desc(1920, 1080, eye=eye, center=center, L=I), L=I)
+        assert bytes(ca) == bytes(cb)
