@@ -7,6 +7,7 @@ Outputs (git-ignored, shipped in-tree):
     research_b200/lib/librr_cuda.so   CUDA kernels + C ABI (include/rr_cuda.h)
     oracle/librr_oracle.so            CPU checker, built by oracle/Makefile
     oracle/librr_inputs.so            the seeded scene/camera generators without CUDA (CPU reference arm)
+    oracle/_ref/librr_slangref.so     the reference's shader text rewritten to C++ (only with the reference checkout)
 
 Numerics flags: the kernels are compiled without FMA contraction and with
 IEEE-rounded division and square root (-fmad=false -prec-div=true
@@ -89,12 +90,21 @@ def build_cuda(force: bool = False, ptxas_v: bool = False, jobs: int | None = No
     return LIB
 
 
+REFERENCE = Path("/root/reference")
+
+
 def build_oracle(force: bool = False) -> Path:
-    """Build the CPU checker (test infrastructure) via oracle/Makefile."""
+    """Build the CPU checker (test infrastructure) via oracle/Makefile: the
+    hand-written restatement, the seeded-input library and, where the
+    reference checkout is present, the reference's own shader text rewritten
+    to C++ (oracle/_ref/librr_slangref.so)."""
     out = ROOT / "oracle" / "librr_oracle.so"
     if force and out.exists():
         out.unlink()
     _run(["make", "-s", "-C", str(ROOT / "oracle")], quiet=True)
+    if (REFERENCE / "assets" / "shaders").is_dir():
+        _run(["make", "-s", "-C", str(ROOT / "oracle"), "ref", f"REFERENCE={REFERENCE}", f"PYTHON={sys.executable}"],
+             quiet=True)
     return out
 
 
