@@ -1,6 +1,7 @@
-"""Regression fixtures of tests/golden/ (written by tests/golden/make_golden.py
-with the CPU oracle on small seeded inputs): the oracle must still produce
-them bit for bit, and so must the CUDA kernels through the C ABI."""
+"""Fixtures of tests/golden/: outputs of the reference's own shader text,
+rewritten to C++ and run on the CPU by tests/golden/make_golden.py, on small
+seeded inputs. The reference-text run and the oracle must still produce them
+bit for bit, and so must the CUDA kernels through the C ABI."""
 import ctypes as C
 import sys
 from pathlib import Path
@@ -34,6 +35,17 @@ def test_oracle_reproduces_golden(rr, O):
     # the fixtures are not trivial
     assert _load("cornell_pt")["images"][..., :3].mean() > 0.05
     assert (_load("restir_di")["gbuf_pos"][..., 3] > 0).mean() > 0.5
+
+
+def test_reference_text_reproduces_golden(rr, O):
+    import slang_ref
+    if not slang_ref.available():
+        pytest.skip("the reference checkout is not present")
+    got = make_golden.compute_reference_text(rr, O, slang_ref)
+    for name, arrays in got.items():
+        ref = _load(name)
+        for k, v in arrays.items():
+            _same(v, ref[k], f"{name}.{k}")
 
 
 @pytest.mark.gpu
