@@ -5,6 +5,7 @@
 
 Outputs (git-ignored, shipped in-tree):
     research_b200/lib/librr_cuda.so   CUDA kernels + C ABI (include/rr_cuda.h)
+    research_b200/lib/librr_passes.so the RenderPass adapters (only with the reference's headers)
     oracle/librr_oracle.so            CPU checker, built by oracle/Makefile
     oracle/librr_inputs.so            the seeded scene/camera generators without CUDA (CPU reference arm)
     oracle/_ref/librr_slangref.so     the reference's shader text rewritten to C++ (only with the reference checkout)
@@ -91,6 +92,27 @@ def build_cuda(force: bool = False, ptxas_v: bool = False, jobs: int | None = No
 
 
 REFERENCE = Path("/root/reference")
+PASSES_LIB = LIBDIR / "librr_passes.so"
+ADAPTERS = PKG / "adapters"
+
+
+def build_passes(force: bool = False) -> Path | None:
+    """The RenderPass adapters (adapters/rr_passes.*) for a host that keeps the
+    reference's pass interface: compiled against that host's headers
+    (src/render/RenderPass.h and what it includes), here the reference
+    checkout's; skipped where it is absent. Links librr_cuda.so."""
+    hdr = REFERENCE / "src" / "render" / "RenderPass.h"
+    if not hdr.exists():
+        return PASSES_LIB if PASSES_LIB.exists() else None
+    src = ADAPTERS / "rr_passes.cpp"
+    deps = [src, ADAPTERS / "rr_passes.h", LIB, ROOT / "include" / "rr_cuda.h", ROOT / "include" / "rr_layouts.h"]
+    if force or _stale(PASSES_LIB, deps):
+        cuda = Path(_nvcc()).resolve().parent.parent
+        _run(["g++", "-O2", "-std=c++20", "-fPIC", "-Wall", "-shared", f"-I{REFERENCE / 'src'}",
+              f"-I{ROOT / 'include'}", f"-I{cuda / 'include'}", "-o", str(PASSES_LIB), str(src),
+              f"-L{LIBDIR}", "-lrr_cuda", f"-L{cuda / 'lib64'}", "-lcudart", "-Wl,-rpath,$ORIGIN",
+              f"-Wl,-rpath,{cuda / 'lib64'}"])
+    return PASSES_LIB
 
 
 def build_oracle(force: bool = False) -> Path:
@@ -116,6 +138,9 @@ def main(argv=None) -> int:
     a = ap.parse_args(argv)
     lib = build_cuda(force=a.force, ptxas_v=a.ptxas_v)
     print(f"built {lib}")
+    passes = build_passes(force=a.force)
+    if passes:
+        print(f"built {passes}")
     if not a.no_oracle:
         print(f"built {build_oracle(force=a.force)}")
     return 0

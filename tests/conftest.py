@@ -20,6 +20,7 @@ def built():
     """Build (incrementally) the CUDA library and the CPU checker."""
     from research_b200 import build
     build.build_cuda()
+    build.build_passes()
     build.build_oracle()
     return True
 
