@@ -11,7 +11,10 @@ frame sequence; only the timing is reduced).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-Prints exactly one JSON line on rank 0.
+Prints exactly one JSON line on rank 0. Beside the timed frames it reports,
+outside the timed region: `parity` (the benchmarked frame against the
+oracle), `cpu_baseline`, and `time_to_rmse` (the metric's second half:
+bench_guiding.measure on the same scene).
 """
 from __future__ import annotations
 
@@ -51,6 +54,10 @@ def parse():
     ap.add_argument("--triangles", type=int, default=CFG["triangles"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the oracle check of the benchmarked frame")
+    ap.add_argument("--no-time-to-rmse", action="store_true", help="skip the guiding time-to-RMSE measurement")
+    ap.add_argument("--rmse-budget-s", type=float, default=6.0,
+                    help="device seconds per method and repeat of the time-to-RMSE measurement")
+    ap.add_argument("--rmse-repeats", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
     ap.add_argument("--variants", default=None,
                     help="E,S: traversal variants for extension and shadow rays instead of the autotuner's choice "
@@ -570,6 +577,21 @@ def run_ours(args, ws, rank, local):
             cpu = {"value": v, "unit": UNIT, "cores": O.threads(), "kind": "port", "sample": d}
         oscene.close()
 
+    # the metric's second half: time to a relative RMSE of 1e-2, learned vs
+    # grid guiding (and unguided), on the same scene, one GPU
+    rmse = None
+    if rank == 0 and ws == 1 and not args.no_time_to_rmse:
+        import bench_guiding
+        r = bench_guiding.measure(rr, torch, ctx, scene, budget_s=args.rmse_budget_s, repeats=args.rmse_repeats)
+        for rs in r["runs"].values():
+            for x in rs:
+                x.pop("curve", None)
+        rmse = {"metric": "time to relative RMSE 1e-2 (learned vs vMF-grid guiding vs unguided)",
+                "workload": "procedural-room-1M-tris, 64x64 centre crop of the 1920x1080 view "
+                            "(Application::compute_mse's region), 256 spp per frame, 5 bounces",
+                "grid": "64^3 cells x 8 vMF lobes, FP64 EM statistics, decay 0.9, alpha 0.5",
+                "mlp": "80-64x4-48 BF16 tcgen05 MLP, Adam lr 1e-2, 2^18 samples per frame, alpha 0.5", **r}
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -591,7 +613,7 @@ def run_ours(args, ws, rank, local):
                 "scene": {"triangles": sst.triangle_count, "bvh_nodes": sst.bvh_node_count,
                           "bvh_depth": sst.bvh_max_depth, "bvh_build_ms": round(sst.build_ms, 1),
                           "lights": sst.light_count},
-                "traversal_per_step": counted, "autotune": tuned}
+                "traversal_per_step": counted, "autotune": tuned, "time_to_rmse": rmse}
         print(json.dumps(line), flush=True)
     scene.close()
     ctx.close()
