@@ -192,6 +192,20 @@ rr_status rr_batch_destroy(rr_batch* batch);
  * given configuration) and replay it; the per-call cameras, frame seed and
  * output pointers travel in a small table copied before the replay. */
 #define RR_PT_FLAG_GRAPH 4u
+/* Emitter sampling (no reference counterpart; the reference's NEE samples
+ * only its point and directional GpuLights, pathtracer.slang:124-177, and
+ * reaches emissive triangles only by BSDF sampling, :225-229). For
+ * rr_pathtracer_execute: next-event estimation picks, per vertex, the
+ * GpuLights (as the reference picks among them) or the scene's emissive
+ * triangles (each with probability 1/2 when both exist); an emissive
+ * triangle is picked in proportion to luminance(emission) x area and a
+ * point uniform on it, with its area-measure density turned into solid
+ * angle; BSDF bounces are weighted by the density brdf_sample actually
+ * draws from, and an emissive surface reached by a bounce is weighted
+ * against the emitter sample by the power heuristic. The default (flag
+ * clear) is the reference's estimator, bit for bit. Not for batches
+ * (RR_ERR_UNSUPPORTED). */
+#define RR_PT_FLAG_EMITTERS 8u
 
 /* cameras[i] and radiance_out[i] (spp images of cameras[i]'s size, device
  * memory) for scene i; params are shared by all scenes (frame_seed,

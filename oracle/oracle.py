@@ -66,6 +66,8 @@ _SIG = {
     "oracle_trace_batch": (None, [P, P, P, F32, F32, C.c_size_t, P, P, I]),
     "oracle_primary_ray": (None, [P, U32, U32, U32, P, P, C.POINTER(U32)]),
     "oracle_pathtrace": (None, [P, P, U32, U32, U32, U32, U32, U32, U32, P, I, P]),
+    "oracle_pathtrace_ex": (None, [P, P, U32, U32, U32, U32, U32, U32, U32, P, I, P, U32]),
+    "oracle_emitters": (U32, [P, P, P, P]),
     "oracle_accumulate": (None, [P, P, C.c_size_t, U32, U32]),
     "oracle_restir_di_initial": (None, [P, P, C.POINTER(DIParams), P, P, P, I]),
     "oracle_restir_di_temporal": (None, [P, P, C.POINTER(DIParams), P, P, P, P, I]),
@@ -208,16 +210,30 @@ def primary_ray(cam, px, py, frame_seed):
     return o, d, s.value
 
 
+PT_EMITTERS = 8   # ORACLE_PT_EMITTERS = RR_PT_FLAG_EMITTERS
+
+
 def pathtrace(scene: OracleScene, cam, frame_seed: int, max_bounces: int, spp: int = 1, region=None,
-              nthreads=None):
-    """Returns (images[spp, h, w, 4], (extension_rays, shadow_rays))."""
+              nthreads=None, flags: int = 0):
+    """Returns (images[spp, h, w, 4], (extension_rays, shadow_rays)).
+    flags=PT_EMITTERS: the emitter-sampling mode."""
     W, H = cam.screen_width, cam.screen_height
     x0, y0, w, h = region if region is not None else (0, 0, W, H)
     out = np.zeros((spp, h, w, 4), np.float32)
     stats = np.zeros(2, np.uint64)
-    lib().oracle_pathtrace(scene.handle, _cam_ptr(cam), frame_seed, max_bounces, spp, x0, y0, w, h, _p(out),
-                           nthreads or threads(), _p(stats))
+    lib().oracle_pathtrace_ex(scene.handle, _cam_ptr(cam), frame_seed, max_bounces, spp, x0, y0, w, h, _p(out),
+                              nthreads or threads(), _p(stats), flags)
     return out, (int(stats[0]), int(stats[1]))
+
+
+def emitters(scene: OracleScene):
+    """The emitter table: (records[n, 12], cdf[n], total power)."""
+    n = lib().oracle_emitters(scene.handle, None, None, None)
+    rec = np.zeros((n, 12), np.float32)
+    cdf = np.zeros(n, np.float32)
+    tot = np.zeros(1, np.float32)
+    lib().oracle_emitters(scene.handle, _p(rec) if n else None, _p(cdf) if n else None, _p(tot))
+    return rec, cdf, float(tot[0])
 
 
 def accumulate(radiance: np.ndarray, acc: np.ndarray, camera_moved: int, spp: int) -> None:

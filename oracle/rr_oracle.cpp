@@ -209,6 +209,39 @@ inline float brdf_pdf(V3 wo, V3 wi, V3 n, float roughness) {  // BRDF.slang:176-
     return 0.5f * pdf_spec + 0.5f * pdf_diff;
 }
 
+// The two densities of brdf_sample's direction wi (the library's
+// brdf_sample_pdfs): `ref`, the value brdf_sample returns as its pdf, and
+// `actual`, the density it really draws from (its specular branch samples
+// the GGX distribution of visible normals, G1(wo) D(h) / (4 wo.z), Heitz 2018,
+// written D / (2 (wo.z + sqrt(a^2 (wo.x^2 + wo.y^2) + wo.z^2)))). Not in the
+// reference: the emitter-sampling mode weights bounces by `actual`.
+struct BrdfPdfs { float ref, actual; };
+inline BrdfPdfs brdf_sample_pdfs(V3 wo, V3 n, V3 base, float metallic, float roughness, V3 wi) {
+    const float r = clampf(roughness, 0.04f, 1.0f);
+    const V3 F0 = lerp(v3(0.04f, 0.04f, 0.04f), base, metallic);
+    const V3 kS = fresnel_schlick(fmaxs(dot(n, wo), 0.0f), F0);
+    const float p_spec = clampf((kS.x + kS.y + kS.z) / 3.0f, 0.1f, 0.9f);
+    V3 T, B;
+    build_onb(n, T, B);
+    const V3 wo_l = world_to_tangent(wo, T, B, n);
+    const V3 wi_l = world_to_tangent(wi, T, B, n);
+    const float NdotWI = fmaxs(wi_l.z, 0.0f);
+    const V3 h = normalize(wo_l + wi_l);
+    const float NdotH = fmaxs(h.z, 1e-6f);
+    const float VdotH = fmaxs(dot(wo_l, h), 1e-6f);
+    const float a = r * r;
+    const float D = distribution_ggx(NdotH, a);
+    const float pdf_diff = NdotWI * kInvPi;
+    const float pdf_spec_ref = D * NdotH / fmaxs(4.0f * VdotH, 1e-6f);
+    const float vz = fmaxs(wo_l.z, 0.0f);
+    const float lam = sqrtf(a * a * (wo_l.x * wo_l.x + wo_l.y * wo_l.y) + vz * vz);
+    const float pdf_spec_vndf = D / fmaxs(2.0f * (vz + lam), 1e-12f);
+    BrdfPdfs q;
+    q.ref = fmaxs(p_spec * pdf_spec_ref + (1.0f - p_spec) * pdf_diff, 1e-6f);
+    q.actual = p_spec * pdf_spec_vndf + (1.0f - p_spec) * pdf_diff;
+    return q;
+}
+
 inline V3 sky(V3 dir) {  // pathtracer.slang:216-217
     float t = 0.5f * (dir.y + 1.0f);
     return lerp(v3(0.1f, 0.1f, 0.1f), v3(0.2f, 0.3f, 0.5f), t);
@@ -281,6 +314,13 @@ struct OracleScene {
     std::vector<uint32_t> order;     // BVH leaf order -> tri index
     std::vector<BNode> nodes;
     bool use_bvh = false;
+    // emitter table (the emitter-sampling mode): every triangle of an emissive
+    // material with non-zero area, instance-major; 12 floats each,
+    // (p0, Le.r), (e1, Le.g), (e2, Le.b), and the inclusive prefix sums of
+    // power = luminance(Le) * area
+    std::vector<float> emit;
+    std::vector<float> emit_cdf;
+    float emit_total = 0.0f;
 };
 
 namespace {
@@ -509,6 +549,169 @@ V3 trace_path(const OracleScene& s, const GpuCameraData& cam, uint32_t px, uint3
             if (rand_float(seed) > survive) break;
             throughput = throughput / survive;
         }
+        ray_orig = sf.pos + n * 1e-4f;
+        ray_dir = wi;
+    }
+    return radiance;
+}
+
+// ── Emitter sampling (no reference counterpart; the library's
+// RR_PT_FLAG_EMITTERS mode) ──────────────────────────────────────────────
+// Next-event estimation over the GpuLights (the reference's point and
+// directional lights, picked as sample_lights picks them) and the scene's
+// emissive triangles (picked in proportion to luminance(Le) * area, a point
+// uniform on the triangle), one group per vertex (each with probability 1/2
+// when both exist); bounces weighted by brdf_sample's actual density, and
+// emissive surfaces reached by a bounce weighted against the emitter sample
+// by the power heuristic.
+inline float lum709(V3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
+
+// Solid-angle density of the emitter sample at a point of emission Le seen
+// at squared distance d2 under |cos| cos_y from the shading point.
+inline float emitter_pdf(float p_group, float lum, float total, float d2, float cos_y) {
+    return p_group * (lum / total) * d2 / cos_y;
+}
+
+// First k with cdf[k] > target (n - 1 when none is).
+inline uint32_t emitter_search(const float* cdf, uint32_t n, float target) {
+    uint32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (cdf[mid] > target) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+
+// sample_lights (pathtracer.slang:124-177) with its light-count factor N
+// replaced by `scale` (N / probability of the GpuLight group).
+V3 sample_lights_scaled(const OracleScene& s, V3 hit_pos, V3 normal, V3 wo, const GpuMaterial& mat, uint32_t& seed,
+                        uint64_t& shadow_rays, float scale) {
+    const uint32_t N = (uint32_t)s.lights.size();
+    uint32_t light_idx = uint32_t(rand_float(seed) * float(N)) % N;
+    const GpuLight& light = s.lights[light_idx];
+    V3 light_dir; float dist; float pdf_light;
+    if (light.type == 0) {
+        V3 to_light = load3(light.position) - hit_pos;
+        dist = length(to_light);
+        light_dir = to_light / dist;
+        float r2 = dist * dist;
+        pdf_light = r2;
+    } else {
+        light_dir = normalize(-load3(light.direction));
+        dist = 1e9f;
+        pdf_light = 1.0f;
+    }
+    if (dot(light_dir, normal) <= 0.0f) return v3(0, 0, 0);
+    ++shadow_rays;
+    Hit sh = trace_scene<true>(s, hit_pos + normal * 1e-4f, light_dir, 0.001f, dist - 0.01f);
+    if (sh.hit) return v3(0, 0, 0);
+    V3 brdf_val = brdf_eval(normal, wo, light_dir, load3(mat.base_color), mat.metallic, mat.roughness);
+    float n_dot_l = fmaxs(dot(normal, light_dir), 0.0f);
+    float denom = light.type == 0 ? (pdf_light + 1e-6f) : 1.0f;
+    V3 irradiance = v3(light.emission[0] * light.intensity / denom,
+                       light.emission[1] * light.intensity / denom,
+                       light.emission[2] * light.intensity / denom);
+    float mis_weight = 1.0f;
+    if (light.type != 0) {
+        float pdf_bsdf = brdf_pdf(wo, light_dir, normal, mat.roughness);
+        mis_weight = (pdf_light * pdf_light) / (pdf_light * pdf_light + pdf_bsdf * pdf_bsdf + 1e-10f);
+    }
+    V3 r = brdf_val * irradiance;
+    r = r * n_dot_l;
+    r = r * mis_weight;
+    return r * scale;
+}
+
+V3 trace_path_emitters(const OracleScene& s, const GpuCameraData& cam, uint32_t px, uint32_t py,
+                       uint32_t frame_seed, uint32_t max_bounces, uint64_t& ext, uint64_t& shd) {
+    uint32_t seed = make_seed(px, py, frame_seed);
+    float jx = rand_float(seed);
+    float jy = rand_float(seed);
+    V3 ray_orig, ray_dir;
+    primary_ray(cam, px, py, jx, jy, ray_orig, ray_dir);
+    V3 radiance = v3(0, 0, 0), throughput = v3(1, 1, 1);
+    const uint32_t NL = (uint32_t)s.lights.size(), NE = (uint32_t)s.emit_cdf.size();
+    const float pe = NE == 0 ? 0.0f : (NL == 0 ? 1.0f : 0.5f);
+    float prev_pdf = 0.0f;   // bounce density of the ray (0: a camera ray)
+    for (uint32_t bounce = 0; bounce < max_bounces; ++bounce) {
+        ++ext;
+        Hit h = trace_scene<false>(s, ray_orig, ray_dir, 0.001f, 1e9f);
+        if (!h.hit) { radiance = radiance + throughput * sky(ray_dir); break; }
+        Surf sf = hit_surface(s, h);
+        const GpuMaterial& mat = s.materials[sf.material];
+        if (any_positive(mat.emissive)) {
+            const V3 Le = load3(mat.emissive);
+            float w = 1.0f;
+            if (prev_pdf > 0.0f) {
+                const Tri& t = s.tris[h.key];
+                const V3 ng = normalize(cross(t.p1 - t.p0, t.p2 - t.p0));
+                const float cos_y = fabsf(dot(ng, ray_dir));
+                const V3 dd = sf.pos - ray_orig;
+                const float pl = cos_y > 0.0f ? emitter_pdf(pe, lum709(Le), s.emit_total, dot(dd, dd), cos_y) : 0.0f;
+                const float a = prev_pdf * prev_pdf;
+                w = a / (a + pl * pl);
+            }
+            radiance = radiance + throughput * (Le * w);
+            break;
+        }
+        V3 wo = -ray_dir;
+        V3 n = sf.normal;
+        if (dot(n, wo) < 0.0f) n = -n;
+        const V3 base = load3(mat.base_color);
+        if (NL + NE > 0) {
+            const bool use_e = NE > 0 && (NL == 0 || rand_float(seed) < 0.5f);
+            if (use_e) {
+                const float u = rand_float(seed);
+                const float u1 = rand_float(seed);
+                const float u2 = rand_float(seed);
+                const uint32_t k = emitter_search(s.emit_cdf.data(), NE, u * s.emit_total);
+                const float* e = &s.emit[size_t(k) * 12];
+                const V3 p0 = v3(e[0], e[1], e[2]), E1 = v3(e[4], e[5], e[6]), E2 = v3(e[8], e[9], e[10]);
+                const V3 Le = v3(e[3], e[7], e[11]);
+                const float su = sqrtf(u1);
+                const float b1 = su * (1.0f - u2), b2 = su * u2;
+                const V3 y = p0 + E1 * b1 + E2 * b2;
+                const V3 to = y - sf.pos;
+                const float d2 = dot(to, to);
+                const float dist = sqrtf(d2);
+                const V3 l = to / dist;
+                const float cos_x = dot(n, l);
+                const V3 ny = normalize(cross(E1, E2));
+                const float cos_y = fabsf(dot(ny, l));
+                if (cos_x > 0.0f && cos_y > 0.0f && d2 > 0.0f) {
+                    const float pl = emitter_pdf(pe, lum709(Le), s.emit_total, d2, cos_y);
+                    const V3 f = brdf_eval(n, wo, l, base, mat.metallic, mat.roughness);
+                    const float pb = brdf_sample_pdfs(wo, n, base, mat.metallic, mat.roughness, l).actual;
+                    const float a = pl * pl;
+                    const float wl = a / (a + pb * pb);
+                    ++shd;
+                    Hit sh = trace_scene<true>(s, sf.pos + n * 1e-4f, l, 0.001f, dist - 0.01f);
+                    if (!sh.hit) {
+                        V3 c = f * Le;
+                        c = c * (cos_x * wl / pl);
+                        radiance = radiance + throughput * c;
+                    }
+                }
+            } else {
+                radiance = radiance + throughput * sample_lights_scaled(s, sf.pos, n, wo, mat, seed, shd,
+                                                                        float(NL) / (1.0f - pe));
+            }
+        }
+        float u0 = rand_float(seed);
+        float u1 = rand_float(seed);
+        V3 wi; float pdf;
+        V3 f = brdf_sample(wo, n, base, mat.metallic, mat.roughness, u0, u1, wi, pdf);
+        if (pdf < 1e-6f) break;
+        const float pa = brdf_sample_pdfs(wo, n, base, mat.metallic, mat.roughness, wi).actual;
+        if (!(pa > 0.0f)) break;
+        float n_dot_wi = fmaxs(dot(n, wi), 0.0f);
+        throughput = throughput * ((f * n_dot_wi) / pa);
+        if (bounce >= 3) {
+            float survive = fmins(fmaxs(throughput.x, fmaxs(throughput.y, throughput.z)), 0.95f);
+            if (rand_float(seed) > survive) break;
+            throughput = throughput / survive;
+        }
+        prev_pdf = pa;
         ray_orig = sf.pos + n * 1e-4f;
         ray_dir = wi;
     }
@@ -862,6 +1065,24 @@ OracleScene* oracle_scene_create(const GpuVertex* vertices, uint32_t vertex_coun
             s->tris.push_back(t);
         }
     }
+    {
+        double acc = 0.0;
+        for (const Tri& t : s->tris) {
+            const GpuMaterial& mat = materials[meshes[instances[t.inst].mesh_index].material_index];
+            if (!any_positive(mat.emissive)) continue;
+            const V3 e1 = t.p1 - t.p0, e2 = t.p2 - t.p0;
+            const V3 c = cross(e1, e2);
+            const float area = 0.5f * sqrtf(dot(c, c));
+            if (!(area > 0.0f)) continue;
+            const float lum = 0.2126f * mat.emissive[0] + 0.7152f * mat.emissive[1] + 0.0722f * mat.emissive[2];
+            acc += double(lum) * double(area);
+            const float rec[12] = {t.p0.x, t.p0.y, t.p0.z, mat.emissive[0], e1.x, e1.y, e1.z, mat.emissive[1],
+                                   e2.x, e2.y, e2.z, mat.emissive[2]};
+            s->emit.insert(s->emit.end(), rec, rec + 12);
+            s->emit_cdf.push_back(float(acc));
+        }
+        s->emit_total = float(acc);
+    }
     s->use_bvh = use_bvh != 0;
     if (s->use_bvh && !s->tris.empty()) {
         std::vector<float> cent(s->tris.size() * 3);
@@ -879,6 +1100,13 @@ OracleScene* oracle_scene_create(const GpuVertex* vertices, uint32_t vertex_coun
 }
 
 void oracle_scene_destroy(OracleScene* s) { delete s; }
+
+uint32_t oracle_emitters(const OracleScene* s, float* records_out, float* cdf_out, float* total_out) {
+    if (records_out) std::memcpy(records_out, s->emit.data(), s->emit.size() * sizeof(float));
+    if (cdf_out) std::memcpy(cdf_out, s->emit_cdf.data(), s->emit_cdf.size() * sizeof(float));
+    if (total_out) *total_out = s->emit_total;
+    return (uint32_t)s->emit_cdf.size();
+}
 uint32_t oracle_scene_triangle_count(const OracleScene* s) { return (uint32_t)s->tris.size(); }
 
 int oracle_trace(const OracleScene* s, const float origin[3], const float dir[3], float tmin,
@@ -922,12 +1150,20 @@ void oracle_primary_ray(const GpuCameraData* cam, uint32_t px, uint32_t py, uint
 void oracle_pathtrace(const OracleScene* s, const GpuCameraData* cam, uint32_t frame_seed,
                       uint32_t max_bounces, uint32_t spp, uint32_t x0, uint32_t y0, uint32_t w,
                       uint32_t h, float* out, int threads, uint64_t* stats) {
+    oracle_pathtrace_ex(s, cam, frame_seed, max_bounces, spp, x0, y0, w, h, out, threads, stats, 0u);
+}
+
+void oracle_pathtrace_ex(const OracleScene* s, const GpuCameraData* cam, uint32_t frame_seed,
+                         uint32_t max_bounces, uint32_t spp, uint32_t x0, uint32_t y0, uint32_t w,
+                         uint32_t h, float* out, int threads, uint64_t* stats, uint32_t flags) {
     std::atomic<uint64_t> ext_total{0}, shd_total{0};
+    const bool emitters = (flags & ORACLE_PT_EMITTERS) != 0;
     parallel_rows(h * spp, threads, [&](uint32_t row) {
         const uint32_t sidx = row / h, y = row % h;
         uint64_t ext = 0, shd = 0;
         for (uint32_t x = 0; x < w; ++x) {
-            V3 r = trace_path(*s, *cam, x0 + x, y0 + y, frame_seed + sidx, max_bounces, ext, shd);
+            V3 r = emitters ? trace_path_emitters(*s, *cam, x0 + x, y0 + y, frame_seed + sidx, max_bounces, ext, shd)
+                            : trace_path(*s, *cam, x0 + x, y0 + y, frame_seed + sidx, max_bounces, ext, shd);
             float* o = out + (((size_t)sidx * h + y) * w + x) * 4;
             o[0] = r.x; o[1] = r.y; o[2] = r.z; o[3] = 1.0f;
         }

@@ -77,6 +77,20 @@ void oracle_pathtrace(const OracleScene* scene, const GpuCameraData* cam,
                       uint32_t frame_seed, uint32_t max_bounces, uint32_t spp,
                       uint32_t x0, uint32_t y0, uint32_t w, uint32_t h,
                       float* out, int threads, uint64_t* stats);
+/* The same with flags: ORACLE_PT_EMITTERS selects the emitter-sampling mode
+ * (no reference counterpart; the library's RR_PT_FLAG_EMITTERS): NEE over the
+ * GpuLights and the emissive triangles (power-proportional pick, uniform
+ * point, area-measure density), bounces weighted by brdf_sample's actual
+ * density, emissive hits weighted by the power heuristic. */
+#define ORACLE_PT_EMITTERS 8u
+void oracle_pathtrace_ex(const OracleScene* scene, const GpuCameraData* cam,
+                         uint32_t frame_seed, uint32_t max_bounces, uint32_t spp,
+                         uint32_t x0, uint32_t y0, uint32_t w, uint32_t h,
+                         float* out, int threads, uint64_t* stats, uint32_t flags);
+/* The emitter table: count, total power, and (if out is non-null) the
+ * 12-float records followed by nothing else; cdf_out (nullable) receives
+ * the prefix sums. */
+uint32_t oracle_emitters(const OracleScene* scene, float* records_out, float* cdf_out, float* total_out);
 
 /* ── Accumulate (accumulate.slang:21-46) ────────────────────────────────── */
 void oracle_accumulate(const float* radiance, float* accumulated, size_t pixels,

@@ -16,6 +16,7 @@
 
 #include "rr_wavefront.cuh"
 #include "rr_batch.h"
+#include "rr_vmf.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -31,6 +32,7 @@ struct ShadeResult {
     float3 new_o = make_float3(0, 0, 0), wi = make_float3(0, 0, 0), thp = make_float3(0, 0, 0);
     float3 sh_o = make_float3(0, 0, 0), sh_d = make_float3(0, 0, 0), contrib = make_float3(0, 0, 0);
     float sh_tmax = 0.0f;
+    float pdf_next = 0.0f;   // RR_PT_FLAG_EMITTERS: the continuation's bounce density
 };
 
 // One ray of the shade stage (a = origin|pid, b = direction|seed, c =
@@ -125,9 +127,176 @@ RR_D void shade_ray(const DevScene& s, float4* __restrict__ out, uint32_t bounce
     }
 }
 
+// ── RR_PT_FLAG_EMITTERS (no reference counterpart) ──────────────────────
+// Next-event estimation over the GpuLights and the scene's emissive
+// triangles: per vertex one group (probability 1/2 each when both exist);
+// in the emitter group one triangle in proportion to luminance(Le) * area
+// (binary search of the prefix sums) and a point uniform on it, with the
+// solid-angle density p_l = P_E (luminance(Le) / total) d^2 / |cos_y|; the
+// GpuLight group is the reference's sample_lights with its factor N divided
+// by the group's probability. Bounces are weighted by f cos / p_act, the
+// density brdf_sample really draws from (rr_vmf.cuh), which the ray carries
+// on (c.w, 0 for camera rays) so that an emissive surface it reaches is
+// weighted p_act^2 / (p_act^2 + p_l^2) against the emitter sample's
+// p_l^2 / (p_l^2 + p_act^2) (power heuristic). Emissive surfaces still end
+// the path.
+RR_D float lum709(float3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
+
+RR_D float emitter_pdf(float p_group, float lum, float total, float d2, float cos_y) {
+    return p_group * (lum / total) * d2 / cos_y;
+}
+
+// First k with cdf[k] > target (n - 1 when none is).
+RR_D uint32_t emitter_search(const float* __restrict__ cdf, uint32_t n, float target) {
+    uint32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(cdf + mid) > target) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+
+RR_D void shade_ray_emitters(const DevScene& s, float4* __restrict__ out, uint32_t bounce, uint32_t last,
+                             const float4 a, const float4 b, const float4 c, const float4 h, ShadeResult& R) {
+    R.pid = __float_as_uint(a.w);
+    R.seed = __float_as_uint(b.w);
+    const float3 ray_dir = f3(b.x, b.y, b.z);
+    R.thp = f3(c.x, c.y, c.z);
+    const float prev_pdf = c.w;
+    const uint32_t inst = __float_as_uint(h.z);
+    const uint32_t NL = s.num_lights, NE = s.num_emitters;
+    const float pe = NE == 0 ? 0.0f : (NL == 0 ? 1.0f : 0.5f);
+    if (inst == kNoIndex) {
+        const float3 L = R.thp * sky_radiance(ray_dir);
+        float4 o = out[R.pid];
+        o.x = o.x + L.x; o.y = o.y + L.y; o.z = o.z + L.z;
+        out[R.pid] = o;
+        return;
+    }
+    const uint32_t prim = __float_as_uint(h.w);
+    const Surface sf = hit_surface(s, inst, prim, h.x, h.y);
+    const float4 m0 = __ldg(s.materials + sf.material * 2);
+    const float4 m1 = __ldg(s.materials + sf.material * 2 + 1);
+    if (m1.x > 0.0f || m1.y > 0.0f || m1.z > 0.0f) {
+        const float3 Le = f3(m1.x, m1.y, m1.z);
+        float w = 1.0f;
+        if (prev_pdf > 0.0f) {
+            const float3 ng = hit_geometric_normal(s, inst, prim);
+            const float cos_y = fabsf(dot(ng, ray_dir));
+            const float3 dd = sf.pos - f3(a.x, a.y, a.z);
+            const float pl = cos_y > 0.0f ? emitter_pdf(pe, lum709(Le), s.emit_total, dot(dd, dd), cos_y) : 0.0f;
+            const float aa = prev_pdf * prev_pdf;
+            w = aa / (aa + pl * pl);
+        }
+        const float3 L = R.thp * (Le * w);
+        float4 o = out[R.pid];
+        o.x = o.x + L.x; o.y = o.y + L.y; o.z = o.z + L.z;
+        out[R.pid] = o;
+        return;
+    }
+    const float3 wo = -ray_dir;
+    float3 n = sf.normal;
+    if (dot(n, wo) < 0.0f) n = -n;
+    const float3 base_c = f3(m0.x, m0.y, m0.z);
+    const float metallic = m0.w, roughness = m1.w;
+    if (NL + NE > 0) {
+        const bool use_e = NE > 0 && (NL == 0 || rand_float(R.seed) < 0.5f);
+        if (use_e) {
+            const float u = rand_float(R.seed);
+            const float u1 = rand_float(R.seed);
+            const float u2 = rand_float(R.seed);
+            const uint32_t k = emitter_search(s.emit_cdf, NE, u * s.emit_total);
+            const float4 e0 = __ldg(s.emitters + k * 3), e1 = __ldg(s.emitters + k * 3 + 1);
+            const float4 e2 = __ldg(s.emitters + k * 3 + 2);
+            const float3 E1 = xyz(e1), E2 = xyz(e2);
+            const float3 Le = f3(e0.w, e1.w, e2.w);
+            const float su = sqrtf(u1);
+            const float b1 = su * (1.0f - u2), b2 = su * u2;
+            const float3 y = xyz(e0) + E1 * b1 + E2 * b2;
+            const float3 to = y - sf.pos;
+            const float d2 = dot(to, to);
+            const float dist = sqrtf(d2);
+            const float3 l = to / dist;
+            const float cos_x = dot(n, l);
+            const float3 ny = normalize(cross(E1, E2));
+            const float cos_y = fabsf(dot(ny, l));
+            if (cos_x > 0.0f && cos_y > 0.0f && d2 > 0.0f) {
+                const float pl = emitter_pdf(pe, lum709(Le), s.emit_total, d2, cos_y);
+                const float3 f = brdf_eval(n, wo, l, base_c, metallic, roughness);
+                const float pb = brdf_sample_pdfs(wo, n, base_c, metallic, roughness, l).actual;
+                const float aa = pl * pl;
+                const float wl = aa / (aa + pb * pb);
+                float3 cc = f * Le;
+                cc = cc * (cos_x * wl / pl);
+                R.contrib = R.thp * cc;
+                R.sh_o = sf.pos + n * 1e-4f;
+                R.sh_d = l;
+                R.sh_tmax = dist - 0.01f;
+                R.emit_shadow = true;
+            }
+        } else {
+            // sample_lights (pathtracer.slang:124-177), factor N / (1 - P_E)
+            const uint32_t li = uint32_t(rand_float(R.seed) * float(NL)) % NL;
+            const float4 l0 = __ldg(s.lights + li * 3);
+            const float4 l1 = __ldg(s.lights + li * 3 + 1);
+            const float4 l2 = __ldg(s.lights + li * 3 + 2);
+            const bool is_point = __float_as_uint(l0.w) == 0u;
+            float3 ldir; float dist, pdf_light;
+            if (is_point) {
+                const float3 to = f3(l0.x, l0.y, l0.z) - sf.pos;
+                dist = length(to);
+                ldir = to / dist;
+                pdf_light = dist * dist;
+            } else {
+                ldir = normalize(-f3(l1.x, l1.y, l1.z));
+                dist = 1e9f;
+                pdf_light = 1.0f;
+            }
+            if (dot(ldir, n) > 0.0f) {
+                const float3 brdf_val = brdf_eval(n, wo, ldir, base_c, metallic, roughness);
+                const float n_dot_l = mx(dot(n, ldir), 0.0f);
+                const float den = is_point ? (pdf_light + 1e-6f) : 1.0f;
+                const float3 irr = f3(l2.x * l2.w / den, l2.y * l2.w / den, l2.z * l2.w / den);
+                float mis = 1.0f;
+                if (!is_point) {
+                    const float pb = brdf_pdf(wo, ldir, n, roughness);
+                    mis = (pdf_light * pdf_light) / (pdf_light * pdf_light + pb * pb + 1e-10f);
+                }
+                float3 Lr = brdf_val * irr;
+                Lr = Lr * n_dot_l;
+                Lr = Lr * mis;
+                Lr = Lr * (float(NL) / (1.0f - pe));
+                R.contrib = R.thp * Lr;
+                R.sh_o = sf.pos + n * 1e-4f;
+                R.sh_d = ldir;
+                R.sh_tmax = dist - 0.01f;
+                R.emit_shadow = true;
+            }
+        }
+    }
+    if (last) return;
+    const float u0 = rand_float(R.seed);
+    const float u1 = rand_float(R.seed);
+    float pdf;
+    const float3 f = brdf_sample(wo, n, base_c, metallic, roughness, u0, u1, R.wi, pdf);
+    if (pdf < 1e-6f) return;
+    const float pa = brdf_sample_pdfs(wo, n, base_c, metallic, roughness, R.wi).actual;
+    if (!(pa > 0.0f)) return;
+    const float ndwi = mx(dot(n, R.wi), 0.0f);
+    R.thp = R.thp * ((f * ndwi) / pa);
+    if (bounce >= 3) {
+        const float survive = mn(mx(R.thp.x, mx(R.thp.y, R.thp.z)), 0.95f);
+        if (rand_float(R.seed) > survive) return;
+        R.thp = R.thp / survive;
+    }
+    R.pdf_next = pa;
+    R.cont = true;
+    R.new_o = sf.pos + n * 1e-4f;
+}
+
 // Multi: a batch of scenes; a ray's scene index is in c.w, its scene is
 // table[index] and its image outs[index]; the index is carried on.
-template <bool Multi>
+template <bool Multi, bool Emit = false>
 __global__ void __launch_bounds__(kBlock, 4) shade_kernel(DevScene s, const DevScene* __restrict__ table,
                                                        float4* const* __restrict__ outs, uint32_t bounce,
                                                        uint32_t last, const float4* __restrict__ qa,
@@ -152,6 +321,8 @@ __global__ void __launch_bounds__(kBlock, 4) shade_kernel(DevScene s, const DevS
             if constexpr (Multi) {
                 sid = __float_as_uint(c.w);
                 shade_ray(table[sid], outs[sid], bounce, last, a, b, c, h, R);
+            } else if constexpr (Emit) {
+                shade_ray_emitters(s, out, bounce, last, a, b, c, h, R);
             } else {
                 shade_ray(s, out, bounce, last, a, b, c, h, R);
             }
@@ -167,7 +338,7 @@ __global__ void __launch_bounds__(kBlock, 4) shade_kernel(DevScene s, const DevS
         if (R.cont) {
             na[rslot] = make_float4(R.new_o.x, R.new_o.y, R.new_o.z, __uint_as_float(R.pid));
             nb[rslot] = make_float4(R.wi.x, R.wi.y, R.wi.z, __uint_as_float(R.seed));
-            nc[rslot] = make_float4(R.thp.x, R.thp.y, R.thp.z, tag);
+            nc[rslot] = make_float4(R.thp.x, R.thp.y, R.thp.z, Emit ? R.pdf_next : tag);
         }
     }
 }
@@ -224,7 +395,10 @@ extern "C" rr_status rr_pathtracer_execute(rr_ctx* ctx, const rr_scene* scene,
     ShadowKernel sh_k = count ? shadow_variant<true>(ctx->shadow_variant) : shadow_variant<false>(ctx->shadow_variant);
     const int g_ext = persistent_grid(ctx, reinterpret_cast<const void*>(ext_k));
     const int g_sh = persistent_grid(ctx, reinterpret_cast<const void*>(sh_k));
-    const int g_shade = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(shade_kernel<false>)),
+    const bool emitters = (p->flags & RR_PT_FLAG_EMITTERS) != 0;
+    using ShadeKernel = decltype(&shade_kernel<false, false>);
+    const ShadeKernel shade_k = emitters ? shade_kernel<false, true> : shade_kernel<false, false>;
+    const int g_shade = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(shade_k)),
                                       int((n + kBlock - 1) / kBlock));
     if (count) RR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->work64, 0, sizeof(unsigned long long) * 4, stream));
     const DevScene& S = scene->dev;
@@ -247,7 +421,7 @@ extern "C" rr_status rr_pathtracer_execute(rr_ctx* ctx, const rr_scene* scene,
         timer.end(1);
         if (overlap && b > 0) RR_TRY_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->shadowed[b - 1], 0));
         timer.begin(2);
-        shade_kernel<false><<<g_shade, kBlock, 0, stream>>>(S, nullptr, nullptr, b, b + 1 == p->max_bounces ? 1u : 0u,
+        shade_k<<<g_shade, kBlock, 0, stream>>>(S, nullptr, nullptr, b, b + 1 == p->max_bounces ? 1u : 0u,
                                                      q.ray_a[cur], q.ray_b[cur], q.ray_c[cur], q.hits,
                                                      q.ray_a[nxt], q.ray_b[nxt], q.ray_c[nxt],
                                                      q.shadow_a, q.shadow_b, q.shadow_c, out,
@@ -535,6 +709,8 @@ extern "C" rr_status rr_batch_execute(rr_ctx* ctx, rr_batch* B, const GpuCameraD
     const bool graph = (p->flags & RR_PT_FLAG_GRAPH) != 0;
     if (graph && (p->flags & (RR_PT_FLAG_COUNT_TRAVERSAL | RR_PT_FLAG_TIME_STAGES)))
         return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute: counting and timing flags need non-graph runs");
+    if (p->flags & RR_PT_FLAG_EMITTERS)
+        return rr_fail(ctx, RR_ERR_UNSUPPORTED, "rr_batch_execute: RR_PT_FLAG_EMITTERS is a single-scene mode");
     cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
     RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
     uint32_t tiles = 0;

@@ -38,6 +38,13 @@ struct DevScene {
     uint32_t num_tris;
     uint32_t num_materials;
     uint32_t num_nodes;
+    // Emissive triangles (RR_PT_FLAG_EMITTERS): world-space (p0, Le.r),
+    // (e1, Le.g), (e2, Le.b) per emitter, instance-major; emit_cdf holds the
+    // inclusive prefix sums of luminance(Le) * area, emit_total their total.
+    const float4* emitters;
+    const float* emit_cdf;
+    uint32_t num_emitters;
+    float emit_total;
 };
 
 // A ray with its shear constants (triangle test) and its slab-test
@@ -297,6 +304,21 @@ struct Surface {
     float3 pos, normal;
     uint32_t material;
 };
+
+// The hit triangle's unit geometric normal in world space, from its
+// vertices transformed as the scene's world-space triangles are.
+RR_D float3 hit_geometric_normal(const DevScene& s, uint32_t inst_idx, uint32_t prim) {
+    const float4* ip = s.instances + inst_idx * 5;
+    const float4 r0 = __ldg(ip + 0), r1 = __ldg(ip + 1), r2 = __ldg(ip + 2);
+    const uint32_t mesh_index = __float_as_uint(__ldg(ip + 4).x);
+    const uint4 m0 = __ldg(s.meshes + mesh_index * 2 + 0);
+    const uint32_t base = m0.z / 4u + prim * 3u;
+    const uint32_t i0 = __ldg(s.indices + base), i1 = __ldg(s.indices + base + 1), i2 = __ldg(s.indices + base + 2);
+    const float3 p0 = mul_rows_point(r0, r1, r2, xyz(__ldg(s.vertices + (m0.x + i0) * 3)), 1.0f);
+    const float3 p1 = mul_rows_point(r0, r1, r2, xyz(__ldg(s.vertices + (m0.x + i1) * 3)), 1.0f);
+    const float3 p2 = mul_rows_point(r0, r1, r2, xyz(__ldg(s.vertices + (m0.x + i2) * 3)), 1.0f);
+    return normalize(cross(p1 - p0, p2 - p0));
+}
 
 RR_D Surface hit_surface(const DevScene& s, uint32_t inst_idx, uint32_t prim, float bu, float bv) {
     const float4* ip = s.instances + inst_idx * 5;

@@ -10,6 +10,7 @@
 #include "rr_internal.h"
 
 #include <chrono>
+#include <cmath>
 #include <cstring>
 #include <thread>
 
@@ -185,6 +186,32 @@ rr_status rr_scene_create(rr_ctx* ctx, const rr_scene_desc* d, rr_scene** out) {
         std::memcpy(&c.w, &t, 4);
         trirec[size_t(i) * 3] = a; trirec[size_t(i) * 3 + 1] = b; trirec[size_t(i) * 3 + 2] = c;
     }
+    // Emitter table: every triangle of an emissive material with non-zero
+    // area, instance-major, with the prefix sums of luminance(Le) * area.
+    std::vector<float4> emit;
+    std::vector<float> emit_cdf;
+    float emit_total = 0.0f;
+    {
+        double acc = 0.0;
+        for (uint32_t k = 0; k < ntri; ++k) {
+            const GpuMaterial& g = d->materials[d->meshes[d->instances[tri_inst[k]].mesh_index].material_index];
+            if (!(g.emissive[0] > 0.0f || g.emissive[1] > 0.0f || g.emissive[2] > 0.0f)) continue;
+            const float* w = &world[size_t(k) * 9];
+            const float e1[3] = {w[3] - w[0], w[4] - w[1], w[5] - w[2]};
+            const float e2[3] = {w[6] - w[0], w[7] - w[1], w[8] - w[2]};
+            const float c[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                                e1[0] * e2[1] - e1[1] * e2[0]};
+            const float area = 0.5f * std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+            if (!(area > 0.0f)) continue;
+            const float lum = 0.2126f * g.emissive[0] + 0.7152f * g.emissive[1] + 0.0722f * g.emissive[2];
+            acc += double(lum) * double(area);
+            emit.push_back(make_float4(w[0], w[1], w[2], g.emissive[0]));
+            emit.push_back(make_float4(e1[0], e1[1], e1[2], g.emissive[1]));
+            emit.push_back(make_float4(e2[0], e2[1], e2[2], g.emissive[2]));
+            emit_cdf.push_back(float(acc));
+        }
+        emit_total = float(acc);
+    }
     std::vector<float4> mats(size_t(d->material_count) * 2);
     for (uint32_t m = 0; m < d->material_count; ++m) {
         const GpuMaterial& g = d->materials[m];
@@ -222,7 +249,11 @@ rr_status rr_scene_create(rr_ctx* ctx, const rr_scene_desc* d, rr_scene** out) {
     RR_UP(d->instances, size_t(d->instance_count) * sizeof(GpuInstance), instances, const float4*);
     RR_UP(mats.data(), mats.size() * sizeof(float4), materials, const float4*);
     RR_UP(d->light_count ? d->lights : nullptr, size_t(d->light_count) * sizeof(GpuLight), lights, const float4*);
+    RR_UP(emit.empty() ? nullptr : emit.data(), emit.size() * sizeof(float4), emitters, const float4*);
+    RR_UP(emit_cdf.empty() ? nullptr : emit_cdf.data(), emit_cdf.size() * sizeof(float), emit_cdf, const float*);
 #undef RR_UP
+    s->dev.num_emitters = uint32_t(emit_cdf.size());
+    s->dev.emit_total = emit_total;
     s->dev.num_lights = d->light_count;
     s->dev.num_instances = d->instance_count;
     s->dev.num_tris = ntri;

@@ -68,6 +68,7 @@ class PtTuneResult(C.Structure):
 PT_FLAG_COUNT_TRAVERSAL = 1
 PT_FLAG_TIME_STAGES = 2
 PT_FLAG_GRAPH = 4
+PT_FLAG_EMITTERS = 8
 PT_VARIANT_COUNT = 8
 BATCH_WAVEFRONT = 0
 BATCH_PER_SCENE = 1

@@ -597,6 +597,37 @@ def _edge_scenes(rr):
     return out
 
 
+@pytest.mark.parametrize("name", ["cornell", "cornell_emitters_only", "procedural", "procedural_emitters_only",
+                                  "directional", "no_lights", "no_geometry"])
+def test_pathtracer_emitters_bit_exact(rr, O, ctx, torch_cuda, procedural, name):
+    """RR_PT_FLAG_EMITTERS (next-event estimation over the GpuLights and the
+    emissive triangles, MIS with bounces weighted by brdf_sample's actual
+    density) against the oracle: both light groups, emissive triangles
+    only, GpuLights only (directional MIS branch), nothing to sample, nothing
+    in view."""
+    torch = torch_cuda
+    cornell = rr.HostScene.cornell(0).arrays
+    scenes = {"cornell": (cornell, "cornell", 8), "procedural": (procedural[0], "procedural", 5),
+              "cornell_emitters_only": (dict(cornell, lights=np.zeros(0, rr.LIGHT)), "cornell", 8),
+              "procedural_emitters_only": (dict(procedural[0], lights=np.zeros(0, rr.LIGHT)), "procedural", 5)}
+    edge = _edge_scenes(rr)
+    arrays, view, depth = scenes[name] if name in scenes else (edge[name], "cornell", 6)
+    scene = rr.Scene(ctx, arrays)
+    osc = O.OracleScene(arrays)
+    W, H = 56, 40
+    cam = cam_for(rr, view, W, H)
+    out = torch.empty((3, H, W, 4), device="cuda")
+    ctx.check(rr.lib().rr_pathtracer_execute(ctx.handle, scene.handle, C.byref(cam),
+                                             C.byref(rr.PtParams(7, depth, 3, rr.PT_FLAG_EMITTERS)), out.data_ptr(),
+                                             _stream(torch)))
+    torch.cuda.synchronize()
+    want, _ = O.pathtrace(osc, cam, 7, depth, 3, flags=O.PT_EMITTERS)
+    np.testing.assert_array_equal(_np(out).view(np.uint32), want.view(np.uint32))
+    if name in ("cornell", "procedural"):
+        assert float(want[..., :3].mean()) > 0.0
+    scene.close()
+
+
 @pytest.mark.parametrize("name", ["directional", "no_lights", "no_geometry"])
 def test_edge_scenes_bit_exact(rr, O, ctx, torch_cuda, name):
     torch = torch_cuda
