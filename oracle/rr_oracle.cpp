@@ -683,7 +683,9 @@ V3 trace_path_emitters(const OracleScene& s, const GpuCameraData& cam, uint32_t 
                     const V3 f = brdf_eval(n, wo, l, base, mat.metallic, mat.roughness);
                     const float pb = brdf_sample_pdfs(wo, n, base, mat.metallic, mat.roughness, l).actual;
                     const float a = pl * pl;
-                    const float wl = a / (a + pb * pb);
+                    // the last vertex traces no bounce that could reach the
+                    // emitter: its sample carries the whole weight there
+                    const float wl = bounce + 1 == max_bounces ? 1.0f : a / (a + pb * pb);
                     ++shd;
                     Hit sh = trace_scene<true>(s, sf.pos + n * 1e-4f, l, 0.001f, dist - 0.01f);
                     if (!sh.hit) {

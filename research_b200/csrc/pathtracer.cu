@@ -138,8 +138,9 @@ RR_D void shade_ray(const DevScene& s, float4* __restrict__ out, uint32_t bounce
 // density brdf_sample really draws from (rr_vmf.cuh), which the ray carries
 // on (c.w, 0 for camera rays) so that an emissive surface it reaches is
 // weighted p_act^2 / (p_act^2 + p_l^2) against the emitter sample's
-// p_l^2 / (p_l^2 + p_act^2) (power heuristic). Emissive surfaces still end
-// the path.
+// p_l^2 / (p_l^2 + p_act^2) (power heuristic; at the last vertex, which
+// traces no bounce, the emitter sample's weight is 1). Emissive surfaces
+// still end the path.
 RR_D float lum709(float3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
 
 RR_D float emitter_pdf(float p_group, float lum, float total, float d2, float cos_y) {
@@ -225,7 +226,9 @@ RR_D void shade_ray_emitters(const DevScene& s, float4* __restrict__ out, uint32
                 const float3 f = brdf_eval(n, wo, l, base_c, metallic, roughness);
                 const float pb = brdf_sample_pdfs(wo, n, base_c, metallic, roughness, l).actual;
                 const float aa = pl * pl;
-                const float wl = aa / (aa + pb * pb);
+                // the last vertex traces no bounce that could reach the
+                // emitter: its sample carries the whole weight there
+                const float wl = last ? 1.0f : aa / (aa + pb * pb);
                 float3 cc = f * Le;
                 cc = cc * (cos_x * wl / pl);
                 R.contrib = R.thp * cc;
