@@ -203,8 +203,9 @@ rr_status rr_batch_destroy(rr_batch* batch);
  * angle; BSDF bounces are weighted by the density brdf_sample actually
  * draws from, and an emissive surface reached by a bounce is weighted
  * against the emitter sample by the power heuristic. The default (flag
- * clear) is the reference's estimator, bit for bit. Not for batches
- * (RR_ERR_UNSUPPORTED). */
+ * clear) is the reference's estimator, bit for bit. Also for
+ * rr_guided_pathtracer_execute, where the bounce density in the weights is
+ * the guided mixture's. Not for batches (RR_ERR_UNSUPPORTED). */
 #define RR_PT_FLAG_EMITTERS 8u
 
 /* cameras[i] and radiance_out[i] (spp images of cameras[i]'s size, device

@@ -115,7 +115,26 @@ struct GuideRefs {
 // (Multi) at slot_map[i] (~0: none). Multi: a batch of scenes; a ray's scene
 // index is in c.w, its scene is table[index], its image outs[index] and its
 // guide gtab[index]; the index is carried on to the next queues.
-template <bool SlotMixture, bool Multi>
+// Emit: RR_PT_FLAG_EMITTERS (single scene): next-event estimation also over
+// the emissive triangles, as shade_ray_emitters in pathtracer.cu, with the
+// bounce's density being the guided mixture alpha p_guide + (1 - alpha)
+// p_act (no actual/ref factor: the estimator is unbiased for the rendering
+// equation), carried on in the ray record's .w for the MIS weight of an
+// emissive surface the bounce reaches.
+RR_D float emitter_pdf(float p_group, float lum, float total, float d2, float cos_y) {
+    return p_group * (lum / total) * d2 / cos_y;
+}
+
+RR_D uint32_t emitter_search(const float* __restrict__ cdf, uint32_t n, float target) {
+    uint32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(cdf + mid) > target) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+
+template <bool SlotMixture, bool Multi, bool Emit = false>
 __global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s0, GuidedLaunch G,
                                                               const DevScene* __restrict__ table,
                                                               float4* const* __restrict__ outs,
@@ -140,6 +159,7 @@ __global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s0, Gu
         float3 new_o = f3(0, 0, 0), wi = f3(0, 0, 0), thp = f3(0, 0, 0);
         float3 sh_o = f3(0, 0, 0), sh_d = f3(0, 0, 0), contrib = f3(0, 0, 0);
         float sh_tmax = 0.0f;
+        float pdf_next = 0.0f;
         if (i < count) {
             const float4 a = qa[i], b = qb[i], c = qc[i];
             const float4 h = hits[i];
@@ -170,7 +190,23 @@ __global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s0, Gu
                 const float4 m0 = __ldg(s.materials + sf.material * 2);
                 const float4 m1 = __ldg(s.materials + sf.material * 2 + 1);
                 if (m1.x > 0.0f || m1.y > 0.0f || m1.z > 0.0f) {
-                    const float3 L = thp * f3(m1.x, m1.y, m1.z);
+                    float w = 1.0f;
+                    if constexpr (Emit) {
+                        const float prev_pdf = c.w;
+                        if (prev_pdf > 0.0f) {
+                            const uint32_t NL = s.num_lights, NE = s.num_emitters;
+                            const float pe = NE == 0 ? 0.0f : (NL == 0 ? 1.0f : 0.5f);
+                            const float3 ng = hit_geometric_normal(s, inst, __float_as_uint(h.w));
+                            const float cos_y = fabsf(dot(ng, ray_dir));
+                            const float3 dd = sf.pos - f3(a.x, a.y, a.z);
+                            const float pl = cos_y > 0.0f ? emitter_pdf(pe, lum709(f3(m1.x, m1.y, m1.z)), s.emit_total,
+                                                                        dot(dd, dd), cos_y)
+                                                          : 0.0f;
+                            const float aa = prev_pdf * prev_pdf;
+                            w = aa / (aa + pl * pl);
+                        }
+                    }
+                    const float3 L = thp * (f3(m1.x, m1.y, m1.z) * w);
                     o.x = o.x + L.x; o.y = o.y + L.y; o.z = o.z + L.z;
                     out[pid] = o;
                 } else {
@@ -179,7 +215,59 @@ __global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s0, Gu
                     if (dot(n, wo) < 0.0f) n = -n;
                     const float3 base_c = f3(m0.x, m0.y, m0.z);
                     const float metallic = m0.w, roughness = m1.w;
-                    if (s.num_lights > 0) {  // NEE exactly as the reference
+                    VmfMixture mix;
+                    bool valid = false;
+                    if (!G.last) {
+                        if constexpr (SlotMixture) {
+                            const uint32_t slot = Multi ? slot_map[i] : i;
+                            if (slot != kNoIndex) load_mixture_slot(G.mix, slot, mix, valid);
+                        } else {
+                            load_mixture_grid(R.grid, sf.pos, mix, valid);
+                        }
+                    }
+                    bool nee_done = false;
+                    if constexpr (Emit) {
+                        const uint32_t NL = s.num_lights, NE = s.num_emitters;
+                        const float pe = NE == 0 ? 0.0f : (NL == 0 ? 1.0f : 0.5f);
+                        if (NE > 0 && (NL == 0 || rand_float(seed) < 0.5f)) {
+                            nee_done = true;
+                            const float u = rand_float(seed);
+                            const float u1 = rand_float(seed);
+                            const float u2 = rand_float(seed);
+                            const uint32_t k = emitter_search(s.emit_cdf, NE, u * s.emit_total);
+                            const float4 e0 = __ldg(s.emitters + k * 3), e1 = __ldg(s.emitters + k * 3 + 1);
+                            const float4 e2 = __ldg(s.emitters + k * 3 + 2);
+                            const float3 E1 = xyz(e1), E2 = xyz(e2);
+                            const float3 Le = f3(e0.w, e1.w, e2.w);
+                            const float su = sqrtf(u1);
+                            const float3 y = xyz(e0) + E1 * (su * (1.0f - u2)) + E2 * (su * u2);
+                            const float3 to = y - sf.pos;
+                            const float d2 = dot(to, to);
+                            const float dist = sqrtf(d2);
+                            const float3 l = to / dist;
+                            const float cos_x = dot(n, l);
+                            const float cos_y = fabsf(dot(normalize(cross(E1, E2)), l));
+                            if (cos_x > 0.0f && cos_y > 0.0f && d2 > 0.0f) {
+                                const float pl = emitter_pdf(pe, lum709(Le), s.emit_total, d2, cos_y);
+                                float wl = 1.0f;   // the last vertex traces no bounce
+                                if (!G.last) {
+                                    const float alpha = valid ? R.alpha : 0.0f;
+                                    const float pg = valid ? mixture_pdf(mix, G.lobes, l) : 0.0f;
+                                    const float pb = alpha * pg + (1.0f - alpha) *
+                                                     brdf_sample_pdfs(wo, n, base_c, metallic, roughness, l).actual;
+                                    const float aa = pl * pl;
+                                    wl = aa / (aa + pb * pb);
+                                }
+                                const float3 f = brdf_eval(n, wo, l, base_c, metallic, roughness);
+                                contrib = thp * ((f * Le) * (cos_x * wl / pl));
+                                sh_o = sf.pos + n * 1e-4f;
+                                sh_d = l;
+                                sh_tmax = dist - 0.01f;
+                                emit_shadow = true;
+                            }
+                        }
+                    }
+                    if (!nee_done && s.num_lights > 0) {  // NEE as the reference (the GpuLight group)
                         const uint32_t N = s.num_lights;
                         const uint32_t li = uint32_t(rand_float(seed) * float(N)) % N;
                         const float4 l0 = __ldg(s.lights + li * 3);
@@ -207,7 +295,11 @@ __global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s0, Gu
                                 const float pb = brdf_pdf(wo, ldir, n, roughness);
                                 mis = (pdf_light * pdf_light) / (pdf_light * pdf_light + pb * pb + 1e-10f);
                             }
-                            contrib = thp * ((((brdf_val * irr) * n_dot_l) * mis) * float(N));
+                            float scale = float(N);
+                            if constexpr (Emit) {
+                                if (s.num_emitters > 0) scale = float(N) / 0.5f;   // the GpuLight group's probability
+                            }
+                            contrib = thp * ((((brdf_val * irr) * n_dot_l) * mis) * scale);
                             sh_o = sf.pos + n * 1e-4f;
                             sh_d = ldir;
                             sh_tmax = dist - 0.01f;
@@ -215,15 +307,6 @@ __global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s0, Gu
                         }
                     }
                     if (!G.last) {
-                        VmfMixture mix;
-                        bool valid;
-                        if constexpr (SlotMixture) {
-                            const uint32_t slot = Multi ? slot_map[i] : i;
-                            valid = false;
-                            if (slot != kNoIndex) load_mixture_slot(G.mix, slot, mix, valid);
-                        } else {
-                            load_mixture_grid(R.grid, sf.pos, mix, valid);
-                        }
                         const float alpha = valid ? R.alpha : 0.0f;
                         const float u_sel = rand_float(seed);
                         const float u0 = rand_float(seed);
@@ -246,7 +329,7 @@ __global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s0, Gu
                             const BrdfPdfs pb = brdf_sample_pdfs(wo, n, base_c, metallic, roughness, wi);
                             const float pg = valid ? mixture_pdf(mix, G.lobes, wi) : 0.0f;
                             pdf = alpha * pg + (1.0f - alpha) * pb.actual;
-                            ratio = pb.actual / pb.ref;
+                            ratio = Emit ? 1.0f : pb.actual / pb.ref;
                         }
                         if (pdf > 1e-6f) {
                             const float3 f = brdf_eval(n, wo, wi, base_c, metallic, roughness);
@@ -259,6 +342,7 @@ __global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s0, Gu
                             }
                             if (alive) {
                                 cont = true;
+                                pdf_next = pdf;
                                 new_o = sf.pos + n * 1e-4f;
                                 const size_t r = size_t(G.bounce) * R.paths + pid;
                                 R.rec0[r] = make_float4(sf.pos.x, sf.pos.y, sf.pos.z, pdf);
@@ -282,7 +366,7 @@ __global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s0, Gu
         if (cont) {
             na[rslot] = make_float4(new_o.x, new_o.y, new_o.z, __uint_as_float(pid));
             nb[rslot] = make_float4(wi.x, wi.y, wi.z, __uint_as_float(seed));
-            nc[rslot] = make_float4(thp.x, thp.y, thp.z, tag);
+            nc[rslot] = make_float4(thp.x, thp.y, thp.z, Emit ? pdf_next : tag);
         }
     }
 }
@@ -808,7 +892,9 @@ extern "C" rr_status rr_guided_pathtracer_execute(rr_ctx* ctx, const rr_scene* s
     ShadowKernel sh_k = shadow_variant<false>(ctx->shadow_variant);
     const int g_ext = persistent_grid(ctx, reinterpret_cast<const void*>(ext_k));
     const int g_sh = persistent_grid(ctx, reinterpret_cast<const void*>(sh_k));
-    auto shade_k = mlp ? guided_shade_kernel<true, false> : guided_shade_kernel<false, false>;
+    const bool emitters = (p->flags & RR_PT_FLAG_EMITTERS) != 0;
+    auto shade_k = mlp ? (emitters ? guided_shade_kernel<true, false, true> : guided_shade_kernel<true, false, false>)
+                       : (emitters ? guided_shade_kernel<false, false, true> : guided_shade_kernel<false, false, false>);
     const int g_shade = std::min<int>(persistent_grid(ctx, reinterpret_cast<const void*>(shade_k)),
                                       int((n + kBlock - 1) / kBlock));
     GuidedLaunch G;
@@ -1185,6 +1271,8 @@ extern "C" rr_status rr_batch_execute_guided(rr_ctx* ctx, rr_batch* B, const Gpu
     if (B->ctx != ctx) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute_guided: batch of another context");
     if (p->spp == 0 || p->max_bounces == 0 || p->max_bounces > uint32_t(kMaxBounces))
         return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_batch_execute_guided: bad spp or max_bounces");
+    if (p->flags & RR_PT_FLAG_EMITTERS)
+        return rr_fail(ctx, RR_ERR_UNSUPPORTED, "rr_batch_execute_guided: RR_PT_FLAG_EMITTERS is a single-scene mode");
     const uint32_t count = uint32_t(B->scenes.size());
     for (uint32_t i = 0; i < count; ++i)
         if (!guides[i] || guides[i]->ctx != ctx)

@@ -249,12 +249,12 @@ def test_grid_em_update_matches_fp64_restatement(rr, ctx, torch_cuda):
     rr.lib().rr_guide_destroy(g)
 
 
-def _render(rr, ctx, torch, scene, cam, frames, guide=None, train=True, spp=1, bounces=5):
+def _render(rr, ctx, torch, scene, cam, frames, guide=None, train=True, spp=1, bounces=5, flags=0):
     W, H = cam.screen_width, cam.screen_height
     acc = np.zeros((H, W, 3))
     rad = torch.empty((spp, H, W, 4), device="cuda")
     for f in range(frames):
-        p = rr.PtParams(1000 + f * spp, bounces, spp, 0)
+        p = rr.PtParams(1000 + f * spp, bounces, spp, flags)
         if guide is None:
             ctx.check(rr.lib().rr_pathtracer_execute(ctx.handle, scene.handle, C.byref(cam), C.byref(p),
                                                      rad.data_ptr(), _stream(torch)))
@@ -327,6 +327,29 @@ def test_guided_pathtracer_is_unbiased(rr, ctx, torch_cuda, kind):
     assert abs(mg - mp) / mp < 0.03, (mg, mp)
     rr.lib().rr_guide_destroy(g)
     scene.close()
+
+
+@pytest.mark.parametrize("kind", ["grid", "mlp"])
+def test_guided_emitter_mode_is_unbiased(rr, ctx, torch_cuda, kind):
+    """RR_PT_FLAG_EMITTERS in the guided tracer (emitter samples weighted
+    against the guided mixture's density) converges to the unguided
+    emitter-mode image: same mean on the Cornell box with its point light and
+    emissive quad, and on the quad alone."""
+    torch = torch_cuda
+    base = rr.HostScene.cornell(1).arrays
+    for arrays in (base, dict(base, lights=np.zeros(0, rr.LIGHT))):
+        scene = rr.Scene(ctx, arrays)
+        cam = rr.camera_data(rr.camera_desc(48, 48))
+        g = make_guide(rr, ctx, rr.GUIDE_GRID if kind == "grid" else rr.GUIDE_MLP, bmin=(-1.01,) * 3,
+                       bmax=(1.01,) * 3, res=16, batch=1 << 14, max_samples=1 << 18)
+        E = rr.PT_FLAG_EMITTERS
+        _render(rr, ctx, torch, scene, cam, 16, guide=g, train=True, spp=4, flags=E)
+        guided = _render(rr, ctx, torch, scene, cam, 96, guide=g, train=False, spp=4, flags=E)
+        plain = _render(rr, ctx, torch, scene, cam, 96, spp=4, flags=E)
+        mg, mp = guided.mean(), plain.mean()
+        assert abs(mg - mp) / mp < 0.02, (len(arrays["lights"]), mg, mp)
+        rr.lib().rr_guide_destroy(g)
+        scene.close()
 
 
 @pytest.mark.parametrize("kind", ["grid", "mlp"])
