@@ -39,20 +39,24 @@ rr_status rr_host_scene_cornell(int variant, rr_host_scene** out);
  * emitting triangles with log-uniform radiance [0.1, 100], each also
  * registered as a point light at its centroid (emission = radiance,
  * intensity = area), mirroring the reference Cornell box, whose emitter has
- * both an emissive quad and a point light. */
+ * both an emissive quad and a point light. flags: RR_SCENE_NO_EMITTER_LIGHTS
+ * leaves those point lights out (the same geometry and materials), for the
+ * emitter-sampling mode (RR_PT_FLAG_EMITTERS), which samples the emissive
+ * triangles themselves. */
+#define RR_SCENE_NO_EMITTER_LIGHTS 1u
 typedef struct rr_procedural_params {
     uint64_t seed;
     uint32_t target_triangles;
     uint32_t emissive_triangles;
     float    box_half;
-    uint32_t _pad;
+    uint32_t flags;
 } rr_procedural_params;
 rr_status rr_host_scene_procedural(const rr_procedural_params* p, rr_host_scene** out);
 
 /* Seeded instanced scene: base_meshes meshes of tris_per_mesh triangles,
  * instance_count instances under random affine transforms (rotation,
  * uniform scale [0.2, 3], translation in a [-box_half, box_half]^3 box) and
- * emissive_triangles emitters (+ point lights as above). */
+ * emissive_triangles emitters (+ point lights as above; flags as above). */
 typedef struct rr_instanced_params {
     uint64_t seed;
     uint32_t base_meshes;
@@ -60,7 +64,7 @@ typedef struct rr_instanced_params {
     uint32_t instance_count;
     uint32_t emissive_triangles;
     float    box_half;
-    uint32_t _pad;
+    uint32_t flags;
 } rr_instanced_params;
 rr_status rr_host_scene_instanced(const rr_instanced_params* p, rr_host_scene** out);
 

@@ -198,8 +198,9 @@ void icosphere(int subdiv, std::vector<F3>& pts, std::vector<uint32_t>& idx) {
     }
 }
 
-// One single-triangle emitter mesh + material + point light.
-void add_emitter(rr_host_scene& s, Rng& rng, float box_half, float size_lo, float size_hi) {
+// One single-triangle emitter mesh + material (+ a point light at it when
+// point_light: the same geometry and random draws either way).
+void add_emitter(rr_host_scene& s, Rng& rng, float box_half, float size_lo, float size_hi, bool point_light) {
     const F3 c = f3(rng.uni(-box_half, box_half), rng.uni(-box_half, box_half), rng.uni(-box_half, box_half));
     F3 n = norm3(f3(rng.uni(-1, 1), rng.uni(-1, 1), rng.uni(-1, 1)));
     if (!(dot3(n, n) > 0.5f)) n = f3(0, -1, 0);
@@ -224,6 +225,7 @@ void add_emitter(rr_host_scene& s, Rng& rng, float box_half, float size_lo, floa
     const uint32_t mat = uint32_t(s.materials.size());
     s.materials.push_back(make_material(f3(1, 1, 1), 0.0f, 1.0f, emit));
     add_mesh(s, v, idx, mat, nullptr);
+    if (!point_light) return;
     const float area = 0.5f * std::sqrt(dot3(e, e));
     GpuLight l{};
     const F3 lp = add(c, scl(n, 0.05f));
@@ -416,7 +418,8 @@ rr_status rr_host_scene_procedural(const rr_procedural_params* p, rr_host_scene*
         tris += base_idx[level].size() / 3;
         add_mesh(*s, v, base_idx[level], mat, nullptr);
     }
-    for (uint32_t e = 0; e < p->emissive_triangles; ++e) add_emitter(*s, rng, 0.9f * H, 0.004f * H, 0.015f * H);
+    for (uint32_t e = 0; e < p->emissive_triangles; ++e) add_emitter(*s, rng, 0.9f * H, 0.004f * H, 0.015f * H,
+                                                                  (p->flags & RR_SCENE_NO_EMITTER_LIGHTS) == 0);
     *out = s;
     return RR_OK;
 }
@@ -492,7 +495,8 @@ rr_status rr_host_scene_instanced(const rr_instanced_params* p, rr_host_scene** 
         inst.mesh_index = mesh_ids[rng.next() % mesh_ids.size()];
         s->instances.push_back(inst);
     }
-    for (uint32_t e = 0; e < p->emissive_triangles; ++e) add_emitter(*s, rng, p->box_half, 0.3f, 1.5f);
+    for (uint32_t e = 0; e < p->emissive_triangles; ++e) add_emitter(*s, rng, p->box_half, 0.3f, 1.5f,
+                                                                  (p->flags & RR_SCENE_NO_EMITTER_LIGHTS) == 0);
     *out = s;
     return RR_OK;
 }

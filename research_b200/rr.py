@@ -167,13 +167,16 @@ MLP_PARAM_COUNT = 20784
 
 class ProceduralParams(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("target_triangles", C.c_uint32), ("emissive_triangles", C.c_uint32),
-                ("box_half", C.c_float), ("_pad", C.c_uint32)]
+                ("box_half", C.c_float), ("flags", C.c_uint32)]
+
+
+SCENE_NO_EMITTER_LIGHTS = 1
 
 
 class InstancedParams(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("base_meshes", C.c_uint32), ("tris_per_mesh", C.c_uint32),
                 ("instance_count", C.c_uint32), ("emissive_triangles", C.c_uint32), ("box_half", C.c_float),
-                ("_pad", C.c_uint32)]
+                ("flags", C.c_uint32)]
 
 
 class CameraDesc(C.Structure):
@@ -346,19 +349,21 @@ class HostScene:
         return HostScene(h, L)
 
     @staticmethod
-    def procedural(seed=0x5EED0002, target_triangles=1_000_000, emissive_triangles=4096, box_half=20.0, L=None):
+    def procedural(seed=0x5EED0002, target_triangles=1_000_000, emissive_triangles=4096, box_half=20.0, L=None,
+                   flags=0):
+        """flags: SCENE_NO_EMITTER_LIGHTS leaves out the emitters' point lights."""
         L = L if L is not None else lib()
         h = P()
-        p = ProceduralParams(seed, target_triangles, emissive_triangles, box_half, 0)
+        p = ProceduralParams(seed, target_triangles, emissive_triangles, box_half, flags)
         _check(None, L.rr_host_scene_procedural(C.byref(p), C.byref(h)))
         return HostScene(h, L)
 
     @staticmethod
     def instanced(seed=0x5EED0005, base_meshes=16, tris_per_mesh=2500, instance_count=4096,
-                  emissive_triangles=16384, box_half=250.0, L=None):
+                  emissive_triangles=16384, box_half=250.0, L=None, flags=0):
         L = L if L is not None else lib()
         h = P()
-        p = InstancedParams(seed, base_meshes, tris_per_mesh, instance_count, emissive_triangles, box_half, 0)
+        p = InstancedParams(seed, base_meshes, tris_per_mesh, instance_count, emissive_triangles, box_half, flags)
         _check(None, L.rr_host_scene_instanced(C.byref(p), C.byref(h)))
         return HostScene(h, L)
 

@@ -157,3 +157,14 @@ def test_inputs_library_builds_the_same_scenes_and_cameras(rr, O):
         ca = rr.camera_data(rr.camera_desc(1920, 1080, eye=eye, center=center))
         cb = rr.camera_data(rr.camera_desc(1920, 1080, eye=eye, center=center, L=I), L=I)
         assert bytes(ca) == bytes(cb)
+
+
+def test_scene_without_emitter_point_lights(rr):
+    """RR_SCENE_NO_EMITTER_LIGHTS keeps the geometry and materials and drops
+    only the emitters' point lights."""
+    a = rr.HostScene.procedural(seed=3, target_triangles=30_000, emissive_triangles=50).arrays
+    b = rr.HostScene.procedural(seed=3, target_triangles=30_000, emissive_triangles=50,
+                                flags=rr.SCENE_NO_EMITTER_LIGHTS).arrays
+    assert len(a["lights"]) == 50 and len(b["lights"]) == 0
+    for k in ("vertices", "indices", "meshes", "materials", "instances"):
+        assert a[k].tobytes() == b[k].tobytes(), k
