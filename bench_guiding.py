@@ -59,8 +59,9 @@ GRID_BOUNDS = 20.5
 class Workload:
     """The crop camera, the scene and the render / accumulate calls."""
 
-    def __init__(self, rr, torch, ctx, scene, crop=64, view_height=1080, spp=256, bounces=5):
+    def __init__(self, rr, torch, ctx, scene, crop=64, view_height=1080, spp=256, bounces=5, flags=0):
         self.rr, self.torch, self.ctx, self.scene = rr, torch, ctx, scene
+        self.flags = flags
         self.L = rr.lib()
         self.W = self.H = crop
         desc = rr.camera_desc(crop, crop, eye=EYE, center=CENTER)
@@ -72,7 +73,7 @@ class Workload:
         self.rad = torch.empty((spp, crop, crop, 4), device="cuda")
 
     def trace(self, seed, guide=None):
-        p = self.rr.PtParams(seed, self.bounces, self.spp, 0)
+        p = self.rr.PtParams(seed, self.bounces, self.spp, self.flags)
         if guide is None:
             self.ctx.check(self.L.rr_pathtracer_execute(self.ctx.handle, self.scene.handle, C.byref(self.cam),
                                                         C.byref(p), self.rad.data_ptr(), self.stream))
@@ -189,14 +190,25 @@ def _ratio(a, b):
 
 def measure(rr, torch, ctx, scene, methods=("unguided", "grid", "mlp"), target=0.01, budget_s=15.0, repeats=1,
             judge_spp=1 << 21, crop=64, spp=256, bounces=5, mlp_batch=1 << 18, grid_resolution=64, alpha=0.5,
-            decay=0.9):
+            decay=0.9, flags=0, grid_variants=()):
     """Time to the target relative RMSE for each method, `repeats` times each
-    (fresh guides, disjoint seeds), against one shared judge."""
-    w = Workload(rr, torch, ctx, scene, crop=crop, spp=spp, bounces=bounces)
+    (fresh guides, disjoint seeds), against one shared judge. flags: the
+    tracers' RR_PT_FLAG_* (RR_PT_FLAG_EMITTERS: every method, the judge
+    included, samples the emissive triangles). grid_variants: extra grid
+    settings (resolution, decay, alpha), each measured as method
+    "grid:<res>:<decay>:<alpha>"."""
+    w = Workload(rr, torch, ctx, scene, crop=crop, spp=spp, bounces=bounces, flags=flags)
     judge = make_judge(w, judge_spp)
-    runs = {m: [] for m in methods}
+    all_methods = list(methods) + [f"grid:{r}:{d}:{a}" for r, d, a in grid_variants]
+    runs = {m: [] for m in all_methods}
     for r in range(repeats):
-        for m in methods:
+        for m in all_methods:
+            if m.startswith("grid:"):
+                _, res, dec, alp = m.split(":")
+                runs[m].append(run_method(w, judge, "grid", target, budget_s, seed_base=r * (1 << 24),
+                                          grid_resolution=int(res), alpha=float(alp), decay=float(dec),
+                                          mlp_batch=mlp_batch))
+                continue
             runs[m].append(run_method(w, judge, m, target, budget_s, seed_base=r * (1 << 24),
                                       grid_resolution=grid_resolution, alpha=alpha, decay=decay, mlp_batch=mlp_batch))
     summary = {}
@@ -247,21 +259,35 @@ def main():
     ap.add_argument("--grid-resolution", type=int, default=64)
     ap.add_argument("--alpha", type=float, default=0.5)
     ap.add_argument("--decay", type=float, default=0.9)
+    ap.add_argument("--emitters", action="store_true",
+                    help="the emitter-sampling mode (RR_PT_FLAG_EMITTERS) on the scene without the emitters' point "
+                         "lights, for every method and the judge")
+    ap.add_argument("--grid-variants", default="",
+                    help="extra grid settings res:decay:alpha[,res:decay:alpha...] measured beside the methods")
     args = ap.parse_args()
 
     import torch
     from research_b200 import rr
     torch.cuda.set_device(0)
     ctx = rr.Context(0)
-    hs = rr.HostScene.procedural(target_triangles=args.triangles)
+    hs = rr.HostScene.procedural(target_triangles=args.triangles,
+                                 flags=rr.SCENE_NO_EMITTER_LIGHTS if args.emitters else 0)
     scene = rr.Scene(ctx, hs.arrays)
-    res = measure(rr, torch, ctx, scene, methods=tuple(args.methods.split(",")), target=args.target,
-                  budget_s=args.budget_s, repeats=args.repeats, judge_spp=args.judge_spp, crop=args.crop,
-                  spp=args.spp, bounces=args.bounces, mlp_batch=args.mlp_batch,
-                  grid_resolution=args.grid_resolution, alpha=args.alpha, decay=args.decay)
+    variants = [tuple(v.split(":")) for v in args.grid_variants.split(",") if v]
+    variants = [(int(r), float(d), float(a)) for r, d, a in variants]
+    res = measure(rr, torch, ctx, scene, methods=tuple(m for m in args.methods.split(",") if m),
+                  target=args.target, budget_s=args.budget_s, repeats=args.repeats, judge_spp=args.judge_spp,
+                  crop=args.crop, spp=args.spp, bounces=args.bounces, mlp_batch=args.mlp_batch,
+                  grid_resolution=args.grid_resolution, alpha=args.alpha, decay=args.decay,
+                  flags=rr.PT_FLAG_EMITTERS if args.emitters else 0, grid_variants=variants)
+    for rs in res["runs"].values():
+        for x in rs:
+            x.pop("curve", None)
     line = {"metric": "time-to-RMSE 1e-2, learned vs vMF-grid guiding, 1xB200",
             "config": {"workload": f"procedural-room-1M-tris, {args.crop}x{args.crop} centre crop of the 1920x1080 "
                                    "view", "spp_per_frame": args.spp, "max_bounces": args.bounces,
+                       "light_sampling": "emitter triangles (RR_PT_FLAG_EMITTERS), no centroid point lights"
+                       if args.emitters else "reference (point lights at the emitters' centroids)",
                        "judge": f"unguided tracer, 2 x {args.judge_spp // 2} spp, FP64 accumulation",
                        "grid": f"{args.grid_resolution}^3 x 8 vMF lobes, FP64 EM, decay {args.decay}, "
                                f"alpha {args.alpha}",

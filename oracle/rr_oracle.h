@@ -7,12 +7,17 @@
  * library. Every function cites the reference file:line it restates
  * (paths are relative to the reference project root).
  *
- * Parity status: the reference cannot be built or run here (Vulkan 1.4 ray
- * query + Slang + a Windows toolchain; no graphics stack exists on either
+ * Parity status: the reference cannot be built or run as shipped (Vulkan 1.4
+ * ray query + Slang + a Windows toolchain; no graphics stack exists on either
  * machine), and it ships no tests, golden images or known-answer vectors.
- * The RNG is pinned by known-answer vectors computed from the formula in
- * Common.slang:18-28 / Sampling.slang:11-30; every other routine is pinned
- * only by this restatement ("parity unpinned" beyond the RNG).
+ * Its shader text is pinned instead: oracle/make_ref.py rewrites the
+ * reference's .slang files mechanically into C++ (oracle/_ref/), and
+ * tests/test_ref_text.py requires this restatement to give the same bits as
+ * that text for the RNG, the BRDF, the guiding grid, the path tracer,
+ * accumulate, ReSTIR DI, A-trous, ReSTIR PT and ReSTIR GI. Unpinned: the
+ * hardware ray/triangle intersection (no source; this file's watertight test
+ * decides hits), the driver's sin/cos/exp/log (rr_detmath.h on both sides)
+ * and glm's camera math (absent; restated in closed form).
  *
  * Arithmetic is IEEE-754 binary32 in the expression order of the Slang source,
  * compiled with -ffp-contract=off; sin/cos/exp/log come from rr_detmath.h.
