@@ -267,8 +267,20 @@ typedef struct rr_di_params {
     uint32_t spatial_num_neighbors;
     uint32_t spatial_radius;
     uint32_t m_cap_factor;
-    uint32_t _pad;
+    uint32_t flags;               /* RR_DI_FLAG_* */
 } rr_di_params;
+
+/* Emitter candidates (no reference counterpart; the reference's candidates
+ * are its GpuLights only, restir_di.slang:229-247). A candidate is the pixel
+ * RNG's next 32-bit state, stored as the reservoir's selection; the light
+ * sample it names is decoded from that state wherever the reservoir is
+ * reused: the group (GpuLights or the scene's emissive triangles, 1/2 each
+ * when both exist), then a GpuLight picked as the reference picks one, or an
+ * emissive triangle picked in proportion to luminance(emission) x area and a
+ * point uniform on it. RIS weights use each sample's own source density; an
+ * emitter point's target is max(n.l, 0) luminance(Le |cos_y| / d^2) and its
+ * shading irradiance Le |cos_y| / d^2. Same reservoir layout and buffers. */
+#define RR_DI_FLAG_EMITTERS 1u
 
 rr_status rr_restir_di_initial(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* camera,
                                const rr_di_params* params, float* gbuf_pos, float* gbuf_norm,

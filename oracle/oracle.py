@@ -21,7 +21,10 @@ P, U32, F32, I = C.c_void_p, C.c_uint32, C.c_float, C.c_int
 class DIParams(C.Structure):
     _fields_ = [("frame_seed", U32), ("num_initial_candidates", U32), ("temporal_enable", U32),
                 ("spatial_enable", U32), ("spatial_num_neighbors", U32), ("spatial_radius", U32),
-                ("m_cap_factor", U32), ("_pad", U32)]
+                ("m_cap_factor", U32), ("flags", U32)]
+
+
+DI_EMITTERS = 1   # ORACLE_DI_EMITTERS = RR_DI_FLAG_EMITTERS
 
 
 class GuidingParams(C.Structure):
@@ -240,8 +243,9 @@ def accumulate(radiance: np.ndarray, acc: np.ndarray, camera_moved: int, spp: in
     lib().oracle_accumulate(_p(radiance), _p(acc), radiance.size // 4, camera_moved, spp)
 
 
-def di_params(frame_seed, m=16, temporal=1, spatial=1, k=4, radius=15, m_cap_factor=20):
-    return DIParams(frame_seed, m, temporal, spatial, k, radius, m_cap_factor, 0)
+def di_params(frame_seed, m=16, temporal=1, spatial=1, k=4, radius=15, m_cap_factor=20, flags=0):
+    """flags=DI_EMITTERS: candidates also from the emissive triangles."""
+    return DIParams(frame_seed, m, temporal, spatial, k, radius, m_cap_factor, flags)
 
 
 def restir_di_initial(scene, cam, p, gpos, gnrm, res, nthreads=None):

@@ -743,6 +743,59 @@ float compute_p_hat(const OracleScene& s, uint32_t light_idx, V3 hit_pos, V3 nor
     return n_dot_l * lum;
 }
 
+// ── ReSTIR DI emitter candidates (ORACLE_DI_EMITTERS; no reference
+// counterpart). A candidate is a 32-bit RNG state; the light sample it names
+// is decoded from it: the group (GpuLights or emissive triangles, 1/2 each
+// when both exist), then a GpuLight picked as the reference picks one, or an
+// emissive triangle picked by power and a point on it. inv_src is 1 / the
+// sample's source density (a probability for a GpuLight, an area density
+// for a point on an emitter); the target is the reference's p_hat for a
+// GpuLight and max(n.l, 0) luminance(Le |cos_y| / d^2) for an emitter point.
+struct DiLightSample {
+    bool emitter;
+    uint32_t li;
+    V3 y, Le, ny;
+    float inv_src;
+};
+DiLightSample di_decode(const OracleScene& s, uint32_t c) {
+    uint32_t st = c;
+    const uint32_t NL = (uint32_t)s.lights.size(), NE = (uint32_t)s.emit_cdf.size();
+    const float pe = NE == 0 ? 0.0f : (NL == 0 ? 1.0f : 0.5f);
+    DiLightSample r{};
+    r.emitter = NE > 0 && (NL == 0 || rand_float(st) < 0.5f);
+    if (r.emitter) {
+        const float u = rand_float(st);
+        const float u1 = rand_float(st);
+        const float u2 = rand_float(st);
+        const uint32_t k = emitter_search(s.emit_cdf.data(), NE, u * s.emit_total);
+        const float* e = &s.emit[size_t(k) * 12];
+        const V3 E1 = v3(e[4], e[5], e[6]), E2 = v3(e[8], e[9], e[10]);
+        const float su = sqrtf(u1);
+        r.y = v3(e[0], e[1], e[2]) + E1 * (su * (1.0f - u2)) + E2 * (su * u2);
+        r.Le = v3(e[3], e[7], e[11]);
+        r.ny = normalize(cross(E1, E2));
+        r.inv_src = s.emit_total / (pe * lum709(r.Le));
+    } else {
+        r.li = uint32_t(rand_float(st) * float(NL)) % NL;
+        r.inv_src = float(NL) / (1.0f - pe);
+    }
+    return r;
+}
+float di_p_hat_emit(const OracleScene& s, const DiLightSample& d, V3 pos, V3 n) {
+    if (!d.emitter) return compute_p_hat(s, d.li, pos, n);
+    const V3 to = d.y - pos;
+    const float d2 = fmaxs(dot(to, to), 1e-6f);
+    const V3 l = normalize(to);
+    const float cos_y = fabsf(dot(d.ny, l));
+    const V3 irr = d.Le * (cos_y / d2);
+    return fmaxs(dot(n, l), 0.0f) * lum709(irr);
+}
+// A candidate state: the RNG's next state (never the empty marker).
+inline uint32_t di_candidate(uint32_t& seed) {
+    (void)rand_float(seed);
+    return seed == 0xffffffffu ? 0xfffffffeu : seed;
+}
+
 // A-trous (atrous.slang:21-39)
 inline float luminance601(V3 c) { return dot(c, v3(0.299f, 0.587f, 0.114f)); }
 inline float kernel_weight(int offset) {
@@ -1193,6 +1246,8 @@ void oracle_restir_di_initial(const OracleScene* s, const GpuCameraData* cam, co
     // restir_di.slang:186-262
     const uint32_t W = cam->screen_width, H = cam->screen_height;
     const uint32_t N = (uint32_t)s->lights.size();
+    const bool E = (p->flags & ORACLE_DI_EMITTERS) != 0;
+    const uint32_t NE = E ? (uint32_t)s->emit_cdf.size() : 0u;
     parallel_rows(H, threads, [&](uint32_t y) {
         for (uint32_t x = 0; x < W; ++x) {
             const size_t i = ((size_t)y * W + x) * 4;
@@ -1215,21 +1270,30 @@ void oracle_restir_di_initial(const OracleScene* s, const GpuCameraData* cam, co
             gbuf_pos[i + 3] = h.t;
             gbuf_norm[i] = normal.x; gbuf_norm[i + 1] = normal.y; gbuf_norm[i + 2] = normal.z;
             gbuf_norm[i + 3] = asfloat(sf.material);
-            if (N == 0) { pack_reservoir(res + i, 0xffffffffu, 0.0f, 0.0f, 0); continue; }
+            if (E ? N + NE == 0 : N == 0) { pack_reservoir(res + i, 0xffffffffu, 0.0f, 0.0f, 0); continue; }
             uint32_t sel = 0xffffffffu;
             float w_sum = 0.0f;
             uint32_t M_count = 0;
             for (uint32_t c = 0; c < p->num_initial_candidates; ++c) {
-                uint32_t cand = uint32_t(rand_float(seed) * float(N)) % N;
-                float ph = compute_p_hat(*s, cand, sf.pos, normal);
-                float w_i = ph * float(N);
+                uint32_t cand;
+                float w_i;
+                if (E) {
+                    cand = di_candidate(seed);
+                    const DiLightSample ds = di_decode(*s, cand);
+                    w_i = di_p_hat_emit(*s, ds, sf.pos, normal) * ds.inv_src;
+                } else {
+                    cand = uint32_t(rand_float(seed) * float(N)) % N;
+                    float ph = compute_p_hat(*s, cand, sf.pos, normal);
+                    w_i = ph * float(N);
+                }
                 w_sum += w_i;
                 M_count++;
                 if (w_sum > 0.0f && rand_float(seed) < w_i / w_sum) sel = cand;
             }
             float W_final = 0.0f;
             if (sel != 0xffffffffu) {
-                float ph_y = compute_p_hat(*s, sel, sf.pos, normal);
+                float ph_y = E ? di_p_hat_emit(*s, di_decode(*s, sel), sf.pos, normal)
+                               : compute_p_hat(*s, sel, sf.pos, normal);
                 W_final = (ph_y > 1e-10f) ? (w_sum / (float(M_count) * ph_y)) : 0.0f;
             }
             pack_reservoir(res + i, sel, w_sum, W_final, M_count);
@@ -1243,6 +1307,10 @@ void oracle_restir_di_temporal(const OracleScene* s, const GpuCameraData* cam, c
     // restir_di.slang:266-335
     if (!p->temporal_enable) return;
     const uint32_t W = cam->screen_width, H = cam->screen_height;
+    const bool E = (p->flags & ORACLE_DI_EMITTERS) != 0;
+    auto phat = [&](uint32_t sel, V3 pos, V3 n) {
+        return E ? di_p_hat_emit(*s, di_decode(*s, sel), pos, n) : compute_p_hat(*s, sel, pos, n);
+    };
     parallel_rows(H, threads, [&](uint32_t y) {
         for (uint32_t x = 0; x < W; ++x) {
             const size_t i = ((size_t)y * W + x) * 4;
@@ -1256,7 +1324,7 @@ void oracle_restir_di_temporal(const OracleScene* s, const GpuCameraData* cam, c
             if (prev_sel == 0xffffffffu || prev_M == 0) continue;
             uint32_t m_cap = std::min(std::max(p->m_cap_factor * p->num_initial_candidates, 1u), 8192u);
             prev_M = std::min(prev_M, m_cap);
-            float ph_prev = compute_p_hat(*s, prev_sel, hit_pos, normal);
+            float ph_prev = phat(prev_sel, hit_pos, normal);
             float contrib = ph_prev * prev_W * float(prev_M);
             curr_wsum += contrib;
             uint32_t new_M = curr_M + prev_M;
@@ -1271,7 +1339,7 @@ void oracle_restir_di_temporal(const OracleScene* s, const GpuCameraData* cam, c
             if (contrib > 0.0f && rand_float(seed) < contrib / curr_wsum) curr_sel = prev_sel;
             float W_new = 0.0f;
             if (curr_sel != 0xffffffffu) {
-                float ph_y = compute_p_hat(*s, curr_sel, hit_pos, normal);
+                float ph_y = phat(curr_sel, hit_pos, normal);
                 W_new = (ph_y > 1e-10f) ? (curr_wsum / (float(curr_M) * ph_y)) : 0.0f;
                 W_new = fmins(W_new, 1e4f);
             }
@@ -1287,6 +1355,11 @@ void oracle_restir_di_spatial_shade(const OracleScene* s, const GpuCameraData* c
     // restir_di.slang:339-472
     const uint32_t W = cam->screen_width, H = cam->screen_height;
     const uint32_t N = (uint32_t)s->lights.size();
+    const bool E = (p->flags & ORACLE_DI_EMITTERS) != 0;
+    const uint32_t NA = E ? N + (uint32_t)s->emit_cdf.size() : N;   // lights the reservoirs can name
+    auto phat = [&](uint32_t sel, V3 pos, V3 n) {
+        return E ? di_p_hat_emit(*s, di_decode(*s, sel), pos, n) : compute_p_hat(*s, sel, pos, n);
+    };
     parallel_rows(H, threads, [&](uint32_t y) {
         for (uint32_t x = 0; x < W; ++x) {
             const size_t i = ((size_t)y * W + x) * 4;
@@ -1312,7 +1385,7 @@ void oracle_restir_di_spatial_shade(const OracleScene* s, const GpuCameraData* c
             }
             uint32_t r_sel = asuint(res[i]); float r_wsum = res[i + 1]; float r_W = res[i + 2];
             uint32_t r_M = asuint(res[i + 3]);
-            if (p->spatial_enable && p->spatial_num_neighbors > 0 && N > 0) {
+            if (p->spatial_enable && p->spatial_num_neighbors > 0 && NA > 0) {
                 uint32_t seed = make_seed(x, y, p->frame_seed + 2u);
                 for (uint32_t k = 0; k < p->spatial_num_neighbors; ++k) {
                     float angle = rand_float(seed) * 6.28318530717958f;
@@ -1325,20 +1398,40 @@ void oracle_restir_di_spatial_shade(const OracleScene* s, const GpuCameraData* c
                     uint32_t nb_sel = asuint(res[j]); float nb_W = res[j + 2];
                     uint32_t nb_M = asuint(res[j + 3]);
                     if (nb_sel == 0xffffffffu || nb_M == 0) continue;
-                    float ph_nb = compute_p_hat(*s, nb_sel, hit_pos, normal);
+                    float ph_nb = phat(nb_sel, hit_pos, normal);
                     float contrib = ph_nb * nb_W * float(nb_M);
                     r_wsum += contrib;
                     r_M += nb_M;
                     if (contrib > 0.0f && rand_float(seed) < contrib / r_wsum) r_sel = nb_sel;
                 }
                 if (r_sel != 0xffffffffu) {
-                    float ph_y = compute_p_hat(*s, r_sel, hit_pos, normal);
+                    float ph_y = phat(r_sel, hit_pos, normal);
                     r_W = (ph_y > 1e-10f) ? (r_wsum / (float(r_M) * ph_y)) : 0.0f;
                 }
             }
             V3 o = v3(0, 0, 0);
-            if (r_sel != 0xffffffffu && r_sel < N && r_W > 0.0f && N > 0) {
-                const GpuLight& light = s->lights[r_sel];
+            DiLightSample ds{};
+            if (E && r_sel != 0xffffffffu && NA > 0) ds = di_decode(*s, r_sel);
+            if (E && r_sel != 0xffffffffu && NA > 0 && ds.emitter && r_W > 0.0f) {
+                // a point on an emissive triangle: irradiance Le |cos_y| / d^2
+                V3 to = ds.y - hit_pos;
+                float dist = length(to);
+                V3 l = to / fmaxs(dist, 1e-6f);
+                float dd = fmaxs(dist * dist, 1e-6f);
+                float cos_y = fabsf(dot(ds.ny, l));
+                V3 irr = ds.Le * (cos_y / dd);
+                float n_dot_l = fmaxs(dot(normal, l), 0.0f);
+                if (n_dot_l > 0.0f) {
+                    Hit sh = trace_scene<true>(*s, hit_pos + normal * 1e-4f, l, 0.001f, dist - 0.01f);
+                    if (!sh.hit) {
+                        V3 wo = normalize(load3(cam->position) - hit_pos);
+                        V3 bv = brdf_eval(normal, wo, l, load3(mat.base_color), mat.metallic, mat.roughness);
+                        o = ((bv * irr) * n_dot_l) * r_W;
+                    }
+                }
+            } else if (E ? (r_sel != 0xffffffffu && NA > 0 && !ds.emitter && r_W > 0.0f && N > 0)
+                         : (r_sel != 0xffffffffu && r_sel < N && r_W > 0.0f && N > 0)) {
+                const GpuLight& light = s->lights[E ? ds.li : r_sel];
                 V3 l, irr; float dist;
                 if (light.type == 0) {
                     V3 to = load3(light.position) - hit_pos;

@@ -110,8 +110,14 @@ typedef struct OracleDIParams {
     uint32_t spatial_num_neighbors;
     uint32_t spatial_radius;
     uint32_t m_cap_factor; /* 20 in the reference (restir_di.slang:300) */
-    uint32_t _pad;
+    uint32_t flags;        /* ORACLE_DI_EMITTERS: candidates also from the emissive triangles */
 } OracleDIParams;
+/* Emitter candidates (no reference counterpart; the library's
+ * RR_DI_FLAG_EMITTERS): a candidate is the pixel RNG's next state, and the
+ * light sample it names (group, then a GpuLight, or an emissive triangle and
+ * a point on it, as the emitter-sampling path tracer picks them) is decoded
+ * from that state wherever the reservoir is reused. */
+#define ORACLE_DI_EMITTERS 1u
 
 void oracle_restir_di_initial(const OracleScene* scene, const GpuCameraData* cam,
                               const OracleDIParams* p, float* gbuf_pos, float* gbuf_norm,

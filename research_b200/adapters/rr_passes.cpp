@@ -59,7 +59,7 @@ void PathTracerCudaPass::execute(rr::render::FrameContext&) {
         status_ = RR_ERR_INVALID_ARGUMENT;
         return;
     }
-    const rr_pt_params p{frame_count_++, max_bounces, 1u, 0u};
+    const rr_pt_params p{frame_count_++, max_bounces, 1u, emitter_sampling ? RR_PT_FLAG_EMITTERS : 0u};
     status_ = rr_pathtracer_execute(ctx_, scene_, &camera_, &p, radiance_.data(), stream_);
 }
 
@@ -123,6 +123,7 @@ void ReSTIRDICudaPass::execute(rr::render::FrameContext&) {
     p.spatial_num_neighbors = spatial_num_neighbors;
     p.spatial_radius = spatial_radius;
     p.m_cap_factor = 20u;   // restir_di.slang:300
+    p.flags = emitter_candidates ? RR_DI_FLAG_EMITTERS : 0u;
     status_ = rr_restir_di_execute(ctx_, scene_, &camera_, &p, gbuf_pos_.data(), gbuf_norm_.data(),
                                    reservoir_[reservoir_flip_].data(), reservoir_[1u - reservoir_flip_].data(),
                                    output_.data(), stream_);

@@ -87,6 +87,7 @@ public:
     [[nodiscard]] const float* radiance() const noexcept { return radiance_.data(); }
 
     uint32_t max_bounces = 5;   // PathTracerPass.h:46
+    bool emitter_sampling = false;   // RR_PT_FLAG_EMITTERS (not in the reference)
 private:
     const rr_scene* scene_ = nullptr;
     GpuCameraData camera_{};
@@ -137,6 +138,7 @@ public:
     uint32_t num_initial_candidates = 16;
     uint32_t spatial_num_neighbors = 4;
     uint32_t spatial_radius = 15;
+    bool emitter_candidates = false;   // RR_DI_FLAG_EMITTERS (not in the reference)
 private:
     const rr_scene* scene_ = nullptr;
     GpuCameraData camera_{};

@@ -39,6 +39,74 @@ RR_D float compute_p_hat(const DevScene& s, uint32_t li, float3 pos, float3 n) {
     return ndl * lum;
 }
 
+// ── Emitter candidates (RR_DI_FLAG_EMITTERS; no reference counterpart). A
+// candidate is a 32-bit RNG state; the light sample it names is decoded
+// from it (group, then a GpuLight or an emissive triangle by power and a
+// point on it). inv_src = 1 / source density (probability for a GpuLight,
+// area density for an emitter point).
+RR_D float lum709(float3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
+
+RR_D uint32_t emitter_search(const float* __restrict__ cdf, uint32_t n, float target) {
+    uint32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(cdf + mid) > target) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+
+struct DiLightSample {
+    bool emitter;
+    uint32_t li;
+    float3 y, Le, ny;
+    float inv_src;
+};
+
+RR_D DiLightSample di_decode(const DevScene& s, uint32_t c) {
+    uint32_t st = c;
+    const uint32_t NL = s.num_lights, NE = s.num_emitters;
+    const float pe = NE == 0 ? 0.0f : (NL == 0 ? 1.0f : 0.5f);
+    DiLightSample r;
+    r.li = 0;
+    r.y = r.Le = r.ny = f3(0.0f, 0.0f, 0.0f);
+    r.emitter = NE > 0 && (NL == 0 || rand_float(st) < 0.5f);
+    if (r.emitter) {
+        const float u = rand_float(st);
+        const float u1 = rand_float(st);
+        const float u2 = rand_float(st);
+        const uint32_t k = emitter_search(s.emit_cdf, NE, u * s.emit_total);
+        const float4 e0 = __ldg(s.emitters + k * 3), e1 = __ldg(s.emitters + k * 3 + 1);
+        const float4 e2 = __ldg(s.emitters + k * 3 + 2);
+        const float3 E1 = xyz(e1), E2 = xyz(e2);
+        const float su = sqrtf(u1);
+        r.y = xyz(e0) + E1 * (su * (1.0f - u2)) + E2 * (su * u2);
+        r.Le = f3(e0.w, e1.w, e2.w);
+        r.ny = normalize(cross(E1, E2));
+        r.inv_src = s.emit_total / (pe * lum709(r.Le));
+    } else {
+        r.li = uint32_t(rand_float(st) * float(NL)) % NL;
+        r.inv_src = float(NL) / (1.0f - pe);
+    }
+    return r;
+}
+
+RR_D float di_p_hat_emit(const DevScene& s, const DiLightSample& d, float3 pos, float3 n) {
+    if (!d.emitter) return compute_p_hat(s, d.li, pos, n);
+    const float3 to = d.y - pos;
+    const float d2 = mx(dot(to, to), 1e-6f);
+    const float3 l = normalize(to);
+    const float cos_y = fabsf(dot(d.ny, l));
+    const float3 irr = d.Le * (cos_y / d2);
+    return mx(dot(n, l), 0.0f) * lum709(irr);
+}
+
+// p_hat of selection sel: a GpuLight index, or (Emit) a candidate state.
+template <bool Emit>
+RR_D float di_p_hat(const DevScene& s, uint32_t sel, float3 pos, float3 n) {
+    if constexpr (Emit) return di_p_hat_emit(s, di_decode(s, sel), pos, n);
+    else return compute_p_hat(s, sel, pos, n);
+}
+
 RR_D bool pixel_of(const GpuCameraData& cam, uint32_t& x, uint32_t& y) {
     x = blockIdx.x * 16 + (threadIdx.x & 15);
     y = blockIdx.y * 8 + (threadIdx.x >> 4);
@@ -46,6 +114,7 @@ RR_D bool pixel_of(const GpuCameraData& cam, uint32_t& x, uint32_t& y) {
 }
 
 // cs_initial (restir_di.slang:186-262)
+template <bool Emit>
 __global__ void __launch_bounds__(128, 8) di_initial_kernel(DevScene s, DiLaunch L, float4* __restrict__ gpos,
                                                          float4* __restrict__ gnrm, float4* __restrict__ res) {
     uint32_t x, y;
@@ -69,7 +138,7 @@ __global__ void __launch_bounds__(128, 8) di_initial_kernel(DevScene s, DiLaunch
     gpos[i] = make_float4(sf.pos.x, sf.pos.y, sf.pos.z, h.t);
     gnrm[i] = make_float4(n.x, n.y, n.z, __uint_as_float(sf.material));
     const uint32_t N = s.num_lights;
-    if (N == 0) {
+    if (Emit ? N + s.num_emitters == 0 : N == 0) {
         res[i] = make_float4(__uint_as_float(kNoIndex), 0.0f, 0.0f, __uint_as_float(0u));
         return;
     }
@@ -77,22 +146,32 @@ __global__ void __launch_bounds__(128, 8) di_initial_kernel(DevScene s, DiLaunch
     float w_sum = 0.0f;
     uint32_t M_count = 0;
     for (uint32_t c = 0; c < L.num_initial_candidates; ++c) {
-        const uint32_t cand = uint32_t(rand_float(seed) * float(N)) % N;
-        const float ph = compute_p_hat(s, cand, sf.pos, n);
-        const float w_i = ph * float(N);
+        uint32_t cand;
+        float w_i;
+        if constexpr (Emit) {
+            (void)rand_float(seed);
+            cand = seed == kNoIndex ? kNoIndex - 1u : seed;   // never the empty marker
+            const DiLightSample ds = di_decode(s, cand);
+            w_i = di_p_hat_emit(s, ds, sf.pos, n) * ds.inv_src;
+        } else {
+            cand = uint32_t(rand_float(seed) * float(N)) % N;
+            const float ph = compute_p_hat(s, cand, sf.pos, n);
+            w_i = ph * float(N);
+        }
         w_sum += w_i;
         M_count++;
         if (w_sum > 0.0f && rand_float(seed) < w_i / w_sum) sel = cand;
     }
     float W_final = 0.0f;
     if (sel != kNoIndex) {
-        const float ph_y = compute_p_hat(s, sel, sf.pos, n);
+        const float ph_y = di_p_hat<Emit>(s, sel, sf.pos, n);
         W_final = (ph_y > 1e-10f) ? (w_sum / (float(M_count) * ph_y)) : 0.0f;
     }
     res[i] = make_float4(__uint_as_float(sel), w_sum, W_final, __uint_as_float(M_count));
 }
 
 // cs_temporal (restir_di.slang:266-335): same-pixel history, M-cap.
+template <bool Emit>
 __global__ void __launch_bounds__(128) di_temporal_kernel(DevScene s, DiLaunch L, const float4* __restrict__ gpos,
                                                           const float4* __restrict__ gnrm, float4* __restrict__ res,
                                                           const float4* __restrict__ prev) {
@@ -111,7 +190,7 @@ __global__ void __launch_bounds__(128) di_temporal_kernel(DevScene s, DiLaunch L
     uint32_t prev_M = __float_as_uint(pr.w);
     if (prev_sel == kNoIndex || prev_M == 0) return;
     prev_M = min(prev_M, L.m_cap);
-    const float ph_prev = compute_p_hat(s, prev_sel, pos, n);
+    const float ph_prev = di_p_hat<Emit>(s, prev_sel, pos, n);
     const float contrib = ph_prev * prev_W * float(prev_M);
     curr_wsum += contrib;
     const uint32_t new_M = curr_M + prev_M;
@@ -126,7 +205,7 @@ __global__ void __launch_bounds__(128) di_temporal_kernel(DevScene s, DiLaunch L
     if (contrib > 0.0f && rand_float(seed) < contrib / curr_wsum) curr_sel = prev_sel;
     float W_new = 0.0f;
     if (curr_sel != kNoIndex) {
-        const float ph_y = compute_p_hat(s, curr_sel, pos, n);
+        const float ph_y = di_p_hat<Emit>(s, curr_sel, pos, n);
         W_new = (ph_y > 1e-10f) ? (curr_wsum / (float(curr_M) * ph_y)) : 0.0f;
         W_new = mn(W_new, 1e4f);
     }
@@ -134,6 +213,7 @@ __global__ void __launch_bounds__(128) di_temporal_kernel(DevScene s, DiLaunch L
 }
 
 // cs_spatial_shade (restir_di.slang:339-472)
+template <bool Emit>
 __global__ void __launch_bounds__(128, 8) di_spatial_shade_kernel(DevScene s, DiLaunch L, const float4* __restrict__ gpos,
                                                                const float4* __restrict__ gnrm,
                                                                const float4* __restrict__ res,
@@ -163,7 +243,8 @@ __global__ void __launch_bounds__(128, 8) di_spatial_shade_kernel(DevScene s, Di
     float r_wsum = r.y, r_W = r.z;
     uint32_t r_M = __float_as_uint(r.w);
     const uint32_t N = s.num_lights;
-    if (L.spatial_on && L.spatial_num_neighbors > 0 && N > 0) {
+    const uint32_t NA = Emit ? N + s.num_emitters : N;   // lights a reservoir can name
+    if (L.spatial_on && L.spatial_num_neighbors > 0 && NA > 0) {
         uint32_t seed = make_seed(x, y, L.frame_seed + 2u);
         for (uint32_t k = 0; k < L.spatial_num_neighbors; ++k) {
             const float angle = rand_float(seed) * 6.28318530717958f;
@@ -177,24 +258,55 @@ __global__ void __launch_bounds__(128, 8) di_spatial_shade_kernel(DevScene s, Di
             const uint32_t nb_sel = __float_as_uint(nr.x);
             const uint32_t nb_M = __float_as_uint(nr.w);
             if (nb_sel == kNoIndex || nb_M == 0) continue;
-            const float ph_nb = compute_p_hat(s, nb_sel, pos, n);
+            const float ph_nb = di_p_hat<Emit>(s, nb_sel, pos, n);
             const float contrib = ph_nb * nr.z * float(nb_M);
             r_wsum += contrib;
             r_M += nb_M;
             if (contrib > 0.0f && rand_float(seed) < contrib / r_wsum) r_sel = nb_sel;
         }
         if (r_sel != kNoIndex) {
-            const float ph_y = compute_p_hat(s, r_sel, pos, n);
+            const float ph_y = di_p_hat<Emit>(s, r_sel, pos, n);
             r_W = (ph_y > 1e-10f) ? (r_wsum / (float(r_M) * ph_y)) : 0.0f;
         }
     }
     float3 o = f3(0.0f, 0.0f, 0.0f);
-    // r_sel < N guards the light fetch for reservoirs that were never written
-    // by this scene; valid reservoirs always satisfy it.
-    if (r_sel != kNoIndex && r_sel < N && r_W > 0.0f && N > 0) {
-        const float4 l0 = __ldg(s.lights + r_sel * 3);
-        const float4 l1 = __ldg(s.lights + r_sel * 3 + 1);
-        const float4 l2 = __ldg(s.lights + r_sel * 3 + 2);
+    uint32_t li = r_sel;
+    bool gpu_light;
+    if constexpr (Emit) {
+        gpu_light = false;
+        if (r_sel != kNoIndex && NA > 0 && r_W > 0.0f) {
+            const DiLightSample ds = di_decode(s, r_sel);
+            if (ds.emitter) {
+                // a point on an emissive triangle: irradiance Le |cos_y| / d^2
+                const float3 to = ds.y - pos;
+                const float dist = length(to);
+                const float3 l = to / mx(dist, 1e-6f);
+                const float dd = mx(dist * dist, 1e-6f);
+                const float cos_y = fabsf(dot(ds.ny, l));
+                const float3 irr = ds.Le * (cos_y / dd);
+                const float ndl = mx(dot(n, l), 0.0f);
+                if (ndl > 0.0f) {
+                    HitRec h;
+                    if (!trace<true>(s, make_ray(pos + n * 1e-4f, l), 0.001f, dist - 0.01f, h)) {
+                        const float3 wo = normalize(f3(L.cam.position[0], L.cam.position[1], L.cam.position[2]) - pos);
+                        const float3 bv = brdf_eval(n, wo, l, f3(m0.x, m0.y, m0.z), m0.w, m1.w);
+                        o = ((bv * irr) * ndl) * r_W;
+                    }
+                }
+            } else {
+                li = ds.li;
+                gpu_light = N > 0;
+            }
+        }
+    } else {
+        // r_sel < N guards the light fetch for reservoirs that were never
+        // written by this scene; valid reservoirs always satisfy it.
+        gpu_light = r_sel != kNoIndex && r_sel < N && r_W > 0.0f && N > 0;
+    }
+    if (gpu_light) {
+        const float4 l0 = __ldg(s.lights + li * 3);
+        const float4 l1 = __ldg(s.lights + li * 3 + 1);
+        const float4 l2 = __ldg(s.lights + li * 3 + 2);
         float3 l, irr; float dist;
         if (__float_as_uint(l0.w) == 0u) {
             const float3 to = f3(l0.x, l0.y, l0.z) - pos;
@@ -238,6 +350,7 @@ dim3 grid_of(const GpuCameraData* cam) { return dim3((cam->screen_width + 15) / 
 
 rr_status check(rr_ctx* ctx, const rr_scene* scene, const GpuCameraData* cam, const rr_di_params* p) {
     if (!scene || !cam || !p) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "ReSTIR DI: null argument");
+    if (p->flags & ~RR_DI_FLAG_EMITTERS) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "ReSTIR DI: unknown flags");
     if (cam->screen_width == 0 || cam->screen_height == 0 || cam->screen_width > 65535u * 16u ||
         cam->screen_height > 65535u * 8u)
         return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "ReSTIR DI: bad image size");
@@ -257,7 +370,8 @@ extern "C" rr_status rr_restir_di_initial(rr_ctx* ctx, const rr_scene* scene, co
     if (st != RR_OK) return st;
     if (!gpos || !gnrm || !res) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "null buffer");
     RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
-    di_initial_kernel<<<grid_of(cam), 128, 0, static_cast<cudaStream_t>(stream)>>>(
+    const auto di_initial_kernel_f = (p->flags & RR_DI_FLAG_EMITTERS) ? di_initial_kernel<true> : di_initial_kernel<false>;
+    di_initial_kernel_f<<<grid_of(cam), 128, 0, static_cast<cudaStream_t>(stream)>>>(
         scene->dev, make_launch(cam, p), reinterpret_cast<float4*>(gpos), reinterpret_cast<float4*>(gnrm),
         reinterpret_cast<float4*>(res));
     RR_CHECK_LAUNCH(ctx);
@@ -274,7 +388,8 @@ extern "C" rr_status rr_restir_di_temporal(rr_ctx* ctx, const rr_scene* scene, c
     if (!gpos || !gnrm || !res || !prev) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "null buffer");
     if (!p->temporal_enable) return RR_OK;  // restir_di.slang:270
     RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
-    di_temporal_kernel<<<grid_of(cam), 128, 0, static_cast<cudaStream_t>(stream)>>>(
+    const auto di_temporal_kernel_f = (p->flags & RR_DI_FLAG_EMITTERS) ? di_temporal_kernel<true> : di_temporal_kernel<false>;
+    di_temporal_kernel_f<<<grid_of(cam), 128, 0, static_cast<cudaStream_t>(stream)>>>(
         scene->dev, make_launch(cam, p), reinterpret_cast<const float4*>(gpos),
         reinterpret_cast<const float4*>(gnrm), reinterpret_cast<float4*>(res),
         reinterpret_cast<const float4*>(prev));
@@ -291,7 +406,8 @@ extern "C" rr_status rr_restir_di_spatial_shade(rr_ctx* ctx, const rr_scene* sce
     if (st != RR_OK) return st;
     if (!gpos || !gnrm || !res || !out) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "null buffer");
     RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
-    di_spatial_shade_kernel<<<grid_of(cam), 128, 0, static_cast<cudaStream_t>(stream)>>>(
+    const auto di_spatial_shade_kernel_f = (p->flags & RR_DI_FLAG_EMITTERS) ? di_spatial_shade_kernel<true> : di_spatial_shade_kernel<false>;
+    di_spatial_shade_kernel_f<<<grid_of(cam), 128, 0, static_cast<cudaStream_t>(stream)>>>(
         scene->dev, make_launch(cam, p), reinterpret_cast<const float4*>(gpos),
         reinterpret_cast<const float4*>(gnrm), reinterpret_cast<const float4*>(res),
         reinterpret_cast<float4*>(out));

@@ -86,7 +86,10 @@ class AccParams(C.Structure):
 class DIParams(C.Structure):
     _fields_ = [("frame_seed", C.c_uint32), ("num_initial_candidates", C.c_uint32), ("temporal_enable", C.c_uint32),
                 ("spatial_enable", C.c_uint32), ("spatial_num_neighbors", C.c_uint32), ("spatial_radius", C.c_uint32),
-                ("m_cap_factor", C.c_uint32), ("_pad", C.c_uint32)]
+                ("m_cap_factor", C.c_uint32), ("flags", C.c_uint32)]
+
+
+DI_FLAG_EMITTERS = 1
 
 
 class AtrousParams(C.Structure):
