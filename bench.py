@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the oracle check of the benchmarked frame")
     ap.add_argument("--no-time-to-rmse", action="store_true", help="skip the guiding time-to-RMSE measurement")
+    ap.add_argument("--no-emitter-mode", action="store_true",
+                    help="skip the frame measured with emitter sampling on the scene without centroid point lights")
     ap.add_argument("--rmse-budget-s", type=float, default=6.0,
                     help="device seconds per method and repeat of the time-to-RMSE measurement")
     ap.add_argument("--rmse-repeats", type=int, default=3)
@@ -271,6 +273,8 @@ class Frame:
         self.ping = [f(H, W, 4), f(H, W, 4)]
         self.frame = 0
         self.spp_acc = 0
+        self.pt_mode = 0      # RR_PT_FLAG_EMITTERS for the emitter-sampling frame
+        self.di_flags = 0     # RR_DI_FLAG_EMITTERS likewise
         self.slot = C.c_uint32()
         self.desc = rr.camera_desc(W, H, eye=CFG["eye"], center=CFG["center"])
         self.cam = rr.camera_data(self.desc)
@@ -297,7 +301,7 @@ class Frame:
             self.di_stream.wait_event(self.fork)
             di_st = self.di_stream.cuda_stream
         mark(); rec()
-        p = rr.PtParams(seed_base + self.frame * CFG["spp"], CFG["max_bounces"], CFG["spp"], pt_flags)
+        p = rr.PtParams(seed_base + self.frame * CFG["spp"], CFG["max_bounces"], CFG["spp"], pt_flags | self.pt_mode)
         ctx.check(L.rr_pathtracer_execute(ctx.handle, self.scene.handle, C.byref(cam), C.byref(p),
                                           self.rad.data_ptr(), stream))
         mark(); rec()
@@ -307,7 +311,7 @@ class Frame:
         self.spp_acc += CFG["spp"]
         mark(); rec()
         dp = rr.DIParams(seed_base + self.frame, CFG["di_candidates"], 1, 1, CFG["di_neighbors"], CFG["di_radius"],
-                         CFG["m_cap_factor"], 0)
+                         CFG["m_cap_factor"], self.di_flags)
         cur, prev = self.res[self.frame & 1], self.res[(self.frame & 1) ^ 1]
         ctx.check(L.rr_restir_di_execute(ctx.handle, self.scene.handle, C.byref(cam), C.byref(dp),
                                          self.gpos.data_ptr(), self.gnrm.data_ptr(), cur.data_ptr(), prev.data_ptr(),
@@ -577,6 +581,47 @@ def run_ours(args, ws, rank, local):
             cpu = {"value": v, "unit": UNIT, "cores": O.threads(), "kind": "port", "sample": d}
         oscene.close()
 
+    # the same frame lit by its emissive triangles alone (no centroid point
+    # lights), with the path tracer and ReSTIR DI sampling the triangles
+    # (RR_PT_FLAG_EMITTERS, RR_DI_FLAG_EMITTERS); device-timed like the main
+    # frames, reported beside them
+    emitter_mode = None
+    if not args.no_emitter_mode:
+        hs_e = rr.HostScene.procedural(seed=CFG["scene_seed"], target_triangles=args.triangles,
+                                       emissive_triangles=CFG["emitters"], box_half=CFG["box_half"],
+                                       flags=rr.SCENE_NO_EMITTER_LIGHTS)
+        scene_e = rr.Scene(ctx, hs_e.arrays)
+        fe = Frame(rr, torch, ctx, scene_e, W, H)
+        fe.concurrent = fr.concurrent
+        fe.pt_mode, fe.di_flags = rr.PT_FLAG_EMITTERS, rr.DI_FLAG_EMITTERS
+        for _ in range(args.warmup):
+            fe.step(stream, seed_base=seed_base)
+        barrier(ws)
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record()
+        for _ in range(args.steps):
+            fe.step(stream, seed_base=seed_base)
+        g1.record()
+        torch.cuda.synchronize()
+        em_ms = max_over_ranks(ws, g0.elapsed_time(g1) / args.steps)
+        fe.frame = args.warmup
+        for _ in range(args.steps):
+            fe.step(stream, pt_flags=rr.PT_FLAG_TIME_STAGES, seed_base=seed_base, stage_timing=True)
+        ctx.check(rr.lib().rr_pathtracer_stats(ctx.handle, C.byref(st), 1))
+        em_stage = fe.stage_ms()
+        emitter_mode = {"value": replicas.job_throughput(paths_per_step, ws, em_ms), "unit": UNIT,
+                        "ms_per_step": em_ms,
+                        "workload": "the same frame on the same scene without its centroid point lights: the path "
+                                    "tracer's NEE and ReSTIR DI's candidates sample the 4096 emissive triangles "
+                                    "(RR_PT_FLAG_EMITTERS, RR_DI_FLAG_EMITTERS)",
+                        "stages_ms": {**{k: round(v, 4) for k, v in em_stage.items()},
+                                      "pt_extend": round(st.ms_extend / args.steps, 4),
+                                      "pt_shade": round(st.ms_shade / args.steps, 4),
+                                      "pt_shadow": round(st.ms_shadow / args.steps, 4)}}
+        del fe
+        scene_e.close()
+
     # the metric's second half: time to a relative RMSE of 1e-2, learned vs
     # grid guiding (and unguided), on the same scene, one GPU
     rmse = None
@@ -613,7 +658,7 @@ def run_ours(args, ws, rank, local):
                 "scene": {"triangles": sst.triangle_count, "bvh_nodes": sst.bvh_node_count,
                           "bvh_depth": sst.bvh_max_depth, "bvh_build_ms": round(sst.build_ms, 1),
                           "lights": sst.light_count},
-                "traversal_per_step": counted, "autotune": tuned, "time_to_rmse": rmse}
+                "traversal_per_step": counted, "autotune": tuned, "emitter_mode": emitter_mode, "time_to_rmse": rmse}
         print(json.dumps(line), flush=True)
     scene.close()
     ctx.close()

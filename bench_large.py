@@ -53,6 +53,9 @@ def main():
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--box-half", type=float, default=250.0,
                     help="half-size of the instance placement box (250: sparse, 40: dense clutter)")
+    ap.add_argument("--emitters", action="store_true",
+                    help="no centroid point lights; the tracers, the judge and ReSTIR DI sample the emissive "
+                         "triangles (RR_PT_FLAG_EMITTERS, RR_DI_FLAG_EMITTERS)")
     args = ap.parse_args()
 
     import torch
@@ -61,7 +64,10 @@ def main():
     L = rr.lib()
     ctx = rr.Context(0)
     t0 = time.perf_counter()
-    hs = rr.HostScene.instanced(instance_count=args.instances, box_half=args.box_half)
+    hs = rr.HostScene.instanced(instance_count=args.instances, box_half=args.box_half,
+                                flags=rr.SCENE_NO_EMITTER_LIGHTS if args.emitters else 0)
+    ptf = rr.PT_FLAG_EMITTERS if args.emitters else 0
+    dif = rr.DI_FLAG_EMITTERS if args.emitters else 0
     scene = rr.Scene(ctx, hs.arrays)
     torch.cuda.synchronize()
     build_s = time.perf_counter() - t0
@@ -87,7 +93,7 @@ def main():
         s64 = torch.zeros((c, c, 4), device="cuda", dtype=torch.float64)
         done = 0
         while done < args.judge_spp // 2:
-            p = rr.PtParams((1 << 28) * (h + 1) + done, args.bounces, jspp, 0)
+            p = rr.PtParams((1 << 28) * (h + 1) + done, args.bounces, jspp, ptf)
             ctx.check(L.rr_pathtracer_execute(ctx.handle, scene.handle, C.byref(ccam), C.byref(p), jrad.data_ptr(),
                                               st))
             a = rr.AccParams(c, c, 1 if done == 0 else 0, done)
@@ -113,7 +119,7 @@ def main():
     rad = torch.empty((1, H, W, 4), device="cuda")
     acc = torch.zeros((H, W, 4), device="cuda")
     gpos, gnrm, dres0, dres1, direct = (torch.zeros((H, W, 4), device="cuda") for _ in range(5))
-    di = rr.DIParams(0, 32, 1, 1, 5, 30, 20, 0)
+    di = rr.DIParams(0, 32, 1, 1, 5, 30, 20, dif)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
     results = {}
     for method in args.methods.split(","):
@@ -135,7 +141,7 @@ def main():
                                              gnrm.data_ptr(), (dres0 if f & 1 else dres1).data_ptr(),
                                              (dres1 if f & 1 else dres0).data_ptr(), direct.data_ptr(), st))
             ev[1].record()
-            p = rr.PtParams(f, args.bounces, 1, 0)
+            p = rr.PtParams(f, args.bounces, 1, ptf)
             if guide is None:
                 ctx.check(L.rr_pathtracer_execute(ctx.handle, scene.handle, C.byref(cam), C.byref(p), rad.data_ptr(),
                                                   st))
@@ -188,6 +194,8 @@ def main():
             "unit": "x (grid time / learned time at the grid's final RMSE)",
             "value": speedup("mse_x_time"), "learned_speedup_trace_only": speedup("mse_x_time_trace_only"),
             "config": {"workload": "instanced 4096 x 2.5k-tri meshes (10.24M tris), 16384 emissive tris, 3840x2160",
+                       "light_sampling": "emitter triangles (RR_PT_FLAG_EMITTERS, RR_DI_FLAG_EMITTERS), no centroid "
+                                         "point lights" if args.emitters else "reference (centroid point lights)",
                        "box_half": args.box_half, "eye": list(eye),
                        "triangles": n_tris, "frames": args.frames, "spp_per_frame": 1, "max_bounces": args.bounces,
                        "restir_di": "32 candidates, M-cap 20, 5 neighbours r=30",
