@@ -627,7 +627,10 @@ def run_ours(args, ws, rank, local):
     rmse = None
     if rank == 0 and ws == 1 and not args.no_time_to_rmse:
         import bench_guiding
+        rclocks = ClockSampler(torch.cuda.get_device_properties(local).uuid)
+        rclocks.start()
         r = bench_guiding.measure(rr, torch, ctx, scene, budget_s=args.rmse_budget_s, repeats=args.rmse_repeats)
+        r["clocks"] = rclocks.stop()
         for rs in r["runs"].values():
             for x in rs:
                 x.pop("curve", None)

@@ -54,7 +54,7 @@ struct Ray {
     float3 o, d, inv;
     float3 alo, ahi;
     float Sx, Sy, Sz;
-    int kx, ky, kz;
+    int k;   // shear axes kx | ky << 2 | kz << 4 (one register across the traversal loop)
 };
 
 RR_D float comp(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
@@ -70,7 +70,7 @@ RR_D Ray make_ray(float3 o, float3 d) {
     int ky = kx + 1; if (ky == 3) ky = 0;
     const float dz = comp(d, kz);
     if (dz < 0.0f) { const int t = kx; kx = ky; ky = t; }
-    r.kx = kx; r.ky = ky; r.kz = kz;
+    r.k = kx | (ky << 2) | (kz << 4);
     r.Sx = comp(d, kx) / dz;
     r.Sy = comp(d, ky) / dz;
     r.Sz = 1.0f / dz;
@@ -100,11 +100,12 @@ RR_D Ray make_ray(float3 o, float3 d) {
 // Watertight test; two-sided. On hit writes t and the weights of v1, v2.
 RR_D bool intersect_triangle(const Ray& r, float3 p0, float3 p1, float3 p2, float tmin,
                              float tmax, float& t, float& bu, float& bv) {
+    const int kx = r.k & 3, ky = (r.k >> 2) & 3, kz = r.k >> 4;
     const float3 A = p0 - r.o, B = p1 - r.o, C = p2 - r.o;
-    const float Az0 = comp(A, r.kz), Bz0 = comp(B, r.kz), Cz0 = comp(C, r.kz);
-    const float Ax = comp(A, r.kx) - r.Sx * Az0, Ay = comp(A, r.ky) - r.Sy * Az0;
-    const float Bx = comp(B, r.kx) - r.Sx * Bz0, By = comp(B, r.ky) - r.Sy * Bz0;
-    const float Cx = comp(C, r.kx) - r.Sx * Cz0, Cy = comp(C, r.ky) - r.Sy * Cz0;
+    const float Az0 = comp(A, kz), Bz0 = comp(B, kz), Cz0 = comp(C, kz);
+    const float Ax = comp(A, kx) - r.Sx * Az0, Ay = comp(A, ky) - r.Sy * Az0;
+    const float Bx = comp(B, kx) - r.Sx * Bz0, By = comp(B, ky) - r.Sy * Bz0;
+    const float Cx = comp(C, kx) - r.Sx * Cz0, Cy = comp(C, ky) - r.Sy * Cz0;
     const float U = Cx * By - Cy * Bx;
     const float V = Ax * Cy - Ay * Cx;
     const float W = Bx * Ay - By * Ax;
@@ -163,23 +164,28 @@ struct TraceWork {
 };
 
 // Traversal state of one ray between node steps. node < 0: no inner node
-// left, only the postponed leaf (pend_count > 0) to intersect.
+// left, only the postponed leaf (pend_count > 0) to intersect. best: the
+// triangle record (index into the scene's triangle array) of the closest hit
+// so far, -1 for none; only hit.t is kept beside it while the ray traverses,
+// and trav_resolve fills in the rest of the hit record at the end.
 struct TravState {
     int node;
     int sp;
-    bool found;
+    int best;
     uint32_t visits;
     int pend_first, pend_count;
+    RR_D bool found() const { return best >= 0; }
 };
 
 RR_D void trav_begin(TravState& st, HitRec& hit, float tmax) {
-    st.node = 0; st.sp = 0; st.found = false; st.visits = 0;
+    st.node = 0; st.sp = 0; st.best = -1; st.visits = 0;
     st.pend_first = 0; st.pend_count = 0;
     hit.t = tmax; hit.key = kNoIndex;
 }
 
 // The triangles [first, first + count) of a leaf against the ray; closest
-// hit: keeps the lowest (t, key); any hit: returns true at the first hit.
+// hit: keeps the lowest (t, key), reading the kept triangle's key only on an
+// exact tie of t; any hit: returns true at the first hit.
 template <bool AnyHit, bool Count>
 RR_D bool leaf_tris(const DevScene& s, const Ray& r, float tmin, HitRec& hit, TravState& st, int first, int count,
                     TraceWork* work) {
@@ -191,23 +197,58 @@ RR_D bool leaf_tris(const DevScene& s, const Ray& r, float tmin, HitRec& hit, Tr
         float tt, uu, vv;
         if (intersect_triangle(r, f3(t0.x, t0.y, t0.z), f3(t0.w, t1.x, t1.y), f3(t1.z, t1.w, t2.x), tmin, hit.t,
                                tt, uu, vv)) {
-            const uint32_t key = __float_as_uint(t2.w);
-            if (AnyHit) { hit.t = tt; st.found = true; return true; }
-            if (!st.found || tt < hit.t || (tt == hit.t && key < hit.key)) {
-                st.found = true;
-                hit.t = tt; hit.u = uu; hit.v = vv; hit.key = key;
-                hit.inst = __float_as_uint(t2.y); hit.prim = __float_as_uint(t2.z);
-            }
+            if (AnyHit) { hit.t = tt; st.best = i; return true; }
+            bool take = st.best < 0 || tt < hit.t;
+            if (!take && tt == hit.t)
+                take = __float_as_uint(t2.w) < __float_as_uint(__ldg(s.tris + st.best * 3 + 2).w);
+            if (take) { st.best = i; hit.t = tt; }
         }
     }
     return false;
 }
 
+// Fills the closest hit's barycentrics, instance, primitive and key from its
+// triangle record: the same test on the same ray and triangle repeats the
+// traversal's arithmetic, so (t, u, v) are the values the traversal found.
+RR_D void trav_resolve(const DevScene& s, const Ray& r, float tmin, HitRec& hit, const TravState& st) {
+    if (st.best < 0) return;
+    const float4 t0 = __ldg(s.tris + st.best * 3 + 0);
+    const float4 t1 = __ldg(s.tris + st.best * 3 + 1);
+    const float4 t2 = __ldg(s.tris + st.best * 3 + 2);
+    float tt = hit.t, uu = 0.0f, vv = 0.0f;
+    intersect_triangle(r, f3(t0.x, t0.y, t0.z), f3(t0.w, t1.x, t1.y), f3(t1.z, t1.w, t2.x), tmin, hit.t, tt, uu, vv);
+    hit.u = uu; hit.v = vv;
+    hit.inst = __float_as_uint(t2.y); hit.prim = __float_as_uint(t2.z); hit.key = __float_as_uint(t2.w);
+}
+
+// Traversal stacks of (node, near distance) entries. LocalStack: all in
+// local memory. SplitStack: the bottom S entries in shared memory, one
+// column per thread of a block of Threads (entry j of a thread at
+// col[j * Threads], so a warp's accesses to one depth are consecutive
+// words), the deeper ones in local memory. Shared-memory entries do not
+// compete with node and triangle fetches for L1 lines.
+struct LocalStack {
+    int2 e[kStackSize];
+    RR_D void put(int i, int2 v) { e[i] = v; }
+    RR_D int2 get(int i) const { return e[i]; }
+};
+template <int S, int Threads>
+struct SplitStack {
+    int2* col;
+    int2 e[kStackSize - S];
+    RR_D void put(int i, int2 v) {
+        if (i < S) col[i * Threads] = v;
+        else e[i - S] = v;
+    }
+    RR_D int2 get(int i) const { return i < S ? col[i * Threads] : e[i - S]; }
+};
+
 // Pops the next stacked node not beyond the current hit; false when none is left.
-RR_D bool pop_node(TravState& st, const int2* stack, const HitRec& hit) {
+template <class Stack>
+RR_D bool pop_node(TravState& st, const Stack& stack, const HitRec& hit) {
     while (st.sp > 0) {
         --st.sp;
-        const int2 e = stack[st.sp];
+        const int2 e = stack.get(st.sp);
         if (__int_as_float(e.y) <= hit.t) { st.node = e.x; return true; }
     }
     return false;
@@ -228,9 +269,9 @@ RR_D bool pop_node(TravState& st, const int2* stack, const HitRec& hit) {
 // at a time (Aila and Laine 2009). Culling meanwhile uses the hit found so
 // far, which only visits more, and the kept (t, key) minimum does not depend
 // on the order, so the result is the same.
-template <bool AnyHit, bool Count, bool Postpone = false>
+template <bool AnyHit, bool Count, bool Postpone = false, class Stack>
 RR_D bool trace_step(const DevScene& s, const Ray& r, float tmin, HitRec& hit, TravState& st,
-                     int2* stack, TraceWork* work) {
+                     Stack& stack, TraceWork* work) {
     if constexpr (Postpone) {
         const bool all_hold = __all_sync(__activemask(), st.pend_count > 0);
         if (st.pend_count > 0 && (st.node < 0 || all_hold)) {
@@ -268,7 +309,7 @@ RR_D bool trace_step(const DevScene& s, const Ray& r, float tmin, HitRec& hit, T
     const bool i1 = h1 && d.y >= 0 && n1 <= hit.t;
     if (i0 && i1) {
         const bool first0 = AnyHit ? n0 > n1 : n0 <= n1;
-        stack[st.sp] = make_int2(first0 ? d.y : d.x, __float_as_int(first0 ? n1 : n0));
+        stack.put(st.sp, make_int2(first0 ? d.y : d.x, __float_as_int(first0 ? n1 : n0)));
         ++st.sp;
         st.node = first0 ? d.x : d.y;
     } else if (i0) {
@@ -289,11 +330,12 @@ RR_D bool trace_step(const DevScene& s, const Ray& r, float tmin, HitRec& hit, T
 // one ray per thread. Returns true on hit; `hit` is filled for closest hit.
 template <bool AnyHit, bool Count = false>
 RR_D bool trace(const DevScene& s, const Ray& r, float tmin, float tmax, HitRec& hit, TraceWork* work = nullptr) {
-    int2 stack[kStackSize];  // (node, near distance)
+    LocalStack stack;
     TravState st;
     trav_begin(st, hit, tmax);
     while (!trace_step<AnyHit, Count>(s, r, tmin, hit, st, stack, work)) {}
-    return st.found;
+    if constexpr (!AnyHit) trav_resolve(s, r, tmin, hit, st);
+    return st.found();
 }
 
 // Hit attributes (pathtracer.slang:69-118 / restir_di.slang:108-144):

@@ -125,12 +125,20 @@ struct WarpPool {
 // in the scene `table[index]` (the lane binds that scene's node and triangle
 // arrays when it loads the ray); otherwise every ray is traced in `s`. Rays
 // start at t = tmin (the path tracer's 0.001).
-template <bool AnyHit, bool Count, bool Refill, bool Multi, bool Postpone = false, class Load, class Finish>
+template <int SmemS> struct QueueStackOf { using type = SplitStack<SmemS, kBlock>; };
+template <> struct QueueStackOf<0> { using type = LocalStack; };
+
+template <bool AnyHit, bool Count, bool Refill, bool Multi, bool Postpone = false, int SmemS = 0, class Load,
+          class Finish>
 __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene* __restrict__ table, uint32_t count,
                                                uint32_t* cursor, unsigned long long* work_out, Load load,
                                                Finish finish, float tmin = 0.001f) {
     TraceWork tw;
-    int2 stack[kStackSize];  // (node, near distance)
+    typename QueueStackOf<SmemS>::type stack;   // (node, near distance) entries
+    if constexpr (SmemS > 0) {
+        __shared__ int2 stack_smem[SmemS * kBlock];
+        stack.col = stack_smem + threadIdx.x;
+    }
     DevScene ls{};           // Multi: the current ray's scene (traversal fields)
     auto bind = [&](uint32_t sid) {
         if constexpr (Multi) {
@@ -142,6 +150,12 @@ __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene
     auto step = [&](const Ray& r, HitRec& h, TravState& st) -> bool {
         if constexpr (Multi) return trace_step<AnyHit, Count, Postpone>(ls, r, tmin, h, st, stack, &tw);
         else return trace_step<AnyHit, Count, Postpone>(s, r, tmin, h, st, stack, &tw);
+    };
+    auto resolve = [&](const Ray& r, HitRec& h, const TravState& st) {
+        if constexpr (!AnyHit) {
+            if constexpr (Multi) trav_resolve(ls, r, tmin, h, st);
+            else trav_resolve(s, r, tmin, h, st);
+        }
     };
     if constexpr (!Refill) {
         while (true) {
@@ -156,7 +170,8 @@ __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene
                 HitRec h; TravState st;
                 trav_begin(st, h, tmax);
                 while (!step(r, h, st)) {}
-                finish(i, st.found, h);
+                resolve(r, h, st);
+                finish(i, st.found(), h);
             }
         }
     } else {
@@ -183,7 +198,8 @@ __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene
                 continue;
             }
             if (has && step(r, h, st)) {
-                finish(idx, st.found, h);
+                resolve(r, h, st);
+                finish(idx, st.found(), h);
                 has = false;
             }
         }
@@ -191,13 +207,13 @@ __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene
     if (Count) flush_work(tw, work_out);
 }
 
-template <bool Count, bool Refill, int MinBlocks, bool Postpone = false>
+template <bool Count, bool Refill, int MinBlocks, bool Postpone = false, int SmemS = 0>
 __global__ void __launch_bounds__(kBlock, MinBlocks) extend_kernel(DevScene s, const float4* __restrict__ qa,
                                                                    const float4* __restrict__ qb,
                                                                    float4* __restrict__ hits,
                                                                    const uint32_t* count_ptr, uint32_t* cursor,
                                                                    unsigned long long* work_out) {
-    traverse_queue<false, Count, Refill, false, Postpone>(
+    traverse_queue<false, Count, Refill, false, Postpone, SmemS>(
         s, nullptr, *count_ptr, cursor, work_out,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = qa[i], b = qb[i];
@@ -212,14 +228,14 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) extend_kernel(DevScene s, c
 }
 
 // Any-hit shadow rays; unoccluded NEE contributions are added to the image.
-template <bool Count, bool Refill, int MinBlocks, bool Postpone = false>
+template <bool Count, bool Refill, int MinBlocks, bool Postpone = false, int SmemS = 0>
 __global__ void __launch_bounds__(kBlock, MinBlocks) shadow_kernel(DevScene s, const float4* __restrict__ sa,
                                                                    const float4* __restrict__ sb,
                                                                    const float4* __restrict__ sc,
                                                                    float4* __restrict__ out,
                                                                    const uint32_t* count_ptr, uint32_t* cursor,
                                                                    unsigned long long* work_out) {
-    traverse_queue<true, Count, Refill, false, Postpone>(
+    traverse_queue<true, Count, Refill, false, Postpone, SmemS>(
         s, nullptr, *count_ptr, cursor, work_out,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = sa[i], b = sb[i];
@@ -288,7 +304,7 @@ __global__ void __launch_bounds__(kBlock) raygen_batch_kernel(const BatchEntry* 
     qc[slot] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(sid));
 }
 
-template <bool Count, bool Refill, int MinBlocks, bool Postpone = false>
+template <bool Count, bool Refill, int MinBlocks, bool Postpone = false, int SmemS = 0>
 __global__ void __launch_bounds__(kBlock, MinBlocks) extend_batch_kernel(const DevScene* __restrict__ table,
                                                                          const float4* __restrict__ qa,
                                                                          const float4* __restrict__ qb,
@@ -297,7 +313,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) extend_batch_kernel(const D
                                                                          const uint32_t* count_ptr, uint32_t* cursor,
                                                                          unsigned long long* work_out) {
     const DevScene none{};
-    traverse_queue<false, Count, Refill, true, Postpone>(
+    traverse_queue<false, Count, Refill, true, Postpone, SmemS>(
         none, table, *count_ptr, cursor, work_out,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = qa[i], b = qb[i];
@@ -311,7 +327,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) extend_batch_kernel(const D
         });
 }
 
-template <bool Count, bool Refill, int MinBlocks, bool Postpone = false>
+template <bool Count, bool Refill, int MinBlocks, bool Postpone = false, int SmemS = 0>
 __global__ void __launch_bounds__(kBlock, MinBlocks) shadow_batch_kernel(const DevScene* __restrict__ table,
                                                                          float4* const* __restrict__ outs,
                                                                          const float4* __restrict__ sa,
@@ -320,7 +336,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) shadow_batch_kernel(const D
                                                                          const uint32_t* count_ptr, uint32_t* cursor,
                                                                          unsigned long long* work_out) {
     const DevScene none{};
-    traverse_queue<true, Count, Refill, true, Postpone>(
+    traverse_queue<true, Count, Refill, true, Postpone, SmemS>(
         none, table, *count_ptr, cursor, work_out,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = sa[i], b = sb[i];
@@ -351,10 +367,10 @@ template <bool Count>
 BatchQueueKernel extend_batch_variant(int v) {
     switch (v) {
     case 1: return extend_batch_kernel<Count, false, 5>;
-    case 2: return extend_batch_kernel<Count, false, 6>;
+    case 2: return extend_batch_kernel<Count, false, 1, false, 8>;
     case 3: return extend_batch_kernel<Count, true, 1>;
     case 4: return extend_batch_kernel<Count, true, 4>;
-    case 5: return extend_batch_kernel<Count, true, 6>;
+    case 5: return extend_batch_kernel<Count, false, 5, false, 8>;
     case 6: return extend_batch_kernel<Count, false, 1, true>;
     case 7: return extend_batch_kernel<Count, false, 4, true>;
     default: return extend_batch_kernel<Count, false, 4>;
@@ -364,10 +380,10 @@ template <bool Count>
 BatchShadowKernel shadow_batch_variant(int v) {
     switch (v) {
     case 1: return shadow_batch_kernel<Count, false, 5>;
-    case 2: return shadow_batch_kernel<Count, false, 6>;
+    case 2: return shadow_batch_kernel<Count, false, 1, false, 8>;
     case 3: return shadow_batch_kernel<Count, true, 1>;
     case 4: return shadow_batch_kernel<Count, true, 4>;
-    case 5: return shadow_batch_kernel<Count, true, 6>;
+    case 5: return shadow_batch_kernel<Count, false, 5, false, 8>;
     case 6: return shadow_batch_kernel<Count, false, 1, true>;
     case 7: return shadow_batch_kernel<Count, false, 4, true>;
     default: return shadow_batch_kernel<Count, false, 1>;
@@ -383,10 +399,10 @@ template <bool Count>
 QueueKernel extend_variant(int v) {
     switch (v) {
     case 1: return extend_kernel<Count, false, 5>;
-    case 2: return extend_kernel<Count, false, 6>;
+    case 2: return extend_kernel<Count, false, 1, false, 8>;
     case 3: return extend_kernel<Count, true, 1>;
     case 4: return extend_kernel<Count, true, 4>;
-    case 5: return extend_kernel<Count, true, 6>;
+    case 5: return extend_kernel<Count, false, 5, false, 8>;
     case 6: return extend_kernel<Count, false, 1, true>;
     case 7: return extend_kernel<Count, false, 4, true>;
     default: return extend_kernel<Count, false, 1>;
@@ -396,10 +412,10 @@ template <bool Count>
 ShadowKernel shadow_variant(int v) {
     switch (v) {
     case 1: return shadow_kernel<Count, false, 5>;
-    case 2: return shadow_kernel<Count, false, 6>;
+    case 2: return shadow_kernel<Count, false, 1, false, 8>;
     case 3: return shadow_kernel<Count, true, 1>;
     case 4: return shadow_kernel<Count, true, 4>;
-    case 5: return shadow_kernel<Count, true, 6>;
+    case 5: return shadow_kernel<Count, false, 5, false, 8>;
     case 6: return shadow_kernel<Count, false, 1, true>;
     case 7: return shadow_kernel<Count, false, 4, true>;
     default: return shadow_kernel<Count, false, 1>;
