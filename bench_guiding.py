@@ -215,10 +215,13 @@ def measure(rr, torch, ctx, scene, methods=("unguided", "grid", "mlp"), target=0
     for m, rs in runs.items():
         ext = [x["time_to_target_extrapolated_ms"] for x in rs]
         meas = [x["time_to_target_ms"] for x in rs]
+        # a run that never stayed under the target counts as slower than
+        # every run that did (null when that decides the median)
+        med = statistics.median([x if x is not None else math.inf for x in meas])
         summary[m] = {"extrapolated_ms": ext, "extrapolated_ms_median": statistics.median(ext),
                       "measured_ms": meas,
-                      "measured_ms_median": statistics.median([x for x in meas if x is not None])
-                      if all(x is not None for x in meas) else None,
+                      "measured_ms_median": med if math.isfinite(med) else None,
+                      "runs_not_reaching_target": sum(x is None for x in meas),
                       "rel_sigma_per_spp": [x["rel_sigma_per_spp"] for x in rs],
                       "image_mean_ratio": [x["image_mean_ratio"] for x in rs],
                       "ms_per_frame": statistics.median([x["ms_per_frame"] for x in rs])}

@@ -74,11 +74,25 @@ constexpr int kSmFwdW = 0;
 constexpr int kSmFwdAct = kSmFwdW + fwd_wtile(kLayers - 1) + kOut * kIn * 2;
 constexpr int kSmFwdBar = kSmFwdAct + kTile * kIn * 2;
 constexpr int kSmFwd = kSmFwdBar + 64;
+// Forward CTAs of NW warpgroups (128 threads each) share one copy of the
+// weights; each warpgroup owns an activation tile, an mbarrier and 64 TMEM
+// columns, and runs its own stream of tiles.
+__host__ __device__ constexpr int fwd_act(int wg) { return kSmFwdAct + wg * kTile * kIn * 2; }
+__host__ __device__ constexpr int fwd_bar(int nw) { return fwd_act(nw); }
+__host__ __device__ constexpr int fwd_smem(int nw) { return fwd_bar(nw) + 64; }
+__host__ __device__ constexpr uint32_t tmem_cols(int nw) { return nw <= 2 ? 128u : (nw <= 4 ? 256u : 512u); }
+constexpr int kInferWG = 5;   // inference: 640 threads, 96 registers each, 149 KB of shared memory
+constexpr int kTrainWG = 3;   // training forward: 384 threads
 constexpr int kSmBwdWt = 0;
 constexpr int kSmBwdAct = kSmBwdWt + 2 * kWeightsBf16;
-constexpr int kSmBwdBar = kSmBwdAct + kTile * kHid * 2;
-constexpr int kSmBwd = kSmBwdBar + 64;
-static_assert(kSmFwdAct % 128 == 0 && kSmBwdAct % 128 == 0, "operand tiles 128-byte aligned");
+// backward CTAs: NW warpgroups sharing W^T, one activation tile, mbarrier and
+// 64 TMEM columns each (as the forward)
+__host__ __device__ constexpr int bwd_act(int wg) { return kSmBwdAct + wg * kTile * kHid * 2; }
+__host__ __device__ constexpr int bwd_bar(int nw) { return bwd_act(nw); }
+__host__ __device__ constexpr int bwd_smem(int nw) { return bwd_bar(nw) + 64; }
+constexpr int kBwdWG = 5;
+static_assert(kSmFwdAct % 128 == 0 && kSmBwdAct % 128 == 0 && (kTile * kIn * 2) % 128 == 0,
+              "operand tiles 128-byte aligned");
 
 // W of every layer as the forward's B operand (out x 80), with the BF16 bias
 // in column kBiasCol(l) and zeros in the other columns past the inputs. Each
@@ -245,6 +259,7 @@ struct FwdArgs {
     const double* wnorm;          // [0] = clamp value, [1] = 1 / (sum of clamped weights)
     __nv_bfloat16* X;             // [batch][kXCols], inputs of every layer
     __nv_bfloat16* dZ;            // [batch][kZCols], the forward writes the output layer's block
+    uint64_t* mask;               // [batch][kLayers - 1]: bit k of word l-1 = (X_l column k > 0)
     float* loss_partial;          // per block
     // grouped inference: group g's rows are slots group_base[g] + [0, group_count[g]) of surf/mix,
     // its tiles [tile_prefix[g], tile_prefix[g + 1]), its network nets[g]
@@ -255,26 +270,26 @@ struct FwdArgs {
     const uint32_t* tile_prefix;
 };
 
+// Bit j of the result: BF16 value j of the eight in q is > 0 (an ordered
+// comparison: zeros and NaN give 0), two values per paired comparison.
+__device__ __forceinline__ uint32_t positive_bf16x8(uint4 q) {
+    const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+    const __nv_bfloat162 zero = __floats2bfloat162_rn(0.0f, 0.0f);
+    uint32_t b = 0;
+    #pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const uint32_t m = __hgt2_mask(*reinterpret_cast<const __nv_bfloat162*>(&w[j]), zero);
+        b |= ((m & 1u) | ((m >> 15) & 2u)) << (2 * j);
+    }
+    return b;
+}
+
 __device__ __forceinline__ void store_row_bf16(__nv_bfloat16* dst, const float* v, int n) {
     uint4* d = reinterpret_cast<uint4*>(dst);
     #pragma unroll
     for (int k = 0; k < n; k += 8)
         d[k / 8] = make_uint4(tc::pack_bf16(v[k], v[k + 1]), tc::pack_bf16(v[k + 2], v[k + 3]),
                               tc::pack_bf16(v[k + 4], v[k + 5]), tc::pack_bf16(v[k + 6], v[k + 7]));
-}
-
-__device__ __forceinline__ void load_row_bf16(const __nv_bfloat16* src, float* v, int n) {
-    const uint4* s = reinterpret_cast<const uint4*>(src);
-    #pragma unroll
-    for (int k = 0; k < n; k += 8) {
-        const uint4 q = s[k / 8];
-        const uint32_t w[4] = {q.x, q.y, q.z, q.w};
-        #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            v[k + 2 * j] = __uint_as_float(w[j] << 16);
-            v[k + 2 * j + 1] = __uint_as_float(w[j] & 0xFFFF0000u);
-        }
-    }
 }
 
 // Issues the MMA chain D = A(128 x K) * B(N x K)^T from two K-major tiles and
@@ -300,25 +315,33 @@ __device__ __forceinline__ void wait_chain(uint64_t* bar, uint32_t phase, bool& 
     tc::fence_after_sync();
 }
 
-// Grouped (inference only): the CTA takes a contiguous range of the groups'
-// tiles and loads a group's weights when its range enters that group.
-template <bool Train, bool Grouped = false>
-__global__ void __launch_bounds__(kTile, 3) mlp_forward_kernel(FwdArgs A) {
+// Grouped (inference only, one warpgroup per CTA): the CTA takes a
+// contiguous range of the groups' tiles and loads a group's weights when its
+// range enters that group. Otherwise warpgroup g of CTA b takes tiles
+// b * NW + g, + gridDim.x * NW, ...; the warpgroups synchronise only among
+// themselves (named barrier 1 + g) inside the tile loop, so one warpgroup's
+// epilogue runs while another's MMA chain is on the tensor cores.
+template <bool Train, bool Grouped = false, int NW = 1>
+__global__ void __launch_bounds__(kTile * NW, Grouped ? 3 : 1) mlp_forward_kernel(FwdArgs A) {
     static_assert(!(Train && Grouped), "grouped forward is inference only");
+    static_assert(!Grouped || NW == 1, "grouped forward runs one warpgroup per CTA");
+    static_assert(NW >= 1 && NW <= 7, "warpgroups per CTA");
     extern __shared__ __align__(1024) unsigned char sm[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kSmFwdBar);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSmFwdBar + 8);
-    unsigned char* act = sm + kSmFwdAct;
-    const int t = threadIdx.x, warp = t >> 5;
+    const int wg = int(threadIdx.x) / kTile;
+    const int t = int(threadIdx.x) % kTile, warp = t >> 5;
+    constexpr int kBar = fwd_bar(NW);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kBar) + wg;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kBar + 56);
+    unsigned char* act = sm + fwd_act(wg);
     MlpView V = A.V;
     if constexpr (!Grouped) load_weights_fwd(sm, V);
-    if (warp == 0) tc::tmem_alloc(tslot, 128);
+    if (threadIdx.x < 32) tc::tmem_alloc(tslot, tmem_cols(NW));
     if (t == 0) tc::mbar_init(bar, 1);
     tc::fence_proxy_async();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    const uint32_t tmem = *tslot;
+    const uint32_t tmem = *tslot + uint32_t(wg * 64);
     uint32_t count = 0, tile_first, tile_end, tile_step;
     if constexpr (Grouped) {
         const uint32_t tiles = A.tile_prefix[A.groups];
@@ -328,10 +351,14 @@ __global__ void __launch_bounds__(kTile, 3) mlp_forward_kernel(FwdArgs A) {
         tile_step = 1;
     } else {
         count = Train ? A.count : *A.count_ptr;
-        tile_first = blockIdx.x;
+        tile_first = blockIdx.x * NW + wg;
         tile_end = (count + kTile - 1) / kTile;
-        tile_step = gridDim.x;
+        tile_step = gridDim.x * NW;
     }
+    auto wg_sync = [&]() {
+        if constexpr (NW == 1) __syncthreads();
+        else asm volatile("bar.sync %0, %1;" ::"r"(1 + wg), "r"(kTile) : "memory");
+    };
     const uint32_t act_addr = tc::smem_addr(act);
     const uint32_t w_addr = tc::smem_addr(sm + kSmFwdW);
     uint32_t phase = 0;
@@ -397,12 +424,14 @@ __global__ void __launch_bounds__(kTile, 3) mlp_forward_kernel(FwdArgs A) {
             const int I = lin(l), O = lout(l);
             tc::fence_proxy_async();
             tc::fence_before_sync();
-            __syncthreads();
+            wg_sync();
             if (t == 0) {
                 tc::fence_after_sync();
                 mma_chain(tmem, act_addr, w_addr + fwd_wtile(l), kIn, O, bar);
             }
-            wait_chain(bar, phase, ok);
+            if (t == 0) ok = tc::mbar_wait(bar, phase) && ok;
+            wg_sync();
+            tc::fence_after_sync();
             phase ^= 1u;
             (void)I;
             const uint32_t trow = tmem + (uint32_t(warp * 32) << 16);
@@ -421,6 +450,7 @@ __global__ void __launch_bounds__(kTile, 3) mlp_forward_kernel(FwdArgs A) {
                 // barrier before the next chain orders every thread's TMEM reads
                 // before that chain's writes.
                 uint4* xrow = reinterpret_cast<uint4*>(A.X + size_t(row) * kXCols + xoff(l + 1));
+                uint64_t mbits = 0;
                 #pragma unroll
                 for (int k = 0; k < O; k += 8) {
                     const uint4 q = make_uint4(tc::pack_bf16_relu(out[k], out[k + 1]),
@@ -428,8 +458,12 @@ __global__ void __launch_bounds__(kTile, 3) mlp_forward_kernel(FwdArgs A) {
                                                tc::pack_bf16_relu(out[k + 4], out[k + 5]),
                                                tc::pack_bf16_relu(out[k + 6], out[k + 7]));
                     *reinterpret_cast<uint4*>(act + tc::tile_offset(t, k, kTile)) = q;
-                    if (Train && valid) xrow[k / 8] = q;
+                    if (Train && valid) {
+                        xrow[k / 8] = q;
+                        mbits |= uint64_t(positive_bf16x8(q)) << k;
+                    }
                 }
+                if (Train && valid) A.mask[size_t(row) * (kLayers - 1) + l] = mbits;
             }
         }
         if (valid) {
@@ -457,224 +491,265 @@ __global__ void __launch_bounds__(kTile, 3) mlp_forward_kernel(FwdArgs A) {
         }
     }
     if (Train) {
-        __shared__ float red[kTile];
-        red[t] = loss_acc;
+        __shared__ float red[kTile * NW];
+        red[threadIdx.x] = loss_acc;
+        __syncthreads();
+        if (threadIdx.x < kTile) {
+            for (int g = 1; g < NW; ++g) red[threadIdx.x] += red[threadIdx.x + g * kTile];
+        }
         __syncthreads();
         for (int s = kTile / 2; s > 0; s >>= 1) {
-            if (t < s) red[t] += red[t + s];
+            if (int(threadIdx.x) < s) red[threadIdx.x] += red[threadIdx.x + s];
             __syncthreads();
         }
-        if (t == 0) A.loss_partial[blockIdx.x] = red[0];
+        if (threadIdx.x == 0) A.loss_partial[blockIdx.x] = red[0];
     }
     if (!ok && t == 0 && V.error) atomicExch(V.error, 1);
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) {
+    if (threadIdx.x < 32) {
         tc::fence_after_sync();
-        tc::tmem_free(tmem, 128);
+        tc::tmem_free(*tslot, tmem_cols(NW));
     }
 }
 
 struct BwdArgs {
     MlpView V;
     uint32_t count;
-    const __nv_bfloat16* X;       // [batch][kXCols]
+    const uint64_t* mask;         // [batch][kLayers - 1], ReLU masks of X_1 .. X_4 (from the forward)
     __nv_bfloat16* dZ;            // [batch][kZCols]; the output layer's block is an input
 };
 
 // dX_l = dZ_l W_l on the tensor cores (M = 128 samples, N = in, K = out),
-// dZ_{l-1} = dX_l * [X_l > 0], for l = 4 .. 1.
-__global__ void __launch_bounds__(kTile, 3) mlp_backward_kernel(BwdArgs A) {
+// dZ_{l-1} = dX_l * [X_l > 0], for l = 4 .. 1. Warpgroups as in the
+// forward. dZ stays packed BF16: the output block goes to the activation
+// tile as loaded, and each layer's dZ_{l-1} is written to the tile (the
+// chain that read it has completed) and to global memory eight columns at a
+// time as it is formed, so few values are live at once.
+template <int NW>
+__global__ void __launch_bounds__(kTile * NW, 1) mlp_backward_kernel(BwdArgs A) {
     extern __shared__ __align__(1024) unsigned char sm[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kSmBwdBar);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSmBwdBar + 8);
-    unsigned char* act = sm + kSmBwdAct;
-    const int t = threadIdx.x, warp = t >> 5;
+    const int wg = int(threadIdx.x) / kTile;
+    const int t = int(threadIdx.x) % kTile, warp = t >> 5;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + bwd_bar(NW)) + wg;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + bwd_bar(NW) + 56);
+    unsigned char* act = sm + bwd_act(wg);
     load_weights_bwd(sm, A.V);
-    if (warp == 0) tc::tmem_alloc(tslot, 128);
+    if (threadIdx.x < 32) tc::tmem_alloc(tslot, tmem_cols(NW));
     if (t == 0) tc::mbar_init(bar, 1);
     tc::fence_proxy_async();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    const uint32_t tmem = *tslot;
+    const uint32_t tmem = *tslot + uint32_t(wg * 64);
+    const uint32_t trow = tmem + (uint32_t(warp * 32) << 16);
     const uint32_t tiles = (A.count + kTile - 1) / kTile;
     const uint32_t act_addr = tc::smem_addr(act);
     const uint32_t wt_addr = tc::smem_addr(sm + kSmBwdWt);
+    auto wg_sync = [&]() { asm volatile("bar.sync %0, %1;" ::"r"(1 + wg), "r"(kTile) : "memory"); };
     uint32_t phase = 0;
     bool ok = true;
-    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    for (uint32_t tile = blockIdx.x * NW + wg; tile < tiles; tile += gridDim.x * NW) {
         const uint32_t row = tile * kTile + t;
         const bool valid = row < A.count;
-        float dz[kHid];
-        #pragma unroll
-        for (int q = 0; q < kHid; ++q) dz[q] = 0.0f;
-        if (valid) load_row_bf16(A.dZ + size_t(row) * kZCols + zoff(kLayers - 1), dz, kOut);
+        {
+            const uint4* src = reinterpret_cast<const uint4*>(A.dZ + size_t(row) * kZCols + zoff(kLayers - 1));
+            #pragma unroll
+            for (int k = 0; k < kOut; k += 8)
+                *reinterpret_cast<uint4*>(act + tc::tile_offset(t, k, kTile)) =
+                    valid ? src[k / 8] : make_uint4(0, 0, 0, 0);
+        }
         #pragma unroll
         for (int l = kLayers - 1; l >= 1; --l) {
             const int I = lin(l), O = lout(l);
-            #pragma unroll
-            for (int k = 0; k < O; k += 8) tc::st_row8(act, kTile, t, k, dz + k);
             tc::fence_proxy_async();
             tc::fence_before_sync();
-            __syncthreads();
+            wg_sync();
             if (t == 0) {
                 tc::fence_after_sync();
                 mma_chain(tmem, act_addr, wt_addr + 2 * hoff(l), O, I, bar);
             }
-            // X_l (the input of layer l >= 1) is ReLU(Z_{l-1}): its mask gates dZ_{l-1};
-            // the row is fetched while the chain runs
-            float xv[kHid];
-            if (valid) load_row_bf16(A.X + size_t(row) * kXCols + xoff(l), xv, I);
-            wait_chain(bar, phase, ok);
+            // X_l (the input of layer l >= 1) is ReLU(Z_{l-1}): its mask (written by
+            // the forward, one bit per column) gates dZ_{l-1}; fetched while the chain runs
+            const uint64_t mk = valid ? A.mask[size_t(row) * (kLayers - 1) + (l - 1)] : 0ull;
+            if (t == 0) ok = tc::mbar_wait(bar, phase) && ok;
+            wg_sync();
+            tc::fence_after_sync();
             phase ^= 1u;
-            float dx[kHid];
-            tc::tmem_ld32_wait(tmem + (uint32_t(warp * 32) << 16), dx);
-            tc::tmem_ld32_wait(tmem + (uint32_t(warp * 32) << 16) + 32, dx + 32);
             static_assert(kHid == 64, "dX is read as two 32-column loads");
+            uint4* zrow = reinterpret_cast<uint4*>(A.dZ + size_t(row) * kZCols + zoff(l - 1));
             #pragma unroll
-            for (int k = 0; k < I; ++k) dz[k] = (valid && xv[k] > 0.0f) ? dx[k] : 0.0f;
-            if (valid) store_row_bf16(A.dZ + size_t(row) * kZCols + zoff(l - 1), dz, I);
+            for (int h = 0; h < 2; ++h) {
+                float dx[32];
+                tc::tmem_ld32_wait(trow + uint32_t(h * 32), dx);
+                #pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const uint32_t mb = uint32_t(mk >> (h * 32 + c * 8)) & 0xFFu;
+                    uint32_t q[4];
+                    #pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float d0 = (mb >> (2 * j)) & 1u ? dx[c * 8 + 2 * j] : 0.0f;
+                        const float d1 = (mb >> (2 * j + 1)) & 1u ? dx[c * 8 + 2 * j + 1] : 0.0f;
+                        q[j] = tc::pack_bf16(d0, d1);
+                    }
+                    const uint4 v = make_uint4(q[0], q[1], q[2], q[3]);
+                    *reinterpret_cast<uint4*>(act + tc::tile_offset(t, h * 32 + c * 8, kTile)) = v;
+                    if (valid) zrow[h * 4 + c] = v;
+                }
+            }
+            (void)I;
         }
     }
     if (!ok && t == 0) atomicExch(A.V.error, 1);
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) {
+    if (threadIdx.x < 32) {
         tc::fence_after_sync();
-        tc::tmem_free(tmem, 128);
+        tc::tmem_free(*tslot, tmem_cols(NW));
     }
 }
 
 // ── weight gradients on the tensor cores ──────────────────────────────────
 // dW_l^T (in x out) = X_l^T dZ_l with the batch as the K dimension. A
-// persistent CTA owns a contiguous range of 64-sample steps. Per step it
-// stages the transposes of the step's X rows (kWgRowsX rows) and dZ rows
-// (kZCols rows) K-major in shared memory; layer l's A operand is the 128-row
-// window from row kWgRow[l]: its I input features, a constant row of ones
-// (whose product with dZ_l is db_l) and rows that are ignored. Layer l
-// accumulates into TMEM columns kWgCol[l] .. + out over all of the CTA's
-// steps; the CTA then writes its FP32 partial gradient, and
-// mlp_reduce_kernel sums the partials in CTA order.
-constexpr int kWgStep = 64;                                  // samples per step (K)
-// first row of layer l's window: layer 0 takes 80 inputs + the ones row (88
-// rows after padding to 8), hidden layers 64 + 1 (72 rows)
+// persistent CTA owns a contiguous range of 32-sample steps. Both operands
+// are MN-major: a sample's row of X (features contiguous) and of dZ (outputs
+// contiguous) lands in shared memory as it lies in global memory, 16 bytes
+// (8 features of one sample) per copy, so the rows are staged by cp.async
+// with no transposition and no registers, four stages deep. Layer l's A
+// operand is the 128-feature window from feature kWgRow[l]: its I inputs, a
+// constant feature of ones (whose product with dZ_l is db_l) and features
+// that are ignored. Layer l accumulates into TMEM columns zoff(l) .. + out
+// over all of the CTA's steps; the CTA then writes its FP32 partial
+// gradient, and mlp_reduce_kernel sums the partials in CTA order.
+//
+// MN-major operand layout (no swizzle): 8 consecutive features (16 bytes)
+// of one sample form a row of a core matrix, the 8 samples of a sample
+// group its 8 rows (128 contiguous bytes); feature groups are 128 bytes
+// apart (SBO) and sample groups kWgLbo* apart (LBO).
+constexpr int kWgStep = 32;                                  // samples per step (K)
+constexpr int kWgStages = 4;
+// first feature of layer l's window: layer 0 takes 80 inputs + the ones
+// feature (88 after padding to 8), hidden layers 64 + 1 (72)
 __host__ __device__ constexpr int wg_row(int l) { return l == 0 ? 0 : 88 + (l - 1) * 72; }
 static_assert(wg_row(1) == ((kIn + 1 + 7) / 8) * 8 && wg_row(2) - wg_row(1) == ((kHid + 1 + 7) / 8) * 8, "rows");
-constexpr int kWgRowsX = wg_row(kLayers - 1) + kTile;        // 432
-constexpr int kWgLboX = kWgRowsX * 16 + 16;                  // K-block stride; +16 B keeps the stores conflict-free
-constexpr int kWgLboZ = kZCols * 16 + 16;
+constexpr int kWgRowsX = wg_row(kLayers - 1) + kTile;        // 432 features staged
+constexpr int kWgLboX = (kWgRowsX / 8) * 128;                // sample-group stride of the X stage
+constexpr int kWgLboZ = (kZCols / 8) * 128;                  // sample-group stride of the dZ stage
 constexpr int kWgBlkX = (kWgStep / 8) * kWgLboX;
-constexpr int kWgBlkZ = (kWgStep / 8) * kWgLboZ;
-constexpr int kWgStage = kWgBlkX + kWgBlkZ;
-constexpr int kSmWg = 2 * kWgStage + 64;
+constexpr int kWgStage = kWgBlkX + (kWgStep / 8) * kWgLboZ;
+constexpr int kSmWg = kWgStages * kWgStage + 64;
 static_assert(kSmWg <= 227 * 1024, "wgrad stages exceed shared memory");
 static_assert(kZCols <= 512 && zoff(kLayers) <= 304, "wgrad TMEM columns");
+static_assert(kXCols % 8 == 0 && kZCols % 8 == 0 && kWgStep % 16 == 0, "16-byte copies, K = 16 per MMA");
 
 constexpr int kWgThreads = 256;                              // 8 warps; warps 0-3 also read TMEM
-constexpr int kWgGroups = (kXCols + kZCols) / 8;             // 8-column groups staged per step
-static_assert(kWgGroups % (kWgThreads / 32) == 0, "groups split evenly over the warps");
+constexpr int kWgChunks = (kXCols + kZCols) / 8;             // 16-byte copies per sample (42 of X, 38 of dZ)
+constexpr int kWgPer = kWgChunks * kWgStep / kWgThreads;     // copies per thread per step
+static_assert(kWgChunks % 4 == 0 && (kWgChunks * kWgStep) % kWgThreads == 0, "copies split evenly");
+
+// kind::f16 instruction descriptor with both operands MN-major.
+__host__ __device__ constexpr uint32_t idesc_bf16_mn(uint32_t M, uint32_t N) {
+    return tc::idesc_bf16(M, N) | (1u << 15) | (1u << 16);
+}
+
 __global__ void __launch_bounds__(kWgThreads, 1) mlp_wgrad_kernel(const __nv_bfloat16* __restrict__ X,
                                                             const __nv_bfloat16* __restrict__ dZ, uint32_t count,
                                                             float* __restrict__ partial, int* error) {
     extern __shared__ __align__(1024) unsigned char sm[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * kWgStage);     // one per stage
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + 2 * kWgStage + 16);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kWgStages * kWgStage);   // one per stage
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kWgStages * kWgStage + 8 * kWgStages);
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const uint32_t steps = (count + kWgStep - 1) / kWgStep;
     const uint32_t s_begin = uint32_t((uint64_t(blockIdx.x) * steps) / gridDim.x);
     const uint32_t s_end = uint32_t((uint64_t(blockIdx.x + 1) * steps) / gridDim.x);
-    // constant rows: zero everything, then the ones rows of both stages
-    for (int e = t; e < 2 * kWgStage / 16; e += kWgThreads) reinterpret_cast<uint4*>(sm)[e] = make_uint4(0, 0, 0, 0);
+    const uint32_t n = s_end - s_begin;
+    // constant features: zero every stage, then the ones feature of each
+    // window (feature wg_row(l) + I, the first of its group) for every sample
+    for (int e = t; e < kWgStages * kWgStage / 16; e += kWgThreads) reinterpret_cast<uint4*>(sm)[e] = make_uint4(0, 0, 0, 0);
     __syncthreads();
-    for (int e = t; e < 2 * kLayers * (kWgStep / 2); e += kWgThreads) {
-        const int stage = e / (kLayers * (kWgStep / 2));
-        const int l = (e / (kWgStep / 2)) % kLayers;
-        const int p = e % (kWgStep / 2);
-        const int r = wg_row(l) + lin(l);
-        *reinterpret_cast<uint32_t*>(sm + stage * kWgStage + (p / 4) * kWgLboX + r * 16 + (p % 4) * 4) = 0x3F803F80u;
+    for (int e = t; e < kWgStages * kLayers * kWgStep; e += kWgThreads) {
+        const int stage = e / (kLayers * kWgStep);
+        const int l = (e / kWgStep) % kLayers;
+        const int smp = e % kWgStep;
+        const int g = (wg_row(l) + lin(l)) / 8;
+        *reinterpret_cast<uint4*>(sm + stage * kWgStage + (smp / 8) * kWgLboX + g * 128 + (smp % 8) * 16) =
+            make_uint4(0x3F80u, 0u, 0u, 0u);
     }
     if (warp == 0) tc::tmem_alloc(tslot, 512);
-    if (t == 0) { tc::mbar_init(bar, 1); tc::mbar_init(bar + 1, 1); }
+    if (t == 0) {
+        for (int k = 0; k < kWgStages; ++k) tc::mbar_init(bar + k, 1);
+    }
     tc::fence_proxy_async();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *tslot;
-    bool ok = true;
-    for (uint32_t step = s_begin; step < s_end; ++step) {
-        const uint32_t i = step - s_begin;
-        const uint32_t buf = i & 1u;
-        // lane = sample pair (samples 2*lane, 2*lane+1 of the step); warp w stages groups w, w+8, ...
-        // all of this thread's global loads are issued before it waits and stores
-        constexpr int kPer = kWgGroups / (kWgThreads / 32);
-        const uint32_t s0 = step * kWgStep + 2 * lane, s1 = s0 + 1;
-        uint4 ra[kPer], rb[kPer];
-        #pragma unroll
-        for (int q = 0; q < kPer; ++q) {
-            const int g = warp + q * (kWgThreads / 32);
-            const bool is_x = g < kXCols / 8;
-            const int col = is_x ? g * 8 : (g - kXCols / 8) * 8;
-            const __nv_bfloat16* base = is_x ? X : dZ;
-            const size_t ld = is_x ? kXCols : kZCols;
-            ra[q] = s0 < count ? *reinterpret_cast<const uint4*>(base + size_t(s0) * ld + col) : make_uint4(0, 0, 0, 0);
-            rb[q] = s1 < count ? *reinterpret_cast<const uint4*>(base + size_t(s1) * ld + col) : make_uint4(0, 0, 0, 0);
-        }
-        if (i >= 2) wait_chain(bar + buf, ((i >> 1) - 1u) & 1u, ok);   // the MMAs of step i-2 are done
-        unsigned char* xb = sm + buf * kWgStage;
-        unsigned char* zb = xb + kWgBlkX;
-        #pragma unroll
-        for (int q = 0; q < kPer; ++q) {
-            const int g = warp + q * (kWgThreads / 32);
-            const bool is_x = g < kXCols / 8;
-            const int col = is_x ? g * 8 : (g - kXCols / 8) * 8;
-            int r0;
-            unsigned char* blk;
-            uint32_t lbo;
-            if (is_x) {
-                int l = 0;
-                #pragma unroll
-                for (int u = 1; u < kLayers; ++u) l += col >= xoff(u) ? 1 : 0;
-                r0 = wg_row(l) + (col - xoff(l));
-                blk = xb;
-                lbo = kWgLboX;
-            } else {
-                r0 = col;
-                blk = zb;
-                lbo = kWgLboZ;
+    // copies of step i into stage i % kWgStages: copy q of this thread is
+    // chunk c of sample (step, sample group sg, sample sg * 8 + lane % 8);
+    // the 8 lanes of a quarter-warp take one chunk of 8 consecutive samples
+    // (128 contiguous bytes of shared memory), a warp 4 consecutive chunks
+    auto issue = [&](uint32_t i) {
+        if (i < n) {
+            unsigned char* xs = sm + (i % kWgStages) * kWgStage;
+            unsigned char* zs = xs + kWgBlkX;
+            const uint32_t step = s_begin + i;
+            #pragma unroll
+            for (int q = 0; q < kWgPer; ++q) {
+                const int u = (q * kWgThreads + t) >> 5;            // warp-sized unit
+                const int sg = u / (kWgChunks / 4);
+                const int c = (u % (kWgChunks / 4)) * 4 + (lane >> 3);
+                const int smp = sg * 8 + (lane & 7);
+                const uint32_t row = step * kWgStep + smp;
+                const bool in = row < count;
+                const uint32_t rr = in ? row : 0u;
+                unsigned char* dst;
+                const __nv_bfloat16* src;
+                if (c < kXCols / 8) {
+                    int l = 0;
+                    #pragma unroll
+                    for (int v = 1; v < kLayers; ++v) l += c * 8 >= xoff(v) ? 1 : 0;
+                    const int g = (wg_row(l) + (c * 8 - xoff(l))) / 8;
+                    dst = xs + (smp / 8) * kWgLboX + g * 128 + (smp % 8) * 16;
+                    src = X + size_t(rr) * kXCols + c * 8;
+                } else {
+                    const int g = c - kXCols / 8;
+                    dst = zs + (smp / 8) * kWgLboZ + g * 128 + (smp % 8) * 16;
+                    src = dZ + size_t(rr) * kZCols + g * 8;
+                }
+                tc::cp_async16_zfill(dst, src, in);
             }
-            unsigned char* dst = blk + (lane / 4) * lbo + r0 * 16 + (lane % 4) * 4;
-            const uint4 a4 = ra[q], b4 = rb[q];
-            *reinterpret_cast<uint32_t*>(dst + 0 * 16) = __byte_perm(a4.x, b4.x, 0x5410);
-            *reinterpret_cast<uint32_t*>(dst + 1 * 16) = __byte_perm(a4.x, b4.x, 0x7632);
-            *reinterpret_cast<uint32_t*>(dst + 2 * 16) = __byte_perm(a4.y, b4.y, 0x5410);
-            *reinterpret_cast<uint32_t*>(dst + 3 * 16) = __byte_perm(a4.y, b4.y, 0x7632);
-            *reinterpret_cast<uint32_t*>(dst + 4 * 16) = __byte_perm(a4.z, b4.z, 0x5410);
-            *reinterpret_cast<uint32_t*>(dst + 5 * 16) = __byte_perm(a4.z, b4.z, 0x7632);
-            *reinterpret_cast<uint32_t*>(dst + 6 * 16) = __byte_perm(a4.w, b4.w, 0x5410);
-            *reinterpret_cast<uint32_t*>(dst + 7 * 16) = __byte_perm(a4.w, b4.w, 0x7632);
         }
+        tc::cp_async_commit();
+    };
+    bool ok = true;
+    issue(0);
+    issue(1);
+    for (uint32_t i = 0; i < n; ++i) {
+        // the stage of step i + 2 was read by the MMAs of step i - 2
+        if (i >= 2) wait_chain(bar + ((i - 2) % kWgStages), ((i - 2) / kWgStages) & 1u, ok);
+        issue(i + 2);
+        tc::cp_async_wait_group2();            // step i has landed (steps i + 1, i + 2 may be in flight)
         tc::fence_proxy_async();
         tc::fence_before_sync();
         __syncthreads();
         if (t == 0) {
             tc::fence_after_sync();
-            const uint32_t xa = tc::smem_addr(xb), za = tc::smem_addr(zb);
+            const uint32_t xa = tc::smem_addr(sm + (i % kWgStages) * kWgStage), za = xa + kWgBlkX;
             #pragma unroll
             for (int l = 0; l < kLayers; ++l) {
-                const uint32_t idesc = tc::idesc_bf16(kTile, uint32_t(lout(l)));
+                const uint32_t idesc = idesc_bf16_mn(kTile, uint32_t(lout(l)));
                 #pragma unroll
-                for (int s = 0; s < kWgStep / 16; ++s) {
-                    const uint64_t ad = tc::smem_desc(xa + wg_row(l) * 16 + s * 2 * kWgLboX, kWgLboX, 128);
-                    const uint64_t bd = tc::smem_desc(za + zoff(l) * 16 + s * 2 * kWgLboZ, kWgLboZ, 128);
-                    tc::mma_bf16(tmem + uint32_t(zoff(l)), ad, bd, idesc, i > 0 || s > 0);
+                for (int ks = 0; ks < kWgStep / 16; ++ks) {
+                    const uint64_t ad = tc::smem_desc(xa + (wg_row(l) / 8) * 128 + ks * 2 * kWgLboX, kWgLboX, 128);
+                    const uint64_t bd = tc::smem_desc(za + (zoff(l) / 8) * 128 + ks * 2 * kWgLboZ, kWgLboZ, 128);
+                    tc::mma_bf16(tmem + uint32_t(zoff(l)), ad, bd, idesc, i > 0 || ks > 0);
                 }
             }
-            tc::mma_commit(bar + buf);
+            tc::mma_commit(bar + (i % kWgStages));
         }
     }
-    const uint32_t n = s_end - s_begin;
-    if (n > 0) wait_chain(bar + ((n - 1) & 1u), ((n - 1) >> 1) & 1u, ok);
+    tc::cp_async_wait_all();
+    if (n > 0) wait_chain(bar + ((n - 1) % kWgStages), ((n - 1) / kWgStages) & 1u, ok);
     float* dst = partial + size_t(blockIdx.x) * kParams;
     const int r = warp * 32 + lane;   // TMEM lane = row of dW^T = input feature (I = bias row)
     #pragma unroll
@@ -802,6 +877,7 @@ struct rr_mlp_state {
     double* wnorm = nullptr;
     __nv_bfloat16* X = nullptr;
     __nv_bfloat16* dZ = nullptr;
+    uint64_t* mask = nullptr;
     float* loss_partial = nullptr;
     float* wpartial = nullptr;    // per wgrad CTA: kParams FP32
     double* wn_partial = nullptr; // per weight-norm block
@@ -854,15 +930,21 @@ rr_status rr_mlp_guide_init(rr_ctx* ctx, rr_guide* g) {
     if ((st = al(reinterpret_cast<void**>(&M.wnorm), 16)) != RR_OK) return st;
     if ((st = al(reinterpret_cast<void**>(&M.X), size_t(B) * kXCols * 2)) != RR_OK) return st;
     if ((st = al(reinterpret_cast<void**>(&M.dZ), size_t(B) * kZCols * 2)) != RR_OK) return st;
+    if ((st = al(reinterpret_cast<void**>(&M.mask), size_t(B) * (kLayers - 1) * 8)) != RR_OK) return st;
     M.grid = 3 * ctx->sm_count;
     if ((st = al(reinterpret_cast<void**>(&M.loss_partial), size_t(M.grid) * 4)) != RR_OK) return st;
     M.wg_grid = ctx->sm_count;
     if ((st = al(reinterpret_cast<void**>(&M.wpartial), size_t(M.wg_grid) * kParams * 4)) != RR_OK) return st;
     if ((st = al(reinterpret_cast<void**>(&M.wn_partial), size_t(kWnBlocks) * 8)) != RR_OK) return st;
     RR_TRY_CUDA(ctx, cudaMallocHost(&M.loss_host, size_t(M.grid) * 4));
-    for (auto k : {mlp_forward_kernel<true>, mlp_forward_kernel<false>, mlp_forward_kernel<false, true>})
-        RR_TRY_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmFwd));
-    RR_TRY_CUDA(ctx, cudaFuncSetAttribute(mlp_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmBwd));
+    RR_TRY_CUDA(ctx, cudaFuncSetAttribute(mlp_forward_kernel<true, false, kTrainWG>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, fwd_smem(kTrainWG)));
+    RR_TRY_CUDA(ctx, cudaFuncSetAttribute(mlp_forward_kernel<false, false, kInferWG>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, fwd_smem(kInferWG)));
+    RR_TRY_CUDA(ctx, cudaFuncSetAttribute(mlp_forward_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          kSmFwd));
+    RR_TRY_CUDA(ctx, cudaFuncSetAttribute(mlp_backward_kernel<kBwdWG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          bwd_smem(kBwdWG)));
     RR_TRY_CUDA(ctx, cudaFuncSetAttribute(mlp_wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmWg));
     return RR_OK;
 }
@@ -901,8 +983,8 @@ rr_status rr_mlp_guide_infer(rr_ctx* ctx, rr_guide* g, const uint32_t* count_dev
     A.mix = g->mlp_mix;
     A.count_ptr = count_dev;
     const uint32_t tiles = (max_count + kTile - 1) / kTile;
-    const int grid = int(std::min<uint32_t>(tiles, uint32_t(3 * ctx->sm_count)));
-    mlp_forward_kernel<false><<<std::max(grid, 1), kTile, kSmFwd, stream>>>(A);
+    const int grid = int(std::min<uint32_t>((tiles + kInferWG - 1) / kInferWG, uint32_t(ctx->sm_count)));
+    mlp_forward_kernel<false, false, kInferWG><<<std::max(grid, 1), kTile * kInferWG, fwd_smem(kInferWG), stream>>>(A);
     RR_CHECK_LAUNCH(ctx);
     g->mlp_infer_launches = 1;
     return RR_OK;
@@ -952,8 +1034,8 @@ rr_status rr_mlp_guide_eval(rr_ctx* ctx, rr_guide* g, const float4* surf, float4
     A.mix = mix;
     A.count_ptr = count_dev;
     const uint32_t tiles = (count + kTile - 1) / kTile;
-    const int grid = int(std::min<uint32_t>(tiles, uint32_t(3 * ctx->sm_count)));
-    mlp_forward_kernel<false><<<std::max(grid, 1), kTile, kSmFwd, stream>>>(A);
+    const int grid = int(std::min<uint32_t>((tiles + kInferWG - 1) / kInferWG, uint32_t(ctx->sm_count)));
+    mlp_forward_kernel<false, false, kInferWG><<<std::max(grid, 1), kTile * kInferWG, fwd_smem(kInferWG), stream>>>(A);
     RR_CHECK_LAUNCH(ctx);
     ctx->launches += 1;
     return RR_OK;
@@ -978,18 +1060,20 @@ rr_status rr_mlp_guide_train(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t 
     A.wnorm = M.wnorm;
     A.X = M.X;
     A.dZ = M.dZ;
+    A.mask = M.mask;
     A.loss_partial = M.loss_partial;
     const uint32_t tiles = (B + kTile - 1) / kTile;
-    const int grid = int(std::min<uint32_t>(tiles, uint32_t(M.grid)));
+    const int fgrid = int(std::min<uint32_t>((tiles + kTrainWG - 1) / kTrainWG, uint32_t(ctx->sm_count)));
     RR_TRY_CUDA(ctx, cudaMemsetAsync(M.loss_partial, 0, size_t(M.grid) * 4, stream));
-    mlp_forward_kernel<true><<<grid, kTile, kSmFwd, stream>>>(A);
+    mlp_forward_kernel<true, false, kTrainWG><<<fgrid, kTile * kTrainWG, fwd_smem(kTrainWG), stream>>>(A);
     RR_CHECK_LAUNCH(ctx);
     BwdArgs Bw{};
     Bw.V = A.V;
     Bw.count = B;
-    Bw.X = M.X;
+    Bw.mask = M.mask;
     Bw.dZ = M.dZ;
-    mlp_backward_kernel<<<grid, kTile, kSmBwd, stream>>>(Bw);
+    const int bgrid = int(std::min<uint32_t>((tiles + kBwdWG - 1) / kBwdWG, uint32_t(ctx->sm_count)));
+    mlp_backward_kernel<kBwdWG><<<bgrid, kTile * kBwdWG, bwd_smem(kBwdWG), stream>>>(Bw);
     RR_CHECK_LAUNCH(ctx);
     const uint32_t wsteps = (B + kWgStep - 1) / kWgStep;
     const int wgrid = int(std::min<uint32_t>(wsteps, uint32_t(M.wg_grid)));

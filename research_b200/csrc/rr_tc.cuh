@@ -154,6 +154,23 @@ __device__ __forceinline__ uint32_t pack_bf16_relu(float a, float b) {
     return d;
 }
 
+// 16-byte asynchronous copy global -> shared (cached in L2 only); the
+// copies a thread issued since its last commit form one group, and
+// cp_async_wait_all waits until all of its groups have landed.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(smem)), "l"(gmem) : "memory");
+}
+// As cp_async16, writing 16 zero bytes (and reading nothing) when !in.
+__device__ __forceinline__ void cp_async16_zfill(void* smem, const void* gmem, bool in) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(smem)), "l"(gmem),
+                 "r"(in ? 16u : 0u)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// Waits until at most two of this thread's most recent groups are pending.
+__device__ __forceinline__ void cp_async_wait_group2() { asm volatile("cp.async.wait_group 2;" ::: "memory"); }
+
 // Stores 8 consecutive K values of row r (k0 multiple of 8) into a tile.
 __device__ __forceinline__ void st_row8(unsigned char* tile, uint32_t rows, uint32_t r, uint32_t k0, const float* v) {
     uint4 q;

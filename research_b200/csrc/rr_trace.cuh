@@ -54,7 +54,7 @@ struct Ray {
     float3 o, d, inv;
     float3 alo, ahi;
     float Sx, Sy, Sz;
-    int k;   // shear axes kx | ky << 2 | kz << 4 (one register across the traversal loop)
+    int kx, ky, kz;
 };
 
 RR_D float comp(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
@@ -70,7 +70,7 @@ RR_D Ray make_ray(float3 o, float3 d) {
     int ky = kx + 1; if (ky == 3) ky = 0;
     const float dz = comp(d, kz);
     if (dz < 0.0f) { const int t = kx; kx = ky; ky = t; }
-    r.k = kx | (ky << 2) | (kz << 4);
+    r.kx = kx; r.ky = ky; r.kz = kz;
     r.Sx = comp(d, kx) / dz;
     r.Sy = comp(d, ky) / dz;
     r.Sz = 1.0f / dz;
@@ -100,12 +100,11 @@ RR_D Ray make_ray(float3 o, float3 d) {
 // Watertight test; two-sided. On hit writes t and the weights of v1, v2.
 RR_D bool intersect_triangle(const Ray& r, float3 p0, float3 p1, float3 p2, float tmin,
                              float tmax, float& t, float& bu, float& bv) {
-    const int kx = r.k & 3, ky = (r.k >> 2) & 3, kz = r.k >> 4;
     const float3 A = p0 - r.o, B = p1 - r.o, C = p2 - r.o;
-    const float Az0 = comp(A, kz), Bz0 = comp(B, kz), Cz0 = comp(C, kz);
-    const float Ax = comp(A, kx) - r.Sx * Az0, Ay = comp(A, ky) - r.Sy * Az0;
-    const float Bx = comp(B, kx) - r.Sx * Bz0, By = comp(B, ky) - r.Sy * Bz0;
-    const float Cx = comp(C, kx) - r.Sx * Cz0, Cy = comp(C, ky) - r.Sy * Cz0;
+    const float Az0 = comp(A, r.kz), Bz0 = comp(B, r.kz), Cz0 = comp(C, r.kz);
+    const float Ax = comp(A, r.kx) - r.Sx * Az0, Ay = comp(A, r.ky) - r.Sy * Az0;
+    const float Bx = comp(B, r.kx) - r.Sx * Bz0, By = comp(B, r.ky) - r.Sy * Bz0;
+    const float Cx = comp(C, r.kx) - r.Sx * Cz0, Cy = comp(C, r.ky) - r.Sy * Cz0;
     const float U = Cx * By - Cy * Bx;
     const float V = Ax * Cy - Ay * Cx;
     const float W = Bx * Ay - By * Ax;
@@ -164,28 +163,23 @@ struct TraceWork {
 };
 
 // Traversal state of one ray between node steps. node < 0: no inner node
-// left, only the postponed leaf (pend_count > 0) to intersect. best: the
-// triangle record (index into the scene's triangle array) of the closest hit
-// so far, -1 for none; only hit.t is kept beside it while the ray traverses,
-// and trav_resolve fills in the rest of the hit record at the end.
+// left, only the postponed leaf (pend_count > 0) to intersect.
 struct TravState {
     int node;
     int sp;
-    int best;
+    bool found;
     uint32_t visits;
     int pend_first, pend_count;
-    RR_D bool found() const { return best >= 0; }
 };
 
 RR_D void trav_begin(TravState& st, HitRec& hit, float tmax) {
-    st.node = 0; st.sp = 0; st.best = -1; st.visits = 0;
+    st.node = 0; st.sp = 0; st.found = false; st.visits = 0;
     st.pend_first = 0; st.pend_count = 0;
     hit.t = tmax; hit.key = kNoIndex;
 }
 
 // The triangles [first, first + count) of a leaf against the ray; closest
-// hit: keeps the lowest (t, key), reading the kept triangle's key only on an
-// exact tie of t; any hit: returns true at the first hit.
+// hit: keeps the lowest (t, key); any hit: returns true at the first hit.
 template <bool AnyHit, bool Count>
 RR_D bool leaf_tris(const DevScene& s, const Ray& r, float tmin, HitRec& hit, TravState& st, int first, int count,
                     TraceWork* work) {
@@ -197,28 +191,16 @@ RR_D bool leaf_tris(const DevScene& s, const Ray& r, float tmin, HitRec& hit, Tr
         float tt, uu, vv;
         if (intersect_triangle(r, f3(t0.x, t0.y, t0.z), f3(t0.w, t1.x, t1.y), f3(t1.z, t1.w, t2.x), tmin, hit.t,
                                tt, uu, vv)) {
-            if (AnyHit) { hit.t = tt; st.best = i; return true; }
-            bool take = st.best < 0 || tt < hit.t;
-            if (!take && tt == hit.t)
-                take = __float_as_uint(t2.w) < __float_as_uint(__ldg(s.tris + st.best * 3 + 2).w);
-            if (take) { st.best = i; hit.t = tt; }
+            const uint32_t key = __float_as_uint(t2.w);
+            if (AnyHit) { hit.t = tt; st.found = true; return true; }
+            if (!st.found || tt < hit.t || (tt == hit.t && key < hit.key)) {
+                st.found = true;
+                hit.t = tt; hit.u = uu; hit.v = vv; hit.key = key;
+                hit.inst = __float_as_uint(t2.y); hit.prim = __float_as_uint(t2.z);
+            }
         }
     }
     return false;
-}
-
-// Fills the closest hit's barycentrics, instance, primitive and key from its
-// triangle record: the same test on the same ray and triangle repeats the
-// traversal's arithmetic, so (t, u, v) are the values the traversal found.
-RR_D void trav_resolve(const DevScene& s, const Ray& r, float tmin, HitRec& hit, const TravState& st) {
-    if (st.best < 0) return;
-    const float4 t0 = __ldg(s.tris + st.best * 3 + 0);
-    const float4 t1 = __ldg(s.tris + st.best * 3 + 1);
-    const float4 t2 = __ldg(s.tris + st.best * 3 + 2);
-    float tt = hit.t, uu = 0.0f, vv = 0.0f;
-    intersect_triangle(r, f3(t0.x, t0.y, t0.z), f3(t0.w, t1.x, t1.y), f3(t1.z, t1.w, t2.x), tmin, hit.t, tt, uu, vv);
-    hit.u = uu; hit.v = vv;
-    hit.inst = __float_as_uint(t2.y); hit.prim = __float_as_uint(t2.z); hit.key = __float_as_uint(t2.w);
 }
 
 // Traversal stacks of (node, near distance) entries. LocalStack: all in
@@ -334,8 +316,7 @@ RR_D bool trace(const DevScene& s, const Ray& r, float tmin, float tmax, HitRec&
     TravState st;
     trav_begin(st, hit, tmax);
     while (!trace_step<AnyHit, Count>(s, r, tmin, hit, st, stack, work)) {}
-    if constexpr (!AnyHit) trav_resolve(s, r, tmin, hit, st);
-    return st.found();
+    return st.found;
 }
 
 // Hit attributes (pathtracer.slang:69-118 / restir_di.slang:108-144):

@@ -128,6 +128,7 @@ struct WarpPool {
 template <int SmemS> struct QueueStackOf { using type = SplitStack<SmemS, kBlock>; };
 template <> struct QueueStackOf<0> { using type = LocalStack; };
 
+// SmemS > 0: the bottom SmemS stack entries of every thread in shared memory.
 template <bool AnyHit, bool Count, bool Refill, bool Multi, bool Postpone = false, int SmemS = 0, class Load,
           class Finish>
 __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene* __restrict__ table, uint32_t count,
@@ -151,12 +152,6 @@ __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene
         if constexpr (Multi) return trace_step<AnyHit, Count, Postpone>(ls, r, tmin, h, st, stack, &tw);
         else return trace_step<AnyHit, Count, Postpone>(s, r, tmin, h, st, stack, &tw);
     };
-    auto resolve = [&](const Ray& r, HitRec& h, const TravState& st) {
-        if constexpr (!AnyHit) {
-            if constexpr (Multi) trav_resolve(ls, r, tmin, h, st);
-            else trav_resolve(s, r, tmin, h, st);
-        }
-    };
     if constexpr (!Refill) {
         while (true) {
             uint32_t base = 0;
@@ -170,8 +165,7 @@ __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene
                 HitRec h; TravState st;
                 trav_begin(st, h, tmax);
                 while (!step(r, h, st)) {}
-                resolve(r, h, st);
-                finish(i, st.found(), h);
+                finish(i, st.found, h);
             }
         }
     } else {
@@ -198,8 +192,7 @@ __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene
                 continue;
             }
             if (has && step(r, h, st)) {
-                resolve(r, h, st);
-                finish(idx, st.found(), h);
+                finish(idx, st.found, h);
                 has = false;
             }
         }
@@ -390,7 +383,7 @@ BatchShadowKernel shadow_batch_variant(int v) {
     }
 }
 
-// Traversal kernel variants: schedule x occupancy target.
+// Traversal kernel variants: schedule x occupancy target x stack placement.
 using QueueKernel = void (*)(DevScene, const float4*, const float4*, float4*, const uint32_t*, uint32_t*,
                              unsigned long long*);
 using ShadowKernel = void (*)(DevScene, const float4*, const float4*, const float4*, float4*, const uint32_t*,
