@@ -40,6 +40,8 @@ CFG = dict(width=1920, height=1080, spp=4, max_bounces=5, di_candidates=32, di_n
            box_half=20.0, eye=(0.0, 4.0, 34.0), center=(0.0, -3.0, 0.0))
 # Algorithmic bytes (per unit): a ray record 32 B in + 16 B hit out, a BVH2
 # node (two child boxes) 64 B, a triangle (3 vertices) 36 B.
+# A node of the 4-wide tree (the wide traversal variants) holds four child
+# boxes: 128 B (rr_pathtracer_variant_width).
 RAY_BYTES, NODE_BYTES, TRI_BYTES = 48, 64, 36
 
 
@@ -541,10 +543,12 @@ def run_ours(args, ws, rank, local):
 
     # roofline of the dominant kernel (BVH traversal of extension rays)
     peak, peak_kind = load_peaks()
-    ext_bytes = (counted["extension_rays"] * RAY_BYTES + counted["extension_nodes"] * NODE_BYTES +
+    node_bytes = {k: NODE_BYTES * rr.lib().rr_pathtracer_variant_width(tuned[k + "_variant"]) // 2
+                  for k in ("extend", "shadow")}
+    ext_bytes = (counted["extension_rays"] * RAY_BYTES + counted["extension_nodes"] * node_bytes["extend"] +
                  counted["extension_tris"] * TRI_BYTES)
     ext_ms = pt_stage["extend"]
-    shadow_bytes = (counted["shadow_rays"] * RAY_BYTES + counted["shadow_nodes"] * NODE_BYTES +
+    shadow_bytes = (counted["shadow_rays"] * RAY_BYTES + counted["shadow_nodes"] * node_bytes["shadow"] +
                     counted["shadow_tris"] * TRI_BYTES)
     achieved = ext_bytes / (ext_ms * 1e-3) / 1e9 if ext_ms > 0 else 0.0
     # DRAM bytes are not measured in this run (that needs ncu): the figure of
@@ -558,13 +562,14 @@ def run_ours(args, ws, rank, local):
         from_profile = {"dram_bytes_per_launch": per_launch, "dram_gbs": dram_gbs, "dram_frac": dram_gbs / peak,
                         "source": "ncu capture of one frame's extend launches, summarised in "
                                   "profiles/extend_traffic.txt; not measured in this run"}
-    roofline = {"kernel": "extend_kernel (closest-hit BVH2 traversal, all bounces of one frame)",
+    roofline = {"kernel": "extend_kernel (closest-hit BVH traversal, all bounces of one frame)",
                 "bound": "latency (L1/L2-served node fetches, SIMT divergence)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": f"{peak_kind} hbm_gbs", "traffic": None, "from_profile": from_profile,
                 "achieved_scope": "algorithmic bytes (rays, BVH nodes and triangles the traversal touches, counted by "
                                   "the kernel) per second of extend time; most are served by L1/L2, not HBM",
                 "algorithmic_bytes_per_step": ext_bytes, "launches_per_step": CFG["max_bounces"],
+                "node_bytes": node_bytes,
                 "shadow_achieved_gbs": shadow_bytes / (pt_stage["shadow"] * 1e-3) / 1e9 if pt_stage["shadow"] else 0}
     rays = counted["extension_rays"] + counted["shadow_rays"]
 

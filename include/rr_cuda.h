@@ -89,6 +89,8 @@ typedef struct rr_scene_stats {
     double   build_ms;            /* host BVH build */
     double   upload_ms;
     uint64_t device_bytes;
+    uint32_t bvh4_node_count;     /* nodes of the same tree laid out 4-wide (four child boxes each) */
+    uint32_t _pad;
 } rr_scene_stats;
 
 rr_status rr_scene_create(rr_ctx* ctx, const rr_scene_desc* desc, rr_scene** out_scene);
@@ -140,14 +142,18 @@ typedef struct rr_pt_stats {
 rr_status rr_pathtracer_stats(rr_ctx* ctx, rr_pt_stats* out, int reset_times);
 
 /* Traversal kernel variants (no reference counterpart; the reference uses
- * hardware ray queries): variant = schedule x occupancy target,
- *   0..2: warps trace 32 consecutive queue entries to completion, with the
- *         compiler's register count (default) / a budget for 5 / 6 blocks of
- *         256 threads per SM;
- *   3..5: persistent warps with per-lane ray refill, with the compiler's
- *         register count / a budget for 4 / 6 blocks;
- *   6..7: as 0, with leaves postponed until every lane of the warp holds one
- *         (the compiler's register count / a budget for 4 blocks).
+ * hardware ray queries): variant = tree x stack x occupancy target; every
+ * warp traces 32 consecutive queue entries to completion.
+ *   0: binary tree, stack in local memory, the compiler's register count
+ *      (default);
+ *   1: as 0 with a register budget for 5 blocks of 256 threads per SM;
+ *   2: as 0 with the bottom 8 stack entries in shared memory;
+ *   5: as 2 with a budget for 5 blocks;
+ *   3, 4, 6: the 4-wide tree (rr_pathtracer_variant_width), stack in local
+ *      memory / bottom 8 entries in shared memory / as 4 with a budget for 3
+ *      blocks;
+ *   7: binary tree with leaves postponed until every lane of the warp holds
+ *      one, budget for 4 blocks.
  * Results are identical for every variant; only speed differs. */
 #define RR_PT_VARIANT_COUNT 8
 rr_status rr_pathtracer_set_variants(rr_ctx* ctx, int extend_variant, int shadow_variant);
@@ -637,16 +643,25 @@ rr_status rr_image_mse(rr_ctx* ctx, const float* a, const float* b, uint32_t wid
 rr_status rr_trace_closest(rr_ctx* ctx, const rr_scene* scene, const float* origins,
                            const float* dirs, float tmin, float tmax, uint32_t count,
                            float* hits, uint32_t* prims, void* stream);
-/* The same query with the traversal's work counters: any_hit selects the
- * shadow-ray (first hit) form; work receives per ray (BVH nodes visited,
- * triangles tested), the counts behind RR_PT_FLAG_COUNT_TRAVERSAL. */
+/* The same query with the traversal's work counters. flags: bit 0
+ * (RR_TRACE_ANY_HIT) selects the shadow-ray (first hit) form, bit 1
+ * (RR_TRACE_WIDE) the 4-wide tree; work receives per ray (BVH nodes
+ * visited, triangles tested), the counts behind RR_PT_FLAG_COUNT_TRAVERSAL. */
+#define RR_TRACE_ANY_HIT 1
+#define RR_TRACE_WIDE 2
 rr_status rr_trace_counted(rr_ctx* ctx, const rr_scene* scene, const float* origins,
-                           const float* dirs, float tmin, float tmax, uint32_t count, int any_hit,
+                           const float* dirs, float tmin, float tmax, uint32_t count, int flags,
                            float* hits, uint32_t* prims, uint32_t* work, void* stream);
 /* Host copies of the scene's BVH (rr_scene_stats.bvh_node_count nodes of
  * 16 floats, layout in rr_trace.cuh) and triangle records (triangle_count
  * records of 12 floats). Synchronous. */
 rr_status rr_scene_copy_bvh(rr_ctx* ctx, const rr_scene* scene, float* nodes_out, float* tris_out);
+/* Host copy of the 4-wide layout of the same tree (rr_scene_stats.
+ * bvh4_node_count nodes of 32 floats, layout in rr_trace.cuh). Synchronous. */
+rr_status rr_scene_copy_bvh4(rr_ctx* ctx, const rr_scene* scene, float* nodes4_out);
+/* Width of the tree a traversal variant walks: 2 or 4 (0 for a variant out
+ * of range). A node of the 4-wide tree is 128 bytes, of the binary one 64. */
+int rr_pathtracer_variant_width(int variant);
 /* Bounded-wait self-test of the tensor-core kernels' mbarrier waits: one
  * block waits (at most `limit` tries, 1..2^22) on a barrier that nothing
  * arrives on and on one that received its arrival. completed_out[0] = 1 if

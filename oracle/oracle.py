@@ -88,6 +88,7 @@ _SIG = {
     "oracle_restir_pt_temporal": (None, [P, P, C.POINTER(PtReuseParams), C.POINTER(PtReuseImages), I]),
     "oracle_restir_pt_spatial_shade": (None, [P, P, C.POINTER(PtReuseParams), C.POINTER(PtReuseImages), I]),
     "oracle_bvh2_trace": (None, [P, U32, P, P, P, F32, F32, U32, I, P, P, P, I]),
+    "oracle_bvh4_trace": (None, [P, U32, P, P, P, F32, F32, U32, I, P, P, P, I]),
     "oracle_restir_gi_initial": (None, [P, P, C.POINTER(GiReuseParams), C.POINTER(GiReuseImages), I]),
     "oracle_restir_gi_temporal": (None, [P, P, C.POINTER(GiReuseParams), C.POINTER(GiReuseImages), I]),
     "oracle_restir_gi_spatial_shade": (None, [P, P, C.POINTER(GiReuseParams), C.POINTER(GiReuseImages), I]),
@@ -304,6 +305,18 @@ def bvh2_trace(nodes, tris, origins, dirs, tmin, tmax, any_hit, nthreads=None):
     prims = np.zeros(n, np.uint32)
     work = np.zeros((n, 2), np.uint32)
     lib().oracle_bvh2_trace(_p(nodes), len(nodes), _p(tris), _p(origins), _p(dirs), tmin, tmax, n, int(any_hit),
+                            _p(hits), _p(prims), _p(work), nthreads or threads())
+    return hits, prims, work
+
+
+def bvh4_trace(nodes4, tris, origins, dirs, tmin, tmax, any_hit, nthreads=None):
+    """bvh2_trace over the library's 4-wide layout of the same tree (nodes4:
+    (n, 32) float32 from rr_scene_copy_bvh4)."""
+    n = len(origins)
+    hits = np.zeros((n, 4), np.float32)
+    prims = np.zeros(n, np.uint32)
+    work = np.zeros((n, 2), np.uint32)
+    lib().oracle_bvh4_trace(_p(nodes4), len(nodes4), _p(tris), _p(origins), _p(dirs), tmin, tmax, n, int(any_hit),
                             _p(hits), _p(prims), _p(work), nthreads or threads())
     return hits, prims, work
 

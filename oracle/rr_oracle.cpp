@@ -1941,6 +1941,123 @@ void oracle_bvh2_trace(const float* nodes, uint32_t num_nodes, const float* tris
     });
 }
 
+// ── traversal work on the library's 4-wide tree ───────────────────────────
+// Restatement of trace_step4 (research_b200/csrc/rr_trace.cuh: box_quad,
+// trace_step4) over the 4-wide node array copied from a scene
+// (rr_scene_copy_bvh4): 8 float4 per node, lo.x, hi.x, lo.y, hi.y, lo.z,
+// hi.z of children 0..3, their references (< 0 a leaf at triangle ~ref) and
+// triangle counts. Hit leaf children are intersected in slot order; hit
+// inner children within the current t are ordered by a five-comparator
+// network on (distance, node) (closest hit ascending, any hit by descending
+// distance, a swap only on a strictly smaller key), the first is visited
+// next and the rest pushed so that they pop in that order.
+void oracle_bvh4_trace(const float* nodes4, uint32_t num_nodes4, const float* tris, const float* origins,
+                       const float* dirs, float tmin, float tmax, uint32_t n, int any_hit, float* hits,
+                       uint32_t* prims, uint32_t* work, int threads) {
+    auto as_i = [](float f) { int32_t i; memcpy(&i, &f, 4); return i; };
+    auto as_u = [](float f) { uint32_t i; memcpy(&i, &f, 4); return i; };
+    parallel_rows(n, threads, [&](uint32_t i) {
+        const RayPre r = ray_pre(load3(origins + 4 * size_t(i)), load3(dirs + 4 * size_t(i)));
+        float alo[3], ahi[3];
+        const float o3[3] = {r.o.x, r.o.y, r.o.z}, inv3[3] = {r.inv.x, r.inv.y, r.inv.z};
+        for (int a = 0; a < 3; ++a) {
+            const float oi = o3[a] * inv3[a];
+            const float m = fabsf(oi) * 2.384185791015625e-7f;
+            const float anear = -oi - m, afar = -oi + m;
+            alo[a] = inv3[a] >= 0.0f ? anear : afar;
+            ahi[a] = inv3[a] >= 0.0f ? afar : anear;
+        }
+        float best_t = tmax, bu = 0, bv = 0;
+        uint32_t best_key = 0xffffffffu, best_inst = 0, best_prim = 0, nn_count = 0, tri_count = 0;
+        bool found = false, done = false;
+        int node = 0, sp = 0, stack_node[192];
+        float stack_t[192];
+        uint32_t visits = 0;
+        auto pop = [&]() -> bool {
+            while (sp > 0) {
+                --sp;
+                if (stack_t[sp] <= best_t) { node = stack_node[sp]; return true; }
+            }
+            return false;
+        };
+        while (!done) {
+            if (++visits > num_nodes4 + 1) break;
+            const float* N = nodes4 + 32 * size_t(node);
+            ++nn_count;
+            const float tlim = best_t * 1.00001f;
+            bool h[4]; float nr[4];
+            for (int k = 0; k < 4; ++k) {
+                const float tx0 = fmaf(N[0 + k], inv3[0], alo[0]), tx1 = fmaf(N[4 + k], inv3[0], ahi[0]);
+                const float ty0 = fmaf(N[8 + k], inv3[1], alo[1]), ty1 = fmaf(N[12 + k], inv3[1], ahi[1]);
+                const float tz0 = fmaf(N[16 + k], inv3[2], alo[2]), tz1 = fmaf(N[20 + k], inv3[2], ahi[2]);
+                const float nn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+                const float ff = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1)) * 1.000002f;
+                h[k] = nn <= fminf(ff, tlim);
+                nr[k] = nn;
+            }
+            int R[4], K[4];
+            for (int k = 0; k < 4; ++k) { R[k] = as_i(N[24 + k]); K[k] = as_i(N[28 + k]); }
+            for (int k = 0; k < 4 && !done; ++k) {
+                if (!(h[k] && R[k] < 0)) continue;
+                const int first = ~R[k];
+                for (int t = first; t < first + K[k]; ++t) {
+                    ++tri_count;
+                    const float* T = tris + 12 * size_t(t);
+                    float tt, uu, vv;
+                    if (intersect_tri(r, v3(T[0], T[1], T[2]), v3(T[3], T[4], T[5]), v3(T[6], T[7], T[8]), tmin,
+                                      best_t, tt, uu, vv)) {
+                        const uint32_t key = as_u(T[11]);
+                        if (any_hit) { best_t = tt; found = true; done = true; break; }
+                        if (!found || tt < best_t || (tt == best_t && key < best_key)) {
+                            found = true; best_t = tt; bu = uu; bv = vv; best_key = key;
+                            best_inst = as_u(T[9]); best_prim = as_u(T[10]);
+                        }
+                    }
+                }
+            }
+            if (done) break;
+            float key[4];
+            int nd[4], m = 0;
+            for (int k = 0; k < 4; ++k) {
+                const bool in = h[k] && R[k] >= 0 && nr[k] <= best_t;
+                m += in ? 1 : 0;
+                key[k] = in ? (any_hit ? -nr[k] : nr[k]) : INFINITY;
+                nd[k] = R[k];
+            }
+            auto cswap = [&](int a, int b) {
+                if (key[b] < key[a]) { std::swap(key[a], key[b]); std::swap(nd[a], nd[b]); }
+            };
+            cswap(0, 1); cswap(2, 3); cswap(0, 2); cswap(1, 3); cswap(1, 2);
+            if (m == 0) {
+                if (!pop()) done = true;
+                continue;
+            }
+            for (int k = 3; k >= 1; --k) {
+                if (k < m) {
+                    stack_node[sp] = nd[k];
+                    stack_t[sp] = any_hit ? -key[k] : key[k];
+                    ++sp;
+                }
+            }
+            node = nd[0];
+        }
+        float* H = hits + 4 * size_t(i);
+        if (found) {
+            H[0] = best_t; H[1] = any_hit ? 0.0f : bu; H[2] = any_hit ? 0.0f : bv;
+            const uint32_t inst = any_hit ? 0u : best_inst;
+            memcpy(&H[3], &inst, 4);
+            prims[i] = any_hit ? 0u : best_prim;
+        } else {
+            H[0] = -1.0f; H[1] = H[2] = 0.0f;
+            const uint32_t none = 0xffffffffu;
+            memcpy(&H[3], &none, 4);
+            prims[i] = none;
+        }
+        work[2 * size_t(i)] = nn_count;
+        work[2 * size_t(i) + 1] = tri_count;
+    });
+}
+
 // ── ReSTIR GI (restir_gi.slang:568-1000; ReSTIRGIPass.cpp:428-650) ────────────
 void oracle_restir_gi_initial(const OracleScene* scene, const GpuCameraData* cam, const OracleRestirGiParams* p,
                               const OracleRestirGiImages* img, int threads) {

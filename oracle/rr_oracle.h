@@ -207,6 +207,9 @@ void oracle_restir_pt_spatial_shade(const OracleScene* scene, const GpuCameraDat
 void oracle_bvh2_trace(const float* nodes, uint32_t num_nodes, const float* tris, const float* origins,
                        const float* dirs, float tmin, float tmax, uint32_t n, int any_hit, float* hits,
                        uint32_t* prims, uint32_t* work, int threads);
+void oracle_bvh4_trace(const float* nodes4, uint32_t num_nodes4, const float* tris, const float* origins,
+                       const float* dirs, float tmin, float tmax, uint32_t n, int any_hit, float* hits,
+                       uint32_t* prims, uint32_t* work, int threads);
 
 /* ── ReSTIR GI (restir_gi.slang:568-1000) ───────────────────────────────── */
 typedef struct OracleRestirGiParams {

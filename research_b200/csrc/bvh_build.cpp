@@ -6,7 +6,10 @@
 // leaves of at most 8 triangles, depth capped at 60 so a 64-entry traversal
 // stack always suffices), then lays it out for the GPU: every inner node
 // stores the boxes of both children, inner nodes in depth-first order.
-// Large subtrees are built on separate threads.
+// Large subtrees are built on separate threads. The same tree is also laid
+// out 4-wide: a 4-wide node's children are a binary node's frontier of up to
+// four nodes, grown by opening the inner frontier node of largest surface
+// area (the leaves are the binary tree's leaves).
 
 #include "rr_bvh.h"
 
@@ -138,6 +141,55 @@ struct Builder {
 inline float4 mk4(float x, float y, float z, float w) { float4 v; v.x = x; v.y = y; v.z = z; v.w = w; return v; }
 inline float i2f(int32_t i) { float f; std::memcpy(&f, &i, 4); return f; }
 
+// 4-wide layout (8 float4 per node): lo.x, hi.x, lo.y, hi.y, lo.z, hi.z of
+// children 0..3, then their references (>= 0 a node, < 0 a leaf starting at
+// triangle ~ref) and their triangle counts. An unused child slot gets a
+// point box at 1e30 on every axis, which no ray reaches within its tmax.
+struct Wide4 {
+    const std::vector<Node>& nodes;
+    std::vector<float4>& out;
+    int32_t emit(const std::vector<uint32_t>& kids) {
+        const int32_t idx = int32_t(out.size() / 8);
+        out.resize(out.size() + 8);
+        float lo[3][4], hi[3][4];
+        int32_t ref[4] = {0, 0, 0, 0}, cnt[4] = {0, 0, 0, 0};
+        for (int k = 0; k < 4; ++k)
+            for (int a = 0; a < 3; ++a) lo[a][k] = hi[a][k] = 1e30f;
+        for (size_t k = 0; k < kids.size(); ++k) {
+            const Node& c = nodes[kids[k]];
+            for (int a = 0; a < 3; ++a) { lo[a][k] = c.box.lo[a]; hi[a][k] = c.box.hi[a]; }
+            if (c.left < 0) { ref[k] = ~int32_t(c.first); cnt[k] = int32_t(c.count); }
+            else ref[k] = emit(frontier(kids[k]));
+        }
+        float4* q = &out[size_t(idx) * 8];
+        for (int a = 0; a < 3; ++a) {
+            q[2 * a] = mk4(lo[a][0], lo[a][1], lo[a][2], lo[a][3]);
+            q[2 * a + 1] = mk4(hi[a][0], hi[a][1], hi[a][2], hi[a][3]);
+        }
+        q[6] = mk4(i2f(ref[0]), i2f(ref[1]), i2f(ref[2]), i2f(ref[3]));
+        q[7] = mk4(i2f(cnt[0]), i2f(cnt[1]), i2f(cnt[2]), i2f(cnt[3]));
+        return idx;
+    }
+    // the up-to-four-node frontier below inner binary node b
+    std::vector<uint32_t> frontier(uint32_t b) const {
+        std::vector<uint32_t> kids{uint32_t(nodes[b].left), uint32_t(nodes[b].right)};
+        while (kids.size() < 4) {
+            int best = -1;
+            float best_area = -1.0f;
+            for (size_t k = 0; k < kids.size(); ++k) {
+                if (nodes[kids[k]].left < 0) continue;
+                const float ar = nodes[kids[k]].box.area();
+                if (ar > best_area) { best_area = ar; best = int(k); }
+            }
+            if (best < 0) break;
+            const uint32_t c = kids[best];
+            kids[best] = uint32_t(nodes[c].left);
+            kids.insert(kids.begin() + best + 1, uint32_t(nodes[c].right));
+        }
+        return kids;
+    }
+};
+
 } // namespace
 
 BvhBuild build_bvh(const std::vector<float>& tri_world, int /*threads*/) {
@@ -160,6 +212,12 @@ BvhBuild build_bvh(const std::vector<float>& tri_world, int /*threads*/) {
     if (n > 0) B.build(0, 0, n, 0);
     else nodes[0].box = Box();
     out.max_depth = B.depth_max.load() + 1;
+    {
+        Wide4 W{nodes, out.nodes4};
+        if (n > 0 && nodes[0].left >= 0) W.emit(W.frontier(0));
+        else if (n > 0) W.emit(std::vector<uint32_t>{0u});   // the root is a leaf
+        else W.emit(std::vector<uint32_t>{});
+    }
 
     // GPU layout: one GPU node per inner binary node, depth-first, left first.
     auto child_ref = [&](const Node& c, std::vector<int32_t>& gidx, int32_t ci, int32_t& ref, int32_t& cnt) {

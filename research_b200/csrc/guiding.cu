@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(128) trace_batch_kernel(DevScene s, const floa
         prims[i] = kNoIndex;
     }
 }
-template <bool AnyHit>
+template <bool AnyHit, bool Wide>
 __global__ void __launch_bounds__(128) trace_counted_kernel(DevScene s, const float4* __restrict__ o,
                                                             const float4* __restrict__ d, float tmin, float tmax,
                                                             uint32_t n, float4* __restrict__ hits,
@@ -148,7 +148,9 @@ __global__ void __launch_bounds__(128) trace_counted_kernel(DevScene s, const fl
     const float4 a = o[i], b = d[i];
     HitRec h;
     TraceWork w;
-    if (trace<AnyHit, true>(s, make_ray(xyz(a), xyz(b)), tmin, tmax, h, &w)) {
+    const Ray ray = make_ray(xyz(a), xyz(b));
+    const bool found = Wide ? trace4<AnyHit, true>(s, ray, tmin, tmax, h, &w) : trace<AnyHit, true>(s, ray, tmin, tmax, h, &w);
+    if (found) {
         hits[i] = make_float4(h.t, AnyHit ? 0.0f : h.u, AnyHit ? 0.0f : h.v,
                               __uint_as_float(AnyHit ? 0u : h.inst));
         prims[i] = AnyHit ? 0u : h.prim;
@@ -162,22 +164,27 @@ __global__ void __launch_bounds__(128) trace_counted_kernel(DevScene s, const fl
 } // namespace rr
 
 extern "C" rr_status rr_trace_counted(rr_ctx* ctx, const rr_scene* scene, const float* origins, const float* dirs,
-                                      float tmin, float tmax, uint32_t count, int any_hit, float* hits,
+                                      float tmin, float tmax, uint32_t count, int flags, float* hits,
                                       uint32_t* prims, uint32_t* work, void* stream) {
     if (!ctx) return RR_ERR_INVALID_ARGUMENT;
-    if (!scene || (count && (!origins || !dirs || !hits || !prims || !work)))
+    if (!scene || (count && (!origins || !dirs || !hits || !prims || !work)) ||
+        (flags & ~(RR_TRACE_ANY_HIT | RR_TRACE_WIDE)))
         return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_trace_counted: bad argument");
     if (count == 0) return RR_OK;
     RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
     const auto o = reinterpret_cast<const float4*>(origins);
     const auto d = reinterpret_cast<const float4*>(dirs);
     const auto st = static_cast<cudaStream_t>(stream);
-    if (any_hit)
-        rr::trace_counted_kernel<true><<<(count + 127) / 128, 128, 0, st>>>(
-            scene->dev, o, d, tmin, tmax, count, reinterpret_cast<float4*>(hits), prims, reinterpret_cast<uint2*>(work));
-    else
-        rr::trace_counted_kernel<false><<<(count + 127) / 128, 128, 0, st>>>(
-            scene->dev, o, d, tmin, tmax, count, reinterpret_cast<float4*>(hits), prims, reinterpret_cast<uint2*>(work));
+    auto launch = [&](auto kernel) {
+        kernel<<<(count + 127) / 128, 128, 0, st>>>(scene->dev, o, d, tmin, tmax, count, reinterpret_cast<float4*>(hits),
+                                                    prims, reinterpret_cast<uint2*>(work));
+    };
+    switch (flags) {
+    case 0: launch(rr::trace_counted_kernel<false, false>); break;
+    case RR_TRACE_ANY_HIT: launch(rr::trace_counted_kernel<true, false>); break;
+    case RR_TRACE_WIDE: launch(rr::trace_counted_kernel<false, true>); break;
+    default: launch(rr::trace_counted_kernel<true, true>); break;
+    }
     RR_CHECK_LAUNCH(ctx);
     ctx->launches += 1;
     return RR_OK;
@@ -190,6 +197,15 @@ extern "C" rr_status rr_scene_copy_bvh(rr_ctx* ctx, const rr_scene* scene, float
     RR_TRY_CUDA(ctx, cudaMemcpy(nodes_out, scene->dev.nodes, size_t(scene->dev.num_nodes) * 4 * sizeof(float4),
                                 cudaMemcpyDeviceToHost));
     RR_TRY_CUDA(ctx, cudaMemcpy(tris_out, scene->dev.tris, size_t(scene->dev.num_tris) * 3 * sizeof(float4),
+                                cudaMemcpyDeviceToHost));
+    return RR_OK;
+}
+
+extern "C" rr_status rr_scene_copy_bvh4(rr_ctx* ctx, const rr_scene* scene, float* nodes4_out) {
+    if (!ctx) return RR_ERR_INVALID_ARGUMENT;
+    if (!scene || !nodes4_out) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "rr_scene_copy_bvh4: bad argument");
+    RR_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    RR_TRY_CUDA(ctx, cudaMemcpy(nodes4_out, scene->dev.nodes4, size_t(scene->dev.num_nodes4) * 8 * sizeof(float4),
                                 cudaMemcpyDeviceToHost));
     return RR_OK;
 }

@@ -259,7 +259,6 @@ struct FwdArgs {
     const double* wnorm;          // [0] = clamp value, [1] = 1 / (sum of clamped weights)
     __nv_bfloat16* X;             // [batch][kXCols], inputs of every layer
     __nv_bfloat16* dZ;            // [batch][kZCols], the forward writes the output layer's block
-    uint64_t* mask;               // [batch][kLayers - 1]: bit k of word l-1 = (X_l column k > 0)
     float* loss_partial;          // per block
     // grouped inference: group g's rows are slots group_base[g] + [0, group_count[g]) of surf/mix,
     // its tiles [tile_prefix[g], tile_prefix[g + 1]), its network nets[g]
@@ -269,20 +268,6 @@ struct FwdArgs {
     const uint32_t* group_count;
     const uint32_t* tile_prefix;
 };
-
-// Bit j of the result: BF16 value j of the eight in q is > 0 (an ordered
-// comparison: zeros and NaN give 0), two values per paired comparison.
-__device__ __forceinline__ uint32_t positive_bf16x8(uint4 q) {
-    const uint32_t w[4] = {q.x, q.y, q.z, q.w};
-    const __nv_bfloat162 zero = __floats2bfloat162_rn(0.0f, 0.0f);
-    uint32_t b = 0;
-    #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const uint32_t m = __hgt2_mask(*reinterpret_cast<const __nv_bfloat162*>(&w[j]), zero);
-        b |= ((m & 1u) | ((m >> 15) & 2u)) << (2 * j);
-    }
-    return b;
-}
 
 __device__ __forceinline__ void store_row_bf16(__nv_bfloat16* dst, const float* v, int n) {
     uint4* d = reinterpret_cast<uint4*>(dst);
@@ -450,7 +435,6 @@ __global__ void __launch_bounds__(kTile * NW, Grouped ? 3 : 1) mlp_forward_kerne
                 // barrier before the next chain orders every thread's TMEM reads
                 // before that chain's writes.
                 uint4* xrow = reinterpret_cast<uint4*>(A.X + size_t(row) * kXCols + xoff(l + 1));
-                uint64_t mbits = 0;
                 #pragma unroll
                 for (int k = 0; k < O; k += 8) {
                     const uint4 q = make_uint4(tc::pack_bf16_relu(out[k], out[k + 1]),
@@ -458,12 +442,8 @@ __global__ void __launch_bounds__(kTile * NW, Grouped ? 3 : 1) mlp_forward_kerne
                                                tc::pack_bf16_relu(out[k + 4], out[k + 5]),
                                                tc::pack_bf16_relu(out[k + 6], out[k + 7]));
                     *reinterpret_cast<uint4*>(act + tc::tile_offset(t, k, kTile)) = q;
-                    if (Train && valid) {
-                        xrow[k / 8] = q;
-                        mbits |= uint64_t(positive_bf16x8(q)) << k;
-                    }
+                    if (Train && valid) xrow[k / 8] = q;
                 }
-                if (Train && valid) A.mask[size_t(row) * (kLayers - 1) + l] = mbits;
             }
         }
         if (valid) {
@@ -516,7 +496,7 @@ __global__ void __launch_bounds__(kTile * NW, Grouped ? 3 : 1) mlp_forward_kerne
 struct BwdArgs {
     MlpView V;
     uint32_t count;
-    const uint64_t* mask;         // [batch][kLayers - 1], ReLU masks of X_1 .. X_4 (from the forward)
+    const __nv_bfloat16* X;       // [batch][kXCols]
     __nv_bfloat16* dZ;            // [batch][kZCols]; the output layer's block is an input
 };
 
@@ -569,9 +549,14 @@ __global__ void __launch_bounds__(kTile * NW, 1) mlp_backward_kernel(BwdArgs A) 
                 tc::fence_after_sync();
                 mma_chain(tmem, act_addr, wt_addr + 2 * hoff(l), O, I, bar);
             }
-            // X_l (the input of layer l >= 1) is ReLU(Z_{l-1}): its mask (written by
-            // the forward, one bit per column) gates dZ_{l-1}; fetched while the chain runs
-            const uint64_t mk = valid ? A.mask[size_t(row) * (kLayers - 1) + (l - 1)] : 0ull;
+            // X_l (the input of layer l >= 1) is ReLU(Z_{l-1}): its mask gates dZ_{l-1};
+            // the row is fetched (packed) while the chain runs
+            uint4 xq[kHid / 8];
+            {
+                const uint4* src = reinterpret_cast<const uint4*>(A.X + size_t(row) * kXCols + xoff(l));
+                #pragma unroll
+                for (int k = 0; k < kHid / 8; ++k) xq[k] = valid ? src[k] : make_uint4(0, 0, 0, 0);
+            }
             if (t == 0) ok = tc::mbar_wait(bar, phase) && ok;
             wg_sync();
             tc::fence_after_sync();
@@ -584,12 +569,14 @@ __global__ void __launch_bounds__(kTile * NW, 1) mlp_backward_kernel(BwdArgs A) 
                 tc::tmem_ld32_wait(trow + uint32_t(h * 32), dx);
                 #pragma unroll
                 for (int c = 0; c < 4; ++c) {
-                    const uint32_t mb = uint32_t(mk >> (h * 32 + c * 8)) & 0xFFu;
+                    const uint4 xw = xq[h * 4 + c];
+                    const uint32_t w[4] = {xw.x, xw.y, xw.z, xw.w};
                     uint32_t q[4];
                     #pragma unroll
                     for (int j = 0; j < 4; ++j) {
-                        const float d0 = (mb >> (2 * j)) & 1u ? dx[c * 8 + 2 * j] : 0.0f;
-                        const float d1 = (mb >> (2 * j + 1)) & 1u ? dx[c * 8 + 2 * j + 1] : 0.0f;
+                        const float x0 = __uint_as_float(w[j] << 16), x1 = __uint_as_float(w[j] & 0xFFFF0000u);
+                        const float d0 = x0 > 0.0f ? dx[c * 8 + 2 * j] : 0.0f;
+                        const float d1 = x1 > 0.0f ? dx[c * 8 + 2 * j + 1] : 0.0f;
                         q[j] = tc::pack_bf16(d0, d1);
                     }
                     const uint4 v = make_uint4(q[0], q[1], q[2], q[3]);
@@ -877,7 +864,6 @@ struct rr_mlp_state {
     double* wnorm = nullptr;
     __nv_bfloat16* X = nullptr;
     __nv_bfloat16* dZ = nullptr;
-    uint64_t* mask = nullptr;
     float* loss_partial = nullptr;
     float* wpartial = nullptr;    // per wgrad CTA: kParams FP32
     double* wn_partial = nullptr; // per weight-norm block
@@ -930,7 +916,6 @@ rr_status rr_mlp_guide_init(rr_ctx* ctx, rr_guide* g) {
     if ((st = al(reinterpret_cast<void**>(&M.wnorm), 16)) != RR_OK) return st;
     if ((st = al(reinterpret_cast<void**>(&M.X), size_t(B) * kXCols * 2)) != RR_OK) return st;
     if ((st = al(reinterpret_cast<void**>(&M.dZ), size_t(B) * kZCols * 2)) != RR_OK) return st;
-    if ((st = al(reinterpret_cast<void**>(&M.mask), size_t(B) * (kLayers - 1) * 8)) != RR_OK) return st;
     M.grid = 3 * ctx->sm_count;
     if ((st = al(reinterpret_cast<void**>(&M.loss_partial), size_t(M.grid) * 4)) != RR_OK) return st;
     M.wg_grid = ctx->sm_count;
@@ -1060,7 +1045,6 @@ rr_status rr_mlp_guide_train(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t 
     A.wnorm = M.wnorm;
     A.X = M.X;
     A.dZ = M.dZ;
-    A.mask = M.mask;
     A.loss_partial = M.loss_partial;
     const uint32_t tiles = (B + kTile - 1) / kTile;
     const int fgrid = int(std::min<uint32_t>((tiles + kTrainWG - 1) / kTrainWG, uint32_t(ctx->sm_count)));
@@ -1070,7 +1054,7 @@ rr_status rr_mlp_guide_train(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t 
     BwdArgs Bw{};
     Bw.V = A.V;
     Bw.count = B;
-    Bw.mask = M.mask;
+    Bw.X = M.X;
     Bw.dZ = M.dZ;
     const int bgrid = int(std::min<uint32_t>((tiles + kBwdWG - 1) / kBwdWG, uint32_t(ctx->sm_count)));
     mlp_backward_kernel<kBwdWG><<<bgrid, kTile * kBwdWG, bwd_smem(kBwdWG), stream>>>(Bw);

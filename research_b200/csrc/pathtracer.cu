@@ -487,6 +487,11 @@ extern "C" rr_status rr_pathtracer_set_overlap(rr_ctx* ctx, int enable) {
     return RR_OK;
 }
 
+extern "C" int rr_pathtracer_variant_width(int v) {
+    if (v < 0 || v >= RR_PT_VARIANT_COUNT) return 0;
+    return (v == 3 || v == 4 || v == 6) ? 4 : 2;   // the Wide variants of the kernel tables (rr_wavefront.cuh)
+}
+
 extern "C" rr_status rr_pathtracer_set_variants(rr_ctx* ctx, int ev, int sv) {
     if (!ctx) return RR_ERR_INVALID_ARGUMENT;
     if (ev < 0 || ev >= RR_PT_VARIANT_COUNT || sv < 0 || sv >= RR_PT_VARIANT_COUNT)

@@ -8,6 +8,7 @@
 namespace rr {
 struct BvhBuild {
     std::vector<float4> nodes;     // 4 float4 per node (layout in rr_trace.cuh)
+    std::vector<float4> nodes4;    // the same tree collapsed 4-wide: 8 float4 per node (layout in rr_trace.cuh)
     std::vector<uint32_t> order;   // leaf order -> flattened triangle id
     uint32_t max_depth = 0;
 };

@@ -125,17 +125,19 @@ struct WarpPool {
 // in the scene `table[index]` (the lane binds that scene's node and triangle
 // arrays when it loads the ray); otherwise every ray is traced in `s`. Rays
 // start at t = tmin (the path tracer's 0.001).
-template <int SmemS> struct QueueStackOf { using type = SplitStack<SmemS, kBlock>; };
-template <> struct QueueStackOf<0> { using type = LocalStack; };
+template <int SmemS, int N> struct QueueStackOf { using type = SplitStack<SmemS, kBlock, N>; };
+template <int N> struct QueueStackOf<0, N> { using type = LocalStackN<N>; };
 
 // SmemS > 0: the bottom SmemS stack entries of every thread in shared memory.
-template <bool AnyHit, bool Count, bool Refill, bool Multi, bool Postpone = false, int SmemS = 0, class Load,
-          class Finish>
+// Wide: the 4-wide tree (trace_step4).
+template <bool AnyHit, bool Count, bool Refill, bool Multi, bool Postpone = false, int SmemS = 0, bool Wide = false,
+          class Load, class Finish>
 __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene* __restrict__ table, uint32_t count,
                                                uint32_t* cursor, unsigned long long* work_out, Load load,
                                                Finish finish, float tmin = 0.001f) {
     TraceWork tw;
-    typename QueueStackOf<SmemS>::type stack;   // (node, near distance) entries
+    static_assert(!(Wide && Postpone), "postponed leaves are a binary-tree schedule");
+    typename QueueStackOf<SmemS, Wide ? kStackSize4 : kStackSize>::type stack;   // (node, near distance) entries
     if constexpr (SmemS > 0) {
         __shared__ int2 stack_smem[SmemS * kBlock];
         stack.col = stack_smem + threadIdx.x;
@@ -146,11 +148,14 @@ __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene
             ls.nodes = table[sid].nodes;
             ls.tris = table[sid].tris;
             ls.num_nodes = table[sid].num_nodes;
+            ls.nodes4 = table[sid].nodes4;
+            ls.num_nodes4 = table[sid].num_nodes4;
         }
     };
     auto step = [&](const Ray& r, HitRec& h, TravState& st) -> bool {
-        if constexpr (Multi) return trace_step<AnyHit, Count, Postpone>(ls, r, tmin, h, st, stack, &tw);
-        else return trace_step<AnyHit, Count, Postpone>(s, r, tmin, h, st, stack, &tw);
+        const DevScene& sc = Multi ? ls : s;
+        if constexpr (Wide) return trace_step4<AnyHit, Count>(sc, r, tmin, h, st, stack, &tw);
+        else return trace_step<AnyHit, Count, Postpone>(sc, r, tmin, h, st, stack, &tw);
     };
     if constexpr (!Refill) {
         while (true) {
@@ -200,13 +205,13 @@ __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene
     if (Count) flush_work(tw, work_out);
 }
 
-template <bool Count, bool Refill, int MinBlocks, bool Postpone = false, int SmemS = 0>
+template <bool Count, bool Refill, int MinBlocks, bool Postpone = false, int SmemS = 0, bool Wide = false>
 __global__ void __launch_bounds__(kBlock, MinBlocks) extend_kernel(DevScene s, const float4* __restrict__ qa,
                                                                    const float4* __restrict__ qb,
                                                                    float4* __restrict__ hits,
                                                                    const uint32_t* count_ptr, uint32_t* cursor,
                                                                    unsigned long long* work_out) {
-    traverse_queue<false, Count, Refill, false, Postpone, SmemS>(
+    traverse_queue<false, Count, Refill, false, Postpone, SmemS, Wide>(
         s, nullptr, *count_ptr, cursor, work_out,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = qa[i], b = qb[i];
@@ -221,14 +226,14 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) extend_kernel(DevScene s, c
 }
 
 // Any-hit shadow rays; unoccluded NEE contributions are added to the image.
-template <bool Count, bool Refill, int MinBlocks, bool Postpone = false, int SmemS = 0>
+template <bool Count, bool Refill, int MinBlocks, bool Postpone = false, int SmemS = 0, bool Wide = false>
 __global__ void __launch_bounds__(kBlock, MinBlocks) shadow_kernel(DevScene s, const float4* __restrict__ sa,
                                                                    const float4* __restrict__ sb,
                                                                    const float4* __restrict__ sc,
                                                                    float4* __restrict__ out,
                                                                    const uint32_t* count_ptr, uint32_t* cursor,
                                                                    unsigned long long* work_out) {
-    traverse_queue<true, Count, Refill, false, Postpone, SmemS>(
+    traverse_queue<true, Count, Refill, false, Postpone, SmemS, Wide>(
         s, nullptr, *count_ptr, cursor, work_out,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = sa[i], b = sb[i];
@@ -297,7 +302,7 @@ __global__ void __launch_bounds__(kBlock) raygen_batch_kernel(const BatchEntry* 
     qc[slot] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(sid));
 }
 
-template <bool Count, bool Refill, int MinBlocks, bool Postpone = false, int SmemS = 0>
+template <bool Count, bool Refill, int MinBlocks, bool Postpone = false, int SmemS = 0, bool Wide = false>
 __global__ void __launch_bounds__(kBlock, MinBlocks) extend_batch_kernel(const DevScene* __restrict__ table,
                                                                          const float4* __restrict__ qa,
                                                                          const float4* __restrict__ qb,
@@ -306,7 +311,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) extend_batch_kernel(const D
                                                                          const uint32_t* count_ptr, uint32_t* cursor,
                                                                          unsigned long long* work_out) {
     const DevScene none{};
-    traverse_queue<false, Count, Refill, true, Postpone, SmemS>(
+    traverse_queue<false, Count, Refill, true, Postpone, SmemS, Wide>(
         none, table, *count_ptr, cursor, work_out,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = qa[i], b = qb[i];
@@ -320,7 +325,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) extend_batch_kernel(const D
         });
 }
 
-template <bool Count, bool Refill, int MinBlocks, bool Postpone = false, int SmemS = 0>
+template <bool Count, bool Refill, int MinBlocks, bool Postpone = false, int SmemS = 0, bool Wide = false>
 __global__ void __launch_bounds__(kBlock, MinBlocks) shadow_batch_kernel(const DevScene* __restrict__ table,
                                                                          float4* const* __restrict__ outs,
                                                                          const float4* __restrict__ sa,
@@ -329,7 +334,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) shadow_batch_kernel(const D
                                                                          const uint32_t* count_ptr, uint32_t* cursor,
                                                                          unsigned long long* work_out) {
     const DevScene none{};
-    traverse_queue<true, Count, Refill, true, Postpone, SmemS>(
+    traverse_queue<true, Count, Refill, true, Postpone, SmemS, Wide>(
         none, table, *count_ptr, cursor, work_out,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = sa[i], b = sb[i];
@@ -361,10 +366,10 @@ BatchQueueKernel extend_batch_variant(int v) {
     switch (v) {
     case 1: return extend_batch_kernel<Count, false, 5>;
     case 2: return extend_batch_kernel<Count, false, 1, false, 8>;
-    case 3: return extend_batch_kernel<Count, true, 1>;
-    case 4: return extend_batch_kernel<Count, true, 4>;
+    case 3: return extend_batch_kernel<Count, false, 1, false, 0, true>;
+    case 4: return extend_batch_kernel<Count, false, 1, false, 8, true>;
     case 5: return extend_batch_kernel<Count, false, 5, false, 8>;
-    case 6: return extend_batch_kernel<Count, false, 1, true>;
+    case 6: return extend_batch_kernel<Count, false, 3, false, 8, true>;
     case 7: return extend_batch_kernel<Count, false, 4, true>;
     default: return extend_batch_kernel<Count, false, 4>;
     }
@@ -374,10 +379,10 @@ BatchShadowKernel shadow_batch_variant(int v) {
     switch (v) {
     case 1: return shadow_batch_kernel<Count, false, 5>;
     case 2: return shadow_batch_kernel<Count, false, 1, false, 8>;
-    case 3: return shadow_batch_kernel<Count, true, 1>;
-    case 4: return shadow_batch_kernel<Count, true, 4>;
+    case 3: return shadow_batch_kernel<Count, false, 1, false, 0, true>;
+    case 4: return shadow_batch_kernel<Count, false, 1, false, 8, true>;
     case 5: return shadow_batch_kernel<Count, false, 5, false, 8>;
-    case 6: return shadow_batch_kernel<Count, false, 1, true>;
+    case 6: return shadow_batch_kernel<Count, false, 3, false, 8, true>;
     case 7: return shadow_batch_kernel<Count, false, 4, true>;
     default: return shadow_batch_kernel<Count, false, 1>;
     }
@@ -393,10 +398,10 @@ QueueKernel extend_variant(int v) {
     switch (v) {
     case 1: return extend_kernel<Count, false, 5>;
     case 2: return extend_kernel<Count, false, 1, false, 8>;
-    case 3: return extend_kernel<Count, true, 1>;
-    case 4: return extend_kernel<Count, true, 4>;
+    case 3: return extend_kernel<Count, false, 1, false, 0, true>;
+    case 4: return extend_kernel<Count, false, 1, false, 8, true>;
     case 5: return extend_kernel<Count, false, 5, false, 8>;
-    case 6: return extend_kernel<Count, false, 1, true>;
+    case 6: return extend_kernel<Count, false, 3, false, 8, true>;
     case 7: return extend_kernel<Count, false, 4, true>;
     default: return extend_kernel<Count, false, 1>;
     }
@@ -406,10 +411,10 @@ ShadowKernel shadow_variant(int v) {
     switch (v) {
     case 1: return shadow_kernel<Count, false, 5>;
     case 2: return shadow_kernel<Count, false, 1, false, 8>;
-    case 3: return shadow_kernel<Count, true, 1>;
-    case 4: return shadow_kernel<Count, true, 4>;
+    case 3: return shadow_kernel<Count, false, 1, false, 0, true>;
+    case 4: return shadow_kernel<Count, false, 1, false, 8, true>;
     case 5: return shadow_kernel<Count, false, 5, false, 8>;
-    case 6: return shadow_kernel<Count, false, 1, true>;
+    case 6: return shadow_kernel<Count, false, 3, false, 8, true>;
     case 7: return shadow_kernel<Count, false, 4, true>;
     default: return shadow_kernel<Count, false, 1>;
     }

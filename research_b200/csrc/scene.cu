@@ -242,6 +242,7 @@ rr_status rr_scene_create(rr_ctx* ctx, const rr_scene_desc* d, rr_scene** out) {
     if ((st = upload((src), (bytes), &p)) != RR_OK) { rr_scene_destroy(s); return st; } \
     s->dev.field = reinterpret_cast<type>(p);
     RR_UP(bvh.nodes.data(), bvh.nodes.size() * sizeof(float4), nodes, const float4*);
+    RR_UP(bvh.nodes4.data(), bvh.nodes4.size() * sizeof(float4), nodes4, const float4*);
     RR_UP(trirec.data(), trirec.size() * sizeof(float4), tris, const float4*);
     RR_UP(d->vertices, size_t(d->vertex_count) * sizeof(GpuVertex), vertices, const float4*);
     RR_UP(d->indices, size_t(d->index_count) * 4, indices, const uint32_t*);
@@ -259,10 +260,12 @@ rr_status rr_scene_create(rr_ctx* ctx, const rr_scene_desc* d, rr_scene** out) {
     s->dev.num_tris = ntri;
     s->dev.num_materials = d->material_count;
     s->dev.num_nodes = uint32_t(bvh.nodes.size() / 4);
+    s->dev.num_nodes4 = uint32_t(bvh.nodes4.size() / 8);
     auto t2 = std::chrono::steady_clock::now();
     s->stats.triangle_count = ntri;
     s->stats.bvh_node_count = uint32_t(bvh.nodes.size() / 4);
     s->stats.bvh_max_depth = bvh.max_depth;
+    s->stats.bvh4_node_count = uint32_t(bvh.nodes4.size() / 8);
     s->stats.light_count = d->light_count;
     s->stats.build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     s->stats.upload_ms = std::chrono::duration<double, std::milli>(t2 - t1).count();

@@ -50,7 +50,7 @@ class SceneDesc(C.Structure):
 class SceneStats(C.Structure):
     _fields_ = [("triangle_count", C.c_uint32), ("bvh_node_count", C.c_uint32), ("bvh_max_depth", C.c_uint32),
                 ("light_count", C.c_uint32), ("build_ms", C.c_double), ("upload_ms", C.c_double),
-                ("device_bytes", C.c_uint64)]
+                ("device_bytes", C.c_uint64), ("bvh4_node_count", C.c_uint32), ("_pad", C.c_uint32)]
 
 
 class PtStats(C.Structure):
@@ -70,6 +70,7 @@ PT_FLAG_TIME_STAGES = 2
 PT_FLAG_GRAPH = 4
 PT_FLAG_EMITTERS = 8
 PT_VARIANT_COUNT = 8
+TRACE_ANY_HIT, TRACE_WIDE = 1, 2   # rr_trace_counted flags
 BATCH_WAVEFRONT = 0
 BATCH_PER_SCENE = 1
 
@@ -261,6 +262,8 @@ _SIGNATURES = {
     "rr_host_scene_instanced": (I, [C.POINTER(InstancedParams), C.POINTER(P)]),
     "rr_trace_counted": (I, [P, P, P, P, C.c_float, C.c_float, U32, I, P, P, P, P]),
     "rr_scene_copy_bvh": (I, [P, P, P, P]),
+    "rr_scene_copy_bvh4": (I, [P, P, P]),
+    "rr_pathtracer_variant_width": (I, [I]),
     "rr_tc_wait_selftest": (I, [P, U32, P]),
     "rr_host_scene_gltf": (I, [C.c_char_p, C.POINTER(P), C.c_char_p, C.c_size_t]),
     "rr_host_scene_desc": (I, [P, C.POINTER(SceneDesc)]),

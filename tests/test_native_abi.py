@@ -45,6 +45,15 @@ def test_struct_sizes_match_headers(rr):
     assert C.sizeof(rr.GpuCameraData) == 304
     assert C.sizeof(rr.PtParams) == 16 and C.sizeof(rr.AccParams) == 16
     assert C.sizeof(rr.DIParams) == 32 and C.sizeof(rr.AtrousParams) == 32 and C.sizeof(rr.GuidingParams) == 32
+    assert C.sizeof(rr.SceneStats) == 48
+
+
+def test_traversal_variant_widths(rr):
+    """Variants 3, 4 and 6 walk the 4-wide tree (128-byte nodes), the others
+    the binary one; out-of-range variants report width 0."""
+    L = rr.lib()
+    assert [L.rr_pathtracer_variant_width(v) for v in range(rr.PT_VARIANT_COUNT)] == [2, 2, 2, 4, 4, 2, 4, 2]
+    assert L.rr_pathtracer_variant_width(-1) == 0 and L.rr_pathtracer_variant_width(rr.PT_VARIANT_COUNT) == 0
 
 
 def test_cornell_factory_matches_reference_restatement(rr):
