@@ -345,7 +345,7 @@ class Frame:
         return {n: v / cnt for n, v in tot.items()}
 
 
-def parity_check(rr, O, torch, ctx, scene, oscene, args, frame_index, seed_base, concurrent):
+def parity_check(rr, O, torch, ctx, scene, oscene, args, frame_index, seed_base, concurrent, pt_mode=0, di_flags=0):
     """The benchmarked frame against the oracle, outside the timed region:
     two frames rendered exactly as the timed loop renders them (fresh
     reservoirs; the second frame uses the first timed frame's seeds). The
@@ -353,7 +353,8 @@ def parity_check(rr, O, torch, ctx, scene, oscene, args, frame_index, seed_base,
     256x256 centre crop (the oracle traces that region of the same camera
     with the same frame seeds); the ReSTIR DI G-buffer and output and the
     A-trous output on the whole 1920x1080 frame. Tolerance zero: every
-    compared float must have the same bits."""
+    compared float must have the same bits. pt_mode / di_flags: the
+    emitter-sampling frame's RR_PT_FLAG_EMITTERS / RR_DI_FLAG_EMITTERS."""
     import numpy as np
     W, H = args.width, args.height
     spp = CFG["spp"]
@@ -362,6 +363,7 @@ def parity_check(rr, O, torch, ctx, scene, oscene, args, frame_index, seed_base,
     t0 = time.perf_counter()
     pf = Frame(rr, torch, ctx, scene, W, H)
     pf.concurrent = concurrent
+    pf.pt_mode, pf.di_flags = pt_mode, di_flags
     pf.frame = frame_index - 1
     stream = torch.cuda.current_stream().cuda_stream
     frames = [pf.frame, pf.frame + 1]
@@ -381,7 +383,7 @@ def parity_check(rr, O, torch, ctx, scene, oscene, args, frame_index, seed_base,
     nth = O.threads()
     for j, f in enumerate(frames):
         img, _ = O.pathtrace(oscene, cam, seed_base + f * spp, CFG["max_bounces"], spp,
-                             region=(x0, y0, cw, ch), nthreads=nth)
+                             region=(x0, y0, cw, ch), nthreads=nth, flags=O.PT_EMITTERS if pt_mode else 0)
         for k in range(spp):
             O.accumulate(np.ascontiguousarray(img[k]), o_acc, 1 if (j == 0 and k == 0) else 0, j * spp + k)
         mism[f"pathtracer_frame{j}"] = int((img.view(np.uint32) != rad_crops[j].view(np.uint32)).any(-1).sum())
@@ -391,7 +393,7 @@ def parity_check(rr, O, torch, ctx, scene, oscene, args, frame_index, seed_base,
     res = [z(), z()]
     for j, f in enumerate(frames):
         dp = O.di_params(seed_base + f, CFG["di_candidates"], 1, 1, CFG["di_neighbors"], CFG["di_radius"],
-                         CFG["m_cap_factor"])
+                         CFG["m_cap_factor"], flags=O.DI_EMITTERS if di_flags else 0)
         cur, prev = res[f & 1], res[(f & 1) ^ 1]
         O.restir_di_initial(oscene, cam, dp, gpos, gnrm, cur, nth)
         O.restir_di_temporal(oscene, cam, dp, gpos, gnrm, cur, prev, nth)
@@ -601,6 +603,7 @@ def run_ours(args, ws, rank, local):
         fe.pt_mode, fe.di_flags = rr.PT_FLAG_EMITTERS, rr.DI_FLAG_EMITTERS
         for _ in range(args.warmup):
             fe.step(stream, seed_base=seed_base)
+        first_timed_e = fe.frame
         barrier(ws)
         torch.cuda.synchronize()
         g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -615,11 +618,20 @@ def run_ours(args, ws, rank, local):
             fe.step(stream, pt_flags=rr.PT_FLAG_TIME_STAGES, seed_base=seed_base, stage_timing=True)
         ctx.check(rr.lib().rr_pathtracer_stats(ctx.handle, C.byref(st), 1))
         em_stage = fe.stage_ms()
+        em_parity = None
+        if rank == 0 and not args.no_parity:
+            sys.path.insert(0, str(ROOT / "oracle"))
+            import oracle as O
+            osc_e = O.OracleScene(hs_e.arrays, use_bvh=True)
+            em_parity = parity_check(rr, O, torch, ctx, scene_e, osc_e, args, first_timed_e, seed_base, fr.concurrent,
+                                     pt_mode=rr.PT_FLAG_EMITTERS, di_flags=rr.DI_FLAG_EMITTERS)
+            osc_e.close()
         emitter_mode = {"value": replicas.job_throughput(paths_per_step, ws, em_ms), "unit": UNIT,
                         "ms_per_step": em_ms,
                         "workload": "the same frame on the same scene without its centroid point lights: the path "
                                     "tracer's NEE and ReSTIR DI's candidates sample the 4096 emissive triangles "
                                     "(RR_PT_FLAG_EMITTERS, RR_DI_FLAG_EMITTERS)",
+                        "parity": em_parity,
                         "stages_ms": {**{k: round(v, 4) for k, v in em_stage.items()},
                                       "pt_extend": round(st.ms_extend / args.steps, 4),
                                       "pt_shade": round(st.ms_shade / args.steps, 4),

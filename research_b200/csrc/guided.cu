@@ -23,8 +23,7 @@
 #include "rr_guide.h"
 #include "rr_batch.h"
 
-#include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_scan.cuh>
+#include "rr_cellsort.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -531,22 +530,23 @@ __global__ void __launch_bounds__(kBlock) resolve_batch_kernel(const GuideEntry*
 }
 
 // ── grid guide update ──────────────────────────────────────────────────────
-__global__ void __launch_bounds__(256) grid_keys_kernel(GridView g, GuideSamples S, uint32_t n,
-                                                        unsigned long long* keys, uint32_t* vals) {
+// Sample i's cell (the sort key) and index (the sorted value).
+__global__ void __launch_bounds__(256) grid_keys_kernel(GridView g, GuideSamples S, uint32_t n, uint32_t* keys,
+                                                        uint32_t* vals) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float4 a = S.s0[i], b = S.s1[i];
-    keys[i] = (static_cast<unsigned long long>(grid_cell(g, xyz(a))) << 32) | __float_as_uint(b.w);
+    keys[i] = grid_cell(g, xyz(S.s0[i]));
     vals[i] = i;
 }
 
-__global__ void __launch_bounds__(256) grid_ranges_kernel(const unsigned long long* keys, uint32_t n,
-                                                          uint32_t* start, uint32_t* end) {
+// Each cell's range [start, end) in the cell-sorted sample order.
+__global__ void __launch_bounds__(256) grid_ranges_kernel(const uint32_t* keys, uint32_t n, uint32_t* start,
+                                                          uint32_t* end) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const uint32_t c = uint32_t(keys[i] >> 32);
-    if (i == 0 || uint32_t(keys[i - 1] >> 32) != c) start[c] = i;
-    if (i + 1 == n || uint32_t(keys[i + 1] >> 32) != c) end[c] = i + 1;
+    const uint32_t c = keys[i];
+    if (i == 0 || keys[i - 1] != c) start[c] = i;
+    if (i + 1 == n || keys[i + 1] != c) end[c] = i + 1;
 }
 
 // The EM update is one batch E-step per frame: every sample's responsibilities
@@ -790,15 +790,17 @@ extern "C" rr_status rr_guide_create(rr_ctx* ctx, const rr_guide_desc* d, rr_gui
         g->chunk_cell = static_cast<uint32_t*>(p);
         if ((st = guide_alloc(ctx, g, &p, g->chunk_capacity * kEmStats * sizeof(double))) != RR_OK) return fail(st);
         g->chunk_partial = static_cast<double*>(p);
-        size_t tmp = 0, scan_tmp = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, tmp, g->keys_in, g->keys_out, g->vals_in, g->vals_out, int(cap), 0, 64);
-        cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp, g->chunk_cnt, g->chunk_off, int(cells));
-        tmp = std::max(tmp, scan_tmp);
-        if ((st = guide_alloc(ctx, g, &p, tmp)) != RR_OK) return fail(st);
+        // the cell sort's per-(digit, tile) counts
+        const size_t hist = size_t(kSortBins) * ((cap + kSortTile - 1) / kSortTile);
+        if ((st = guide_alloc(ctx, g, &p, hist * sizeof(uint32_t))) != RR_OK) return fail(st);
         g->sort_tmp = p;
-        g->sort_tmp_bytes = tmp;
-        g->key_bits = 32;
-        while ((size_t(1) << (g->key_bits - 32)) < cells) ++g->key_bits;
+        g->sort_tmp_bytes = hist * sizeof(uint32_t);
+        if (std::max<size_t>(hist, cells) > size_t(kScanChunk) * kScanThreads) return fail(RR_ERR_UNSUPPORTED);
+        const size_t sums = std::max<size_t>(hist, cells) / kScanChunk + 1;
+        if ((st = guide_alloc(ctx, g, &p, sums * sizeof(uint32_t))) != RR_OK) return fail(st);
+        g->scan_sums = static_cast<uint32_t*>(p);
+        g->key_bits = 1;
+        while ((size_t(1) << g->key_bits) < cells) ++g->key_bits;
     } else {
         if ((st = rr_mlp_guide_init(ctx, g)) != RR_OK) return fail(st);
     }
@@ -969,26 +971,38 @@ static rr_status guide_update_n(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream
         RR_TRY_CUDA(ctx, cudaMemsetAsync(g->cell_end, 0, size_t(v.cells) * 4, stream));
         RR_TRY_CUDA(ctx, cudaMemsetAsync(g->samples.count + 1, 0, sizeof(uint32_t), stream));
         if (n > 0) {
-            grid_keys_kernel<<<(n + 255) / 256, 256, 0, stream>>>(v, g->samples, n, g->keys_in, g->vals_in);
+            uint32_t* kin = reinterpret_cast<uint32_t*>(g->keys_in);
+            uint32_t* kout = reinterpret_cast<uint32_t*>(g->keys_out);
+            uint32_t* vin = g->vals_in;
+            uint32_t* vout = g->vals_out;
+            grid_keys_kernel<<<(n + 255) / 256, 256, 0, stream>>>(v, g->samples, n, kin, vin);
             RR_CHECK_LAUNCH(ctx);
-            size_t tmp = g->sort_tmp_bytes;
-            RR_TRY_CUDA(ctx, cub::DeviceRadixSort::SortPairs(g->sort_tmp, tmp, g->keys_in, g->keys_out, g->vals_in,
-                                                             g->vals_out, int(n), 0, g->key_bits, stream));
-            grid_ranges_kernel<<<(n + 255) / 256, 256, 0, stream>>>(g->keys_out, n, g->cell_start, g->cell_end);
+            const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
+            uint32_t* hist = static_cast<uint32_t*>(g->sort_tmp);
+            for (int shift = 0; shift < g->key_bits; shift += 8) {
+                sort_hist_kernel<<<tiles, kSortThreads, 0, stream>>>(kin, n, shift, tiles, hist);
+                scan_exclusive(hist, hist, uint32_t(kSortBins) * tiles, g->scan_sums, stream);
+                sort_scatter_kernel<<<tiles, kSortThreads, 0, stream>>>(kin, vin, kout, vout, n, shift, tiles, hist);
+                RR_CHECK_LAUNCH(ctx);
+                std::swap(kin, kout);
+                std::swap(vin, vout);
+                ctx->launches += 5;
+            }
+            g->sorted_vals = vin;   // after the last pass's swap, the sorted arrays are the "in" pair
+            grid_ranges_kernel<<<(n + 255) / 256, 256, 0, stream>>>(kin, n, g->cell_start, g->cell_end);
             RR_CHECK_LAUNCH(ctx);
         }
         const uint32_t cb = (v.cells + 255) / 256;
         grid_chunk_count_kernel<<<cb, 256, 0, stream>>>(g->cell_start, g->cell_end, v.cells, g->chunk_cnt);
         RR_CHECK_LAUNCH(ctx);
-        size_t tmp = g->sort_tmp_bytes;
-        RR_TRY_CUDA(ctx, cub::DeviceScan::ExclusiveSum(g->sort_tmp, tmp, g->chunk_cnt, g->chunk_off, int(v.cells),
-                                                       stream));
+        scan_exclusive(g->chunk_cnt, g->chunk_off, v.cells, g->scan_sums, stream);
+        RR_CHECK_LAUNCH(ctx);
         grid_chunk_map_kernel<<<cb, 256, 0, stream>>>(g->chunk_cnt, g->chunk_off, v.cells, g->chunk_cell);
         RR_CHECK_LAUNCH(ctx);
         if (n > 0) {
             const size_t warps = std::min<size_t>(v.cells, n) + n / kEmChunk + 1;
             grid_chunk_kernel<<<unsigned((warps * 32 + 127) / 128), 128, 0, stream>>>(
-                v, g->samples, g->vals_out, g->cell_start, g->cell_end, g->chunk_cnt, g->chunk_off, g->chunk_cell,
+                v, g->samples, g->sorted_vals, g->cell_start, g->cell_end, g->chunk_cnt, g->chunk_off, g->chunk_cell,
                 g->chunk_partial);
             RR_CHECK_LAUNCH(ctx);
         }
@@ -996,7 +1010,7 @@ static rr_status guide_update_n(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream
                                                                    g->stats64, v.lobes, v.weights, g->desc.decay,
                                                                    g->samples.count + 1);
         RR_CHECK_LAUNCH(ctx);
-        ctx->launches += 8;
+        ctx->launches += n > 0 ? 9 : 6;   // besides the sort passes counted above
     } else {
         rr_status st = rr_mlp_guide_train(ctx, g, n, stream);
         if (st != RR_OK) return st;

@@ -82,9 +82,11 @@ struct rr_guide {
     unsigned long long* keys_out = nullptr;
     uint32_t* vals_in = nullptr;
     uint32_t* vals_out = nullptr;
-    void* sort_tmp = nullptr;       // shared by the key sort and the chunk scan
+    void* sort_tmp = nullptr;       // the cell sort's per-(digit, tile) counts (rr_cellsort.cuh)
     size_t sort_tmp_bytes = 0;
-    int key_bits = 64;              // sorted key bits: 32 (vertex id) + cell index bits
+    int key_bits = 32;              // sorted key bits: the cell index's
+    uint32_t* sorted_vals = nullptr;  // vals_in or vals_out: the cell-sorted sample indices of the last update
+    uint32_t* scan_sums = nullptr;    // chunk sums of the scans (rr_cellsort.cuh)
     uint32_t* chunk_cnt = nullptr;  // per cell: EM chunks of its samples
     uint32_t* chunk_off = nullptr;  // per cell: exclusive scan of chunk_cnt
     uint32_t* chunk_cell = nullptr; // per chunk: its cell
