@@ -82,7 +82,7 @@ __host__ __device__ constexpr int fwd_bar(int nw) { return fwd_act(nw); }
 __host__ __device__ constexpr int fwd_smem(int nw) { return fwd_bar(nw) + 64; }
 __host__ __device__ constexpr uint32_t tmem_cols(int nw) { return nw <= 2 ? 128u : (nw <= 4 ? 256u : 512u); }
 constexpr int kInferWG = 5;   // inference: 640 threads, 96 registers each, 149 KB of shared memory
-constexpr int kTrainWG = 3;   // training forward: 384 threads
+constexpr int kTrainWG = 3;   // training forward: 384 threads (4 warpgroups at 128 registers measured 120.5 against 116.9 us)
 constexpr int kSmBwdWt = 0;
 constexpr int kSmBwdAct = kSmBwdWt + 2 * kWeightsBf16;
 // backward CTAs: NW warpgroups sharing W^T, one activation tile, mbarrier and
