@@ -23,7 +23,7 @@ __global__ void __launch_bounds__(kBlock, 4) wave_extend_kernel(DevScene s, cons
                                                                 const float4* __restrict__ qb,
                                                                 float4* __restrict__ hits, uint32_t* c0,
                                                                 float tmin) {
-    traverse_queue<false, false, false, false>(
+    traverse_queue<false, false, false>(
         s, nullptr, c0[0], c0 + 1, nullptr,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             r = make_ray(xyz(qa[i]), xyz(qb[i]));
@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(kBlock, 5) wave_shadow_kernel(DevScene s, cons
                                                                 const float4* __restrict__ sb,
                                                                 const float4* __restrict__ sc, float4* sum,
                                                                 uint32_t* c0, float tmin) {
-    traverse_queue<true, false, false, false>(
+    traverse_queue<true, false, false>(
         s, nullptr, c0[2], c0 + 3, nullptr,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 b = sb[i];

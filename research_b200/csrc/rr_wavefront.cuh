@@ -72,54 +72,10 @@ __device__ __forceinline__ void flush_work(const TraceWork& w, unsigned long lon
     if (lane_id() == 0 && (n | t)) { atomicAdd(out, n); atomicAdd(out + 1, t); }
 }
 
-// Warp-cooperative ray pool: hands queue indices [0, count) to idle lanes,
-// taking kChunk indices at a time from the launch's global cursor (one
-// atomic per chunk). All fields are warp-uniform.
-constexpr uint32_t kChunk = 64;
-constexpr uint32_t kRefillLanes = 8;
-
-struct WarpPool {
-    uint32_t next = 0, end = 0;
-    bool exhausted = false;
-    __device__ __forceinline__ bool done() const { return exhausted && next >= end; }
-    // Every lane calls this with the same idle mask; idle lanes get an index
-    // (or kNoIndex when the queue is drained).
-    __device__ __forceinline__ uint32_t refill(uint32_t idle_mask, bool idle, uint32_t count, uint32_t* cursor) {
-        const uint32_t n_idle = __popc(idle_mask);
-        const uint32_t rank = __popc(idle_mask & ((1u << lane_id()) - 1u));
-        const uint32_t avail = end - next;
-        const bool need = avail < n_idle && !exhausted;
-        uint32_t nb = 0;
-        if (need) {
-            if (lane_id() == 0) nb = atomicAdd(cursor, kChunk);
-            nb = __shfl_sync(kFull, nb, 0);
-        }
-        uint32_t idx = kNoIndex;
-        if (idle) {
-            if (rank < avail) idx = next + rank;
-            else if (need) idx = nb + (rank - avail);
-        }
-        if (idx >= count) idx = kNoIndex;
-        if (!need) {
-            next = min(next + n_idle, end);
-        } else if (nb >= count) {
-            exhausted = true;
-            next = end = 0;
-        } else {
-            end = min(nb + kChunk, count);
-            next = min(nb + (n_idle - avail), end);
-        }
-        return idx;
-    }
-};
-
-// Queue traversal, two schedules (chosen per context, see rr_pathtracer_tune):
-//  Refill = false: each warp takes 32 consecutive queue entries (neighbouring
-//    paths after compaction, hence coherent rays) and traces them to the end;
-//  Refill = true: persistent warps; a lane whose ray is finished takes a new
-//    one as soon as kRefillLanes lanes are idle, so warps do not wait for
-//    their slowest ray (less coherence, fewer idle lanes).
-// MinBlocks is the occupancy target handed to the register allocator.
+// Queue traversal: each warp takes 32 consecutive queue entries (neighbouring
+// paths after compaction, hence coherent rays) and traces them to the end,
+// then takes the next 32 (the grid is persistent). MinBlocks is the
+// occupancy target handed to the register allocator.
 // `Finish(i, found, hit)` consumes a finished ray; `Load(i, ray, tmax)` makes
 // one and returns its scene index. Multi: a batch of scenes, each ray traced
 // in the scene `table[index]` (the lane binds that scene's node and triangle
@@ -130,8 +86,8 @@ template <int N> struct QueueStackOf<0, N> { using type = LocalStackN<N>; };
 
 // SmemS > 0: the bottom SmemS stack entries of every thread in shared memory.
 // Wide: the 4-wide tree (trace_step4).
-template <bool AnyHit, bool Count, bool Refill, bool Multi, bool Postpone = false, int SmemS = 0, bool Wide = false,
-          class Load, class Finish>
+template <bool AnyHit, bool Count, bool Multi, bool Postpone = false, int SmemS = 0, bool Wide = false, class Load,
+          class Finish>
 __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene* __restrict__ table, uint32_t count,
                                                uint32_t* cursor, unsigned long long* work_out, Load load,
                                                Finish finish, float tmin = 0.001f) {
@@ -157,61 +113,31 @@ __device__ __forceinline__ void traverse_queue(const DevScene& s, const DevScene
         if constexpr (Wide) return trace_step4<AnyHit, Count>(sc, r, tmin, h, st, stack, &tw);
         else return trace_step<AnyHit, Count, Postpone>(sc, r, tmin, h, st, stack, &tw);
     };
-    if constexpr (!Refill) {
-        while (true) {
-            uint32_t base = 0;
-            if (lane_id() == 0) base = atomicAdd(cursor, 32u);
-            base = __shfl_sync(kFull, base, 0);
-            if (base >= count) break;
-            const uint32_t i = base + lane_id();
-            if (i < count) {
-                Ray r; float tmax;
-                bind(load(i, r, tmax));
-                HitRec h; TravState st;
-                trav_begin(st, h, tmax);
-                while (!step(r, h, st)) {}
-                finish(i, st.found, h);
-            }
-        }
-    } else {
-        WarpPool pool;
-        Ray r;
-        HitRec h;
-        TravState st;
-        uint32_t idx = kNoIndex;
-        bool has = false;
-        while (true) {
-            const uint32_t idle = __ballot_sync(kFull, !has);
-            if (idle && !pool.done() && (idle == kFull || __popc(idle) >= kRefillLanes)) {
-                const uint32_t ni = pool.refill(idle, !has, count, cursor);
-                if (!has && ni != kNoIndex) {
-                    idx = ni;
-                    float tmax;
-                    bind(load(idx, r, tmax));
-                    trav_begin(st, h, tmax);
-                    has = true;
-                }
-            }
-            if (!__any_sync(kFull, has)) {
-                if (pool.done()) break;
-                continue;
-            }
-            if (has && step(r, h, st)) {
-                finish(idx, st.found, h);
-                has = false;
-            }
+    while (true) {
+        uint32_t base = 0;
+        if (lane_id() == 0) base = atomicAdd(cursor, 32u);
+        base = __shfl_sync(kFull, base, 0);
+        if (base >= count) break;
+        const uint32_t i = base + lane_id();
+        if (i < count) {
+            Ray r; float tmax;
+            bind(load(i, r, tmax));
+            HitRec h; TravState st;
+            trav_begin(st, h, tmax);
+            while (!step(r, h, st)) {}
+            finish(i, st.found, h);
         }
     }
     if (Count) flush_work(tw, work_out);
 }
 
-template <bool Count, bool Refill, int MinBlocks, bool Postpone = false, int SmemS = 0, bool Wide = false>
+template <bool Count, int MinBlocks, bool Postpone = false, int SmemS = 0, bool Wide = false>
 __global__ void __launch_bounds__(kBlock, MinBlocks) extend_kernel(DevScene s, const float4* __restrict__ qa,
                                                                    const float4* __restrict__ qb,
                                                                    float4* __restrict__ hits,
                                                                    const uint32_t* count_ptr, uint32_t* cursor,
                                                                    unsigned long long* work_out) {
-    traverse_queue<false, Count, Refill, false, Postpone, SmemS, Wide>(
+    traverse_queue<false, Count, false, Postpone, SmemS, Wide>(
         s, nullptr, *count_ptr, cursor, work_out,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = qa[i], b = qb[i];
@@ -226,14 +152,14 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) extend_kernel(DevScene s, c
 }
 
 // Any-hit shadow rays; unoccluded NEE contributions are added to the image.
-template <bool Count, bool Refill, int MinBlocks, bool Postpone = false, int SmemS = 0, bool Wide = false>
+template <bool Count, int MinBlocks, bool Postpone = false, int SmemS = 0, bool Wide = false>
 __global__ void __launch_bounds__(kBlock, MinBlocks) shadow_kernel(DevScene s, const float4* __restrict__ sa,
                                                                    const float4* __restrict__ sb,
                                                                    const float4* __restrict__ sc,
                                                                    float4* __restrict__ out,
                                                                    const uint32_t* count_ptr, uint32_t* cursor,
                                                                    unsigned long long* work_out) {
-    traverse_queue<true, Count, Refill, false, Postpone, SmemS, Wide>(
+    traverse_queue<true, Count, false, Postpone, SmemS, Wide>(
         s, nullptr, *count_ptr, cursor, work_out,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = sa[i], b = sb[i];
@@ -302,7 +228,7 @@ __global__ void __launch_bounds__(kBlock) raygen_batch_kernel(const BatchEntry* 
     qc[slot] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(sid));
 }
 
-template <bool Count, bool Refill, int MinBlocks, bool Postpone = false, int SmemS = 0, bool Wide = false>
+template <bool Count, int MinBlocks, bool Postpone = false, int SmemS = 0, bool Wide = false>
 __global__ void __launch_bounds__(kBlock, MinBlocks) extend_batch_kernel(const DevScene* __restrict__ table,
                                                                          const float4* __restrict__ qa,
                                                                          const float4* __restrict__ qb,
@@ -311,7 +237,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) extend_batch_kernel(const D
                                                                          const uint32_t* count_ptr, uint32_t* cursor,
                                                                          unsigned long long* work_out) {
     const DevScene none{};
-    traverse_queue<false, Count, Refill, true, Postpone, SmemS, Wide>(
+    traverse_queue<false, Count, true, Postpone, SmemS, Wide>(
         none, table, *count_ptr, cursor, work_out,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = qa[i], b = qb[i];
@@ -325,7 +251,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) extend_batch_kernel(const D
         });
 }
 
-template <bool Count, bool Refill, int MinBlocks, bool Postpone = false, int SmemS = 0, bool Wide = false>
+template <bool Count, int MinBlocks, bool Postpone = false, int SmemS = 0, bool Wide = false>
 __global__ void __launch_bounds__(kBlock, MinBlocks) shadow_batch_kernel(const DevScene* __restrict__ table,
                                                                          float4* const* __restrict__ outs,
                                                                          const float4* __restrict__ sa,
@@ -334,7 +260,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks) shadow_batch_kernel(const D
                                                                          const uint32_t* count_ptr, uint32_t* cursor,
                                                                          unsigned long long* work_out) {
     const DevScene none{};
-    traverse_queue<true, Count, Refill, true, Postpone, SmemS, Wide>(
+    traverse_queue<true, Count, true, Postpone, SmemS, Wide>(
         none, table, *count_ptr, cursor, work_out,
         [&](uint32_t i, Ray& r, float& tmax) -> uint32_t {
             const float4 a = sa[i], b = sb[i];
@@ -364,27 +290,27 @@ using BatchShadowKernel = void (*)(const DevScene*, float4* const*, const float4
 template <bool Count>
 BatchQueueKernel extend_batch_variant(int v) {
     switch (v) {
-    case 1: return extend_batch_kernel<Count, false, 5>;
-    case 2: return extend_batch_kernel<Count, false, 1, false, 8>;
-    case 3: return extend_batch_kernel<Count, false, 1, false, 0, true>;
-    case 4: return extend_batch_kernel<Count, false, 1, false, 8, true>;
-    case 5: return extend_batch_kernel<Count, false, 5, false, 8>;
-    case 6: return extend_batch_kernel<Count, false, 3, false, 8, true>;
-    case 7: return extend_batch_kernel<Count, false, 4, true>;
-    default: return extend_batch_kernel<Count, false, 4>;
+    case 1: return extend_batch_kernel<Count, 5>;
+    case 2: return extend_batch_kernel<Count, 1, false, 8>;
+    case 3: return extend_batch_kernel<Count, 1, false, 0, true>;
+    case 4: return extend_batch_kernel<Count, 1, false, 8, true>;
+    case 5: return extend_batch_kernel<Count, 5, false, 8>;
+    case 6: return extend_batch_kernel<Count, 3, false, 8, true>;
+    case 7: return extend_batch_kernel<Count, 4, true>;
+    default: return extend_batch_kernel<Count, 4>;
     }
 }
 template <bool Count>
 BatchShadowKernel shadow_batch_variant(int v) {
     switch (v) {
-    case 1: return shadow_batch_kernel<Count, false, 5>;
-    case 2: return shadow_batch_kernel<Count, false, 1, false, 8>;
-    case 3: return shadow_batch_kernel<Count, false, 1, false, 0, true>;
-    case 4: return shadow_batch_kernel<Count, false, 1, false, 8, true>;
-    case 5: return shadow_batch_kernel<Count, false, 5, false, 8>;
-    case 6: return shadow_batch_kernel<Count, false, 3, false, 8, true>;
-    case 7: return shadow_batch_kernel<Count, false, 4, true>;
-    default: return shadow_batch_kernel<Count, false, 1>;
+    case 1: return shadow_batch_kernel<Count, 5>;
+    case 2: return shadow_batch_kernel<Count, 1, false, 8>;
+    case 3: return shadow_batch_kernel<Count, 1, false, 0, true>;
+    case 4: return shadow_batch_kernel<Count, 1, false, 8, true>;
+    case 5: return shadow_batch_kernel<Count, 5, false, 8>;
+    case 6: return shadow_batch_kernel<Count, 3, false, 8, true>;
+    case 7: return shadow_batch_kernel<Count, 4, true>;
+    default: return shadow_batch_kernel<Count, 1>;
     }
 }
 
@@ -396,27 +322,27 @@ using ShadowKernel = void (*)(DevScene, const float4*, const float4*, const floa
 template <bool Count>
 QueueKernel extend_variant(int v) {
     switch (v) {
-    case 1: return extend_kernel<Count, false, 5>;
-    case 2: return extend_kernel<Count, false, 1, false, 8>;
-    case 3: return extend_kernel<Count, false, 1, false, 0, true>;
-    case 4: return extend_kernel<Count, false, 1, false, 8, true>;
-    case 5: return extend_kernel<Count, false, 5, false, 8>;
-    case 6: return extend_kernel<Count, false, 3, false, 8, true>;
-    case 7: return extend_kernel<Count, false, 4, true>;
-    default: return extend_kernel<Count, false, 1>;
+    case 1: return extend_kernel<Count, 5>;
+    case 2: return extend_kernel<Count, 1, false, 8>;
+    case 3: return extend_kernel<Count, 1, false, 0, true>;
+    case 4: return extend_kernel<Count, 1, false, 8, true>;
+    case 5: return extend_kernel<Count, 5, false, 8>;
+    case 6: return extend_kernel<Count, 3, false, 8, true>;
+    case 7: return extend_kernel<Count, 4, true>;
+    default: return extend_kernel<Count, 1>;
     }
 }
 template <bool Count>
 ShadowKernel shadow_variant(int v) {
     switch (v) {
-    case 1: return shadow_kernel<Count, false, 5>;
-    case 2: return shadow_kernel<Count, false, 1, false, 8>;
-    case 3: return shadow_kernel<Count, false, 1, false, 0, true>;
-    case 4: return shadow_kernel<Count, false, 1, false, 8, true>;
-    case 5: return shadow_kernel<Count, false, 5, false, 8>;
-    case 6: return shadow_kernel<Count, false, 3, false, 8, true>;
-    case 7: return shadow_kernel<Count, false, 4, true>;
-    default: return shadow_kernel<Count, false, 1>;
+    case 1: return shadow_kernel<Count, 5>;
+    case 2: return shadow_kernel<Count, 1, false, 8>;
+    case 3: return shadow_kernel<Count, 1, false, 0, true>;
+    case 4: return shadow_kernel<Count, 1, false, 8, true>;
+    case 5: return shadow_kernel<Count, 5, false, 8>;
+    case 6: return shadow_kernel<Count, 3, false, 8, true>;
+    case 7: return shadow_kernel<Count, 4, true>;
+    default: return shadow_kernel<Count, 1>;
     }
 }
 
