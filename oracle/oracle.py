@@ -70,7 +70,7 @@ _SIG = {
     "oracle_primary_ray": (None, [P, U32, U32, U32, P, P, C.POINTER(U32)]),
     "oracle_pathtrace": (None, [P, P, U32, U32, U32, U32, U32, U32, U32, P, I, P]),
     "oracle_pathtrace_ex": (None, [P, P, U32, U32, U32, U32, U32, U32, U32, P, I, P, U32]),
-    "oracle_emitters": (U32, [P, P, P, P]),
+    "oracle_emitters": (U32, [P, P, P, P, P]),
     "oracle_accumulate": (None, [P, P, C.c_size_t, U32, U32]),
     "oracle_restir_di_initial": (None, [P, P, C.POINTER(DIParams), P, P, P, I]),
     "oracle_restir_di_temporal": (None, [P, P, C.POINTER(DIParams), P, P, P, P, I]),
@@ -231,13 +231,16 @@ def pathtrace(scene: OracleScene, cam, frame_seed: int, max_bounces: int, spp: i
 
 
 def emitters(scene: OracleScene):
-    """The emitter table: (records[n, 12], cdf[n], total power)."""
-    n = lib().oracle_emitters(scene.handle, None, None, None)
+    """The emitter table: (records[n, 12], alias probabilities[n], aliases[n],
+    total power)."""
+    n = lib().oracle_emitters(scene.handle, None, None, None, None)
     rec = np.zeros((n, 12), np.float32)
-    cdf = np.zeros(n, np.float32)
+    prob = np.zeros(n, np.float32)
+    alias = np.zeros(n, np.uint32)
     tot = np.zeros(1, np.float32)
-    lib().oracle_emitters(scene.handle, _p(rec) if n else None, _p(cdf) if n else None, _p(tot))
-    return rec, cdf, float(tot[0])
+    lib().oracle_emitters(scene.handle, _p(rec) if n else None, _p(prob) if n else None, _p(alias) if n else None,
+                          _p(tot))
+    return rec, prob, alias, float(tot[0])
 
 
 def accumulate(radiance: np.ndarray, acc: np.ndarray, camera_moved: int, spp: int) -> None:

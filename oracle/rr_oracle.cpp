@@ -318,9 +318,11 @@ struct OracleScene {
     // material with non-zero area, instance-major; 12 floats each,
     // (p0, Le.r), (e1, Le.g), (e2, Le.b), and the inclusive prefix sums of
     // power = luminance(Le) * area
-    std::vector<float> emit;
-    std::vector<float> emit_cdf;
+    std::vector<float> emit;             // 12 floats per emitter
+    std::vector<float> emit_prob;        // alias table over the emitters' powers
+    std::vector<uint32_t> emit_alias;
     float emit_total = 0.0f;
+    uint32_t num_emitters() const { return (uint32_t)emit_prob.size(); }
 };
 
 namespace {
@@ -572,14 +574,12 @@ inline float emitter_pdf(float p_group, float lum, float total, float d2, float 
     return p_group * (lum / total) * d2 / cos_y;
 }
 
-// First k with cdf[k] > target (n - 1 when none is).
-inline uint32_t emitter_search(const float* cdf, uint32_t n, float target) {
-    uint32_t lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (cdf[mid] > target) hi = mid; else lo = mid + 1;
-    }
-    return lo;
+// The emitter a pair of uniforms picks from the alias table: column
+// min(floor(u n), n - 1), kept when uc < its probability, else its alias.
+inline uint32_t emitter_pick(const OracleScene& s, float u, float uc) {
+    const uint32_t n = s.num_emitters();
+    const uint32_t k = std::min((uint32_t)(u * (float)n), n - 1u);
+    return uc < s.emit_prob[k] ? k : s.emit_alias[k];
 }
 
 // sample_lights (pathtracer.slang:124-177) with its light-count factor N
@@ -630,7 +630,7 @@ V3 trace_path_emitters(const OracleScene& s, const GpuCameraData& cam, uint32_t 
     V3 ray_orig, ray_dir;
     primary_ray(cam, px, py, jx, jy, ray_orig, ray_dir);
     V3 radiance = v3(0, 0, 0), throughput = v3(1, 1, 1);
-    const uint32_t NL = (uint32_t)s.lights.size(), NE = (uint32_t)s.emit_cdf.size();
+    const uint32_t NL = (uint32_t)s.lights.size(), NE = s.num_emitters();
     const float pe = NE == 0 ? 0.0f : (NL == 0 ? 1.0f : 0.5f);
     float prev_pdf = 0.0f;   // bounce density of the ray (0: a camera ray)
     for (uint32_t bounce = 0; bounce < max_bounces; ++bounce) {
@@ -662,9 +662,10 @@ V3 trace_path_emitters(const OracleScene& s, const GpuCameraData& cam, uint32_t 
             const bool use_e = NE > 0 && (NL == 0 || rand_float(seed) < 0.5f);
             if (use_e) {
                 const float u = rand_float(seed);
+                const float uc = rand_float(seed);
                 const float u1 = rand_float(seed);
                 const float u2 = rand_float(seed);
-                const uint32_t k = emitter_search(s.emit_cdf.data(), NE, u * s.emit_total);
+                const uint32_t k = emitter_pick(s, u, uc);
                 const float* e = &s.emit[size_t(k) * 12];
                 const V3 p0 = v3(e[0], e[1], e[2]), E1 = v3(e[4], e[5], e[6]), E2 = v3(e[8], e[9], e[10]);
                 const V3 Le = v3(e[3], e[7], e[11]);
@@ -759,15 +760,16 @@ struct DiLightSample {
 };
 DiLightSample di_decode(const OracleScene& s, uint32_t c) {
     uint32_t st = c;
-    const uint32_t NL = (uint32_t)s.lights.size(), NE = (uint32_t)s.emit_cdf.size();
+    const uint32_t NL = (uint32_t)s.lights.size(), NE = s.num_emitters();
     const float pe = NE == 0 ? 0.0f : (NL == 0 ? 1.0f : 0.5f);
     DiLightSample r{};
     r.emitter = NE > 0 && (NL == 0 || rand_float(st) < 0.5f);
     if (r.emitter) {
         const float u = rand_float(st);
+        const float uc = rand_float(st);
         const float u1 = rand_float(st);
         const float u2 = rand_float(st);
-        const uint32_t k = emitter_search(s.emit_cdf.data(), NE, u * s.emit_total);
+        const uint32_t k = emitter_pick(s, u, uc);
         const float* e = &s.emit[size_t(k) * 12];
         const V3 E1 = v3(e[4], e[5], e[6]), E2 = v3(e[8], e[9], e[10]);
         const float su = sqrtf(u1);
@@ -1122,6 +1124,7 @@ OracleScene* oracle_scene_create(const GpuVertex* vertices, uint32_t vertex_coun
     }
     {
         double acc = 0.0;
+        std::vector<double> power;
         for (const Tri& t : s->tris) {
             const GpuMaterial& mat = materials[meshes[instances[t.inst].mesh_index].material_index];
             if (!any_positive(mat.emissive)) continue;
@@ -1134,9 +1137,36 @@ OracleScene* oracle_scene_create(const GpuVertex* vertices, uint32_t vertex_coun
             const float rec[12] = {t.p0.x, t.p0.y, t.p0.z, mat.emissive[0], e1.x, e1.y, e1.z, mat.emissive[1],
                                    e2.x, e2.y, e2.z, mat.emissive[2]};
             s->emit.insert(s->emit.end(), rec, rec + 12);
-            s->emit_cdf.push_back(float(acc));
+            power.push_back(double(lum) * double(area));
         }
         s->emit_total = float(acc);
+        // Vose's alias table over the powers (FP64): column k keeps a draw with
+        // probability prob_k, else hands it to alias_k; columns paired in stack
+        // order, the last "small" with the last "large"; leftovers keep all.
+        const size_t n = power.size();
+        s->emit_prob.assign(n, 1.0f);
+        s->emit_alias.resize(n);
+        for (size_t i = 0; i < n; ++i) s->emit_alias[i] = (uint32_t)i;
+        if (n > 0) {
+            double total = 0.0;
+            for (double x : power) total += x;
+            std::vector<double> sc(n);
+            std::vector<uint32_t> small, large;
+            for (size_t i = 0; i < n; ++i) {
+                sc[i] = power[i] * double(n) / total;
+                (sc[i] < 1.0 ? small : large).push_back((uint32_t)i);
+            }
+            while (!small.empty() && !large.empty()) {
+                const uint32_t a = small.back();
+                small.pop_back();
+                const uint32_t b = large.back();
+                large.pop_back();
+                s->emit_prob[a] = (float)sc[a];
+                s->emit_alias[a] = b;
+                sc[b] = (sc[b] + sc[a]) - 1.0;
+                (sc[b] < 1.0 ? small : large).push_back(b);
+            }
+        }
     }
     s->use_bvh = use_bvh != 0;
     if (s->use_bvh && !s->tris.empty()) {
@@ -1156,11 +1186,13 @@ OracleScene* oracle_scene_create(const GpuVertex* vertices, uint32_t vertex_coun
 
 void oracle_scene_destroy(OracleScene* s) { delete s; }
 
-uint32_t oracle_emitters(const OracleScene* s, float* records_out, float* cdf_out, float* total_out) {
+uint32_t oracle_emitters(const OracleScene* s, float* records_out, float* prob_out, uint32_t* alias_out,
+                         float* total_out) {
     if (records_out) std::memcpy(records_out, s->emit.data(), s->emit.size() * sizeof(float));
-    if (cdf_out) std::memcpy(cdf_out, s->emit_cdf.data(), s->emit_cdf.size() * sizeof(float));
+    if (prob_out) std::memcpy(prob_out, s->emit_prob.data(), s->emit_prob.size() * sizeof(float));
+    if (alias_out) std::memcpy(alias_out, s->emit_alias.data(), s->emit_alias.size() * sizeof(uint32_t));
     if (total_out) *total_out = s->emit_total;
-    return (uint32_t)s->emit_cdf.size();
+    return s->num_emitters();
 }
 uint32_t oracle_scene_triangle_count(const OracleScene* s) { return (uint32_t)s->tris.size(); }
 
@@ -1247,7 +1279,7 @@ void oracle_restir_di_initial(const OracleScene* s, const GpuCameraData* cam, co
     const uint32_t W = cam->screen_width, H = cam->screen_height;
     const uint32_t N = (uint32_t)s->lights.size();
     const bool E = (p->flags & ORACLE_DI_EMITTERS) != 0;
-    const uint32_t NE = E ? (uint32_t)s->emit_cdf.size() : 0u;
+    const uint32_t NE = E ? s->num_emitters() : 0u;
     parallel_rows(H, threads, [&](uint32_t y) {
         for (uint32_t x = 0; x < W; ++x) {
             const size_t i = ((size_t)y * W + x) * 4;
@@ -1356,7 +1388,7 @@ void oracle_restir_di_spatial_shade(const OracleScene* s, const GpuCameraData* c
     const uint32_t W = cam->screen_width, H = cam->screen_height;
     const uint32_t N = (uint32_t)s->lights.size();
     const bool E = (p->flags & ORACLE_DI_EMITTERS) != 0;
-    const uint32_t NA = E ? N + (uint32_t)s->emit_cdf.size() : N;   // lights the reservoirs can name
+    const uint32_t NA = E ? N + s->num_emitters() : N;   // lights the reservoirs can name
     auto phat = [&](uint32_t sel, V3 pos, V3 n) {
         return E ? di_p_hat_emit(*s, di_decode(*s, sel), pos, n) : compute_p_hat(*s, sel, pos, n);
     };

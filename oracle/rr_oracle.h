@@ -95,7 +95,8 @@ void oracle_pathtrace_ex(const OracleScene* scene, const GpuCameraData* cam,
 /* The emitter table: count, total power, and (if out is non-null) the
  * 12-float records followed by nothing else; cdf_out (nullable) receives
  * the prefix sums. */
-uint32_t oracle_emitters(const OracleScene* scene, float* records_out, float* cdf_out, float* total_out);
+uint32_t oracle_emitters(const OracleScene* scene, float* records_out, float* prob_out, uint32_t* alias_out,
+                         float* total_out);
 
 /* ── Accumulate (accumulate.slang:21-46) ────────────────────────────────── */
 void oracle_accumulate(const float* radiance, float* accumulated, size_t pixels,

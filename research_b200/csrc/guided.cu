@@ -124,15 +124,6 @@ RR_D float emitter_pdf(float p_group, float lum, float total, float d2, float co
     return p_group * (lum / total) * d2 / cos_y;
 }
 
-RR_D uint32_t emitter_search(const float* __restrict__ cdf, uint32_t n, float target) {
-    uint32_t lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (__ldg(cdf + mid) > target) hi = mid; else lo = mid + 1;
-    }
-    return lo;
-}
-
 template <bool SlotMixture, bool Multi, bool Emit = false>
 __global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s0, GuidedLaunch G,
                                                               const DevScene* __restrict__ table,
@@ -231,9 +222,10 @@ __global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s0, Gu
                         if (NE > 0 && (NL == 0 || rand_float(seed) < 0.5f)) {
                             nee_done = true;
                             const float u = rand_float(seed);
+                            const float uc = rand_float(seed);
                             const float u1 = rand_float(seed);
                             const float u2 = rand_float(seed);
-                            const uint32_t k = emitter_search(s.emit_cdf, NE, u * s.emit_total);
+                            const uint32_t k = emitter_pick(s, u, uc);
                             const float4 e0 = __ldg(s.emitters + k * 3), e1 = __ldg(s.emitters + k * 3 + 1);
                             const float4 e2 = __ldg(s.emitters + k * 3 + 2);
                             const float3 E1 = xyz(e1), E2 = xyz(e2);

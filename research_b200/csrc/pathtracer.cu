@@ -131,7 +131,7 @@ RR_D void shade_ray(const DevScene& s, float4* __restrict__ out, uint32_t bounce
 // Next-event estimation over the GpuLights and the scene's emissive
 // triangles: per vertex one group (probability 1/2 each when both exist);
 // in the emitter group one triangle in proportion to luminance(Le) * area
-// (binary search of the prefix sums) and a point uniform on it, with the
+// (emitter_pick: the scene's alias table) and a point uniform on it, with the
 // solid-angle density p_l = P_E (luminance(Le) / total) d^2 / |cos_y|; the
 // GpuLight group is the reference's sample_lights with its factor N divided
 // by the group's probability. Bounces are weighted by f cos / p_act, the
@@ -148,15 +148,6 @@ RR_D float emitter_pdf(float p_group, float lum, float total, float d2, float co
 }
 
 // First k with cdf[k] > target (n - 1 when none is).
-RR_D uint32_t emitter_search(const float* __restrict__ cdf, uint32_t n, float target) {
-    uint32_t lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (__ldg(cdf + mid) > target) hi = mid; else lo = mid + 1;
-    }
-    return lo;
-}
-
 RR_D void shade_ray_emitters(const DevScene& s, float4* __restrict__ out, uint32_t bounce, uint32_t last,
                              const float4 a, const float4 b, const float4 c, const float4 h, ShadeResult& R) {
     R.pid = __float_as_uint(a.w);
@@ -204,9 +195,10 @@ RR_D void shade_ray_emitters(const DevScene& s, float4* __restrict__ out, uint32
         const bool use_e = NE > 0 && (NL == 0 || rand_float(R.seed) < 0.5f);
         if (use_e) {
             const float u = rand_float(R.seed);
+            const float uc = rand_float(R.seed);
             const float u1 = rand_float(R.seed);
             const float u2 = rand_float(R.seed);
-            const uint32_t k = emitter_search(s.emit_cdf, NE, u * s.emit_total);
+            const uint32_t k = emitter_pick(s, u, uc);
             const float4 e0 = __ldg(s.emitters + k * 3), e1 = __ldg(s.emitters + k * 3 + 1);
             const float4 e2 = __ldg(s.emitters + k * 3 + 2);
             const float3 E1 = xyz(e1), E2 = xyz(e2);

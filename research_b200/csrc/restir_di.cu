@@ -46,15 +46,6 @@ RR_D float compute_p_hat(const DevScene& s, uint32_t li, float3 pos, float3 n) {
 // area density for an emitter point).
 RR_D float lum709(float3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
 
-RR_D uint32_t emitter_search(const float* __restrict__ cdf, uint32_t n, float target) {
-    uint32_t lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (__ldg(cdf + mid) > target) hi = mid; else lo = mid + 1;
-    }
-    return lo;
-}
-
 struct DiLightSample {
     bool emitter;
     uint32_t li;
@@ -72,9 +63,10 @@ RR_D DiLightSample di_decode(const DevScene& s, uint32_t c) {
     r.emitter = NE > 0 && (NL == 0 || rand_float(st) < 0.5f);
     if (r.emitter) {
         const float u = rand_float(st);
+        const float uc = rand_float(st);
         const float u1 = rand_float(st);
         const float u2 = rand_float(st);
-        const uint32_t k = emitter_search(s.emit_cdf, NE, u * s.emit_total);
+        const uint32_t k = emitter_pick(s, u, uc);
         const float4 e0 = __ldg(s.emitters + k * 3), e1 = __ldg(s.emitters + k * 3 + 1);
         const float4 e2 = __ldg(s.emitters + k * 3 + 2);
         const float3 E1 = xyz(e1), E2 = xyz(e2);

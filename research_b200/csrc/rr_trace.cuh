@@ -41,13 +41,24 @@ struct DevScene {
     uint32_t num_nodes;
     uint32_t num_nodes4;
     // Emissive triangles (RR_PT_FLAG_EMITTERS): world-space (p0, Le.r),
-    // (e1, Le.g), (e2, Le.b) per emitter, instance-major; emit_cdf holds the
-    // inclusive prefix sums of luminance(Le) * area, emit_total their total.
+    // (e1, Le.g), (e2, Le.b) per emitter, instance-major; emit_alias is an
+    // alias table over their powers luminance(Le) * area (emitter_pick),
+    // emit_total the total power.
     const float4* emitters;
-    const float* emit_cdf;
+    const float2* emit_alias;
     uint32_t num_emitters;
     float emit_total;
 };
+
+// An emitter drawn with probability proportional to its power from two
+// uniforms: u picks a column of the alias table, uc keeps it or takes its
+// alias (one table read instead of a search of prefix sums).
+RR_D uint32_t emitter_pick(const DevScene& s, float u, float uc) {
+    const uint32_t n = s.num_emitters;
+    const uint32_t k = min(uint32_t(u * float(n)), n - 1u);
+    const float2 t = __ldg(s.emit_alias + k);
+    return uc < t.x ? k : __float_as_uint(t.y);
+}
 
 // A ray with its shear constants (triangle test) and its slab-test
 // constants: a box plane x is at t = fma(x, inv, alo) for a lower plane and

@@ -119,6 +119,43 @@ static inline float row_point(const float* M, int r, const float* p) {
     return M[r * 4 + 0] * p[0] + M[r * 4 + 1] * p[1] + M[r * 4 + 2] * p[2] + M[r * 4 + 3] * 1.0f;
 }
 
+// Vose's alias table over weights w (FP64, w_k > 0): column k keeps a draw
+// with probability prob_k and hands it to alias_k otherwise, so that column
+// k is picked with probability w_k / sum(w). Entry k is (prob_k, alias_k as
+// float bits). Columns are paired in stack order (the last "small" with the
+// last "large"); columns left over by rounding keep every draw.
+static std::vector<float2> alias_table(const std::vector<double>& w) {
+    const size_t n = w.size();
+    std::vector<float2> t(n);
+    if (n == 0) return t;
+    double total = 0.0;
+    for (double x : w) total += x;
+    std::vector<double> sc(n);
+    std::vector<uint32_t> small, large;
+    for (size_t i = 0; i < n; ++i) {
+        sc[i] = w[i] * double(n) / total;
+        (sc[i] < 1.0 ? small : large).push_back(uint32_t(i));
+    }
+    std::vector<float> prob(n, 1.0f);
+    std::vector<uint32_t> alias(n);
+    for (size_t i = 0; i < n; ++i) alias[i] = uint32_t(i);
+    while (!small.empty() && !large.empty()) {
+        const uint32_t a = small.back();
+        small.pop_back();
+        const uint32_t b = large.back();
+        large.pop_back();
+        prob[a] = float(sc[a]);
+        alias[a] = b;
+        sc[b] = (sc[b] + sc[a]) - 1.0;
+        (sc[b] < 1.0 ? small : large).push_back(b);
+    }
+    for (size_t i = 0; i < n; ++i) {
+        t[i].x = prob[i];
+        std::memcpy(&t[i].y, &alias[i], 4);
+    }
+    return t;
+}
+
 rr_status rr_scene_create(rr_ctx* ctx, const rr_scene_desc* d, rr_scene** out) {
     if (!ctx || !d || !out) return rr_fail(ctx, RR_ERR_INVALID_ARGUMENT, "null argument");
     *out = nullptr;
@@ -187,9 +224,10 @@ rr_status rr_scene_create(rr_ctx* ctx, const rr_scene_desc* d, rr_scene** out) {
         trirec[size_t(i) * 3] = a; trirec[size_t(i) * 3 + 1] = b; trirec[size_t(i) * 3 + 2] = c;
     }
     // Emitter table: every triangle of an emissive material with non-zero
-    // area, instance-major, with the prefix sums of luminance(Le) * area.
+    // area, instance-major, and an alias table over their powers
+    // luminance(Le) * area (alias_table below).
     std::vector<float4> emit;
-    std::vector<float> emit_cdf;
+    std::vector<double> emit_power;
     float emit_total = 0.0f;
     {
         double acc = 0.0;
@@ -208,10 +246,11 @@ rr_status rr_scene_create(rr_ctx* ctx, const rr_scene_desc* d, rr_scene** out) {
             emit.push_back(make_float4(w[0], w[1], w[2], g.emissive[0]));
             emit.push_back(make_float4(e1[0], e1[1], e1[2], g.emissive[1]));
             emit.push_back(make_float4(e2[0], e2[1], e2[2], g.emissive[2]));
-            emit_cdf.push_back(float(acc));
+            emit_power.push_back(double(lum) * double(area));
         }
         emit_total = float(acc);
     }
+    const std::vector<float2> emit_alias = alias_table(emit_power);
     std::vector<float4> mats(size_t(d->material_count) * 2);
     for (uint32_t m = 0; m < d->material_count; ++m) {
         const GpuMaterial& g = d->materials[m];
@@ -251,9 +290,10 @@ rr_status rr_scene_create(rr_ctx* ctx, const rr_scene_desc* d, rr_scene** out) {
     RR_UP(mats.data(), mats.size() * sizeof(float4), materials, const float4*);
     RR_UP(d->light_count ? d->lights : nullptr, size_t(d->light_count) * sizeof(GpuLight), lights, const float4*);
     RR_UP(emit.empty() ? nullptr : emit.data(), emit.size() * sizeof(float4), emitters, const float4*);
-    RR_UP(emit_cdf.empty() ? nullptr : emit_cdf.data(), emit_cdf.size() * sizeof(float), emit_cdf, const float*);
+    RR_UP(emit_alias.empty() ? nullptr : emit_alias.data(), emit_alias.size() * sizeof(float2), emit_alias,
+          const float2*);
 #undef RR_UP
-    s->dev.num_emitters = uint32_t(emit_cdf.size());
+    s->dev.num_emitters = uint32_t(emit_power.size());
     s->dev.emit_total = emit_total;
     s->dev.num_lights = d->light_count;
     s->dev.num_instances = d->instance_count;

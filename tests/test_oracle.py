@@ -195,3 +195,29 @@ def test_restir_di_emitter_candidates_are_unbiased(rr, O, keep_point_light):
     surf = g[..., 3] >= 0
     md, mp = di[surf].mean(), pt[surf].mean()
     assert abs(md - mp) / mp < 0.02, (md, mp)
+
+
+def test_emitter_alias_table_reproduces_the_power_distribution(rr, O):
+    """The alias table the emitter sampling draws from picks emitter k with
+    probability power_k / total (power = luminance(Le) * area), summed from the
+    table's columns: (prob_k + sum over columns aliasing to k of 1 - prob_j) / n.
+    On the procedural room's 4096 emitters of radiance log-uniform in
+    [0.1, 100]."""
+    hs = rr.HostScene.procedural(seed=0x5EED0002, target_triangles=20_000, emissive_triangles=4096,
+                                 box_half=20.0, L=O.inputs_lib())
+    osc = O.OracleScene(hs.arrays, use_bvh=False)
+    rec, prob, alias, total = O.emitters(osc)
+    n = len(prob)
+    assert n >= 1000 and np.all((prob >= 0) & (prob <= 1)) and np.all(alias < n)
+    e1, e2 = rec[:, 4:7].astype(np.float64), rec[:, 8:11].astype(np.float64)
+    area = 0.5 * np.linalg.norm(np.cross(e1, e2), axis=1)
+    le = rec[:, [3, 7, 11]].astype(np.float64)
+    power = (0.2126 * le[:, 0] + 0.7152 * le[:, 1] + 0.0722 * le[:, 2]) * area
+    implied = prob.astype(np.float64).copy()
+    np.add.at(implied, alias, 1.0 - prob.astype(np.float64))
+    implied -= np.where(alias == np.arange(n), 1.0 - prob, 0.0)   # a column's own alias adds nothing
+    implied /= n
+    np.testing.assert_allclose(implied, power / power.sum(), rtol=2e-5, atol=1e-9)
+    assert abs(power.sum() - total) / total < 1e-5
+    osc.close()
+    hs.close()
