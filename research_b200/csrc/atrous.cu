@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(256) atrous_tma_kernel(const __grid_constant__
 } // namespace rr
 
 // cuTensorMapEncodeTiled from the driver (no link-time dependency on it).
-static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+PFN_cuTensorMapEncodeTiled_v12000 rr_tensor_map_encoder() {
     // looked up once (a function-local static: initialised once, thread-safe)
     static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
         void* p = nullptr;
@@ -145,7 +145,7 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 // (4, bw, bh); false if the driver refuses it (the caller then uses the
 // direct-load kernel).
 static bool image_map(CUtensorMap* m, const void* img, uint32_t W, uint32_t H, uint32_t bw, uint32_t bh) {
-    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    PFN_cuTensorMapEncodeTiled_v12000 enc = rr_tensor_map_encoder();
     if (!enc || (reinterpret_cast<uintptr_t>(img) & 15u) != 0) return false;
     const cuuint64_t dims[3] = {4, W, H};
     const cuuint64_t strides[2] = {16, cuuint64_t(W) * 16};

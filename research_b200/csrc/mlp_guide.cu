@@ -25,6 +25,12 @@
 //    column against a BF16 bias column of the weight tile).
 
 #include "rr_guide.h"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+// cuTensorMapEncodeTiled from the driver (atrous.cu).
+PFN_cuTensorMapEncodeTiled_v12000 rr_tensor_map_encoder();
 #include "rr_vmf.cuh"
 #include "rr_tc.cuh"
 
@@ -599,162 +605,178 @@ __global__ void __launch_bounds__(kTile * NW, 1) mlp_backward_kernel(BwdArgs A) 
 // ── weight gradients on the tensor cores ──────────────────────────────────
 // dW_l^T (in x out) = X_l^T dZ_l with the batch as the K dimension. A
 // persistent CTA owns a contiguous range of 32-sample steps. Both operands
-// are MN-major: a sample's row of X (features contiguous) and of dZ (outputs
-// contiguous) lands in shared memory as it lies in global memory, 16 bytes
-// (8 features of one sample) per copy, so the rows are staged by cp.async
-// with no transposition and no registers, four stages deep. Layer l's A
-// operand is the 128-feature window from feature kWgRow[l]: its I inputs, a
-// constant feature of ones (whose product with dZ_l is db_l) and features
-// that are ignored. Layer l accumulates into TMEM columns zoff(l) .. + out
-// over all of the CTA's steps; the CTA then writes its FP32 partial
-// gradient, and mlp_reduce_kernel sums the partials in CTA order.
+// are MN-major, so X and dZ need no transposition: one 2-D tensor copy (TMA)
+// of a box of 64 features x 32 samples puts 128 bytes of each sample's row
+// in shared memory with the 128-byte swizzle. A step is 11 such blocks: X
+// columns 0-63 and 64-127 (layer 0's 80 inputs; the rest are ignored rows),
+// each hidden layer's 64 inputs, and dZ in blocks of 64 columns (the last
+// one zero-filled past column 304). One thread issues a step's copies into
+// a stage and completes the stage's mbarrier with their bytes, four stages
+// deep, and issues the step's MMAs once the copies have landed.
 //
-// MN-major operand layout (no swizzle): 8 consecutive features (16 bytes)
-// of one sample form a row of a core matrix, the 8 samples of a sample
-// group its 8 rows (128 contiguous bytes); feature groups are 128 bytes
-// apart (SBO) and sample groups kWgLbo* apart (LBO).
-constexpr int kWgStep = 32;                                  // samples per step (K)
+// Layer l's A operand is 128 features: its input block and, 64 features
+// further, the next block. For a hidden layer that next block is a constant
+// block in shared memory whose feature 0 is 1 for every sample (the
+// descriptor's leading offset reaches it from any stage), so row 64 of the
+// product is db_l. Layer 0's second block holds inputs 64-79, so its bias is
+// a separate product (the constant block times dZ_0) in TMEM columns
+// kWgBiasCol... Layer l accumulates into TMEM columns zoff(l) .. + out over
+// all of the CTA's steps; the CTA then writes its FP32 partial gradient and
+// mlp_reduce_kernel sums the partials in CTA order. Samples past the batch
+// are the copies' zero fill.
+//
+// Operand layout (MN-major, 128-byte swizzle): a block is 32 rows (samples)
+// of 128 bytes (64 features); within each 1024-byte group of 8 rows, the
+// 16-byte chunk c of row r is stored at chunk c ^ (r % 8). Blocks of one
+// operand are LBO bytes apart along M/N, 8-row groups 1024 bytes (SBO)
+// apart along K; one MMA takes K = 16 (two groups).
+constexpr int kWgStep = 32;                                   // samples per step (K)
 constexpr int kWgStages = 4;
-// first feature of layer l's window: layer 0 takes 80 inputs + the ones
-// feature (88 after padding to 8), hidden layers 64 + 1 (72)
-__host__ __device__ constexpr int wg_row(int l) { return l == 0 ? 0 : 88 + (l - 1) * 72; }
-static_assert(wg_row(1) == ((kIn + 1 + 7) / 8) * 8 && wg_row(2) - wg_row(1) == ((kHid + 1 + 7) / 8) * 8, "rows");
-constexpr int kWgRowsX = wg_row(kLayers - 1) + kTile;        // 432 features staged
-constexpr int kWgLboX = (kWgRowsX / 8) * 128;                // sample-group stride of the X stage
-constexpr int kWgLboZ = (kZCols / 8) * 128;                  // sample-group stride of the dZ stage
-constexpr int kWgBlkX = (kWgStep / 8) * kWgLboX;
-constexpr int kWgStage = kWgBlkX + (kWgStep / 8) * kWgLboZ;
-constexpr int kSmWg = kWgStages * kWgStage + 64;
+constexpr int kWgBlock = kWgStep * 128;                       // one 64-feature block of a step
+constexpr int kWgXBlocks = 2 + (kLayers - 1);                 // X copies per step
+constexpr int kWgZBlocks = (kZCols + 63) / 64;                // dZ copies per step
+constexpr int kWgStage = (kWgXBlocks + kWgZBlocks) * kWgBlock;
+constexpr int kWgConst = kWgStages * kWgStage;                // two constant blocks (ones, zeros)
+constexpr int kSmWg = kWgConst + 2 * kWgBlock + 128 + 1024;   // + mbarriers, + 1024-byte alignment
+constexpr int kWgBiasCol = zoff(kLayers);                     // TMEM columns of layer 0's bias sums
 static_assert(kSmWg <= 227 * 1024, "wgrad stages exceed shared memory");
-static_assert(kZCols <= 512 && zoff(kLayers) <= 304, "wgrad TMEM columns");
-static_assert(kXCols % 8 == 0 && kZCols % 8 == 0 && kWgStep % 16 == 0, "16-byte copies, K = 16 per MMA");
+static_assert(kHid == 64 && kIn > 64 && kIn < kTile, "block plan: 64 hidden units, 65..127 inputs");
+static_assert(kWgBiasCol + lout(0) <= 512, "wgrad TMEM columns");
+static_assert(kWgStage % 1024 == 0, "stages keep the 1024-byte swizzle alignment");
+// first X column of copy b of a step (16-byte aligned: x * 2 % 16 == 0)
+__host__ __device__ constexpr int wg_xcol(int b) { return b < 2 ? b * 64 : xoff(b - 1); }
+static_assert(wg_xcol(2) % 8 == 0 && wg_xcol(3) % 8 == 0 && wg_xcol(kWgXBlocks - 1) + 64 == kXCols, "X blocks");
 
-constexpr int kWgThreads = 256;                              // 8 warps; warps 0-3 also read TMEM
-constexpr int kWgChunks = (kXCols + kZCols) / 8;             // 16-byte copies per sample (42 of X, 38 of dZ)
-constexpr int kWgPer = kWgChunks * kWgStep / kWgThreads;     // copies per thread per step
-static_assert(kWgChunks % 4 == 0 && (kWgChunks * kWgStep) % kWgThreads == 0, "copies split evenly");
+constexpr int kWgThreads = 128;                               // 4 warps read TMEM's 128 lanes
 
 // kind::f16 instruction descriptor with both operands MN-major.
 __host__ __device__ constexpr uint32_t idesc_bf16_mn(uint32_t M, uint32_t N) {
     return tc::idesc_bf16(M, N) | (1u << 15) | (1u << 16);
 }
 
-__global__ void __launch_bounds__(kWgThreads, 1) mlp_wgrad_kernel(const __nv_bfloat16* __restrict__ X,
-                                                            const __nv_bfloat16* __restrict__ dZ, uint32_t count,
+// Shared-memory descriptor with the 128-byte swizzle (layout type 2).
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return tc::smem_desc(addr, lbo, sbo) | (uint64_t(2) << 61);
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int c0, int c1, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(tc::smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(tc::smem_addr(bar))
+        : "memory");
+}
+
+__global__ void __launch_bounds__(kWgThreads, 1) mlp_wgrad_kernel(const __grid_constant__ CUtensorMap mx,
+                                                            const __grid_constant__ CUtensorMap mz, uint32_t count,
                                                             float* __restrict__ partial, int* error) {
-    extern __shared__ __align__(1024) unsigned char sm[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kWgStages * kWgStage);   // one per stage
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kWgStages * kWgStage + 8 * kWgStages);
+    extern __shared__ unsigned char sm_raw[];
+    unsigned char* sm = sm_raw + ((1024u - (tc::smem_addr(sm_raw) & 1023u)) & 1023u);
+    unsigned char* cblk = sm + kWgConst;
+    uint64_t* full = reinterpret_cast<uint64_t*>(cblk + 2 * kWgBlock);   // copies of a stage landed
+    uint64_t* done = full + kWgStages;                                   // MMAs of a stage completed
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(done + kWgStages);
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const uint32_t steps = (count + kWgStep - 1) / kWgStep;
     const uint32_t s_begin = uint32_t((uint64_t(blockIdx.x) * steps) / gridDim.x);
     const uint32_t s_end = uint32_t((uint64_t(blockIdx.x + 1) * steps) / gridDim.x);
     const uint32_t n = s_end - s_begin;
-    // constant features: zero every stage, then the ones feature of each
-    // window (feature wg_row(l) + I, the first of its group) for every sample
-    for (int e = t; e < kWgStages * kWgStage / 16; e += kWgThreads) reinterpret_cast<uint4*>(sm)[e] = make_uint4(0, 0, 0, 0);
-    __syncthreads();
-    for (int e = t; e < kWgStages * kLayers * kWgStep; e += kWgThreads) {
-        const int stage = e / (kLayers * kWgStep);
-        const int l = (e / kWgStep) % kLayers;
-        const int smp = e % kWgStep;
-        const int g = (wg_row(l) + lin(l)) / 8;
-        *reinterpret_cast<uint4*>(sm + stage * kWgStage + (smp / 8) * kWgLboX + g * 128 + (smp % 8) * 16) =
-            make_uint4(0x3F80u, 0u, 0u, 0u);
+    // constant blocks: the first has feature 0 (logical chunk 0, stored at
+    // chunk r % 8 of row r) = 1 in every row, the second is zero
+    for (int e = t; e < 2 * kWgBlock / 16; e += kWgThreads) {
+        const int r = e / 8, c = e % 8;
+        reinterpret_cast<uint4*>(cblk)[e] = make_uint4(r < kWgStep && c == (r & 7) ? 0x3F80u : 0u, 0u, 0u, 0u);
     }
     if (warp == 0) tc::tmem_alloc(tslot, 512);
     if (t == 0) {
-        for (int k = 0; k < kWgStages; ++k) tc::mbar_init(bar + k, 1);
+        for (int k = 0; k < kWgStages; ++k) { tc::mbar_init(full + k, 1); tc::mbar_init(done + k, 1); }
     }
     tc::fence_proxy_async();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *tslot;
-    // copies of step i into stage i % kWgStages: copy q of this thread is
-    // chunk c of sample (step, sample group sg, sample sg * 8 + lane % 8);
-    // the 8 lanes of a quarter-warp take one chunk of 8 consecutive samples
-    // (128 contiguous bytes of shared memory), a warp 4 consecutive chunks
-    auto issue = [&](uint32_t i) {
-        if (i < n) {
-            unsigned char* xs = sm + (i % kWgStages) * kWgStage;
-            unsigned char* zs = xs + kWgBlkX;
-            const uint32_t step = s_begin + i;
-            #pragma unroll
-            for (int q = 0; q < kWgPer; ++q) {
-                const int u = (q * kWgThreads + t) >> 5;            // warp-sized unit
-                const int sg = u / (kWgChunks / 4);
-                const int c = (u % (kWgChunks / 4)) * 4 + (lane >> 3);
-                const int smp = sg * 8 + (lane & 7);
-                const uint32_t row = step * kWgStep + smp;
-                const bool in = row < count;
-                const uint32_t rr = in ? row : 0u;
-                unsigned char* dst;
-                const __nv_bfloat16* src;
-                if (c < kXCols / 8) {
-                    int l = 0;
-                    #pragma unroll
-                    for (int v = 1; v < kLayers; ++v) l += c * 8 >= xoff(v) ? 1 : 0;
-                    const int g = (wg_row(l) + (c * 8 - xoff(l))) / 8;
-                    dst = xs + (smp / 8) * kWgLboX + g * 128 + (smp % 8) * 16;
-                    src = X + size_t(rr) * kXCols + c * 8;
-                } else {
-                    const int g = c - kXCols / 8;
-                    dst = zs + (smp / 8) * kWgLboZ + g * 128 + (smp % 8) * 16;
-                    src = dZ + size_t(rr) * kZCols + g * 8;
-                }
-                tc::cp_async16_zfill(dst, src, in);
-            }
-        }
-        tc::cp_async_commit();
-    };
     bool ok = true;
-    issue(0);
-    issue(1);
-    for (uint32_t i = 0; i < n; ++i) {
-        // the stage of step i + 2 was read by the MMAs of step i - 2
-        if (i >= 2) wait_chain(bar + ((i - 2) % kWgStages), ((i - 2) / kWgStages) & 1u, ok);
-        issue(i + 2);
-        tc::cp_async_wait_group2();            // step i has landed (steps i + 1, i + 2 may be in flight)
-        tc::fence_proxy_async();
-        tc::fence_before_sync();
-        __syncthreads();
-        if (t == 0) {
+    if (t == 0) {
+        const CUtensorMap* pmx = &mx;
+        const CUtensorMap* pmz = &mz;
+        // the step's copies into stage j % kWgStages, completing full[j % kWgStages]
+        auto produce = [&](uint32_t j) {
+            const uint32_t k = j % kWgStages;
+            unsigned char* st = sm + k * kWgStage;
+            const int row = int((s_begin + j) * kWgStep);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_addr(full + k)),
+                         "r"(uint32_t(kWgStage))
+                         : "memory");
+            #pragma unroll
+            for (int b = 0; b < kWgXBlocks; ++b) tma_load_2d(st + b * kWgBlock, pmx, wg_xcol(b), row, full + k);
+            #pragma unroll
+            for (int b = 0; b < kWgZBlocks; ++b)
+                tma_load_2d(st + (kWgXBlocks + b) * kWgBlock, pmz, b * 64, row, full + k);
+        };
+        const uint32_t ahead = min(n, uint32_t(kWgStages - 1));
+        for (uint32_t j = 0; j < ahead; ++j) produce(j);
+        const uint32_t ca = tc::smem_addr(cblk);
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint32_t j = i + kWgStages - 1;
+            if (j < n) {
+                // stage j % kWgStages was last read by the MMAs of step i - 1
+                if (i >= 1) ok = tc::mbar_wait(done + (i - 1) % kWgStages, ((i - 1) / kWgStages) & 1u) && ok;
+                produce(j);
+            }
+            ok = tc::mbar_wait(full + i % kWgStages, (i / kWgStages) & 1u) && ok;
             tc::fence_after_sync();
-            const uint32_t xa = tc::smem_addr(sm + (i % kWgStages) * kWgStage), za = xa + kWgBlkX;
+            const uint32_t sa = tc::smem_addr(sm + (i % kWgStages) * kWgStage);
+            const bool acc = i > 0;
             #pragma unroll
             for (int l = 0; l < kLayers; ++l) {
+                const uint32_t a0 = sa + uint32_t(l == 0 ? 0 : l + 1) * kWgBlock;
+                const uint32_t lbo = l == 0 ? uint32_t(kWgBlock) : ca - a0;
+                const uint32_t b0 = sa + uint32_t(kWgXBlocks + l) * kWgBlock;
                 const uint32_t idesc = idesc_bf16_mn(kTile, uint32_t(lout(l)));
                 #pragma unroll
                 for (int ks = 0; ks < kWgStep / 16; ++ks) {
-                    const uint64_t ad = tc::smem_desc(xa + (wg_row(l) / 8) * 128 + ks * 2 * kWgLboX, kWgLboX, 128);
-                    const uint64_t bd = tc::smem_desc(za + (zoff(l) / 8) * 128 + ks * 2 * kWgLboZ, kWgLboZ, 128);
-                    tc::mma_bf16(tmem + uint32_t(zoff(l)), ad, bd, idesc, i > 0 || ks > 0);
+                    const uint64_t bd = smem_desc_sw128(b0 + ks * 2048, kWgBlock, 1024);
+                    tc::mma_bf16(tmem + uint32_t(zoff(l)), smem_desc_sw128(a0 + ks * 2048, lbo, 1024), bd, idesc,
+                                 acc || ks > 0);
+                    if (l == 0)
+                        tc::mma_bf16(tmem + uint32_t(kWgBiasCol), smem_desc_sw128(ca + ks * 2048, kWgBlock, 1024),
+                                     bd, idesc, acc || ks > 0);
                 }
             }
-            tc::mma_commit(bar + (i % kWgStages));
+            tc::mma_commit(done + i % kWgStages);
         }
+        // the last commit covers every earlier MMA of this thread
+        if (n > 0) ok = tc::mbar_wait(done + (n - 1) % kWgStages, ((n - 1) / kWgStages) & 1u) && ok;
     }
-    tc::cp_async_wait_all();
-    if (n > 0) wait_chain(bar + ((n - 1) % kWgStages), ((n - 1) / kWgStages) & 1u, ok);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
     float* dst = partial + size_t(blockIdx.x) * kParams;
     const int r = warp * 32 + lane;   // TMEM lane = row of dW^T = input feature (I = bias row)
+    const uint32_t lanes = uint32_t(warp * 32) << 16;
     #pragma unroll
-    for (int l = 0; l < kLayers && warp < 4; ++l) {
+    for (int l = 0; l < kLayers; ++l) {
         const int I = lin(l), O = lout(l);
         #pragma unroll
         for (int c = 0; c < O; c += 16) {
             float v[16];
-            tc::tmem_ld16_wait(tmem + (uint32_t(warp * 32) << 16) + uint32_t(zoff(l) + c), v);
+            tc::tmem_ld16_wait(tmem + lanes + uint32_t(zoff(l) + c), v);
+            if (l == 0) {
+                float vb[16];
+                tc::tmem_ld16_wait(tmem + lanes + uint32_t(kWgBiasCol + c), vb);
+                #pragma unroll
+                for (int q = 0; q < 16; ++q)
+                    if (r == 0) dst[boff(0) + c + q] = n > 0 ? vb[q] : 0.0f;
+            }
             #pragma unroll
             for (int q = 0; q < 16; ++q) {
                 const float val = n > 0 ? v[q] : 0.0f;
                 if (r < I) dst[woff(l) + (c + q) * I + r] = val;
-                else if (r == I) dst[boff(l) + c + q] = val;
+                else if (l > 0 && r == I) dst[boff(l) + c + q] = val;
             }
         }
     }
-    if (!ok && t == 0) atomicExch(error, 1);
+    if (!ok && error) atomicExch(error, 1);
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) {
@@ -1026,6 +1048,21 @@ rr_status rr_mlp_guide_eval(rr_ctx* ctx, rr_guide* g, const float4* surf, float4
     return RR_OK;
 }
 
+// A [rows][cols] BF16 row-major array as a 2-D tensor for the weight
+// gradients' copies: box of 64 columns x kWgStep rows with the 128-byte
+// swizzle; columns and rows past the array read as zeros.
+static bool operand_map(CUtensorMap* m, const void* base, uint32_t cols, uint32_t rows) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = rr_tensor_map_encoder();
+    if (!enc || (reinterpret_cast<uintptr_t>(base) & 15u) != 0 || rows == 0) return false;
+    const cuuint64_t dims[2] = {cols, rows};
+    const cuuint64_t strides[1] = {cuuint64_t(cols) * 2};
+    const cuuint32_t box[2] = {64, kWgStep};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 rr_status rr_mlp_guide_train(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t stream) {
     rr_mlp_state& M = *g->mlp;
     if (n == 0) return RR_OK;
@@ -1061,7 +1098,10 @@ rr_status rr_mlp_guide_train(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t 
     RR_CHECK_LAUNCH(ctx);
     const uint32_t wsteps = (B + kWgStep - 1) / kWgStep;
     const int wgrid = int(std::min<uint32_t>(wsteps, uint32_t(M.wg_grid)));
-    mlp_wgrad_kernel<<<wgrid, kWgThreads, kSmWg, stream>>>(M.X, M.dZ, B, M.wpartial, M.error);
+    CUtensorMap mx, mz;
+    if (!operand_map(&mx, M.X, kXCols, B) || !operand_map(&mz, M.dZ, kZCols, B))
+        return rr_fail(ctx, RR_ERR_CUDA, "rr_mlp_guide_train: tensor map encoding failed");
+    mlp_wgrad_kernel<<<wgrid, kWgThreads, kSmWg, stream>>>(mx, mz, B, M.wpartial, M.error);
     RR_CHECK_LAUNCH(ctx);
     mlp_reduce_kernel<<<(kParams + 255) / 256, 256, 0, stream>>>(M.wpartial, uint32_t(wgrid), M.grad);
     RR_CHECK_LAUNCH(ctx);
