@@ -15,10 +15,13 @@
 //    bias, applies ReLU and writes the next BF16 activation tile. Inference
 //    writes the mixture of each query; training also keeps the activations
 //    and evaluates the weighted negative log-likelihood and its gradient.
-//  - mlp_backward_kernel: dX_l = dZ_l W_l on the tensor cores (M=128,
-//    N=64, K=out), dZ_{l-1} = dX_l * [X_l > 0].
-//  - mlp_wgrad_kernel / mlp_reduce_kernel: dW_l = dZ_l^T X_l, db_l = sum dZ_l
-//    on the CUDA cores in FP32, per-block partials reduced in a fixed order.
+//  - mlp_backward_kernel: per 128-sample tile and layer l = 4 .. 1,
+//    dX_l = dZ_l W_l (M=128, N=64, K=out) and dW_l^T += X_l^T dZ_l (M=128
+//    features, N=out, K=128 samples) on the tensor cores, then
+//    dZ_{l-1} = dX_l * [X_l > 0] in place in shared memory; dW_0^T last.
+//    X_l and dZ_4 arrive by tensor copies (TMA); every CTA accumulates its
+//    tiles' weight gradients in TMEM and writes one FP32 partial;
+//    mlp_reduce_kernel sums the partials in CTA order.
 //  - mlp_adam_kernel: Adam on FP32 master weights and biases (gradients carry
 //    a static loss scale), refreshing the BF16 copy used by the tensor cores;
 //    the forward kernel adds the biases inside the MMA (a constant-1 input
@@ -89,16 +92,29 @@ __host__ __device__ constexpr int fwd_smem(int nw) { return fwd_bar(nw) + 64; }
 __host__ __device__ constexpr uint32_t tmem_cols(int nw) { return nw <= 2 ? 128u : (nw <= 4 ? 256u : 512u); }
 constexpr int kInferWG = 5;   // inference: 640 threads, 96 registers each, 149 KB of shared memory
 constexpr int kTrainWG = 3;   // training forward: 384 threads (4 warpgroups at 128 registers measured 120.5 against 116.9 us)
-constexpr int kSmBwdWt = 0;
-constexpr int kSmBwdAct = kSmBwdWt + 2 * kWeightsBf16;
-// backward CTAs: NW warpgroups sharing W^T, one activation tile, mbarrier and
-// 64 TMEM columns each (as the forward)
-__host__ __device__ constexpr int bwd_act(int wg) { return kSmBwdAct + wg * kTile * kHid * 2; }
-__host__ __device__ constexpr int bwd_bar(int nw) { return bwd_act(nw); }
-__host__ __device__ constexpr int bwd_smem(int nw) { return bwd_bar(nw) + 64; }
-constexpr int kBwdWG = 5;
-static_assert(kSmFwdAct % 128 == 0 && kSmBwdAct % 128 == 0 && (kTile * kIn * 2) % 128 == 0,
-              "operand tiles 128-byte aligned");
+static_assert(kSmFwdAct % 128 == 0 && (kTile * kIn * 2) % 128 == 0, "operand tiles 128-byte aligned");
+
+// Backward CTAs: kBwdWG warpgroups, each with its own tile stream, a dZ tile
+// and three X buffers (each 128 samples x 64 features, 128-byte rows with
+// the 128-byte swizzle); then W^T of layers 1..4 (the B operand of dX, N =
+// in, K = out, K-major without swizzle), a block of 16 rows whose feature 0
+// is 1 (the bias rows of the weight gradients), the mbarriers and the TMEM
+// address. TMEM: 64 columns of dX per warpgroup, then the five dW^T
+// accumulators at kDwCol + zoff(l).
+constexpr int kBwdWG = 3;
+constexpr int kBwdBlk = kTile * 128;                            // 16 KB
+constexpr int kBwdWGBytes = 4 * kBwdBlk;                        // dZ tile + three X buffers
+__host__ __device__ constexpr int hoff1(int l) { return hoff(l) - hoff(1); }
+constexpr int kBwdWt = kBwdWG * kBwdWGBytes;
+constexpr int kBwdOnes = kBwdWt + 2 * hoff1(kLayers);
+constexpr int kBwdBar = kBwdOnes + 16 * 128;
+constexpr int kBwdBars = 5 + kLayers;                           // mbarriers per warpgroup
+constexpr int kBwdSmem = kBwdBar + kBwdWG * kBwdBars * 8 + 16 + 1024;   // + 1024-byte alignment of the base
+constexpr int kDwCol = kBwdWG * 64;
+static_assert(kBwdOnes % 1024 == 0, "the ones block keeps the 1024-byte swizzle alignment");
+static_assert(kBwdSmem <= 227 * 1024, "backward shared memory");
+static_assert(kDwCol + kZCols <= 512, "backward TMEM columns");
+static_assert(kHid == 64 && kIn > 64 && kIn <= 128 && kBiasCol(0) < kIn, "block plan");
 
 // W of every layer as the forward's B operand (out x 80), with the BF16 bias
 // in column kBiasCol(l) and zeros in the other columns past the inputs. Each
@@ -129,10 +145,10 @@ __device__ void load_weights_fwd(unsigned char* sm, const MlpView& V) {
     }
 }
 
-// W^T of every layer as the backward's B operand (8 loads in flight per thread).
+// W^T of layers 1..4 as the backward's B operand (8 loads in flight per thread).
 __device__ void load_weights_bwd(unsigned char* sm, const MlpView& V) {
     #pragma unroll
-    for (int l = 0; l < kLayers; ++l) {
+    for (int l = 1; l < kLayers; ++l) {
         const int I = lin(l), O = lout(l);
         const unsigned short* src = reinterpret_cast<const unsigned short*>(V.w16 + hoff(l));
         for (int e0 = threadIdx.x; e0 < I * O; e0 += 8 * blockDim.x) {
@@ -146,7 +162,7 @@ __device__ void load_weights_bwd(unsigned char* sm, const MlpView& V) {
             for (int u = 0; u < 8; ++u) {
                 const int e = e0 + u * blockDim.x, o = e / I, i = e % I;
                 if (e < I * O)
-                    *reinterpret_cast<unsigned short*>(sm + kSmBwdWt + 2 * hoff(l) + tc::tile_offset(i, o, I)) = v[u];
+                    *reinterpret_cast<unsigned short*>(sm + kBwdWt + 2 * hoff1(l) + tc::tile_offset(i, o, I)) = v[u];
             }
         }
     }
@@ -404,8 +420,9 @@ __global__ void __launch_bounds__(kTile * NW, Grouped ? 3 : 1) mlp_forward_kerne
                 #pragma unroll
                 for (int k = 0; k < kIn; ++k) f[k] = 0.0f;
             }
-            if (Train && valid) store_row_bf16(A.X + size_t(row) * kXCols, f, kIn);
             f[kBiasCol(0)] = 1.0f;
+            // X_0 keeps the constant 1 (the backward's bias row of dW_0)
+            if (Train && valid) store_row_bf16(A.X + size_t(row) * kXCols, f, kIn);
             #pragma unroll
             for (int k = 0; k < kIn; k += 8) tc::st_row8(act, kTile, t, k, f + k);
         }
@@ -502,284 +519,241 @@ __global__ void __launch_bounds__(kTile * NW, Grouped ? 3 : 1) mlp_forward_kerne
 struct BwdArgs {
     MlpView V;
     uint32_t count;
-    const __nv_bfloat16* X;       // [batch][kXCols]
-    __nv_bfloat16* dZ;            // [batch][kZCols]; the output layer's block is an input
+    float* partial;               // per CTA: kParams FP32 (weights and biases of every layer)
 };
-
-// dX_l = dZ_l W_l on the tensor cores (M = 128 samples, N = in, K = out),
-// dZ_{l-1} = dX_l * [X_l > 0], for l = 4 .. 1. Warpgroups as in the
-// forward. dZ stays packed BF16: the output block goes to the activation
-// tile as loaded, and each layer's dZ_{l-1} is written to the tile (the
-// chain that read it has completed) and to global memory eight columns at a
-// time as it is formed, so few values are live at once.
-template <int NW>
-__global__ void __launch_bounds__(kTile * NW, 1) mlp_backward_kernel(BwdArgs A) {
-    extern __shared__ __align__(1024) unsigned char sm[];
-    const int wg = int(threadIdx.x) / kTile;
-    const int t = int(threadIdx.x) % kTile, warp = t >> 5;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + bwd_bar(NW)) + wg;
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + bwd_bar(NW) + 56);
-    unsigned char* act = sm + bwd_act(wg);
-    load_weights_bwd(sm, A.V);
-    if (threadIdx.x < 32) tc::tmem_alloc(tslot, tmem_cols(NW));
-    if (t == 0) tc::mbar_init(bar, 1);
-    tc::fence_proxy_async();
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
-    const uint32_t tmem = *tslot + uint32_t(wg * 64);
-    const uint32_t trow = tmem + (uint32_t(warp * 32) << 16);
-    const uint32_t tiles = (A.count + kTile - 1) / kTile;
-    const uint32_t act_addr = tc::smem_addr(act);
-    const uint32_t wt_addr = tc::smem_addr(sm + kSmBwdWt);
-    auto wg_sync = [&]() { asm volatile("bar.sync %0, %1;" ::"r"(1 + wg), "r"(kTile) : "memory"); };
-    uint32_t phase = 0;
-    bool ok = true;
-    for (uint32_t tile = blockIdx.x * NW + wg; tile < tiles; tile += gridDim.x * NW) {
-        const uint32_t row = tile * kTile + t;
-        const bool valid = row < A.count;
-        {
-            const uint4* src = reinterpret_cast<const uint4*>(A.dZ + size_t(row) * kZCols + zoff(kLayers - 1));
-            #pragma unroll
-            for (int k = 0; k < kOut; k += 8)
-                *reinterpret_cast<uint4*>(act + tc::tile_offset(t, k, kTile)) =
-                    valid ? src[k / 8] : make_uint4(0, 0, 0, 0);
-        }
-        #pragma unroll
-        for (int l = kLayers - 1; l >= 1; --l) {
-            const int I = lin(l), O = lout(l);
-            tc::fence_proxy_async();
-            tc::fence_before_sync();
-            wg_sync();
-            if (t == 0) {
-                tc::fence_after_sync();
-                mma_chain(tmem, act_addr, wt_addr + 2 * hoff(l), O, I, bar);
-            }
-            // X_l (the input of layer l >= 1) is ReLU(Z_{l-1}): its mask gates dZ_{l-1};
-            // the row is fetched (packed) while the chain runs
-            uint4 xq[kHid / 8];
-            {
-                const uint4* src = reinterpret_cast<const uint4*>(A.X + size_t(row) * kXCols + xoff(l));
-                #pragma unroll
-                for (int k = 0; k < kHid / 8; ++k) xq[k] = valid ? src[k] : make_uint4(0, 0, 0, 0);
-            }
-            if (t == 0) ok = tc::mbar_wait(bar, phase) && ok;
-            wg_sync();
-            tc::fence_after_sync();
-            phase ^= 1u;
-            static_assert(kHid == 64, "dX is read as two 32-column loads");
-            uint4* zrow = reinterpret_cast<uint4*>(A.dZ + size_t(row) * kZCols + zoff(l - 1));
-            #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                float dx[32];
-                tc::tmem_ld32_wait(trow + uint32_t(h * 32), dx);
-                #pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    const uint4 xw = xq[h * 4 + c];
-                    const uint32_t w[4] = {xw.x, xw.y, xw.z, xw.w};
-                    uint32_t q[4];
-                    #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const float x0 = __uint_as_float(w[j] << 16), x1 = __uint_as_float(w[j] & 0xFFFF0000u);
-                        const float d0 = x0 > 0.0f ? dx[c * 8 + 2 * j] : 0.0f;
-                        const float d1 = x1 > 0.0f ? dx[c * 8 + 2 * j + 1] : 0.0f;
-                        q[j] = tc::pack_bf16(d0, d1);
-                    }
-                    const uint4 v = make_uint4(q[0], q[1], q[2], q[3]);
-                    *reinterpret_cast<uint4*>(act + tc::tile_offset(t, h * 32 + c * 8, kTile)) = v;
-                    if (valid) zrow[h * 4 + c] = v;
-                }
-            }
-            (void)I;
-        }
-    }
-    if (!ok && t == 0) atomicExch(A.V.error, 1);
-    tc::fence_before_sync();
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        tc::fence_after_sync();
-        tc::tmem_free(*tslot, tmem_cols(NW));
-    }
-}
-
-// ── weight gradients on the tensor cores ──────────────────────────────────
-// dW_l^T (in x out) = X_l^T dZ_l with the batch as the K dimension. A
-// persistent CTA owns a contiguous range of 32-sample steps. Both operands
-// are MN-major, so X and dZ need no transposition: one 2-D tensor copy (TMA)
-// of a box of 64 features x 32 samples puts 128 bytes of each sample's row
-// in shared memory with the 128-byte swizzle. A step is 11 such blocks: X
-// columns 0-63 and 64-127 (layer 0's 80 inputs; the rest are ignored rows),
-// each hidden layer's 64 inputs, and dZ in blocks of 64 columns (the last
-// one zero-filled past column 304). One thread issues a step's copies into
-// a stage and completes the stage's mbarrier with their bytes, four stages
-// deep, and issues the step's MMAs once the copies have landed.
-//
-// Layer l's A operand is 128 features: its input block and, 64 features
-// further, the next block. For a hidden layer that next block is a constant
-// block in shared memory whose feature 0 is 1 for every sample (the
-// descriptor's leading offset reaches it from any stage), so row 64 of the
-// product is db_l. Layer 0's second block holds inputs 64-79, so its bias is
-// a separate product (the constant block times dZ_0) in TMEM columns
-// kWgBiasCol... Layer l accumulates into TMEM columns zoff(l) .. + out over
-// all of the CTA's steps; the CTA then writes its FP32 partial gradient and
-// mlp_reduce_kernel sums the partials in CTA order. Samples past the batch
-// are the copies' zero fill.
-//
-// Operand layout (MN-major, 128-byte swizzle): a block is 32 rows (samples)
-// of 128 bytes (64 features); within each 1024-byte group of 8 rows, the
-// 16-byte chunk c of row r is stored at chunk c ^ (r % 8). Blocks of one
-// operand are LBO bytes apart along M/N, 8-row groups 1024 bytes (SBO)
-// apart along K; one MMA takes K = 16 (two groups).
-constexpr int kWgStep = 32;                                   // samples per step (K)
-constexpr int kWgStages = 4;
-constexpr int kWgBlock = kWgStep * 128;                       // one 64-feature block of a step
-constexpr int kWgXBlocks = 2 + (kLayers - 1);                 // X copies per step
-constexpr int kWgZBlocks = (kZCols + 63) / 64;                // dZ copies per step
-constexpr int kWgStage = (kWgXBlocks + kWgZBlocks) * kWgBlock;
-constexpr int kWgConst = kWgStages * kWgStage;                // two constant blocks (ones, zeros)
-constexpr int kSmWg = kWgConst + 2 * kWgBlock + 128 + 1024;   // + mbarriers, + 1024-byte alignment
-constexpr int kWgBiasCol = zoff(kLayers);                     // TMEM columns of layer 0's bias sums
-static_assert(kSmWg <= 227 * 1024, "wgrad stages exceed shared memory");
-static_assert(kHid == 64 && kIn > 64 && kIn < kTile, "block plan: 64 hidden units, 65..127 inputs");
-static_assert(kWgBiasCol + lout(0) <= 512, "wgrad TMEM columns");
-static_assert(kWgStage % 1024 == 0, "stages keep the 1024-byte swizzle alignment");
-// first X column of copy b of a step (16-byte aligned: x * 2 % 16 == 0)
-__host__ __device__ constexpr int wg_xcol(int b) { return b < 2 ? b * 64 : xoff(b - 1); }
-static_assert(wg_xcol(2) % 8 == 0 && wg_xcol(3) % 8 == 0 && wg_xcol(kWgXBlocks - 1) + 64 == kXCols, "X blocks");
-
-constexpr int kWgThreads = 128;                               // 4 warps read TMEM's 128 lanes
 
 // kind::f16 instruction descriptor with both operands MN-major.
 __host__ __device__ constexpr uint32_t idesc_bf16_mn(uint32_t M, uint32_t N) {
     return tc::idesc_bf16(M, N) | (1u << 15) | (1u << 16);
 }
 
-// Shared-memory descriptor with the 128-byte swizzle (layout type 2).
-__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-    return tc::smem_desc(addr, lbo, sbo) | (uint64_t(2) << 61);
+// Shared-memory descriptor with the 128-byte swizzle (layout type 2). The
+// operand's 8-row groups are 1024 bytes apart (SBO); for an MN-major operand
+// LBO is the distance to its next block of 64 features.
+__device__ __forceinline__ uint64_t desc_sw128(uint32_t addr, uint32_t lbo) {
+    return tc::smem_desc(addr, lbo, 1024) | (uint64_t(2) << 61);
 }
 
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int c0, int c1, uint64_t* bar) {
+// One 2-D tensor copy (box of 64 features x 128 samples) into shared memory,
+// completing `bar` with its bytes.
+__device__ __forceinline__ void tma_tile(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_addr(bar)),
+                 "r"(uint32_t(kBwdBlk))
+                 : "memory");
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-        ::"r"(tc::smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(tc::smem_addr(bar))
+        ::"r"(tc::smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(tc::smem_addr(bar))
         : "memory");
 }
 
-__global__ void __launch_bounds__(kWgThreads, 1) mlp_wgrad_kernel(const __grid_constant__ CUtensorMap mx,
-                                                            const __grid_constant__ CUtensorMap mz, uint32_t count,
-                                                            float* __restrict__ partial, int* error) {
+// Byte offset of 16-byte chunk c (features 8c .. 8c+7) of row r in a tile
+// with 128-byte rows and the 128-byte swizzle.
+__device__ __forceinline__ uint32_t sw_chunk(uint32_t r, uint32_t c) { return r * 128u + ((c ^ (r & 7u)) << 4); }
+
+// Backward pass and weight gradients of one training batch. Warpgroup g of
+// CTA b takes tiles b * kBwdWG + g, + gridDim.x * kBwdWG, ...; thread t of
+// a warpgroup owns sample t of the tile (TMEM lane t). Per tile:
+//   layer l = 4 .. 1: dX_l = dZ_l W_l into the warpgroup's TMEM columns and
+//     dW_l^T += X_l^T dZ_l into the CTA's accumulator; once both have
+//     completed, thread t forms dZ_{l-1} = dX_l * [X_l > 0] of its sample in
+//     place of dZ_l in the dZ tile;
+//   dW_0^T += X_0^T dZ_0.
+// Operands in shared memory (128-byte swizzle, rows of 128 bytes): the dZ
+// tile is the K-major A operand of dX (M = samples, K = out) and the
+// MN-major B operand of dW (N = out, K = samples); an X tile is the MN-major
+// A operand of dW (M = features, K = samples), its second block of 64
+// features the ones block (row 64 of the product is db_l); X_0's two blocks
+// give rows 0..127 with its constant-1 column 78 (db_0). X_l and dZ_4 come
+// by tensor copies: the tile's dZ_4, X_4, X_3, X_2 when the previous tile's
+// last product has completed, X_1 and X_0 into buffers the tile has
+// finished with. The CTA's dW accumulators are shared by its warpgroups;
+// their products are issued in tile order (warpgroup g's k-th tile is the
+// CTA's tile k * kBwdWG + g, and it waits until the product of the tile
+// before it has completed), so the sums do not depend on timing.
+__global__ void __launch_bounds__(kTile * kBwdWG, 1) mlp_backward_kernel(const __grid_constant__ CUtensorMap mx,
+                                                                   const __grid_constant__ CUtensorMap mz,
+                                                                   BwdArgs A) {
     extern __shared__ unsigned char sm_raw[];
     unsigned char* sm = sm_raw + ((1024u - (tc::smem_addr(sm_raw) & 1023u)) & 1023u);
-    unsigned char* cblk = sm + kWgConst;
-    uint64_t* full = reinterpret_cast<uint64_t*>(cblk + 2 * kWgBlock);   // copies of a stage landed
-    uint64_t* done = full + kWgStages;                                   // MMAs of a stage completed
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(done + kWgStages);
-    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-    const uint32_t steps = (count + kWgStep - 1) / kWgStep;
-    const uint32_t s_begin = uint32_t((uint64_t(blockIdx.x) * steps) / gridDim.x);
-    const uint32_t s_end = uint32_t((uint64_t(blockIdx.x + 1) * steps) / gridDim.x);
-    const uint32_t n = s_end - s_begin;
-    // constant blocks: the first has feature 0 (logical chunk 0, stored at
-    // chunk r % 8 of row r) = 1 in every row, the second is zero
-    for (int e = t; e < 2 * kWgBlock / 16; e += kWgThreads) {
+    const int wg = int(threadIdx.x) / kTile;
+    const int t = int(threadIdx.x) % kTile, warp = t >> 5;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kBwdBar);
+    uint64_t* act_full = bars + wg * kBwdBars;   // dZ_4 copied
+    uint64_t* buf_full = act_full + 1;           // X buffer 0..2 copied
+    uint64_t* mma_done = act_full + 4;           // the warpgroup's products completed
+    uint64_t* dw_done = act_full + 5;            // per layer: the warpgroup's dW product completed
+    // the warpgroup whose dW products come just before this one's
+    const int pred = (wg + kBwdWG - 1) % kBwdWG;
+    uint64_t* dw_pred = bars + pred * kBwdBars + 5;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + kBwdWG * kBwdBars);
+    unsigned char* act = sm + wg * kBwdWGBytes;
+    unsigned char* buf[3] = {act + kBwdBlk, act + 2 * kBwdBlk, act + 3 * kBwdBlk};
+    unsigned char* ones = sm + kBwdOnes;
+    load_weights_bwd(sm, A.V);
+    for (int e = threadIdx.x; e < 16 * 8; e += blockDim.x) {   // 16 rows x 8 chunks of 16 bytes
         const int r = e / 8, c = e % 8;
-        reinterpret_cast<uint4*>(cblk)[e] = make_uint4(r < kWgStep && c == (r & 7) ? 0x3F80u : 0u, 0u, 0u, 0u);
+        reinterpret_cast<uint4*>(ones)[e] = make_uint4(c == (r & 7) ? 0x3F80u : 0u, 0u, 0u, 0u);
     }
-    if (warp == 0) tc::tmem_alloc(tslot, 512);
-    if (t == 0) {
-        for (int k = 0; k < kWgStages; ++k) { tc::mbar_init(full + k, 1); tc::mbar_init(done + k, 1); }
+    if (threadIdx.x < 32) tc::tmem_alloc(tslot, 512);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < kBwdWG * kBwdBars; ++k) tc::mbar_init(bars + k, 1);
     }
     tc::fence_proxy_async();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *tslot;
+    const uint32_t tdx = tmem + uint32_t(wg * 64) + (uint32_t(warp * 32) << 16);
+    const uint32_t tiles = (A.count + kTile - 1) / kTile;
+    const uint32_t act_a = tc::smem_addr(act), ones_a = tc::smem_addr(ones);
+    const uint32_t buf_a[3] = {tc::smem_addr(buf[0]), tc::smem_addr(buf[1]), tc::smem_addr(buf[2])};
+    const uint32_t wt_a = tc::smem_addr(sm + kBwdWt);
+    auto wg_sync = [&]() { asm volatile("bar.sync %0, %1;" ::"r"(1 + wg), "r"(kTile) : "memory"); };
+    uint32_t ph_act = 0, ph_buf[3] = {0, 0, 0}, ph_mma = 0;
     bool ok = true;
-    if (t == 0) {
-        const CUtensorMap* pmx = &mx;
-        const CUtensorMap* pmz = &mz;
-        // the step's copies into stage j % kWgStages, completing full[j % kWgStages]
-        auto produce = [&](uint32_t j) {
-            const uint32_t k = j % kWgStages;
-            unsigned char* st = sm + k * kWgStage;
-            const int row = int((s_begin + j) * kWgStep);
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_addr(full + k)),
-                         "r"(uint32_t(kWgStage))
-                         : "memory");
-            #pragma unroll
-            for (int b = 0; b < kWgXBlocks; ++b) tma_load_2d(st + b * kWgBlock, pmx, wg_xcol(b), row, full + k);
-            #pragma unroll
-            for (int b = 0; b < kWgZBlocks; ++b)
-                tma_load_2d(st + (kWgXBlocks + b) * kWgBlock, pmz, b * 64, row, full + k);
-        };
-        const uint32_t ahead = min(n, uint32_t(kWgStages - 1));
-        for (uint32_t j = 0; j < ahead; ++j) produce(j);
-        const uint32_t ca = tc::smem_addr(cblk);
-        for (uint32_t i = 0; i < n; ++i) {
-            const uint32_t j = i + kWgStages - 1;
-            if (j < n) {
-                // stage j % kWgStages was last read by the MMAs of step i - 1
-                if (i >= 1) ok = tc::mbar_wait(done + (i - 1) % kWgStages, ((i - 1) / kWgStages) & 1u) && ok;
-                produce(j);
+    const uint32_t first = blockIdx.x * kBwdWG + wg, stride = gridDim.x * kBwdWG;
+    // the copies that open a tile: dZ_4, X_3, X_2 (X_4 goes ahead, as soon
+    // as buffer 0 is free)
+    auto open_tile = [&](uint32_t tile) {
+        const int y = int(tile * kTile);
+        tma_tile(act, &mz, zoff(kLayers - 1), y, act_full);
+        tma_tile(buf[1], &mx, xoff(3), y, buf_full + 1);
+        tma_tile(buf[2], &mx, xoff(2), y, buf_full + 2);
+    };
+    auto wait_buf = [&](int b) {
+        ok = tc::mbar_wait(buf_full + b, ph_buf[b]) && ok;
+        ph_buf[b] ^= 1u;
+    };
+    // the dW_l products of the warpgroup's k-th tile (the CTA's tile
+    // j = k kBwdWG + wg), after the CTA's tile j - 1 ones have completed: the
+    // predecessor's k-th (wg > 0) or (k-1)-th (wg = 0) completion. Each
+    // barrier gets one completion per tile of its warpgroup and a waiter has
+    // seen the one before, so a parity names exactly one completion.
+    auto issue_dw = [&](int l, uint32_t k, uint32_t j, uint32_t a0, uint32_t lbo_fixed) {
+        if (j > 0) ok = tc::mbar_wait(dw_pred + l, (wg > 0 ? k : k - 1) & 1u) && ok;
+        tc::fence_after_sync();
+        const uint32_t idesc = idesc_bf16_mn(kTile, uint32_t(lout(l)));
+        #pragma unroll
+        for (int ks = 0; ks < kTile / 16; ++ks) {
+            const uint32_t a = a0 + uint32_t(ks) * 2048u;
+            const uint32_t lbo = lbo_fixed ? lbo_fixed : ones_a - a;
+            tc::mma_bf16(tmem + uint32_t(kDwCol + zoff(l)), desc_sw128(a, lbo),
+                         desc_sw128(act_a + uint32_t(ks) * 2048u, 16u), idesc, j > 0 || ks > 0);
+        }
+    };
+    if (t == 0 && first < tiles) {
+        tma_tile(buf[0], &mx, xoff(4), int(first * kTile), buf_full + 0);
+        open_tile(first);
+    }
+    uint32_t k = 0;
+    for (uint32_t tile = first; tile < tiles; tile += stride, ++k) {
+        const uint32_t j = k * kBwdWG + uint32_t(wg);
+        const int y = int(tile * kTile);
+        #pragma unroll
+        for (int l = kLayers - 1; l >= 1; --l) {
+            const int b = l == 4 ? 0 : (l == 3 ? 1 : (l == 2 ? 2 : 0));
+            tc::fence_proxy_async();
+            tc::fence_before_sync();
+            wg_sync();
+            if (t == 0) {
+                tc::fence_after_sync();
+                // buffers this tile has finished with take X_1 and X_0
+                if (l == 3) tma_tile(buf[0], &mx, xoff(1), y, buf_full + 0);
+                if (l == 2) tma_tile(buf[1], &mx, 0, y, buf_full + 1);
+                if (l == 1) tma_tile(buf[2], &mx, 64, y, buf_full + 2);
+                if (l == kLayers - 1) {
+                    ok = tc::mbar_wait(act_full, ph_act) && ok;
+                    ph_act ^= 1u;
+                }
+                wait_buf(b);
+                tc::fence_after_sync();
+                const int O = lout(l);
+                const uint32_t idesc = tc::idesc_bf16(kTile, uint32_t(kHid));
+                const uint32_t wt = wt_a + uint32_t(2 * hoff1(l));
+                for (int s = 0; s < O / 16; ++s) {
+                    const uint64_t bd = tc::smem_desc(wt + s * 2 * (kHid / 8) * 128, (kHid / 8) * 128, 128);
+                    tc::mma_bf16(tmem + uint32_t(wg * 64), desc_sw128(act_a + uint32_t(s) * 32u, 16u), bd, idesc,
+                                 s > 0);
+                }
+                issue_dw(l, k, j, buf_a[b], 0u);
+                tc::mma_commit(mma_done);
+                tc::mma_commit(dw_done + l);
+                ok = tc::mbar_wait(mma_done, ph_mma) && ok;
             }
-            ok = tc::mbar_wait(full + i % kWgStages, (i / kWgStages) & 1u) && ok;
+            ph_mma ^= 1u;
+            wg_sync();
             tc::fence_after_sync();
-            const uint32_t sa = tc::smem_addr(sm + (i % kWgStages) * kWgStage);
-            const bool acc = i > 0;
+            // dZ_{l-1} of sample t, eight features at a time, in place of dZ_l
+            const unsigned char* xrow = buf[b];
             #pragma unroll
-            for (int l = 0; l < kLayers; ++l) {
-                const uint32_t a0 = sa + uint32_t(l == 0 ? 0 : l + 1) * kWgBlock;
-                const uint32_t lbo = l == 0 ? uint32_t(kWgBlock) : ca - a0;
-                const uint32_t b0 = sa + uint32_t(kWgXBlocks + l) * kWgBlock;
-                const uint32_t idesc = idesc_bf16_mn(kTile, uint32_t(lout(l)));
+            for (int h = 0; h < 2; ++h) {
+                float dx[32];
+                tc::tmem_ld32_wait(tdx + uint32_t(h * 32), dx);
                 #pragma unroll
-                for (int ks = 0; ks < kWgStep / 16; ++ks) {
-                    const uint64_t bd = smem_desc_sw128(b0 + ks * 2048, kWgBlock, 1024);
-                    tc::mma_bf16(tmem + uint32_t(zoff(l)), smem_desc_sw128(a0 + ks * 2048, lbo, 1024), bd, idesc,
-                                 acc || ks > 0);
-                    if (l == 0)
-                        tc::mma_bf16(tmem + uint32_t(kWgBiasCol), smem_desc_sw128(ca + ks * 2048, kWgBlock, 1024),
-                                     bd, idesc, acc || ks > 0);
+                for (int c = 0; c < 4; ++c) {
+                    const uint32_t off = sw_chunk(uint32_t(t), uint32_t(h * 4 + c));
+                    const uint4 xw = *reinterpret_cast<const uint4*>(xrow + off);
+                    const uint32_t w[4] = {xw.x, xw.y, xw.z, xw.w};
+                    uint32_t q[4];
+                    #pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const float x0 = __uint_as_float(w[e] << 16), x1 = __uint_as_float(w[e] & 0xFFFF0000u);
+                        const float d0 = x0 > 0.0f ? dx[c * 8 + 2 * e] : 0.0f;
+                        const float d1 = x1 > 0.0f ? dx[c * 8 + 2 * e + 1] : 0.0f;
+                        q[e] = tc::pack_bf16(d0, d1);
+                    }
+                    *reinterpret_cast<uint4*>(act + off) = make_uint4(q[0], q[1], q[2], q[3]);
                 }
             }
-            tc::mma_commit(done + i % kWgStages);
         }
-        // the last commit covers every earlier MMA of this thread
-        if (n > 0) ok = tc::mbar_wait(done + (n - 1) % kWgStages, ((n - 1) / kWgStages) & 1u) && ok;
+        // dW_0^T += X_0^T dZ_0 (X_0 in buffers 1 and 2)
+        tc::fence_proxy_async();
+        tc::fence_before_sync();
+        wg_sync();
+        if (t == 0) {
+            tc::fence_after_sync();
+            // buffer 0 (X_1) is done with: the next tile's X_4
+            if (tile + stride < tiles) tma_tile(buf[0], &mx, xoff(4), int((tile + stride) * kTile), buf_full + 0);
+            wait_buf(1);
+            wait_buf(2);
+            issue_dw(0, k, j, buf_a[1], buf_a[2] - buf_a[1]);
+            tc::mma_commit(mma_done);
+            tc::mma_commit(dw_done + 0);
+            ok = tc::mbar_wait(mma_done, ph_mma) && ok;
+            // every buffer of this warpgroup is free: the next tile's copies
+            if (tile + stride < tiles) open_tile(tile + stride);
+        }
+        ph_mma ^= 1u;
     }
+    // every product has completed (each warpgroup waited for its last one,
+    // and each dW product waited for the one before it); warpgroup g writes
+    // the partial gradient of layers g, g + kBwdWG
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    float* dst = partial + size_t(blockIdx.x) * kParams;
-    const int r = warp * 32 + lane;   // TMEM lane = row of dW^T = input feature (I = bias row)
+    float* dst = A.partial + size_t(blockIdx.x) * kParams;
+    const int r = t;   // TMEM lane = row of dW^T = input feature
     const uint32_t lanes = uint32_t(warp * 32) << 16;
     #pragma unroll
     for (int l = 0; l < kLayers; ++l) {
-        const int I = lin(l), O = lout(l);
+        if (l % kBwdWG != wg) continue;
+        const int I = lin(l), O = lout(l), bias = kBiasCol(l);
         #pragma unroll
         for (int c = 0; c < O; c += 16) {
             float v[16];
-            tc::tmem_ld16_wait(tmem + lanes + uint32_t(zoff(l) + c), v);
-            if (l == 0) {
-                float vb[16];
-                tc::tmem_ld16_wait(tmem + lanes + uint32_t(kWgBiasCol + c), vb);
-                #pragma unroll
-                for (int q = 0; q < 16; ++q)
-                    if (r == 0) dst[boff(0) + c + q] = n > 0 ? vb[q] : 0.0f;
-            }
+            tc::tmem_ld16_wait(tmem + lanes + uint32_t(kDwCol + zoff(l) + c), v);
             #pragma unroll
             for (int q = 0; q < 16; ++q) {
-                const float val = n > 0 ? v[q] : 0.0f;
-                if (r < I) dst[woff(l) + (c + q) * I + r] = val;
-                else if (l > 0 && r == I) dst[boff(l) + c + q] = val;
+                if (r == bias) dst[boff(l) + c + q] = v[q];
+                // layer 0's column kBiasCol(0) is the bias's place in the weight tile: no weight
+                if (r < I) dst[woff(l) + (c + q) * I + r] = r == bias ? 0.0f : v[q];
             }
         }
     }
-    if (!ok && error) atomicExch(error, 1);
+    if (!ok && t == 0) atomicExch(A.V.error, 1);
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) {
+    if (threadIdx.x < 32) {
         tc::fence_after_sync();
         tc::tmem_free(tmem, 512);
     }
@@ -887,7 +861,7 @@ struct rr_mlp_state {
     __nv_bfloat16* X = nullptr;
     __nv_bfloat16* dZ = nullptr;
     float* loss_partial = nullptr;
-    float* wpartial = nullptr;    // per wgrad CTA: kParams FP32
+    float* wpartial = nullptr;    // per backward CTA: kParams FP32
     double* wn_partial = nullptr; // per weight-norm block
     int wg_grid = 0;
     uint32_t batch_cap = 0;
@@ -950,9 +924,8 @@ rr_status rr_mlp_guide_init(rr_ctx* ctx, rr_guide* g) {
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, fwd_smem(kInferWG)));
     RR_TRY_CUDA(ctx, cudaFuncSetAttribute(mlp_forward_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           kSmFwd));
-    RR_TRY_CUDA(ctx, cudaFuncSetAttribute(mlp_backward_kernel<kBwdWG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          bwd_smem(kBwdWG)));
-    RR_TRY_CUDA(ctx, cudaFuncSetAttribute(mlp_wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmWg));
+    RR_TRY_CUDA(ctx, cudaFuncSetAttribute(mlp_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          kBwdSmem));
     return RR_OK;
 }
 
@@ -1048,15 +1021,15 @@ rr_status rr_mlp_guide_eval(rr_ctx* ctx, rr_guide* g, const float4* surf, float4
     return RR_OK;
 }
 
-// A [rows][cols] BF16 row-major array as a 2-D tensor for the weight
-// gradients' copies: box of 64 columns x kWgStep rows with the 128-byte
-// swizzle; columns and rows past the array read as zeros.
+// A [rows][cols] BF16 row-major array as a 2-D tensor for the backward's
+// copies: box of 64 columns x 128 rows with the 128-byte swizzle; columns
+// and rows past the array read as zeros.
 static bool operand_map(CUtensorMap* m, const void* base, uint32_t cols, uint32_t rows) {
     PFN_cuTensorMapEncodeTiled_v12000 enc = rr_tensor_map_encoder();
     if (!enc || (reinterpret_cast<uintptr_t>(base) & 15u) != 0 || rows == 0) return false;
     const cuuint64_t dims[2] = {cols, rows};
     const cuuint64_t strides[1] = {cuuint64_t(cols) * 2};
-    const cuuint32_t box[2] = {64, kWgStep};
+    const cuuint32_t box[2] = {64, kTile};
     const cuuint32_t estr[2] = {1, 1};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -1088,22 +1061,17 @@ rr_status rr_mlp_guide_train(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t 
     RR_TRY_CUDA(ctx, cudaMemsetAsync(M.loss_partial, 0, size_t(M.grid) * 4, stream));
     mlp_forward_kernel<true, false, kTrainWG><<<fgrid, kTile * kTrainWG, fwd_smem(kTrainWG), stream>>>(A);
     RR_CHECK_LAUNCH(ctx);
-    BwdArgs Bw{};
-    Bw.V = A.V;
-    Bw.count = B;
-    Bw.X = M.X;
-    Bw.dZ = M.dZ;
-    const int bgrid = int(std::min<uint32_t>((tiles + kBwdWG - 1) / kBwdWG, uint32_t(ctx->sm_count)));
-    mlp_backward_kernel<kBwdWG><<<bgrid, kTile * kBwdWG, bwd_smem(kBwdWG), stream>>>(Bw);
-    RR_CHECK_LAUNCH(ctx);
-    const uint32_t wsteps = (B + kWgStep - 1) / kWgStep;
-    const int wgrid = int(std::min<uint32_t>(wsteps, uint32_t(M.wg_grid)));
     CUtensorMap mx, mz;
     if (!operand_map(&mx, M.X, kXCols, B) || !operand_map(&mz, M.dZ, kZCols, B))
         return rr_fail(ctx, RR_ERR_CUDA, "rr_mlp_guide_train: tensor map encoding failed");
-    mlp_wgrad_kernel<<<wgrid, kWgThreads, kSmWg, stream>>>(mx, mz, B, M.wpartial, M.error);
+    BwdArgs Bw{};
+    Bw.V = A.V;
+    Bw.count = B;
+    Bw.partial = M.wpartial;
+    const int bgrid = int(std::min<uint32_t>((tiles + kBwdWG - 1) / kBwdWG, uint32_t(M.wg_grid)));
+    mlp_backward_kernel<<<bgrid, kTile * kBwdWG, kBwdSmem, stream>>>(mx, mz, Bw);
     RR_CHECK_LAUNCH(ctx);
-    mlp_reduce_kernel<<<(kParams + 255) / 256, 256, 0, stream>>>(M.wpartial, uint32_t(wgrid), M.grad);
+    mlp_reduce_kernel<<<(kParams + 255) / 256, 256, 0, stream>>>(M.wpartial, uint32_t(bgrid), M.grad);
     RR_CHECK_LAUNCH(ctx);
     M.steps += 1;
     const float bc1 = 1.0f - std::pow(0.9f, float(M.steps));
@@ -1112,7 +1080,7 @@ rr_status rr_mlp_guide_train(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t 
                                                                g->desc.learning_rate, bc1, bc2);
     RR_CHECK_LAUNCH(ctx);
     RR_TRY_CUDA(ctx, cudaMemcpyAsync(M.loss_host, M.loss_partial, size_t(M.grid) * 4, cudaMemcpyDeviceToHost, stream));
-    ctx->launches += 11;
+    ctx->launches += 10;
     return RR_OK;
 }
 

@@ -92,11 +92,15 @@ def _direction_samples(rng, N, axis):
     return pos, om, nrm, wo, w
 
 
-def test_mlp_gradient_matches_fp64(rr, ctx, torch_cuda):
+@pytest.mark.parametrize("N", [2000, 148 * 32 * 9 + 17])
+def test_mlp_gradient_matches_fp64(rr, ctx, torch_cuda, N):
+    """N = 2000: one 32-sample step per weight-gradient CTA, a ragged last
+    step; 42,641: about nine steps per CTA, so every one of the four copy
+    stages is reused twice (mbarrier phases flip) and the last step is
+    ragged again."""
     import mlp_ref
     torch = torch_cuda
     rng = np.random.default_rng(5)
-    N = 2000
     g = make_guide(rr, ctx, rr.GUIDE_MLP, batch=N, max_samples=N)
     params = (rng.normal(size=mlp_ref.PARAM_COUNT) * 0.1).astype(np.float32)
     ctx.check(rr.lib().rr_guide_mlp_params(ctx.handle, g, None, None, params.ctypes.data, rr.MLP_PARAM_COUNT, None))
@@ -134,8 +138,19 @@ def test_mlp_gradient_matches_fp64(rr, ctx, torch_cuda):
     st = rr.GuideStats()
     ctx.check(rr.lib().rr_guide_get_stats(ctx.handle, g, C.byref(st)))
     assert st.last_loss == pytest.approx(loss, rel=0.05)
-    del keep
+    # a second guide with the same parameters and samples gets the same
+    # gradient bits: the warpgroups' shared weight-gradient sums run in a
+    # fixed order
+    g2 = make_guide(rr, ctx, rr.GUIDE_MLP, batch=N, max_samples=N)
+    ctx.check(rr.lib().rr_guide_mlp_params(ctx.handle, g2, None, None, params.ctypes.data, rr.MLP_PARAM_COUNT, None))
+    keep2 = set_samples(rr, ctx, torch, g2, pos, om, w, nrm, wo)
+    ctx.check(rr.lib().rr_guide_update(ctx.handle, g2, _stream(torch)))
+    grad2 = np.zeros(mlp_ref.PARAM_COUNT, np.float32)
+    ctx.check(rr.lib().rr_guide_mlp_params(ctx.handle, g2, None, grad2.ctypes.data, None, rr.MLP_PARAM_COUNT, None))
+    assert np.array_equal(grad.view(np.uint32), grad2.view(np.uint32))
+    del keep, keep2
     rr.lib().rr_guide_destroy(g)
+    rr.lib().rr_guide_destroy(g2)
 
 
 def test_mlp_training_lowers_loss(rr, ctx, torch_cuda):
