@@ -248,7 +248,8 @@ rr_status rr_batch_get_mode(const rr_batch* batch, int* mode_out);
  * order, as image_count reference frames would (the first with the given
  * camera_moved flag). oracle_sum (nullable, double[4*W*H]) keeps the FP64
  * per-pixel sum of every folded image (reset together with the FP32 mean),
- * the judge buffer for RMSE; it is the only FP64 state of the path. */
+ * the judge buffer for RMSE; it is the only FP64 state of the path.
+ * width * height must be below 2^30 (RR_ERR_INVALID_ARGUMENT otherwise). */
 typedef struct rr_acc_params {
     uint32_t width;
     uint32_t height;

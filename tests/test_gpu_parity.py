@@ -183,14 +183,15 @@ def test_accumulate_bit_exact_and_fp64(rr, O, ctx, torch_cuda):
     torch = torch_cuda
     rng = np.random.default_rng(5)
     W, H = 33, 17
-    frames = rng.random((6, H, W, 4)).astype(np.float32) * 3
+    frames = rng.random((43, H, W, 4)).astype(np.float32) * 3
     acc_o = np.zeros((H, W, 4), np.float32)
     acc_g = torch.zeros((H, W, 4), device="cuda")
     sum64 = torch.zeros((H, W, 4), device="cuda", dtype=torch.float64)
     fr = torch.from_numpy(frames).cuda()
     spp = 0
-    # one frame with camera_moved, then batches of 2 and 3 frames
-    for start, count, moved in ((0, 1, 1), (1, 2, 0), (3, 3, 0)):
+    # one frame with camera_moved, then batches of 2, 3 and 37 frames (the
+    # kernel reads 16 images at a time: 37 crosses two of those boundaries)
+    for start, count, moved in ((0, 1, 1), (1, 2, 0), (3, 3, 0), (6, 37, 0)):
         for k in range(count):
             O.accumulate(np.ascontiguousarray(frames[start + k]), acc_o, moved if k == 0 else 0, spp + k)
         p = rr.AccParams(W, H, moved, spp)
