@@ -362,41 +362,97 @@ __global__ void __launch_bounds__(kBlock, 4) guided_shade_kernel(DevScene s0, Gu
     }
 }
 
-// One training sample per recorded vertex whose continuation was traced.
-__global__ void __launch_bounds__(kBlock) resolve_kernel(const float4* __restrict__ out, const float4* __restrict__ rec0,
-                                                         const float4* __restrict__ rec1, const float4* __restrict__ rec2,
-                                                         const float4* __restrict__ rec3, uint32_t paths,
-                                                         uint32_t bounces, GuideSamples S) {
-    const uint64_t total = uint64_t(paths) * bounces;
-    for (uint64_t k = uint64_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u); k < total;
-         k += uint64_t(gridDim.x) * blockDim.x) {
-        const uint64_t r = k + lane_id();
-        bool emit = false;
+// One training sample per recorded vertex whose continuation was traced:
+// record r (bounce r / paths, path r % paths) gives a sample when its
+// continuation brought back positive radiance.
+__device__ __forceinline__ bool resolve_record(const float4* __restrict__ out, const float4* __restrict__ rec0,
+                                               const float4* __restrict__ rec1, const float4* __restrict__ rec2,
+                                               const float4* __restrict__ rec3, uint32_t paths, uint32_t r,
+                                               float4& s0, float4& s1, float4& s2, float4& s3) {
+    const float4 c = rec2[r];
+    const float before = c.w;
+    if (!(before >= 0.0f)) return false;   // NaN (never filled) fails this test
+    const float4 a = rec0[r], b = rec1[r];
+    const uint32_t pid = r % paths;
+    const float final_l = lum709(xyz(out[pid]));
+    const float lin = mx(final_l - before, 0.0f) / mx(b.w, 1e-20f);
+    const float w = lin / a.w;
+    if (!(w > 0.0f && w < 3.0e38f)) return false;
+    s0 = make_float4(a.x, a.y, a.z, w);
+    s1 = make_float4(b.x, b.y, b.z, __uint_as_float(r));
+    s2 = make_float4(c.x, c.y, c.z, 0.0f);
+    const float4 d = rec3[r];
+    s3 = make_float4(d.x, d.y, d.z, 0.0f);
+    return true;
+}
+
+// The samples are compacted in record order, without a shared counter: tile
+// t of kResolveTile records counts its samples (resolve_count_kernel), an
+// exclusive scan turns the counts into the tiles' first slots, and
+// resolve_write_kernel writes each tile's samples from there, round by round
+// (kResolveItems rounds of kBlock consecutive records; within a round, warp
+// by warp and lane by lane). The sample order, and so everything trained
+// from it, does not depend on timing.
+constexpr uint32_t kResolveItems = 8;
+constexpr uint32_t kResolveTile = kBlock * kResolveItems;
+
+__global__ void __launch_bounds__(kBlock) resolve_count_kernel(const float4* __restrict__ out,
+                                                               const float4* __restrict__ rec0,
+                                                               const float4* __restrict__ rec1,
+                                                               const float4* __restrict__ rec2,
+                                                               const float4* __restrict__ rec3, uint32_t paths,
+                                                               uint32_t total, uint32_t* __restrict__ tile_count) {
+    __shared__ uint32_t red[kBlock / 32];
+    uint32_t n = 0;
+    #pragma unroll 2
+    for (uint32_t k = 0; k < kResolveItems; ++k) {
+        const uint32_t r = blockIdx.x * kResolveTile + k * kBlock + threadIdx.x;
         float4 s0, s1, s2, s3;
-        if (r < total) {
-            const float4 c = rec2[r];
-            const float before = c.w;
-            if (before >= 0.0f) {  // NaN (never filled) fails this test
-                const float4 a = rec0[r], b = rec1[r];
-                const uint32_t pid = uint32_t(r % paths);
-                const float final_l = lum709(xyz(out[pid]));
-                const float lin = mx(final_l - before, 0.0f) / mx(b.w, 1e-20f);
-                const float w = lin / a.w;
-                if (w > 0.0f && w < 3.0e38f) {
-                    emit = true;
-                    s0 = make_float4(a.x, a.y, a.z, w);
-                    s1 = make_float4(b.x, b.y, b.z, __uint_as_float(uint32_t(r)));
-                    s2 = make_float4(c.x, c.y, c.z, 0.0f);
-                    const float4 d = rec3[r];
-                    s3 = make_float4(d.x, d.y, d.z, 0.0f);
-                }
-            }
+        if (r < total && resolve_record(out, rec0, rec1, rec2, rec3, paths, r, s0, s1, s2, s3)) ++n;
+    }
+    #pragma unroll
+    for (int off = 16; off > 0; off >>= 1) n += __shfl_xor_sync(kFull, n, off);
+    if (lane_id() == 0) red[threadIdx.x >> 5] = n;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < kBlock / 32; ++w) t += red[w];
+        tile_count[blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) resolve_write_kernel(const float4* __restrict__ out,
+                                                               const float4* __restrict__ rec0,
+                                                               const float4* __restrict__ rec1,
+                                                               const float4* __restrict__ rec2,
+                                                               const float4* __restrict__ rec3, uint32_t paths,
+                                                               uint32_t total, const uint32_t* __restrict__ tile_first,
+                                                               GuideSamples S) {
+    __shared__ uint32_t wcount[kBlock / 32];
+    const uint32_t w = threadIdx.x >> 5;
+    uint32_t base = tile_first[blockIdx.x];
+    for (uint32_t k = 0; k < kResolveItems; ++k) {
+        const uint32_t r = blockIdx.x * kResolveTile + k * kBlock + threadIdx.x;
+        float4 s0, s1, s2, s3;
+        const bool emit = r < total && resolve_record(out, rec0, rec1, rec2, rec3, paths, r, s0, s1, s2, s3);
+        const uint32_t bal = __ballot_sync(kFull, emit);
+        if (lane_id() == 0) wcount[w] = __popc(bal);
+        __syncthreads();
+        uint32_t before = 0, all = 0;
+        for (uint32_t v = 0; v < kBlock / 32; ++v) {
+            const uint32_t c = wcount[v];
+            before += v < w ? c : 0u;
+            all += c;
         }
-        const uint32_t slot = warp_alloc(emit, S.count);
+        const uint32_t slot = base + before + __popc(bal & ((1u << lane_id()) - 1u));
         if (emit && slot < S.capacity) {
             S.s0[slot] = s0; S.s1[slot] = s1; S.s2[slot] = s2; S.s3[slot] = s3;
         }
+        base += all;
+        __syncthreads();
     }
+    // the last tile knows the total
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) S.count[0] = base;
 }
 
 // ── guided batches ─────────────────────────────────────────────────────────
@@ -835,8 +891,17 @@ static rr_status ensure_records(rr_ctx* ctx, rr_guide* g, size_t paths, uint32_t
     const size_t need = paths * bounces;
     if (g->rec_capacity >= need) return RR_OK;
     for (int k = 0; k < 4; ++k) { cudaFree(g->rec[k]); g->rec[k] = nullptr; }
+    cudaFree(g->resolve_first);
+    cudaFree(g->resolve_sums);
+    g->resolve_first = g->resolve_sums = nullptr;
     g->rec_capacity = 0;
+    if (need >= (size_t(1) << 32))
+        return rr_fail(ctx, RR_ERR_UNSUPPORTED, "guided execute: paths x bounces must be below 2^32");
     for (int k = 0; k < 4; ++k) RR_TRY_CUDA(ctx, cudaMalloc(&g->rec[k], need * sizeof(float4)));
+    // the resolve's per-tile counts / first slots and its scan's chunk sums
+    const size_t tiles = (need + kResolveTile - 1) / kResolveTile + 1;
+    RR_TRY_CUDA(ctx, cudaMalloc(&g->resolve_first, tiles * sizeof(uint32_t)));
+    RR_TRY_CUDA(ctx, cudaMalloc(&g->resolve_sums, (tiles / kScanChunk + 2) * sizeof(uint32_t)));
     g->rec_capacity = need;
     return RR_OK;
 }
@@ -938,11 +1003,17 @@ extern "C" rr_status rr_guided_pathtracer_execute(rr_ctx* ctx, const rr_scene* s
         launches += 3;
     }
     if (overlap) RR_TRY_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->shadowed[p->max_bounces - 1], 0));
-    if (p->max_bounces > 1) {
-        resolve_kernel<<<std::max(1, ctx->sm_count * 8), kBlock, 0, stream>>>(
-            out, g->rec[0], g->rec[1], g->rec[2], g->rec[3], uint32_t(n), p->max_bounces - 1, g->samples);
+    const uint32_t total = p->max_bounces > 1 ? uint32_t(n * (p->max_bounces - 1)) : 0u;
+    if (total > 0) {
+        const uint32_t tiles = (total + kResolveTile - 1) / kResolveTile;
+        resolve_count_kernel<<<tiles, kBlock, 0, stream>>>(out, g->rec[0], g->rec[1], g->rec[2], g->rec[3],
+                                                          uint32_t(n), total, g->resolve_first);
         RR_CHECK_LAUNCH(ctx);
-        launches += 1;
+        scan_exclusive(g->resolve_first, g->resolve_first, tiles, g->resolve_sums, stream);
+        resolve_write_kernel<<<tiles, kBlock, 0, stream>>>(out, g->rec[0], g->rec[1], g->rec[2], g->rec[3],
+                                                          uint32_t(n), total, g->resolve_first, g->samples);
+        RR_CHECK_LAUNCH(ctx);
+        launches += 5;
     }
     ctx->launches += launches;
     ctx->last_max_bounces = p->max_bounces;

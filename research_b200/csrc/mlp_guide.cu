@@ -873,6 +873,8 @@ struct rr_mlp_state {
 
 rr_guide::~rr_guide() {
     for (int k = 0; k < 4; ++k) cudaFree(rec[k]);
+    cudaFree(resolve_first);
+    cudaFree(resolve_sums);
     cudaFree(mlp_surf);
     cudaFree(mlp_mix);
     if (mlp) cudaFreeHost(mlp->loss_host);

@@ -72,6 +72,8 @@ struct rr_guide {
     uint32_t* count_host = nullptr;   // pinned: the sample count read back by an update
     float4* rec[4] = {nullptr, nullptr, nullptr, nullptr};
     size_t rec_capacity = 0;
+    uint32_t* resolve_first = nullptr;  // per resolve tile: its sample count, then its first slot
+    uint32_t* resolve_sums = nullptr;   // chunk sums of the resolve's scan
     uint32_t frame_paths = 0;
     // grid
     rr::GridView grid;
