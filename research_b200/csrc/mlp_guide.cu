@@ -789,7 +789,8 @@ __global__ void __launch_bounds__(256) mlp_adam_kernel(float* __restrict__ param
 
 // Batch weight normalisation (clamp = 20 x mean, then 1 / sum of clamped
 // weights), as two fixed-order reductions: block b sums the batch slice
-// [b n / G, (b+1) n / G) in FP64, then one thread adds the G partials in order.
+// [b n / G, (b+1) n / G) in FP64, then one warp adds the G partials in a
+// fixed order.
 constexpr int kWnBlocks = 148;
 __global__ void __launch_bounds__(256) mlp_wsum_kernel(GuideSamples S, const uint32_t* __restrict__ sel, uint32_t n,
                                                        const double* __restrict__ wnorm, bool clamped,
@@ -813,10 +814,15 @@ __global__ void __launch_bounds__(256) mlp_wsum_kernel(GuideSamples S, const uin
     if (t == 0) partial[blockIdx.x] = red[0];
 }
 
-__global__ void mlp_wfinish_kernel(const double* __restrict__ partial, uint32_t parts, uint32_t n, bool clamped,
-                                   double* __restrict__ wnorm) {
+// One warp: lane l adds partials l, l + 32, ... in order, then the lanes'
+// sums are combined by a fixed butterfly (the same order every run).
+__global__ void __launch_bounds__(32) mlp_wfinish_kernel(const double* __restrict__ partial, uint32_t parts,
+                                                         uint32_t n, bool clamped, double* __restrict__ wnorm) {
     double s = 0.0;
-    for (uint32_t c = 0; c < parts; ++c) s += partial[c];
+    for (uint32_t c = threadIdx.x; c < parts; c += 32) s += partial[c];
+    #pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (threadIdx.x != 0) return;
     if (!clamped) wnorm[0] = 20.0 * (s / double(n > 0 ? n : 1));
     else wnorm[1] = s > 0.0 ? 1.0 / s : 0.0;
 }
@@ -1045,9 +1051,9 @@ rr_status rr_mlp_guide_train(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t 
     mlp_select_kernel<<<(B + 255) / 256, 256, 0, stream>>>(M.sel, B, n, (M.steps * 7919u) % n);
     RR_CHECK_LAUNCH(ctx);
     mlp_wsum_kernel<<<kWnBlocks, 256, 0, stream>>>(g->samples, M.sel, B, M.wnorm, false, M.wn_partial);
-    mlp_wfinish_kernel<<<1, 1, 0, stream>>>(M.wn_partial, kWnBlocks, B, false, M.wnorm);
+    mlp_wfinish_kernel<<<1, 32, 0, stream>>>(M.wn_partial, kWnBlocks, B, false, M.wnorm);
     mlp_wsum_kernel<<<kWnBlocks, 256, 0, stream>>>(g->samples, M.sel, B, M.wnorm, true, M.wn_partial);
-    mlp_wfinish_kernel<<<1, 1, 0, stream>>>(M.wn_partial, kWnBlocks, B, true, M.wnorm);
+    mlp_wfinish_kernel<<<1, 32, 0, stream>>>(M.wn_partial, kWnBlocks, B, true, M.wnorm);
     RR_CHECK_LAUNCH(ctx);
     FwdArgs A{};
     A.V = rr_mlp_guide_view(g);

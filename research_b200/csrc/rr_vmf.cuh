@@ -1,6 +1,6 @@
 // rr_vmf.cuh — von Mises-Fisher lobe sampling and density
-// (GuidingGrid.slang:160-189), shared by the hash-grid guide and the guided
-// path tracer's mixture guides.
+// (GuidingGrid.slang:160-189) for the hash-grid guide and the grid guide's EM,
+// and the guided path tracer's mixtures (fast forms, below).
 #pragma once
 
 #include "rr_dev.cuh"
@@ -85,10 +85,35 @@ struct VmfMixture {
     float weight[kMaxLobes];
 };
 
+// The guided tracer's mixtures (no reference counterpart) use the same vMF
+// formulas with the hardware approximations (__expf, __logf, __sincosf,
+// __fdividef) instead of the deterministic functions the reference-parity
+// paths need: the guided estimator only needs the density it evaluates to
+// be the one it samples, and both use these forms. Per lobe the density is
+// w_j k_j e^{k_j (mu_j.dir - 1)} / (2 pi (1 - e^{-2 k_j})).
+RR_D float vmf_pdf_fast(float3 mu, float kappa, float3 dir) {
+    const float k = mx(kappa, 1.0e-3f);
+    const float w = clampf(dot(mu, dir), -1.0f, 1.0f);
+    const float denom = kTwoPi * (1.0f - __expf(-2.0f * k));
+    return __fdividef(k * __expf(k * (w - 1.0f)), mx(denom, 1.0e-8f));
+}
+
+RR_D float3 vmf_sample_fast(float3 mu, float kappa, float ux, float uy) {
+    const float k = mx(kappa, 1.0e-3f);
+    float w = 1.0f + __fdividef(__logf(ux + (1.0f - ux) * __expf(-2.0f * k)), k);
+    w = clampf(w, -1.0f, 1.0f);
+    const float s = sqrtf(mx(0.0f, 1.0f - w * w));
+    float sp, cp;
+    __sincosf(kTwoPi * uy, &sp, &cp);
+    float3 T, B;
+    build_onb(mu, T, B);
+    return tangent_to_world(f3(s * cp, s * sp, w), T, B, mu);
+}
+
 RR_D float mixture_pdf(const VmfMixture& m, int lobes, float3 dir) {
     float p = 0.0f;
     for (int j = 0; j < lobes; ++j)
-        if (m.weight[j] > 0.0f) p += m.weight[j] * vmf_pdf(xyz(m.lobe[j]), m.lobe[j].w, dir);
+        if (m.weight[j] > 0.0f) p += m.weight[j] * vmf_pdf_fast(xyz(m.lobe[j]), m.lobe[j].w, dir);
     return p;
 }
 
@@ -102,8 +127,7 @@ RR_D float3 mixture_sample(const VmfMixture& m, int lobes, float u_pick, float u
         c += m.weight[k];
         if (u_pick < c) break;
     }
-    float pdf;
-    return vmf_sample(xyz(m.lobe[j]), m.lobe[j].w, ux, uy, pdf);
+    return vmf_sample_fast(xyz(m.lobe[j]), m.lobe[j].w, ux, uy);
 }
 
 } // namespace rr
