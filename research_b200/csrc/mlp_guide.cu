@@ -570,7 +570,9 @@ __device__ __forceinline__ uint32_t sw_chunk(uint32_t r, uint32_t c) { return r 
 // their products are issued in tile order (warpgroup g's k-th tile is the
 // CTA's tile k * kBwdWG + g, and it waits until the product of the tile
 // before it has completed), so the sums do not depend on timing.
-__global__ void __launch_bounds__(kTile * kBwdWG, 1) mlp_backward_kernel(const __grid_constant__ CUtensorMap mx,
+// kTile * kBwdWG threads, one CTA per SM (its shared memory and TMEM);
+// registers capped at 128 (no spills).
+__global__ void __maxnreg__(128) mlp_backward_kernel(const __grid_constant__ CUtensorMap mx,
                                                                    const __grid_constant__ CUtensorMap mz,
                                                                    BwdArgs A) {
     extern __shared__ unsigned char sm_raw[];
