@@ -420,9 +420,7 @@ __global__ void __launch_bounds__(kTile * NW, Grouped ? 3 : 1) mlp_forward_kerne
                 #pragma unroll
                 for (int k = 0; k < kIn; ++k) f[k] = 0.0f;
             }
-            f[kBiasCol(0)] = 1.0f;
-            // X_0 keeps the constant 1 (the backward's bias row of dW_0)
-            if (Train && valid) store_row_bf16(A.X + size_t(row) * kXCols, f, kIn);
+            f[kBiasCol(0)] = 1.0f;   // X_0 keeps it too (the backward's bias row of dW_0)
             #pragma unroll
             for (int k = 0; k < kIn; k += 8) tc::st_row8(act, kTile, t, k, f + k);
         }
@@ -436,6 +434,27 @@ __global__ void __launch_bounds__(kTile * NW, Grouped ? 3 : 1) mlp_forward_kerne
             if (t == 0) {
                 tc::fence_after_sync();
                 mma_chain(tmem, act_addr, w_addr + fwd_wtile(l), kIn, O, bar);
+            }
+            if constexpr (Train) {
+                // X_l (this layer's input, now complete in the tile) to global
+                // memory while the chain runs, by the warpgroup together: a
+                // warp store covers 8 rows x 4 chunks of 16 bytes (64
+                // contiguous bytes per row); chunk c of row r is at
+                // c * 2048 + r * 16 in the tile, so a warp's reads touch
+                // every bank once per chunk.
+                constexpr int kRowBlocks = kTile / 8;
+                const int chunks = l == 0 ? kIn / 8 : kHid / 8;
+                const int groups = kRowBlocks * ((chunks + 3) / 4);
+                const int lane = t & 31;
+                for (int g = warp; g < groups; g += kTile / 32) {
+                    const int r = (g % kRowBlocks) * 8 + (lane & 7);
+                    const int c = (g / kRowBlocks) * 4 + (lane >> 3);
+                    const uint32_t xr = tile * kTile + uint32_t(r);
+                    if (c < chunks && xr < count) {
+                        const uint4 v = *reinterpret_cast<const uint4*>(act + tc::tile_offset(r, c * 8, kTile));
+                        *reinterpret_cast<uint4*>(A.X + size_t(xr) * kXCols + xoff(l) + c * 8) = v;
+                    }
+                }
             }
             if (t == 0) ok = tc::mbar_wait(bar, phase) && ok;
             wg_sync();
@@ -452,12 +471,11 @@ __global__ void __launch_bounds__(kTile * NW, Grouped ? 3 : 1) mlp_forward_kerne
                 *reinterpret_cast<uint4*>(act + tc::tile_offset(t, kHid + 8, kTile)) = make_uint4(0u, 0u, 0u, 0u);
             }
             if (l + 1 < kLayers) {
-                // ReLU in the BF16 conversion; the same words go to the activation
-                // tile and (training) to X. The chain that read the tile has
-                // completed (mbarrier), so each thread may overwrite its row; the
-                // barrier before the next chain orders every thread's TMEM reads
-                // before that chain's writes.
-                uint4* xrow = reinterpret_cast<uint4*>(A.X + size_t(row) * kXCols + xoff(l + 1));
+                // ReLU in the BF16 conversion, into the activation tile. The
+                // chain that read the tile has completed (mbarrier), so each
+                // thread may overwrite its row; the barrier before the next
+                // chain orders every thread's TMEM reads before that chain's
+                // writes.
                 #pragma unroll
                 for (int k = 0; k < O; k += 8) {
                     const uint4 q = make_uint4(tc::pack_bf16_relu(out[k], out[k + 1]),
@@ -465,7 +483,6 @@ __global__ void __launch_bounds__(kTile * NW, Grouped ? 3 : 1) mlp_forward_kerne
                                                tc::pack_bf16_relu(out[k + 4], out[k + 5]),
                                                tc::pack_bf16_relu(out[k + 6], out[k + 7]));
                     *reinterpret_cast<uint4*>(act + tc::tile_offset(t, k, kTile)) = q;
-                    if (Train && valid) xrow[k / 8] = q;
                 }
             }
         }
