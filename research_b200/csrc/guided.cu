@@ -520,9 +520,11 @@ __global__ void __launch_bounds__(kBlock) guided_surface_batch_kernel(const DevS
     }
 }
 
-// resolve_kernel over the records of every scene of a batch: record k of
-// the batch is record k - rec_prefix[g] of scene g (the last g with
-// rec_prefix[g] <= k); samples go to that scene's guide.
+// The resolve over the records of every scene of a batch: record k of the
+// batch is record k - rec_prefix[g] of scene g (the last g with
+// rec_prefix[g] <= k); samples go to that scene's guide through its
+// counter, in an order that depends on timing (the single-scene resolve
+// above compacts in record order).
 __global__ void __launch_bounds__(kBlock) resolve_batch_kernel(const GuideEntry* __restrict__ gtab,
                                                                float4* const* __restrict__ outs,
                                                                const unsigned long long* __restrict__ rec_prefix,
