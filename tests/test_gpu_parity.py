@@ -179,10 +179,12 @@ def test_pathtracer_region_odd_size(rr, O, ctx, torch_cuda, cornell):
     np.testing.assert_array_equal(g.view(np.uint32), o.view(np.uint32))
 
 
-def test_accumulate_bit_exact_and_fp64(rr, O, ctx, torch_cuda):
+@pytest.mark.parametrize("W,H", [(33, 17), (640, 480)])
+def test_accumulate_bit_exact_and_fp64(rr, O, ctx, torch_cuda, W, H):
+    """33 x 17: one thread per channel (small images); 640 x 480 (307,200
+    pixels): one thread per pixel."""
     torch = torch_cuda
     rng = np.random.default_rng(5)
-    W, H = 33, 17
     frames = rng.random((43, H, W, 4)).astype(np.float32) * 3
     acc_o = np.zeros((H, W, 4), np.float32)
     acc_g = torch.zeros((H, W, 4), device="cuda")
