@@ -24,19 +24,112 @@ __global__ void __launch_bounds__(256) normalize_kernel(const float4* __restrict
     out[i] = make_float4(v.x, v.y, v.z, 0.0f);
 }
 
-// `nrm`: unit normals (from normalize_kernel)
-__global__ void __launch_bounds__(128) atrous_kernel(const float4* __restrict__ in,
-                                                     const float4* __restrict__ gpos,
-                                                     const float4* __restrict__ nrm,
-                                                     float4* __restrict__ out, int W, int H, int stride,
-                                                     float sp2, float sn2, float sl2) {
+// Direct-load filter, one iteration in two launches. A pixel's tap on a
+// neighbour has the same weight as the neighbour's opposite tap on the pixel
+// (tap_weight), so the 24 neighbour weights of every pixel need only 12
+// evaluations, each with three divisions and three exponentials:
+//   atrous_pair_weights_kernel: for every pixel, the weights of its 12
+//     forward taps (kPairFwd: (1,0), (2,0), then ty = 1, 2 with tx = -2..2),
+//     on the clamped neighbour, -1 where either pixel is a G-buffer miss,
+//     into 12 planes of W x H floats;
+//   atrous_pair_sum_kernel: every pixel's 25 taps in atrous_pixel's order;
+//     a forward tap reads its own weight, a backward tap whose neighbour is
+//     in the image reads the neighbour's forward weight, and the centre and
+//     backward taps clamped at the border are evaluated on the spot.
+// The sums see the same weights in the same order as atrous_pixel: the
+// same bits. `nrm`: unit normals (from normalize_kernel).
+constexpr int kPairFwd = 12;
+RR_D int2 pair_offset(int j) { return j < 2 ? make_int2(j + 1, 0) : make_int2((j - 2) % 5 - 2, (j - 2) / 5 + 1); }
+RR_D bool pair_forward(int tx, int ty) { return ty > 0 || (ty == 0 && tx > 0); }
+RR_D int pair_index(int tx, int ty) { return ty == 0 ? tx - 1 : 2 + (ty - 1) * 5 + (tx + 2); }
+
+__global__ void __launch_bounds__(128) atrous_pair_weights_kernel(const float4* __restrict__ in,
+                                                                  const float4* __restrict__ gpos,
+                                                                  const float4* __restrict__ nrm,
+                                                                  float* __restrict__ wt, int W, int H, int stride,
+                                                                  float sp2, float sn2, float sl2) {
     const int x = blockIdx.x * 16 + (threadIdx.x & 15);
     const int y = blockIdx.y * 8 + (threadIdx.x >> 4);
     if (x >= W || y >= H) return;
-    out[size_t(y) * W + x] = atrous_pixel(GlobalFetch{in, gpos, nrm, W}, x, y, W, H, stride, sp2, sn2, sl2);
+    const size_t plane = size_t(W) * H;
+    const size_t i = size_t(y) * W + x;
+    const float4 cpos = __ldg(gpos + i);
+    if (cpos.w < 0.0f) {
+        #pragma unroll
+        for (int j = 0; j < kPairFwd; ++j) wt[j * plane + i] = -1.0f;
+        return;
+    }
+    const float3 cn = xyz(__ldg(nrm + i));
+    const float cl = luminance601(xyz(__ldg(in + i)));
+    #pragma unroll
+    for (int j = 0; j < kPairFwd; ++j) {
+        const int2 o = pair_offset(j);
+        const int sx = min(max(x + o.x * stride, 0), W - 1);
+        const int sy = min(max(y + o.y * stride, 0), H - 1);
+        const size_t k = size_t(sy) * W + sx;
+        const float4 spos = __ldg(gpos + k);
+        float w = -1.0f;
+        if (!(spos.w < 0.0f))
+            w = tap_weight(o.x, o.y, xyz(cpos), cn, cl, xyz(spos), xyz(__ldg(nrm + k)), xyz(__ldg(in + k)), sp2, sn2,
+                           sl2);
+        wt[j * plane + i] = w;
+    }
 }
 
-// TMA-staged form of atrous_kernel for strides 1, 2 and 4: a block of 32 x 8
+__global__ void __launch_bounds__(128) atrous_pair_sum_kernel(const float4* __restrict__ in,
+                                                              const float4* __restrict__ gpos,
+                                                              const float4* __restrict__ nrm,
+                                                              const float* __restrict__ wt,
+                                                              float4* __restrict__ out, int W, int H, int stride,
+                                                              float sp2, float sn2, float sl2) {
+    const int x = blockIdx.x * 16 + (threadIdx.x & 15);
+    const int y = blockIdx.y * 8 + (threadIdx.x >> 4);
+    if (x >= W || y >= H) return;
+    const size_t plane = size_t(W) * H;
+    const size_t i = size_t(y) * W + x;
+    const float4 cpos = __ldg(gpos + i);
+    const float4 crad = __ldg(in + i);
+    if (cpos.w < 0.0f) {
+        out[i] = crad;
+        return;
+    }
+    const float3 cn = xyz(__ldg(nrm + i));
+    const float cl = luminance601(xyz(crad));
+    float3 filtered = f3(0.0f, 0.0f, 0.0f);
+    float wsum = 0.0f;
+    #pragma unroll
+    for (int ty = -2; ty <= 2; ++ty) {
+        const int uy = y + ty * stride;
+        const int sy = min(max(uy, 0), H - 1);
+        #pragma unroll
+        for (int tx = -2; tx <= 2; ++tx) {
+            const int ux = x + tx * stride;
+            const int sx = min(max(ux, 0), W - 1);
+            const size_t k = size_t(sy) * W + sx;
+            float w;
+            if (tx == 0 && ty == 0) {
+                w = tap_weight(0, 0, xyz(cpos), cn, cl, xyz(cpos), cn, xyz(crad), sp2, sn2, sl2);
+            } else if (pair_forward(tx, ty)) {
+                w = __ldg(wt + pair_index(tx, ty) * plane + i);
+            } else if (ux == sx && uy == sy) {
+                w = __ldg(wt + pair_index(-tx, -ty) * plane + k);
+            } else {
+                const float4 spos = __ldg(gpos + k);
+                w = spos.w < 0.0f ? -1.0f
+                                  : tap_weight(tx, ty, xyz(cpos), cn, cl, xyz(spos), xyz(__ldg(nrm + k)),
+                                               xyz(__ldg(in + k)), sp2, sn2, sl2);
+            }
+            if (w < 0.0f) continue;   // a G-buffer miss
+            const float3 srad = xyz(__ldg(in + k));
+            filtered = filtered + srad * w;
+            wsum += w;
+        }
+    }
+    const float3 o = wsum > 0.0f ? filtered / wsum : xyz(crad);
+    out[i] = make_float4(o.x, o.y, o.z, crad.w);
+}
+
+// TMA-staged form of the filter for strides 1, 2 and 4: a block of 32 x 8
 // output pixels first loads its halo tile (the 5x5 taps reach 2*S pixels
 // beyond the block on every side) of radiance, position and unit normal
 // with three 3-D tensor copies (cp.async.bulk.tensor, box (4 floats,
@@ -224,12 +317,24 @@ static rr_status atrous_launch(rr_ctx* ctx, const float* input, const float* gpo
             return RR_OK;
         }
     }
+    const size_t need = size_t(rr::kPairFwd) * W * H;
+    if (ctx->atrous_wt_floats < need) {
+        cudaFree(ctx->atrous_wt);
+        ctx->atrous_wt = nullptr;
+        ctx->atrous_wt_floats = 0;
+        RR_TRY_CUDA(ctx, cudaMalloc(&ctx->atrous_wt, need * sizeof(float)));
+        ctx->atrous_wt_floats = need;
+    }
     dim3 grid((W + 15) / 16, (H + 7) / 8);
-    rr::atrous_kernel<<<grid, 128, 0, stream>>>(
-        reinterpret_cast<const float4*>(input), reinterpret_cast<const float4*>(gpos), nrm,
+    rr::atrous_pair_weights_kernel<<<grid, 128, 0, stream>>>(
+        reinterpret_cast<const float4*>(input), reinterpret_cast<const float4*>(gpos), nrm, ctx->atrous_wt, int(W),
+        int(H), int(stride), sp2, sn2, sl2);
+    RR_CHECK_LAUNCH(ctx);
+    rr::atrous_pair_sum_kernel<<<grid, 128, 0, stream>>>(
+        reinterpret_cast<const float4*>(input), reinterpret_cast<const float4*>(gpos), nrm, ctx->atrous_wt,
         reinterpret_cast<float4*>(output), int(W), int(H), int(stride), sp2, sn2, sl2);
     RR_CHECK_LAUNCH(ctx);
-    ctx->launches += 1;
+    ctx->launches += 2;
     return RR_OK;
 }
 

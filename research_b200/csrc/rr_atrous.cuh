@@ -12,6 +12,23 @@ namespace rr {
 RR_D float luminance601(float3 c) { return dot(c, f3(0.299f, 0.587f, 0.114f)); }
 RR_D float kernel_weight(int o) { return (o == 2 || o == -2) ? 1.0f : ((o == 1 || o == -1) ? 4.0f : 6.0f); }
 
+// The weight of tap (tx, ty) of a centre pixel (position cp, unit normal cn,
+// luminance cl) on a neighbour (sp, sn, srad). Every factor is the same bits
+// with the two pixels swapped and (tx, ty) negated: (-d).(-d) = d.d,
+// dot(a, b) = dot(b, a) term by term, (-l)^2 = l^2, and the B3 weights are
+// symmetric; atrous_pair_weights_kernel relies on it.
+RR_D float tap_weight(int tx, int ty, float3 cp, float3 cn, float cl, float3 sp, float3 sn, float3 srad, float sp2,
+                      float sn2, float sl2) {
+    const float base_w = (kernel_weight(tx) * kernel_weight(ty)) / 256.0f;
+    const float3 pd = sp - cp;
+    const float pos_w = rr_expf(-dot(pd, pd) / sp2);
+    const float nd = mx(0.0f, 1.0f - dot(cn, sn));
+    const float normal_w = rr_expf(-nd / sn2);
+    const float ld = luminance601(srad) - cl;
+    const float luma_w = rr_expf(-(ld * ld) / sl2);
+    return base_w * pos_w * normal_w * luma_w;
+}
+
 // One output pixel of atrous.slang:cs_main (atrous.slang:41-106) at stride
 // `stride`, reading the three images through `f` (global memory or a tile
 // in shared memory: the same values, so the same bits either way).
@@ -32,16 +49,8 @@ RR_D float4 atrous_pixel(const Fetch& f, int x, int y, int W, int H, int stride,
             const int sx = min(max(x + tx * stride, 0), W - 1);
             const float4 spos = f.pos(sx, sy);
             if (spos.w < 0.0f) continue;
-            const float base_w = (kernel_weight(tx) * kernel_weight(ty)) / 256.0f;
-            const float3 pd = xyz(spos) - xyz(cpos);
-            const float pos_w = rr_expf(-dot(pd, pd) / sp2);
-            const float3 sn = xyz(f.nrm(sx, sy));
-            const float nd = mx(0.0f, 1.0f - dot(cn, sn));
-            const float normal_w = rr_expf(-nd / sn2);
             const float3 srad = xyz(f.rad(sx, sy));
-            const float ld = luminance601(srad) - cl;
-            const float luma_w = rr_expf(-(ld * ld) / sl2);
-            const float w = base_w * pos_w * normal_w * luma_w;
+            const float w = tap_weight(tx, ty, xyz(cpos), cn, cl, xyz(spos), xyz(f.nrm(sx, sy)), srad, sp2, sn2, sl2);
             filtered = filtered + srad * w;
             wsum += w;
         }

@@ -58,6 +58,8 @@ struct rr_ctx {
     double* mse_partial = nullptr;         // rr_image_mse block partials
     float4* atrous_nrm = nullptr;          // A-trous: the G-buffer normals, normalized once per call
     size_t atrous_nrm_px = 0;
+    float* atrous_wt = nullptr;            // A-trous: the forward tap weights of every pixel (12 planes)
+    size_t atrous_wt_floats = 0;
     bool atrous_tma = true;                // strides 1, 2, 4 through TMA-staged tiles
     int* atrous_error = nullptr;           // host-mapped word, set when a tile's copies missed the bounded wait
     int* atrous_error_dev = nullptr;       // its device address

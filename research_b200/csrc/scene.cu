@@ -90,6 +90,7 @@ rr_status rr_ctx_destroy(rr_ctx* ctx) {
     cudaFree(ctx->work64);
     cudaFree(ctx->mse_partial);
     cudaFree(ctx->atrous_nrm);
+    cudaFree(ctx->atrous_wt);
     if (ctx->atrous_error) cudaFreeHost(ctx->atrous_error);
     for (int b = 0; b < kMaxBounces; ++b) {
         if (ctx->shaded[b]) cudaEventDestroy(ctx->shaded[b]);

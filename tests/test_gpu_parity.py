@@ -305,8 +305,12 @@ def test_room_1m_frame_bit_exact(rr, O, ctx, torch_cuda, room_1m):
     assert (o[-1][2][..., 3].view(np.uint32) > 32).any()   # temporal history was merged
 
 
+@pytest.mark.parametrize("tma", [1, 0])
 @pytest.mark.parametrize("iterations", [1, 5, 7])
-def test_atrous_bit_exact(rr, O, ctx, torch_cuda, procedural, iterations):
+def test_atrous_bit_exact(rr, O, ctx, torch_cuda, procedural, iterations, tma):
+    """tma 1: TMA tiles for strides 1, 2, 4, the pair-weight kernels beyond;
+    tma 0: the pair-weight kernels at every stride (up to 64 on a 72 x 40
+    image: taps clamped on every side)."""
     torch = torch_cuda
     _, scene, oscene = procedural
     cam = cam_for(rr, "procedural", 72, 40)
@@ -322,9 +326,14 @@ def test_atrous_bit_exact(rr, O, ctx, torch_cuda, procedural, iterations):
     ping = [torch.empty_like(tin), torch.empty_like(tin)]
     ap = rr.AtrousParams(W, H, iterations, 0, 0.25, 0.20, 1.0, 0)
     slot = C.c_uint32()
-    ctx.check(rr.lib().rr_atrous_execute(ctx.handle, tin.data_ptr(), tp.data_ptr(), tn.data_ptr(), ping[0].data_ptr(),
-                                         ping[1].data_ptr(), C.byref(ap), C.byref(slot), _stream(torch)))
-    torch.cuda.synchronize()
+    ctx.check(rr.lib().rr_atrous_set_tma(ctx.handle, tma))
+    try:
+        ctx.check(rr.lib().rr_atrous_execute(ctx.handle, tin.data_ptr(), tp.data_ptr(), tn.data_ptr(),
+                                             ping[0].data_ptr(), ping[1].data_ptr(), C.byref(ap), C.byref(slot),
+                                             _stream(torch)))
+        torch.cuda.synchronize()
+    finally:
+        ctx.check(rr.lib().rr_atrous_set_tma(ctx.handle, 1))
     assert slot.value == (min(iterations, 7) - 1) & 1
     np.testing.assert_array_equal(_np(ping[slot.value]).view(np.uint32), ref.view(np.uint32))
 
