@@ -67,12 +67,14 @@ __global__ void __launch_bounds__(128) atrous_pair_weights_kernel(const float4* 
         const int sx = min(max(x + o.x * stride, 0), W - 1);
         const int sy = min(max(y + o.y * stride, 0), H - 1);
         const size_t k = size_t(sy) * W + sx;
+        // the neighbour's three values are loaded whether or not it is a miss
+        // (the address is in the image), so the loads of all taps can be in
+        // flight together
         const float4 spos = __ldg(gpos + k);
-        float w = -1.0f;
-        if (!(spos.w < 0.0f))
-            w = tap_weight(o.x, o.y, xyz(cpos), cn, cl, xyz(spos), xyz(__ldg(nrm + k)), xyz(__ldg(in + k)), sp2, sn2,
-                           sl2);
-        wt[j * plane + i] = w;
+        const float3 sn = xyz(__ldg(nrm + k));
+        const float3 srad = xyz(__ldg(in + k));
+        const float w = tap_weight(o.x, o.y, xyz(cpos), cn, cl, xyz(spos), sn, srad, sp2, sn2, sl2);
+        wt[j * plane + i] = spos.w < 0.0f ? -1.0f : w;
     }
 }
 
@@ -119,10 +121,12 @@ __global__ void __launch_bounds__(128) atrous_pair_sum_kernel(const float4* __re
                                   : tap_weight(tx, ty, xyz(cpos), cn, cl, xyz(spos), xyz(__ldg(nrm + k)),
                                                xyz(__ldg(in + k)), sp2, sn2, sl2);
             }
-            if (w < 0.0f) continue;   // a G-buffer miss
+            // loaded before the weight is known (the address is in the image)
             const float3 srad = xyz(__ldg(in + k));
-            filtered = filtered + srad * w;
-            wsum += w;
+            if (!(w < 0.0f)) {   // w < 0: a G-buffer miss
+                filtered = filtered + srad * w;
+                wsum += w;
+            }
         }
     }
     const float3 o = wsum > 0.0f ? filtered / wsum : xyz(crad);
