@@ -47,10 +47,13 @@ RR_D float4 atrous_pixel(const Fetch& f, int x, int y, int W, int H, int stride,
         #pragma unroll
         for (int tx = -2; tx <= 2; ++tx) {
             const int sx = min(max(x + tx * stride, 0), W - 1);
+            // the tap's values are read before its miss test (the address is
+            // in the image), so the taps' loads can be in flight together
             const float4 spos = f.pos(sx, sy);
-            if (spos.w < 0.0f) continue;
             const float3 srad = xyz(f.rad(sx, sy));
-            const float w = tap_weight(tx, ty, xyz(cpos), cn, cl, xyz(spos), xyz(f.nrm(sx, sy)), srad, sp2, sn2, sl2);
+            const float3 sn = xyz(f.nrm(sx, sy));
+            if (spos.w < 0.0f) continue;
+            const float w = tap_weight(tx, ty, xyz(cpos), cn, cl, xyz(spos), sn, srad, sp2, sn2, sl2);
             filtered = filtered + srad * w;
             wsum += w;
         }
