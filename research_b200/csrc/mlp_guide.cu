@@ -1088,8 +1088,16 @@ rr_status rr_mlp_guide_train(rr_ctx* ctx, rr_guide* g, uint32_t n, cudaStream_t 
     RR_TRY_CUDA(ctx, cudaMemsetAsync(M.loss_partial, 0, size_t(M.grid) * 4, stream));
     mlp_forward_kernel<true, false, kTrainWG><<<fgrid, kTile * kTrainWG, fwd_smem(kTrainWG), stream>>>(A);
     RR_CHECK_LAUNCH(ctx);
+    // The backward's copies are boxes of kTile rows; a batch of fewer rows
+    // is mapped as kTile rows whose tail is zeroed here (the buffers hold
+    // at least kTile rows), larger ones read zeros past the batch.
+    const uint32_t map_rows = std::max(B, uint32_t(kTile));
+    if (B < map_rows) {
+        RR_TRY_CUDA(ctx, cudaMemsetAsync(M.X + size_t(B) * kXCols, 0, size_t(map_rows - B) * kXCols * 2, stream));
+        RR_TRY_CUDA(ctx, cudaMemsetAsync(M.dZ + size_t(B) * kZCols, 0, size_t(map_rows - B) * kZCols * 2, stream));
+    }
     CUtensorMap mx, mz;
-    if (!operand_map(&mx, M.X, kXCols, B) || !operand_map(&mz, M.dZ, kZCols, B))
+    if (!operand_map(&mx, M.X, kXCols, map_rows) || !operand_map(&mz, M.dZ, kZCols, map_rows))
         return rr_fail(ctx, RR_ERR_CUDA, "rr_mlp_guide_train: tensor map encoding failed");
     BwdArgs Bw{};
     Bw.V = A.V;

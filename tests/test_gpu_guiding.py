@@ -92,12 +92,13 @@ def _direction_samples(rng, N, axis):
     return pos, om, nrm, wo, w
 
 
-@pytest.mark.parametrize("N", [2000, 148 * 32 * 9 + 17])
+@pytest.mark.parametrize("N", [100, 2000, 148 * 32 * 9 + 17])
 def test_mlp_gradient_matches_fp64(rr, ctx, torch_cuda, N):
-    """N = 2000: one 32-sample step per weight-gradient CTA, a ragged last
-    step; 42,641: about nine steps per CTA, so every one of the four copy
-    stages is reused twice (mbarrier phases flip) and the last step is
-    ragged again."""
+    """N = 100: less than one 128-sample tile (the backward's copies map a
+    zeroed tail); 2000: a ragged last tile, one or two tiles per
+    warpgroup; 42,641: several tiles per warpgroup, so the dW products of
+    the CTA's warpgroups are chained over many tiles, and a ragged last
+    tile."""
     import mlp_ref
     torch = torch_cuda
     rng = np.random.default_rng(5)
