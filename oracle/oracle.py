@@ -76,6 +76,7 @@ _SIG = {
     "oracle_restir_di_temporal": (None, [P, P, C.POINTER(DIParams), P, P, P, P, I]),
     "oracle_restir_di_spatial_shade": (None, [P, P, C.POINTER(DIParams), P, P, P, P, I]),
     "oracle_atrous_iteration": (None, [P, P, P, P, U32, U32, U32, F32, F32, F32, I]),
+    "oracle_atrous_tap_weight": (F32, [P, P, F32, P, P, P, I, I, F32, F32, F32]),
     "oracle_guiding_cell_index": (U32, [P, U32, P, C.POINTER(GuidingParams)]),
     "oracle_guiding_splat": (None, [P, P, P, P, C.c_size_t, P, C.POINTER(GuidingParams)]),
     "oracle_guiding_fit": (None, [P, P, C.POINTER(GuidingParams)]),

@@ -1492,6 +1492,25 @@ void oracle_restir_di_spatial_shade(const OracleScene* s, const GpuCameraData* c
     });
 }
 
+// The weight of tap (tx, ty) of a centre pixel (position cp, unit normal cn,
+// luminance cl) on a neighbour (sp, sn, radiance srad) (atrous.slang:70-95).
+inline float atrous_tap_weight(int tx, int ty, V3 cp, V3 cn, float cl, V3 sp, V3 sn, V3 srad, float sigma_pos_sq,
+                               float sigma_norm_sq, float sigma_luma_sq) {
+    float base_w = (kernel_weight(tx) * kernel_weight(ty)) / 256.0f;
+    V3 pd = sp - cp;
+    float pos_w = rr_expf(-dot(pd, pd) / sigma_pos_sq);
+    float nd = fmaxs(0.0f, 1.0f - dot(cn, sn));
+    float normal_w = rr_expf(-nd / sigma_norm_sq);
+    float ld = luminance601(srad) - cl;
+    float luma_w = rr_expf(-(ld * ld) / sigma_luma_sq);
+    return base_w * pos_w * normal_w * luma_w;
+}
+
+float oracle_atrous_tap_weight(const float cp[3], const float cn[3], float cl, const float sp[3], const float sn[3],
+                               const float srad[3], int tx, int ty, float sp2, float sn2, float sl2) {
+    return atrous_tap_weight(tx, ty, load3(cp), load3(cn), cl, load3(sp), load3(sn), load3(srad), sp2, sn2, sl2);
+}
+
 void oracle_atrous_iteration(const float* input, const float* gpos, const float* gnrm, float* output,
                              uint32_t width, uint32_t height, uint32_t stride_u, float sp, float sn,
                              float sl, int threads) {
@@ -1518,15 +1537,9 @@ void oracle_atrous_iteration(const float* input, const float* gpos, const float*
                     int sy = std::min(std::max((int)y + ty * stride, 0), my);
                     const size_t j = ((size_t)sy * width + sx) * 4;
                     if (gpos[j + 3] < 0.0f) continue;
-                    float base_w = (kernel_weight(tx) * kernel_weight(ty)) / 256.0f;
-                    V3 pd = load3(gpos + j) - load3(cpos);
-                    float pos_w = rr_expf(-dot(pd, pd) / sigma_pos_sq);
-                    V3 sn3 = normalize(load3(gnrm + j));
-                    float nd = fmaxs(0.0f, 1.0f - dot(center_normal, sn3));
-                    float normal_w = rr_expf(-nd / sigma_norm_sq);
-                    float ld = luminance601(load3(input + j)) - center_luma;
-                    float luma_w = rr_expf(-(ld * ld) / sigma_luma_sq);
-                    float weight = base_w * pos_w * normal_w * luma_w;
+                    float weight = atrous_tap_weight(tx, ty, load3(cpos), center_normal, center_luma,
+                                                     load3(gpos + j), normalize(load3(gnrm + j)),
+                                                     load3(input + j), sigma_pos_sq, sigma_norm_sq, sigma_luma_sq);
                     filtered = filtered + load3(input + j) * weight;
                     weight_sum += weight;
                 }

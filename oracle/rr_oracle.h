@@ -133,6 +133,11 @@ void oracle_restir_di_spatial_shade(const OracleScene* scene, const GpuCameraDat
                                     float* output, int threads);
 
 /* ── A-trous (atrous.slang:41-106) ──────────────────────────────────────── */
+/* One tap's weight (the loop of oracle_atrous_iteration): centre position,
+ * unit normal and luminance, neighbour position, unit normal and radiance,
+ * tap offset, squared sigmas. */
+float oracle_atrous_tap_weight(const float cp[3], const float cn[3], float cl, const float sp[3], const float sn[3],
+                               const float srad[3], int tx, int ty, float sp2, float sn2, float sl2);
 void oracle_atrous_iteration(const float* input, const float* gbuf_pos,
                              const float* gbuf_norm, float* output,
                              uint32_t width, uint32_t height, uint32_t stride,

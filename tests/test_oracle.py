@@ -129,6 +129,39 @@ def test_atrous_flat_image_is_fixed_point(O):
     np.testing.assert_allclose(out, inp, rtol=1e-6)
 
 
+def test_atrous_tap_weight_is_symmetric(O):
+    """A pixel's tap on a neighbour weighs the same, bit for bit, as the
+    neighbour's opposite tap on the pixel (what the pair-weight A-trous
+    kernels rely on): random positions (small and far apart), unit normals,
+    radiances over six decades, every offset, the library's default and
+    extreme sigmas."""
+    import ctypes as C
+    lib = O.lib()
+    rng = np.random.default_rng(17)
+    fp = lambda a: np.ascontiguousarray(a, np.float32).ctypes.data_as(C.c_void_p)
+    lum = lambda c: np.float32(np.float32(np.float32(c[0] * np.float32(0.299)) + np.float32(c[1] * np.float32(0.587)))
+                               + np.float32(c[2] * np.float32(0.114)))
+    n = 0
+    for sig in ((0.25, 0.20, 1.0), (1e-3, 1e-3, 1e-3), (40.0, 3.0, 50.0)):
+        sp2, sn2, sl2 = (max(np.float32(v) * np.float32(v), np.float32(1e-6)) for v in sig)
+        for _ in range(400):
+            scale = 10.0 ** rng.uniform(-3, 3)
+            p, q = (rng.normal(size=3) * scale).astype(np.float32), (rng.normal(size=3) * scale).astype(np.float32)
+            np_, nq = rng.normal(size=3), rng.normal(size=3)
+            np_ = (np_ / np.linalg.norm(np_)).astype(np.float32)
+            nq = (nq / np.linalg.norm(nq)).astype(np.float32)
+            rp = (10.0 ** rng.uniform(-3, 3, 3)).astype(np.float32)
+            rq = (10.0 ** rng.uniform(-3, 3, 3)).astype(np.float32)
+            lp, lq = lum(rp), lum(rq)
+            for ty in range(-2, 3):
+                for tx in range(-2, 3):
+                    a = lib.oracle_atrous_tap_weight(fp(p), fp(np_), lp, fp(q), fp(nq), fp(rq), tx, ty, sp2, sn2, sl2)
+                    b = lib.oracle_atrous_tap_weight(fp(q), fp(nq), lq, fp(p), fp(np_), fp(rp), -tx, -ty, sp2, sn2, sl2)
+                    assert np.float32(a).view(np.uint32) == np.float32(b).view(np.uint32), (a, b, tx, ty)
+                    n += 1
+    assert n == 3 * 400 * 25
+
+
 def test_atrous_kernel_weights_sum_to_one():
     k = np.array([1, 4, 6, 4, 1], np.float32)
     assert (np.outer(k, k) / 256.0).sum() == 1.0
