@@ -581,17 +581,17 @@ __device__ __forceinline__ uint32_t sw_chunk(uint32_t r, uint32_t c) { return r 
 // A operand of dW (M = features, K = samples), its second block of 64
 // features the ones block (row 64 of the product is db_l); X_0's two blocks
 // give rows 0..127 with its constant-1 column 78 (db_0). X_l and dZ_4 come
-// by tensor copies: the tile's dZ_4, X_4, X_3, X_2 when the previous tile's
-// last product has completed, X_1 and X_0 into buffers the tile has
-// finished with. The CTA's dW accumulators are shared by its warpgroups;
+// by tensor copies: the tile's X_4 once the previous tile's layer-1 step is
+// done with buffer 0, its dZ_4, X_3, X_2 when the previous tile's last
+// product has completed, X_1 and X_0 into buffers the tile has finished
+// with. The CTA's dW accumulators are shared by its warpgroups;
 // their products are issued in tile order (warpgroup g's k-th tile is the
 // CTA's tile k * kBwdWG + g, and it waits until the product of the tile
 // before it has completed), so the sums do not depend on timing.
 // kTile * kBwdWG threads, one CTA per SM (its shared memory and TMEM);
 // registers capped at 128 (no spills).
 __global__ void __maxnreg__(128) mlp_backward_kernel(const __grid_constant__ CUtensorMap mx,
-                                                                   const __grid_constant__ CUtensorMap mz,
-                                                                   BwdArgs A) {
+                                                     const __grid_constant__ CUtensorMap mz, BwdArgs A) {
     extern __shared__ unsigned char sm_raw[];
     unsigned char* sm = sm_raw + ((1024u - (tc::smem_addr(sm_raw) & 1023u)) & 1023u);
     const int wg = int(threadIdx.x) / kTile;
